@@ -1,0 +1,207 @@
+"""Python mirror of the reference's bem3_aw_qd2.h API over the native library.
+
+    case = Case.from_files(pw, periodicity, medium, mesh)   # read_aqd2 + initialize_aqd2
+    case.solve()                                             # solve_bieq_aqd2 (on the GPU)
+    F, N = case.force(type=0)                                # force_FN_aqd2
+    case.dat_write("out.dat")                                # dat_write_aqd2
+
+Everything below the ctypes calls runs in lib/libbem3_aw_qd2.so (C host
+code) and lib/libbemgpu.so (CUDA kernels + C ABI, include/bemgpu.h).  There
+is no Python or CPU implementation of the compute: if the native library is
+missing, importing this module fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+_host = None
+_gpu = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+
+
+def libs():
+    """Load lib/libbemgpu.so and lib/libbem3_aw_qd2.so (raises if absent)."""
+    global _host, _gpu
+    if _host is None:
+        gpath = os.path.join(LIBDIR, "libbemgpu.so")
+        hpath = os.path.join(LIBDIR, "libbem3_aw_qd2.so")
+        if not (os.path.exists(gpath) and os.path.exists(hpath)):
+            raise RuntimeError("native library not built: run bem3_aw_qd2_b200/build.py (%s)" % LIBDIR)
+        g = ctypes.CDLL(gpath)
+        h = ctypes.CDLL(hpath)
+        vp = ctypes.c_void_p
+        g.bemgpu_create.argtypes = [ctypes.c_int, vp, ctypes.POINTER(vp)]
+        g.bemgpu_destroy.argtypes = [vp]
+        g.bemgpu_error.argtypes = [vp]
+        g.bemgpu_error.restype = ctypes.c_char_p
+        g.bemgpu_status.argtypes = [vp]
+        g.bemgpu_status.restype = ctypes.c_uint
+        for name in ("bemgpu_assemble", "bemgpu_solve", "bemgpu_run", "bemgpu_sync"):
+            getattr(g, name).argtypes = [vp]
+        g.bemgpu_get_solution.argtypes = [vp, ctypes.c_int, _d, _d, _d, _d]
+        g.bemgpu_get_matrix.argtypes = [vp, ctypes.c_int, ctypes.c_int, _d]
+        g.bemgpu_force.argtypes = [vp, ctypes.c_int, _d, _d, _d]
+        g.bemgpu_faddeeva_w.argtypes = [_d, ctypes.c_int, _d]
+        g.bemgpu_qpgf.argtypes = [_d, _d, ctypes.c_int, _d, _d, _i]
+        h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
+        for name in ("print_aqd2", "initialize_aqd2", "finalize_aqd2", "solve_bieq_aqd2"):
+            getattr(h, name).argtypes = [vp]
+        h.dat_write_aqd2.argtypes = [ctypes.c_char_p, vp]
+        h.dat_read_aqd2.argtypes = [ctypes.c_char_p, vp]
+        h.force_FN_aqd2.argtypes = [_d, _d, _d, ctypes.c_int, vp]
+        h.aqd2_device_context.argtypes = [vp]
+        h.aqd2_device_context.restype = vp
+        h.aqd2_last_timing.argtypes = [_d]
+        h.aqd2_set_device.argtypes = [ctypes.c_int]
+        _host, _gpu = h, g
+    return _host, _gpu
+
+
+def _p(a):
+    return a.ctypes.data_as(_d)
+
+
+AQD2_SIZE = 2720  # sizeof(AQD2) on x86-64, fixed by the .dat format
+
+
+class Case:
+    """One AQD2 object (the reference's solver state) and its device context."""
+
+    def __init__(self):
+        libs()
+        self.buf = ctypes.create_string_buffer(AQD2_SIZE)
+        self.qd = ctypes.cast(self.buf, ctypes.c_void_p)
+        self._alive = False
+
+    @classmethod
+    def from_files(cls, pw, per, med, msh, rotation=None):
+        """read_aqd2 + initialize_aqd2; rotation = (rvx, rvy, rvz, theta, tx, ty, tz) or None."""
+        h, _ = libs()
+        c = cls()
+        args = ["bem3_aw_qd2", pw, per, med, msh, "unused.dat"]
+        if rotation is not None:
+            args += ["%.17g" % v for v in rotation]
+        argv = (ctypes.c_char_p * len(args))(*[a.encode() for a in args])
+        h.read_aqd2(len(args), argv, c.qd)
+        h.initialize_aqd2(c.qd)
+        c._alive = True
+        return c
+
+    @classmethod
+    def from_dat(cls, path):
+        h, _ = libs()
+        c = cls()
+        h.dat_read_aqd2(path.encode(), c.qd)
+        c._alive = True
+        return c
+
+    def solve(self):
+        """solve_bieq_aqd2: upload, assemble, solve, download (host buffers in and out)."""
+        libs()[0].solve_bieq_aqd2(self.qd)
+
+    def timing(self):
+        t = np.zeros(4)
+        libs()[0].aqd2_last_timing(_p(t))
+        return t
+
+    def force(self, type=0, rc=(0.0, 0.0, 0.0)):
+        F = np.zeros(3)
+        N = np.zeros(3)
+        rc = np.ascontiguousarray(rc, dtype=np.float64)
+        libs()[0].force_FN_aqd2(_p(F), _p(N), _p(rc), type, self.qd)
+        return F, N
+
+    def dat_write(self, path):
+        libs()[0].dat_write_aqd2(path.encode(), self.qd)
+
+    # ---- device context access (tests, benchmarks)
+    @property
+    def ctx(self):
+        c = libs()[0].aqd2_device_context(self.qd)
+        if not c:
+            raise RuntimeError("no device context: call solve() first")
+        return c
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("%s failed (%d): %s" % (what, rc, libs()[1].bemgpu_error(self.ctx).decode()))
+
+    def run_device(self):
+        """bemgpu_run on the resident problem (inputs already on the device)."""
+        self._check(libs()[1].bemgpu_run(self.ctx), "bemgpu_run")
+
+    def sync(self):
+        self._check(libs()[1].bemgpu_sync(self.ctx), "bemgpu_sync")
+
+    def status(self):
+        return libs()[1].bemgpu_status(self.ctx)
+
+    def domain_sizes(self):
+        return [int(n) for n in self._dom_ne()]
+
+    def _dom_ne(self):
+        # read via the solution shape: ask the device for domain sizes through the matrices
+        raise NotImplementedError
+
+    def matrix(self, d, which, N):
+        """which: 'G', 'H', 'dG', 'dH', 'dF'; N = 4 * elements of domain d."""
+        w = {"G": 0, "H": 1, "dG": 2, "dH": 3, "dF": 4}[which]
+        if w == 4:
+            out = np.zeros((N, 3))
+        elif w >= 2:
+            out = np.zeros((2 * N, N), np.complex128)
+        else:
+            out = np.zeros((N, N), np.complex128)
+        self._check(libs()[1].bemgpu_get_matrix(self.ctx, d, w, _p(out.view(np.float64) if out.dtype == np.complex128 else out)),
+                    "get_matrix")
+        return out
+
+    def solution(self, d, ne):
+        P = np.zeros((ne, 4), np.complex128)
+        dP = np.zeros((ne, 4), np.complex128)
+        pv = np.zeros((ne, 4, 3), np.complex128)
+        dpv = np.zeros((ne, 4, 3), np.complex128)
+        self._check(libs()[1].bemgpu_get_solution(self.ctx, d, _p(P.view(np.float64)), _p(dP.view(np.float64)),
+                                                  _p(pv.view(np.float64)), _p(dpv.view(np.float64))), "get_solution")
+        return P, dP, pv, dpv
+
+    def close(self):
+        if self._alive:
+            libs()[0].finalize_aqd2(self.qd)
+            self._alive = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def faddeeva_w(z):
+    """Device Faddeeva function at the complex points z (numpy array)."""
+    z = np.ascontiguousarray(np.asarray(z, dtype=np.complex128))
+    w = np.zeros_like(z)
+    rc = libs()[1].bemgpu_faddeeva_w(_p(z.view(np.float64)), z.size, _p(w.view(np.float64)))
+    if rc != 0:
+        raise RuntimeError("bemgpu_faddeeva_w failed")
+    return w
+
+
+def qpgf(qp, r):
+    """Device quasi-periodic Green's function and gradient at points r[n,3]."""
+    qp = np.ascontiguousarray(qp, dtype=np.float64)
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+    n = len(r)
+    G = np.zeros(n, np.complex128)
+    dG = np.zeros((n, 3), np.complex128)
+    ret = np.zeros(n, np.int32)
+    rc = libs()[1].bemgpu_qpgf(_p(qp), _p(r), n, _p(G.view(np.float64)), _p(dG.view(np.float64)),
+                               ret.ctypes.data_as(_i))
+    if rc != 0:
+        raise RuntimeError("bemgpu_qpgf failed")
+    return G, dG, ret

@@ -1,0 +1,889 @@
+// Boundary-integral coefficient matrices of one domain on the device.
+//
+// Replaces create_cmatrix_domain (d3qd2_src/bem3_aw_qd2_solve_bieq.c:133-218)
+// and the element integrals it calls.  Outputs use the reference's layout so
+// they can be compared with its temporary files entry by entry:
+//   G[p][4 s + i], H[p][4 s + i]   (N x N, row-major complex128, p = 4 t + tn)
+//   dG[2 p + {0,1}][4 s + i], dH   (2N x N, tangential derivatives, interior only)
+//   dF[p][3] = {(1+)F, dF/dt_zeta, dF/dt_eta}
+//
+// Work is split by pair class, each class in its own kernel:
+//   classify  geometric F, dF/dt on 12x12 points for every (p, s); flags the
+//             near-singular pairs (|dF/dt| > 0.5, d3qd2_elem.c:851,537)
+//   regular   12x12 points: periodic domain one thread per point (each point is
+//             a full quasi-periodic Green's function, ~100 lattice terms);
+//             free-space domain one thread per pair (cheap integrand)
+//   near      64x64 points for flagged pairs, one block per pair
+//   self      singular polar quadrature on the collocation element, one block
+//             per collocation node
+//   diag      adds (1+)F to the diagonal of H and writes dF
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "bem_qpgf.cuh"
+#include "bem_geom.cuh"
+#include "bem_kernels.h"
+
+
+// ------------------------------------------------------------------ helpers
+struct bem_node { double rt[3], vz[3], vt[3]; };  // collocation point, unit tangents
+
+__device__ __forceinline__ void bem_load_node(const bem_dom_dev &D, int p, bem_node &n, int &t, int &te) {
+  t = p >> 2;
+  const int tn = p & 3;
+  te = abs(D.sid[t]) - 1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) n.rt[d] = __ldg(D.ren + (size_t)te * 12 + tn * 3 + d);
+  // tz_te_bd_node (d3qd2_elem.c:125)
+  double az = 0, ae = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    n.vz[d] = __ldg(D.cr + (size_t)te * 12 + d * 4 + 1) + __ldg(D.cr + (size_t)te * 12 + d * 4 + 3) * c_q.et[tn];
+    n.vt[d] = __ldg(D.cr + (size_t)te * 12 + d * 4 + 2) + __ldg(D.cr + (size_t)te * 12 + d * 4 + 3) * c_q.zt[tn];
+    az += n.vz[d] * n.vz[d];
+    ae += n.vt[d] * n.vt[d];
+  }
+  az = sqrt(az);
+  ae = sqrt(ae);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { n.vz[d] /= az; n.vt[d] /= ae; }
+}
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+__device__ __forceinline__ void set_status(unsigned *st, unsigned bits) { if (bits) atomicOr(st, bits); }
+
+// geometric F and its tangential derivatives at one quadrature point:
+// tD = (R.W)/R^3, dF_v = (3 (R.v)(R.W)/R^2 - W.v)/R^3   (q0_bil_dcoef_v2_cc.c:165-200)
+__device__ __forceinline__ void geomF(const double vR[3], const double vW[3], const bem_node &n, double &f, double &fz, double &fe) {
+  const double aR = sqrt(vR[0] * vR[0] + vR[1] * vR[1] + vR[2] * vR[2]);
+  const double iR = 1.0 / aR;
+  const double rdW = dot3(vR, vW) * iR;
+  const double rdz = dot3(vR, n.vz) * iR, rde = dot3(vR, n.vt) * iR;
+  const double Wdz = dot3(vW, n.vz), Wde = dot3(vW, n.vt);
+  const double i3 = iR * iR * iR;
+  f = rdW * iR * iR;
+  fz = i3 * (3.0 * rdz * rdW - Wdz);
+  fe = i3 * (3.0 * rde * rdW - Wde);
+}
+
+// ------------------------------------------------------------------ classify
+// One block per collocation node p; threads stride over source elements.
+__global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restrict__ rowF,
+                                                   int *__restrict__ near_s, int *__restrict__ near_n,
+                                                   uint8_t *__restrict__ flag, unsigned *status) {
+  const int p = blockIdx.x;
+  bem_node nd;
+  int t, te;
+  bem_load_node(D, p, nd, t, te);
+  __shared__ int cnt;
+  __shared__ int list[BEM_MAXNEAR];
+  __shared__ double red[3][128];
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  double sF = 0, sFz = 0, sFe = 0;
+  for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
+    const int se = abs(D.sid[s]) - 1;
+    uint8_t fl = 0;
+    if (se == te) {
+      fl = 2;  // self pair
+    } else {
+      bem_el el;
+      bem_load_el(D.cr, D.cw, se, el);
+      double F = 0, Fz = 0, Fe = 0;
+      for (int i = 0; i < BEM_GLN; ++i) {
+        double f = 0, fz = 0, fe = 0;
+        for (int j = 0; j < BEM_GLN; ++j) {
+          double vR[3], vW[3];
+          bem_rw(el, c_q.xl[i], c_q.xl[j], vR, vW);
+          for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+          double a, b, c;
+          geomF(vR, vW, nd, a, b, c);
+          f += c_q.wl[j] * a;
+          fz += c_q.wl[j] * b;
+          fe += c_q.wl[j] * c;
+        }
+        F += c_q.wl[i] * f;
+        Fz += c_q.wl[i] * fz;
+        Fe += c_q.wl[i] * fe;
+      }
+      F *= BEM_I_FP; Fz *= BEM_I_FP; Fe *= BEM_I_FP;
+      if (D.sid[s] < 0) { F = -F; Fz = -Fz; Fe = -Fe; }  // bil_convert_CC / _dCC
+      if (fabs(Fz) > BEM_CBD_SDF || fabs(Fe) > BEM_CBD_SDF) {
+        fl = 1;
+        const int k = atomicAdd(&cnt, 1);
+        if (k < BEM_MAXNEAR) list[k] = s;
+      } else {
+        sF += F; sFz += Fz; sFe += Fe;
+      }
+    }
+    flag[(size_t)p * D.ne + s] = fl;
+  }
+  red[0][threadIdx.x] = sF;
+  red[1][threadIdx.x] = sFz;
+  red[2][threadIdx.x] = sFe;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    int n = cnt;
+    if (n > BEM_MAXNEAR) { set_status(status, BEM_ST_NEAR_OVERFLOW); n = BEM_MAXNEAR; }
+    // deterministic order: sort the row's near-singular sources by index
+    for (int a = 1; a < n; ++a) {
+      const int v = list[a];
+      int b = a - 1;
+      while (b >= 0 && list[b] > v) { list[b + 1] = list[b]; --b; }
+      list[b + 1] = v;
+    }
+    for (int a = 0; a < n; ++a) near_s[(size_t)p * BEM_MAXNEAR + a] = list[a];
+    near_n[p] = n;
+    rowF[3 * p + 0] = red[0][0];
+    rowF[3 * p + 1] = red[1][0];
+    rowF[3 * p + 2] = red[2][0];
+  }
+}
+
+// ------------------------------------------------------------------ periodic regular pairs
+// 2 pairs x 144 points per block; one quasi-periodic Green's function per thread
+// (q0_bil_dcoef_v2_cc_GL, q0_bil_dcoef_v2_cc.c:129-204, evaluated once per
+// point and shared by the four interpolation functions).
+#define RP_THREADS 288
+__global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp q, const uint8_t *__restrict__ flag,
+                                                           double *__restrict__ G, double *__restrict__ H,
+                                                           unsigned *status, long long pair0, long long npairs) {
+  __shared__ double acc[16][RP_THREADS + 1];
+  const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
+  const long long pair = pair0 + 2LL * blockIdx.x + lp;
+  const bool valid = pair < pair0 + npairs;
+  const int p = valid ? (int)(pair / D.ne) : 0;
+  const int s = valid ? (int)(pair % D.ne) : 0;
+  const bool work = valid && flag[(size_t)p * D.ne + s] == 0;
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  if (work) {
+    bem_node nd;
+    int t, te;
+    bem_load_node(D, p, nd, t, te);
+    bem_el el;
+    bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+    const int i = pt / BEM_GLN, j = pt % BEM_GLN;
+    const double z = c_q.xl[i], e = c_q.xl[j];
+    double vR[3], vW[3];
+    bem_rw(el, z, e, vR, vW);
+    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+    bem_gval gv;
+    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+    if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
+    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+    const double wt = c_q.wl[i] * c_q.wl[j];
+    const cplx g = cscale(gv.g, aW * wt);
+    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      v[2 * a] = g.re * N[a];
+      v[2 * a + 1] = g.im * N[a];
+      v[8 + 2 * a] = h.re * N[a];
+      v[8 + 2 * a + 1] = h.im * N[a];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
+    const long long pr = pair0 + 2LL * blockIdx.x + q2;
+    if (pr < pair0 + npairs) {
+      const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
+      if (flag[(size_t)pp * D.ne + ss] == 0) {
+        double sum = 0.0;
+        for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
+        const size_t N = (size_t)D.ne * 4;
+        double *dst = c < 8 ? G : H;
+        const int a = (c & 7) >> 1, part = c & 1;
+        dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ periodic near-singular pairs
+// 64x64 points (q0_bil_dcoef_v2_cc_GH, q0_bil_dcoef_v2_cc.c:206-281).
+#define NP_THREADS 256
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*NP_THREADS */) {
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    double x = v[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) sm[c * (NP_THREADS / 32) + (threadIdx.x >> 5)] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double x = 0.0;
+    for (int w = 0; w < NP_THREADS / 32; ++w) x += sm[threadIdx.x * (NP_THREADS / 32) + w];
+    sm[NV * (NP_THREADS / 32) + threadIdx.x] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NV; ++c) v[c] = sm[NV * (NP_THREADS / 32) + c];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q, const int *__restrict__ near_s,
+                                                        const int *__restrict__ near_n, double *__restrict__ G,
+                                                        double *__restrict__ H, double *__restrict__ nearF, unsigned *status) {
+  const int p = blockIdx.x, k = blockIdx.y;
+  if (k >= near_n[p]) return;
+  const int s = near_s[(size_t)p * BEM_MAXNEAR + k];
+  bem_node nd;
+  int t, te;
+  bem_load_node(D, p, nd, t, te);
+  bem_el el;
+  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  double v[19];
+#pragma unroll
+  for (int c = 0; c < 19; ++c) v[c] = 0.0;
+  unsigned st = 0;
+  for (int pt = threadIdx.x; pt < BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+    const int i = pt / BEM_GHN, j = pt % BEM_GHN;
+    const double z = c_q.xh[i], e = c_q.xh[j];
+    double vR[3], vW[3];
+    bem_rw(el, z, e, vR, vW);
+    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+    bem_gval gv;
+    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+    if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+    const double wt = c_q.wh[i] * c_q.wh[j];
+    const cplx g = cscale(gv.g, aW * wt);
+    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      v[2 * a] += g.re * N[a];
+      v[2 * a + 1] += g.im * N[a];
+      v[8 + 2 * a] += h.re * N[a];
+      v[8 + 2 * a + 1] += h.im * N[a];
+    }
+    double f, fz, fe;
+    geomF(vR, vW, nd, f, fz, fe);
+    v[16] += wt * f;
+    v[17] += wt * fz;
+    v[18] += wt * fe;
+  }
+  set_status(status, st);
+  __shared__ double sm[19 * (NP_THREADS / 32) + 19];
+  block_reduce<19>(v, sm);
+  if (threadIdx.x < 16) {
+    const size_t N = (size_t)D.ne * 4;
+    const int c = threadIdx.x;
+    double *dst = c < 8 ? G : H;
+    const int a = (c & 7) >> 1, part = c & 1;
+    dst[2 * ((size_t)p * N + 4 * s + a) + part] = v[c];
+  } else if (threadIdx.x < 19) {
+    nearF[((size_t)p * BEM_MAXNEAR + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
+  }
+}
+
+// ------------------------------------------------------------------ singular (self) integrals
+// Polar quadrature around the collocation point (zt,et) of the element itself:
+// 4 sub-triangles x (2 x 64) angles x 12 radii (q0_bil_coef_bd, q0_bil_coef.c:246-338,
+// and bil_coef_bd, bil_coef.c:244-342).  The angular rule of the reference
+// splits each sub-triangle's angle range in two halves with 64 points each.
+struct polar_pt { double th, wth; int j; };
+__device__ __forceinline__ polar_pt polar_theta(const double th[5], int idx /* 0..511 */) {
+  const int j = idx >> 7, h = (idx >> 6) & 1, m = idx & 63;
+  const double t0 = th[j], t1 = th[j + 1];
+  polar_pt r;
+  r.th = h == 0 ? 0.25 * (t1 - t0) * c_q.xh[m] + 0.25 * (t1 + 3.0 * t0) : 0.25 * (t1 - t0) * c_q.xh[m] + 0.25 * (3.0 * t1 + t0);
+  r.wth = c_q.wh[m] * 0.25 * (t1 - t0);
+  r.j = j;
+  return r;
+}
+
+// geometric F of the element at parameter point (zt,et) by the polar rule (q0_bil_coef_bd_F,
+// q0_bil_dcoef_v2_cc.c:401-454 / bil_sF_theta): returns the un-normalised sum (times bdC/4pi later)
+__device__ double polar_F_partial(const bem_el &el, double zt, double et, unsigned &st) {
+  double r[5], th[5];
+  bem_node_r_th(zt, et, r, th);
+  double acc = 0.0;
+  for (int idx = threadIdx.x; idx < 512; idx += blockDim.x) {
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    double inner = 0.0;
+    for (int ir = 0; ir < BEM_GLN; ++ir) {
+      const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+      double K[3];
+      bem_K(el, rr, cth, sth, zt, et, K);
+      const double aK = sqrt(K[0] * K[0] + K[1] * K[1] + K[2] * K[2]);
+      inner += c_q.wl[ir] / (aK * aK * aK) * cth * sth;
+    }
+    acc += tp.wth * 0.5 * rm * inner;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ double bem_bdC(const bem_el &el) {
+  return el.cr[0][1] * el.cw[0][2] + el.cr[1][1] * el.cw[1][2] + el.cr[2][1] * el.cw[2][2];
+}
+
+// periodic self pair: one block per collocation node p
+__global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q, double *__restrict__ G,
+                                                        double *__restrict__ H, double *__restrict__ selfF,
+                                                        unsigned *status) {
+  const int p = blockIdx.x;
+  const int t = p >> 2, tn = p & 3;
+  const int te = abs(D.sid[t]) - 1;
+  bem_el el;
+  bem_load_el(D.cr, D.cw, te, el);
+  const double zt = c_q.zt[tn], et = c_q.et[tn];
+  double r[5], th[5];
+  bem_node_r_th(zt, et, r, th);
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  unsigned st = 0;
+  for (int pt = threadIdx.x; pt < 512 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+    const double w = tp.wth * 0.5 * rm * c_q.wl[ir];
+    const double z = rr * cth + zt, e = rr * sth + et;
+    double K[3], vR[3], vW[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    for (int d = 0; d < 3; ++d) {
+      vR[d] = rr * K[d];
+      vW[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+    }
+    bem_gval gv;
+    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+    if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+    const cplx g = cscale(gv.g, aW * rr * w);
+    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), rr * w);
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      v[2 * a] += g.re * N[a];
+      v[2 * a + 1] += g.im * N[a];
+      v[8 + 2 * a] += h.re * N[a];
+      v[8 + 2 * a + 1] += h.im * N[a];
+    }
+  }
+  // F at the node and at (zt+-h, et), (zt, et+-h) for the central differences
+  // (q0_bil_dcoef_bd_tz0_cc_DV / _te0_, q0_bil_dcoef_v2_cc.c:336-399)
+  const bool plane = D.plane[te] != 0;
+  double f[5] = {0, 0, 0, 0, 0};
+  if (!plane) {
+    f[0] = polar_F_partial(el, zt, et, st);
+    f[1] = polar_F_partial(el, zt + BEM_CDFH, et, st);
+    f[2] = polar_F_partial(el, zt - BEM_CDFH, et, st);
+    f[3] = polar_F_partial(el, zt, et + BEM_CDFH, st);
+    f[4] = polar_F_partial(el, zt, et - BEM_CDFH, st);
+  }
+  set_status(status, st);
+  __shared__ double sm[21 * (NP_THREADS / 32) + 21];
+  double all[21];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) all[c] = v[c];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) all[16 + c] = f[c];
+  block_reduce<21>(all, sm);
+  if (threadIdx.x < 16) {
+    const size_t N = (size_t)D.ne * 4;
+    const int c = threadIdx.x;
+    double *dst = c < 8 ? G : H;
+    const int a = (c & 7) >> 1, part = c & 1;
+    dst[2 * ((size_t)p * N + 4 * t + a) + part] = all[c];
+  } else if (threadIdx.x == 16) {
+    const double bdC = bem_bdC(el);
+    const double F0 = plane ? 0.0 : all[16] * BEM_I_FP * bdC;
+    const double Fzp = all[17] * BEM_I_FP * bdC, Fzm = all[18] * BEM_I_FP * bdC;
+    const double Fep = all[19] * BEM_I_FP * bdC, Fem = all[20] * BEM_I_FP * bdC;
+    double Tz[3], Te[3];
+    for (int d = 0; d < 3; ++d) {
+      Tz[d] = el.cr[d][1] + el.cr[d][3] * et;
+      Te[d] = el.cr[d][2] + el.cr[d][3] * zt;
+    }
+    const double iTz = 1.0 / sqrt(dot3(Tz, Tz)), iTe = 1.0 / sqrt(dot3(Te, Te));
+    selfF[3 * p + 0] = F0;
+    selfF[3 * p + 1] = plane ? 0.0 : iTz * (Fzp - Fzm) / (2.0 * BEM_CDFH);
+    selfF[3 * p + 2] = plane ? 0.0 : iTe * (Fep - Fem) / (2.0 * BEM_CDFH);
+  }
+}
+
+// ------------------------------------------------------------------ free-space (interior) pairs
+// Integrand of bil_dcoef_v2_GL / _GH (bil_dcoef_v2.c:141-325) at one point,
+// accumulated into 24 complex sums + 3 geometric ones.
+struct fs_acc { double g[8], h[8], gz[8], ge[8], hz[8], he[8], f, fz, fe; };
+
+__device__ __forceinline__ void fs_zero(fs_acc &a) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) { a.g[c] = a.h[c] = a.gz[c] = a.ge[c] = a.hz[c] = a.he[c] = 0.0; }
+  a.f = a.fz = a.fe = 0.0;
+}
+
+__device__ __forceinline__ void fs_point(const bem_el &el, const bem_node &nd, double k, double z, double e, double wt, fs_acc &a) {
+  double vR[3], vW[3];
+  bem_rw(el, z, e, vR, vW);
+  for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+  const double aR = sqrt(vR[0] * vR[0] + vR[1] * vR[1] + vR[2] * vR[2]);
+  const double iR = 1.0 / aR;
+  const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+  const cplx ce = cexpi(k * aR);
+  const cplx cb = cmk(-1.0, k * aR);  // i k R - 1
+  const double rdW = dot3(vR, vW) * iR;
+  const double tD = rdW * iR * iR;
+  const double rdz = dot3(vR, nd.vz) * iR, rde = dot3(vR, nd.vt) * iR;
+  const double Wdz = dot3(vW, nd.vz), Wde = dot3(vW, nd.vt);
+  const double i3 = iR * iR * iR;
+  double N[4];
+  bem_Nn4(z, e, N);
+  const cplx cbce = cmul(cb, ce);
+  const cplx g = cscale(ce, iR * aW * wt);                       // e^{ikR}/R |W|
+  const cplx h = cscale(cbce, tD * wt);                          // (ikR-1) e^{ikR} (R.W)/R^3
+  const cplx gz = cscale(cbce, iR * iR * rdz * aW * wt);         // dG/dv before the -1/4pi
+  const cplx ge = cscale(cbce, iR * iR * rde * aW * wt);
+  const cplx kk3 = cmk(k * k * aR * aR + 3.0 * cb.re, 3.0 * cb.im);  // k^2 R^2 + 3 (ikR-1)
+  const cplx hz = cscale(cmul(ce, csub(cscale(kk3, rdz * rdW), cscale(cb, Wdz))), i3 * wt);
+  const cplx he = cscale(cmul(ce, csub(cscale(kk3, rde * rdW), cscale(cb, Wde))), i3 * wt);
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    a.g[2 * n] += g.re * N[n];  a.g[2 * n + 1] += g.im * N[n];
+    a.h[2 * n] += h.re * N[n];  a.h[2 * n + 1] += h.im * N[n];
+    a.gz[2 * n] += gz.re * N[n]; a.gz[2 * n + 1] += gz.im * N[n];
+    a.ge[2 * n] += ge.re * N[n]; a.ge[2 * n + 1] += ge.im * N[n];
+    a.hz[2 * n] += hz.re * N[n]; a.hz[2 * n + 1] += hz.im * N[n];
+    a.he[2 * n] += he.re * N[n]; a.he[2 * n + 1] += he.im * N[n];
+  }
+  a.f += wt * tD;
+  a.fz += wt * i3 * (3.0 * rdz * rdW - Wdz);
+  a.fe += wt * i3 * (3.0 * rde * rdW - Wde);
+}
+
+// write one pair's 24 complex coefficients with the reference's scale factors
+// (1/4pi, -1/4pi for dG) and the sign flip for negative element ids
+__device__ __forceinline__ void fs_store(const bem_dom_dev &D, int p, int s, const fs_acc &a, double *G, double *H,
+                                         double *dG, double *dH) {
+  const size_t N = (size_t)D.ne * 4;
+  const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
+  const double c = BEM_I_FP;
+  double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * s));
+  double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * s));
+  double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * s));
+  double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * s));
+  double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * s));
+  double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * s));
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    g2[n] = make_double2(a.g[2 * n] * c, a.g[2 * n + 1] * c);
+    h2[n] = make_double2(sg * a.h[2 * n] * c, sg * a.h[2 * n + 1] * c);
+    gz[n] = make_double2(-a.gz[2 * n] * c, -a.gz[2 * n + 1] * c);
+    ge[n] = make_double2(-a.ge[2 * n] * c, -a.ge[2 * n + 1] * c);
+    hz[n] = make_double2(sg * a.hz[2 * n] * c, sg * a.hz[2 * n + 1] * c);
+    he[n] = make_double2(sg * a.he[2 * n] * c, sg * a.he[2 * n + 1] * c);
+  }
+}
+
+// one thread per (p, s) pair, 12x12 points
+__global__ void __launch_bounds__(128) k_fs_regular(bem_dom_dev D, double k, const uint8_t *__restrict__ flag,
+                                                    double *__restrict__ G, double *__restrict__ H,
+                                                    double *__restrict__ dG, double *__restrict__ dH) {
+  const long long pair = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)D.ne * 4 * D.ne;
+  if (pair >= total) return;
+  const int p = (int)(pair / D.ne), s = (int)(pair % D.ne);
+  if (flag[pair] != 0) return;
+  bem_node nd;
+  int t, te;
+  bem_load_node(D, p, nd, t, te);
+  bem_el el;
+  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  fs_acc a;
+  fs_zero(a);
+  for (int i = 0; i < BEM_GLN; ++i)
+    for (int j = 0; j < BEM_GLN; ++j) fs_point(el, nd, k, c_q.xl[i], c_q.xl[j], c_q.wl[i] * c_q.wl[j], a);
+  fs_store(D, p, s, a, G, H, dG, dH);
+}
+
+// one block per flagged pair, 64x64 points
+__global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k, const int *__restrict__ near_s,
+                                                        const int *__restrict__ near_n, double *__restrict__ G,
+                                                        double *__restrict__ H, double *__restrict__ dG,
+                                                        double *__restrict__ dH, double *__restrict__ nearF) {
+  const int p = blockIdx.x, kk = blockIdx.y;
+  if (kk >= near_n[p]) return;
+  const int s = near_s[(size_t)p * BEM_MAXNEAR + kk];
+  bem_node nd;
+  int t, te;
+  bem_load_node(D, p, nd, t, te);
+  bem_el el;
+  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  fs_acc a;
+  fs_zero(a);
+  for (int pt = threadIdx.x; pt < BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+    const int i = pt / BEM_GHN, j = pt % BEM_GHN;
+    fs_point(el, nd, k, c_q.xh[i], c_q.xh[j], c_q.wh[i] * c_q.wh[j], a);
+  }
+  __shared__ double sm[51 * (NP_THREADS / 32) + 51];
+  double *av = reinterpret_cast<double *>(&a);
+  double v[51];
+#pragma unroll
+  for (int c = 0; c < 51; ++c) v[c] = av[c];
+  block_reduce<51>(v, sm);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < 51; ++c) av[c] = v[c];
+    fs_store(D, p, s, a, G, H, dG, dH);
+    const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
+    double *nf = nearF + ((size_t)p * BEM_MAXNEAR + kk) * 3;
+    nf[0] = sg * a.f * BEM_I_FP;
+    nf[1] = sg * a.fz * BEM_I_FP;
+    nf[2] = sg * a.fe * BEM_I_FP;
+  }
+}
+
+// free-space self pair with the principal-value derivative integrals
+// (bil_dcoef_bd_vt2_PV -> bil_coef_bd, bil_dcoef_bd_tz0_PV, bil_dcoef_bd_te0_PV;
+//  bil_coef.c:244-342, bil_dcoef.c:369-740, integrands bil_dcoef.c:916-1630).
+// Accumulators (complex unless noted), per interpolation function n:
+//   G, H, and F (real)                       over the 12-radius polar rule
+//   dG (shared rule, vt differs), dHz, dHe   over D-bar-eps (64 radii from DEPS to rm),
+//   D-eps (4 x 64 angles, 12 radii) and the PV pair (2 x 64 angles, 12 radii)
+//   dFz, dFe (real)                           over D-bar-eps and the PV pair
+struct self_acc {
+  double g[8], h[8];
+  double dgz[8], dge[8], dhz[8], dhe[8];
+  double f, fz, fe;
+};
+
+__global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k, double *__restrict__ G,
+                                                        double *__restrict__ H, double *__restrict__ dG,
+                                                        double *__restrict__ dH, double *__restrict__ selfF,
+                                                        unsigned *status) {
+  const int p = blockIdx.x;
+  const int t = p >> 2, tn = p & 3;
+  const int te = abs(D.sid[t]) - 1;
+  bem_el el;
+  bem_load_el(D.cr, D.cw, te, el);
+  const double zt = c_q.zt[tn], et = c_q.et[tn];
+  double r[5], th[5];
+  bem_node_r_th(zt, et, r, th);
+  double vz[3], ve[3];  // T_zeta, T_eta at (zt,et) (not normalised), bil_t_zeta / bil_t_eta
+  for (int d = 0; d < 3; ++d) {
+    vz[d] = el.cr[d][1] + el.cr[d][3] * et;
+    ve[d] = el.cr[d][2] + el.cr[d][3] * zt;
+  }
+  self_acc A;
+  double *Av = reinterpret_cast<double *>(&A);
+#pragma unroll
+  for (int c = 0; c < 51; ++c) Av[c] = 0.0;
+  unsigned st = 0;
+  // (1) G, H, F over the polar rule with 12 radii from 0 to rm
+  for (int pt = threadIdx.x; pt < 512 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+    const double w = tp.wth * 0.5 * rm * c_q.wl[ir];
+    const double z = rr * cth + zt, e = rr * sth + et;
+    double K[3], W[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    for (int d = 0; d < 3; ++d) W[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+    const double aK = sqrt(dot3(K, K)), aW = sqrt(dot3(W, W));
+    const double kR = k * aK * rr;
+    const cplx ce = cexpi(kR);
+    const cplx g = cscale(ce, w * aW / aK);                                          // bil_sG_r
+    const cplx h = cscale(cmul(cmk(-1.0, kR), ce), w * cth * sth / (aK * aK * aK));  // bil_sH_r
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      A.g[2 * n] += g.re * N[n]; A.g[2 * n + 1] += g.im * N[n];
+      A.h[2 * n] += h.re * N[n]; A.h[2 * n + 1] += h.im * N[n];
+    }
+    A.f += w * cth * sth / (aK * aK * aK);                                           // bil_sF_r
+  }
+  // (2) D-bar-eps: 512 angles x 64 radii from DEPS to rm
+  for (int pt = threadIdx.x; pt < 512 * BEM_GHN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GHN, ir = pt % BEM_GHN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * (rm - BEM_DEPS) * c_q.xh[ir] + 0.5 * (rm + BEM_DEPS);
+    const double w = tp.wth * 0.5 * (rm - BEM_DEPS) * c_q.wh[ir];
+    const double z = rr * cth + zt, e = rr * sth + et;
+    double K[3], W[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    for (int d = 0; d < 3; ++d) W[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+    const double aK = sqrt(dot3(K, K)), aW = sqrt(dot3(W, W));
+    const double iK = 1.0 / aK;
+    const double kR = k * aK * rr;
+    const cplx ce = cexpi(kR);
+    const cplx cb = cmk(-1.0, kR);
+    const cplx cbce = cmul(cb, ce);
+    const double KTz = dot3(K, vz), KTe = dot3(K, ve);
+    // bil_sdG_Db_r: cb ce / aK^2 / r * (K.vt/aK) * N * aW
+    const double gfac = w * iK * iK / rr * aW * iK;
+    const cplx dgz = cscale(cbce, gfac * KTz), dge = cscale(cbce, gfac * KTe);
+    // bil_sdHz_Db_r: ce/(r aK^5) ((kR^2 + 3cb) K.vt cth - cb aK^2), then * sth (outer)
+    // bil_sdHe_Db_r: same with sth inside and cth outer
+    const double i5 = 1.0 / (rr * aK * aK * aK * aK * aK);
+    const cplx kk3 = cmk(kR * kR + 3.0 * cb.re, 3.0 * cb.im);
+    const cplx hz = cscale(cmul(ce, csub(cscale(kk3, KTz * cth), cscale(cb, aK * aK))), w * i5 * sth);
+    const cplx he = cscale(cmul(ce, csub(cscale(kk3, KTe * sth), cscale(cb, aK * aK))), w * i5 * cth);
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      A.dgz[2 * n] += dgz.re * N[n]; A.dgz[2 * n + 1] += dgz.im * N[n];
+      A.dge[2 * n] += dge.re * N[n]; A.dge[2 * n + 1] += dge.im * N[n];
+      A.dhz[2 * n] += hz.re * N[n];  A.dhz[2 * n + 1] += hz.im * N[n];
+      A.dhe[2 * n] += he.re * N[n];  A.dhe[2 * n + 1] += he.im * N[n];
+    }
+    A.fz += w * i5 * (3.0 * KTz * cth - aK * aK) * sth;   // bil_sdFz_Db_r
+    A.fe += w * i5 * (3.0 * KTe * sth - aK * aK) * cth;   // bil_sdFe_Db_r
+  }
+  // (3) D-eps: 4 x 64 angles over [0, 2 pi), 12 radii from 0 to DEPS
+  for (int pt = threadIdx.x; pt < 256 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const int qd = idx >> 6, m = idx & 63;
+    const double tht = 0.25 * CUDART_PI * c_q.xh[m] + (-0.75 + 0.5 * qd) * CUDART_PI;
+    const double wth = 0.25 * CUDART_PI * c_q.wh[m];
+    double sth, cth;
+    sincos(tht, &sth, &cth);
+    const double rr = 0.5 * BEM_DEPS * (c_q.xl[ir] + 1.0);
+    const double w = wth * 0.5 * BEM_DEPS * c_q.wl[ir];
+    const double z = rr * cth + zt, e = rr * sth + et;
+    double K[3], W[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    for (int d = 0; d < 3; ++d) W[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+    const double aK = sqrt(dot3(K, K)), aW = sqrt(dot3(W, W));
+    const double iK = 1.0 / aK;
+    const double kR = k * aK * rr;
+    double skr, ckr;
+    sincos(kR, &skr, &ckr);
+    const cplx ce = cmk(ckr, skr);
+    const double KTz = dot3(K, vz), KTe = dot3(K, ve);
+    // bil_sdG_De_r: (cb sin kR + kR cos kR)/aK^2/r * (K.vt/aK) aW N, times i (outer)
+    const cplx cbsk = cmk(-skr + kR * ckr, kR * skr);
+    const double gfac = w * iK * iK / rr * aW * iK;
+    const cplx dgz = cmul(cmk(0.0, 1.0), cscale(cbsk, gfac * KTz));
+    const cplx dge = cmul(cmk(0.0, 1.0), cscale(cbsk, gfac * KTe));
+    // bil_sdHz_De0_r: ce/aK^4 ((k kR + 3 i k) K.vt cth - i k aK^2);  _De1_r: sin(kR)/(aK^5 r)(3 K.vt cth - aK^2)
+    // theta function: sth * (De0 - i De1)
+    const double i4 = 1.0 / (aK * aK * aK * aK);
+    const double i5 = i4 / (aK * rr);
+    const cplx h0z = cmul(ce, cmk(k * kR * KTz * cth, 3.0 * k * KTz * cth - k * aK * aK));
+    const cplx h0e = cmul(ce, cmk(k * kR * KTe * sth, 3.0 * k * KTe * sth - k * aK * aK));
+    const double h1z = skr * i5 * (3.0 * KTz * cth - aK * aK);
+    const double h1e = skr * i5 * (3.0 * KTe * sth - aK * aK);
+    const cplx hz = cscale(cmk(h0z.re * i4, h0z.im * i4 - h1z), w * sth);
+    const cplx he = cscale(cmk(h0e.re * i4, h0e.im * i4 - h1e), w * cth);
+    double N[4];
+    bem_Nn4(z, e, N);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      A.dgz[2 * n] += dgz.re * N[n]; A.dgz[2 * n + 1] += dgz.im * N[n];
+      A.dge[2 * n] += dge.re * N[n]; A.dge[2 * n + 1] += dge.im * N[n];
+      A.dhz[2 * n] += hz.re * N[n];  A.dhz[2 * n + 1] += hz.im * N[n];
+      A.dhe[2 * n] += he.re * N[n];  A.dhe[2 * n + 1] += he.im * N[n];
+    }
+  }
+  // (4) PV pair: 2 x 64 angles over [0, pi), 12 radii, symmetric points +-r (subtracted)
+  for (int pt = threadIdx.x; pt < 128 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const int hh = idx >> 6, m = idx & 63;
+    const double tht = 0.25 * CUDART_PI * c_q.xh[m] + (0.25 + 0.5 * hh) * CUDART_PI;
+    const double wth = 0.25 * CUDART_PI * c_q.wh[m];
+    double sth, cth;
+    sincos(tht, &sth, &cth);
+    const double rr = 0.5 * BEM_DEPS * (c_q.xl[ir] + 1.0);
+    const double w = wth * 0.5 * BEM_DEPS * c_q.wl[ir] / rr;
+    double Np[4], Nm[4], Kp[3], Km[3], Wp[3], Wm[3];
+    const double zp = rr * cth + zt, ep = rr * sth + et, zm = -rr * cth + zt, em = -rr * sth + et;
+    bem_K(el, rr, cth, sth, zt, et, Kp);
+    bem_K(el, -rr, cth, sth, zt, et, Km);
+    for (int d = 0; d < 3; ++d) {
+      Wp[d] = el.cw[d][0] + el.cw[d][1] * zp + el.cw[d][2] * ep;
+      Wm[d] = el.cw[d][0] + el.cw[d][1] * zm + el.cw[d][2] * em;
+    }
+    bem_Nn4(zp, ep, Np);
+    bem_Nn4(zm, em, Nm);
+    const double aKp = sqrt(dot3(Kp, Kp)), aKm = sqrt(dot3(Km, Km));
+    const double aWp = sqrt(dot3(Wp, Wp)), aWm = sqrt(dot3(Wm, Wm));
+    const double ccp = cos(k * aKp * rr), ccm = cos(-k * aKm * rr);
+    const double KpTz = dot3(Kp, vz), KmTz = dot3(Km, vz), KpTe = dot3(Kp, ve), KmTe = dot3(Km, ve);
+    // bil_sdG_DP_r: ccp/aKp^2 (Kp.vt/aKp) N(p) aWp - (same with m)
+    const double gzp = ccp / (aKp * aKp) * (KpTz / aKp) * aWp, gzm = ccm / (aKm * aKm) * (KmTz / aKm) * aWm;
+    const double gep = ccp / (aKp * aKp) * (KpTe / aKp) * aWp, gem = ccm / (aKm * aKm) * (KmTe / aKm) * aWm;
+    // bil_sdHz_DP_r: ccp/aKp^5 (3 Kp.vt cth - aKp^2) N(p) - (m); outer sth
+    const double ip5 = 1.0 / (aKp * aKp * aKp * aKp * aKp), im5 = 1.0 / (aKm * aKm * aKm * aKm * aKm);
+    const double hzp = ccp * ip5 * (3.0 * KpTz * cth - aKp * aKp), hzm = ccm * im5 * (3.0 * KmTz * cth - aKm * aKm);
+    const double hep = ccp * ip5 * (3.0 * KpTe * sth - aKp * aKp), hem = ccm * im5 * (3.0 * KmTe * sth - aKm * aKm);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      // subtracted from dG and dH (the reference's "dCC[i] -= tC"), real-valued
+      A.dgz[2 * n] -= w * (gzp * Np[n] - gzm * Nm[n]);
+      A.dge[2 * n] -= w * (gep * Np[n] - gem * Nm[n]);
+      A.dhz[2 * n] -= w * sth * (hzp * Np[n] - hzm * Nm[n]);
+      A.dhe[2 * n] -= w * cth * (hep * Np[n] - hem * Nm[n]);
+    }
+    // bil_sdFz_DP_r / _Fe_: added
+    A.fz += w * sth * (ip5 * (3.0 * KpTz * cth - aKp * aKp) - im5 * (3.0 * KmTz * cth - aKm * aKm));
+    A.fe += w * cth * (ip5 * (3.0 * KpTe * sth - aKp * aKp) - im5 * (3.0 * KmTe * sth - aKm * aKm));
+  }
+  set_status(status, st);
+  __shared__ double sm[51 * (NP_THREADS / 32) + 51];
+  double v[51];
+#pragma unroll
+  for (int c = 0; c < 51; ++c) v[c] = Av[c];
+  block_reduce<51>(v, sm);
+  if (threadIdx.x == 0) {
+    const size_t N = (size_t)D.ne * 4;
+    const double sg = D.sid[t] < 0 ? -1.0 : 1.0;
+    const bool plane = D.plane[te] != 0;
+    const double bdC = bem_bdC(el);
+    const double iTz = 1.0 / sqrt(dot3(vz, vz)), iTe = 1.0 / sqrt(dot3(ve, ve));
+    const double c = BEM_I_FP;
+    double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
+    double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
+    double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * t));
+    double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
+    double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * t));
+    double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
+    for (int n = 0; n < 4; ++n) {
+      g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
+      const double hs = plane ? 0.0 : sg * bdC * c;
+      h2[n] = make_double2(v[8 + 2 * n] * hs, v[8 + 2 * n + 1] * hs);
+      // dG: times -1/4pi/|T|; not affected by the element orientation
+      gz[n] = make_double2(-c * iTz * v[16 + 2 * n], -c * iTz * v[16 + 2 * n + 1]);
+      ge[n] = make_double2(-c * iTe * v[24 + 2 * n], -c * iTe * v[24 + 2 * n + 1]);
+      const double hzs = plane ? 0.0 : sg * bdC * c * iTz, hes = plane ? 0.0 : sg * bdC * c * iTe;
+      hz[n] = make_double2(v[32 + 2 * n] * hzs, v[32 + 2 * n + 1] * hzs);
+      he[n] = make_double2(v[40 + 2 * n] * hes, v[40 + 2 * n + 1] * hes);
+    }
+    selfF[3 * p + 0] = plane ? 0.0 : sg * v[48] * bdC * c;
+    selfF[3 * p + 1] = plane ? 0.0 : sg * v[49] * bdC * c * iTz;
+    selfF[3 * p + 2] = plane ? 0.0 : sg * v[50] * bdC * c * iTe;
+  }
+}
+
+// ------------------------------------------------------------------ diagonal / dF
+__global__ void k_diag(bem_dom_dev D, int exterior, const double *__restrict__ rowF, const int *__restrict__ near_n,
+                       const double *__restrict__ nearF, const double *__restrict__ selfF, double *__restrict__ H,
+                       double *__restrict__ dF, unsigned *status) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= D.ne * 4) return;
+  double F = rowF[3 * p], Fz = rowF[3 * p + 1], Fe = rowF[3 * p + 2];
+  const int n = near_n[p];
+  for (int k = 0; k < n; ++k) {
+    const double *nf = nearF + ((size_t)p * BEM_MAXNEAR + k) * 3;
+    F += nf[0]; Fz += nf[1]; Fe += nf[2];
+  }
+  F += selfF[3 * p]; Fz += selfF[3 * p + 1]; Fe += selfF[3 * p + 2];
+  const double d = exterior ? 1.0 + F : F;
+  const size_t N = (size_t)D.ne * 4;
+  H[2 * ((size_t)p * N + p)] += d;
+  dF[3 * p] = d;
+  dF[3 * p + 1] = Fz;
+  dF[3 * p + 2] = Fe;
+  if (!isfinite(d) || !isfinite(Fz) || !isfinite(Fe)) set_status(status, BEM_ST_NONFINITE);
+}
+
+// ------------------------------------------------------------------ point evaluators (tests)
+__global__ void k_faddeeva(const double *__restrict__ z, int n, double *__restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const cplx r = bem_faddeeva(z[2 * i], z[2 * i + 1]);
+  w[2 * i] = r.re;
+  w[2 * i + 1] = r.im;
+}
+
+__global__ void __launch_bounds__(128) k_qpgf_points(bem_qp q, const double *__restrict__ r, int n, double *__restrict__ G,
+                                                     double *__restrict__ dG, int *__restrict__ ret) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bem_gval v;
+  const int e = bem_qpgf(q, r[3 * i], r[3 * i + 1], r[3 * i + 2], v);
+  ret[i] = e;
+  G[2 * i] = v.g.re; G[2 * i + 1] = v.g.im;
+  dG[6 * i + 0] = v.gx.re; dG[6 * i + 1] = v.gx.im;
+  dG[6 * i + 2] = v.gy.re; dG[6 * i + 3] = v.gy.im;
+  dG[6 * i + 4] = v.gz.re; dG[6 * i + 5] = v.gz.im;
+}
+
+// ------------------------------------------------------------------ host launchers
+extern "C" int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh) {
+  bem_quad qq;
+  for (int i = 0; i < BEM_GLN; ++i) { qq.xl[i] = xl[i]; qq.wl[i] = wl[i]; }
+  for (int i = 0; i < BEM_GHN; ++i) { qq.xh[i] = xh[i]; qq.wh[i] = wh[i]; }
+  const double zt[4] = {-BEM_P44, BEM_P44, BEM_P44, -BEM_P44}, et[4] = {-BEM_P44, -BEM_P44, BEM_P44, BEM_P44};
+  for (int i = 0; i < 4; ++i) { qq.zt[i] = zt[i]; qq.et[i] = et[i]; }
+  bem_wconst wc;
+  wc.relerr = BEM_MEPS;
+  wc.a = CUDART_PI / sqrt(-log(wc.relerr * 0.5));
+  wc.a2 = wc.a * wc.a;
+  wc.c = 2.0 / CUDART_PI * wc.a;
+  for (int n = 1; n <= BEM_W_TAB; ++n) wc.tab[n - 1] = exp(-wc.a2 * n * n);
+  if (cudaMemcpyToSymbol(c_q, &qq, sizeof(qq)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_w, &wc, sizeof(wc)) != cudaSuccess) return -1;
+  return 0;
+}
+
+extern "C" int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_faddeeva<<<(n + 127) / 128, 128, 0, st>>>(z, n, w);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_qpgf_points<<<(n + 127) / 128, 128, 0, st>>>(*q, r, n, G, dG, ret);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
+                                   bem_scratch *S, double *G, double *H, double *dG, double *dH, double *dF,
+                                   cudaStream_t st) {
+  const int N = D->ne * 4;
+  if (D->ne <= 0) return 0;
+  k_classify<<<N, 128, 0, st>>>(*D, S->rowF, S->near_s, S->near_n, S->flag, S->status);
+  if (periodic) {
+    const long long npairs = (long long)N * D->ne;
+    const long long chunk = 1LL << 26;  // keep grid.x well inside limits
+    for (long long p0 = 0; p0 < npairs; p0 += chunk) {
+      const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
+      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, p0, np);
+    }
+    k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status);
+    k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status);
+  } else {
+    const long long npairs = (long long)N * D->ne;
+    k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
+    k_fs_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
+    k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+  }
+  k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, exterior, S->rowF, S->near_n, S->nearF, S->selfF, H, dF, S->status);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}

@@ -1,0 +1,513 @@
+// C ABI (include/bemgpu.h): device buffers, problem upload, the assembly /
+// solve sequence and the cuSOLVER factorisations.
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+#include <vector>
+#include "../../include/bemgpu.h"
+#include "bem_kernels.h"
+#include "bem_solve.h"
+
+#define BEMGPU_MAXDOM 8
+
+struct bemgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cusolverDnHandle_t solver = nullptr;
+  cusolverDnParams_t params = nullptr;
+  char err[512] = {0};
+  // problem
+  bool loaded = false;
+  int Ne = 0, NN = 0, MN = 0, n = 0;
+  bem_qp qp;
+  std::vector<int> dom_ne, dom_off;
+  std::vector<double> k0, c0, rho0, k2;
+  // device problem data
+  double *cr = nullptr, *cw = nullptr, *ren = nullptr, *wen = nullptr;
+  uint8_t *plane = nullptr;
+  int *sid = nullptr, *rowidx = nullptr, *npe = nullptr, *eni = nullptr, *md = nullptr, *dom_ne_d = nullptr, *dom_off_d = nullptr;
+  double *hk2 = nullptr, *Pi = nullptr, *dPi = nullptr, *p_inc = nullptr, *v_inc = nullptr, *rho0_d = nullptr, *k2_d = nullptr;
+  // per-domain matrices and boundary values
+  double *G[BEMGPU_MAXDOM] = {}, *H[BEMGPU_MAXDOM] = {}, *dG[BEMGPU_MAXDOM] = {}, *dH[BEMGPU_MAXDOM] = {}, *dF[BEMGPU_MAXDOM] = {};
+  double *P[BEMGPU_MAXDOM] = {}, *dP[BEMGPU_MAXDOM] = {}, *pv[BEMGPU_MAXDOM] = {}, *dpv[BEMGPU_MAXDOM] = {};
+  bem_scratch scr = {};
+  // solve work
+  double *A = nullptr, *b = nullptr, *tpv = nullptr, *W = nullptr, *B3 = nullptr;
+  int64_t *ipiv = nullptr;
+  int *info = nullptr;
+  void *dwork = nullptr;
+  size_t dwork_sz = 0;
+  std::vector<char> hwork;
+  double *fout = nullptr, *rc_d = nullptr;
+  unsigned *status = nullptr;
+  bem_sys_dev sys;
+};
+
+static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
+  if (c) snprintf(c->err, sizeof(c->err), "%s: %s", what, cudaGetErrorString(e));
+  return -1;
+}
+#define CK(call, what)                           \
+  do {                                           \
+    cudaError_t _e = (call);                     \
+    if (_e != cudaSuccess) return fail(c, what, _e); \
+  } while (0)
+#define CKS(call, what)                                                         \
+  do {                                                                          \
+    cusolverStatus_t _s = (call);                                               \
+    if (_s != CUSOLVER_STATUS_SUCCESS) {                                        \
+      snprintf(c->err, sizeof(c->err), "%s: cusolver status %d", what, (int)_s); \
+      return -1;                                                                \
+    }                                                                           \
+  } while (0)
+
+template <class T>
+static cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)p, count * sizeof(T));
+}
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Gauss-Legendre tables and Faddeeva constants are uploaded once per device.
+static int g_const_dev = -1;
+
+static void free_problem(bemgpu_ctx *c) {
+  dfree(c->cr); dfree(c->cw); dfree(c->ren); dfree(c->wen); dfree(c->plane);
+  dfree(c->sid); dfree(c->rowidx); dfree(c->npe); dfree(c->eni); dfree(c->md); dfree(c->dom_ne_d); dfree(c->dom_off_d);
+  dfree(c->hk2); dfree(c->Pi); dfree(c->dPi); dfree(c->p_inc); dfree(c->v_inc); dfree(c->rho0_d); dfree(c->k2_d);
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
+    dfree(c->G[d]); dfree(c->H[d]); dfree(c->dG[d]); dfree(c->dH[d]); dfree(c->dF[d]);
+    dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
+  }
+  dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
+  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv);
+  if (c->dwork) cudaFree(c->dwork);
+  c->dwork = nullptr;
+  c->dwork_sz = 0;
+  c->loaded = false;
+}
+
+extern "C" int bemgpu_create(int device, void *stream, bemgpu_ctx **out) {
+  *out = nullptr;
+  bemgpu_ctx *c = new bemgpu_ctx();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { delete c; return -1; }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return -1; }
+    c->own_stream = true;
+  }
+  if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS || cusolverDnSetStream(c->solver, c->stream) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnCreateParams(&c->params) != CUSOLVER_STATUS_SUCCESS) {
+    delete c;
+    return -1;
+  }
+  if (dalloc(&c->info, 1) != cudaSuccess || dalloc(&c->status, 1) != cudaSuccess || dalloc(&c->fout, 8) != cudaSuccess ||
+      dalloc(&c->rc_d, 4) != cudaSuccess) {
+    delete c;
+    return -1;
+  }
+  cudaMemset(c->status, 0, sizeof(unsigned));
+  *out = c;
+  return 0;
+}
+
+extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_problem(c);
+  dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d);
+  if (c->params) cusolverDnDestroyParams(c->params);
+  if (c->solver) cusolverDnDestroy(c->solver);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" const char *bemgpu_error(const bemgpu_ctx *c) { return c ? c->err : "no context"; }
+
+extern "C" unsigned bemgpu_status(bemgpu_ctx *c) {
+  unsigned s = 0;
+  cudaMemcpyAsync(&s, c->status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+  cudaStreamSynchronize(c->stream);
+  return s;
+}
+
+extern "C" int bemgpu_sync(bemgpu_ctx *c) {
+  CK(cudaStreamSynchronize(c->stream), "sync");
+  return 0;
+}
+
+// Lattice quantities derived once per (k, k_par, lattice): the reference
+// recomputes them inside every Green's-function call (d3_qpgf_d2.c:126-156,
+// 1679-1681, 1850-1856).
+static void qp_prepare(const double *p, bem_qp *q) {
+  memset(q, 0, sizeof(*q));
+  q->k = p[0]; q->kx = p[1]; q->ky = p[2];
+  q->d1x = p[4]; q->d1y = p[5]; q->d2x = p[6]; q->d2y = p[7];
+  q->det = q->d1x * q->d2y - q->d2x * q->d1y;
+  q->idet = 1.0 / q->det;
+  q->aidet = fabs(q->idet);
+  const double cpd = 2.0 * M_PI * q->idet;
+  q->g1x = cpd * q->d2y; q->g1y = -cpd * q->d2x;
+  q->g2x = -cpd * q->d1y; q->g2y = cpd * q->d1x;
+  q->d2sq = q->d2x * q->d2x + q->d2y * q->d2y;
+  q->g2sq = q->g2x * q->g2x + q->g2y * q->g2y;
+  q->g1g2 = q->g1x * q->g2x + q->g1y * q->g2y;
+  const double adp = sqrt(pow(q->d1x + q->d2x, 2) + pow(q->d1y + q->d2y, 2));
+  const double adm = sqrt(pow(q->d1x - q->d2x, 2) + pow(q->d1y - q->d2y, 2));
+  q->eta0 = sqrt(fabs(q->det) / (4.0 * M_PI) * adp / adm);
+  q->nc1 = (int)round((q->kx * q->d1x + q->ky * q->d1y) / (2.0 * M_PI));
+  // choice between the Ewald and the pure spectral sum (d3hm_qpgf_d2_v1)
+  const double k2 = q->k * q->k;
+  const int n1 = q->nc1, n2 = (int)round((q->kx * q->d2x + q->ky * q->d2y) / (2.0 * M_PI));
+  const double ad12 = q->d1x * q->d1x + q->d1y * q->d1y, ad22 = q->d2sq;
+  const double aNx = -q->kx + n1 * cpd * q->d2y - n2 * cpd * q->d1y;
+  const double aNy = -q->ky - n1 * cpd * q->d2x + n2 * cpd * q->d1x;
+  const double bN = sqrt(k2 - aNx * aNx - aNy * aNy);
+  double aNpx, aNpy, aNmx, aNmy;
+  if (ad22 < ad12) {
+    aNpx = -q->kx + (n1 + 15) * cpd * q->d2y - n2 * cpd * q->d1y;
+    aNpy = -q->ky - (n1 + 15) * cpd * q->d2x + n2 * cpd * q->d1x;
+    aNmx = -q->kx + (n1 - 15) * cpd * q->d2y - n2 * cpd * q->d1y;
+    aNmy = -q->ky - (n1 - 15) * cpd * q->d2x + n2 * cpd * q->d1x;
+  } else {
+    aNpx = -q->kx + n1 * cpd * q->d2y - (n2 + 15) * cpd * q->d1y;
+    aNpy = -q->ky - n1 * cpd * q->d2x + (n2 + 15) * cpd * q->d1x;
+    aNmx = -q->kx + n1 * cpd * q->d2y - (n2 - 15) * cpd * q->d1y;
+    aNmy = -q->ky - n1 * cpd * q->d2x + (n2 - 15) * cpd * q->d1x;
+  }
+  const double bNp = k2 - aNpx * aNpx - aNpy * aNpy;
+  const double bNm = k2 - aNmx * aNmx - aNmy * aNmy;
+  if (bNp > 0.0 || bNm > 0.0) {
+    q->ewald_only = 1;
+  } else {
+    q->ewald_only = 0;
+    q->sel_bp = sqrt(-bNp);
+    q->sel_bm = sqrt(-bNm);
+    q->sel_cp = bN / q->sel_bp;
+    q->sel_cm = bN / q->sel_bm;
+  }
+}
+
+// Gauss-Legendre nodes and weights on [-1,1] by Newton iteration on the
+// three-term Legendre recurrence (the rule the reference tabulates with
+// gauleg, com_src/gauleg.c).
+static void gl_rule(int n, double *x, double *w) {
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p2 = p1;
+        p1 = p0;
+        p0 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p2) / j;
+      }
+      dp = n * (z * p0 - p1) / (z * z - 1.0);
+      const double dz = p0 / dp;
+      z -= dz;
+      if (fabs(dz) <= 3e-16) break;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+  if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+static int ensure_constants(bemgpu_ctx *c, const double *xl, const double *wl, const double *xh, const double *wh) {
+  double bxl[BEM_GLN_H], bwl[BEM_GLN_H], bxh[BEM_GHN_H], bwh[BEM_GHN_H];
+  if (!xl) { gl_rule(BEM_GLN_H, bxl, bwl); xl = bxl; wl = bwl; }
+  if (!xh) { gl_rule(BEM_GHN_H, bxh, bwh); xh = bxh; wh = bwh; }
+  if (bem_set_constants(xl, wl, xh, wh) != 0) {
+    if (c) snprintf(c->err, sizeof(c->err), "constant upload failed");
+    return -1;
+  }
+  g_const_dev = c ? c->device : 0;
+  return 0;
+}
+
+template <class T>
+static int upload(bemgpu_ctx *c, T **dst, const T *src, size_t count, const char *what) {
+  CK(dalloc(dst, count), what);
+  if (src && count) CK(cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
+  return 0;
+}
+
+extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
+  CK(cudaSetDevice(c->device), "set device");
+  free_problem(c);
+  if (pr->MN + 1 > BEMGPU_MAXDOM) { snprintf(c->err, sizeof(c->err), "at most %d domains", BEMGPU_MAXDOM); return -2; }
+  if (pr->ps != 1) { snprintf(c->err, sizeof(c->err), "only the quasi-periodic problem (ps=1) is implemented"); return -2; }
+  for (int e = 0; e < pr->Ne; ++e)
+    if (pr->npe[e] != 4) { snprintf(c->err, sizeof(c->err), "element %d: only bilinear (4-node) elements are implemented", e + 1); return -2; }
+  if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
+  c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
+  qp_prepare(pr->qp, &c->qp);
+  const int nd = pr->MN + 1;
+  c->dom_ne.assign(pr->dom_ne, pr->dom_ne + nd);
+  c->dom_off.assign(nd, 0);
+  int tot = 0;
+  for (int d = 0; d < nd; ++d) { c->dom_off[d] = tot; tot += c->dom_ne[d]; }
+  c->k0.assign(pr->k0, pr->k0 + nd);
+  c->c0.assign(pr->c0, pr->c0 + nd);
+  c->rho0.assign(pr->rho0, pr->rho0 + nd);
+  c->k2.assign(pr->k2, pr->k2 + 2 * nd);
+  // global row of each (domain, element, node): the reference's row order
+  // (create_matrix_csr_dac writes rows domain by domain, element by element)
+  std::vector<int> rowidx(4 * (size_t)tot, -1);
+  int row = 0;
+  for (int d = 0; d < nd; ++d)
+    for (int s = 0; s < c->dom_ne[d]; ++s) {
+      const int asd = abs(pr->sid[c->dom_off[d] + s]) - 1;
+      for (int l = 0; l < pr->npe[asd]; ++l) rowidx[4 * (size_t)(c->dom_off[d] + s) + l] = row++;
+    }
+  if (row != c->n) { snprintf(c->err, sizeof(c->err), "row count %d != 2 NN = %d", row, c->n); return -2; }
+  std::vector<double> hk2(2 * (size_t)pr->Ne);
+  for (int e = 0; e < pr->Ne; ++e) {
+    const double *km = pr->k2 + 2 * pr->md[e], *ks = pr->k2 + 2 * pr->sd[e];
+    const double den = ks[0] * ks[0] + ks[1] * ks[1];
+    hk2[2 * e] = (km[0] * ks[0] + km[1] * ks[1]) / den;
+    hk2[2 * e + 1] = (km[1] * ks[0] - km[0] * ks[1]) / den;
+  }
+  const size_t Ne = pr->Ne;
+  if (upload(c, &c->cr, pr->cr, Ne * 12, "cr") || upload(c, &c->cw, pr->cw, Ne * 9, "cw") ||
+      upload(c, &c->ren, pr->ren, Ne * 12, "ren") || upload(c, &c->wen, pr->wen, Ne * 12, "wen") ||
+      upload(c, &c->plane, pr->plane, Ne, "plane") || upload(c, &c->sid, pr->sid, (size_t)tot, "sid") ||
+      upload(c, &c->rowidx, rowidx.data(), rowidx.size(), "rowidx") || upload(c, &c->npe, pr->npe, Ne, "npe") ||
+      upload(c, &c->eni, pr->eni, Ne * 4, "eni") || upload(c, &c->md, pr->md, Ne, "md") ||
+      upload(c, &c->dom_ne_d, c->dom_ne.data(), (size_t)nd, "dom_ne") || upload(c, &c->dom_off_d, c->dom_off.data(), (size_t)nd, "dom_off") ||
+      upload(c, &c->hk2, hk2.data(), hk2.size(), "hk2") || upload(c, &c->Pi, pr->Pi, Ne * 8, "Pi") ||
+      upload(c, &c->dPi, pr->dPi, Ne * 8, "dPi") || upload(c, &c->p_inc, pr->p_inc, Ne * 8, "p_inc") ||
+      upload(c, &c->v_inc, pr->v_inc, Ne * 24, "v_inc") || upload(c, &c->rho0_d, pr->rho0, (size_t)nd, "rho0") ||
+      upload(c, &c->k2_d, pr->k2, 2 * (size_t)nd, "k2"))
+    return -1;
+  // per-domain outputs
+  int maxN = 0;
+  for (int d = 0; d < nd; ++d) {
+    const size_t N = 4 * (size_t)c->dom_ne[d];
+    if ((int)N > maxN) maxN = (int)N;
+    CK(dalloc(&c->G[d], 2 * N * N), "G");
+    CK(dalloc(&c->H[d], 2 * N * N), "H");
+    if (d > 0) {
+      CK(dalloc(&c->dG[d], 4 * N * N), "dG");
+      CK(dalloc(&c->dH[d], 4 * N * N), "dH");
+    }
+    CK(dalloc(&c->dF[d], 3 * N), "dF");
+    CK(dalloc(&c->P[d], 2 * N), "P");
+    CK(dalloc(&c->dP[d], 2 * N), "dP");
+    CK(dalloc(&c->pv[d], 6 * N), "pv");
+    CK(dalloc(&c->dpv[d], 6 * N), "dpv");
+    CK(cudaMemsetAsync(c->pv[d], 0, 6 * N * sizeof(double), c->stream), "pv");
+  }
+  int maxNe = 0;
+  for (int d = 0; d < nd; ++d) maxNe = c->dom_ne[d] > maxNe ? c->dom_ne[d] : maxNe;
+  CK(dalloc(&c->scr.rowF, 3 * (size_t)maxN), "rowF");
+  CK(dalloc(&c->scr.near_s, (size_t)maxN * BEM_MAXNEAR_H), "near_s");
+  CK(dalloc(&c->scr.near_n, (size_t)maxN), "near_n");
+  CK(dalloc(&c->scr.nearF, (size_t)maxN * BEM_MAXNEAR_H * 3), "nearF");
+  CK(dalloc(&c->scr.selfF, 3 * (size_t)maxN), "selfF");
+  CK(dalloc(&c->scr.flag, (size_t)maxN * maxNe), "flag");
+  c->scr.status = c->status;
+  const size_t n = c->n;
+  CK(dalloc(&c->A, 2 * n * n), "A");
+  CK(dalloc(&c->b, 2 * n), "b");
+  CK(dalloc(&c->tpv, 6 * (size_t)c->NN), "tpv");
+  CK(dalloc(&c->W, 2 * (size_t)maxN * maxN), "W");
+  CK(dalloc(&c->B3, 6 * (size_t)maxN), "B3");
+  CK(dalloc(&c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
+  CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "status");
+  // device view of the system
+  bem_sys_dev &S = c->sys;
+  memset(&S, 0, sizeof(S));
+  S.n = c->n; S.NN = c->NN; S.MN = c->MN;
+  S.dom_ne = c->dom_ne_d; S.dom_off = c->dom_off_d;
+  for (int d = 0; d < nd; ++d) S.dom_ne_h[d] = c->dom_ne[d];
+  S.sid = c->sid; S.rowidx = c->rowidx; S.npe = c->npe; S.eni = c->eni; S.md = c->md; S.hk2 = c->hk2;
+  S.Pi = c->Pi; S.dPi = c->dPi; S.p_inc = c->p_inc; S.v_inc = c->v_inc;
+  S.cr = c->cr; S.ren = c->ren; S.wen = c->wen; S.rho0 = c->rho0_d; S.k2 = c->k2_d;
+  const double a = 0.5773502691896257645091;
+  const double zt[4] = {-a, a, a, -a}, et[4] = {-a, -a, a, a};
+  for (int i = 0; i < 4; ++i) { S.zt44[i] = zt[i]; S.et44[i] = et[i]; }
+  c->loaded = true;
+  return 0;
+}
+
+extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  for (int d = 0; d <= c->MN; ++d) {
+    bem_dom_dev D;
+    D.ne = c->dom_ne[d];
+    D.sid = c->sid + c->dom_off[d];
+    D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane;
+    const int periodic = d == 0;
+    if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], &c->scr, c->G[d], c->H[d], c->dG[d], c->dH[d], c->dF[d],
+                            c->stream) != 0)
+      return fail(c, "assembly launch", cudaGetLastError());
+  }
+  return 0;
+}
+
+// LU factorisation of the row-major n x n complex matrix M in place; cuSOLVER
+// sees the column-major transpose, so solves below use op = T.
+static int lu_factor(bemgpu_ctx *c, double *M, int64_t n, const char *what) {
+  size_t dsz = 0, hsz = 0;
+  CKS(cusolverDnXgetrf_bufferSize(c->solver, c->params, n, n, CUDA_C_64F, M, n, CUDA_C_64F, &dsz, &hsz), what);
+  if (dsz > c->dwork_sz) {
+    if (c->dwork) cudaFree(c->dwork);
+    CK(cudaMalloc(&c->dwork, dsz), what);
+    c->dwork_sz = dsz;
+  }
+  if (hsz > c->hwork.size()) c->hwork.resize(hsz);
+  CKS(cusolverDnXgetrf(c->solver, c->params, n, n, CUDA_C_64F, M, n, c->ipiv, CUDA_C_64F, c->dwork, c->dwork_sz,
+                       hsz ? c->hwork.data() : nullptr, hsz, c->info),
+      what);
+  return 0;
+}
+
+static int lu_solve(bemgpu_ctx *c, const double *M, int64_t n, int64_t nrhs, double *B, const char *what) {
+  CKS(cusolverDnXgetrs(c->solver, c->params, CUBLAS_OP_T, n, nrhs, CUDA_C_64F, M, n, c->ipiv, CUDA_C_64F, B, n, c->info), what);
+  return 0;
+}
+
+static int check_info(bemgpu_ctx *c, const char *what) {
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->info, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
+  CK(cudaStreamSynchronize(c->stream), what);
+  if (info != 0) {
+    snprintf(c->err, sizeof(c->err), "%s: factorisation info %d", what, info);
+    return -3;
+  }
+  return 0;
+}
+
+extern "C" int bemgpu_solve(bemgpu_ctx *c) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  const size_t n = c->n;
+  CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
+  CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
+  for (int d = 0; d <= c->MN; ++d)
+    if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], c->A, c->b, c->stream)) return fail(c, "gather", cudaGetLastError());
+  if (lu_factor(c, c->A, (int64_t)n, "global LU")) return -1;
+  if (check_info(c, "global LU")) return -3;
+  if (lu_solve(c, c->A, (int64_t)n, 1, c->b, "global solve")) return -1;
+  for (int d = 0; d <= c->MN; ++d)
+    if (bem_launch_store(&c->sys, d, c->b, c->P[d], c->dP[d], c->stream)) return fail(c, "store", cudaGetLastError());
+  // particle velocity: interior domains first, then domain 0 from the interface condition
+  CK(cudaMemsetAsync(c->tpv, 0, 6 * (size_t)c->NN * sizeof(double), c->stream), "tpv");
+  for (int d = 1; d <= c->MN; ++d)
+    if (bem_launch_pv(&c->sys, d, c->dG[d], c->dH[d], c->dF[d], c->P[d], c->dP[d], c->pv[d], c->tpv, c->stream))
+      return fail(c, "pv", cudaGetLastError());
+  if (bem_launch_pv(&c->sys, 0, nullptr, nullptr, nullptr, nullptr, nullptr, c->pv[0], c->tpv, c->stream))
+    return fail(c, "pv0", cudaGetLastError());
+  // dpv: G_d dpv = H_d pv per domain (solve_dpv_bv)
+  for (int d = 0; d <= c->MN; ++d) {
+    const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
+    if (Nd == 0) continue;
+    if (bem_launch_dpv_rhs((int)Nd, c->H[d], c->pv[d], c->B3, c->stream)) return fail(c, "dpv rhs", cudaGetLastError());
+    CK(cudaMemcpyAsync(c->W, c->G[d], 2 * Nd * Nd * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "G copy");
+    if (lu_factor(c, c->W, Nd, "dpv LU")) return -1;
+    if (check_info(c, "dpv LU")) return -3;
+    if (lu_solve(c, c->W, Nd, 3, c->B3, "dpv solve")) return -1;
+    if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
+  }
+  return 0;
+}
+
+extern "C" int bemgpu_run(bemgpu_ctx *c) {
+  int r = bemgpu_assemble(c);
+  if (r) return r;
+  return bemgpu_solve(c);
+}
+
+extern "C" int bemgpu_get_solution(bemgpu_ctx *c, int d, double *P, double *dP, double *pv, double *dpv) {
+  if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain"); return -2; }
+  const size_t N = 4 * (size_t)c->dom_ne[d];
+  if (P) CK(cudaMemcpyAsync(P, c->P[d], 2 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "P");
+  if (dP) CK(cudaMemcpyAsync(dP, c->dP[d], 2 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "dP");
+  if (pv) CK(cudaMemcpyAsync(pv, c->pv[d], 6 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "pv");
+  if (dpv) CK(cudaMemcpyAsync(dpv, c->dpv[d], 6 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "dpv");
+  CK(cudaStreamSynchronize(c->stream), "get solution");
+  return 0;
+}
+
+extern "C" int bemgpu_get_matrix(bemgpu_ctx *c, int d, int which, double *dst) {
+  if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain"); return -2; }
+  const size_t N = 4 * (size_t)c->dom_ne[d];
+  const double *src = nullptr;
+  size_t cnt = 0;
+  switch (which) {
+    case 0: src = c->G[d]; cnt = 2 * N * N; break;
+    case 1: src = c->H[d]; cnt = 2 * N * N; break;
+    case 2: src = c->dG[d]; cnt = 4 * N * N; break;
+    case 3: src = c->dH[d]; cnt = 4 * N * N; break;
+    case 4: src = c->dF[d]; cnt = 3 * N; break;
+    default: break;
+  }
+  if (!src) { snprintf(c->err, sizeof(c->err), "matrix %d of domain %d is not kept", which, d); return -2; }
+  CK(cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "get matrix");
+  CK(cudaStreamSynchronize(c->stream), "get matrix");
+  return 0;
+}
+
+extern "C" int bemgpu_force(bemgpu_ctx *c, int type, const double *rc, double *F, double *N) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  if (type != 0) { snprintf(c->err, sizeof(c->err), "force type %d not implemented on the device", type); return -2; }
+  CK(cudaMemcpyAsync(c->rc_d, rc, 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "rc");
+  if (bem_launch_force0(&c->sys, c->P[0], c->pv[0], c->rc_d, c->c0[0], c->rho0[0], c->fout, c->stream))
+    return fail(c, "force", cudaGetLastError());
+  double out[6];
+  CK(cudaMemcpyAsync(out, c->fout, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "force");
+  CK(cudaStreamSynchronize(c->stream), "force");
+  for (int i = 0; i < 3; ++i) { F[i] = out[i]; N[i] = out[3 + i]; }
+  return 0;
+}
+
+// ---------------------------------------------------------------- point evaluators
+extern "C" int bemgpu_faddeeva_w(const double *z, int n, double *w) {
+  if (n <= 0) return 0;
+  if (ensure_constants(nullptr, nullptr, nullptr, nullptr, nullptr) != 0) return -1;
+  double *dz = nullptr, *dw = nullptr;
+  if (cudaMalloc(&dz, 2 * sizeof(double) * n) != cudaSuccess) return -1;
+  if (cudaMalloc(&dw, 2 * sizeof(double) * n) != cudaSuccess) { cudaFree(dz); return -1; }
+  cudaMemcpy(dz, z, 2 * sizeof(double) * n, cudaMemcpyHostToDevice);
+  int r = bem_launch_faddeeva(dz, n, dw, 0);
+  if (r == 0 && cudaMemcpy(w, dw, 2 * sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess) r = -1;
+  cudaFree(dz);
+  cudaFree(dw);
+  return r;
+}
+
+extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G, double *dG, int *ret) {
+  if (n <= 0) return 0;
+  if (ensure_constants(nullptr, nullptr, nullptr, nullptr, nullptr) != 0) return -1;
+  bem_qp q;
+  qp_prepare(qpar, &q);
+  double *dr = nullptr, *dg = nullptr, *ddg = nullptr;
+  int *dret = nullptr;
+  int rc = -1;
+  if (cudaMalloc(&dr, 3 * sizeof(double) * n) == cudaSuccess && cudaMalloc(&dg, 2 * sizeof(double) * n) == cudaSuccess &&
+      cudaMalloc(&ddg, 6 * sizeof(double) * n) == cudaSuccess && cudaMalloc(&dret, sizeof(int) * n) == cudaSuccess) {
+    cudaMemcpy(dr, r, 3 * sizeof(double) * n, cudaMemcpyHostToDevice);
+    rc = bem_launch_qpgf(&q, dr, n, dg, ddg, dret, 0);
+    if (rc == 0) {
+      if (cudaMemcpy(G, dg, 2 * sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(dG, ddg, 6 * sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(ret, dret, sizeof(int) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = -1;
+    }
+  }
+  cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret);
+  return rc;
+}

@@ -1,0 +1,81 @@
+// Element geometry and quadrature tables on the device.
+//
+// Bilinear element (d3qd2_src/d3qd2_elem.c:890-1028):
+//   r(z,e) = cr0 + cr1 z + cr2 e + cr3 z e,  W(z,e) = cw0 + cw1 z + cw2 e
+//   interpolation functions with nodes at (+-1/sqrt3, +-1/sqrt3)  (bil_Nn, :903)
+#pragma once
+#include <cuda_runtime.h>
+
+#define BEM_GLN 12
+#define BEM_GHN 64
+#define BEM_CBD_SDF 0.5        // near-singular switch on |dF/dt|   (d3qd2_const.h:80)
+#define BEM_CDFH 1.0e-3        // central-difference step           (d3qd2_const.h:35)
+#define BEM_DEPS 0.1           // radius of the PV disc D_eps        (d3qd2_const.h:34)
+#define BEM_I_FP 7.957747154594766788444e-2  // 1/(4 pi)
+#define BEM_P44 0.5773502691896257645091     // 1/sqrt(3)
+#define BEM_MAXNEAR 64         // near-singular sources kept per collocation node
+
+struct bem_quad {
+  double xl[BEM_GLN], wl[BEM_GLN];
+  double xh[BEM_GHN], wh[BEM_GHN];
+  double zt[4], et[4];        // collocation node parameters (zt_44, et_44)
+};
+static __constant__ bem_quad c_q;  // one copy per translation unit
+
+// element constants of element e (0-based), 21 doubles
+struct bem_el { double cr[3][4]; double cw[3][3]; };
+
+__device__ __forceinline__ void bem_load_el(const double *__restrict__ cr, const double *__restrict__ cw, int e, bem_el &el) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) el.cr[d][c] = __ldg(cr + (size_t)e * 12 + d * 4 + c);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) el.cw[d][c] = __ldg(cw + (size_t)e * 9 + d * 3 + c);
+  }
+}
+
+// interpolation function N_n(z,e) (bil_Nn)
+__device__ __forceinline__ void bem_Nn4(double z, double e, double N[4]) {
+  const double ia = 1.0 / BEM_P44;
+  const double zm = 1.0 - z * ia, zp = 1.0 + z * ia, em = 1.0 - e * ia, ep = 1.0 + e * ia;
+  N[0] = 0.25 * zm * em;
+  N[1] = 0.25 * zp * em;
+  N[2] = 0.25 * zp * ep;
+  N[3] = 0.25 * zm * ep;
+}
+
+__device__ __forceinline__ void bem_rw(const bem_el &el, double z, double e, double r[3], double w[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r[d] = el.cr[d][0] + el.cr[d][1] * z + el.cr[d][2] * e + el.cr[d][3] * z * e;
+    w[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+  }
+}
+
+// corner distances and angles seen from (zt,et) (bil_calc_node_r_th, d3qd2_elem.c:1014)
+__device__ __forceinline__ void bem_node_r_th(double zt, double et, double r[5], double th[5]) {
+  const double ztp = 1.0 - zt, ztm = -1.0 - zt, etp = 1.0 - et, etm = -1.0 - et;
+  r[0] = sqrt(ztm * ztm + etm * etm);
+  r[1] = sqrt(ztp * ztp + etm * etm);
+  r[2] = sqrt(ztp * ztp + etp * etp);
+  r[3] = sqrt(ztm * ztm + etp * etp);
+  r[4] = r[0];
+  th[0] = atan2(etm, ztm);
+  th[1] = atan2(etm, ztp);
+  th[2] = atan2(etp, ztp);
+  th[3] = atan2(etp, ztm);
+  th[4] = th[0] + 2.0 * CUDART_PI;
+}
+
+// polar radius of the edge of sub-triangle (r0,th0)-(r1,th1) at angle th
+__device__ __forceinline__ double bem_rmax(double r0, double r1, double th0, double th1, double th) {
+  return r0 * r1 * sin(th1 - th0) / (r0 * sin(th - th0) - r1 * sin(th - th1));
+}
+
+// K(r,theta) = d r(zeta,eta) / d rho along the ray (the bracket in bil_sG_r, bil_coef.c:408)
+__device__ __forceinline__ void bem_K(const bem_el &el, double rr, double cth, double sth, double zt, double et, double K[3]) {
+  const double cross = rr * cth * sth + zt * sth + et * cth;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) K[d] = el.cr[d][1] * cth + el.cr[d][2] * sth + el.cr[d][3] * cross;
+}

@@ -1,0 +1,37 @@
+// Device-side views and launcher prototypes shared by the .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "bem_types.h"
+
+// One domain's element list and the element tables it indexes (device pointers).
+struct bem_dom_dev {
+  int ne;                       // elements bordering the domain
+  const int *sid;               // signed element ids (1-based, sign = orientation)
+  const double *cr, *cw, *ren;  // element tables, see bem_types.h
+  const uint8_t *plane;         // 1 if the element is plane (bil_check_plane)
+};
+
+// Scratch used by one domain assembly (sized for N = 4 ne rows).
+struct bem_scratch {
+  double *rowF;     // [N][3] geometric F, dF/dtz, dF/dte summed over regular sources
+  int *near_s;      // [N][BEM_MAXNEAR] near-singular source indices, sorted
+  int *near_n;      // [N]
+  double *nearF;    // [N][BEM_MAXNEAR][3]
+  double *selfF;    // [N][3]
+  uint8_t *flag;    // [N][ne] 0 regular, 1 near-singular, 2 self
+  unsigned *status; // BEM_ST_* bits
+};
+
+extern "C" {
+int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh);
+int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
+int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
+int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,
+                        double *G, double *H, double *dG, double *dH, double *dF, cudaStream_t st);
+}
+
+// host-side copies of the table sizes
+#define BEM_GLN_H 12
+#define BEM_GHN_H 64
+#define BEM_MAXNEAR_H 64

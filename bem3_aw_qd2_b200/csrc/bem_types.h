@@ -1,0 +1,46 @@
+/* Plain-C types shared by the host library (C99) and the CUDA kernels.
+ *
+ * Element tables follow the reference's element constants
+ * (d3qd2_src/d3qd2_elem.h:22-45, filled by init_elem_const,
+ * d3qd2_src/bem3_aw_qd2.c:941-1023), flattened to contiguous arrays indexed by
+ * (absolute element id - 1):
+ *   cr [e][3][4]  r(zeta,eta) = cr0 + cr1 zeta + cr2 eta + cr3 zeta eta
+ *   cw [e][3][3]  W(zeta,eta) = cw0 + cw1 zeta + cw2 eta   (normal, |W| = Jacobian)
+ *   ren[e][4][3]  collocation node coordinates (zeta,eta = +-1/sqrt(3))
+ *   wen[e][4][3]  W at the collocation nodes
+ */
+#ifndef BEM_TYPES_H
+#define BEM_TYPES_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Lattice / Bloch data for the quasi-periodic Green's function (the reference's
+ * QPD2, qgf2_src/d3_qpgf_d2.h:32-36) plus quantities derived once per
+ * (k, k_par, lattice) by bem_qp_prepare(). */
+typedef struct bem_qp {
+  double k, kx, ky;             /* wave number and in-plane Bloch wave vector */
+  double d1x, d1y, d2x, d2y;    /* lattice vectors */
+  double det, idet, aidet;      /* det = d1 x d2, 1/det, |1/det| */
+  double g1x, g1y, g2x, g2y;    /* reciprocal lattice vectors */
+  double d2sq, g2sq, g1g2;      /* |d2|^2, |g2|^2, g1.g2 */
+  double eta0;                  /* Ewald splitting parameter before the per-point cap */
+  double sel_cp, sel_bp;        /* spectral-only test: bN/bNp, bNp  */
+  double sel_cm, sel_bm;        /*                     bN/bNm, bNm  */
+  int nc1;                      /* round(k_par . d1 / 2 pi) */
+  int ewald_only;               /* 1: always use the Ewald sum */
+} bem_qp;
+
+/* status word bits written by the kernels (never trapped on the device) */
+#define BEM_ST_QPGF_LIMIT   0x01  /* a lattice sum reached its term limit */
+#define BEM_ST_RAYLEIGH     0x02  /* beta_n == 0 (Rayleigh anomaly) */
+#define BEM_ST_NEAR_OVERFLOW 0x04 /* more near-singular sources in a row than the table holds */
+#define BEM_ST_NONFINITE    0x08  /* a non-finite coefficient was produced */
+#define BEM_ST_GEOMETRY     0x10  /* negative polar radius in a singular integral */
+#define BEM_ST_SOLVE        0x20  /* singular matrix in a factorisation */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,110 @@
+/* bemgpu.h -- C ABI of the B200 boundary-element engine.
+ *
+ * Plain C types only (pointers, sizes, doubles as interleaved re/im pairs);
+ * no CUDA or PyTorch types.  Every entry point returns 0 on success and a
+ * negative code on failure; bemgpu_error() gives the message.  Device faults
+ * are never used as an error channel: kernels write status bits
+ * (BEMGPU_ST_*) that the host turns into an error return.
+ *
+ * These entry points replace the compute inside the reference's drop-in API
+ * (d3qd2_src/bem3_aw_qd2.h); the host library in bem3_aw_qd2_b200/csrc/host
+ * calls them from its re-implementation of that API, so the reference's
+ * drivers (aw_d3qd2_bv_solver.c, example1.c) link against it unchanged.
+ */
+#ifndef BEMGPU_H
+#define BEMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEMGPU_ST_QPGF_LIMIT    0x01 /* a lattice sum reached its term limit (d3_qpgf_d2.c error -1/-2) */
+#define BEMGPU_ST_RAYLEIGH      0x02 /* beta_n == 0: Rayleigh anomaly (d3_qpgf_d2.c:882, 2006) */
+#define BEMGPU_ST_NEAR_OVERFLOW 0x04 /* > 64 near-singular sources for one collocation node */
+#define BEMGPU_ST_NONFINITE     0x08 /* non-finite coefficient */
+#define BEMGPU_ST_GEOMETRY      0x10 /* negative polar radius in a singular integral */
+#define BEMGPU_ST_SOLVE         0x20 /* singular matrix in an LU factorisation */
+
+/* The boundary-value problem, in the reference's element-table form
+ * (AQD2/BOUD, d3qd2_src/d3qd2_elem.h:13-65).  Element e (0-based) is the
+ * reference's element id e+1.  Complex numbers are (re, im) pairs. */
+typedef struct bemgpu_problem {
+  int Ne;              /* elements */
+  int NN;              /* element nodes, sum of nodes per element */
+  int MN;              /* media; domains are 0 (host, open) .. MN; MN <= 7 */
+  int ps;              /* 1: quasi-periodic host domain (the only mode implemented) */
+  double qp[8];        /* QPD2: k, kx, ky, kz, d1x, d1y, d2x, d2y */
+  const double *cr;    /* [Ne][3][4] element geometry constants */
+  const double *cw;    /* [Ne][3][3] normal-vector constants */
+  const double *ren;   /* [Ne][4][3] collocation nodes */
+  const double *wen;   /* [Ne][4][3] normal (Jacobian) vectors at the nodes */
+  const int *npe;      /* [Ne] nodes per element (4: bilinear quad) */
+  const int *eni;      /* [Ne][4] element node ids 0..NN-1 */
+  const int *md;       /* [Ne] main domain */
+  const int *sd;       /* [Ne] sub domain */
+  const int *dom_ne;   /* [MN+1] elements bordering each domain */
+  const int *sid;      /* signed element ids (1-based) of domain 0, then 1, ... */
+  const double *k0;    /* [MN+1] wave numbers */
+  const double *k2;    /* [MN+1] complex i omega rho */
+  const double *rho0;  /* [MN+1] densities */
+  const double *c0;    /* [MN+1] sound speeds */
+  const double *Pi;    /* [Ne][4] complex incident potential at the nodes (init_boundary_data) */
+  const double *dPi;   /* [Ne][4] complex normal derivative of Pi */
+  const double *p_inc; /* [Ne][4] complex incident pressure at the nodes */
+  const double *v_inc; /* [Ne][4][3] complex incident particle velocity at the nodes */
+  const double *xl, *wl; /* 12-point Gauss-Legendre nodes/weights on [-1,1] (BOUD xli/wli) */
+  const double *xh, *wh; /* 64-point Gauss-Legendre nodes/weights (BOUD xhi/whi) */
+  const unsigned char *plane; /* [Ne] 1 if the element is plane (bil_check_plane, d3qd2_elem.c:986) */
+} bemgpu_problem;
+
+typedef struct bemgpu_ctx bemgpu_ctx;
+
+/* Context on one CUDA device; stream may be NULL (a private stream is made). */
+int bemgpu_create(int device, void *stream, bemgpu_ctx **out);
+void bemgpu_destroy(bemgpu_ctx *ctx);
+const char *bemgpu_error(const bemgpu_ctx *ctx);
+unsigned bemgpu_status(bemgpu_ctx *ctx); /* BEMGPU_ST_* bits accumulated since load */
+
+/* Copy a problem from host memory to the device (replaces the state that
+ * read_aqd2/initialize_aqd2 build, bem3_aw_qd2.c:3-109). */
+int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
+
+/* Coefficient matrices of every domain (create_cmatrix,
+ * bem3_aw_qd2_solve_bieq.c:124-218). */
+int bemgpu_assemble(bemgpu_ctx *ctx);
+
+/* Global system, LU solve, P/dP, pv, dpv (bem3_aw_qd2_solve_bieq.c:220-750). */
+int bemgpu_solve(bemgpu_ctx *ctx);
+
+/* solve_bieq_aqd2 (bem3_aw_qd2_solve_bieq.c:3): assemble + solve. */
+int bemgpu_run(bemgpu_ctx *ctx);
+
+/* Boundary values of domain d to host arrays: P, dP [Ne_d][4] complex,
+ * pv, dpv [Ne_d][4][3] complex (SUBD, d3qd2_elem.h:13-19). */
+int bemgpu_get_solution(bemgpu_ctx *ctx, int d, double *P, double *dP, double *pv, double *dpv);
+
+/* Coefficient matrix of domain d to a host array, in the layout of the
+ * reference's temporary files (bem3_aw_qd2_solve_bieq.c:176-182):
+ * which 0: G [N][N] complex, 1: H, 2: dG [2N][N] complex, 3: dH, 4: dF [N][3] real. */
+int bemgpu_get_matrix(bemgpu_ctx *ctx, int d, int which, double *dst);
+
+/* Radiation force and torque about rc (force_FN_aqd2, bem3_aw_qd2_force.c:4).
+ * type 0: 4-point rule on the node values. */
+int bemgpu_force(bemgpu_ctx *ctx, int type, const double *rc, double *F, double *N);
+
+/* Wait for all queued work of the context. */
+int bemgpu_sync(bemgpu_ctx *ctx);
+
+/* Faddeeva w(z) at n points (host arrays of (re, im) pairs), relative error
+ * 1e-15 (Faddeeva_w, qgf2_src/Faddeeva.cc:679, called with MEPS). */
+int bemgpu_faddeeva_w(const double *z, int n, double *w);
+
+/* Quasi-periodic Green's function and gradient at n points r[n][3] (host
+ * arrays): G[n] complex, dG[n][3] complex, ret[n] = lattice terms used or the
+ * reference's negative error code (d3hm_qpgf_d2_v1, qgf2_src/d3_qpgf_d2.c:124). */
+int bemgpu_qpgf(const double *qp, const double *r, int n, double *G, double *dG, int *ret);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,138 @@
+"""CPU-only checks: the native libraries load and export their C ABI, the
+drop-in structs keep the reference's byte layout, the host-side set-up
+(read_aqd2 + initialize_aqd2) reproduces the reference's element tables, and
+the oracle reproduces the reference's shipped results."""
+import ctypes
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+INC = os.path.join(ROOT, "include")
+LIB = os.path.join(ROOT, "bem3_aw_qd2_b200", "lib")
+
+
+def declared_functions(header):
+    src = open(os.path.join(INC, header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"typedef struct[^;]*?\}[^;]*;", "", src, flags=re.S)
+    names = re.findall(r"^(?:const\s+)?(?:void|int|double|char|unsigned|struct\s+\w+)\s*\**\s*(\w+)\s*\([^;]*\)\s*;",
+                       src, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.mark.parametrize("header,lib", [("bemgpu.h", "libbemgpu.so"), ("bem3_aw_qd2.h", "libbem3_aw_qd2.so")])
+def test_library_exports_every_declared_symbol(header, lib):
+    L = ctypes.CDLL(os.path.join(LIB, lib))
+    names = declared_functions(header)
+    assert len(names) > 8
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_struct_layout_matches_dat_format(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text('#include "bem3_aw_qd2.h"\nint main(){printf("%zu %zu\\n",sizeof(AQD2),sizeof(Apw));return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I" + INC, str(src), "-o", str(exe)])
+    assert subprocess.check_output([str(exe)]).split() == [b"2720", b"240"]
+
+
+_DUMP = r"""
+import ctypes, sys
+lib = ctypes.CDLL(sys.argv[1])
+args = [b"x"] + [a.encode() for a in sys.argv[2:6]] + [b"unused.dat"]
+argv = (ctypes.c_char_p * 6)(*args)
+buf = ctypes.create_string_buffer(2720)
+lib.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_void_p]
+lib.read_aqd2(6, argv, buf)
+lib.initialize_aqd2(buf)
+lib.dat_write_aqd2.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+lib.dat_write_aqd2(sys.argv[6].encode(), buf)
+"""
+
+
+def _write_dat(libpath, files, out):
+    subprocess.check_call([sys.executable, "-c", _DUMP, libpath, *files, out])
+    return open(out, "rb").read()
+
+
+def test_host_setup_matches_reference():
+    from oracle import refwrap
+    from bem3_aw_qd2_b200 import meshgen
+    if not refwrap.available():
+        pytest.skip("oracle/_ref not built")
+    d = tempfile.mkdtemp()
+    files = meshgen.write_inputs(d, **meshgen.CONFIGS["sphere24"])
+    mine = _write_dat(os.path.join(LIB, "libbem3_aw_qd2.so"), files, os.path.join(d, "mine.dat"))
+    ref = _write_dat(refwrap.LIBPATH, files, os.path.join(d, "ref.dat"))
+    assert len(mine) == len(ref)
+    # everything after the raw AQD2 struct: media, plane wave, mesh, element
+    # tables, incident data, domain lists (bit-identical)
+    assert mine[2720:] == ref[2720:]
+    # inside the struct: Gauss-Legendre tables within 2 ulp
+    off_bd = 3 * 128 + 7 * 8 + 8 + 6 * 8 + 240  # file names, rv/th/tv, MN(+pad), 6 pointers, Apw
+    a = np.frombuffer(mine[:2720], dtype=np.uint8)
+    b = np.frombuffer(ref[:2720], dtype=np.uint8)
+    assert off_bd > 0 and a.size == b.size
+    tail_m = np.frombuffer(mine[2720 - 8 - 2 * 8 * (12 + 64):2720 - 8], dtype=np.float64)
+    tail_r = np.frombuffer(ref[2720 - 8 - 2 * 8 * (12 + 64):2720 - 8], dtype=np.float64)
+    assert np.max(np.abs(tail_m - tail_r)) < 4.5e-16
+
+
+def test_meshgen_orientation_and_pairs():
+    from bem3_aw_qd2_b200 import meshgen
+    nodes, quads = meshgen.cube_sphere(4)
+    assert quads.shape == (96, 4)
+    c = nodes.mean(axis=0)
+    for q in quads:
+        r = nodes[q]
+        assert np.dot(np.cross(r[1] - r[0], r[3] - r[0]), r.mean(axis=0) - c) > 0
+    assert np.allclose(np.linalg.norm(nodes, axis=1), 0.3)
+
+
+def test_oracle_reproduces_reference_example1_log():
+    """Pins the reference build: force (type 0) and field (type 0) on the
+    reference's own shipped ex.dat must equal example1.log."""
+    from oracle import refwrap
+    exdat = "/root/reference/ex.dat"
+    if not (refwrap.available() and os.path.exists(exdat)):
+        pytest.skip("needs oracle/_ref and the reference sources")
+    code = r"""
+import ctypes, sys
+import numpy as np
+L = ctypes.CDLL(sys.argv[1])
+buf = ctypes.create_string_buffer(2720)
+L.dat_read_aqd2.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+L.dat_read_aqd2(sys.argv[2].encode(), buf)
+F = np.zeros(3); N = np.zeros(3); rc = np.zeros(3)
+d = ctypes.POINTER(ctypes.c_double)
+L.force_FN_aqd2.argtypes = [d, d, d, ctypes.c_int, ctypes.c_void_p]
+L.force_FN_aqd2(F.ctypes.data_as(d), N.ctypes.data_as(d), rc.ctypes.data_as(d), 0, buf)
+p = np.zeros(2); v = np.zeros(6); r = np.array([-0.03, 0.01, 0.002])
+L.pv_t_aqd2.argtypes = [d, d, d, ctypes.c_int, ctypes.c_void_p]
+L.pv_t_aqd2(p.ctypes.data_as(d), v.ctypes.data_as(d), r.ctypes.data_as(d), 0, buf)
+print(repr(F.tolist()), repr(N.tolist()), repr(p.tolist()), repr(v.tolist()))
+"""
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    out = subprocess.check_output([sys.executable, "-c", code, refwrap.LIBPATH, exdat], env=env, timeout=600).decode()
+    F, N, p, v = [np.array(eval(s)) for s in out.strip().split(" [")[0:1] + ["[" + s for s in out.strip().split(" [")[1:]]]
+    # example1.log:52-53 (type 0) and :39-42 (p, v at (-0.03, 0.01, 0.002), type 0)
+    assert np.allclose(F, [1.17265981863126e-12, -4.25894012043065e-24, 3.30594943545801e-12], rtol=1e-12, atol=1e-22)
+    assert abs(N[1] - (-1.74832751729785e-17)) < 1e-27
+    assert np.allclose(p, [-1.60864515194396e+01, 7.21171164151370e+00], rtol=1e-13)
+    assert np.allclose(v, [-2.95881854346144e-06, -4.77748008913537e-07, -8.75837999315613e-06, -8.48556131494143e-06,
+                           -6.43210173002179e-06, -7.67679566899160e-06], rtol=1e-12)
+
+
+def test_golden_fixtures_present(golden_dir):
+    for f in ("faddeeva.npz", "qpgf.npz", "sphere24.npz"):
+        assert os.path.exists(os.path.join(golden_dir, f))
+    g = np.load(os.path.join(golden_dir, "sphere24.npz"))
+    assert g["G0"].shape == (96, 96) and g["dG1"].shape == (192, 96)

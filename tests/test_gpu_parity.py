@@ -1,0 +1,103 @@
+"""Parity of the CUDA path with the reference (golden fixtures made by the
+reference's own code, tests/golden/make_golden.py).
+
+Tolerances (stated here, used below):
+  Faddeeva w(z)                 relative 1e-13
+  quasi-periodic G, grad G      relative 1e-12 of the point's |G|, |grad G|
+  coefficient matrices G,H,dG,dH  1e-10 relative to the row maximum
+  dF (geometric)                1e-10 relative to the column maximum
+  P, dP, pv, dpv                1e-9 relative to the array maximum
+  force / torque (type 0)       1e-9 relative to |F| (|N| for the torque)
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(ROOT, "tests", "golden")
+
+
+def rel_rows(a, b):
+    scale = np.max(np.abs(b), axis=1, keepdims=True)
+    scale[scale == 0] = 1.0
+    return float(np.max(np.abs(a - b) / scale))
+
+
+def rel_max(a, b):
+    s = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / (s if s > 0 else 1.0))
+
+
+def test_faddeeva_matches_reference():
+    from bem3_aw_qd2_b200 import api
+    g = np.load(os.path.join(GOLD, "faddeeva.npz"))
+    w = api.faddeeva_w(g["z"])
+    ref = g["w"]
+    err = np.abs(w - ref) / np.maximum(np.abs(ref), 1e-300)
+    assert np.all(np.isfinite(w))
+    assert err.max() < 1e-13, "worst z=%s" % g["z"][np.argmax(err)]
+
+
+@pytest.mark.parametrize("lattice", ["square", "oblique"])
+def test_qpgf_matches_reference(lattice):
+    from bem3_aw_qd2_b200 import api
+    g = np.load(os.path.join(GOLD, "qpgf.npz"))
+    qp, r = g[lattice + "_qp"], g[lattice + "_r"]
+    G, dG, ret = api.qpgf(qp, r)
+    Gr, dGr, retr = g[lattice + "_v1_G"], g[lattice + "_v1_dG"], g[lattice + "_v1_ret"]
+    ok = retr > 0
+    assert np.all((ret > 0) == ok)
+    eG = np.abs(G - Gr)[ok] / np.abs(Gr)[ok]
+    edG = np.linalg.norm(dG - dGr, axis=1)[ok] / np.linalg.norm(dGr, axis=1)[ok]
+    assert eG.max() < 1e-12
+    assert edG.max() < 1e-12
+
+
+@pytest.fixture(scope="module")
+def sphere24():
+    from bem3_aw_qd2_b200 import api, meshgen
+    d = tempfile.mkdtemp(prefix="bem24_")
+    files = meshgen.write_inputs(d, **meshgen.CONFIGS["sphere24"])
+    case = api.Case.from_files(*files)
+    case.solve()
+    return case, np.load(os.path.join(GOLD, "sphere24.npz"))
+
+
+def test_sphere24_matrices(sphere24):
+    case, g = sphere24
+    N = 96
+    assert rel_rows(case.matrix(0, "G", N), g["G0"]) < 1e-10
+    assert rel_rows(case.matrix(0, "H", N), g["H0"]) < 1e-10
+    assert rel_rows(case.matrix(1, "G", N), g["G1"]) < 1e-10
+    assert rel_rows(case.matrix(1, "H", N), g["H1"]) < 1e-10
+    assert rel_rows(case.matrix(1, "dG", N), g["dG1"]) < 1e-10
+    assert rel_rows(case.matrix(1, "dH", N), g["dH1"]) < 1e-10
+    for d in (0, 1):
+        dF = case.matrix(d, "dF", N)
+        ref = g["dF%d" % d]
+        # column 0 is (1+)F ~ 0.5; columns 1, 2 are sums of O(1/4pi) terms that
+        # cancel to ~1e-8 on a closed surface, so they are compared absolutely
+        assert np.max(np.abs(dF[:, 0] - ref[:, 0])) < 1e-10 * np.max(np.abs(ref[:, 0]))
+        assert np.max(np.abs(dF[:, 1:] - ref[:, 1:])) < 1e-11
+
+
+def test_sphere24_solution(sphere24):
+    case, g = sphere24
+    for d in (0, 1):
+        P, dP, pv, dpv = case.solution(d, 24)
+        assert rel_max(P, g["P%d" % d]) < 1e-9
+        assert rel_max(dP, g["dP%d" % d]) < 1e-9
+        assert rel_max(pv, g["pv%d" % d]) < 1e-9
+        assert rel_max(dpv, g["dpv%d" % d]) < 1e-9
+
+
+def test_sphere24_force(sphere24):
+    case, g = sphere24
+    F, N = case.force(0)
+    assert np.linalg.norm(F - g["F0"]) < 1e-9 * np.linalg.norm(g["F0"])
+    assert np.linalg.norm(N - g["N0"]) < 1e-9 * max(np.linalg.norm(g["N0"]), 1e-30) + 1e-9 * np.linalg.norm(g["F0"]) * 0.3
+    assert case.status() == 0
