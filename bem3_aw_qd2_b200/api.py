@@ -48,6 +48,11 @@ def libs():
         g.bemgpu_force.argtypes = [vp, ctypes.c_int, _d, _d, _d]
         g.bemgpu_faddeeva_w.argtypes = [_d, ctypes.c_int, _d]
         g.bemgpu_qpgf.argtypes = [_d, _d, ctypes.c_int, _d, _d, _i]
+        g.bemgpu_stream.argtypes = [vp]
+        g.bemgpu_stream.restype = vp
+        g.bemgpu_set_profiling.argtypes = [vp, ctypes.c_int]
+        g.bemgpu_phase_times.argtypes = [vp, _d, ctypes.c_int]
+        g.bemgpu_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
         h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
         for name in ("print_aqd2", "initialize_aqd2", "finalize_aqd2", "solve_bieq_aqd2"):
             getattr(h, name).argtypes = [vp]
@@ -58,6 +63,7 @@ def libs():
         h.aqd2_device_context.restype = vp
         h.aqd2_last_timing.argtypes = [_d]
         h.aqd2_set_device.argtypes = [ctypes.c_int]
+        h.aqd2_set_verbose.argtypes = [ctypes.c_int]
         _host, _gpu = h, g
     return _host, _gpu
 

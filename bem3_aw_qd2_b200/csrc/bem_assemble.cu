@@ -52,6 +52,20 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) { r
 
 __device__ __forceinline__ void set_status(unsigned *st, unsigned bits) { if (bits) atomicOr(st, bits); }
 
+// warp-aggregated work counters (lattice terms and Green's-function points);
+// every lane of the warp must call it
+__device__ __forceinline__ void count_work(unsigned long long *ctr, unsigned long long terms, unsigned long long pts) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    terms += __shfl_down_sync(0xffffffffu, terms, o);
+    pts += __shfl_down_sync(0xffffffffu, pts, o);
+  }
+  if ((threadIdx.x & 31) == 0 && pts) {
+    atomicAdd(ctr, terms);
+    atomicAdd(ctr + 3, pts);
+  }
+}
+
 // geometric F and its tangential derivatives at one quadrature point:
 // tD = (R.W)/R^3, dF_v = (3 (R.v)(R.W)/R^2 - W.v)/R^3   (q0_bil_dcoef_v2_cc.c:165-200)
 __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], const bem_node &n, double &f, double &fz, double &fe) {
@@ -152,7 +166,8 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restr
 #define RP_THREADS 288
 __global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp q, const uint8_t *__restrict__ flag,
                                                            double *__restrict__ G, double *__restrict__ H,
-                                                           unsigned *status, long long pair0, long long npairs) {
+                                                           unsigned *status, unsigned long long *terms, long long pair0,
+                                                           long long npairs) {
   __shared__ double acc[16][RP_THREADS + 1];
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long pair = pair0 + 2LL * blockIdx.x + lp;
@@ -163,6 +178,7 @@ __global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp
   double v[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  unsigned long long nterm = 0, npt = 0;
   if (work) {
     bem_node nd;
     int t, te;
@@ -177,6 +193,8 @@ __global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp
     bem_gval gv;
     const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
     if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
+    nterm = rc > 0 ? (unsigned long long)rc : 0ULL;
+    npt = 1;
     const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
     const double wt = c_q.wl[i] * c_q.wl[j];
     const cplx g = cscale(gv.g, aW * wt);
@@ -191,6 +209,7 @@ __global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp
       v[8 + 2 * a + 1] = h.im * N[a];
     }
   }
+  count_work(terms + 0, nterm, npt);
 #pragma unroll
   for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
   __syncthreads();
@@ -237,7 +256,8 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*N
 
 __global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q, const int *__restrict__ near_s,
                                                         const int *__restrict__ near_n, double *__restrict__ G,
-                                                        double *__restrict__ H, double *__restrict__ nearF, unsigned *status) {
+                                                        double *__restrict__ H, double *__restrict__ nearF, unsigned *status,
+                                                        unsigned long long *terms) {
   const int p = blockIdx.x, k = blockIdx.y;
   if (k >= near_n[p]) return;
   const int s = near_s[(size_t)p * BEM_MAXNEAR + k];
@@ -250,6 +270,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q,
 #pragma unroll
   for (int c = 0; c < 19; ++c) v[c] = 0.0;
   unsigned st = 0;
+  unsigned long long nterm = 0, npt = 0;
   for (int pt = threadIdx.x; pt < BEM_GHN * BEM_GHN; pt += NP_THREADS) {
     const int i = pt / BEM_GHN, j = pt % BEM_GHN;
     const double z = c_q.xh[i], e = c_q.xh[j];
@@ -259,6 +280,8 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q,
     bem_gval gv;
     const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+    ++npt;
     const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
     const double wt = c_q.wh[i] * c_q.wh[j];
     const cplx g = cscale(gv.g, aW * wt);
@@ -278,6 +301,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q,
     v[17] += wt * fz;
     v[18] += wt * fe;
   }
+  count_work(terms + 1, nterm, npt);
   set_status(status, st);
   __shared__ double sm[19 * (NP_THREADS / 32) + 19];
   block_reduce<19>(v, sm);
@@ -340,7 +364,7 @@ __device__ __forceinline__ double bem_bdC(const bem_el &el) {
 // periodic self pair: one block per collocation node p
 __global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ selfF,
-                                                        unsigned *status) {
+                                                        unsigned *status, unsigned long long *terms) {
   const int p = blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
@@ -349,6 +373,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q,
   const double zt = c_q.zt[tn], et = c_q.et[tn];
   double r[5], th[5];
   bem_node_r_th(zt, et, r, th);
+  unsigned long long nterm = 0, npt = 0;
   double v[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = 0.0;
@@ -372,6 +397,8 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q,
     bem_gval gv;
     const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+    ++npt;
     const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
     const cplx g = cscale(gv.g, aW * rr * w);
     const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), rr * w);
@@ -385,6 +412,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q,
       v[8 + 2 * a + 1] += h.im * N[a];
     }
   }
+  count_work(terms + 2, nterm, npt);
   // F at the node and at (zt+-h, et), (zt, et+-h) for the central differences
   // (q0_bil_dcoef_bd_tz0_cc_DV / _te0_, q0_bil_dcoef_v2_cc.c:336-399)
   const bool plane = D.plane[te] != 0;
@@ -865,25 +893,33 @@ extern "C" int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *
 
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
                                    bem_scratch *S, double *G, double *H, double *dG, double *dH, double *dF,
-                                   cudaStream_t st) {
+                                   cudaStream_t st, cudaEvent_t *ev) {
+  // ev (optional): 6 events recorded around classify | regular | near | self | diag
   const int N = D->ne * 4;
   if (D->ne <= 0) return 0;
+  if (ev) cudaEventRecord(ev[0], st);
   k_classify<<<N, 128, 0, st>>>(*D, S->rowF, S->near_s, S->near_n, S->flag, S->status);
+  if (ev) cudaEventRecord(ev[1], st);
+  const long long npairs = (long long)N * D->ne;
   if (periodic) {
-    const long long npairs = (long long)N * D->ne;
     const long long chunk = 1LL << 26;  // keep grid.x well inside limits
     for (long long p0 = 0; p0 < npairs; p0 += chunk) {
       const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
-      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, p0, np);
+      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
     }
-    k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status);
-    k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status);
+    if (ev) cudaEventRecord(ev[2], st);
+    k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
+    if (ev) cudaEventRecord(ev[3], st);
+    k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
   } else {
-    const long long npairs = (long long)N * D->ne;
     k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
+    if (ev) cudaEventRecord(ev[2], st);
     k_fs_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
+    if (ev) cudaEventRecord(ev[3], st);
     k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
   }
+  if (ev) cudaEventRecord(ev[4], st);
   k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, exterior, S->rowF, S->near_n, S->nearF, S->selfF, H, dF, S->status);
+  if (ev) cudaEventRecord(ev[5], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -44,7 +44,11 @@ struct bemgpu_ctx {
   std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
   unsigned *status = nullptr;
+  unsigned long long *terms = nullptr;
   bem_sys_dev sys;
+  // optional per-phase timing: 6 events per domain (0, 1), then 5 for the solve
+  bool prof = false;
+  cudaEvent_t ev[17] = {};
 };
 
 static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
@@ -114,11 +118,14 @@ extern "C" int bemgpu_create(int device, void *stream, bemgpu_ctx **out) {
     return -1;
   }
   if (dalloc(&c->info, 1) != cudaSuccess || dalloc(&c->status, 1) != cudaSuccess || dalloc(&c->fout, 8) != cudaSuccess ||
-      dalloc(&c->rc_d, 4) != cudaSuccess) {
+      dalloc(&c->rc_d, 4) != cudaSuccess || dalloc(&c->terms, 6) != cudaSuccess) {
     delete c;
     return -1;
   }
+  for (int i = 0; i < 17; ++i)
+    if (cudaEventCreate(&c->ev[i]) != cudaSuccess) { delete c; return -1; }
   cudaMemset(c->status, 0, sizeof(unsigned));
+  cudaMemset(c->terms, 0, 6 * sizeof(unsigned long long));
   *out = c;
   return 0;
 }
@@ -128,7 +135,9 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_problem(c);
-  dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d);
+  dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
+  for (int i = 0; i < 17; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->params) cusolverDnDestroyParams(c->params);
   if (c->solver) cusolverDnDestroy(c->solver);
   if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -320,6 +329,8 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   CK(dalloc(&c->scr.selfF, 3 * (size_t)maxN), "selfF");
   CK(dalloc(&c->scr.flag, (size_t)maxN * maxNe), "flag");
   c->scr.status = c->status;
+  c->scr.terms = c->terms;
+  CK(cudaMemsetAsync(c->terms, 0, 6 * sizeof(unsigned long long), c->stream), "counters");
   const size_t n = c->n;
   CK(dalloc(&c->A, 2 * n * n), "A");
   CK(dalloc(&c->b, 2 * n), "b");
@@ -352,8 +363,9 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
     D.sid = c->sid + c->dom_off[d];
     D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane;
     const int periodic = d == 0;
+    cudaEvent_t *ev = c->prof && d < 2 ? c->ev + 6 * d : nullptr;
     if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], &c->scr, c->G[d], c->H[d], c->dG[d], c->dH[d], c->dF[d],
-                            c->stream) != 0)
+                            c->stream, ev) != 0)
       return fail(c, "assembly launch", cudaGetLastError());
   }
   return 0;
@@ -395,15 +407,18 @@ static int check_info(bemgpu_ctx *c, const char *what) {
 extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   const size_t n = c->n;
+  if (c->prof) cudaEventRecord(c->ev[12], c->stream);
   CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
   CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], c->A, c->b, c->stream)) return fail(c, "gather", cudaGetLastError());
+  if (c->prof) cudaEventRecord(c->ev[13], c->stream);
   if (lu_factor(c, c->A, (int64_t)n, "global LU")) return -1;
   if (check_info(c, "global LU")) return -3;
   if (lu_solve(c, c->A, (int64_t)n, 1, c->b, "global solve")) return -1;
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_store(&c->sys, d, c->b, c->P[d], c->dP[d], c->stream)) return fail(c, "store", cudaGetLastError());
+  if (c->prof) cudaEventRecord(c->ev[14], c->stream);
   // particle velocity: interior domains first, then domain 0 from the interface condition
   CK(cudaMemsetAsync(c->tpv, 0, 6 * (size_t)c->NN * sizeof(double), c->stream), "tpv");
   for (int d = 1; d <= c->MN; ++d)
@@ -411,6 +426,7 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
       return fail(c, "pv", cudaGetLastError());
   if (bem_launch_pv(&c->sys, 0, nullptr, nullptr, nullptr, nullptr, nullptr, c->pv[0], c->tpv, c->stream))
     return fail(c, "pv0", cudaGetLastError());
+  if (c->prof) cudaEventRecord(c->ev[15], c->stream);
   // dpv: G_d dpv = H_d pv per domain (solve_dpv_bv)
   for (int d = 0; d <= c->MN; ++d) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
@@ -422,8 +438,43 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
     if (lu_solve(c, c->W, Nd, 3, c->B3, "dpv solve")) return -1;
     if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
   }
+  if (c->prof) cudaEventRecord(c->ev[16], c->stream);
   return 0;
 }
+
+extern "C" int bemgpu_set_profiling(bemgpu_ctx *c, int on) {
+  c->prof = on != 0;
+  return 0;
+}
+
+// phases: domain 0 classify, regular, near, self, diag; domain 1 the same;
+// gather, global LU + solve, boundary values (P, dP, pv), dpv solves
+extern "C" int bemgpu_phase_times(bemgpu_ctx *c, double *ms, int max) {
+  if (!c->prof) return 0;
+  CK(cudaStreamSynchronize(c->stream), "phase times");
+  int k = 0;
+  for (int d = 0; d < 2 && d <= c->MN; ++d)
+    for (int i = 0; i < 5 && k < max; ++i) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, c->ev[6 * d + i], c->ev[6 * d + i + 1]) != cudaSuccess) t = -1.f;
+      ms[k++] = t;
+    }
+  for (int i = 12; i < 16 && k < max; ++i) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]) != cudaSuccess) t = -1.f;
+    ms[k++] = t;
+  }
+  return k;
+}
+
+extern "C" int bemgpu_work_counters(bemgpu_ctx *c, unsigned long long *out6, int reset) {
+  CK(cudaMemcpyAsync(out6, c->terms, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream), "counters");
+  if (reset) CK(cudaMemsetAsync(c->terms, 0, 6 * sizeof(unsigned long long), c->stream), "counters");
+  CK(cudaStreamSynchronize(c->stream), "counters");
+  return 0;
+}
+
+extern "C" void *bemgpu_stream(bemgpu_ctx *c) { return (void *)c->stream; }
 
 extern "C" int bemgpu_run(bemgpu_ctx *c) {
   int r = bemgpu_assemble(c);

@@ -21,6 +21,7 @@ struct bem_scratch {
   double *selfF;    // [N][3]
   uint8_t *flag;    // [N][ne] 0 regular, 1 near-singular, 2 self
   unsigned *status; // BEM_ST_* bits
+  unsigned long long *terms;  // [6] lattice terms of regular / near / self pairs, then point counts
 };
 
 extern "C" {
@@ -28,7 +29,7 @@ int bem_set_constants(const double *xl, const double *wl, const double *xh, cons
 int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
 int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,
-                        double *G, double *H, double *dG, double *dH, double *dF, cudaStream_t st);
+                        double *G, double *H, double *dG, double *dH, double *dF, cudaStream_t st, cudaEvent_t *ev);
 }
 
 // host-side copies of the table sizes

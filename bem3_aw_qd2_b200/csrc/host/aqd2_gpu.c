@@ -14,6 +14,9 @@
 static struct { AQD2 *qd; bemgpu_ctx *ctx; } g_tab[AQD2_MAXCTX];
 static int g_device = 0;
 static double g_timing[4];
+static int g_verbose = 1;
+
+void aqd2_set_verbose(int on) { g_verbose = on; }
 
 void aqd2_set_device(int device) { g_device = device; }
 void aqd2_last_timing(double *t4) { for (int i = 0; i < 4; i++) t4[i] = g_timing[i]; }
@@ -150,18 +153,22 @@ static void download_solution(AQD2 *qd, bemgpu_ctx *c)
 void solve_bieq_aqd2(AQD2 *qd)
 {
   bemgpu_ctx *c = ctx_for(qd, 1);
-  printf("\nsolve acoustic wave boundary value \n");
+  if (g_verbose) printf("\nsolve acoustic wave boundary value \n");
   double t0 = aqd2_now();
   load_problem(qd, c);
   double t1 = aqd2_now();
-  printf("  coefficient matrix          ");
-  fflush(stdout);
+  if (g_verbose) {
+    printf("  coefficient matrix          ");
+    fflush(stdout);
+  }
   gpu_check(c, bemgpu_assemble(c), "assembly");
   gpu_check(c, bemgpu_sync(c), "assembly");
   double t2 = aqd2_now();
-  printf("finished. Elapsed time : %5g (sec)\n", t2 - t1);
-  printf("  solve VP and PV boundary value ");
-  fflush(stdout);
+  if (g_verbose) {
+    printf("finished. Elapsed time : %5g (sec)\n", t2 - t1);
+    printf("  solve VP and PV boundary value ");
+    fflush(stdout);
+  }
   gpu_check(c, bemgpu_solve(c), "solve");
   gpu_check(c, bemgpu_sync(c), "solve");
   unsigned st = bemgpu_status(c);
@@ -170,11 +177,11 @@ void solve_bieq_aqd2(AQD2 *qd)
     exit(1);
   }
   double t3 = aqd2_now();
-  printf("finished. Elapsed time : %5g (sec)\n", t3 - t2);
+  if (g_verbose) printf("finished. Elapsed time : %5g (sec)\n", t3 - t2);
   download_solution(qd, c);
   double t4 = aqd2_now();
   g_timing[0] = t1 - t0; g_timing[1] = t2 - t1; g_timing[2] = t3 - t2; g_timing[3] = t4 - t3;
-  printf("Total elapsed time : %g (sec)\n", t4 - t0);
+  if (g_verbose) printf("Total elapsed time : %g (sec)\n", t4 - t0);
 }
 
 /* Upload the boundary values held in the AQD2 (for example after dat_read_aqd2)

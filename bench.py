@@ -1,0 +1,309 @@
+"""Benchmark of the boundary-value solve (assembly + LU + boundary values +
+radiation force) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sphere216]
+
+A step is one complete solve of the workload: both domains' coefficient
+matrices, the global LU solve, P/dP, pv, the dpv solves and the type-0
+radiation force.  Rank 0 prints one JSON line.
+
+  value  solves/s with the problem resident on the device (bemgpu_run +
+         bemgpu_force), CUDA events on the library's stream, L2 flushed
+         (256 MB write) between steps, max over ranks
+  e2e    the same solves through the drop-in C API with host buffers
+         (solve_bieq_aqd2 uploads the element tables, solves, downloads P, dP,
+         pv, dpv; force_FN_aqd2 returns F, N)
+  roofline  the dominant kernel (periodic regular-pair assembly), FP64 work
+         = lattice terms x a fixed FP64 operation count per term
+  cpu_baseline  the reference's own assembly loop (oracle/_ref) timed on a
+         bounded sample of collocation elements on the host cores,
+         extrapolated linearly in elements, plus the dense solves
+
+--impl reference runs only the CPU arm (rank 0; other ranks exit).  N > 1
+runs independent replicas (the solve of one system does not shard without a
+distributed LU; requests are independent), scaling "weak".
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# FP64 operations per lattice term of the Green's-function sums (real-space or
+# spectral term with its Faddeeva / erfc evaluation, per-point set-up
+# amortised): counted once with ncu's FP64 instruction counters on the first
+# implementation of the periodic regular-pair kernel on the 216-quad sphere
+# (1.88e12 flop / 6.727e9 terms); frozen, never re-tuned.
+C_TERM_FLOPS = 280.0
+# nominal FP64 peak of B200 (148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz): no
+# measured FP64 peak is available on this pool
+FP64_PEAK_TFLOPS = 37.2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sphere216")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 7:
+                for n, v in zip(names, r[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(files, budget_s, threads=None):
+    """The reference's own assembly (oracle/_ref) on a sample of collocation
+    elements, extrapolated to the full assembly, plus the dense solves."""
+    from oracle import refwrap
+    if not refwrap.available():
+        return None
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    case = refwrap.RefCase(*files)
+    ne0, ne1 = case.dom_ne[0], case.dom_ne[1]
+    # one collocation element per thread of each domain (the reference's
+    # OpenMP loop runs over collocation elements, dynamic schedule)
+    m0 = min(ne0, threads)
+    t0 = time.perf_counter(); case.assemble_rows(0, 1, 1 + m0); s0 = time.perf_counter() - t0
+    m1 = min(ne1, threads)
+    t0 = time.perf_counter(); case.assemble_rows(1, 1, 1 + m1); s1 = time.perf_counter() - t0
+    t_asm = s0 * ne0 / m0 + s1 * ne1 / m1
+    # dense solves with the same OpenBLAS the reference build links (n = 2 NN; dpv: NN with 3 rhs per domain)
+    n = 8 * ne0
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal(n) + 0j
+    t0 = time.perf_counter(); np.linalg.solve(A, b); ts = time.perf_counter() - t0
+    A2 = A[: n // 2, : n // 2].copy()
+    B2 = rng.standard_normal((n // 2, 3)) + 0j
+    t0 = time.perf_counter(); np.linalg.solve(A2, B2); np.linalg.solve(A2, B2); td = time.perf_counter() - t0
+    total = t_asm + ts + td
+    return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "reference",
+            "sample": "reference create_cmatrix_domain loop on %d of %d collocation elements (domain 0) and %d of %d "
+                      "(domain 1), %d OpenMP threads, extrapolated linearly (%.1f s measured); dense solves timed "
+                      "at n=%d (OpenBLAS zgesv, as linked by the reference build)" % (m0, ne0, m1, ne1, threads,
+                                                                                        s0 + s1, n),
+            "seconds_per_solve": total, "assembly_seconds_extrapolated": t_asm}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from bem3_aw_qd2_b200 import meshgen
+    d = tempfile.mkdtemp(prefix="bench_ref_")
+    files = meshgen.write_inputs(d, **meshgen.CONFIGS[args.workload])
+    from oracle import refwrap
+    if not refwrap.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference build) is missing"}))
+        return
+    warm = refwrap.RefCase(*files)
+    for _ in range(args.warmup):  # warm-up: one interior collocation element (pages in code and data)
+        warm.assemble_rows(1, 1, 2)
+    vals = []
+    for _ in range(args.steps):
+        cb = cpu_baseline(files, args.cpu_seconds)
+        vals.append(cb["value"])
+    v = statistics.mean(vals)
+    cb["value"] = v
+    print(json.dumps({"impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": args.workload, **workload_desc(args.workload)},
+                      "cpu_baseline": cb, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                                  "d2h_bytes_per_step": 0}}))
+
+
+def workload_desc(name):
+    from bem3_aw_qd2_b200 import meshgen
+    c = meshgen.CONFIGS[name]
+    n = c["n"]
+    return {"quads": 6 * n * n, "unknowns": 2 * 4 * 6 * n * n, "semi_axes": list(c["semi_axes"]),
+            "lattice": [list(v) for v in c["lattice"]], "theta_deg": c["theta_deg"], "phi_deg": c["phi_deg"],
+            "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
+            "l2": "256 MB flush between timed steps"}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from bem3_aw_qd2_b200 import api, meshgen
+    h, g = api.libs()
+    h.aqd2_set_device(local)
+    h.aqd2_set_verbose(0)
+    d = tempfile.mkdtemp(prefix="bench_")
+    files = meshgen.write_inputs(d, **meshgen.CONFIGS[args.workload])
+    case = api.Case.from_files(*files)
+    case.solve()  # creates the device context, uploads, first solve
+    ctx = case.ctx
+    stream = torch.cuda.ExternalStream(int(g.bemgpu_stream(ctx)))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    g.bemgpu_set_profiling(ctx, 1)
+    rc = np.zeros(3)
+    F = np.zeros(3)
+    N = np.zeros(3)
+    _d = api._d
+
+    def device_step():
+        if g.bemgpu_run(ctx) != 0:
+            raise RuntimeError(g.bemgpu_error(ctx).decode())
+        if g.bemgpu_force(ctx, 0, api._p(rc), api._p(F), api._p(N)) != 0:
+            raise RuntimeError(g.bemgpu_error(ctx).decode())
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        device_step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    times, phases = [], []
+    g.bemgpu_work_counters(ctx, (api.ctypes.c_ulonglong * 6)(), 1)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        device_step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        ph = (api.ctypes.c_double * 16)()
+        n = g.bemgpu_phase_times(ctx, ph, 16)
+        phases.append([ph[i] for i in range(n)])
+    torch.cuda.synchronize()
+    cnt = (api.ctypes.c_ulonglong * 6)()
+    g.bemgpu_work_counters(ctx, cnt, 1)
+    total_ms = sum(times)
+    # e2e: the public drop-in API with host buffers
+    e2e_times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        case.solve()
+        Fh, Nh = case.force(0)
+        e2e_times.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms, sum(e2e_times)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+    else:
+        e2e_total = sum(e2e_times)
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1000.0)
+    e2e_value = world * args.steps / e2e_total
+    ph = np.array(phases).mean(axis=0)
+    names = ["d0_classify", "d0_regular", "d0_near", "d0_self", "d0_diag", "d1_classify", "d1_regular", "d1_near",
+             "d1_self", "d1_diag", "gather", "lu_solve", "boundary_values", "dpv_solves"]
+    phase_ms = {names[i]: float(ph[i]) for i in range(min(len(names), len(ph)))}
+    terms_reg = cnt[0] / args.steps
+    t_reg = phase_ms.get("d0_regular", float("nan")) / 1000.0
+    achieved = terms_reg * C_TERM_FLOPS / t_reg / 1e12 if t_reg > 0 else None
+    nq = meshgen.CONFIGS[args.workload]["n"]
+    ne = 6 * nq * nq
+    h2d = ne * (12 + 9 + 12 + 12 + 8 + 8 + 8 + 24 + 2) * 8 + ne * (1 + 4 + 1 + 2 + 8) * 4 + ne
+    d2h = 2 * (4 * ne) * (2 + 2 + 6 + 6) * 8 + 48 + 4
+    lat = sorted(times)
+    out = {
+        "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "precision": "plain FP64 (assembly and LU)", **workload_desc(args.workload)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "solve_bieq_aqd2 + force_FN_aqd2 (C ABI, host buffers)"},
+        "phase_ms": phase_ms,
+        "roofline": {"bound": "fp64", "kernel": "k_q0_regular", "achieved": achieved, "peak": FP64_PEAK_TFLOPS,
+                     "unit": "TFLOP/s", "frac": (achieved / FP64_PEAK_TFLOPS) if achieved else None, "traffic": None,
+                     "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+                     "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
+                     "mean_terms_per_point": cnt[0] / max(cnt[3], 1)},
+        "clocks": clk,
+        "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out))
+    case.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -140,6 +140,8 @@ void calc_apw_dpdn(double complex *p, double complex *dpdn, double *r, double *n
 /* -- additions of this library (no counterpart in the reference) */
 /* GPU device used by solve_bieq_aqd2 / force_FN_aqd2 (default 0). */
 void aqd2_set_device(int device);
+/* 0: solve_bieq_aqd2 prints nothing (default 1: the reference's progress lines). */
+void aqd2_set_verbose(int on);
 /* Last wall time of the solve phases in seconds: [0] upload, [1] assembly,
  * [2] solve, [3] download. */
 void aqd2_last_timing(double *t4);

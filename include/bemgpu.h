@@ -95,6 +95,21 @@ int bemgpu_force(bemgpu_ctx *ctx, int type, const double *rc, double *F, double 
 /* Wait for all queued work of the context. */
 int bemgpu_sync(bemgpu_ctx *ctx);
 
+/* The CUDA stream (cudaStream_t) all work of the context is queued on. */
+void *bemgpu_stream(bemgpu_ctx *ctx);
+
+/* Per-phase device timing (CUDA events on the context's stream). With
+ * profiling on, bemgpu_phase_times fills up to max entries (ms) and returns
+ * their number: domain 0 classify, regular, near-singular, self, diagonal;
+ * domain 1 the same; gather, global LU + solve, boundary values, dpv solves. */
+int bemgpu_set_profiling(bemgpu_ctx *ctx, int on);
+int bemgpu_phase_times(bemgpu_ctx *ctx, double *ms, int max);
+
+/* Work done by the periodic-domain kernels since load (or the last reset):
+ * out6 = lattice terms of regular, near-singular and self pairs, then the
+ * number of Green's-function points of each class. */
+int bemgpu_work_counters(bemgpu_ctx *ctx, unsigned long long *out6, int reset);
+
 /* Faddeeva w(z) at n points (host arrays of (re, im) pairs), relative error
  * 1e-15 (Faddeeva_w, qgf2_src/Faddeeva.cc:679, called with MEPS). */
 int bemgpu_faddeeva_w(const double *z, int n, double *w);
