@@ -1,0 +1,162 @@
+// bemgpu_assemble_domain_static: the coefficient matrices of one domain with
+// no device allocation at all.
+//
+// Some callers cannot call cudaMalloc: a host application whose device memory
+// belongs to another allocator (a framework's fixed-size memory pool that must
+// not be bypassed), a plugin loaded into such a process, or a caller through a
+// foreign-function interface that can hand over device buffers but has no way
+// to manage CUDA allocations itself.  They pass their own inputs and outputs;
+// the assembly's scratch (near-singular tables, pair flags, per-row sums,
+// status word) lives in the file-scope device array below, sized for at most
+// BEMGPU_STATIC_MAX_NE elements per domain.
+//
+// The array belongs to the process for its whole life on every GPU that loads
+// the library (about 21 MB).  Each call reuses it: calls that overlap on the
+// GPU (different streams or host threads at the same time) race on it and must
+// be serialised by the caller.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <mutex>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include "../../include/bemgpu.h"
+#include "bem_kernels.h"
+
+#define SMAX_N (4 * BEMGPU_STATIC_MAX_NE)
+#define ALIGN256(x) (((x) + 255) & ~(size_t)255)
+
+// scratch carve-up for N = 4 ne <= SMAX_N rows
+#define OFF_ROWF 0
+#define OFF_NEARS ALIGN256(OFF_ROWF + sizeof(double) * 3 * (size_t)SMAX_N)
+#define OFF_NEARN ALIGN256(OFF_NEARS + sizeof(int) * (size_t)SMAX_N * BEM_MAXNEAR_H)
+#define OFF_NEARF ALIGN256(OFF_NEARN + sizeof(int) * (size_t)SMAX_N)
+#define OFF_SELFF ALIGN256(OFF_NEARF + sizeof(double) * 3 * (size_t)SMAX_N * BEM_MAXNEAR_H)
+#define OFF_FLAG ALIGN256(OFF_SELFF + sizeof(double) * 3 * (size_t)SMAX_N)
+#define OFF_STATUS ALIGN256(OFF_FLAG + (size_t)SMAX_N * BEMGPU_STATIC_MAX_NE)
+#define OFF_TERMS ALIGN256(OFF_STATUS + sizeof(unsigned))
+#define SCRATCH_BYTES ALIGN256(OFF_TERMS + 6 * sizeof(unsigned long long))
+
+static __device__ __align__(256) unsigned char g_static_scratch[SCRATCH_BYTES];
+
+#define MAXDEV 64
+static std::mutex g_mu;
+static unsigned char *g_addr[MAXDEV];  // device address of g_static_scratch, per device
+
+// 12- and 64-point Gauss-Legendre rules (Newton on the Legendre recurrence)
+static void gl_nodes(int n, double *x, double *w) {
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p2 = p1;
+        p1 = p0;
+        p0 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p2) / j;
+      }
+      dp = n * (z * p0 - p1) / (z * z - 1.0);
+      const double dz = p0 / dp;
+      z -= dz;
+      if (fabs(dz) <= 3e-16) break;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+  if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+// Lattice quantities of the quasi-periodic Green's function for qp = {k, kx,
+// ky, kz, d1x, d1y, d2x, d2y} (the reference derives them inside every call,
+// qgf2_src/d3_qpgf_d2.c:126-156, 1679-1681, 1850-1856).
+static void lattice(const double *p, bem_qp *q) {
+  memset(q, 0, sizeof(*q));
+  q->k = p[0]; q->kx = p[1]; q->ky = p[2];
+  q->d1x = p[4]; q->d1y = p[5]; q->d2x = p[6]; q->d2y = p[7];
+  q->det = q->d1x * q->d2y - q->d2x * q->d1y;
+  q->idet = 1.0 / q->det;
+  q->aidet = fabs(q->idet);
+  const double cpd = 2.0 * M_PI * q->idet;
+  q->g1x = cpd * q->d2y; q->g1y = -cpd * q->d2x;
+  q->g2x = -cpd * q->d1y; q->g2y = cpd * q->d1x;
+  q->d2sq = q->d2x * q->d2x + q->d2y * q->d2y;
+  q->g2sq = q->g2x * q->g2x + q->g2y * q->g2y;
+  q->g1g2 = q->g1x * q->g2x + q->g1y * q->g2y;
+  const double adp = sqrt(pow(q->d1x + q->d2x, 2) + pow(q->d1y + q->d2y, 2));
+  const double adm = sqrt(pow(q->d1x - q->d2x, 2) + pow(q->d1y - q->d2y, 2));
+  q->eta0 = sqrt(fabs(q->det) / (4.0 * M_PI) * adp / adm);
+  q->nc1 = (int)round((q->kx * q->d1x + q->ky * q->d1y) / (2.0 * M_PI));
+  const double k2 = q->k * q->k;
+  const int n1 = q->nc1, n2 = (int)round((q->kx * q->d2x + q->ky * q->d2y) / (2.0 * M_PI));
+  const double ad12 = q->d1x * q->d1x + q->d1y * q->d1y, ad22 = q->d2sq;
+  const double aNx = -q->kx + n1 * cpd * q->d2y - n2 * cpd * q->d1y;
+  const double aNy = -q->ky - n1 * cpd * q->d2x + n2 * cpd * q->d1x;
+  const double bN = sqrt(k2 - aNx * aNx - aNy * aNy);
+  const int a1 = ad22 < ad12 ? 15 : 0, a2 = ad22 < ad12 ? 0 : 15;
+  const double aNpx = -q->kx + (n1 + a1) * cpd * q->d2y - (n2 + a2) * cpd * q->d1y;
+  const double aNpy = -q->ky - (n1 + a1) * cpd * q->d2x + (n2 + a2) * cpd * q->d1x;
+  const double aNmx = -q->kx + (n1 - a1) * cpd * q->d2y - (n2 - a2) * cpd * q->d1y;
+  const double aNmy = -q->ky - (n1 - a1) * cpd * q->d2x + (n2 - a2) * cpd * q->d1x;
+  const double bNp = k2 - aNpx * aNpx - aNpy * aNpy, bNm = k2 - aNmx * aNmx - aNmy * aNmy;
+  if (bNp > 0.0 || bNm > 0.0) {
+    q->ewald_only = 1;
+  } else {
+    q->sel_bp = sqrt(-bNp);
+    q->sel_bm = sqrt(-bNm);
+    q->sel_cp = bN / q->sel_bp;
+    q->sel_cm = bN / q->sel_bm;
+  }
+}
+
+// Once per device, with that device current: the device address of the
+// scratch array and the quadrature / Faddeeva constant tables.
+static unsigned char *device_setup(int dev) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_addr[dev]) return g_addr[dev];
+  unsigned char *p = nullptr;
+  if (cudaGetSymbolAddress((void **)&p, g_static_scratch) != cudaSuccess || p == nullptr) return nullptr;
+  double xl[BEM_GLN_H], wl[BEM_GLN_H], xh[BEM_GHN_H], wh[BEM_GHN_H];
+  gl_nodes(BEM_GLN_H, xl, wl);
+  gl_nodes(BEM_GHN_H, xh, wh);
+  if (bem_set_constants(xl, wl, xh, wh) != 0) return nullptr;
+  g_addr[dev] = p;
+  return p;
+}
+
+extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw, const double *ren,
+                                             const unsigned char *plane, const int *sid, int ne, const double *qp,
+                                             int periodic, double k, double *G, double *H, double *dG, double *dH,
+                                             double *dF, void *stream) {
+  if (ne <= 0 || ne > BEMGPU_STATIC_MAX_NE) {
+    fprintf(stderr, "bemgpu_assemble_domain_static: %d elements; this entry point handles 1..%d elements per domain\n",
+            ne, BEMGPU_STATIC_MAX_NE);
+    return -2;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return -3;
+  unsigned char *base = device_setup(dev);
+  if (!base) return -3;
+  cudaStream_t st = (cudaStream_t)stream;
+  bem_scratch S;
+  S.rowF = (double *)(base + OFF_ROWF);
+  S.near_s = (int *)(base + OFF_NEARS);
+  S.near_n = (int *)(base + OFF_NEARN);
+  S.nearF = (double *)(base + OFF_NEARF);
+  S.selfF = (double *)(base + OFF_SELFF);
+  S.flag = (uint8_t *)(base + OFF_FLAG);
+  S.status = (unsigned *)(base + OFF_STATUS);
+  S.terms = (unsigned long long *)(base + OFF_TERMS);
+  // the previous call's contents stay in the array: the status word and the
+  // work counters must start at zero; every other table is fully rewritten
+  if (cudaMemsetAsync(base + OFF_STATUS, 0, OFF_TERMS + 6 * sizeof(unsigned long long) - OFF_STATUS, st) != cudaSuccess)
+    return -4;
+  bem_dom_dev D;
+  D.ne = ne; D.sid = sid; D.cr = cr; D.cw = cw; D.ren = ren; D.plane = plane;
+  bem_qp q;
+  lattice(qp, &q);
+  if (bem_launch_assemble(&D, &q, periodic != 0, periodic != 0, k, &S, G, H, dG, dH, dF, st, nullptr) != 0) return -4;
+  unsigned status = 0;
+  if (cudaMemcpyAsync(&status, S.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -4;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return -4;
+  return status ? -5 : 0;
+}

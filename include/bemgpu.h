@@ -110,6 +110,40 @@ int bemgpu_phase_times(bemgpu_ctx *ctx, double *ms, int max);
  * number of Green's-function points of each class. */
 int bemgpu_work_counters(bemgpu_ctx *ctx, unsigned long long *out6, int reset);
 
+/* Coefficient matrices of one domain without any device allocation.
+ *
+ * No counterpart in the reference (the reference has no GPU code).  This is
+ * for callers that cannot allocate device memory, neither themselves nor
+ * through this library: a process whose device memory belongs to another
+ * allocator's fixed pool that must not be bypassed, or a caller through a
+ * foreign-function interface that can hand over device buffers but has no
+ * way to manage CUDA allocations.
+ *
+ * The caller passes device pointers for every input and output: the element
+ * tables cr, cw, ren and plane (laid out as in bemgpu_problem), the domain's
+ * signed element ids sid[ne], and the outputs G, H [4 ne][4 ne] complex,
+ * dF [4 ne][3], and for an interior domain dG, dH [8 ne][4 ne] complex (may
+ * be NULL when periodic = 1).  qp is a host array as bemgpu_problem.qp.
+ * periodic = 1: the host domain 0 with the quasi-periodic Green's function
+ * (H gets 1 + F on its diagonal); 0: an interior domain in free space with
+ * wave number k (H gets F).  The layouts are those of bemgpu_get_matrix.
+ *
+ * The scratch the assembly needs lives in one fixed array inside the library
+ * (about 21 MB on every GPU that loads it, kept until the process exits), so
+ * a domain may have at most BEMGPU_STATIC_MAX_NE elements; more is rejected
+ * with -2 and a message on stderr.  The first call on each device sets the
+ * array up (finds its device address, uploads the quadrature tables); make
+ * that first call before any stream capture.  Every call reuses the array and
+ * finds the previous call's contents in it (the status word is cleared at
+ * the start of each call); calls that overlap on the GPU race on it, so the
+ * caller must not run two at once.  The call returns after its work on
+ * stream has finished.  Returns 0; -2 size out of range; -3 device set-up
+ * failed; -4 launch or copy failed; -5 a BEMGPU_ST_* status bit was set. */
+#define BEMGPU_STATIC_MAX_NE 1536
+int bemgpu_assemble_domain_static(const double *cr, const double *cw, const double *ren, const unsigned char *plane,
+                                  const int *sid, int ne, const double *qp, int periodic, double k, double *G,
+                                  double *H, double *dG, double *dH, double *dF, void *stream);
+
 /* Faddeeva w(z) at n points (host arrays of (re, im) pairs), relative error
  * 1e-15 (Faddeeva_w, qgf2_src/Faddeeva.cc:679, called with MEPS). */
 int bemgpu_faddeeva_w(const double *z, int n, double *w);
