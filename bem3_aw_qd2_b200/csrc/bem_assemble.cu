@@ -164,7 +164,10 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restr
 // (q0_bil_dcoef_v2_cc_GL, q0_bil_dcoef_v2_cc.c:129-204, evaluated once per
 // point and shared by the four interpolation functions).
 #define RP_THREADS 288
-__global__ void __launch_bounds__(RP_THREADS) k_q0_regular(bem_dom_dev D, bem_qp q, const uint8_t *__restrict__ flag,
+#ifndef RP_MINB
+#define RP_MINB 2  // two blocks (18 warps) per SM: caps registers at 113
+#endif
+__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, bem_qp q, const uint8_t *__restrict__ flag,
                                                            double *__restrict__ G, double *__restrict__ H,
                                                            unsigned *status, unsigned long long *terms, long long pair0,
                                                            long long npairs) {
@@ -861,7 +864,35 @@ __global__ void __launch_bounds__(128) k_qpgf_points(bem_qp q, const double *__r
   dG[6 * i + 4] = v.gz.re; dG[6 * i + 5] = v.gz.im;
 }
 
+// ------------------------------------------------------------------ w(x + i y) table
+// One block per interval j of width BEM_WT_H: w at the BEM_WT_DEG Chebyshev
+// nodes of the interval, then the Chebyshev coefficients (discrete cosine sums).
+__global__ void k_wtab_build(double x, double *__restrict__ out) {
+  __shared__ double fr[BEM_WT_DEG], fi[BEM_WT_DEG];
+  const int j = blockIdx.x, m = threadIdx.x;
+  const double n = BEM_WT_DEG;
+  const double tm = cos(CUDART_PI * (m + 0.5) / n);
+  const cplx w = bem_faddeeva(x, (j + 0.5 * (1.0 + tm)) * BEM_WT_H);
+  fr[m] = w.re;
+  fi[m] = w.im;
+  __syncthreads();
+  double sr = 0.0, si = 0.0;
+  for (int mm = 0; mm < BEM_WT_DEG; ++mm) {
+    const double c = cos(CUDART_PI * m * (mm + 0.5) / n);
+    sr += fr[mm] * c;
+    si += fi[mm] * c;
+  }
+  const double f = (m == 0 ? 1.0 : 2.0) / n;
+  out[2 * ((size_t)j * BEM_WT_DEG + m)] = sr * f;
+  out[2 * ((size_t)j * BEM_WT_DEG + m) + 1] = si * f;
+}
+
 // ------------------------------------------------------------------ host launchers
+extern "C" int bem_launch_wtab(double x, double *out, cudaStream_t st) {
+  k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(x, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh) {
   bem_quad qq;
   for (int i = 0; i < BEM_GLN; ++i) { qq.xl[i] = xl[i]; qq.wl[i] = wl[i]; }

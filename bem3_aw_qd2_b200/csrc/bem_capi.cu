@@ -43,6 +43,7 @@ struct bemgpu_ctx {
   size_t dwork_sz = 0;
   std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
+  double *wtab = nullptr;  // w(k eta0 + i y) table of the Ewald real-space sums
   unsigned *status = nullptr;
   unsigned long long *terms = nullptr;
   bem_sys_dev sys;
@@ -93,7 +94,7 @@ static void free_problem(bemgpu_ctx *c) {
     dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
-  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv);
+  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab);
   if (c->dwork) cudaFree(c->dwork);
   c->dwork = nullptr;
   c->dwork_sz = 0;
@@ -264,6 +265,11 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   qp_prepare(pr->qp, &c->qp);
+  CK(dalloc(&c->wtab, BEM_WT_SIZE), "w table");
+  if (bem_launch_wtab(c->qp.k * c->qp.eta0, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
+  c->qp.wt = c->wtab;
+  c->qp.wt_h = 0.125;
+  c->qp.wt_n = 64;
   const int nd = pr->MN + 1;
   c->dom_ne.assign(pr->dom_ne, pr->dom_ne + nd);
   c->dom_off.assign(nd, 0);
@@ -545,6 +551,12 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   if (ensure_constants(nullptr, nullptr, nullptr, nullptr, nullptr) != 0) return -1;
   bem_qp q;
   qp_prepare(qpar, &q);
+  double *wt = nullptr;
+  if (cudaMalloc(&wt, BEM_WT_SIZE * sizeof(double)) != cudaSuccess) return -1;
+  if (bem_launch_wtab(q.k * q.eta0, wt, 0) != 0) { cudaFree(wt); return -1; }
+  q.wt = wt;
+  q.wt_h = 0.125;
+  q.wt_n = 64;
   double *dr = nullptr, *dg = nullptr, *ddg = nullptr;
   int *dret = nullptr;
   int rc = -1;
@@ -559,6 +571,6 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
         rc = -1;
     }
   }
-  cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret);
+  cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret); cudaFree(wt);
   return rc;
 }

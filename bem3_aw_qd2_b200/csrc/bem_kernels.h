@@ -27,6 +27,8 @@ struct bem_scratch {
 extern "C" {
 int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh);
 int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
+// table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)
+int bem_launch_wtab(double x, double *out, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
 int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,
                         double *G, double *H, double *dG, double *dH, double *dF, cudaStream_t st, cudaEvent_t *ev);
@@ -36,3 +38,4 @@ int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int
 #define BEM_GLN_H 12
 #define BEM_GHN_H 64
 #define BEM_MAXNEAR_H 64
+#define BEM_WT_SIZE (2 * 14 * 64)  // doubles in the w table (BEM_WT_DEG x BEM_WT_N complex)

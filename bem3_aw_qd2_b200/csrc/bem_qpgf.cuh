@@ -33,6 +33,10 @@
 #define BEM_EW_EXPM 3.0        // d3_qpgf_d2.h:26
 #define BEM_S_LIMIT 15         // d3_qpgf_d2.h:19
 #define BEM_W_TAB 48           // exp(-a^2 n^2) table length
+#define BEM_FD_MAX_TERMS 250.0 // spectral-only sum used when it needs fewer terms than this
+#define BEM_WT_DEG 14          // Chebyshev terms per interval of the w(x + i y) table
+#define BEM_WT_H 0.125         // interval width in y
+#define BEM_WT_N 64            // intervals: y in [0, 8)
 
 // Algorithm 916 constants for relerr = 1e-15: a = pi / sqrt(-ln(relerr/2)),
 // c = 2a/pi, tab[n-1] = exp(-a^2 n^2).  Filled once by bem_device_init().
@@ -148,29 +152,48 @@ __device__ __forceinline__ bool bem_small(cplx t, cplx s, double eps) {
 
 struct bem_gval { cplx g, gx, gy, gz; };
 
-// Ewald real-space term for lattice point (l1,l2)  (ew_qG1_v1_cFl, d3_qpgf_d2.c:1814)
-__device__ __forceinline__ void ew_real_term(const bem_qp &q, double rx, double ry, double rz, int l1, int l2,
-                                             double ke, double ke2, double ive, cplx &F, cplx &cf) {
-  const double Rx = l1 * q.d1x + l2 * q.d2x, Ry = l1 * q.d1y + l2 * q.d2y;
-  const double px = rx + Rx, py = ry + Ry;
+// w(x + i y) from the per-problem table (x = k eta0, 0 <= y < 8): Clenshaw
+// recurrence on the interval's Chebyshev series.  Terms with y >= 8 are below
+// 1e-27 of the leading one and never reached by the stopping rule; they fall
+// back to the direct evaluation.
+__device__ __forceinline__ cplx bem_wtab(const bem_qp &q, double x, double y) {
+  const double u = y * (1.0 / BEM_WT_H);
+  const int j = (int)u;
+  if (j >= q.wt_n) return bem_faddeeva(x, y);
+  const double t = 2.0 * (u - j) - 1.0, t2 = 2.0 * t;
+  const double2 *c = reinterpret_cast<const double2 *>(q.wt) + (size_t)j * BEM_WT_DEG;
+  double br = 0.0, bi = 0.0, b1r = 0.0, b1i = 0.0;
+#pragma unroll
+  for (int k = BEM_WT_DEG - 1; k >= 1; --k) {
+    const double2 ck = __ldg(c + k);
+    const double nr = ck.x + t2 * br - b1r, ni = ck.y + t2 * bi - b1i;
+    b1r = br; b1i = bi;
+    br = nr; bi = ni;
+  }
+  const double2 c0 = __ldg(c);
+  return cmk(c0.x + t * br - b1r, c0.y + t * bi - b1i);
+}
+
+// Ewald real-space term for lattice point (l1,l2)  (ew_qG1_v1_cFl, d3_qpgf_d2.c:1814).
+// ce = exp(i k_par . R_l) is supplied by the caller, which advances it along the
+// row by one complex multiplication per term instead of a sincos.
+__device__ __forceinline__ void ew_real_term(const bem_qp &q, double px, double py, double rz, cplx ce,
+                                             double ke, double ke2, double ive, bool tab, cplx &F, cplx &cf) {
   const double rl = sqrt(px * px + py * py + rz * rz);
   const double irl = 1.0 / rl;
   const double rl2e = rl * 0.5 * ive;
-  const cplx ce = cexpi(q.kx * Rx + q.ky * Ry);
   const double ef = exp(ke2 - rl2e * rl2e);
-  const cplx w = bem_faddeeva(ke, rl2e);
+  const cplx w = tab ? bem_wtab(q, ke, rl2e) : bem_faddeeva(ke, rl2e);
   F = cscale(ce, irl * ef * w.re);
   cf = cscale(ce, irl * irl * ef * (irl * w.re - q.k * w.im + ive * 0.56418958354775628695));
 }
 
-// Ewald spectral term for reciprocal point (n1,n2) (ew_qG2_v1_cFn, d3_qpgf_d2.c:1965).
+// Ewald spectral term for reciprocal point (n1,n2) (ew_qG2_v1_cFn, d3_qpgf_d2.c:1965);
+// ce = exp(i alpha_n . r) supplied by the caller (recurrence along n2).
 // returns 0 propagating, 1 evanescent, -3 beta_n == 0
-__device__ __forceinline__ int ew_spec_term(const bem_qp &q, double rx, double ry, double rz, int n1, int n2,
+__device__ __forceinline__ int ew_spec_term(const bem_qp &q, double anx, double any, double rz, cplx ce,
                                             double ve, cplx &Fn, cplx &dF0, cplx &dF1, cplx &dF2) {
-  const double anx = -q.kx + n1 * q.g1x + n2 * q.g2x;
-  const double any = -q.ky + n1 * q.g1y + n2 * q.g2y;
   const double bn2 = q.k * q.k - anx * anx - any * any;
-  const cplx ce = cexpi(anx * rx + any * ry);
   const double azve = rz / (2.0 * ve);
   if (bn2 > 0.0) {
     const double bn = sqrt(bn2);
@@ -198,16 +221,23 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, double rx, double r
   return -3;
 }
 
+__device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.re, -a.im); }
+
 // Ewald evaluation in the home cell (d3hm_qpgf_d2v1_ew_sd, d3_qpgf_d2.c:1671).
 // Returns the number of lattice terms, or a negative reference error code.
+// The lattice rows are walked exactly as in the reference (centre, then up,
+// then down, each stopped by the reference's tests); the Bloch phases along a
+// row are advanced by a unit complex factor, so a row costs one sincos.
 __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
   double ve = q.eta0;
   const double r2 = rx * rx + ry * ry + rz * rz;
   if (q.k * q.k * ve * ve - r2 / (4.0 * ve * ve) > BEM_EW_EXPM)
     ve = sqrt(BEM_EW_EXPM + sqrt(q.k * q.k * r2 + BEM_EW_EXPM * BEM_EW_EXPM)) / (1.4142135623730950488 * q.k);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
+  const bool tab = q.wt != nullptr && ve == q.eta0;  // table built for x = k eta0
   const double eps = BEM_MEPS;
   int cc = 0;
+  const cplx E2 = cexpi(q.kx * q.d2x + q.ky * q.d2y);  // exp(i k_par . d2)
 
   // ---- real-space sum (ew_qG1_v1, :1714-1812)
   cplx s = cmk(0, 0), sx = cmk(0, 0), sy = cmk(0, 0), sz = cmk(0, 0);
@@ -219,22 +249,26 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
     for (int it = 0; it < (dir == 0 ? 1 : BEM_EW_LIMIT - 1); ++it, l1 += step) {
       const cplx old = s;
       const int lc = -(int)round(((rx + l1 * q.d1x) * q.d2x + (ry + l1 * q.d1y) * q.d2y) / q.d2sq);
+      const cplx pc = cexpi(q.kx * (l1 * q.d1x + lc * q.d2x) + q.ky * (l1 * q.d1y + lc * q.d2y));
       // centre term, then l2 > lc, then l2 < lc
       for (int side = 0; side < 3; ++side) {
         int l2 = side == 0 ? lc : (side == 1 ? lc + 1 : lc - 1);
         const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(E2) : E2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
         const int nmax = side == 0 ? 1 : BEM_EW_LIMIT - 1;
         int k = 0;
         for (; k < nmax; ++k, l2 += st) {
+          const double px = rx + l1 * q.d1x + l2 * q.d2x, py = ry + l1 * q.d1y + l2 * q.d2y;
           cplx F, cf;
-          ew_real_term(q, rx, ry, rz, l1, l2, ke, ke2, ive, F, cf);
+          ew_real_term(q, px, py, rz, ce, ke, ke2, ive, tab, F, cf);
           ++cc;
           s = cadd(s, F);
-          const double px = rx + l1 * q.d1x + l2 * q.d2x, py = ry + l1 * q.d1y + l2 * q.d2y;
           sx = cadd(sx, cscale(cf, px));
           sy = cadd(sy, cscale(cf, py));
           sz = cadd(sz, cf);
           if (side != 0 && bem_small(F, s, eps)) break;
+          ce = cmul(ce, E);
         }
         if (side != 0 && k == nmax) return -21;
       }
@@ -249,6 +283,7 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
   out.gz = cscale(sz, -rz * i4p);
 
   // ---- spectral sum (ew_qG2_v1, :1840-1963)
+  const cplx G2 = cexpi(q.g2x * rx + q.g2y * ry);  // exp(i g2 . r)
   cplx t = cmk(0, 0), tx = cmk(0, 0), ty = cmk(0, 0), tz = cmk(0, 0);
   for (int dir = 0; dir < 3; ++dir) {
     int n1 = q.nc1 + (dir == 2 ? -1 : (dir == 1 ? 1 : 0));
@@ -257,15 +292,19 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
     for (int it = 0; it < (dir == 0 ? 1 : BEM_EW_LIMIT - 1); ++it, n1 += step) {
       const cplx old = tz;
       const int nc = (int)round(-((-q.kx + n1 * q.g1x) * q.g2x + (-q.ky + n1 * q.g1y) * q.g2y) / q.g2sq);
+      const double a0x = -q.kx + n1 * q.g1x, a0y = -q.ky + n1 * q.g1y;
+      const cplx pc = cexpi((a0x + nc * q.g2x) * rx + (a0y + nc * q.g2y) * ry);
       int flg = 0;
       for (int side = 0; side < 3; ++side) {
         int n2 = side == 0 ? nc : (side == 1 ? nc + 1 : nc - 1);
         const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(G2) : G2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
         const int nmax = side == 0 ? 1 : BEM_EW_LIMIT - 1;
         int k = 0;
         for (; k < nmax; ++k, n2 += st) {
           cplx Fn, d0, d1, d2;
-          const int e = ew_spec_term(q, rx, ry, rz, n1, n2, ve, Fn, d0, d1, d2);
+          const int e = ew_spec_term(q, a0x + n2 * q.g2x, a0y + n2 * q.g2y, rz, ce, ve, Fn, d0, d1, d2);
           if (e < 0) return -23;
           ++cc;
           t = cadd(t, Fn);
@@ -276,6 +315,7 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
             if (e > 0) { if (bem_small(d2, tz, eps)) break; }
             else ++flg;
           }
+          ce = cmul(ce, E);
         }
         if (side != 0 && k == nmax) return -22;
       }
@@ -296,6 +336,7 @@ __device__ int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double r
   if (rz == 0.0) return -14;
   const double eps = BEM_MEPS, az = fabs(rz);
   int cc = 0;
+  const cplx G2 = cexpi(q.g2x * rx + q.g2y * ry);  // exp(i g2 . r)
   cplx t = cmk(0, 0), tx = cmk(0, 0), ty = cmk(0, 0), tz = cmk(0, 0);
   for (int dir = 0; dir < 3; ++dir) {
     int n1 = q.nc1 + (dir == 2 ? -1 : (dir == 1 ? 1 : 0));
@@ -304,25 +345,29 @@ __device__ int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double r
     for (int it = 0; it < (dir == 0 ? 1 : BEM_FD_LIMIT - 1); ++it, n1 += step) {
       const cplx old = tz;
       const int nc = (int)round((q.kx * q.g2x + q.ky * q.g2y - n1 * q.g1g2) / q.g2sq);
+      const double a0x = -q.kx + n1 * q.g1x, a0y = -q.ky + n1 * q.g1y;
+      const cplx pc = cexpi((a0x + nc * q.g2x) * rx + (a0y + nc * q.g2y) * ry);
       for (int side = 0; side < 3; ++side) {
         int n2 = side == 0 ? nc : (side == 1 ? nc + 1 : nc - 1);
         const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(G2) : G2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
         const int nmax = side == 0 ? 1 : BEM_FD_LIMIT - 1;
         int k = 0;
         for (; k < nmax; ++k, n2 += st) {
-          const double anx = -q.kx + n1 * q.g1x + n2 * q.g2x;
-          const double any = -q.ky + n1 * q.g1y + n2 * q.g2y;
+          const double anx = a0x + n2 * q.g2x;
+          const double any = a0y + n2 * q.g2y;
           const double bn2 = q.k * q.k - anx * anx - any * any;
           cplx d2, Fn;
           int e;
           if (bn2 > 0.0) {
             const double bn = sqrt(bn2);
-            d2 = cexpi(anx * rx + any * ry + bn * az);
+            d2 = cmul(ce, cexpi(bn * az));
             Fn = cscale(d2, 1.0 / bn);
             e = 0;
           } else if (bn2 < 0.0) {
             const double bn = sqrt(-bn2);
-            d2 = cscale(cexpi(anx * rx + any * ry), exp(-bn * az));
+            d2 = cscale(ce, exp(-bn * az));
             Fn = cmk(d2.im / bn, -d2.re / bn);  // -i d2 / bn
             e = 1;
           } else {
@@ -334,6 +379,7 @@ __device__ int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double r
           ty = cadd(ty, cscale(Fn, any));
           tz = cadd(tz, d2);
           if (side != 0 && e > 0 && bem_small(d2, tz, eps)) break;
+          ce = cmul(ce, E);
         }
         if (side != 0 && k == nmax) return -11;
       }
@@ -356,6 +402,11 @@ __device__ int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gv
   if (!q.ewald_only) {
     const double az = fabs(rz);
     spectral = q.sel_cp * exp(-q.sel_bp * az) < BEM_MEPS && q.sel_cm * exp(-q.sel_bm * az) < BEM_MEPS;
+    // Where the reference allows the pure spectral sum, both sums converge to
+    // 1e-15 and agree to round-off; keep the spectral one only where it is the
+    // cheaper: it needs about (36/|z|)^2 |det| / 4 pi terms (|beta_n| |z| < 36)
+    // against ~110 costlier Ewald terms.
+    if (spectral && (36.0 / az) * (36.0 / az) * fabs(q.det) * 0.0795774715459476679 > BEM_FD_MAX_TERMS) spectral = false;
   }
   const int l1 = (int)floor((rx * q.d2y - ry * q.d2x) * q.idet + 0.5);
   const int l2 = (int)floor(-(rx * q.d1y - ry * q.d1x) * q.idet + 0.5);

@@ -30,6 +30,12 @@ typedef struct bem_qp {
   double sel_cm, sel_bm;        /*                     bN/bNm, bNm  */
   int nc1;                      /* round(k_par . d1 / 2 pi) */
   int ewald_only;               /* 1: always use the Ewald sum */
+  /* optional table of w(x + i y) for the Ewald real-space terms at
+     x = k eta0: piecewise Chebyshev, wt_n intervals of width wt_h on
+     y in [0, wt_n wt_h), BEM_WT_DEG (re, im) coefficients each; NULL: none */
+  const double *wt;
+  double wt_h;
+  int wt_n;
 } bem_qp;
 
 /* status word bits written by the kernels (never trapped on the device) */
