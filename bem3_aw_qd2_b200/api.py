@@ -122,6 +122,40 @@ class Case:
         libs()[0].force_FN_aqd2(_p(F), _p(N), _p(rc), type, self.qd)
         return F, N
 
+    def field(self, fn, rt, type=1):
+        """Field function fn of the reference API ("phi_s", "phi_t", "p_s", "p_t", "pv_s",
+        "pv_t", ...) at point rt.  Returns (domain id, phi or p, pv or None)."""
+        h = libs()[0]
+        rt = np.ascontiguousarray(rt, dtype=np.float64)
+        a = np.zeros(2)
+        v = np.zeros(6)
+        f = getattr(h, fn + "_aqd2")
+        f.restype = ctypes.c_int
+        if fn.startswith("pv"):
+            f.argtypes = [_d, _d, _d, ctypes.c_int, ctypes.c_void_p]
+            did = f(_p(a), _p(v), _p(rt), type, self.qd)
+            return did, complex(a[0], a[1]), v.view(np.complex128).copy()
+        f.argtypes = [_d, _d, ctypes.c_int, ctypes.c_void_p]
+        did = f(_p(a), _p(rt), type, self.qd)
+        return did, complex(a[0], a[1]), None
+
+    def boundary(self, fn, did, t, zeta, eta, type=1):
+        """Boundary function fn ("phi_s_bd", "pv_t_bd", ...) at (zeta, eta) of element t
+        (1-based) of domain did.  Returns (phi or p, pv or None)."""
+        h = libs()[0]
+        a = np.zeros(2)
+        v = np.zeros(6)
+        f = getattr(h, fn + "_aqd2")
+        f.restype = None
+        ints = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+        if fn.startswith("pv"):
+            f.argtypes = [_d, _d] + ints
+            f(_p(a), _p(v), did, t, zeta, eta, type, self.qd)
+            return complex(a[0], a[1]), v.view(np.complex128).copy()
+        f.argtypes = [_d] + ints
+        f(_p(a), did, t, zeta, eta, type, self.qd)
+        return complex(a[0], a[1]), None
+
     def dat_write(self, path):
         libs()[0].dat_write_aqd2(path.encode(), self.qd)
 
@@ -146,13 +180,6 @@ class Case:
 
     def status(self):
         return libs()[1].bemgpu_status(self.ctx)
-
-    def domain_sizes(self):
-        return [int(n) for n in self._dom_ne()]
-
-    def _dom_ne(self):
-        # read via the solution shape: ask the device for domain sizes through the matrices
-        raise NotImplementedError
 
     def matrix(self, d, which, N):
         """which: 'G', 'H', 'dG', 'dH', 'dF'; N = 4 * elements of domain d."""

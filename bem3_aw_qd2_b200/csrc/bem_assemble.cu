@@ -899,6 +899,12 @@ extern "C" int bem_set_constants(const double *xl, const double *wl, const doubl
   for (int i = 0; i < BEM_GHN; ++i) { qq.xh[i] = xh[i]; qq.wh[i] = wh[i]; }
   const double zt[4] = {-BEM_P44, BEM_P44, BEM_P44, -BEM_P44}, et[4] = {-BEM_P44, -BEM_P44, BEM_P44, BEM_P44};
   for (int i = 0; i < 4; ++i) { qq.zt[i] = zt[i]; qq.et[i] = et[i]; }
+  // 9-point product Gauss rule on [-1,1]^2 (nodes 0, +-sqrt(3/5); weights 25/81, 40/81, 64/81),
+  // ordered as the reference's zt_49/et_49 (bem3_aw_qd2.c:997-1008)
+  const double b = 0.7745966692414833770359, w0 = 25.0 / 81.0, w1 = 40.0 / 81.0, w2 = 64.0 / 81.0;
+  const double z9[9] = {-b, b, b, -b, 0.0, b, 0.0, -b, 0.0}, e9[9] = {-b, -b, b, b, -b, 0.0, b, 0.0, 0.0};
+  const double w9[9] = {w0, w0, w0, w0, w1, w1, w1, w1, w2};
+  for (int i = 0; i < 9; ++i) { qq.z9[i] = z9[i]; qq.e9[i] = e9[i]; qq.w9[i] = w9[i]; }
   bem_wconst wc;
   wc.relerr = BEM_MEPS;
   wc.a = CUDART_PI / sqrt(-log(wc.relerr * 0.5));
@@ -954,3 +960,5 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   if (ev) cudaEventRecord(ev[5], st);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
+
+#include "bem_post.cuh"

@@ -10,6 +10,7 @@
 #include "../../include/bemgpu.h"
 #include "bem_kernels.h"
 #include "bem_solve.h"
+#include "bem_lattice.h"
 
 #define BEMGPU_MAXDOM 8
 
@@ -44,6 +45,16 @@ struct bemgpu_ctx {
   std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
   double *wtab = nullptr;  // w(k eta0 + i y) table of the Ewald real-space sums
+  double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
+  double *pw_d = nullptr;
+  // 9-point targets on the domain-0 elements for the type-1 force
+  int ntgt = 0;
+  int *tgt_t = nullptr;
+  double *tgt_ze = nullptr, *tgt_w = nullptr, *bdv = nullptr;
+  // staging buffers of the point evaluators (grown on demand, kept until destroy)
+  size_t pt_cap = 0;
+  double *pt_in = nullptr, *pt_out = nullptr;
+  int *pt_t = nullptr;
   unsigned *status = nullptr;
   unsigned long long *terms = nullptr;
   bem_sys_dev sys;
@@ -95,6 +106,8 @@ static void free_problem(bemgpu_ctx *c) {
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
   dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab);
+  dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
+  c->ntgt = 0;
   if (c->dwork) cudaFree(c->dwork);
   c->dwork = nullptr;
   c->dwork_sz = 0;
@@ -137,6 +150,7 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_problem(c);
   dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
+  dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
   for (int i = 0; i < 17; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->params) cusolverDnDestroyParams(c->params);
@@ -159,57 +173,6 @@ extern "C" int bemgpu_sync(bemgpu_ctx *c) {
   return 0;
 }
 
-// Lattice quantities derived once per (k, k_par, lattice): the reference
-// recomputes them inside every Green's-function call (d3_qpgf_d2.c:126-156,
-// 1679-1681, 1850-1856).
-static void qp_prepare(const double *p, bem_qp *q) {
-  memset(q, 0, sizeof(*q));
-  q->k = p[0]; q->kx = p[1]; q->ky = p[2];
-  q->d1x = p[4]; q->d1y = p[5]; q->d2x = p[6]; q->d2y = p[7];
-  q->det = q->d1x * q->d2y - q->d2x * q->d1y;
-  q->idet = 1.0 / q->det;
-  q->aidet = fabs(q->idet);
-  const double cpd = 2.0 * M_PI * q->idet;
-  q->g1x = cpd * q->d2y; q->g1y = -cpd * q->d2x;
-  q->g2x = -cpd * q->d1y; q->g2y = cpd * q->d1x;
-  q->d2sq = q->d2x * q->d2x + q->d2y * q->d2y;
-  q->g2sq = q->g2x * q->g2x + q->g2y * q->g2y;
-  q->g1g2 = q->g1x * q->g2x + q->g1y * q->g2y;
-  const double adp = sqrt(pow(q->d1x + q->d2x, 2) + pow(q->d1y + q->d2y, 2));
-  const double adm = sqrt(pow(q->d1x - q->d2x, 2) + pow(q->d1y - q->d2y, 2));
-  q->eta0 = sqrt(fabs(q->det) / (4.0 * M_PI) * adp / adm);
-  q->nc1 = (int)round((q->kx * q->d1x + q->ky * q->d1y) / (2.0 * M_PI));
-  // choice between the Ewald and the pure spectral sum (d3hm_qpgf_d2_v1)
-  const double k2 = q->k * q->k;
-  const int n1 = q->nc1, n2 = (int)round((q->kx * q->d2x + q->ky * q->d2y) / (2.0 * M_PI));
-  const double ad12 = q->d1x * q->d1x + q->d1y * q->d1y, ad22 = q->d2sq;
-  const double aNx = -q->kx + n1 * cpd * q->d2y - n2 * cpd * q->d1y;
-  const double aNy = -q->ky - n1 * cpd * q->d2x + n2 * cpd * q->d1x;
-  const double bN = sqrt(k2 - aNx * aNx - aNy * aNy);
-  double aNpx, aNpy, aNmx, aNmy;
-  if (ad22 < ad12) {
-    aNpx = -q->kx + (n1 + 15) * cpd * q->d2y - n2 * cpd * q->d1y;
-    aNpy = -q->ky - (n1 + 15) * cpd * q->d2x + n2 * cpd * q->d1x;
-    aNmx = -q->kx + (n1 - 15) * cpd * q->d2y - n2 * cpd * q->d1y;
-    aNmy = -q->ky - (n1 - 15) * cpd * q->d2x + n2 * cpd * q->d1x;
-  } else {
-    aNpx = -q->kx + n1 * cpd * q->d2y - (n2 + 15) * cpd * q->d1y;
-    aNpy = -q->ky - n1 * cpd * q->d2x + (n2 + 15) * cpd * q->d1x;
-    aNmx = -q->kx + n1 * cpd * q->d2y - (n2 - 15) * cpd * q->d1y;
-    aNmy = -q->ky - n1 * cpd * q->d2x + (n2 - 15) * cpd * q->d1x;
-  }
-  const double bNp = k2 - aNpx * aNpx - aNpy * aNpy;
-  const double bNm = k2 - aNmx * aNmx - aNmy * aNmy;
-  if (bNp > 0.0 || bNm > 0.0) {
-    q->ewald_only = 1;
-  } else {
-    q->ewald_only = 0;
-    q->sel_bp = sqrt(-bNp);
-    q->sel_bm = sqrt(-bNm);
-    q->sel_cp = bN / q->sel_bp;
-    q->sel_cm = bN / q->sel_bm;
-  }
-}
 
 // Gauss-Legendre nodes and weights on [-1,1] by Newton iteration on the
 // three-term Legendre recurrence (the rule the reference tabulates with
@@ -264,12 +227,14 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     if (pr->npe[e] != 4) { snprintf(c->err, sizeof(c->err), "element %d: only bilinear (4-node) elements are implemented", e + 1); return -2; }
   if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
-  qp_prepare(pr->qp, &c->qp);
+  bem_qp_prepare(pr->qp, &c->qp);
   CK(dalloc(&c->wtab, BEM_WT_SIZE), "w table");
   if (bem_launch_wtab(c->qp.k * c->qp.eta0, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
   c->qp.wt_h = 0.125;
   c->qp.wt_n = 64;
+  memcpy(c->pw, pr->pw, sizeof(c->pw));
+  if (upload(c, &c->pw_d, c->pw, 16, "pw")) return -1;
   const int nd = pr->MN + 1;
   c->dom_ne.assign(pr->dom_ne, pr->dom_ne + nd);
   c->dom_off.assign(nd, 0);
@@ -518,16 +483,124 @@ extern "C" int bemgpu_get_matrix(bemgpu_ctx *c, int d, int which, double *dst) {
   return 0;
 }
 
+static int ensure_force_targets(bemgpu_ctx *c);
+static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
+
 extern "C" int bemgpu_force(bemgpu_ctx *c, int type, const double *rc, double *F, double *N) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
-  if (type != 0) { snprintf(c->err, sizeof(c->err), "force type %d not implemented on the device", type); return -2; }
   CK(cudaMemcpyAsync(c->rc_d, rc, 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "rc");
-  if (bem_launch_force0(&c->sys, c->P[0], c->pv[0], c->rc_d, c->c0[0], c->rho0[0], c->fout, c->stream))
-    return fail(c, "force", cudaGetLastError());
+  if (type == 0) {
+    if (bem_launch_force0(&c->sys, c->P[0], c->pv[0], c->rc_d, c->c0[0], c->rho0[0], c->fout, c->stream))
+      return fail(c, "force", cudaGetLastError());
+  } else {
+    // boundary values at the 9 rule points of every domain-0 element, then the stress integral
+    if (ensure_force_targets(c)) return -1;
+    bem_dom_dev D = dom_view(c, 0);
+    if (bem_launch_bdval(&D, &c->qp, 1, c->k0[0], 1, c->ntgt, c->tgt_t, c->tgt_ze, c->P[0], c->dP[0], c->pv[0], c->dpv[0], c->bdv,
+                         c->status, c->stream) ||
+        bem_launch_force_bd(&D, c->ntgt, c->tgt_t, c->tgt_ze, c->tgt_w, c->bdv, c->pw_d, c->k2[0], c->k2[1], c->rc_d,
+                            c->c0[0], c->rho0[0], c->fout, c->stream))
+      return fail(c, "force", cudaGetLastError());
+  }
   double out[6];
   CK(cudaMemcpyAsync(out, c->fout, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "force");
   CK(cudaStreamSynchronize(c->stream), "force");
   for (int i = 0; i < 3; ++i) { F[i] = out[i]; N[i] = out[3 + i]; }
+  return 0;
+}
+
+static bem_dom_dev dom_view(bemgpu_ctx *c, int d) {
+  bem_dom_dev D;
+  D.ne = c->dom_ne[d];
+  D.sid = c->sid + c->dom_off[d];
+  D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane; D.wen = c->wen;
+  return D;
+}
+
+extern "C" int bemgpu_set_solution(bemgpu_ctx *c, int d, const double *P, const double *dP, const double *pv,
+                                   const double *dpv) {
+  if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain"); return -2; }
+  const size_t N = 4 * (size_t)c->dom_ne[d];
+  CK(cudaMemcpyAsync(c->P[d], P, 2 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream), "P");
+  CK(cudaMemcpyAsync(c->dP[d], dP, 2 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream), "dP");
+  CK(cudaMemcpyAsync(c->pv[d], pv, 6 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream), "pv");
+  CK(cudaMemcpyAsync(c->dpv[d], dpv, 6 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream), "dpv");
+  CK(cudaStreamSynchronize(c->stream), "set solution");
+  return 0;
+}
+
+// room for n points of the point evaluators (inputs: 3 doubles + 1 int each, outputs: 18 doubles)
+static int ensure_points(bemgpu_ctx *c, int n) {
+  if ((size_t)n <= c->pt_cap) return 0;
+  dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
+  c->pt_cap = 0;
+  size_t cap = 256;
+  while (cap < (size_t)n) cap *= 2;
+  CK(dalloc(&c->pt_in, 3 * cap), "point buffers");
+  CK(dalloc(&c->pt_out, 18 * cap), "point buffers");
+  CK(dalloc(&c->pt_t, cap), "point buffers");
+  c->pt_cap = cap;
+  return 0;
+}
+
+extern "C" int bemgpu_field(bemgpu_ctx *c, int d, int type, int n, const double *r, double *out) {
+  if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain %d", d); return -2; }
+  if (type < 0 || type > 3) { snprintf(c->err, sizeof(c->err), "field rule type %d not available (0..3)", type); return -2; }
+  if (n <= 0) return 0;
+  if (ensure_points(c, n)) return -1;
+  bem_dom_dev D = dom_view(c, d);
+  CK(cudaMemcpyAsync(c->pt_in, r, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, c->stream), "field points");
+  if (bem_launch_field(&D, &c->qp, d == 0, c->k0[d], type, n, c->pt_in, c->P[d], c->dP[d], c->pv[d], c->dpv[d],
+                       c->pt_out, c->status, c->stream))
+    return fail(c, "field", cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->pt_out, 18 * sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream), "field");
+  CK(cudaStreamSynchronize(c->stream), "field");
+  return 0;
+}
+
+extern "C" int bemgpu_boundary_field(bemgpu_ctx *c, int d, int type, int n, const int *t, const double *ze,
+                                     double *out) {
+  if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain %d", d); return -2; }
+  if (type < 0 || type > 3) { snprintf(c->err, sizeof(c->err), "rule type %d not available (0..3)", type); return -2; }
+  if (n <= 0) return 0;
+  for (int i = 0; i < n; ++i)
+    if (t[i] < 0 || t[i] >= c->dom_ne[d]) {
+      snprintf(c->err, sizeof(c->err), "element %d is not in domain %d (0..%d)", t[i], d, c->dom_ne[d] - 1);
+      return -2;
+    }
+  if (ensure_points(c, n)) return -1;
+  bem_dom_dev D = dom_view(c, d);
+  CK(cudaMemcpyAsync(c->pt_t, t, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream), "targets");
+  CK(cudaMemcpyAsync(c->pt_in, ze, 2 * sizeof(double) * n, cudaMemcpyHostToDevice, c->stream), "targets");
+  if (bem_launch_bdval(&D, &c->qp, d == 0, c->k0[d], type, n, c->pt_t, c->pt_in, c->P[d], c->dP[d], c->pv[d],
+                       c->dpv[d], c->pt_out, c->status, c->stream))
+    return fail(c, "boundary field", cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->pt_out, 9 * sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream), "boundary field");
+  CK(cudaStreamSynchronize(c->stream), "boundary field");
+  return 0;
+}
+
+// targets of the 9-point force rule: every domain-0 element x 9 rule points
+static int ensure_force_targets(bemgpu_ctx *c) {
+  if (c->ntgt) return 0;
+  const int ne = c->dom_ne[0], n = 9 * ne;
+  const double b = 0.7745966692414833770359, w0 = 25.0 / 81.0, w1 = 40.0 / 81.0, w2 = 64.0 / 81.0;
+  const double z9[9] = {-b, b, b, -b, 0.0, b, 0.0, -b, 0.0}, e9[9] = {-b, -b, b, b, -b, 0.0, b, 0.0, 0.0};
+  const double w9[9] = {w0, w0, w0, w0, w1, w1, w1, w1, w2};
+  std::vector<int> t(n);
+  std::vector<double> ze(2 * (size_t)n), w(n);
+  for (int s = 0; s < ne; ++s)
+    for (int i = 0; i < 9; ++i) {
+      t[9 * s + i] = s;
+      ze[2 * (9 * s + i)] = z9[i];
+      ze[2 * (9 * s + i) + 1] = e9[i];
+      w[9 * s + i] = w9[i];
+    }
+  if (upload(c, &c->tgt_t, t.data(), t.size(), "targets") || upload(c, &c->tgt_ze, ze.data(), ze.size(), "targets") ||
+      upload(c, &c->tgt_w, w.data(), w.size(), "targets"))
+    return -1;
+  CK(dalloc(&c->bdv, 9 * (size_t)n), "boundary values");
+  c->ntgt = n;
   return 0;
 }
 
@@ -550,7 +623,7 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   if (n <= 0) return 0;
   if (ensure_constants(nullptr, nullptr, nullptr, nullptr, nullptr) != 0) return -1;
   bem_qp q;
-  qp_prepare(qpar, &q);
+  bem_qp_prepare(qpar, &q);
   double *wt = nullptr;
   if (cudaMalloc(&wt, BEM_WT_SIZE * sizeof(double)) != cudaSuccess) return -1;
   if (bem_launch_wtab(q.k * q.eta0, wt, 0) != 0) { cudaFree(wt); return -1; }

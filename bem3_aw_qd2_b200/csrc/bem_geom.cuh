@@ -19,6 +19,7 @@ struct bem_quad {
   double xl[BEM_GLN], wl[BEM_GLN];
   double xh[BEM_GHN], wh[BEM_GHN];
   double zt[4], et[4];        // collocation node parameters (zt_44, et_44)
+  double z9[9], e9[9], w9[9]; // 9-point rule (zt_49, et_49, wt_49)
 };
 static __constant__ bem_quad c_q;  // one copy per translation unit
 
@@ -49,6 +50,22 @@ __device__ __forceinline__ void bem_rw(const bem_el &el, double z, double e, dou
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     r[d] = el.cr[d][0] + el.cr[d][1] * z + el.cr[d][2] * e + el.cr[d][3] * z * e;
+    w[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+  }
+}
+
+// The same point with every product and sum rounded separately, in the
+// reference's order ((cr0 + cr1 z) + cr2 e) + (cr3 z) e (bil_rw_zeta_eta,
+// d3qd2_elem.c:963, r_bd, :18, compiled without fused multiply-add).  The
+// boundary-value sums use it so that R = r_s - r_t is bit-identical to the
+// reference's: on mirror-symmetric meshes R_z is then exactly 0 where the
+// reference's is, and the lattice sums take the same stopping decisions
+// (an identically zero z-derivative sum ends the spectral rows at once).
+__device__ __forceinline__ void bem_rw_ref(const bem_el &el, double z, double e, double r[3], double w[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r[d] = __dadd_rn(__dadd_rn(__dadd_rn(el.cr[d][0], __dmul_rn(el.cr[d][1], z)), __dmul_rn(el.cr[d][2], e)),
+                     __dmul_rn(__dmul_rn(el.cr[d][3], z), e));
     w[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
   }
 }

@@ -9,6 +9,7 @@ struct bem_dom_dev {
   int ne;                       // elements bordering the domain
   const int *sid;               // signed element ids (1-based, sign = orientation)
   const double *cr, *cw, *ren;  // element tables, see bem_types.h
+  const double *wen;            // normal vectors at the collocation nodes (field rule 0)
   const uint8_t *plane;         // 1 if the element is plane (bil_check_plane)
 };
 
@@ -30,6 +31,16 @@ int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 // table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)
 int bem_launch_wtab(double x, double *out, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
+int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int npts, const double *pts,
+                     const double *P, const double *dP, const double *pv, const double *dpv, double *out,
+                     unsigned *status, cudaStream_t st);
+int bem_launch_bdval(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int ntgt, const int *tgt_t,
+                     const double *tgt_ze,
+                     const double *P, const double *dP, const double *pv, const double *dpv, double *out,
+                     unsigned *status, cudaStream_t st);
+int bem_launch_force_bd(const bem_dom_dev *D, int ntgt, const int *tgt_t, const double *tgt_ze, const double *wts,
+                        const double *bdv, const double *pw, double k2r, double k2i, const double *rc, double c0,
+                        double rho0, double *out, cudaStream_t st);
 int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,
                         double *G, double *H, double *dG, double *dH, double *dF, cudaStream_t st, cudaEvent_t *ev);
 }

@@ -191,12 +191,80 @@ __device__ __forceinline__ void ew_real_term(const bem_qp &q, double px, double 
 // Ewald spectral term for reciprocal point (n1,n2) (ew_qG2_v1_cFn, d3_qpgf_d2.c:1965);
 // ce = exp(i alpha_n . r) supplied by the caller (recurrence along n2).
 // returns 0 propagating, 1 evanescent, -3 beta_n == 0
-__device__ __forceinline__ int ew_spec_term(const bem_qp &q, double anx, double any, double rz, cplx ce,
+// Quantities that decide a lattice sum's stopping point on the lattice plane
+// are rounded as the reference's C code rounds them (each product and sum
+// separately, no fused multiply-add), so that exact zeros and exact ties
+// come out where the reference's do.
+__device__ __forceinline__ double bem_sub2(double r, int l1, double d1, int l2, double d2) {
+  return __dadd_rn(__dadd_rn(r, -__dmul_rn((double)l1, d1)), -__dmul_rn((double)l2, d2));
+}
+// exp(a) rounded to nearest.  Used only where the reference's rounding of
+// exp decides a stopping test (the lattice plane below): the reference calls
+// the C library's exp, whose results are correctly rounded except in rare
+// near-midpoint cases, so a correctly rounded exp reproduces its decisions.
+// Method: a = n ln2 + r (|r| <= ln2 / 2, ln2 as a double-double), e = exp(r / 1024) - 1
+// by its Taylor series in double-double arithmetic, ten squarings
+// (1 + e)^2 = 1 + (2 e + e^2), then 2^n (1 + e) rounded once.
+struct bem_dd { double hi, lo; };
+__device__ __forceinline__ bem_dd dd_two_sum(double a, double b) {
+  const double s = a + b, bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ bem_dd dd_add(bem_dd x, bem_dd y) {
+  bem_dd s = dd_two_sum(x.hi, y.hi);
+  s.lo += x.lo + y.lo;
+  return dd_two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ bem_dd dd_mul(bem_dd x, bem_dd y) {
+  const double p = x.hi * y.hi;
+  const double e = fma(x.hi, y.hi, -p) + (x.hi * y.lo + x.lo * y.hi);
+  return dd_two_sum(p, e);
+}
+__device__ __forceinline__ bem_dd dd_scale(bem_dd x, double s) {  // s a power of two
+  return {x.hi * s, x.lo * s};
+}
+__device__ double bem_exp_cr(double a) {
+  if (!(a > -700.0 && a < 700.0)) return exp(a);
+  const double ln2_hi = 0.69314718055994528623, ln2_lo = 2.3190468138462995584e-17;
+  const double n = rint(a * 1.4426950408889634074);
+  // r = a - n ln2 in double-double (n ln2_hi exact as a two-product)
+  const double ph = n * ln2_hi, pl = fma(n, ln2_hi, -ph);
+  bem_dd r = dd_two_sum(a - ph, -pl);  // a - ph is exact (Sterbenz)
+  r = dd_add(r, {-n * ln2_lo, -fma(n, ln2_lo, -n * ln2_lo)});
+  r = dd_scale(r, 1.0 / 1024.0);
+  // e = r + r^2/2! + ... + r^10/10! (|r| < 3.4e-4: the next term is below 1e-40)
+  bem_dd term = r, e = r;
+  for (int k = 2; k <= 10; ++k) {
+    term = dd_mul(term, r);
+    term = dd_mul(term, {1.0 / k, fma(-1.0 / k, (double)k, 1.0) / k});
+    e = dd_add(e, term);
+  }
+  for (int i = 0; i < 10; ++i) e = dd_add(dd_scale(e, 2.0), dd_mul(e, e));
+  const bem_dd v = dd_add({1.0, 0.0}, e);
+  return ldexp(v.hi + v.lo, (int)n);
+}
+
+// a_n = -k_par + n1 g1 + n2 g2 (ew_qG2_v1_cFn, d3_qpgf_d2.c:1970)
+__device__ __forceinline__ double bem_an(double mk, int n1, double g1, int n2, double g2) {
+  return __dadd_rn(__dadd_rn(mk, __dmul_rn((double)n1, g1)), __dmul_rn((double)n2, g2));
+}
+// Ewald parameter, capped where k^2 eta^2 - r^2 / 4 eta^2 > EW_EXPM (d3_qpgf_d2.c:1684-1697)
+__device__ __forceinline__ double bem_ewald_eta(const bem_qp &q, double rx, double ry, double rz) {
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+  const double ve = q.eta0, kk = __dmul_rn(q.k, q.k);
+  const double lhs = __dadd_rn(__dmul_rn(__dmul_rn(kk, ve), ve), -__ddiv_rn(r2, __dmul_rn(__dmul_rn(4.0, ve), ve)));
+  if (lhs > BEM_EW_EXPM)
+    return __ddiv_rn(__dsqrt_rn(__dadd_rn(BEM_EW_EXPM, __dsqrt_rn(__dadd_rn(__dmul_rn(kk, r2), BEM_EW_EXPM * BEM_EW_EXPM)))),
+                     __dmul_rn(1.4142135623730950488, q.k));
+  return ve;
+}
+
+__device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, double anx, double any, double rz, cplx ce,
                                             double ve, cplx &Fn, cplx &dF0, cplx &dF1, cplx &dF2) {
-  const double bn2 = q.k * q.k - anx * anx - any * any;
+  const double bn2 = __dadd_rn(__dadd_rn(__dmul_rn(q.k, q.k), -__dmul_rn(anx, anx)), -__dmul_rn(any, any));
   const double azve = rz / (2.0 * ve);
   if (bn2 > 0.0) {
-    const double bn = sqrt(bn2);
+    const double bn = __dsqrt_rn(bn2);
     const double ef = exp(bn2 * ve * ve - azve * azve);
     const cplx ff = cexpi(bn * rz);
     const cplx w = bem_faddeeva(bn * ve, azve);
@@ -204,7 +272,27 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, double anx, double 
     Fn = cscale(cmul(ce, cmk(ff.re, ef * w.im + ff.im)), 2.0 / bn);
     dF0 = cscale(Fn, anx);
     dF1 = cscale(Fn, any);
-    dF2 = cscale(cmul(ce, cmk(ef * w.re - ff.re, -ff.im)), 2.0);
+    if (rz == 0.0) {
+      // On the lattice plane ef Re w(bn ve) - 1 is zero up to rounding; the
+      // reference's rows stop on an identically zero z-derivative sum, so the
+      // residue must be the reference's rounded value: the host's table at
+      // eta0, else formed as the reference forms it (Faddeeva_w on the real
+      // axis is exp(-x^2), Faddeeva.cc:684; ef = exp(bn2 ve ve)).
+      double d = 0.0;
+      int hit = -1;
+      if (ve == q.eta0)
+        for (int i = 0; i < q.pz_n; ++i)
+          if (q.pz_n1[i] == n1 && q.pz_n2[i] == n2) { hit = i; break; }
+      if (hit >= 0) {
+        d = q.pz_d[hit];
+      } else {
+        const double x = __dmul_rn(bn, ve);
+        d = __dadd_rn(__dmul_rn(bem_exp_cr(__dmul_rn(__dmul_rn(bn2, ve), ve)), bem_exp_cr(-__dmul_rn(x, x))), -1.0);
+      }
+      dF2 = cscale(ce, 2.0 * d);
+    } else {
+      dF2 = cscale(cmul(ce, cmk(ef * w.re - ff.re, -ff.im)), 2.0);
+    }
     return 0;
   } else if (bn2 < 0.0) {
     const double bn = sqrt(-bn2);
@@ -229,10 +317,7 @@ __device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.re, -a.im); }
 // then down, each stopped by the reference's tests); the Bloch phases along a
 // row are advanced by a unit complex factor, so a row costs one sincos.
 __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
-  double ve = q.eta0;
-  const double r2 = rx * rx + ry * ry + rz * rz;
-  if (q.k * q.k * ve * ve - r2 / (4.0 * ve * ve) > BEM_EW_EXPM)
-    ve = sqrt(BEM_EW_EXPM + sqrt(q.k * q.k * r2 + BEM_EW_EXPM * BEM_EW_EXPM)) / (1.4142135623730950488 * q.k);
+  const double ve = bem_ewald_eta(q, rx, ry, rz);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
   const bool tab = q.wt != nullptr && ve == q.eta0;  // table built for x = k eta0
   const double eps = BEM_MEPS;
@@ -304,7 +389,8 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
         int k = 0;
         for (; k < nmax; ++k, n2 += st) {
           cplx Fn, d0, d1, d2;
-          const int e = ew_spec_term(q, a0x + n2 * q.g2x, a0y + n2 * q.g2y, rz, ce, ve, Fn, d0, d1, d2);
+          const int e = ew_spec_term(q, n1, n2, bem_an(-q.kx, n1, q.g1x, n2, q.g2x),
+                                     bem_an(-q.ky, n1, q.g1y, n2, q.g2y), rz, ce, ve, Fn, d0, d1, d2);
           if (e < 0) return -23;
           ++cc;
           t = cadd(t, Fn);
@@ -410,8 +496,8 @@ __device__ int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gv
   }
   const int l1 = (int)floor((rx * q.d2y - ry * q.d2x) * q.idet + 0.5);
   const int l2 = (int)floor(-(rx * q.d1y - ry * q.d1x) * q.idet + 0.5);
-  const double hx = rx - l1 * q.d1x - l2 * q.d2x;
-  const double hy = ry - l1 * q.d1y - l2 * q.d2y;
+  const double hx = bem_sub2(rx, l1, q.d1x, l2, q.d2x);
+  const double hy = bem_sub2(ry, l1, q.d1y, l2, q.d2y);
   const int e = spectral ? bem_qpgf_spectral(q, hx, hy, rz, out) : bem_qpgf_ewald(q, hx, hy, rz, out);
   if (e > 0 && (l1 != 0 || l2 != 0)) {
     const cplx cf = cexpi(-(q.kx * (l1 * q.d1x + l2 * q.d2x) + q.ky * (l1 * q.d1y + l2 * q.d2y)));
@@ -419,6 +505,263 @@ __device__ int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gv
     out.gx = cmul(out.gx, cf);
     out.gy = cmul(out.gy, cf);
     out.gz = cmul(out.gz, cf);
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------- second derivatives
+// G_qp, grad G_qp and the second derivatives d2 = {xx, yy, zz, xy, yz, zx}
+// (d3hm_qpgf_d2_v2, d3_qpgf_d2.c:178-230; Ewald terms :2011-2399, spectral
+// :887-1044).  Used by the field evaluation at points off the boundary.  The
+// stopping tests are the reference's for this variant: the real-space and
+// Ewald-spectral sums test d2_xx and d2_yy, the pure spectral sum d2_zz.
+struct bem_gval2 { cplx g, d[3], d2[6]; };
+
+__device__ __forceinline__ cplx cmuli(cplx a) { return cmk(-a.im, a.re); }  // i a
+
+__device__ int bem_qpgf2_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval2 &o) {
+  const double ve = bem_ewald_eta(q, rx, ry, rz);
+  const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
+  const bool tab = q.wt != nullptr && ve == q.eta0;
+  const double eps = BEM_MEPS, isp = 0.56418958354775628695;
+  int cc = 0;
+  const cplx E2 = cexpi(q.kx * q.d2x + q.ky * q.d2y);
+  cplx s = cmk(0, 0), sd[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, s2[6];
+  for (int c = 0; c < 6; ++c) s2[c] = cmk(0, 0);
+  for (int dir = 0; dir < 3; ++dir) {
+    int l1 = dir == 2 ? -1 : (dir == 1 ? 1 : 0);
+    const int step = dir == 2 ? -1 : 1;
+    bool done = false;
+    for (int it = 0; it < (dir == 0 ? 1 : BEM_EW_LIMIT - 1); ++it, l1 += step) {
+      const cplx o0 = s2[0], o1 = s2[1];
+      const int lc = -(int)round(((rx + l1 * q.d1x) * q.d2x + (ry + l1 * q.d1y) * q.d2y) / q.d2sq);
+      const cplx pc = cexpi(q.kx * (l1 * q.d1x + lc * q.d2x) + q.ky * (l1 * q.d1y + lc * q.d2y));
+      for (int side = 0; side < 3; ++side) {
+        int l2 = side == 0 ? lc : (side == 1 ? lc + 1 : lc - 1);
+        const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(E2) : E2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
+        const int nmax = side == 0 ? 1 : BEM_EW_LIMIT - 1;
+        int k = 0;
+        for (; k < nmax; ++k, l2 += st) {
+          const double px = rx + l1 * q.d1x + l2 * q.d2x, py = ry + l1 * q.d1y + l2 * q.d2y;
+          const double rl = sqrt(px * px + py * py + rz * rz);
+          const double irl = 1.0 / rl, irl2 = irl * irl;
+          const double rl2e = rl * 0.5 * ive;
+          const double ef = exp(ke2 - rl2e * rl2e);
+          const cplx w = tab ? bem_wtab(q, ke, rl2e) : bem_faddeeva(ke, rl2e);
+          const cplx cef = cscale(ce, ef);
+          const cplx cf1 = cscale(cef, irl2 * (irl * w.re - q.k * w.im + ive * isp));
+          const cplx cf2 = cscale(cef, irl2 * (q.k * q.k * irl * 2.0 * w.re - ive * ive * ive * isp));
+          const cplx cf3 = cadd(cscale(cf1, -6.0 * irl2), cf2);
+          ++cc;
+          s = cadd(s, cscale(cef, irl * w.re));
+          sd[0] = cadd(sd[0], cscale(cf1, px));
+          sd[1] = cadd(sd[1], cscale(cf1, py));
+          sd[2] = cadd(sd[2], cf1);
+          const cplx t0 = cadd(cscale(cf1, 2.0), cscale(cf3, px * px));
+          const cplx t1 = cadd(cscale(cf1, 2.0), cscale(cf3, py * py));
+          s2[0] = cadd(s2[0], t0);
+          s2[1] = cadd(s2[1], t1);
+          s2[2] = cadd(s2[2], cadd(cscale(cf1, 2.0), cscale(cf3, rz * rz)));
+          s2[3] = cadd(s2[3], cscale(cf3, px * py));
+          s2[4] = cadd(s2[4], cscale(cf3, py));
+          s2[5] = cadd(s2[5], cscale(cf3, px));
+          if (side != 0 && bem_small(t0, s2[0], eps) && bem_small(t1, s2[1], eps)) break;
+          ce = cmul(ce, E);
+        }
+        if (side != 0 && k == nmax) return -21;
+      }
+      if (dir != 0 && bem_same(s2[0], o0, eps) && bem_same(s2[1], o1, eps)) { done = true; break; }
+    }
+    if (dir != 0 && !done) return -21;
+  }
+  const double i4p = 0.07957747154594766788, i8p = 0.5 * i4p;
+  o.g = cscale(s, i4p);
+  o.d[0] = cscale(sd[0], -i4p);
+  o.d[1] = cscale(sd[1], -i4p);
+  o.d[2] = cscale(sd[2], -rz * i4p);
+  for (int c = 0; c < 4; ++c) o.d2[c] = cscale(s2[c], -i8p);
+  o.d2[4] = cscale(s2[4], -rz * i8p);
+  o.d2[5] = cscale(s2[5], -rz * i8p);
+
+  const cplx G2 = cexpi(q.g2x * rx + q.g2y * ry);
+  cplx t = cmk(0, 0), td[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, t2[6];
+  for (int c = 0; c < 6; ++c) t2[c] = cmk(0, 0);
+  const double azve = rz / (2.0 * ve), c2pi = 2.0 * isp * ive;
+  for (int dir = 0; dir < 3; ++dir) {
+    int n1 = q.nc1 + (dir == 2 ? -1 : (dir == 1 ? 1 : 0));
+    const int step = dir == 2 ? -1 : 1;
+    bool done = false;
+    for (int it = 0; it < (dir == 0 ? 1 : BEM_EW_LIMIT - 1); ++it, n1 += step) {
+      const cplx o0 = t2[0], o1 = t2[1];
+      const int nc = (int)round(-((-q.kx + n1 * q.g1x) * q.g2x + (-q.ky + n1 * q.g1y) * q.g2y) / q.g2sq);
+      const double a0x = -q.kx + n1 * q.g1x, a0y = -q.ky + n1 * q.g1y;
+      const cplx pc = cexpi((a0x + nc * q.g2x) * rx + (a0y + nc * q.g2y) * ry);
+      int flg = 0;
+      for (int side = 0; side < 3; ++side) {
+        int n2 = side == 0 ? nc : (side == 1 ? nc + 1 : nc - 1);
+        const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(G2) : G2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
+        const int nmax = side == 0 ? 1 : BEM_EW_LIMIT - 1;
+        int k = 0;
+        for (; k < nmax; ++k, n2 += st) {
+          const double anx = a0x + n2 * q.g2x, any = a0y + n2 * q.g2y;
+          const double bn2 = q.k * q.k - anx * anx - any * any;
+          const double ef = exp(bn2 * ve * ve - azve * azve);
+          cplx Fn, dz, dzz;
+          int e;
+          if (bn2 > 0.0) {
+            const double bn = sqrt(bn2);
+            const cplx ff = cexpi(bn * rz);
+            const cplx w = bem_faddeeva(bn * ve, azve);
+            const cplx F = cmk(2.0 * ff.re, 2.0 * (ef * w.im + ff.im));
+            const cplx Gq = cmk(2.0 * (ef * w.re - ff.re), -2.0 * ff.im);
+            Fn = cscale(cmul(ce, F), 1.0 / bn);
+            dz = cmul(ce, Gq);
+            dzz = cmul(ce, cadd(cscale(cmuli(F), bn), cmk(c2pi * ef, 0.0)));
+            e = 0;
+          } else if (bn2 < 0.0) {
+            const double bn = sqrt(-bn2);
+            const double ebz = exp(bn * rz);
+            const double f1 = ebz * erfc(bn * ve + azve), f2 = erfc(bn * ve - azve) / ebz;
+            Fn = cmul(ce, cmk(0.0, -(f1 + f2) / bn));
+            dz = cscale(ce, f1 - f2);
+            dzz = cscale(ce, -bn * (f1 + f2) + c2pi * ef);
+            e = 1;
+          } else {
+            return -23;
+          }
+          ++cc;
+          const cplx d0 = cscale(Fn, anx), d1 = cscale(Fn, any);
+          const cplx e0 = cscale(d0, anx), e1 = cscale(d1, any);
+          t = cadd(t, Fn);
+          td[0] = cadd(td[0], d0);
+          td[1] = cadd(td[1], d1);
+          td[2] = cadd(td[2], dz);
+          t2[0] = cadd(t2[0], e0);
+          t2[1] = cadd(t2[1], e1);
+          t2[2] = cadd(t2[2], dzz);
+          t2[3] = cadd(t2[3], cscale(d0, any));
+          t2[4] = cadd(t2[4], cscale(dz, any));
+          t2[5] = cadd(t2[5], cscale(dz, anx));
+          if (side != 0) {
+            if (e > 0) { if (bem_small(e0, t2[0], eps) && bem_small(e1, t2[1], eps)) break; }
+            else ++flg;
+          }
+          ce = cmul(ce, E);
+        }
+        if (side != 0 && k == nmax) return -22;
+      }
+      if (dir != 0 && flg == 0 && bem_same(t2[0], o0, eps) && bem_same(t2[1], o1, eps)) { done = true; break; }
+    }
+    if (dir != 0 && !done) return -22;
+  }
+  const double cd = 0.25 * q.aidet;
+  o.g = cadd(o.g, cscale(cmuli(t), cd));
+  o.d[0] = cadd(o.d[0], cscale(td[0], -cd));
+  o.d[1] = cadd(o.d[1], cscale(td[1], -cd));
+  o.d[2] = cadd(o.d[2], cscale(td[2], cd));
+  o.d2[0] = cadd(o.d2[0], cscale(cmuli(t2[0]), -cd));
+  o.d2[1] = cadd(o.d2[1], cscale(cmuli(t2[1]), -cd));
+  o.d2[2] = cadd(o.d2[2], cscale(t2[2], -cd));
+  o.d2[3] = cadd(o.d2[3], cscale(cmuli(t2[3]), -cd));
+  o.d2[4] = cadd(o.d2[4], cscale(cmuli(t2[4]), cd));
+  o.d2[5] = cadd(o.d2[5], cscale(cmuli(t2[5]), cd));
+  return cc;
+}
+
+__device__ int bem_qpgf2_spectral(const bem_qp &q, double rx, double ry, double rz, bem_gval2 &o) {
+  if (rz == 0.0) return -14;
+  const double eps = BEM_MEPS, az = fabs(rz);
+  int cc = 0;
+  const cplx G2 = cexpi(q.g2x * rx + q.g2y * ry);
+  cplx t = cmk(0, 0), td[3] = {cmk(0, 0), cmk(0, 0), cmk(0, 0)}, t2[6];
+  for (int c = 0; c < 6; ++c) t2[c] = cmk(0, 0);
+  for (int dir = 0; dir < 3; ++dir) {
+    int n1 = q.nc1 + (dir == 2 ? -1 : (dir == 1 ? 1 : 0));
+    const int step = dir == 2 ? -1 : 1;
+    bool done = false;
+    for (int it = 0; it < (dir == 0 ? 1 : BEM_FD_LIMIT - 1); ++it, n1 += step) {
+      const cplx old = t2[2];
+      const int nc = (int)round((q.kx * q.g2x + q.ky * q.g2y - n1 * q.g1g2) / q.g2sq);
+      const double a0x = -q.kx + n1 * q.g1x, a0y = -q.ky + n1 * q.g1y;
+      const cplx pc = cexpi((a0x + nc * q.g2x) * rx + (a0y + nc * q.g2y) * ry);
+      for (int side = 0; side < 3; ++side) {
+        int n2 = side == 0 ? nc : (side == 1 ? nc + 1 : nc - 1);
+        const int st = side == 2 ? -1 : 1;
+        const cplx E = side == 2 ? cconj(G2) : G2;
+        cplx ce = side == 0 ? pc : cmul(pc, E);
+        const int nmax = side == 0 ? 1 : BEM_FD_LIMIT - 1;
+        int k = 0;
+        for (; k < nmax; ++k, n2 += st) {
+          const double anx = a0x + n2 * q.g2x, any = a0y + n2 * q.g2y;
+          const double bn2 = q.k * q.k - anx * anx - any * any;
+          cplx d2, Fn;
+          int e;
+          if (bn2 > 0.0) {
+            const double bn = sqrt(bn2);
+            d2 = cmul(ce, cexpi(bn * az));
+            Fn = cscale(d2, 1.0 / bn);
+            e = 0;
+          } else if (bn2 < 0.0) {
+            const double bn = sqrt(-bn2);
+            d2 = cscale(ce, exp(-bn * az));
+            Fn = cmk(d2.im / bn, -d2.re / bn);
+            e = 1;
+          } else {
+            return -12;
+          }
+          ++cc;
+          const cplx d0 = cscale(Fn, anx), d1 = cscale(Fn, any), zz = cscale(Fn, bn2);
+          t = cadd(t, Fn);
+          td[0] = cadd(td[0], d0);
+          td[1] = cadd(td[1], d1);
+          td[2] = cadd(td[2], d2);
+          t2[0] = cadd(t2[0], cscale(d0, anx));
+          t2[1] = cadd(t2[1], cscale(d1, any));
+          t2[2] = cadd(t2[2], zz);
+          t2[3] = cadd(t2[3], cscale(d1, anx));
+          t2[4] = cadd(t2[4], cscale(d2, any));
+          t2[5] = cadd(t2[5], cscale(d2, anx));
+          if (side != 0 && e > 0 && bem_small(zz, t2[2], eps)) break;
+          ce = cmul(ce, E);
+        }
+        if (side != 0 && k == nmax) return -11;
+      }
+      if (dir != 0 && bem_same(t2[2], old, eps)) { done = true; break; }
+    }
+    if (dir != 0 && !done) return -11;
+  }
+  const double c = 0.5 * q.aidet, sz = rz > 0 ? 1.0 : -1.0;
+  o.g = cscale(cmuli(t), c);
+  o.d[0] = cscale(td[0], -c);
+  o.d[1] = cscale(td[1], -c);
+  o.d[2] = cscale(td[2], -c * sz);
+  for (int m = 0; m < 4; ++m) o.d2[m] = cscale(cmuli(t2[m]), -c);
+  o.d2[4] = cscale(cmuli(t2[4]), -c * sz);
+  o.d2[5] = cscale(cmuli(t2[5]), -c * sz);
+  return cc;
+}
+
+__device__ int bem_qpgf2(const bem_qp &q, double rx, double ry, double rz, bem_gval2 &out) {
+  bool spectral = false;
+  if (!q.ewald_only) {
+    const double az = fabs(rz);
+    spectral = q.sel_cp * exp(-q.sel_bp * az) < BEM_MEPS && q.sel_cm * exp(-q.sel_bm * az) < BEM_MEPS;
+    if (spectral && (36.0 / az) * (36.0 / az) * fabs(q.det) * 0.0795774715459476679 > BEM_FD_MAX_TERMS) spectral = false;
+  }
+  const int l1 = (int)floor((rx * q.d2y - ry * q.d2x) * q.idet + 0.5);
+  const int l2 = (int)floor(-(rx * q.d1y - ry * q.d1x) * q.idet + 0.5);
+  const double hx = bem_sub2(rx, l1, q.d1x, l2, q.d2x);
+  const double hy = bem_sub2(ry, l1, q.d1y, l2, q.d2y);
+  const int e = spectral ? bem_qpgf2_spectral(q, hx, hy, rz, out) : bem_qpgf2_ewald(q, hx, hy, rz, out);
+  if (e > 0 && (l1 != 0 || l2 != 0)) {
+    const cplx cf = cexpi(-(q.kx * (l1 * q.d1x + l2 * q.d2x) + q.ky * (l1 * q.d1y + l2 * q.d2y)));
+    out.g = cmul(out.g, cf);
+    for (int c = 0; c < 3; ++c) out.d[c] = cmul(out.d[c], cf);
+    for (int c = 0; c < 6; ++c) out.d2[c] = cmul(out.d2[c], cf);
   }
   return e;
 }

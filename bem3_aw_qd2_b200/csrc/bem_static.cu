@@ -22,6 +22,7 @@
 #include <string.h>
 #include "../../include/bemgpu.h"
 #include "bem_kernels.h"
+#include "bem_lattice.h"
 
 #define SMAX_N (4 * BEMGPU_STATIC_MAX_NE)
 #define ALIGN256(x) (((x) + 255) & ~(size_t)255)
@@ -66,47 +67,6 @@ static void gl_nodes(int n, double *x, double *w) {
   if (n % 2 == 1) x[n / 2] = 0.0;
 }
 
-// Lattice quantities of the quasi-periodic Green's function for qp = {k, kx,
-// ky, kz, d1x, d1y, d2x, d2y} (the reference derives them inside every call,
-// qgf2_src/d3_qpgf_d2.c:126-156, 1679-1681, 1850-1856).
-static void lattice(const double *p, bem_qp *q) {
-  memset(q, 0, sizeof(*q));
-  q->k = p[0]; q->kx = p[1]; q->ky = p[2];
-  q->d1x = p[4]; q->d1y = p[5]; q->d2x = p[6]; q->d2y = p[7];
-  q->det = q->d1x * q->d2y - q->d2x * q->d1y;
-  q->idet = 1.0 / q->det;
-  q->aidet = fabs(q->idet);
-  const double cpd = 2.0 * M_PI * q->idet;
-  q->g1x = cpd * q->d2y; q->g1y = -cpd * q->d2x;
-  q->g2x = -cpd * q->d1y; q->g2y = cpd * q->d1x;
-  q->d2sq = q->d2x * q->d2x + q->d2y * q->d2y;
-  q->g2sq = q->g2x * q->g2x + q->g2y * q->g2y;
-  q->g1g2 = q->g1x * q->g2x + q->g1y * q->g2y;
-  const double adp = sqrt(pow(q->d1x + q->d2x, 2) + pow(q->d1y + q->d2y, 2));
-  const double adm = sqrt(pow(q->d1x - q->d2x, 2) + pow(q->d1y - q->d2y, 2));
-  q->eta0 = sqrt(fabs(q->det) / (4.0 * M_PI) * adp / adm);
-  q->nc1 = (int)round((q->kx * q->d1x + q->ky * q->d1y) / (2.0 * M_PI));
-  const double k2 = q->k * q->k;
-  const int n1 = q->nc1, n2 = (int)round((q->kx * q->d2x + q->ky * q->d2y) / (2.0 * M_PI));
-  const double ad12 = q->d1x * q->d1x + q->d1y * q->d1y, ad22 = q->d2sq;
-  const double aNx = -q->kx + n1 * cpd * q->d2y - n2 * cpd * q->d1y;
-  const double aNy = -q->ky - n1 * cpd * q->d2x + n2 * cpd * q->d1x;
-  const double bN = sqrt(k2 - aNx * aNx - aNy * aNy);
-  const int a1 = ad22 < ad12 ? 15 : 0, a2 = ad22 < ad12 ? 0 : 15;
-  const double aNpx = -q->kx + (n1 + a1) * cpd * q->d2y - (n2 + a2) * cpd * q->d1y;
-  const double aNpy = -q->ky - (n1 + a1) * cpd * q->d2x + (n2 + a2) * cpd * q->d1x;
-  const double aNmx = -q->kx + (n1 - a1) * cpd * q->d2y - (n2 - a2) * cpd * q->d1y;
-  const double aNmy = -q->ky - (n1 - a1) * cpd * q->d2x + (n2 - a2) * cpd * q->d1x;
-  const double bNp = k2 - aNpx * aNpx - aNpy * aNpy, bNm = k2 - aNmx * aNmx - aNmy * aNmy;
-  if (bNp > 0.0 || bNm > 0.0) {
-    q->ewald_only = 1;
-  } else {
-    q->sel_bp = sqrt(-bNp);
-    q->sel_bm = sqrt(-bNm);
-    q->sel_cp = bN / q->sel_bp;
-    q->sel_cm = bN / q->sel_bm;
-  }
-}
 
 // Once per device, with that device current: the device address of the
 // scratch array and the quadrature / Faddeeva constant tables.
@@ -153,7 +113,7 @@ extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw,
   bem_dom_dev D;
   D.ne = ne; D.sid = sid; D.cr = cr; D.cw = cw; D.ren = ren; D.plane = plane;
   bem_qp q;
-  lattice(qp, &q);
+  bem_qp_prepare(qp, &q);
   if (bem_launch_assemble(&D, &q, periodic != 0, periodic != 0, k, &S, G, H, dG, dH, dF, st, nullptr) != 0) return -4;
   unsigned status = 0;
   if (cudaMemcpyAsync(&status, S.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -4;

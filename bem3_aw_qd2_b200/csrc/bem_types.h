@@ -19,6 +19,8 @@ extern "C" {
 /* Lattice / Bloch data for the quasi-periodic Green's function (the reference's
  * QPD2, qgf2_src/d3_qpgf_d2.h:32-36) plus quantities derived once per
  * (k, k_par, lattice) by bem_qp_prepare(). */
+#define BEM_PZ_MAX 24
+
 typedef struct bem_qp {
   double k, kx, ky;             /* wave number and in-plane Bloch wave vector */
   double d1x, d1y, d2x, d2y;    /* lattice vectors */
@@ -36,6 +38,11 @@ typedef struct bem_qp {
   const double *wt;
   double wt_h;
   int wt_n;
+  /* residues ef Re w - 1 of the propagating spectral orders (pz_n1, pz_n2) on
+     the lattice plane at eta0; pz_n = -1: more orders than the table holds */
+  int pz_n;
+  int pz_n1[BEM_PZ_MAX], pz_n2[BEM_PZ_MAX];
+  double pz_d[BEM_PZ_MAX];
 } bem_qp;
 
 /* status word bits written by the kernels (never trapped on the device) */

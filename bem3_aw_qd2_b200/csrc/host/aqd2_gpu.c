@@ -122,6 +122,12 @@ static void load_problem(AQD2 *qd, bemgpu_ctx *c)
   pr.dom_ne = dom_ne; pr.sid = sid; pr.k0 = qd->k0; pr.k2 = k2; pr.rho0 = qd->rho0; pr.c0 = qd->c0;
   pr.Pi = Pi; pr.dPi = dPi; pr.p_inc = pinc; pr.v_inc = vinc;
   pr.xl = bd->xli; pr.wl = bd->wli; pr.xh = bd->xhi; pr.wh = bd->whi; pr.plane = plane;
+  pr.pw[0] = creal(qd->pw.p);
+  pr.pw[1] = cimag(qd->pw.p);
+  for (int i = 0; i < 9; i++) pr.pw[2 + i] = qd->pw.wd.R[i];
+  for (int i = 0; i < 3; i++) pr.pw[11 + i] = qd->pw.tv[i];
+  pr.pw[14] = qd->pw.wd.k0;
+  pr.pw[15] = qd->pw.rho0 * qd->pw.c0;
   gpu_check(c, bemgpu_load(c, &pr), "load");
   gpu_check(c, bemgpu_sync(c), "load");
   free(cr); free(cw); free(ren); free(wen); free(Pi); free(dPi); free(pinc); free(vinc);
@@ -184,20 +190,59 @@ void solve_bieq_aqd2(AQD2 *qd)
   if (g_verbose) printf("Total elapsed time : %g (sec)\n", t4 - t0);
 }
 
-/* Upload the boundary values held in the AQD2 (for example after dat_read_aqd2)
- * into a device context that has the problem loaded. */
+static void upload_solution(AQD2 *qd, bemgpu_ctx *c)
+{
+  for (int d = 0; d <= qd->MN; d++) {
+    SUBD *s = &qd->bd.sb[d];
+    size_t N = 4 * (size_t)s->Ne;
+    double *P = aqd2_calloc(2 * N, sizeof(double), "P"), *dP = aqd2_calloc(2 * N, sizeof(double), "dP");
+    double *pv = aqd2_calloc(6 * N, sizeof(double), "pv"), *dpv = aqd2_calloc(6 * N, sizeof(double), "dpv");
+    for (int t = 1; t <= s->Ne; t++)
+      for (int n = 0; n < 4; n++) {
+        size_t q = (size_t)(t - 1) * 4 + n;
+        P[2 * q] = creal(s->P[t][n]);
+        P[2 * q + 1] = cimag(s->P[t][n]);
+        dP[2 * q] = creal(s->dP[t][n]);
+        dP[2 * q + 1] = cimag(s->dP[t][n]);
+        for (int l = 0; l < 3; l++) {
+          pv[2 * (3 * q + l)] = creal(s->pv[t][n][l]);
+          pv[2 * (3 * q + l) + 1] = cimag(s->pv[t][n][l]);
+          dpv[2 * (3 * q + l)] = creal(s->dpv[t][n][l]);
+          dpv[2 * (3 * q + l) + 1] = cimag(s->dpv[t][n][l]);
+        }
+      }
+    gpu_check(c, bemgpu_set_solution(c, d, P, dP, pv, dpv), "upload");
+    free(P); free(dP); free(pv); free(dpv);
+  }
+}
+
+/* The device context holding qd's boundary values.  After solve_bieq_aqd2 the
+ * context already has them; for an object filled by dat_read_aqd2 the problem
+ * and the stored boundary values are uploaded on first use. */
 static bemgpu_ctx *ready_ctx(AQD2 *qd)
 {
   bemgpu_ctx *c = ctx_for(qd, 0);
   if (c) return c;
-  printf("bem3_aw_qd2: the device post-processing needs the solution on the device; call solve_bieq_aqd2 first. Exit...\n");
-  exit(1);
+  c = ctx_for(qd, 1);
+  load_problem(qd, c);
+  upload_solution(qd, c);
+  return c;
+}
+
+static void status_check(bemgpu_ctx *c, const char *what)
+{
+  unsigned st = bemgpu_status(c);
+  if (st) {
+    printf("bem3_aw_qd2 (%s): device status 0x%x (1: lattice-sum limit, 2: Rayleigh anomaly, 4: near-singular table, 8: non-finite, 16: geometry). Exit...\n", what, st);
+    exit(1);
+  }
 }
 
 void force_FN_aqd2(double *F, double *N, double *rc, int type, AQD2 *qd)
 {
   bemgpu_ctx *c = ready_ctx(qd);
   gpu_check(c, bemgpu_force(c, type, rc, F, N), "force");
+  status_check(c, "force");
 }
 
 int pv_i_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd)
@@ -224,18 +269,202 @@ int phi_i_aqd2(double complex *phi, double *rt, int type, AQD2 *qd)
   return domain_id_aqd2(rt, qd);
 }
 
-static void not_yet(const char *fn)
+static int domain_id_home(double *rt, AQD2 *qd);
+
+/* Element sums of one field point (bem3_aw_qd2_field.c:3-54, 128-297): the
+ * point is moved to the home lattice cell (domain_id_l_aqd2), its domain found
+ * by the solid-angle test, and the sums of that domain evaluated on the
+ * device.  Returns the domain id; o = bemgpu_field's 18 values, ce the Bloch
+ * phase of the cell shift. */
+static int field_sums(double o[18], double complex *ce, double *rt, int type, AQD2 *qd)
 {
-  printf("bem3_aw_qd2: %s is not implemented on the device in this build. Exit...\n", fn);
-  exit(1);
+  int l1 = 0, l2 = 0;
+  double r0[3] = {rt[0], rt[1], rt[2]};
+  if (type < 0 || type > 3) {
+    printf("bem3_aw_qd2: field rule type=%d is not available (0: 4-point, 1: 9-point, 2: GLN-point, 3: GHN-point). Exit...\n", type);
+    exit(1);
+  }
+  if (qd->bd.ps == 1) {
+    domain_id_l_aqd2(&l1, &l2, rt, qd);
+    r0[0] = rt[0] - l1 * qd->bd.qd.vd1[0] - l2 * qd->bd.qd.vd2[0];
+    r0[1] = rt[1] - l1 * qd->bd.qd.vd1[1] - l2 * qd->bd.qd.vd2[1];
+  }
+  int did = domain_id_home(r0, qd);
+  if (did < 0) {
+    printf("bem3_aw_qd2: the point (%g, %g, %g) lies in no domain. Exit...\n", rt[0], rt[1], rt[2]);
+    exit(1);
+  }
+  bemgpu_ctx *c = ready_ctx(qd);
+  gpu_check(c, bemgpu_field(c, did, type, 1, r0, o), "field");
+  status_check(c, "field");
+  *ce = 1.0;
+  if (l1 != 0 || l2 != 0) {
+    double arg = qd->bd.qd.vk[0] * (l1 * qd->bd.qd.vd1[0] + l2 * qd->bd.qd.vd2[0]) +
+                 qd->bd.qd.vk[1] * (l1 * qd->bd.qd.vd1[1] + l2 * qd->bd.qd.vd2[1]);
+    *ce = cos(arg) + I * sin(arg);
+  }
+  return did;
 }
 
-int phi_s_aqd2(double complex *phi, double *rt, int type, AQD2 *qd) { (void)phi; (void)rt; (void)type; (void)qd; not_yet("phi_s_aqd2"); return -1; }
-int phi_t_aqd2(double complex *phi, double *rt, int type, AQD2 *qd) { (void)phi; (void)rt; (void)type; (void)qd; not_yet("phi_t_aqd2"); return -1; }
-int p_s_aqd2(double complex *p, double *rt, int type, AQD2 *qd) { (void)p; (void)rt; (void)type; (void)qd; not_yet("p_s_aqd2"); return -1; }
-int p_t_aqd2(double complex *p, double *rt, int type, AQD2 *qd) { (void)p; (void)rt; (void)type; (void)qd; not_yet("p_t_aqd2"); return -1; }
-int pv_s_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd) { (void)p; (void)pv; (void)rt; (void)type; (void)qd; not_yet("pv_s_aqd2"); return -1; }
-int pv_t_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd) { (void)p; (void)pv; (void)rt; (void)type; (void)qd; not_yet("pv_t_aqd2"); return -1; }
+#define FS_S0(o) ((o)[0] + I * (o)[1])
+#define FS_S1(o, j) ((o)[2 + 2 * (j)] + I * (o)[3 + 2 * (j)])
+#define FS_S2(o, j) ((o)[12 + 2 * (j)] + I * (o)[13 + 2 * (j)])
+
+int phi_s_aqd2(double complex *phi, double *rt, int type, AQD2 *qd)
+{
+  double o[18];
+  double complex ce;
+  int did = field_sums(o, &ce, rt, type, qd);
+  *phi = FS_S0(o) / (did == 0 ? 1.0 + o[8] : o[8]) * ce;
+  return did;
+}
+
+int phi_t_aqd2(double complex *phi, double *rt, int type, AQD2 *qd)
+{
+  double complex p, v[3];
+  int did = phi_s_aqd2(phi, rt, type, qd);
+  if (did == 0) {
+    calc_apw_pv(&p, v, rt, &qd->pw);
+    *phi += -p / qd->pw.wd.k2;
+  }
+  return did;
+}
+
+int p_s_aqd2(double complex *p, double *rt, int type, AQD2 *qd)
+{
+  int did = phi_s_aqd2(p, rt, type, qd);
+  *p *= -qd->k2[did];
+  return did;
+}
+
+int p_t_aqd2(double complex *p, double *rt, int type, AQD2 *qd)
+{
+  int did = phi_t_aqd2(p, rt, type, qd);
+  *p *= -qd->k2[did];
+  return did;
+}
+
+/* pv_s_aqd2 = pv_s_dbieq_aqd2, or pv_s_bieq_aqd2 near the boundary, where a
+ * component of grad F exceeds CBD_CDF (bem3_aw_qd2_field.c:128-144, 231-297). */
+int pv_s_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd)
+{
+  double o[18];
+  double complex ce;
+  int did = field_sums(o, &ce, rt, type, qd);
+  double iC = 1.0 / (did == 0 ? 1.0 + o[8] : o[8]);
+  double complex P = FS_S0(o);
+  if (fabs(o[9]) > AQD2_CBD_CDF || fabs(o[10]) > AQD2_CBD_CDF || fabs(o[11]) > AQD2_CBD_CDF) {
+    *p = -qd->k2[did] * P * iC;
+    for (int i = 0; i < 3; i++) pv[i] = FS_S2(o, i) * iC;
+  } else {
+    *p = -qd->k2[did] * P * iC;
+    for (int i = 0; i < 3; i++) pv[i] = -(FS_S1(o, i) - P * o[9 + i]) * iC;
+  }
+  *p *= ce;
+  for (int i = 0; i < 3; i++) pv[i] *= ce;
+  return did;
+}
+
+int pv_t_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd)
+{
+  double complex pi, vi[3];
+  int did = pv_s_aqd2(p, pv, rt, type, qd);
+  if (did == 0) {
+    calc_apw_pv(&pi, vi, rt, &qd->pw);
+    *p += pi;
+    for (int l = 0; l < 3; l++) pv[l] += vi[l];
+  }
+  return did;
+}
+
+/* Boundary sums at (zeta_t, eta_t) of element t (1-based) of domain did
+ * (bem3_aw_qd2_field.c:299-492).  o = bemgpu_boundary_field's 9 values. */
+static void bd_sums(double o[9], double *rt, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  if (did < 0 || did > qd->MN || t < 1 || t > qd->bd.sb[did].Ne) {
+    printf("bem3_aw_qd2: boundary point of element %d in domain %d is out of range. Exit...\n", t, did);
+    exit(1);
+  }
+  if (type < 0 || type > 3) {
+    printf("bem3_aw_qd2: boundary rule type=%d is not available (0..3). Exit...\n", type);
+    exit(1);
+  }
+  bemgpu_ctx *c = ready_ctx(qd);
+  int t0 = t - 1;
+  double ze[2] = {zeta_t, eta_t};
+  gpu_check(c, bemgpu_boundary_field(c, did, type, 1, &t0, ze, o), "boundary field");
+  status_check(c, "boundary field");
+  aqd2_r_bd(rt, abs(qd->bd.sb[did].sid[t]), zeta_t, eta_t, &qd->bd);
+}
+
+void phi_s_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double o[9], rt[3];
+  bd_sums(o, rt, did, t, zeta_t, eta_t, type, qd);
+  *phi = (o[0] + I * o[1]) / (did == 0 ? 1.0 + o[8] : o[8]);
+}
+
+void phi_t_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double o[9], rt[3];
+  double complex pi, v[3];
+  bd_sums(o, rt, did, t, zeta_t, eta_t, type, qd);
+  *phi = (o[0] + I * o[1]) / (did == 0 ? 1.0 + o[8] : o[8]);
+  if (did == 0) {
+    calc_apw_pv(&pi, v, rt, &qd->pw);
+    *phi += -pi / qd->pw.wd.k2;
+  }
+}
+
+void phi_i_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double complex v[3];
+  double rt[3];
+  (void)type;
+  if (did == 0) {
+    aqd2_r_bd(rt, abs(qd->bd.sb[did].sid[t]), zeta_t, eta_t, &qd->bd);
+    calc_apw_pv(phi, v, rt, &qd->pw);
+    *phi /= -qd->pw.wd.k2;
+  } else
+    *phi = 0.0;
+}
+
+void pv_s_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double o[9], rt[3];
+  bd_sums(o, rt, did, t, zeta_t, eta_t, type, qd);
+  double cf = 1.0 / (did == 0 ? 1.0 + o[8] : o[8]);
+  *p = -(o[0] + I * o[1]) * cf * qd->k2[did];
+  for (int l = 0; l < 3; l++) pv[l] = (o[2 + 2 * l] + I * o[3 + 2 * l]) * cf;
+}
+
+void pv_t_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double o[9], rt[3];
+  double complex pi, vi[3];
+  bd_sums(o, rt, did, t, zeta_t, eta_t, type, qd);
+  double cf = 1.0 / (did == 0 ? 1.0 + o[8] : o[8]);
+  *p = -(o[0] + I * o[1]) * cf * qd->k2[did];
+  for (int l = 0; l < 3; l++) pv[l] = (o[2 + 2 * l] + I * o[3 + 2 * l]) * cf;
+  if (did == 0) {
+    calc_apw_pv(&pi, vi, rt, &qd->pw);
+    *p += pi;
+    for (int l = 0; l < 3; l++) pv[l] += vi[l];
+  }
+}
+
+void pv_i_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd)
+{
+  double rt[3];
+  (void)type;
+  if (did == 0) {
+    aqd2_r_bd(rt, abs(qd->bd.sb[did].sid[t]), zeta_t, eta_t, &qd->bd);
+    calc_apw_pv(p, pv, rt, &qd->pw);
+  } else {
+    *p = 0.0;
+    for (int i = 0; i < 3; i++) pv[i] = 0.0;
+  }
+}
 
 /* Solid-angle domain test (bem3_aw_qd2.c:130-183, 1148-1257): the sum of the
  * solid angles subtended by a domain's boundary is 4 pi inside, 0 outside. */

@@ -160,6 +160,12 @@ void aqd2_init_elem_const(BOUD *bd)
   aqd2_gauss_legendre(bd->xhi, bd->whi, GHN);
 }
 
+void aqd2_r_bd(double *r, int e, double zeta, double eta, BOUD *bd)
+{
+  double zh = bd->ed[e][3] == 0 ? 0.0 : zeta * eta;
+  for (int i = 0; i < 3; i++) r[i] = bd->cr[e][i][0] + bd->cr[e][i][1] * zeta + bd->cr[e][i][2] * eta + bd->cr[e][i][3] * zh;
+}
+
 /* bil_check_plane (d3qd2_elem.c:986): the twist vector cr[.][1] is
  * perpendicular to cw[.][2] only for plane elements. */
 int aqd2_elem_plane(BOUD *bd, int e)

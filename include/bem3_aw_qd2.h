@@ -130,6 +130,15 @@ int pv_s_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 
 int pv_t_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd);
 int pv_i_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 *qd);
 
+/* -- boundary values at parameter points of element t (1-based) of domain did
+ *    (bem3_aw_qd2_field.c:299-492) */
+void phi_s_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+void phi_t_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+void phi_i_bd_aqd2(double complex *phi, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+void pv_s_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+void pv_t_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+void pv_i_bd_aqd2(double complex *p, double complex *pv, int did, int t, double zeta_t, double eta_t, int type, AQD2 *qd);
+
 /* -- plane wave (aw_pw.h) */
 void read_data_apw(char *fname, Apw *pw);
 void print_data_apw(Apw *pw);

@@ -55,6 +55,8 @@ typedef struct bemgpu_problem {
   const double *xl, *wl; /* 12-point Gauss-Legendre nodes/weights on [-1,1] (BOUD xli/wli) */
   const double *xh, *wh; /* 64-point Gauss-Legendre nodes/weights (BOUD xhi/whi) */
   const unsigned char *plane; /* [Ne] 1 if the element is plane (bil_check_plane, d3qd2_elem.c:986) */
+  double pw[16];       /* incident plane wave: amplitude (re, im), rotation R[9], translation tv[3],
+                          k0, rho0 c0 (Apw, aw_pw.h:16-34; evaluated as calc_apw_pv) */
 } bemgpu_problem;
 
 typedef struct bemgpu_ctx bemgpu_ctx;
@@ -89,8 +91,32 @@ int bemgpu_get_solution(bemgpu_ctx *ctx, int d, double *P, double *dP, double *p
 int bemgpu_get_matrix(bemgpu_ctx *ctx, int d, int which, double *dst);
 
 /* Radiation force and torque about rc (force_FN_aqd2, bem3_aw_qd2_force.c:4).
- * type 0: 4-point rule on the node values. */
+ * type 0: 4-point rule on the node values (bil_force_4p); type != 0: the
+ * 9-point rule with the boundary values evaluated at the rule points
+ * (bil_force_9p + pv_t_bd_aqd2 with the 9-point coefficients). */
 int bemgpu_force(bemgpu_ctx *ctx, int type, const double *rc, double *F, double *N);
+
+/* Replace the boundary values of domain d (same layout as
+ * bemgpu_get_solution), e.g. after reading a .dat file, so that the force and
+ * field functions can run without a new solve. */
+int bemgpu_set_solution(bemgpu_ctx *ctx, int d, const double *P, const double *dP, const double *pv, const double *dpv);
+
+/* Field sums at n points r[n][3] of domain d, already reduced to the home
+ * lattice cell (pv_s_dbieq_aqd2 / pv_s_bieq_aqd2 / phi_s_aqd2,
+ * bem3_aw_qd2_field.c:3-297).  type: 0 4-point, 1 9-point, 2 12x12, 3 64x64
+ * rule.  out[n][18] = S0 (complex) = sum(G dP - H P), S1[3] (complex) its
+ * gradient with respect to r, F, dF[3], S2[3] (complex) = sum(G dpv - H pv);
+ * the caller applies the normalisation 1/(1+F) (domain 0) or 1/F. */
+int bemgpu_field(bemgpu_ctx *ctx, int d, int type, int n, const double *r, double *out);
+
+/* Boundary sums of domain d at parameter points ze[n][2] = (zeta, eta) of its
+ * elements t[n] (0-based index into domain d's element list; the reference's
+ * t - 1): out[n][9] = S0 (complex) = sum(G dP - H P), S2[3] (complex) =
+ * sum(G dpv - H pv), F (pv_s_bd_aqd2, bem3_aw_qd2_field.c:394-433, with
+ * q0_coef_bd for domain 0 and coef_bd for the others); the caller applies the
+ * normalisation.  type as bemgpu_field; the element itself always gets the
+ * singular polar rule. */
+int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t, const double *ze, double *out);
 
 /* Wait for all queued work of the context. */
 int bemgpu_sync(bemgpu_ctx *ctx);

@@ -177,3 +177,24 @@ void ref_load(AQD2 *qd, const char *pw, const char *per, const char *med, const 
   read_aqd2(6, argv, qd);
   initialize_aqd2(qd);
 }
+
+/* Coefficients CC[9] of source s (1-based index into domain did) at the
+ * boundary point (zeta, eta) of element t of the same domain, as the boundary
+ * field functions use them (q0_coef_bd / coef_bd, d3qd2_src/d3qd2_elem.c:684,
+ * :187).  out = 9 complex numbers. */
+void ref_bd_coef(AQD2 *qd, int did, int t, double zeta, double eta, int s, int type, double *out)
+{
+  double complex CC[9];
+  double rt[3];
+  int td = qd->bd.sb[did].sid[t], sd = qd->bd.sb[did].sid[s];
+  r_bd(rt, td, zeta, eta, &(qd->bd));
+  if (did == 0 && qd->bd.ps == 1) q0_coef_bd(CC, rt, td, zeta, eta, sd, (double complex)qd->k0[did], type, &(qd->bd));
+  else coef_bd(CC, rt, td, zeta, eta, sd, (double complex)qd->k0[did], type, &(qd->bd));
+  for (int i = 0; i < 9; i++) { out[2 * i] = creal(CC[i]); out[2 * i + 1] = cimag(CC[i]); }
+}
+
+/* Point of element t (1-based index into domain did) at (zeta, eta) (r_bd, d3qd2_src/d3qd2_elem.c:18). */
+void ref_r_bd(AQD2 *qd, int did, int t, double zeta, double eta, double *r)
+{
+  r_bd(r, qd->bd.sb[did].sid[t], zeta, eta, &(qd->bd));
+}

@@ -116,6 +116,35 @@ class RefCase:
         lib().force_FN_aqd2(_p(F), _p(N), _p(rc), type_, self.qd)
         return F, N
 
+    def field(self, fn, rt, type_):
+        """Reference field function fn ("pv_t", "pv_s", "phi_s", "p_t", ...) at point rt.
+        Returns (domain id, p or phi, pv or None)."""
+        L = lib()
+        rt = np.ascontiguousarray(rt, dtype=np.float64)
+        a = np.zeros(2)
+        v = np.zeros(6)
+        f = getattr(L, fn + "_aqd2")
+        f.restype = ctypes.c_int
+        if fn.startswith("pv"):
+            did = f(_p(a), _p(v), _p(rt), type_, self.qd)
+            return did, complex(a[0], a[1]), v.view(np.complex128).copy()
+        did = f(_p(a), _p(rt), type_, self.qd)
+        return did, complex(a[0], a[1]), None
+
+    def boundary(self, fn, did, t, zeta, eta, type_):
+        """Reference boundary function fn ("pv_t_bd", "phi_s_bd", ...) at (zeta, eta) of
+        element t (1-based) of domain did.  Returns (p or phi, pv or None)."""
+        L = lib()
+        a = np.zeros(2)
+        v = np.zeros(6)
+        f = getattr(L, fn + "_aqd2")
+        f.restype = None
+        if fn.startswith("pv"):
+            f(_p(a), _p(v), did, t, ctypes.c_double(zeta), ctypes.c_double(eta), type_, self.qd)
+            return complex(a[0], a[1]), v.view(np.complex128).copy()
+        f(_p(a), did, t, ctypes.c_double(zeta), ctypes.c_double(eta), type_, self.qd)
+        return complex(a[0], a[1]), None
+
     def assemble_rows(self, did, t0, t1):
         """Time the reference's own assembly loop on collocation elements [t0, t1) (1-based)."""
         return lib().ref_assemble_rows(self.qd, did, t0, t1)

@@ -11,8 +11,17 @@ outputs as compressed .npz files:
                  216-quad configuration's media, lattice and incidence:
                  coefficient matrices of both domains (the reference's temporary
                  files), P, dP, pv, dpv, force and torque (type 0)
+  qpgf_plane.npz d3hm_qpgf_d2_v1 on points of the lattice plane (z = 0
+                 exactly), where the reference's spectral rows stop on an
+                 identically zero z-derivative sum
+  fields24.npz   on the same solved system: force and torque with the
+                 9-point rule (type 1), field values (phi_s, p_t, pv_s, pv_t)
+                 at points in the home cell, in shifted lattice cells, inside
+                 the sphere and next to the boundary with rules 0-3, and
+                 boundary values (phi_s_bd, pv_t_bd) on elements of both domains
 
-Usage: python tests/golden/make_golden.py  (needs oracle/_ref; about a minute)
+Usage: python tests/golden/make_golden.py [fields|plane]  (needs oracle/_ref; a
+few minutes; "fields" / "plane" regenerate fields24.npz / qpgf_plane.npz only)
 """
 import math
 import os
@@ -46,8 +55,75 @@ def faddeeva_points(rng):
     return np.array(pts)
 
 
+FIELD_POINTS = [  # (point, rule type)
+    ((0.1, 0.2, 0.45), 1), ((0.35, -0.3, -0.1), 1), ((0.0, 0.0, 1.2), 1), ((1.7, -0.9, 0.2), 1),
+    ((-0.75, 2.45, -0.5), 1), ((0.05, -0.1, 0.1), 1), ((0.0, 0.0, 0.305), 1), ((0.0, 0.0, 0.295), 1),
+    ((0.12, 0.05, 0.42), 0), ((0.12, 0.05, 0.42), 2), ((0.12, 0.05, 0.42), 3), ((-0.02, 0.08, -0.15), 2),
+    ((0.31, 0.02, 0.0), 2), ((0.2, 0.3, -0.38), 3),
+]
+BOUNDARY_POINTS = [  # (domain, element 1-based, zeta, eta, rule type)
+    (0, 1, 0.3, -0.5, 1), (0, 7, 0.0, 0.0, 1), (0, 18, -0.7745966692414834, 0.7745966692414834, 1),
+    (0, 3, 0.5, 0.25, 2), (0, 11, -0.2, 0.6, 0), (1, 2, 0.3, -0.5, 1), (1, 9, 0.0, 0.0, 2), (1, 20, -0.6, -0.1, 3),
+]
+
+
+def make_plane():
+    rng = np.random.default_rng(20241204)
+    out = {}
+    for name, qp in [("square", qp_of(2 * math.pi, 20.0, 30.0, (0.8, 0.0), (0.0, 0.8))),
+                     ("oblique", qp_of(2 * math.pi, 35.0, 15.0, (1.0, 0.0), (0.3, 0.9)))]:
+        r = np.column_stack([rng.uniform(-0.9, 0.9, (200, 2)), np.zeros(200)])
+        G, dG, ret = refwrap.qpgf(qp, r, 0)
+        out.update({name + "_qp": qp, name + "_r": r, name + "_G": G, name + "_dG": dG, name + "_ret": ret})
+    np.savez_compressed(os.path.join(OUT, "qpgf_plane.npz"), **out)
+
+
+def make_fields(case):
+    out = {}
+    out["F1"], out["N1"] = case.force(1)
+    out["F1c"], out["N1c"] = case.force(1, (0.05, -0.02, 0.1))
+    pts = np.array([p for p, _ in FIELD_POINTS])
+    types = np.array([t for _, t in FIELD_POINTS], np.int32)
+    res = {k: [] for k in ["did", "phi_s", "p_t", "pv_s_p", "pv_s_v", "pv_t_p", "pv_t_v"]}
+    for p, t in FIELD_POINTS:
+        did, phi, _ = case.field("phi_s", p, t)
+        res["did"].append(did)
+        res["phi_s"].append(phi)
+        res["p_t"].append(case.field("p_t", p, t)[1])
+        _, a, v = case.field("pv_s", p, t)
+        res["pv_s_p"].append(a)
+        res["pv_s_v"].append(v)
+        _, a, v = case.field("pv_t", p, t)
+        res["pv_t_p"].append(a)
+        res["pv_t_v"].append(v)
+    out["pts"], out["types"] = pts, types
+    out.update({k: np.array(v) for k, v in res.items()})
+    bd = np.array([b[:4] for b in BOUNDARY_POINTS], np.float64)
+    btypes = np.array([b[4] for b in BOUNDARY_POINTS], np.int32)
+    phib, pb, vb = [], [], []
+    for did, t, z, e, ty in BOUNDARY_POINTS:
+        phib.append(case.boundary("phi_s_bd", did, t, z, e, ty)[0])
+        a, v = case.boundary("pv_t_bd", did, t, z, e, ty)
+        pb.append(a)
+        vb.append(v)
+    out.update(bd=bd, btypes=btypes, phi_s_bd=np.array(phib), pv_t_bd_p=np.array(pb), pv_t_bd_v=np.array(vb))
+    np.savez_compressed(os.path.join(OUT, "fields24.npz"), **out)
+
+
 def main():
     rng = np.random.default_rng(20241203)
+    if sys.argv[1:] == ["plane"]:
+        make_plane()
+        print("qpgf_plane.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["fields"]:
+        tmp = tempfile.mkdtemp(prefix="golden_")
+        files = meshgen.write_inputs(tmp, **meshgen.CONFIGS["sphere24"])
+        case = refwrap.RefCase(*files)
+        case.solve(tmp)
+        make_fields(case)
+        print("fields24.npz written to", OUT)
+        return
     # Faddeeva
     z = faddeeva_points(rng)
     np.savez_compressed(os.path.join(OUT, "faddeeva.npz"), z=z, w=refwrap.faddeeva_w(z))
@@ -66,6 +142,7 @@ def main():
             out["%s_%s_dG" % (name, tag)] = dG
             out["%s_%s_ret" % (name, tag)] = ret
     np.savez_compressed(os.path.join(OUT, "qpgf.npz"), **out)
+    make_plane()
     # full solve, 24 quads
     tmp = tempfile.mkdtemp(prefix="golden_")
     files = meshgen.write_inputs(tmp, **meshgen.CONFIGS["sphere24"])
@@ -78,6 +155,7 @@ def main():
     F0, N0 = case.force(0)
     keep = {k: v for k, v in mats.items() if not (k.startswith("dG0") or k.startswith("dH0"))}
     np.savez_compressed(os.path.join(OUT, "sphere24.npz"), F0=F0, N0=N0, **keep, **sol)
+    make_fields(case)
     print("fixtures written to", OUT)
 
 
