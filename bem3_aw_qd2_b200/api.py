@@ -53,6 +53,9 @@ def libs():
         g.bemgpu_set_profiling.argtypes = [vp, ctypes.c_int]
         g.bemgpu_phase_times.argtypes = [vp, _d, ctypes.c_int]
         g.bemgpu_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+        g.bemgpu_set_precision.argtypes = [vp, ctypes.c_int]
+        g.bemgpu_get_precision.argtypes = [vp]
+        g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
         h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
         for name in ("print_aqd2", "initialize_aqd2", "finalize_aqd2", "solve_bieq_aqd2"):
             getattr(h, name).argtypes = [vp]
@@ -174,6 +177,22 @@ class Case:
     def run_device(self):
         """bemgpu_run on the resident problem (inputs already on the device)."""
         self._check(libs()[1].bemgpu_run(self.ctx), "bemgpu_run")
+
+    def set_precision(self, mode):
+        """0 FP64 LU; 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates with FP64 refinement."""
+        self._check(libs()[1].bemgpu_set_precision(self.ctx, int(mode)), "set_precision")
+
+    def precision(self):
+        """The precision mode in effect (see bemgpu.h)."""
+        return libs()[1].bemgpu_get_precision(self.ctx)
+
+    def solve_stats(self):
+        """(iterations, final relative correction, fell back to FP64) per dense system of the last solve."""
+        it = np.zeros(16, np.int32)
+        rc = np.zeros(16)
+        fb = np.zeros(16, np.int32)
+        k = libs()[1].bemgpu_solve_stats(self.ctx, it.ctypes.data_as(_i), _p(rc), fb.ctypes.data_as(_i), 16)
+        return it[:k], rc[:k], fb[:k]
 
     def sync(self):
         self._check(libs()[1].bemgpu_sync(self.ctx), "bemgpu_sync")

@@ -11,6 +11,7 @@
 #include "bem_kernels.h"
 #include "bem_solve.h"
 #include "bem_lattice.h"
+#include "bem_mixed.h"
 
 #define BEMGPU_MAXDOM 8
 
@@ -61,6 +62,13 @@ struct bemgpu_ctx {
   // optional per-phase timing: 6 events per domain (0, 1), then 5 for the solve
   bool prof = false;
   cudaEvent_t ev[17] = {};
+  // precision of the dense solves: 0 FP64 LU; BEM_MIXED_* complex FP32 LU + FP64 refinement
+  int precision = 0;
+  bool mx_ready = false;
+  bem_mixed mx;
+  double *b0 = nullptr, *B3s = nullptr;  // saved right-hand sides (FP64 fallback)
+  int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
+  double st_corr[BEMGPU_MAXDOM + 1] = {};
 };
 
 static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
@@ -105,7 +113,7 @@ static void free_problem(bemgpu_ctx *c) {
     dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
-  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab);
+  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->b0); dfree(c->B3s);
   dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
   c->ntgt = 0;
   if (c->dwork) cudaFree(c->dwork);
@@ -151,6 +159,7 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   free_problem(c);
   dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
   dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
+  if (c->mx_ready) bem_mixed_free(&c->mx);
   for (int i = 0; i < 17; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->params) cusolverDnDestroyParams(c->params);
@@ -375,6 +384,74 @@ static int check_info(bemgpu_ctx *c, const char *what) {
   return 0;
 }
 
+// Solve the row-major FP64 system M X = B (n x nrhs, column-major) in the
+// context's precision.  Mixed: FP32 LU + FP64 refinement; a system whose
+// refinement does not reach 1e-12 (or that has a zero FP32 pivot) is solved
+// again by the FP64 LU from the saved right-hand side.  M_scratch: M may be
+// overwritten by the FP64 factors.  slot: statistics entry.
+static int dense_solve(bemgpu_ctx *c, double *M, int64_t n, int64_t nrhs, double *B, double *Bsave, int slot,
+                       bool M_scratch, const char *what) {
+  c->st_iters[slot] = 0;
+  c->st_corr[slot] = 0.0;
+  c->st_fallback[slot] = 0;
+  bool fp64 = c->precision == 0;
+  if (!fp64) {
+    CK(cudaMemcpyAsync(Bsave, B, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+    if (bem_mixed_factor(&c->mx, M, (int)n, c->stream)) {
+      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mx.err);
+      return -1;
+    }
+    int it = 0;
+    double rc = 1.0;
+    const bool zero_pivot = (bem_mixed_status(&c->mx, c->stream) & 0x20u) != 0;
+    if (!zero_pivot && bem_mixed_solve(&c->mx, M, (int)n, (int)nrhs, B, 30, 4.0 * 1.1102230246251565e-16, &it, &rc, c->stream)) {
+      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mx.err);
+      return -1;
+    }
+    c->st_iters[slot] = it;
+    c->st_corr[slot] = rc;
+    if (zero_pivot || !(rc <= 1e-12)) {
+      c->st_fallback[slot] = 1;
+      CK(cudaMemcpyAsync(B, Bsave, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+      fp64 = true;
+    }
+  }
+  if (fp64) {
+    double *F = M;
+    if (!M_scratch) {
+      CK(cudaMemcpyAsync(c->W, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+      F = c->W;
+    }
+    if (lu_factor(c, F, n, what)) return -1;
+    if (check_info(c, what)) return -3;
+    if (lu_solve(c, F, n, nrhs, B, what)) return -1;
+  }
+  return 0;
+}
+
+extern "C" int bemgpu_set_precision(bemgpu_ctx *c, int mode) {
+  if (mode < 0 || mode > BEM_MIXED_BF16) { snprintf(c->err, sizeof(c->err), "precision mode %d (0..4)", mode); return -2; }
+  if (mode != 0 && !c->mx_ready) {
+    if (bem_mixed_init(&c->mx, mode, c->stream)) { snprintf(c->err, sizeof(c->err), "cuBLAS set-up failed"); return -1; }
+    c->mx_ready = true;
+  }
+  if (c->mx_ready) c->mx.mode = mode;
+  c->precision = mode;
+  return 0;
+}
+
+extern "C" int bemgpu_get_precision(bemgpu_ctx *c) { return c->precision == 0 ? 0 : c->mx.mode; }
+
+extern "C" int bemgpu_solve_stats(bemgpu_ctx *c, int *iters, double *rel_corr, int *fallback, int max) {
+  int k = 0;
+  for (; k < c->st_n && k < max; ++k) {
+    if (iters) iters[k] = c->st_iters[k];
+    if (rel_corr) rel_corr[k] = c->st_corr[k];
+    if (fallback) fallback[k] = c->st_fallback[k];
+  }
+  return k;
+}
+
 extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   const size_t n = c->n;
@@ -384,9 +461,15 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], c->A, c->b, c->stream)) return fail(c, "gather", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[13], c->stream);
-  if (lu_factor(c, c->A, (int64_t)n, "global LU")) return -1;
-  if (check_info(c, "global LU")) return -3;
-  if (lu_solve(c, c->A, (int64_t)n, 1, c->b, "global solve")) return -1;
+  if (c->precision != 0 && !c->b0) {
+    CK(dalloc(&c->b0, 2 * n), "b copy");
+    CK(dalloc(&c->B3s, 6 * (size_t)c->NN), "B3 copy");
+  }
+  c->st_n = c->MN + 2;
+  {
+    const int rc = dense_solve(c, c->A, (int64_t)n, 1, c->b, c->b0, 0, true, "global LU");
+    if (rc) return rc;
+  }
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_store(&c->sys, d, c->b, c->P[d], c->dP[d], c->stream)) return fail(c, "store", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[14], c->stream);
@@ -403,10 +486,10 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
     if (Nd == 0) continue;
     if (bem_launch_dpv_rhs((int)Nd, c->H[d], c->pv[d], c->B3, c->stream)) return fail(c, "dpv rhs", cudaGetLastError());
-    CK(cudaMemcpyAsync(c->W, c->G[d], 2 * Nd * Nd * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "G copy");
-    if (lu_factor(c, c->W, Nd, "dpv LU")) return -1;
-    if (check_info(c, "dpv LU")) return -3;
-    if (lu_solve(c, c->W, Nd, 3, c->B3, "dpv solve")) return -1;
+    {
+      const int rc = dense_solve(c, c->G[d], Nd, 3, c->B3, c->B3s, 1 + d, false, "dpv LU");
+      if (rc) return rc;
+    }
     if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
   }
   if (c->prof) cudaEventRecord(c->ev[16], c->stream);

@@ -13,12 +13,21 @@
 #define AQD2_MAXCTX 64
 static struct { AQD2 *qd; bemgpu_ctx *ctx; } g_tab[AQD2_MAXCTX];
 static int g_device = 0;
+static int g_precision = -1; /* -1: from the environment (AQD2_PRECISION), else 0 */
 static double g_timing[4];
 static int g_verbose = 1;
 
 void aqd2_set_verbose(int on) { g_verbose = on; }
 
 void aqd2_set_device(int device) { g_device = device; }
+void aqd2_set_precision(int mode) { g_precision = mode; }
+
+static int precision_mode(void)
+{
+  if (g_precision >= 0) return g_precision;
+  const char *e = getenv("AQD2_PRECISION");
+  return e ? atoi(e) : 0;
+}
 void aqd2_last_timing(double *t4) { for (int i = 0; i < 4; i++) t4[i] = g_timing[i]; }
 
 static bemgpu_ctx *ctx_for(AQD2 *qd, int create)
@@ -31,6 +40,10 @@ static bemgpu_ctx *ctx_for(AQD2 *qd, int create)
       bemgpu_ctx *c = NULL;
       if (bemgpu_create(g_device, NULL, &c) != 0) {
         printf("bem3_aw_qd2: failed to create a CUDA context on device %d. Exit...\n", g_device);
+        exit(1);
+      }
+      if (bemgpu_set_precision(c, precision_mode()) != 0) {
+        printf("bem3_aw_qd2: %s. Exit...\n", bemgpu_error(c));
         exit(1);
       }
       g_tab[i].qd = qd;

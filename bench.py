@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--workload", default="sphere216")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-mode", type=int, default=3,
+                    help="precision of the mixed form: 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates; 0: skip it")
     return ap.parse_args()
 
 
@@ -190,6 +192,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    # load the library (and the CUDA 12.9 cuBLAS it links) before torch brings its own
+    from bem3_aw_qd2_b200 import api
+    api.libs()
     import torch
     torch.cuda.set_device(local)
     if world > 1:
@@ -248,6 +253,47 @@ def main():
     cnt = (api.ctypes.c_ulonglong * 6)()
     g.bemgpu_work_counters(ctx, cnt, 1)
     total_ms = sum(times)
+    F_fp64, N_fp64 = F.copy(), N.copy()
+    mixed = None
+    if args.mixed_mode:
+        # the mixed-precision form on the same workload: FP32 LU (tensor-core
+        # trailing updates) + FP64 refinement, force checked against FP64
+        case.set_precision(args.mixed_mode)
+        for _ in range(args.warmup):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            device_step()
+        torch.cuda.synchronize()
+        mt, mph = [], []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            device_step()
+            e1.record(stream)
+            e1.synchronize()
+            mt.append(e0.elapsed_time(e1))
+            ph = (api.ctypes.c_double * 16)()
+            k = g.bemgpu_phase_times(ctx, ph, 16)
+            mph.append([ph[i] for i in range(k)])
+        it, rcorr, fb = case.solve_stats()
+        eff_mode = case.precision()
+        F1m, N1m = case.force(1)
+        case.set_precision(0)
+        case.run_device()
+        F1d, N1d = case.force(1)
+        mp = np.array(mph).mean(axis=0)
+        mixed = {"value": args.steps / (sum(mt) / 1000.0), "unit": "solves/s",
+                 "mode": {1: "FP32", 2: "TF32", 3: "BF16x9", 4: "BF16"}[eff_mode] + " LU updates + FP64 refinement",
+                 "latency_ms": {"p50": float(np.percentile(mt, 50)), "p99": float(np.percentile(mt, 99))},
+                 "force_rel_err_vs_fp64": {"type0": float(np.linalg.norm(F - F_fp64) / np.linalg.norm(F_fp64)),
+                                           "type1": float(np.linalg.norm(F1m - F1d) / np.linalg.norm(F1d))},
+                 "refine_iters": [int(x) for x in it], "refine_rel_corr": [float(x) for x in rcorr],
+                 "fp64_fallbacks": int(np.sum(fb)),
+                 "lu_solve_ms": float(mp[11]) if len(mp) > 11 else None,
+                 "dpv_solves_ms": float(mp[13]) if len(mp) > 13 else None}
     # e2e: the public drop-in API with host buffers
     e2e_times = []
     for _ in range(args.steps):
@@ -294,6 +340,7 @@ def main():
                      "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
                      "mean_terms_per_point": cnt[0] / max(cnt[3], 1)},
         "clocks": clk,
+        "mixed": mixed,
         "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -118,6 +118,36 @@ int bemgpu_field(bemgpu_ctx *ctx, int d, int type, int n, const double *r, doubl
  * singular polar rule. */
 int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t, const double *ze, double *out);
 
+/* Precision of the dense solves (the global system and the per-domain dpv
+ * systems; the reference uses FP64 PARDISO and LAPACKE_zgesv,
+ * d3qd2_mkl_solver.c:18-148, bem3_aw_qd2_solve_bieq.c:533-653).  Assembly,
+ * residuals and the force integral stay FP64 in every mode.
+ *   0 BEMGPU_FP64      FP64 LU (default; the drop-in)
+ *   1 BEMGPU_MIXED_FP32   complex FP32 LU, FP32 CUDA-core GEMM updates
+ *   2 BEMGPU_MIXED_TF32   complex FP32 LU, TF32 tensor-core GEMM updates
+ *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, GEMM updates as three BF16 products
+ *                         on the tensor cores (FP32-accurate)
+ *   4 BEMGPU_MIXED_BF16   complex FP32 LU, BF16 tensor-core GEMM updates
+ * Modes 1-4 refine in FP64 against the FP64 matrix until the correction is
+ * below 1e-15 of the solution; a system that does not get below 1e-12 is
+ * solved again in FP64 (reported by bemgpu_solve_stats). */
+#define BEMGPU_FP64 0
+#define BEMGPU_MIXED_FP32 1
+#define BEMGPU_MIXED_TF32 2
+#define BEMGPU_MIXED_BF16X9 3
+#define BEMGPU_MIXED_BF16 4
+int bemgpu_set_precision(bemgpu_ctx *ctx, int mode);
+/* The mode in effect: BF16X9 needs cuBLAS 12.9 or later in the process and
+ * becomes TF32 with an older one (for example when another library loaded
+ * its own cuBLAS first). */
+int bemgpu_get_precision(bemgpu_ctx *ctx);
+
+/* Refinement record of the last bemgpu_solve, one entry per dense system
+ * (0: global system, 1 + d: dpv system of domain d): refinement steps, final
+ * max|correction| / max|solution|, 1 if solved again in FP64.  Returns the
+ * number of entries written (at most max). */
+int bemgpu_solve_stats(bemgpu_ctx *ctx, int *iters, double *rel_corr, int *fallback, int max);
+
 /* Wait for all queued work of the context. */
 int bemgpu_sync(bemgpu_ctx *ctx);
 

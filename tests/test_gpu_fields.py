@@ -120,3 +120,29 @@ def test_dat_file_postprocessing(solved):
     assert did == g["did"][0]
     assert abs(a - g["pv_t_p"][0]) <= TOL * np.max(np.abs(g["pv_t_p"]))
     other.close()
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+def test_mixed_precision_matches_fp64(solved, mode):
+    """Complex FP32 LU (FP32 / TF32 / BF16x9 / BF16 trailing updates) with FP64
+    refinement: surface values to 1e-11 of the FP64 solve, force and torque of
+    both rules to 1e-8 (the radiation-force tolerance of the mixed form)."""
+    case, g, _ = solved
+    case.set_precision(0)
+    case.run_device()
+    ref = [case.solution(d, 24) for d in (0, 1)]
+    F0, N0 = case.force(0)
+    F1, N1 = case.force(1)
+    case.set_precision(mode)
+    case.run_device()
+    it, rc, fb = case.solve_stats()
+    assert len(it) == 3 and np.all(fb == 0) and np.all(it >= 1) and np.all(rc <= 1e-12)
+    for d in (0, 1):
+        for a, b in zip(case.solution(d, 24), ref[d]):
+            assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(b))
+    for t, (Fr, Nr) in ((0, (F0, N0)), (1, (F1, N1))):
+        F, N = case.force(t)
+        assert np.linalg.norm(F - Fr) <= 1e-8 * np.linalg.norm(Fr)
+        assert np.linalg.norm(N - Nr) <= 1e-8 * np.linalg.norm(Fr) * 0.3
+    case.set_precision(0)
+    case.run_device()
