@@ -67,8 +67,33 @@ def libs():
         h.aqd2_last_timing.argtypes = [_d]
         h.aqd2_set_device.argtypes = [ctypes.c_int]
         h.aqd2_set_verbose.argtypes = [ctypes.c_int]
+        h.aqd2_problem_build.argtypes = [vp, ctypes.POINTER(Problem)]
+        h.aqd2_problem_free.argtypes = [ctypes.POINTER(Problem)]
+        g.bemgpu_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(vp)]
+        g.bemgpu_server_submit.argtypes = [vp, ctypes.POINTER(Problem), ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
+                                           _d, ctypes.c_longlong]
+        g.bemgpu_server_poll.argtypes = [vp, ctypes.POINTER(Result), ctypes.c_int, ctypes.c_int]
+        g.bemgpu_server_stats.argtypes = [vp, _d]
+        g.bemgpu_server_destroy.argtypes = [vp]
         _host, _gpu = h, g
     return _host, _gpu
+
+
+class Problem(ctypes.Structure):
+    """bemgpu_problem (include/bemgpu.h)."""
+    _fields_ = [("Ne", ctypes.c_int), ("NN", ctypes.c_int), ("MN", ctypes.c_int), ("ps", ctypes.c_int),
+                ("qp", ctypes.c_double * 8)] + \
+               [(n, ctypes.c_void_p) for n in ("cr", "cw", "ren", "wen", "npe", "eni", "md", "sd", "dom_ne", "sid",
+                                              "k0", "k2", "rho0", "c0", "Pi", "dPi", "p_inc", "v_inc", "xl", "wl",
+                                              "xh", "wh", "plane")] + \
+               [("pw", ctypes.c_double * 16)]
+
+
+class Result(ctypes.Structure):
+    """bemgpu_result (include/bemgpu.h)."""
+    _fields_ = [("id", ctypes.c_longlong), ("status", ctypes.c_int), ("reused", ctypes.c_int),
+                ("F", ctypes.c_double * 3), ("N", ctypes.c_double * 3), ("queue_ms", ctypes.c_double),
+                ("service_ms", ctypes.c_double), ("error", ctypes.c_char * 160)]
 
 
 def _p(a):
@@ -158,6 +183,17 @@ class Case:
         f.argtypes = [_d] + ints
         f(_p(a), did, t, zeta, eta, type, self.qd)
         return complex(a[0], a[1]), None
+
+    def problem(self):
+        """The initialised problem as a bemgpu_problem with library-owned host arrays
+        (aqd2_problem_build); release with free_problem."""
+        pr = Problem()
+        libs()[0].aqd2_problem_build(self.qd, ctypes.byref(pr))
+        return pr
+
+    @staticmethod
+    def free_problem(pr):
+        libs()[0].aqd2_problem_free(ctypes.byref(pr))
 
     def dat_write(self, path):
         libs()[0].dat_write_aqd2(path.encode(), self.qd)
@@ -257,3 +293,44 @@ def qpgf(qp, r):
     if rc != 0:
         raise RuntimeError("bemgpu_qpgf failed")
     return G, dG, ret
+
+
+class Server:
+    """The request server of the C ABI (bemgpu_server_*): continuous batching,
+    factorisation reuse by key, admission by a device-memory budget."""
+
+    def __init__(self, device=0, hbm_budget=64 << 30, slots=4):
+        _, g = libs()
+        self.g = g
+        self.h = ctypes.c_void_p()
+        if g.bemgpu_server_create(device, hbm_budget, slots, ctypes.byref(self.h)) != 0:
+            raise RuntimeError("bemgpu_server_create failed")
+
+    def submit(self, problem, key, rid, precision=0, force_type=0, rc=(0.0, 0.0, 0.0)):
+        rc = np.ascontiguousarray(rc, dtype=np.float64)
+        r = self.g.bemgpu_server_submit(self.h, ctypes.byref(problem), key & 0xFFFFFFFFFFFFFFFF, precision, force_type,
+                                        _p(rc), rid)
+        if r != 0:
+            raise RuntimeError("request %d not admissible (%d)" % (rid, r))
+
+    def poll(self, max_results=64, timeout_ms=100):
+        buf = (Result * max_results)()
+        k = self.g.bemgpu_server_poll(self.h, buf, max_results, timeout_ms)
+        return [buf[i] for i in range(k)]
+
+    def stats(self):
+        out = np.zeros(8)
+        self.g.bemgpu_server_stats(self.h, _p(out))
+        keys = ["submitted", "completed", "reused", "running", "queued", "bytes_resident", "bytes_peak", "evictions"]
+        return dict(zip(keys, out.tolist()))
+
+    def close(self):
+        if self.h:
+            self.g.bemgpu_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -38,7 +38,7 @@ struct bemgpu_ctx {
   double *P[BEMGPU_MAXDOM] = {}, *dP[BEMGPU_MAXDOM] = {}, *pv[BEMGPU_MAXDOM] = {}, *dpv[BEMGPU_MAXDOM] = {};
   bem_scratch scr = {};
   // solve work
-  double *A = nullptr, *b = nullptr, *tpv = nullptr, *W = nullptr, *B3 = nullptr;
+  double *A = nullptr, *b = nullptr, *tpv = nullptr, *B3 = nullptr;
   int64_t *ipiv = nullptr;
   int *info = nullptr;
   void *dwork = nullptr;
@@ -64,8 +64,13 @@ struct bemgpu_ctx {
   cudaEvent_t ev[17] = {};
   // precision of the dense solves: 0 FP64 LU; BEM_MIXED_* complex FP32 LU + FP64 refinement
   int precision = 0;
-  bool mx_ready = false;
-  bem_mixed mx;
+  bem_mixed mxs[BEMGPU_MAXDOM + 1];  // FP32 factors per dense system (0 global, 1 + d dpv of domain d)
+  bool mx_ready[BEMGPU_MAXDOM + 1] = {};
+  // FP64 factors: the global system in A (ipiv), domain d's dpv system in Wd[d] (ipd[d])
+  double *Wd[BEMGPU_MAXDOM] = {};
+  int64_t *ipd[BEMGPU_MAXDOM] = {};
+  bool fac_fp64[BEMGPU_MAXDOM + 1] = {};
+  bool factored = false;  // factors of the current matrices are held (bemgpu_solve_rhs may run)
   double *b0 = nullptr, *B3s = nullptr;  // saved right-hand sides (FP64 fallback)
   int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
   double st_corr[BEMGPU_MAXDOM + 1] = {};
@@ -113,7 +118,9 @@ static void free_problem(bemgpu_ctx *c) {
     dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
-  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->W); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->b0); dfree(c->B3s);
+  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->b0); dfree(c->B3s);
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); }
+  c->factored = false;
   dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
   c->ntgt = 0;
   if (c->dwork) cudaFree(c->dwork);
@@ -159,7 +166,8 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   free_problem(c);
   dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
   dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
-  if (c->mx_ready) bem_mixed_free(&c->mx);
+  for (int i = 0; i <= BEMGPU_MAXDOM; ++i)
+    if (c->mx_ready[i]) { bem_mixed_free(&c->mxs[i]); c->mx_ready[i] = false; }
   for (int i = 0; i < 17; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->params) cusolverDnDestroyParams(c->params);
@@ -315,7 +323,11 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   CK(dalloc(&c->A, 2 * n * n), "A");
   CK(dalloc(&c->b, 2 * n), "b");
   CK(dalloc(&c->tpv, 6 * (size_t)c->NN), "tpv");
-  CK(dalloc(&c->W, 2 * (size_t)maxN * maxN), "W");
+  for (int d = 0; d < nd; ++d) {
+    const size_t N = 4 * (size_t)c->dom_ne[d];
+    CK(dalloc(&c->Wd[d], 2 * N * N), "dpv factors");
+    CK(dalloc(&c->ipd[d], N), "dpv pivots");
+  }
   CK(dalloc(&c->B3, 6 * (size_t)maxN), "B3");
   CK(dalloc(&c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "status");
@@ -335,7 +347,15 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   return 0;
 }
 
+extern "C" int bemgpu_unload(bemgpu_ctx *c) {
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_problem(c);
+  return 0;
+}
+
 extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
+  c->factored = false;
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   for (int d = 0; d <= c->MN; ++d) {
     bem_dom_dev D;
@@ -353,26 +373,6 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
 
 // LU factorisation of the row-major n x n complex matrix M in place; cuSOLVER
 // sees the column-major transpose, so solves below use op = T.
-static int lu_factor(bemgpu_ctx *c, double *M, int64_t n, const char *what) {
-  size_t dsz = 0, hsz = 0;
-  CKS(cusolverDnXgetrf_bufferSize(c->solver, c->params, n, n, CUDA_C_64F, M, n, CUDA_C_64F, &dsz, &hsz), what);
-  if (dsz > c->dwork_sz) {
-    if (c->dwork) cudaFree(c->dwork);
-    CK(cudaMalloc(&c->dwork, dsz), what);
-    c->dwork_sz = dsz;
-  }
-  if (hsz > c->hwork.size()) c->hwork.resize(hsz);
-  CKS(cusolverDnXgetrf(c->solver, c->params, n, n, CUDA_C_64F, M, n, c->ipiv, CUDA_C_64F, c->dwork, c->dwork_sz,
-                       hsz ? c->hwork.data() : nullptr, hsz, c->info),
-      what);
-  return 0;
-}
-
-static int lu_solve(bemgpu_ctx *c, const double *M, int64_t n, int64_t nrhs, double *B, const char *what) {
-  CKS(cusolverDnXgetrs(c->solver, c->params, CUBLAS_OP_T, n, nrhs, CUDA_C_64F, M, n, c->ipiv, CUDA_C_64F, B, n, c->info), what);
-  return 0;
-}
-
 static int check_info(bemgpu_ctx *c, const char *what) {
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->info, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
@@ -384,63 +384,90 @@ static int check_info(bemgpu_ctx *c, const char *what) {
   return 0;
 }
 
-// Solve the row-major FP64 system M X = B (n x nrhs, column-major) in the
-// context's precision.  Mixed: FP32 LU + FP64 refinement; a system whose
-// refinement does not reach 1e-12 (or that has a zero FP32 pivot) is solved
-// again by the FP64 LU from the saved right-hand side.  M_scratch: M may be
-// overwritten by the FP64 factors.  slot: statistics entry.
-static int dense_solve(bemgpu_ctx *c, double *M, int64_t n, int64_t nrhs, double *B, double *Bsave, int slot,
-                       bool M_scratch, const char *what) {
+// Dense systems M X = B with M row-major FP64 (n x n), B column-major (n x nrhs).
+// slot 0 is the global system (factors in place of A), slot 1 + d the dpv
+// system of domain d (M = G[d], FP64 factors in Wd[d]).  Mixed precision: FP32
+// factors + FP64 refinement against M, which stays intact; a system with a
+// zero FP32 pivot, or whose refinement does not reach 1e-12, switches to FP64
+// factors (then kept for later right-hand sides).
+static int dense_factor_fp64(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what) {
+  double *F = slot == 0 ? M : c->Wd[slot - 1];
+  int64_t *ip = slot == 0 ? c->ipiv : c->ipd[slot - 1];
+  if (F != M) CK(cudaMemcpyAsync(F, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+  size_t dsz = 0, hsz = 0;
+  CKS(cusolverDnXgetrf_bufferSize(c->solver, c->params, n, n, CUDA_C_64F, F, n, CUDA_C_64F, &dsz, &hsz), what);
+  if (dsz > c->dwork_sz) {
+    if (c->dwork) cudaFree(c->dwork);
+    CK(cudaMalloc(&c->dwork, dsz), what);
+    c->dwork_sz = dsz;
+  }
+  if (hsz > c->hwork.size()) c->hwork.resize(hsz);
+  CKS(cusolverDnXgetrf(c->solver, c->params, n, n, CUDA_C_64F, F, n, ip, CUDA_C_64F, c->dwork, c->dwork_sz,
+                       hsz ? c->hwork.data() : nullptr, hsz, c->info),
+      what);
+  if (check_info(c, what)) return -3;
+  c->fac_fp64[slot] = true;
+  return 0;
+}
+
+static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what) {
+  c->fac_fp64[slot] = false;
+  if (c->precision == 0) return dense_factor_fp64(c, slot, M, n, what);
+  if (!c->mx_ready[slot]) {
+    if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) { snprintf(c->err, sizeof(c->err), "%s: cuBLAS set-up", what); return -1; }
+    c->mx_ready[slot] = true;
+  }
+  c->mxs[slot].mode = c->precision;
+  if (bem_mixed_factor(&c->mxs[slot], M, (int)n, c->stream)) {
+    snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
+    return -1;
+  }
+  if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
+    c->st_fallback[slot] = 1;
+    return dense_factor_fp64(c, slot, M, n, what);
+  }
+  return 0;
+}
+
+static int dense_apply(bemgpu_ctx *c, int slot, double *M, int64_t n, int64_t nrhs, double *B, double *Bsave,
+                       const char *what) {
   c->st_iters[slot] = 0;
   c->st_corr[slot] = 0.0;
-  c->st_fallback[slot] = 0;
-  bool fp64 = c->precision == 0;
-  if (!fp64) {
+  if (!c->fac_fp64[slot]) {
     CK(cudaMemcpyAsync(Bsave, B, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
-    if (bem_mixed_factor(&c->mx, M, (int)n, c->stream)) {
-      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mx.err);
-      return -1;
-    }
     int it = 0;
     double rc = 1.0;
-    const bool zero_pivot = (bem_mixed_status(&c->mx, c->stream) & 0x20u) != 0;
-    if (!zero_pivot && bem_mixed_solve(&c->mx, M, (int)n, (int)nrhs, B, 30, 4.0 * 1.1102230246251565e-16, &it, &rc, c->stream)) {
-      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mx.err);
+    if (bem_mixed_solve(&c->mxs[slot], M, (int)n, (int)nrhs, B, 30, 4.0 * 1.1102230246251565e-16, &it, &rc,
+                        c->stream)) {
+      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
       return -1;
     }
     c->st_iters[slot] = it;
     c->st_corr[slot] = rc;
-    if (zero_pivot || !(rc <= 1e-12)) {
-      c->st_fallback[slot] = 1;
-      CK(cudaMemcpyAsync(B, Bsave, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
-      fp64 = true;
-    }
+    if (rc <= 1e-12) return 0;
+    // not refined to FP64 accuracy: FP64 factors from the intact M
+    c->st_fallback[slot] = 1;
+    CK(cudaMemcpyAsync(B, Bsave, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+    const int r = dense_factor_fp64(c, slot, M, n, what);
+    if (r) return r;
   }
-  if (fp64) {
-    double *F = M;
-    if (!M_scratch) {
-      CK(cudaMemcpyAsync(c->W, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
-      F = c->W;
-    }
-    if (lu_factor(c, F, n, what)) return -1;
-    if (check_info(c, what)) return -3;
-    if (lu_solve(c, F, n, nrhs, B, what)) return -1;
-  }
+  double *F = slot == 0 ? M : c->Wd[slot - 1];
+  int64_t *ip = slot == 0 ? c->ipiv : c->ipd[slot - 1];
+  CKS(cusolverDnXgetrs(c->solver, c->params, CUBLAS_OP_T, n, nrhs, CUDA_C_64F, F, n, ip, CUDA_C_64F, B, n, c->info), what);
   return 0;
 }
 
 extern "C" int bemgpu_set_precision(bemgpu_ctx *c, int mode) {
   if (mode < 0 || mode > BEM_MIXED_BF16) { snprintf(c->err, sizeof(c->err), "precision mode %d (0..4)", mode); return -2; }
-  if (mode != 0 && !c->mx_ready) {
-    if (bem_mixed_init(&c->mx, mode, c->stream)) { snprintf(c->err, sizeof(c->err), "cuBLAS set-up failed"); return -1; }
-    c->mx_ready = true;
-  }
-  if (c->mx_ready) c->mx.mode = mode;
   c->precision = mode;
+  c->factored = false;  // factors of the other precision are not reused
   return 0;
 }
 
-extern "C" int bemgpu_get_precision(bemgpu_ctx *c) { return c->precision == 0 ? 0 : c->mx.mode; }
+extern "C" int bemgpu_get_precision(bemgpu_ctx *c) {
+  if (c->precision == 0) return 0;
+  return c->mx_ready[0] ? c->mxs[0].mode : c->precision;
+}
 
 extern "C" int bemgpu_solve_stats(bemgpu_ctx *c, int *iters, double *rel_corr, int *fallback, int max) {
   int k = 0;
@@ -452,24 +479,10 @@ extern "C" int bemgpu_solve_stats(bemgpu_ctx *c, int *iters, double *rel_corr, i
   return k;
 }
 
-extern "C" int bemgpu_solve(bemgpu_ctx *c) {
-  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
-  const size_t n = c->n;
-  if (c->prof) cudaEventRecord(c->ev[12], c->stream);
-  CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
-  CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
-  for (int d = 0; d <= c->MN; ++d)
-    if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], c->A, c->b, c->stream)) return fail(c, "gather", cudaGetLastError());
-  if (c->prof) cudaEventRecord(c->ev[13], c->stream);
-  if (c->precision != 0 && !c->b0) {
-    CK(dalloc(&c->b0, 2 * n), "b copy");
-    CK(dalloc(&c->B3s, 6 * (size_t)c->NN), "B3 copy");
-  }
-  c->st_n = c->MN + 2;
-  {
-    const int rc = dense_solve(c, c->A, (int64_t)n, 1, c->b, c->b0, 0, true, "global LU");
-    if (rc) return rc;
-  }
+// After the global solution X (in b): surface values, particle velocity and
+// dpv of every domain (tmatrix_bd_store, q_solve_pv_bv, solve_dpv_bv,
+// bem3_aw_qd2_solve_bieq.c:370-750).  factor: factor the dpv systems first.
+static int solve_tail(bemgpu_ctx *c, bool factor) {
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_store(&c->sys, d, c->b, c->P[d], c->dP[d], c->stream)) return fail(c, "store", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[14], c->stream);
@@ -486,13 +499,74 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
     if (Nd == 0) continue;
     if (bem_launch_dpv_rhs((int)Nd, c->H[d], c->pv[d], c->B3, c->stream)) return fail(c, "dpv rhs", cudaGetLastError());
-    {
-      const int rc = dense_solve(c, c->G[d], Nd, 3, c->B3, c->B3s, 1 + d, false, "dpv LU");
+    if (factor) {
+      const int rc = dense_factor(c, 1 + d, c->G[d], Nd, "dpv LU");
       if (rc) return rc;
     }
+    const int rc = dense_apply(c, 1 + d, c->G[d], Nd, 3, c->B3, c->B3s, "dpv solve");
+    if (rc) return rc;
     if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
   }
   if (c->prof) cudaEventRecord(c->ev[16], c->stream);
+  return 0;
+}
+
+static int ensure_saves(bemgpu_ctx *c) {
+  if (c->precision != 0 && !c->b0) {
+    CK(dalloc(&c->b0, 2 * (size_t)c->n), "b copy");
+    CK(dalloc(&c->B3s, 6 * (size_t)c->NN), "B3 copy");
+  }
+  c->st_n = c->MN + 2;
+  for (int i = 0; i < c->st_n; ++i) c->st_fallback[i] = 0;
+  return 0;
+}
+
+extern "C" int bemgpu_solve(bemgpu_ctx *c) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  const size_t n = c->n;
+  c->factored = false;
+  if (ensure_saves(c)) return -1;
+  if (c->prof) cudaEventRecord(c->ev[12], c->stream);
+  CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
+  CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
+  for (int d = 0; d <= c->MN; ++d)
+    if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], c->A, c->b, c->stream)) return fail(c, "gather", cudaGetLastError());
+  if (c->prof) cudaEventRecord(c->ev[13], c->stream);
+  int rc = dense_factor(c, 0, c->A, (int64_t)n, "global LU");
+  if (!rc) rc = dense_apply(c, 0, c->A, (int64_t)n, 1, c->b, c->b0, "global solve");
+  if (!rc) rc = solve_tail(c, true);
+  if (rc) return rc;
+  c->factored = true;
+  return 0;
+}
+
+extern "C" int bemgpu_solve_rhs(bemgpu_ctx *c) {
+  if (!c->loaded || !c->factored) {
+    snprintf(c->err, sizeof(c->err), "no factorisation of the current matrices (run bemgpu_solve first)");
+    return -2;
+  }
+  if (ensure_saves(c)) return -1;
+  if (c->prof) cudaEventRecord(c->ev[12], c->stream);
+  CK(cudaMemsetAsync(c->b, 0, 2 * (size_t)c->n * sizeof(double), c->stream), "b clear");
+  for (int d = 0; d <= c->MN; ++d)
+    if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], nullptr, c->b, c->stream)) return fail(c, "rhs", cudaGetLastError());
+  if (c->prof) cudaEventRecord(c->ev[13], c->stream);
+  int rc = dense_apply(c, 0, c->A, (int64_t)c->n, 1, c->b, c->b0, "global solve");
+  if (!rc) rc = solve_tail(c, false);
+  return rc;
+}
+
+extern "C" int bemgpu_set_incident(bemgpu_ctx *c, const double *Pi, const double *dPi, const double *p_inc,
+                                   const double *v_inc, const double *pw) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  const size_t Ne = c->Ne;
+  CK(cudaMemcpyAsync(c->Pi, Pi, Ne * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "Pi");
+  CK(cudaMemcpyAsync(c->dPi, dPi, Ne * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "dPi");
+  CK(cudaMemcpyAsync(c->p_inc, p_inc, Ne * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "p_inc");
+  CK(cudaMemcpyAsync(c->v_inc, v_inc, Ne * 24 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "v_inc");
+  memcpy(c->pw, pw, sizeof(c->pw));
+  CK(cudaMemcpyAsync(c->pw_d, c->pw, 16 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "pw");
+  CK(cudaStreamSynchronize(c->stream), "incident");
   return 0;
 }
 

@@ -283,7 +283,7 @@ extern "C" int bem_launch_gather(const bem_sys_dev *S, int d, const double *G, c
                                  cudaStream_t st) {
   const long long Nd = (long long)S->dom_ne_h[d] * 4;
   if (Nd == 0) return 0;
-  k_gather<<<(unsigned)((Nd * Nd + 255) / 256), 256, 0, st>>>(*S, d, G, H, A);
+  if (A) k_gather<<<(unsigned)((Nd * Nd + 255) / 256), 256, 0, st>>>(*S, d, G, H, A);
   k_rhs<<<(unsigned)((Nd + 7) / 8), 256, 0, st>>>(*S, d, G, H, b);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

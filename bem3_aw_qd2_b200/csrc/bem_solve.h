@@ -25,6 +25,7 @@ struct bem_sys_dev {
 };
 
 extern "C" {
+// A == NULL: the right-hand side b only
 int bem_launch_gather(const bem_sys_dev *S, int d, const double *G, const double *H, double *A, double *b, cudaStream_t st);
 int bem_launch_store(const bem_sys_dev *S, int d, const double *X, double *P, double *dP, cudaStream_t st);
 int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, const double *dH, const double *dF, const double *P,

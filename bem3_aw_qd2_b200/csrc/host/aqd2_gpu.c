@@ -74,8 +74,10 @@ static void gpu_check(bemgpu_ctx *c, int rc, const char *what)
   }
 }
 
-/* flatten AQD2 into host arrays and upload */
-static void load_problem(AQD2 *qd, bemgpu_ctx *c)
+/* Flatten an initialised AQD2 into a bemgpu_problem whose arrays are malloc'ed
+ * here (aqd2_problem_free releases them): element tables, domain lists, media
+ * and the incident field at the element nodes (calc_apw_pv, aw_pw.c:129). */
+void aqd2_problem_build(AQD2 *qd, bemgpu_problem *pr)
 {
   BOUD *bd = &qd->bd;
   int Ne = bd->Ne, nd = qd->MN + 1, tot = 0;
@@ -88,6 +90,10 @@ static void load_problem(AQD2 *qd, bemgpu_ctx *c)
   int *md = aqd2_calloc(Ne, sizeof(int), "md"), *sd = aqd2_calloc(Ne, sizeof(int), "sd");
   int *dom_ne = aqd2_calloc(nd, sizeof(int), "dom_ne"), *sid = aqd2_calloc(tot, sizeof(int), "sid");
   double *k2 = aqd2_calloc(2 * nd, sizeof(double), "k2");
+  double *k0 = aqd2_calloc(nd, sizeof(double), "k0"), *rho0 = aqd2_calloc(nd, sizeof(double), "rho0");
+  double *c0 = aqd2_calloc(nd, sizeof(double), "c0");
+  double *xl = aqd2_calloc(GLN, sizeof(double), "xl"), *wl = aqd2_calloc(GLN, sizeof(double), "wl");
+  double *xh = aqd2_calloc(GHN, sizeof(double), "xh"), *wh = aqd2_calloc(GHN, sizeof(double), "wh");
   unsigned char *plane = aqd2_calloc(Ne, 1, "plane");
   for (int e = 0; e < Ne; e++) {
     int i = e + 1;
@@ -125,26 +131,47 @@ static void load_problem(AQD2 *qd, bemgpu_ctx *c)
     for (int s = 1; s <= bd->sb[d].Ne; s++) sid[o++] = bd->sb[d].sid[s];
     k2[2 * d] = creal(qd->k2[d]);
     k2[2 * d + 1] = cimag(qd->k2[d]);
+    k0[d] = qd->k0[d];
+    rho0[d] = qd->rho0[d];
+    c0[d] = qd->c0[d];
   }
+  for (int i = 0; i < GLN; i++) { xl[i] = bd->xli[i]; wl[i] = bd->wli[i]; }
+  for (int i = 0; i < GHN; i++) { xh[i] = bd->xhi[i]; wh[i] = bd->whi[i]; }
+  memset(pr, 0, sizeof(*pr));
+  pr->Ne = Ne; pr->NN = bd->NN; pr->MN = qd->MN; pr->ps = bd->ps;
+  pr->qp[0] = bd->qd.k; pr->qp[1] = bd->qd.vk[0]; pr->qp[2] = bd->qd.vk[1]; pr->qp[3] = bd->qd.vk[2];
+  pr->qp[4] = bd->qd.vd1[0]; pr->qp[5] = bd->qd.vd1[1]; pr->qp[6] = bd->qd.vd2[0]; pr->qp[7] = bd->qd.vd2[1];
+  pr->cr = cr; pr->cw = cw; pr->ren = ren; pr->wen = wen; pr->npe = npe; pr->eni = eni; pr->md = md; pr->sd = sd;
+  pr->dom_ne = dom_ne; pr->sid = sid; pr->k0 = k0; pr->k2 = k2; pr->rho0 = rho0; pr->c0 = c0;
+  pr->Pi = Pi; pr->dPi = dPi; pr->p_inc = pinc; pr->v_inc = vinc;
+  pr->xl = xl; pr->wl = wl; pr->xh = xh; pr->wh = wh; pr->plane = plane;
+  pr->pw[0] = creal(qd->pw.p);
+  pr->pw[1] = cimag(qd->pw.p);
+  for (int i = 0; i < 9; i++) pr->pw[2 + i] = qd->pw.wd.R[i];
+  for (int i = 0; i < 3; i++) pr->pw[11 + i] = qd->pw.tv[i];
+  pr->pw[14] = qd->pw.wd.k0;
+  pr->pw[15] = qd->pw.rho0 * qd->pw.c0;
+}
+
+void aqd2_problem_free(bemgpu_problem *pr)
+{
+  free((void *)pr->cr); free((void *)pr->cw); free((void *)pr->ren); free((void *)pr->wen);
+  free((void *)pr->Pi); free((void *)pr->dPi); free((void *)pr->p_inc); free((void *)pr->v_inc);
+  free((void *)pr->npe); free((void *)pr->eni); free((void *)pr->md); free((void *)pr->sd);
+  free((void *)pr->dom_ne); free((void *)pr->sid); free((void *)pr->k2); free((void *)pr->k0);
+  free((void *)pr->rho0); free((void *)pr->c0); free((void *)pr->xl); free((void *)pr->wl);
+  free((void *)pr->xh); free((void *)pr->wh); free((void *)pr->plane);
+  memset(pr, 0, sizeof(*pr));
+}
+
+/* flatten AQD2 and upload */
+static void load_problem(AQD2 *qd, bemgpu_ctx *c)
+{
   bemgpu_problem pr;
-  memset(&pr, 0, sizeof(pr));
-  pr.Ne = Ne; pr.NN = bd->NN; pr.MN = qd->MN; pr.ps = bd->ps;
-  pr.qp[0] = bd->qd.k; pr.qp[1] = bd->qd.vk[0]; pr.qp[2] = bd->qd.vk[1]; pr.qp[3] = bd->qd.vk[2];
-  pr.qp[4] = bd->qd.vd1[0]; pr.qp[5] = bd->qd.vd1[1]; pr.qp[6] = bd->qd.vd2[0]; pr.qp[7] = bd->qd.vd2[1];
-  pr.cr = cr; pr.cw = cw; pr.ren = ren; pr.wen = wen; pr.npe = npe; pr.eni = eni; pr.md = md; pr.sd = sd;
-  pr.dom_ne = dom_ne; pr.sid = sid; pr.k0 = qd->k0; pr.k2 = k2; pr.rho0 = qd->rho0; pr.c0 = qd->c0;
-  pr.Pi = Pi; pr.dPi = dPi; pr.p_inc = pinc; pr.v_inc = vinc;
-  pr.xl = bd->xli; pr.wl = bd->wli; pr.xh = bd->xhi; pr.wh = bd->whi; pr.plane = plane;
-  pr.pw[0] = creal(qd->pw.p);
-  pr.pw[1] = cimag(qd->pw.p);
-  for (int i = 0; i < 9; i++) pr.pw[2 + i] = qd->pw.wd.R[i];
-  for (int i = 0; i < 3; i++) pr.pw[11 + i] = qd->pw.tv[i];
-  pr.pw[14] = qd->pw.wd.k0;
-  pr.pw[15] = qd->pw.rho0 * qd->pw.c0;
+  aqd2_problem_build(qd, &pr);
   gpu_check(c, bemgpu_load(c, &pr), "load");
   gpu_check(c, bemgpu_sync(c), "load");
-  free(cr); free(cw); free(ren); free(wen); free(Pi); free(dPi); free(pinc); free(vinc);
-  free(npe); free(eni); free(md); free(sd); free(dom_ne); free(sid); free(k2); free(plane);
+  aqd2_problem_free(&pr);
 }
 
 static void download_solution(AQD2 *qd, bemgpu_ctx *c)

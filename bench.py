@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--workload", default="sphere216")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rate", type=float, default=10.0, help="stream workload: mean arrivals per second")
+    ap.add_argument("--slots", type=int, default=4, help="stream workload: server slots")
+    ap.add_argument("--hbm-gb", type=float, default=64.0, help="stream workload: device-memory budget")
     ap.add_argument("--mixed-mode", type=int, default=3,
                     help="precision of the mixed form: 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates; 0: skip it")
     return ap.parse_args()
@@ -177,6 +180,118 @@ def run_reference(args, rank, world):
                                                   "d2h_bytes_per_step": 0}}))
 
 
+STREAM_DESC = ("seeded Poisson request stream (numpy default_rng(2024)), scaled down from the 216-6144-quad "
+               "stream to 216/384/600-quad cube-spheres and spheroids (radius 0.2-0.3), square or triangular "
+               "lattice of period 0.7-1.1, k.a in [1, 2.5], theta 0-60 deg, phi 0-360 deg, 30% repeats of an "
+               "earlier (mesh, k, in-plane wave vector) with a new amplitude or the mirrored polar angle; draws "
+               "within 2% of a Rayleigh anomaly are redrawn")
+
+
+def stream_requests(count, rng):
+    """The request stream: (meshgen arguments, reuse key) per request."""
+    import math
+    reqs, seen = [], []
+    while len(reqs) < count:
+        if seen and rng.random() < 0.3:
+            base = seen[int(rng.integers(len(seen)))]
+            r = dict(base[0])
+            if rng.random() < 0.5:
+                r["theta_deg"] = 180.0 - r["theta_deg"]
+            r["amp"] = (float(rng.uniform(0.5, 1.5)), float(rng.uniform(-1, 1)))
+            reqs.append((r, base[1]))
+            continue
+        n = int(rng.choice([6, 8, 10]))
+        rad = float(rng.uniform(0.2, 0.3))
+        axes = (rad, rad, rad) if rng.random() < 0.5 else (0.85 * rad, 0.85 * rad, 1.15 * rad)
+        a = float(rng.uniform(0.7, 1.1))
+        lat = ((a, 0.0), (0.0, a)) if rng.random() < 0.5 else ((a, 0.0), (0.5 * a, 0.5 * math.sqrt(3.0) * a))
+        k = float(rng.uniform(1.0, 2.5)) / a
+        th, ph = float(rng.uniform(0.0, 60.0)), float(rng.uniform(0.0, 360.0))
+        kx, ky = k * math.sin(math.radians(th)) * math.cos(math.radians(ph)), k * math.sin(math.radians(th)) * math.sin(math.radians(ph))
+        # Rayleigh anomalies |k_par + g| = k: keep 2% away
+        det = lat[0][0] * lat[1][1] - lat[1][0] * lat[0][1]
+        g1 = (2 * math.pi * lat[1][1] / det, -2 * math.pi * lat[1][0] / det)
+        g2 = (-2 * math.pi * lat[0][1] / det, 2 * math.pi * lat[0][0] / det)
+        bad = any(abs(math.hypot(kx + i * g1[0] + j * g2[0], ky + i * g1[1] + j * g2[1]) - k) < 0.02 * k
+                  for i in range(-6, 7) for j in range(-6, 7))
+        if bad or th < 0.5:  # the reference rejects kx = ky = 0
+            continue
+        r = dict(n=n, semi_axes=axes, lattice=lat, theta_deg=th, phi_deg=ph, wavelength=2 * math.pi / k)
+        key = hash((n, axes, lat, round(k, 14), round(kx, 12), round(ky, 12))) & 0xFFFFFFFFFFFFFFFF
+        seen.append((r, key))
+        reqs.append((r, key))
+    return reqs
+
+
+def run_stream(args, rank, world):
+    """Serving: the request stream through the native server (continuous
+    batching, factorisation reuse, HBM admission), plain FP64 and mixed."""
+    from bem3_aw_qd2_b200 import api, meshgen
+    h, g = api.libs()
+    h.aqd2_set_verbose(0)
+    rng = np.random.default_rng(2024)
+    count = max(args.steps, 8) * 8
+    reqs = stream_requests(count, rng)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, count))
+    # requests are built (mesh, element tables, incident field) before the clock starts
+    cases, probs = [], []
+    for i, (r, key) in enumerate(reqs):
+        d = tempfile.mkdtemp(prefix="stream_")
+        c = api.Case.from_files(*meshgen.write_inputs(d, **r))
+        cases.append(c)
+        probs.append(c.problem())
+    out = {}
+    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 3)):
+        srv = api.Server(device=0, hbm_budget=int(args.hbm_gb * (1 << 30)), slots=args.slots)
+        # warm-up: one request per mesh size
+        for i, n in enumerate(sorted({r["n"] for r, _ in reqs})):
+            j = next(k for k, (r, _) in enumerate(reqs) if r["n"] == n)
+            srv.submit(probs[j], 0xFFFF0000 + i, -1 - i, precision=prec)
+        got = 0
+        while got < len({r["n"] for r, _ in reqs}):
+            got += len(srv.poll(timeout_ms=1000))
+        done, t_sub = {}, {}
+        t0 = time.perf_counter()
+        for i in range(count):
+            while time.perf_counter() - t0 < arrivals[i]:
+                for r in srv.poll(timeout_ms=1):
+                    done[r.id] = (r, time.perf_counter())
+            t_sub[i] = time.perf_counter()
+            srv.submit(probs[i], reqs[i][1], i, precision=prec)
+        while len(done) < count:
+            for r in srv.poll(timeout_ms=100):
+                done[r.id] = (r, time.perf_counter())
+        t1 = max(t for _, t in done.values())
+        st = srv.stats()
+        srv.close()
+        lat = [(done[i][1] - t_sub[i]) * 1000.0 for i in range(count)]
+        bad = [done[i][0].error.decode() for i in range(count) if done[i][0].status != 0]
+        out[tag] = {"value": count / (t1 - t0), "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                                               "p99": float(np.percentile(lat, 99))},
+                    "reused": int(st["reused"]), "evictions": int(st["evictions"]),
+                    "bytes_peak": st["bytes_peak"], "failed": len(bad),
+                    "F": {i: list(done[i][0].F[:]) for i in range(count)}}
+    errs = []
+    for i in range(count):
+        a, b = np.array(out["fp64"]["F"][i]), np.array(out["mixed"]["F"][i])
+        errs.append(float(np.linalg.norm(a - b) / np.linalg.norm(a)))
+    for tag in out:
+        del out[tag]["F"]
+    for c, p in zip(cases, probs):
+        c.free_problem(p)
+        c.close()
+    mixed = out["mixed"]
+    line = {"metric": "solves/s", "value": mixed["value"], "unit": "solves/s", "n_gpus": 1, "steps": count,
+            "warmup": 3, "ms_per_step": 1000.0 / mixed["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 assembly, complex-FP32 LU + FP64 refinement", "data": "synthetic",
+            "config": {"workload": "stream", "requests": count, "rate_per_s": args.rate, "slots": args.slots,
+                       "hbm_budget_gb": args.hbm_gb, "stream": STREAM_DESC},
+            "latency_ms": mixed["latency_ms"], "fp64": out["fp64"], "mixed": mixed,
+            "force_rel_err_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def workload_desc(name):
     from bem3_aw_qd2_b200 import meshgen
     c = meshgen.CONFIGS[name]
@@ -190,8 +305,14 @@ def workload_desc(name):
 def main():
     args = parse()
     rank, world, local = dist_env()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.workload != "stream":
         return run_reference(args, rank, world)
+    if args.workload == "stream":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; its per-solve "
+                                                                  "time is the sphere216 reference line"}))
+            return
+        return run_stream(args, rank, world)
     # load the library (and the CUDA 12.9 cuBLAS it links) before torch brings its own
     from bem3_aw_qd2_b200 import api
     api.libs()

@@ -158,6 +158,12 @@ void aqd2_set_verbose(int on);
 /* Last wall time of the solve phases in seconds: [0] upload, [1] assembly,
  * [2] solve, [3] download. */
 void aqd2_last_timing(double *t4);
+/* Flatten an initialised AQD2 into a bemgpu_problem (bemgpu.h) with freshly
+ * allocated host arrays, e.g. for the request server; aqd2_problem_free
+ * releases them. */
+struct bemgpu_problem;
+void aqd2_problem_build(AQD2 *qd, struct bemgpu_problem *pr);
+void aqd2_problem_free(struct bemgpu_problem *pr);
 /* The device context that solve_bieq_aqd2 used for qd (NULL before the first
  * solve); its type is declared in bemgpu.h. */
 struct bemgpu_ctx *aqd2_device_context(AQD2 *qd);

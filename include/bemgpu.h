@@ -14,6 +14,8 @@
 #ifndef BEMGPU_H
 #define BEMGPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -71,12 +73,27 @@ unsigned bemgpu_status(bemgpu_ctx *ctx); /* BEMGPU_ST_* bits accumulated since l
  * read_aqd2/initialize_aqd2 build, bem3_aw_qd2.c:3-109). */
 int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
 
+/* Free the loaded problem's device memory (the context stays usable). */
+int bemgpu_unload(bemgpu_ctx *ctx);
+
 /* Coefficient matrices of every domain (create_cmatrix,
  * bem3_aw_qd2_solve_bieq.c:124-218). */
 int bemgpu_assemble(bemgpu_ctx *ctx);
 
 /* Global system, LU solve, P/dP, pv, dpv (bem3_aw_qd2_solve_bieq.c:220-750). */
 int bemgpu_solve(bemgpu_ctx *ctx);
+
+/* Factorisation reuse: replace the incident field (same layouts as
+ * bemgpu_problem: Pi, dPi, p_inc [Ne][4] complex, v_inc [Ne][4][3] complex,
+ * pw[16]) and solve again with the factors of the last bemgpu_solve; only the
+ * right-hand side changes (same mesh, media, frequency and in-plane Bloch
+ * wave vector: the matrices are those of init_boundary_data's new incident
+ * field, bem3_aw_qd2.c:1104-1146).  bemgpu_solve_rhs returns -2 when no
+ * factorisation of the current matrices is held (after bemgpu_load,
+ * bemgpu_assemble or bemgpu_set_precision). */
+int bemgpu_set_incident(bemgpu_ctx *ctx, const double *Pi, const double *dPi, const double *p_inc, const double *v_inc,
+                        const double *pw);
+int bemgpu_solve_rhs(bemgpu_ctx *ctx);
 
 /* solve_bieq_aqd2 (bem3_aw_qd2_solve_bieq.c:3): assemble + solve. */
 int bemgpu_run(bemgpu_ctx *ctx);
@@ -199,6 +216,45 @@ int bemgpu_work_counters(bemgpu_ctx *ctx, unsigned long long *out6, int reset);
 int bemgpu_assemble_domain_static(const double *cr, const double *cw, const double *ren, const unsigned char *plane,
                                   const int *sid, int ne, const double *qp, int periodic, double k, double *G,
                                   double *H, double *dG, double *dH, double *dF, void *stream);
+
+/* ---- Request server (no counterpart in the reference: there each request
+ * is one solve_bieq_aqd2 + force_FN_aqd2 run).
+ *
+ * Continuous batching on one GPU: submitted requests queue and are admitted
+ * to one of `slots` solver slots as slots and device memory free up; each
+ * slot has its own CUDA stream and host worker thread, so admitted requests'
+ * assemblies and solves overlap on the device.  A slot keeps its problem's
+ * matrices and factors: a request whose reuse_key equals an idle slot's (the
+ * caller's hash of mesh, media, lattice, frequency and in-plane Bloch wave
+ * vector) is routed there and only its right-hand side is solved
+ * (bemgpu_set_incident + bemgpu_solve_rhs).  Admission keeps the resident
+ * problems' device bytes within hbm_budget (per problem: 16 n^2 for the
+ * global matrix, 48 N_d^2 per domain and 64 N_d^2 more for interior domains,
+ * 8 n^2 + 8 N_d^2 more in mixed precision, plus tables and 64 MB of solver
+ * workspace), evicting idle slots' problems least recently used first; later
+ * requests that fit may pass one that does not until it has waited 2 s.
+ * The problem's arrays are copied on submit.  Results (radiation force and
+ * torque of the given rule about rc) come back through bemgpu_server_poll in
+ * completion order. */
+typedef struct bemgpu_server bemgpu_server;
+typedef struct bemgpu_result {
+  long long id;        /* the id given to bemgpu_server_submit */
+  int status;          /* 0, or the failing call's return code */
+  int reused;          /* 1: solved with a resident factorisation (right-hand side only) */
+  double F[3], N[3];   /* force and torque */
+  double queue_ms;     /* submit -> admitted to a slot */
+  double service_ms;   /* admitted -> result */
+  char error[160];
+} bemgpu_result;
+int bemgpu_server_create(int device, size_t hbm_budget, int slots, bemgpu_server **out);
+/* 0 queued; -2 the problem needs more than the whole budget */
+int bemgpu_server_submit(bemgpu_server *srv, const bemgpu_problem *prob, unsigned long long reuse_key, int precision,
+                         int force_type, const double *rc, long long id);
+/* Up to max finished results; waits up to timeout_ms for the first one.  Returns the count. */
+int bemgpu_server_poll(bemgpu_server *srv, bemgpu_result *out, int max, int timeout_ms);
+/* out8: submitted, completed, solved by reuse, running, queued, device bytes resident, peak, evictions */
+int bemgpu_server_stats(bemgpu_server *srv, double *out8);
+void bemgpu_server_destroy(bemgpu_server *srv);
 
 /* Faddeeva w(z) at n points (host arrays of (re, im) pairs), relative error
  * 1e-15 (Faddeeva_w, qgf2_src/Faddeeva.cc:679, called with MEPS). */
