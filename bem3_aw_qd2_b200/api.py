@@ -55,6 +55,8 @@ def libs():
         g.bemgpu_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
         g.bemgpu_set_precision.argtypes = [vp, ctypes.c_int]
         g.bemgpu_get_precision.argtypes = [vp]
+        g.bemgpu_set_ewald_scale.argtypes = [vp, ctypes.c_double]
+        g.bemgpu_autotune.argtypes = [vp, _d]
         g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
         h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
         for name in ("print_aqd2", "initialize_aqd2", "finalize_aqd2", "solve_bieq_aqd2"):
@@ -217,6 +219,15 @@ class Case:
     def set_precision(self, mode):
         """0 FP64 LU; 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates with FP64 refinement."""
         self._check(libs()[1].bemgpu_set_precision(self.ctx, int(mode)), "set_precision")
+
+    def autotune(self):
+        """Pick the Ewald parameter for the loaded problem (bemgpu_autotune); returns the scale."""
+        out = np.zeros(1)
+        self._check(libs()[1].bemgpu_autotune(self.ctx, _p(out)), "autotune")
+        return float(out[0])
+
+    def set_ewald_scale(self, scale):
+        self._check(libs()[1].bemgpu_set_ewald_scale(self.ctx, float(scale)), "set_ewald_scale")
 
     def precision(self):
         """The precision mode in effect (see bemgpu.h)."""

@@ -890,7 +890,7 @@ __global__ void k_wtab_build(double x, double *__restrict__ out) {
 // ------------------------------------------------------------------ host launchers
 extern "C" int bem_launch_wtab(double x, double *out, cudaStream_t st) {
   k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(x, out);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh) {
@@ -919,13 +919,13 @@ extern "C" int bem_set_constants(const double *xl, const double *wl, const doubl
 extern "C" int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st) {
   if (n <= 0) return 0;
   k_faddeeva<<<(n + 127) / 128, 128, 0, st>>>(z, n, w);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st) {
   if (n <= 0) return 0;
   k_qpgf_points<<<(n + 127) / 128, 128, 0, st>>>(*q, r, n, G, dG, ret);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
@@ -958,7 +958,37 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   if (ev) cudaEventRecord(ev[4], st);
   k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, exterior, S->rowF, S->near_n, S->nearF, S->selfF, H, dF, S->status);
   if (ev) cudaEventRecord(ev[5], st);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
+// Time the periodic regular-pair kernel on a sample of the pairs (nchunk
+// chunks of frac / nchunk of all pairs, spread over the node range) for the
+// Ewald-parameter autotuner; the pair flags must be current (k_classify).
+extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H,
+                                double frac, int nchunk, cudaStream_t st, float *ms) {
+  const long long npairs = (long long)D->ne * 4 * D->ne;
+  const long long len = (long long)(npairs * frac / nchunk) + 1;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1;
+  cudaEventRecord(e0, st);
+  for (int c = 0; c < nchunk; ++c) {
+    const long long p0 = npairs * c / nchunk;
+    const long long np = p0 + len <= npairs ? len : npairs - p0;
+    if (np > 0)
+      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+  }
+  cudaEventRecord(e1, st);
+  int rc = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(ms, e0, e1) == cudaSuccess ? 0 : -1;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (cudaPeekAtLastError() != cudaSuccess) rc = -1;
+  return rc;
+}
+
+extern "C" int bem_launch_classify(const bem_dom_dev *D, bem_scratch *S, cudaStream_t st) {
+  if (D->ne <= 0) return 0;
+  k_classify<<<D->ne * 4, 128, 0, st>>>(*D, S->rowF, S->near_s, S->near_n, S->flag, S->status);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 #include "bem_post.cuh"

@@ -47,6 +47,7 @@ struct bemgpu_ctx {
   double *fout = nullptr, *rc_d = nullptr;
   double *wtab = nullptr;  // w(k eta0 + i y) table of the Ewald real-space sums
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
+  double eta_scale = 1.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale
   double *pw_d = nullptr;
   // 9-point targets on the domain-0 elements for the type-1 force
   int ntgt = 0;
@@ -72,6 +73,14 @@ struct bemgpu_ctx {
   bool fac_fp64[BEMGPU_MAXDOM + 1] = {};
   bool factored = false;  // factors of the current matrices are held (bemgpu_solve_rhs may run)
   double *b0 = nullptr, *B3s = nullptr;  // saved right-hand sides (FP64 fallback)
+  // side lane: the dpv factorisations run there, overlapping the global system
+  cudaStream_t side = nullptr;
+  cusolverDnHandle_t solver2 = nullptr;
+  void *dwork2 = nullptr;
+  size_t dwork2_sz = 0;
+  std::vector<char> hwork2;
+  int *info2 = nullptr;  // [BEMGPU_MAXDOM] getrf info of the dpv systems
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
   double st_corr[BEMGPU_MAXDOM + 1] = {};
 };
@@ -126,6 +135,9 @@ static void free_problem(bemgpu_ctx *c) {
   if (c->dwork) cudaFree(c->dwork);
   c->dwork = nullptr;
   c->dwork_sz = 0;
+  if (c->dwork2) cudaFree(c->dwork2);
+  c->dwork2 = nullptr;
+  c->dwork2_sz = 0;
   c->loaded = false;
 }
 
@@ -143,6 +155,14 @@ extern "C" int bemgpu_create(int device, void *stream, bemgpu_ctx **out) {
   }
   if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS || cusolverDnSetStream(c->solver, c->stream) != CUSOLVER_STATUS_SUCCESS ||
       cusolverDnCreateParams(&c->params) != CUSOLVER_STATUS_SUCCESS) {
+    delete c;
+    return -1;
+  }
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cusolverDnCreate(&c->solver2) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnSetStream(c->solver2, c->side) != CUSOLVER_STATUS_SUCCESS ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess || dalloc(&c->info2, BEMGPU_MAXDOM) != cudaSuccess) {
     delete c;
     return -1;
   }
@@ -172,6 +192,11 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->params) cusolverDnDestroyParams(c->params);
   if (c->solver) cusolverDnDestroy(c->solver);
+  if (c->solver2) cusolverDnDestroy(c->solver2);
+  if (c->side) { cudaStreamSynchronize(c->side); cudaStreamDestroy(c->side); }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  dfree(c->info2);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -246,7 +271,8 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   bem_qp_prepare(pr->qp, &c->qp);
   CK(dalloc(&c->wtab, BEM_WT_SIZE), "w table");
-  if (bem_launch_wtab(c->qp.k * c->qp.eta0, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
+  c->qp.eta_run = c->qp.eta0 * c->eta_scale;
+  if (bem_launch_wtab(c->qp.k * c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
   c->qp.wt_h = 0.125;
   c->qp.wt_n = 64;
@@ -347,6 +373,53 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   return 0;
 }
 
+extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
+  if (!(scale >= 0.25 && scale <= 4.0)) { snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale); return -2; }
+  c->eta_scale = scale;
+  c->factored = false;
+  if (!c->loaded) return 0;
+  c->qp.eta_run = c->qp.eta0 * scale;
+  if (bem_launch_wtab(c->qp.k * c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
+  return 0;
+}
+
+static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
+
+// Ewald-parameter autotuner: time the periodic regular-pair kernel on a
+// sample of the pairs for eta0 x {1.0, 1.1, 1.2, 1.3} (larger factors meet the
+// per-point cap and lose the tabulated real-space terms) and keep the fastest.
+extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  bem_dom_dev D = dom_view(c, 0);
+  if (bem_launch_classify(&D, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
+  double *tab = nullptr;
+  CK(dalloc(&tab, BEM_WT_SIZE), "autotune");
+  const double cand[4] = {1.0, 1.1, 1.2, 1.3};
+  double best = 1.0;
+  float tbest = 1e30f;
+  int rc = 0;
+  for (int i = 0; i < 4 && !rc; ++i) {
+    bem_qp q = c->qp;
+    q.eta_run = q.eta0 * cand[i];
+    q.wt = tab;
+    if (bem_launch_wtab(q.k * q.eta_run, tab, c->stream)) { rc = fail(c, "autotune", cudaGetLastError()); break; }
+    float t = 0.f, tmin = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (bem_time_regular(&D, &q, &c->scr, c->G[0], c->H[0], 0.125, 4, c->stream, &t)) {
+        rc = fail(c, "autotune", cudaGetLastError());
+        break;
+      }
+      tmin = t < tmin ? t : tmin;
+    }
+    if (tmin < tbest) { tbest = tmin; best = cand[i]; }
+  }
+  cudaStreamSynchronize(c->stream);
+  cudaFree(tab);
+  if (rc) return rc;
+  if (best_scale) *best_scale = best;
+  return bemgpu_set_ewald_scale(c, best);
+}
+
 extern "C" int bemgpu_unload(bemgpu_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
@@ -390,41 +463,73 @@ static int check_info(bemgpu_ctx *c, const char *what) {
 // factors + FP64 refinement against M, which stays intact; a system with a
 // zero FP32 pivot, or whose refinement does not reach 1e-12, switches to FP64
 // factors (then kept for later right-hand sides).
-static int dense_factor_fp64(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what) {
+// lane 0: the context's stream (checked at once); lane 1: the side stream
+// (dpv systems, checked after the join in bemgpu_solve)
+static int dense_factor_fp64(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what, int lane = 0) {
   double *F = slot == 0 ? M : c->Wd[slot - 1];
   int64_t *ip = slot == 0 ? c->ipiv : c->ipd[slot - 1];
-  if (F != M) CK(cudaMemcpyAsync(F, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+  cudaStream_t st = lane ? c->side : c->stream;
+  cusolverDnHandle_t sv = lane ? c->solver2 : c->solver;
+  void **dw = lane ? &c->dwork2 : &c->dwork;
+  size_t *dws = lane ? &c->dwork2_sz : &c->dwork_sz;
+  std::vector<char> &hw = lane ? c->hwork2 : c->hwork;
+  int *info = lane ? c->info2 + (slot - 1) : c->info;
+  if (F != M) CK(cudaMemcpyAsync(F, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, st), what);
   size_t dsz = 0, hsz = 0;
-  CKS(cusolverDnXgetrf_bufferSize(c->solver, c->params, n, n, CUDA_C_64F, F, n, CUDA_C_64F, &dsz, &hsz), what);
-  if (dsz > c->dwork_sz) {
-    if (c->dwork) cudaFree(c->dwork);
-    CK(cudaMalloc(&c->dwork, dsz), what);
-    c->dwork_sz = dsz;
+  CKS(cusolverDnXgetrf_bufferSize(sv, c->params, n, n, CUDA_C_64F, F, n, CUDA_C_64F, &dsz, &hsz), what);
+  if (dsz > *dws) {
+    // the lane's stream may still use the old workspace
+    CK(cudaStreamSynchronize(st), what);
+    if (*dw) cudaFree(*dw);
+    CK(cudaMalloc(dw, dsz), what);
+    *dws = dsz;
   }
-  if (hsz > c->hwork.size()) c->hwork.resize(hsz);
-  CKS(cusolverDnXgetrf(c->solver, c->params, n, n, CUDA_C_64F, F, n, ip, CUDA_C_64F, c->dwork, c->dwork_sz,
-                       hsz ? c->hwork.data() : nullptr, hsz, c->info),
+  if (hsz > hw.size()) hw.resize(hsz);
+  CKS(cusolverDnXgetrf(sv, c->params, n, n, CUDA_C_64F, F, n, ip, CUDA_C_64F, *dw, *dws, hsz ? hw.data() : nullptr, hsz,
+                       info),
       what);
-  if (check_info(c, what)) return -3;
   c->fac_fp64[slot] = true;
+  if (lane == 0 && check_info(c, what)) return -3;
   return 0;
 }
 
-static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what) {
+static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what, int lane = 0) {
   c->fac_fp64[slot] = false;
-  if (c->precision == 0) return dense_factor_fp64(c, slot, M, n, what);
+  if (c->precision == 0) return dense_factor_fp64(c, slot, M, n, what, lane);
   if (!c->mx_ready[slot]) {
     if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) { snprintf(c->err, sizeof(c->err), "%s: cuBLAS set-up", what); return -1; }
     c->mx_ready[slot] = true;
   }
   c->mxs[slot].mode = c->precision;
-  if (bem_mixed_factor(&c->mxs[slot], M, (int)n, c->stream)) {
+  cudaStream_t st = lane ? c->side : c->stream;
+  if (bem_mixed_factor(&c->mxs[slot], M, (int)n, st)) {
     snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
     return -1;
   }
-  if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
+  if (lane == 0 && (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u)) {
     c->st_fallback[slot] = 1;
     return dense_factor_fp64(c, slot, M, n, what);
+  }
+  return 0;
+}
+
+// After the side lane joined: the dpv factorisations' outcome (zero pivots).
+static int check_side_factors(bemgpu_ctx *c) {
+  int info[BEMGPU_MAXDOM] = {};
+  CK(cudaMemcpyAsync(info, c->info2, sizeof(int) * (c->MN + 1), cudaMemcpyDeviceToHost, c->stream), "dpv LU");
+  CK(cudaStreamSynchronize(c->stream), "dpv LU");
+  for (int d = 0; d <= c->MN; ++d) {
+    const int slot = 1 + d;
+    if (c->fac_fp64[slot]) {
+      if (info[d] != 0) {
+        snprintf(c->err, sizeof(c->err), "dpv LU of domain %d: factorisation info %d", d, info[d]);
+        return -3;
+      }
+    } else if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
+      c->st_fallback[slot] = 1;
+      const int r = dense_factor_fp64(c, slot, c->G[d], 4 * (int64_t)c->dom_ne[d], "dpv LU");
+      if (r) return r;
+    }
   }
   return 0;
 }
@@ -481,8 +586,8 @@ extern "C" int bemgpu_solve_stats(bemgpu_ctx *c, int *iters, double *rel_corr, i
 
 // After the global solution X (in b): surface values, particle velocity and
 // dpv of every domain (tmatrix_bd_store, q_solve_pv_bv, solve_dpv_bv,
-// bem3_aw_qd2_solve_bieq.c:370-750).  factor: factor the dpv systems first.
-static int solve_tail(bemgpu_ctx *c, bool factor) {
+// bem3_aw_qd2_solve_bieq.c:370-750), with the dpv factors already held.
+static int solve_tail(bemgpu_ctx *c) {
   for (int d = 0; d <= c->MN; ++d)
     if (bem_launch_store(&c->sys, d, c->b, c->P[d], c->dP[d], c->stream)) return fail(c, "store", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[14], c->stream);
@@ -499,10 +604,6 @@ static int solve_tail(bemgpu_ctx *c, bool factor) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
     if (Nd == 0) continue;
     if (bem_launch_dpv_rhs((int)Nd, c->H[d], c->pv[d], c->B3, c->stream)) return fail(c, "dpv rhs", cudaGetLastError());
-    if (factor) {
-      const int rc = dense_factor(c, 1 + d, c->G[d], Nd, "dpv LU");
-      if (rc) return rc;
-    }
     const int rc = dense_apply(c, 1 + d, c->G[d], Nd, 3, c->B3, c->B3s, "dpv solve");
     if (rc) return rc;
     if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
@@ -516,6 +617,15 @@ static int ensure_saves(bemgpu_ctx *c) {
     CK(dalloc(&c->b0, 2 * (size_t)c->n), "b copy");
     CK(dalloc(&c->B3s, 6 * (size_t)c->NN), "B3 copy");
   }
+  // mixed-precision state of every dense system, set up before any lane uses it
+  for (int slot = 0; c->precision != 0 && slot <= c->MN + 1; ++slot)
+    if (!c->mx_ready[slot]) {
+      if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) {
+        snprintf(c->err, sizeof(c->err), "cuBLAS set-up failed");
+        return -1;
+      }
+      c->mx_ready[slot] = true;
+    }
   c->st_n = c->MN + 2;
   for (int i = 0; i < c->st_n; ++i) c->st_fallback[i] = 0;
   return 0;
@@ -527,6 +637,18 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   c->factored = false;
   if (ensure_saves(c)) return -1;
   if (c->prof) cudaEventRecord(c->ev[12], c->stream);
+  // the dpv systems depend only on G_d: factor them on the side lane while the
+  // global system is gathered, factored and solved here
+  CK(cudaEventRecord(c->ev_fork, c->stream), "fork");
+  CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "fork");
+  CK(cudaMemsetAsync(c->info2, 0, sizeof(int) * BEMGPU_MAXDOM, c->side), "fork");
+  for (int d = 0; d <= c->MN; ++d) {
+    const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
+    if (Nd == 0) continue;
+    const int r = dense_factor(c, 1 + d, c->G[d], Nd, "dpv LU", 1);
+    if (r) return r;
+  }
+  CK(cudaEventRecord(c->ev_join, c->side), "join");
   CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
   CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
   for (int d = 0; d <= c->MN; ++d)
@@ -534,7 +656,11 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   if (c->prof) cudaEventRecord(c->ev[13], c->stream);
   int rc = dense_factor(c, 0, c->A, (int64_t)n, "global LU");
   if (!rc) rc = dense_apply(c, 0, c->A, (int64_t)n, 1, c->b, c->b0, "global solve");
-  if (!rc) rc = solve_tail(c, true);
+  // join the side lane before anything reads the dpv factors
+  const cudaError_t je = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+  if (!rc && je != cudaSuccess) rc = fail(c, "join", je);
+  if (!rc) rc = check_side_factors(c);
+  if (!rc) rc = solve_tail(c);
   if (rc) return rc;
   c->factored = true;
   return 0;
@@ -552,7 +678,7 @@ extern "C" int bemgpu_solve_rhs(bemgpu_ctx *c) {
     if (bem_launch_gather(&c->sys, d, c->G[d], c->H[d], nullptr, c->b, c->stream)) return fail(c, "rhs", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[13], c->stream);
   int rc = dense_apply(c, 0, c->A, (int64_t)c->n, 1, c->b, c->b0, "global solve");
-  if (!rc) rc = solve_tail(c, false);
+  if (!rc) rc = solve_tail(c);
   return rc;
 }
 
@@ -584,12 +710,18 @@ extern "C" int bemgpu_phase_times(bemgpu_ctx *c, double *ms, int max) {
   for (int d = 0; d < 2 && d <= c->MN; ++d)
     for (int i = 0; i < 5 && k < max; ++i) {
       float t = 0.f;
-      if (cudaEventElapsedTime(&t, c->ev[6 * d + i], c->ev[6 * d + i + 1]) != cudaSuccess) t = -1.f;
+      if (cudaEventElapsedTime(&t, c->ev[6 * d + i], c->ev[6 * d + i + 1]) != cudaSuccess) {
+        t = -1.f;            // a phase that did not run since profiling was switched on
+        cudaGetLastError();  // (clear the error so that it does not surface in a later launch check)
+      }
       ms[k++] = t;
     }
   for (int i = 12; i < 16 && k < max; ++i) {
     float t = 0.f;
-    if (cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]) != cudaSuccess) t = -1.f;
+    if (cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]) != cudaSuccess) {
+      t = -1.f;
+      cudaGetLastError();
+    }
     ms[k++] = t;
   }
   return k;
@@ -783,7 +915,7 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   bem_qp_prepare(qpar, &q);
   double *wt = nullptr;
   if (cudaMalloc(&wt, BEM_WT_SIZE * sizeof(double)) != cudaSuccess) return -1;
-  if (bem_launch_wtab(q.k * q.eta0, wt, 0) != 0) { cudaFree(wt); return -1; }
+  if (bem_launch_wtab(q.k * q.eta_run, wt, 0) != 0) { cudaFree(wt); return -1; }
   q.wt = wt;
   q.wt_h = 0.125;
   q.wt_n = 64;

@@ -68,6 +68,7 @@ static void bem_qp_prepare(const double *p, bem_qp *q) {
   const double adp = sqrt(pow(q->d1x + q->d2x, 2) + pow(q->d1y + q->d2y, 2));
   const double adm = sqrt(pow(q->d1x - q->d2x, 2) + pow(q->d1y - q->d2y, 2));
   q->eta0 = sqrt(fabs(q->det) / (4.0 * M_PI) * adp / adm);
+  q->eta_run = q->eta0;
   q->nc1 = (int)round((q->kx * q->d1x + q->ky * q->d1y) / (2.0 * M_PI));
   // choice between the Ewald and the pure spectral sum (d3hm_qpgf_d2_v1)
   const double k2 = q->k * q->k;

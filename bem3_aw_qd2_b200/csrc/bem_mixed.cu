@@ -260,6 +260,7 @@ extern "C" void bem_mixed_free(bem_mixed *m) {
 }
 
 extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream_t st) {
+  CKB(cublasSetStream(m->blas, st));
   if (grow(m, &m->M, &m->M_cap, (size_t)n * n) || grow(m, &m->piv, &m->piv_cap, (size_t)n)) return -1;
   const size_t count = (size_t)n * n;
   k_round_c32<<<grid_for(count), 256, 0, st>>>((const double2 *)A, m->M, count);
@@ -270,6 +271,7 @@ extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream
 // B (n x nrhs, column-major complex FP64): right-hand sides in, solutions out
 extern "C" int bem_mixed_solve(bem_mixed *m, const double *A, int n, int nrhs, double *B, int max_iter, double tol,
                                int *iters, double *rel_corr, cudaStream_t st) {
+  CKB(cublasSetStream(m->blas, st));
   const size_t cnt = (size_t)n * nrhs;
   if (grow(m, &m->R32, &m->R32_cap, cnt) || grow(m, &m->X, &m->X_cap, cnt) || grow(m, &m->R, &m->R_cap, cnt) ||
       grow(m, &m->D, &m->D_cap, cnt))

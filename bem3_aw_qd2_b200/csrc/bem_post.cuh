@@ -355,7 +355,7 @@ extern "C" int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int perio
                                 const double *dpv, double *out, unsigned *status, cudaStream_t st) {
   if (npts <= 0) return 0;
   k_field<<<npts, FIELD_THREADS, 0, st>>>(*D, *q, periodic, k, type, pts, P, dP, pv, dpv, out, status);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_bdval(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int ntgt,
@@ -364,12 +364,12 @@ extern "C" int bem_launch_bdval(const bem_dom_dev *D, const bem_qp *q, int perio
                                 const double *dpv, double *out, unsigned *status, cudaStream_t st) {
   if (ntgt <= 0) return 0;
   k_bdval<<<ntgt, FIELD_THREADS, 0, st>>>(*D, *q, periodic, k, type, tgt_t, tgt_ze, P, dP, pv, dpv, out, status);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_force_bd(const bem_dom_dev *D, int ntgt, const int *tgt_t, const double *tgt_ze,
                                    const double *wts, const double *bdv, const double *pw, double k2r, double k2i,
                                    const double *rc, double c0, double rho0, double *out, cudaStream_t st) {
   k_force_bd<<<1, 256, 0, st>>>(*D, ntgt, tgt_t, tgt_ze, wts, bdv, pw, k2r, k2i, rc, c0, rho0, out);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }

@@ -152,7 +152,7 @@ __device__ __forceinline__ bool bem_small(cplx t, cplx s, double eps) {
 
 struct bem_gval { cplx g, gx, gy, gz; };
 
-// w(x + i y) from the per-problem table (x = k eta0, 0 <= y < 8): Clenshaw
+// w(x + i y) from the per-problem table (x = k eta_run, 0 <= y < 8): Clenshaw
 // recurrence on the interval's Chebyshev series.  Terms with y >= 8 are below
 // 1e-27 of the leading one and never reached by the stopping rule; they fall
 // back to the direct evaluation.
@@ -248,10 +248,12 @@ __device__ double bem_exp_cr(double a) {
 __device__ __forceinline__ double bem_an(double mk, int n1, double g1, int n2, double g2) {
   return __dadd_rn(__dadd_rn(mk, __dmul_rn((double)n1, g1)), __dmul_rn((double)n2, g2));
 }
-// Ewald parameter, capped where k^2 eta^2 - r^2 / 4 eta^2 > EW_EXPM (d3_qpgf_d2.c:1684-1697)
+// Ewald parameter, capped where k^2 eta^2 - r^2 / 4 eta^2 > EW_EXPM (d3_qpgf_d2.c:1684-1697).
+// On the lattice plane the reference's eta0 (its truncation there depends on it),
+// elsewhere eta_run (eta0 unless a tuned value is set: both sums converge).
 __device__ __forceinline__ double bem_ewald_eta(const bem_qp &q, double rx, double ry, double rz) {
   const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
-  const double ve = q.eta0, kk = __dmul_rn(q.k, q.k);
+  const double ve = rz == 0.0 ? q.eta0 : q.eta_run, kk = __dmul_rn(q.k, q.k);
   const double lhs = __dadd_rn(__dmul_rn(__dmul_rn(kk, ve), ve), -__ddiv_rn(r2, __dmul_rn(__dmul_rn(4.0, ve), ve)));
   if (lhs > BEM_EW_EXPM)
     return __ddiv_rn(__dsqrt_rn(__dadd_rn(BEM_EW_EXPM, __dsqrt_rn(__dadd_rn(__dmul_rn(kk, r2), BEM_EW_EXPM * BEM_EW_EXPM)))),
@@ -295,10 +297,12 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     }
     return 0;
   } else if (bn2 < 0.0) {
-    const double bn = sqrt(-bn2);
-    const double ebz = exp(bn * rz);
-    const double f1 = ebz * erfc(bn * ve + azve);
-    const double f2 = erfc(bn * ve - azve) / ebz;
+    // f1 = e^{bn z} erfc(bn ve + z/2ve), f2 = e^{-bn z} erfc(bn ve - z/2ve)
+    // = e^{-Q} erfcx(bn ve +- z/2ve) with Q = bn^2 ve^2 + (z/2ve)^2: one exp
+    const double bn = sqrt(-bn2), bv = bn * ve;
+    const double eq = exp(-(bv * bv + azve * azve));
+    const double f1 = eq * erfcx(bv + azve);
+    const double f2 = eq * erfcx(bv - azve);
     // Fn = ce / (i bn) (f1 + f2)
     Fn = cmul(ce, cmk(0.0, -(f1 + f2) / bn));
     dF0 = cscale(Fn, anx);
@@ -319,7 +323,7 @@ __device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.re, -a.im); }
 __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
   const double ve = bem_ewald_eta(q, rx, ry, rz);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
-  const bool tab = q.wt != nullptr && ve == q.eta0;  // table built for x = k eta0
+  const bool tab = q.wt != nullptr && ve == q.eta_run;  // table built for x = k eta_run
   const double eps = BEM_MEPS;
   int cc = 0;
   const cplx E2 = cexpi(q.kx * q.d2x + q.ky * q.d2y);  // exp(i k_par . d2)
@@ -522,7 +526,7 @@ __device__ __forceinline__ cplx cmuli(cplx a) { return cmk(-a.im, a.re); }  // i
 __device__ int bem_qpgf2_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval2 &o) {
   const double ve = bem_ewald_eta(q, rx, ry, rz);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
-  const bool tab = q.wt != nullptr && ve == q.eta0;
+  const bool tab = q.wt != nullptr && ve == q.eta_run;
   const double eps = BEM_MEPS, isp = 0.56418958354775628695;
   int cc = 0;
   const cplx E2 = cexpi(q.kx * q.d2x + q.ky * q.d2y);
@@ -623,9 +627,9 @@ __device__ int bem_qpgf2_ewald(const bem_qp &q, double rx, double ry, double rz,
             dzz = cmul(ce, cadd(cscale(cmuli(F), bn), cmk(c2pi * ef, 0.0)));
             e = 0;
           } else if (bn2 < 0.0) {
-            const double bn = sqrt(-bn2);
-            const double ebz = exp(bn * rz);
-            const double f1 = ebz * erfc(bn * ve + azve), f2 = erfc(bn * ve - azve) / ebz;
+            const double bn = sqrt(-bn2), bv = bn * ve;  // see ew_spec_term
+            const double eq = exp(-(bv * bv + azve * azve));
+            const double f1 = eq * erfcx(bv + azve), f2 = eq * erfcx(bv - azve);
             Fn = cmul(ce, cmk(0.0, -(f1 + f2) / bn));
             dz = cscale(ce, f1 - f2);
             dzz = cscale(ce, -bn * (f1 + f2) + c2pi * ef);

@@ -285,14 +285,14 @@ extern "C" int bem_launch_gather(const bem_sys_dev *S, int d, const double *G, c
   if (Nd == 0) return 0;
   if (A) k_gather<<<(unsigned)((Nd * Nd + 255) / 256), 256, 0, st>>>(*S, d, G, H, A);
   k_rhs<<<(unsigned)((Nd + 7) / 8), 256, 0, st>>>(*S, d, G, H, b);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_store(const bem_sys_dev *S, int d, const double *X, double *P, double *dP, cudaStream_t st) {
   const int n = S->dom_ne_h[d] * 4;
   if (n == 0) return 0;
   k_store<<<(n + 127) / 128, 128, 0, st>>>(*S, d, X, P, dP);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, const double *dH, const double *dF,
@@ -301,23 +301,23 @@ extern "C" int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, cons
   if (n == 0) return 0;
   if (d == 0) k_pv_exterior<<<(n + 127) / 128, 128, 0, st>>>(*S, tpv, pv);
   else k_pv_interior<<<(n + 7) / 8, 256, 0, st>>>(*S, d, dG, dH, dF, P, dP, pv, tpv);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_dpv_rhs(int Nd, const double *H, const double *pv, double *B, cudaStream_t st) {
   if (Nd == 0) return 0;
   k_dpv_rhs<<<(Nd + 7) / 8, 256, 0, st>>>(Nd, H, pv, B);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_dpv_store(int Nd, const double *B, double *dpv, cudaStream_t st) {
   if (Nd == 0) return 0;
   k_dpv_store<<<(Nd + 127) / 128, 128, 0, st>>>(Nd, B, dpv);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_force0(const bem_sys_dev *S, const double *P0, const double *pv0, const double *rc, double c0,
                                  double rho0, double *out, cudaStream_t st) {
   k_force0<<<1, 256, 0, st>>>(*S, P0, pv0, rc, c0, rho0, out);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }

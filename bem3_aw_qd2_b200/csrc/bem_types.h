@@ -27,13 +27,14 @@ typedef struct bem_qp {
   double det, idet, aidet;      /* det = d1 x d2, 1/det, |1/det| */
   double g1x, g1y, g2x, g2y;    /* reciprocal lattice vectors */
   double d2sq, g2sq, g1g2;      /* |d2|^2, |g2|^2, g1.g2 */
-  double eta0;                  /* Ewald splitting parameter before the per-point cap */
+  double eta0;                  /* the reference's Ewald splitting parameter (before the per-point cap) */
+  double eta_run;               /* the one used off the lattice plane (eta0 unless tuned) */
   double sel_cp, sel_bp;        /* spectral-only test: bN/bNp, bNp  */
   double sel_cm, sel_bm;        /*                     bN/bNm, bNm  */
   int nc1;                      /* round(k_par . d1 / 2 pi) */
   int ewald_only;               /* 1: always use the Ewald sum */
   /* optional table of w(x + i y) for the Ewald real-space terms at
-     x = k eta0: piecewise Chebyshev, wt_n intervals of width wt_h on
+     x = k eta_run: piecewise Chebyshev, wt_n intervals of width wt_h on
      y in [0, wt_n wt_h), BEM_WT_DEG (re, im) coefficients each; NULL: none */
   const double *wt;
   double wt_h;

@@ -73,6 +73,20 @@ unsigned bemgpu_status(bemgpu_ctx *ctx); /* BEMGPU_ST_* bits accumulated since l
  * read_aqd2/initialize_aqd2 build, bem3_aw_qd2.c:3-109). */
 int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
 
+/* Ewald splitting parameter used off the lattice plane: eta0 x scale, where
+ * eta0 is the reference's (d3_qpgf_d2.c:1683-1693; the per-point cap still
+ * applies).  Both lattice sums converge to the reference's 1e-15 tolerance for
+ * any scale, so the results agree to round-off while the split of the terms
+ * between the real-space and spectral sums, and so the cost, changes.  On the
+ * lattice plane (z = 0) eta0 is always used.  Default 1; kept across loads. */
+int bemgpu_set_ewald_scale(bemgpu_ctx *ctx, double scale);
+
+/* Autotuner of the Ewald parameter for the loaded problem: times the periodic
+ * regular-pair kernel on an eighth of the pairs for scales 1.0, 1.1, 1.2, 1.3
+ * of eta0 and sets the fastest (bemgpu_set_ewald_scale); *best_scale gets it.
+ * Costs about half of one regular-pair launch. */
+int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
+
 /* Free the loaded problem's device memory (the context stays usable). */
 int bemgpu_unload(bemgpu_ctx *ctx);
 
