@@ -50,6 +50,14 @@ __device__ __forceinline__ void bem_load_node(const bem_dom_dev &D, int p, bem_n
 
 __device__ __forceinline__ double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
+// element e (0-based) is a linear triangle
+__device__ __forceinline__ bool bem_is_tri(const bem_dom_dev &D, int e) { return D.has_tri && __ldg(D.npe + e) == 3; }
+// row p = 4 t + 3 of a triangle t is padding: the reference leaves it zero
+// (create_cmatrix_domain computes tn < 3 for triangles, bem3_aw_qd2_solve_bieq.c:160-161)
+__device__ __forceinline__ bool bem_pad_row(const bem_dom_dev &D, int p) {
+  return (p & 3) == 3 && bem_is_tri(D, abs(D.sid[p >> 2]) - 1);
+}
+
 __device__ __forceinline__ void set_status(unsigned *st, unsigned bits) { if (bits) atomicOr(st, bits); }
 
 // warp-aggregated work counters (lattice terms and Green's-function points);
@@ -86,6 +94,14 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restr
                                                    int *__restrict__ near_s, int *__restrict__ near_n,
                                                    uint8_t *__restrict__ flag, unsigned *status) {
   const int p = blockIdx.x;
+  if (bem_pad_row(D, p)) {
+    for (int s = threadIdx.x; s < D.ne; s += blockDim.x) flag[(size_t)p * D.ne + s] = 0;
+    if (threadIdx.x == 0) {
+      near_n[p] = 0;
+      rowF[3 * p] = rowF[3 * p + 1] = rowF[3 * p + 2] = 0.0;
+    }
+    return;
+  }
   bem_node nd;
   int t, te;
   bem_load_node(D, p, nd, t, te);
@@ -103,23 +119,30 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restr
     } else {
       bem_el el;
       bem_load_el(D.cr, D.cw, se, el);
+      const bool tri = bem_is_tri(D, se);
       double F = 0, Fz = 0, Fe = 0;
-      for (int i = 0; i < BEM_GLN; ++i) {
-        double f = 0, fz = 0, fe = 0;
-        for (int j = 0; j < BEM_GLN; ++j) {
-          double vR[3], vW[3];
-          bem_rw(el, c_q.xl[i], c_q.xl[j], vR, vW);
-          for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
-          double a, b, c;
-          geomF(vR, vW, nd, a, b, c);
-          f += c_q.wl[j] * a;
-          fz += c_q.wl[j] * b;
-          fe += c_q.wl[j] * c;
+      for (int part = 0; part < (tri ? 3 : 1); ++part)
+        for (int i = 0; i < BEM_GLN; ++i) {
+          double f = 0, fz = 0, fe = 0;
+          for (int j = 0; j < BEM_GLN; ++j) {
+            double z = c_q.xl[i], e = c_q.xl[j], wf = 1.0;
+            if (tri) {
+              bem_tri_point(part, z, e, z, e);
+              wf = bem_tri_wfac(c_q.xl[i], c_q.xl[j]);
+            }
+            double vR[3], vW[3];
+            bem_rw(el, z, e, vR, vW);
+            for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+            double a, b, c;
+            geomF(vR, vW, nd, a, b, c);
+            f += c_q.wl[j] * wf * a;
+            fz += c_q.wl[j] * wf * b;
+            fe += c_q.wl[j] * wf * c;
+          }
+          F += c_q.wl[i] * f;
+          Fz += c_q.wl[i] * fz;
+          Fe += c_q.wl[i] * fe;
         }
-        F += c_q.wl[i] * f;
-        Fz += c_q.wl[i] * fz;
-        Fe += c_q.wl[i] * fe;
-      }
       F *= BEM_I_FP; Fz *= BEM_I_FP; Fe *= BEM_I_FP;
       if (D.sid[s] < 0) { F = -F; Fz = -Fz; Fe = -Fe; }  // bil_convert_CC / _dCC
       if (fabs(Fz) > BEM_CBD_SDF || fabs(Fe) > BEM_CBD_SDF) {
@@ -167,7 +190,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, double *__restr
 #ifndef RP_MINB
 #define RP_MINB 2  // two blocks (18 warps) per SM: caps registers at 113
 #endif
-__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, bem_qp q, const uint8_t *__restrict__ flag,
+__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, const __grid_constant__ bem_qp q, const uint8_t *__restrict__ flag,
                                                            double *__restrict__ G, double *__restrict__ H,
                                                            unsigned *status, unsigned long long *terms, long long pair0,
                                                            long long npairs) {
@@ -177,7 +200,8 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
   const bool valid = pair < pair0 + npairs;
   const int p = valid ? (int)(pair / D.ne) : 0;
   const int s = valid ? (int)(pair % D.ne) : 0;
-  const bool work = valid && flag[(size_t)p * D.ne + s] == 0;
+  // triangle sources are k_q0_regular_tri's; padded rows keep their zeros
+  const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && !bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
   double v[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = 0.0;
@@ -221,7 +245,82 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
     const long long pr = pair0 + 2LL * blockIdx.x + q2;
     if (pr < pair0 + npairs) {
       const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
-      if (flag[(size_t)pp * D.ne + ss] == 0) {
+      if (flag[(size_t)pp * D.ne + ss] == 0 && !bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
+        double sum = 0.0;
+        for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
+        const size_t N = (size_t)D.ne * 4;
+        double *dst = c < 8 ? G : H;
+        const int a = (c & 7) >> 1, part = c & 1;
+        dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+      }
+    }
+  }
+}
+
+// Triangle sources (q0_lit_dcoef_v2_cc_GL, q0_lit_dcoef_v2_cc.c:156-237 with
+// q0_lit_sdqGHF_v2_cc_zeta_eta, :345-381): 3 parts x 12 x 12 points; a thread
+// takes the 3 parts of one (a, b) point, 2 pairs per 288-thread block.
+__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_dev D, const __grid_constant__ bem_qp q,
+                                                               const uint8_t *__restrict__ flag, double *__restrict__ G,
+                                                               double *__restrict__ H, unsigned *status,
+                                                               unsigned long long *terms, long long pair0,
+                                                               long long npairs) {
+  __shared__ double acc[16][RP_THREADS + 1];
+  const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
+  const long long pair = pair0 + 2LL * blockIdx.x + lp;
+  const bool valid = pair < pair0 + npairs;
+  const int p = valid ? (int)(pair / D.ne) : 0;
+  const int s = valid ? (int)(pair % D.ne) : 0;
+  const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  unsigned long long nterm = 0, npt = 0;
+  if (work) {
+    bem_node nd;
+    int t, te;
+    bem_load_node(D, p, nd, t, te);
+    bem_el el;
+    bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+    const int i = pt / BEM_GLN, j = pt % BEM_GLN;
+    const double a = c_q.xl[i], b = c_q.xl[j];
+    const double wt = c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(a, b);
+    unsigned st = 0;
+    for (int part = 0; part < 3; ++part) {
+      double z, e, vR[3], vW[3];
+      bem_tri_point_ref(part, a, b, z, e);
+      bem_rw_ref(el, z, e, vR, vW);
+      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+      if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+      const cplx g = cscale(gv.g, aW * wt);
+      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+      double N[4];
+      bem_Nn3(z, e, N);
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        v[2 * n] += g.re * N[n];
+        v[2 * n + 1] += g.im * N[n];
+        v[8 + 2 * n] += h.re * N[n];
+        v[8 + 2 * n + 1] += h.im * N[n];
+      }
+    }
+    set_status(status, st);
+  }
+  count_work(terms + 0, nterm, npt);
+#pragma unroll
+  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
+    const long long pr = pair0 + 2LL * blockIdx.x + q2;
+    if (pr < pair0 + npairs) {
+      const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
+      if (flag[(size_t)pp * D.ne + ss] == 0 && bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
         double sum = 0.0;
         for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
         const size_t N = (size_t)D.ne * 4;
@@ -236,6 +335,15 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
 // ------------------------------------------------------------------ periodic near-singular pairs
 // 64x64 points (q0_bil_dcoef_v2_cc_GH, q0_bil_dcoef_v2_cc.c:206-281).
 #define NP_THREADS 256
+// register cap of the periodic near-singular and self kernels (0: compiler's choice)
+#ifndef NP_MAXREG
+#define NP_MAXREG 0
+#endif
+#if NP_MAXREG > 0
+#define NP_BOUNDS __maxnreg__(NP_MAXREG)
+#else
+#define NP_BOUNDS __launch_bounds__(NP_THREADS)
+#endif
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*NP_THREADS */) {
 #pragma unroll
@@ -257,7 +365,7 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*N
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q, const int *__restrict__ near_s,
+__global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_qp q, const int *__restrict__ near_s,
                                                         const int *__restrict__ near_n, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ nearF, unsigned *status,
                                                         unsigned long long *terms) {
@@ -268,29 +376,38 @@ __global__ void __launch_bounds__(NP_THREADS) k_q0_near(bem_dom_dev D, bem_qp q,
   int t, te;
   bem_load_node(D, p, nd, t, te);
   bem_el el;
-  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  const int se = abs(D.sid[s]) - 1;
+  bem_load_el(D.cr, D.cw, se, el);
+  const bool tri = bem_is_tri(D, se);  // q0_lit_dcoef_v2_cc_GH: 3 parts x 64 x 64
   double v[19];
 #pragma unroll
   for (int c = 0; c < 19; ++c) v[c] = 0.0;
   unsigned st = 0;
   unsigned long long nterm = 0, npt = 0;
-  for (int pt = threadIdx.x; pt < BEM_GHN * BEM_GHN; pt += NP_THREADS) {
-    const int i = pt / BEM_GHN, j = pt % BEM_GHN;
-    const double z = c_q.xh[i], e = c_q.xh[j];
+  for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+    const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
+    const int i = ij / BEM_GHN, j = ij % BEM_GHN;
+    double z = c_q.xh[i], e = c_q.xh[j], wt = c_q.wh[i] * c_q.wh[j];
     double vR[3], vW[3];
-    bem_rw(el, z, e, vR, vW);
-    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+    if (tri) {
+      bem_tri_point_ref(part, c_q.xh[i], c_q.xh[j], z, e);
+      wt *= bem_tri_wfac(c_q.xh[i], c_q.xh[j]);
+      bem_rw_ref(el, z, e, vR, vW);
+      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
+    } else {
+      bem_rw(el, z, e, vR, vW);
+      for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+    }
     bem_gval gv;
     const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
     nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
     ++npt;
     const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-    const double wt = c_q.wh[i] * c_q.wh[j];
     const cplx g = cscale(gv.g, aW * wt);
     const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
     double N[4];
-    bem_Nn4(z, e, N);
+    bem_Nn(tri, z, e, N);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       v[2 * a] += g.re * N[a];
@@ -365,12 +482,13 @@ __device__ __forceinline__ double bem_bdC(const bem_el &el) {
 }
 
 // periodic self pair: one block per collocation node p
-__global__ void __launch_bounds__(NP_THREADS) k_q0_self(bem_dom_dev D, bem_qp q, double *__restrict__ G,
+__global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_qp q, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ selfF,
                                                         unsigned *status, unsigned long long *terms) {
   const int p = blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
+  if (bem_is_tri(D, te)) return;  // k_q0_self_tri
   bem_el el;
   bem_load_el(D.cr, D.cw, te, el);
   const double zt = c_q.zt[tn], et = c_q.et[tn];
@@ -469,7 +587,8 @@ __device__ __forceinline__ void fs_zero(fs_acc &a) {
   a.f = a.fz = a.fe = 0.0;
 }
 
-__device__ __forceinline__ void fs_point(const bem_el &el, const bem_node &nd, double k, double z, double e, double wt, fs_acc &a) {
+__device__ __forceinline__ void fs_point(const bem_el &el, const bem_node &nd, double k, double z, double e, double wt, fs_acc &a,
+                                         bool tri = false) {
   double vR[3], vW[3];
   bem_rw(el, z, e, vR, vW);
   for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
@@ -484,7 +603,7 @@ __device__ __forceinline__ void fs_point(const bem_el &el, const bem_node &nd, d
   const double Wdz = dot3(vW, nd.vz), Wde = dot3(vW, nd.vt);
   const double i3 = iR * iR * iR;
   double N[4];
-  bem_Nn4(z, e, N);
+  bem_Nn(tri, z, e, N);
   const cplx cbce = cmul(cb, ce);
   const cplx g = cscale(ce, iR * aW * wt);                       // e^{ikR}/R |W|
   const cplx h = cscale(cbce, tD * wt);                          // (ikR-1) e^{ikR} (R.W)/R^3
@@ -539,16 +658,28 @@ __global__ void __launch_bounds__(128) k_fs_regular(bem_dom_dev D, double k, con
   const long long total = (long long)D.ne * 4 * D.ne;
   if (pair >= total) return;
   const int p = (int)(pair / D.ne), s = (int)(pair % D.ne);
-  if (flag[pair] != 0) return;
+  if (flag[pair] != 0 || bem_pad_row(D, p)) return;
   bem_node nd;
   int t, te;
   bem_load_node(D, p, nd, t, te);
   bem_el el;
-  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  const int se = abs(D.sid[s]) - 1;
+  bem_load_el(D.cr, D.cw, se, el);
   fs_acc a;
   fs_zero(a);
-  for (int i = 0; i < BEM_GLN; ++i)
-    for (int j = 0; j < BEM_GLN; ++j) fs_point(el, nd, k, c_q.xl[i], c_q.xl[j], c_q.wl[i] * c_q.wl[j], a);
+  if (bem_is_tri(D, se)) {
+    // lit_dcoef_v2_GL (lit_dcoef_v2.c:185-270): 3 parts x 12 x 12
+    for (int part = 0; part < 3; ++part)
+      for (int i = 0; i < BEM_GLN; ++i)
+        for (int j = 0; j < BEM_GLN; ++j) {
+          double z, e;
+          bem_tri_point(part, c_q.xl[i], c_q.xl[j], z, e);
+          fs_point(el, nd, k, z, e, c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(c_q.xl[i], c_q.xl[j]), a, true);
+        }
+  } else {
+    for (int i = 0; i < BEM_GLN; ++i)
+      for (int j = 0; j < BEM_GLN; ++j) fs_point(el, nd, k, c_q.xl[i], c_q.xl[j], c_q.wl[i] * c_q.wl[j], a);
+  }
   fs_store(D, p, s, a, G, H, dG, dH);
 }
 
@@ -564,12 +695,21 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k,
   int t, te;
   bem_load_node(D, p, nd, t, te);
   bem_el el;
-  bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+  const int se = abs(D.sid[s]) - 1;
+  bem_load_el(D.cr, D.cw, se, el);
+  const bool tri = bem_is_tri(D, se);  // lit_dcoef_v2_GH: 3 parts x 64 x 64
   fs_acc a;
   fs_zero(a);
-  for (int pt = threadIdx.x; pt < BEM_GHN * BEM_GHN; pt += NP_THREADS) {
-    const int i = pt / BEM_GHN, j = pt % BEM_GHN;
-    fs_point(el, nd, k, c_q.xh[i], c_q.xh[j], c_q.wh[i] * c_q.wh[j], a);
+  for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+    const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
+    const int i = ij / BEM_GHN, j = ij % BEM_GHN;
+    if (tri) {
+      double z, e;
+      bem_tri_point(part, c_q.xh[i], c_q.xh[j], z, e);
+      fs_point(el, nd, k, z, e, c_q.wh[i] * c_q.wh[j] * bem_tri_wfac(c_q.xh[i], c_q.xh[j]), a, true);
+    } else {
+      fs_point(el, nd, k, c_q.xh[i], c_q.xh[j], c_q.wh[i] * c_q.wh[j], a);
+    }
   }
   __shared__ double sm[51 * (NP_THREADS / 32) + 51];
   double *av = reinterpret_cast<double *>(&a);
@@ -610,6 +750,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k,
   const int p = blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
+  if (bem_is_tri(D, te)) return;  // k_fs_self_tri
   bem_el el;
   bem_load_el(D.cr, D.cw, te, el);
   const double zt = c_q.zt[tn], et = c_q.et[tn];
@@ -820,12 +961,213 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k,
   }
 }
 
+// ------------------------------------------------------------------ triangle self pairs
+// Periodic: q0_lit_coef_bd (q0_lit_coef.c:297-371): polar rule around the node
+// over the 3 sub-triangles, G and H (F = 0: the element is plane; the
+// tangential derivatives vanish too, q0_lit_dcoef_bd_vt2_cc_DV).  With the
+// Jacobian vector J = cw0 2 / (3 sqrt3) the integrands are the quad kernel's.
+__global__ void NP_BOUNDS k_q0_self_tri(bem_dom_dev D, const __grid_constant__ bem_qp q, double *__restrict__ G,
+                                        double *__restrict__ H, double *__restrict__ selfF, unsigned *status,
+                                        unsigned long long *terms) {
+  const int p = blockIdx.x;
+  const int t = p >> 2, tn = p & 3;
+  const int te = abs(D.sid[t]) - 1;
+  if (!bem_is_tri(D, te) || tn == 3) return;
+  bem_el el;
+  bem_load_el(D.cr, D.cw, te, el);
+  double zt, et, r[5], th[5];
+  bem_tri_node(tn, zt, et);
+  bem_tri_node_r_th(zt, et, r, th);
+  double J[3];
+  for (int d = 0; d < 3; ++d) J[d] = el.cw[d][0] * (2.0 / (3.0 * BEM_SQ3));
+  const double aJ = sqrt(dot3(J, J));
+  double v[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  unsigned st = 0;
+  unsigned long long nterm = 0, npt = 0;
+  for (int pt = threadIdx.x; pt < 384 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+    const double w = tp.wth * 0.5 * rm * c_q.wl[ir];
+    const double z = rr * cth + zt, e = rr * sth + et;
+    double K[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    bem_gval gv;
+    const int rc = bem_qpgf(q, rr * K[0], rr * K[1], rr * K[2], gv);
+    if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+    ++npt;
+    const cplx g = cscale(gv.g, aJ * rr * w);
+    const cplx h = cscale(cadd(cadd(cscale(gv.gx, J[0]), cscale(gv.gy, J[1])), cscale(gv.gz, J[2])), rr * w);
+    double N[4];
+    bem_Nn3(z, e, N);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      v[2 * a] += g.re * N[a];
+      v[2 * a + 1] += g.im * N[a];
+      v[8 + 2 * a] += h.re * N[a];
+      v[8 + 2 * a + 1] += h.im * N[a];
+    }
+  }
+  count_work(terms + 2, nterm, npt);
+  set_status(status, st);
+  __shared__ double sm[16 * (NP_THREADS / 32) + 16];
+  block_reduce<16>(v, sm);
+  if (threadIdx.x < 16) {
+    const size_t N = (size_t)D.ne * 4;
+    const int c = threadIdx.x;
+    double *dst = c < 8 ? G : H;
+    const int a = (c & 7) >> 1, part = c & 1;
+    dst[2 * ((size_t)p * N + 4 * t + a) + part] = v[c];
+  } else if (threadIdx.x < 19) {
+    selfF[3 * p + (threadIdx.x - 16)] = 0.0;
+  }
+}
+
+// Free space: lit_coef_bd (lit_coef.c:290-350) for G (H, F vanish on the plane
+// element) and the principal-value tangential derivatives of G,
+// lit_dcoef_bd_tz0_PV / _te0_PV (lit_dcoef.c:461-640, integrands :858-950):
+// D-bar-eps (polar, 64 radii from DEPS to the edge), D-eps (closed form in the
+// radius over [-pi, pi)) and the PV pair (over [0, pi)); dH vanishes.
+__global__ void __launch_bounds__(NP_THREADS) k_fs_self_tri(bem_dom_dev D, double k, double *__restrict__ G,
+                                                            double *__restrict__ H, double *__restrict__ dG,
+                                                            double *__restrict__ dH, double *__restrict__ selfF,
+                                                            unsigned *status) {
+  const int p = blockIdx.x;
+  const int t = p >> 2, tn = p & 3;
+  const int te = abs(D.sid[t]) - 1;
+  if (!bem_is_tri(D, te) || tn == 3) return;
+  bem_el el;
+  bem_load_el(D.cr, D.cw, te, el);
+  double zt, et, r[5], th[5];
+  bem_tri_node(tn, zt, et);
+  bem_tri_node_r_th(zt, et, r, th);
+  double vz[3], ve[3], cw0[3];
+  for (int d = 0; d < 3; ++d) {
+    vz[d] = el.cr[d][1];
+    ve[d] = el.cr[d][2];
+    cw0[d] = el.cw[d][0];
+  }
+  const double aJ = sqrt(dot3(cw0, cw0)) * (2.0 / (3.0 * BEM_SQ3));
+  // accumulators: G (8), dGz (8), dGe (8)
+  double v[24];
+#pragma unroll
+  for (int c = 0; c < 24; ++c) v[c] = 0.0;
+  unsigned st = 0;
+  // (1) G: 3 x 128 angles x 12 radii from 0 to the edge (lit_sG_r: e^{ik aK r} / aK N)
+  for (int pt = threadIdx.x; pt < 384 * BEM_GLN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+    const double w = tp.wth * 0.5 * rm * c_q.wl[ir];
+    double K[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    const double aK = sqrt(dot3(K, K));
+    const cplx g = cscale(cexpi(k * aK * rr), w / aK);
+    double N[4];
+    bem_Nn3(rr * cth + zt, rr * sth + et, N);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { v[2 * n] += g.re * N[n]; v[2 * n + 1] += g.im * N[n]; }
+  }
+  // (2) D-bar-eps: 3 x 128 angles x 64 radii from DEPS to the edge (lit_sdG_Db_r)
+  for (int pt = threadIdx.x; pt < 384 * BEM_GHN; pt += NP_THREADS) {
+    const int idx = pt / BEM_GHN, ir = pt % BEM_GHN;
+    const polar_pt tp = polar_theta(th, idx);
+    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
+    double sth, cth;
+    sincos(tp.th, &sth, &cth);
+    const double rr = 0.5 * (rm - BEM_DEPS) * c_q.xh[ir] + 0.5 * (rm + BEM_DEPS);
+    const double w = tp.wth * 0.5 * (rm - BEM_DEPS) * c_q.wh[ir];
+    double K[3];
+    bem_K(el, rr, cth, sth, zt, et, K);
+    const double aK = sqrt(dot3(K, K)), iK = 1.0 / aK;
+    const double kR = k * aK * rr;
+    const cplx cbce = cmul(cmk(-1.0, kR), cexpi(kR));
+    const double f = w / rr * iK * iK * iK;  // (K.v / aK) / aK^2 / r
+    const cplx gz = cscale(cbce, f * dot3(K, vz)), ge = cscale(cbce, f * dot3(K, ve));
+    double N[4];
+    bem_Nn3(rr * cth + zt, rr * sth + et, N);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      v[8 + 2 * n] += gz.re * N[n];  v[8 + 2 * n + 1] += gz.im * N[n];
+      v[16 + 2 * n] += ge.re * N[n]; v[16 + 2 * n + 1] += ge.im * N[n];
+    }
+  }
+  // (3) D-eps, times i/k: 4 x 64 angles over [-pi, pi) (lit_sdG_De_theta)
+  // (4) PV pair, times -1/k: 2 x 64 angles over [0, pi) (lit_sdG_DP_theta)
+  for (int idx = threadIdx.x; idx < 384; idx += NP_THREADS) {
+    const bool de = idx < 256;
+    const int qd = de ? idx >> 6 : (idx - 256) >> 6, m = idx & 63;
+    const double tht = 0.25 * CUDART_PI * c_q.xh[m] + (de ? (-0.75 + 0.5 * qd) : (0.25 + 0.5 * qd)) * CUDART_PI;
+    const double wth = 0.25 * CUDART_PI * c_q.wh[m];
+    double sth, cth;
+    sincos(tht, &sth, &cth);
+    double K[3];
+    for (int d = 0; d < 3; ++d) K[d] = el.cr[d][1] * cth + el.cr[d][2] * sth;
+    const double aK = sqrt(dot3(K, K)), iK = 1.0 / aK;
+    const double keK = k * BEM_DEPS * aK;
+    double sk, ck;
+    sincos(keK, &sk, &ck);
+    double dN[4];
+    bem_dNn3(cth, sth, dN);
+    const double i4 = iK * iK * iK * iK;  // (K.v / aK) / aK^3
+    cplx f;
+    if (de) {
+      // (keK + i) sin keK + (2 - i keK) cos keK - 2, times i / k
+      const cplx c = cmk(keK * sk + 2.0 * ck - 2.0, sk - keK * ck);
+      f = cscale(cmk(-c.im, c.re), wth * i4 / k);
+    } else {
+      f = cmk(-wth * i4 * sk / k, 0.0);
+    }
+    const cplx gz = cscale(f, dot3(K, vz)), ge = cscale(f, dot3(K, ve));
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      v[8 + 2 * n] += gz.re * dN[n];  v[8 + 2 * n + 1] += gz.im * dN[n];
+      v[16 + 2 * n] += ge.re * dN[n]; v[16 + 2 * n + 1] += ge.im * dN[n];
+    }
+  }
+  set_status(status, st);
+  __shared__ double sm[24 * (NP_THREADS / 32) + 24];
+  block_reduce<24>(v, sm);
+  if (threadIdx.x == 0) {
+    const size_t N = (size_t)D.ne * 4;
+    const double c = BEM_I_FP * aJ;
+    const double iTz = 1.0 / sqrt(dot3(vz, vz)), iTe = 1.0 / sqrt(dot3(ve, ve));
+    double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
+    double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
+    double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * t));
+    double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
+    double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * t));
+    double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
+    for (int n = 0; n < 4; ++n) {
+      g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
+      h2[n] = make_double2(0.0, 0.0);
+      gz[n] = make_double2(-c * iTz * v[8 + 2 * n], -c * iTz * v[8 + 2 * n + 1]);
+      ge[n] = make_double2(-c * iTe * v[16 + 2 * n], -c * iTe * v[16 + 2 * n + 1]);
+      hz[n] = make_double2(0.0, 0.0);
+      he[n] = make_double2(0.0, 0.0);
+    }
+    selfF[3 * p] = selfF[3 * p + 1] = selfF[3 * p + 2] = 0.0;
+  }
+}
+
 // ------------------------------------------------------------------ diagonal / dF
 __global__ void k_diag(bem_dom_dev D, int exterior, const double *__restrict__ rowF, const int *__restrict__ near_n,
                        const double *__restrict__ nearF, const double *__restrict__ selfF, double *__restrict__ H,
                        double *__restrict__ dF, unsigned *status) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= D.ne * 4) return;
+  if (p >= D.ne * 4 || bem_pad_row(D, p)) return;
   double F = rowF[3 * p], Fz = rowF[3 * p + 1], Fe = rowF[3 * p + 2];
   const int n = near_n[p];
   for (int k = 0; k < n; ++k) {
@@ -851,7 +1193,7 @@ __global__ void k_faddeeva(const double *__restrict__ z, int n, double *__restri
   w[2 * i + 1] = r.im;
 }
 
-__global__ void __launch_bounds__(128) k_qpgf_points(bem_qp q, const double *__restrict__ r, int n, double *__restrict__ G,
+__global__ void __launch_bounds__(128) k_qpgf_points(const __grid_constant__ bem_qp q, const double *__restrict__ r, int n, double *__restrict__ G,
                                                      double *__restrict__ dG, int *__restrict__ ret) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -934,6 +1276,17 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   // ev (optional): 6 events recorded around classify | regular | near | self | diag
   const int N = D->ne * 4;
   if (D->ne <= 0) return 0;
+  if (D->has_tri) {
+    // triangles leave padding rows and columns zero (the reference's calloc'ed matrices)
+    const size_t nn = (size_t)N * N;
+    if (cudaMemsetAsync(G, 0, 2 * nn * sizeof(double), st) != cudaSuccess ||
+        cudaMemsetAsync(H, 0, 2 * nn * sizeof(double), st) != cudaSuccess ||
+        cudaMemsetAsync(dF, 0, 3 * (size_t)N * sizeof(double), st) != cudaSuccess)
+      return -1;
+    if (dG && (cudaMemsetAsync(dG, 0, 4 * nn * sizeof(double), st) != cudaSuccess ||
+               cudaMemsetAsync(dH, 0, 4 * nn * sizeof(double), st) != cudaSuccess))
+      return -1;
+  }
   if (ev) cudaEventRecord(ev[0], st);
   k_classify<<<N, 128, 0, st>>>(*D, S->rowF, S->near_s, S->near_n, S->flag, S->status);
   if (ev) cudaEventRecord(ev[1], st);
@@ -943,17 +1296,22 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
     for (long long p0 = 0; p0 < npairs; p0 += chunk) {
       const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
       k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+      if (D->has_tri)
+        k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0,
+                                                                          np);
     }
     if (ev) cudaEventRecord(ev[2], st);
     k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
     if (ev) cudaEventRecord(ev[3], st);
     k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+    if (D->has_tri) k_q0_self_tri<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
   } else {
     k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
     if (ev) cudaEventRecord(ev[2], st);
     k_fs_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
     if (ev) cudaEventRecord(ev[3], st);
     k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+    if (D->has_tri) k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
   }
   if (ev) cudaEventRecord(ev[4], st);
   k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, exterior, S->rowF, S->near_n, S->nearF, S->selfF, H, dF, S->status);

@@ -26,7 +26,7 @@ struct bemgpu_ctx {
   bool loaded = false;
   int Ne = 0, NN = 0, MN = 0, n = 0;
   bem_qp qp;
-  std::vector<int> dom_ne, dom_off;
+  std::vector<int> dom_ne, dom_off, dom_tri;
   std::vector<double> k0, c0, rho0, k2;
   // device problem data
   double *cr = nullptr, *cw = nullptr, *ren = nullptr, *wen = nullptr;
@@ -53,6 +53,10 @@ struct bemgpu_ctx {
   int ntgt = 0;
   int *tgt_t = nullptr;
   double *tgt_ze = nullptr, *tgt_w = nullptr, *bdv = nullptr;
+  // centres of the domain-0 triangles for the 4-point force rule
+  int nctr = 0;
+  int *ctr_t = nullptr, *ctr_idx = nullptr;
+  double *ctr_ze = nullptr, *ctr_bdv = nullptr;
   // staging buffers of the point evaluators (grown on demand, kept until destroy)
   size_t pt_cap = 0;
   double *pt_in = nullptr, *pt_out = nullptr;
@@ -69,6 +73,11 @@ struct bemgpu_ctx {
   bool mx_ready[BEMGPU_MAXDOM + 1] = {};
   // FP64 factors: the global system in A (ipiv), domain d's dpv system in Wd[d] (ipd[d])
   double *Wd[BEMGPU_MAXDOM] = {};
+  // domains with triangles: the dpv system without padding (compact -> full index, size, matrix)
+  int *cinv[BEMGPU_MAXDOM] = {};
+  int cn[BEMGPU_MAXDOM] = {};
+  double *Gc[BEMGPU_MAXDOM] = {};
+  double *B3c = nullptr;
   int64_t *ipd[BEMGPU_MAXDOM] = {};
   bool fac_fp64[BEMGPU_MAXDOM + 1] = {};
   bool factored = false;  // factors of the current matrices are held (bemgpu_solve_rhs may run)
@@ -128,9 +137,15 @@ static void free_problem(bemgpu_ctx *c) {
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
   dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->b0); dfree(c->B3s);
-  for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); }
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
+    dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]);
+    c->cn[d] = 0;
+  }
+  dfree(c->B3c);
   c->factored = false;
   dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
+  dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
+  c->nctr = 0;
   c->ntgt = 0;
   if (c->dwork) cudaFree(c->dwork);
   c->dwork = nullptr;
@@ -266,7 +281,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   if (pr->MN + 1 > BEMGPU_MAXDOM) { snprintf(c->err, sizeof(c->err), "at most %d domains", BEMGPU_MAXDOM); return -2; }
   if (pr->ps != 1) { snprintf(c->err, sizeof(c->err), "only the quasi-periodic problem (ps=1) is implemented"); return -2; }
   for (int e = 0; e < pr->Ne; ++e)
-    if (pr->npe[e] != 4) { snprintf(c->err, sizeof(c->err), "element %d: only bilinear (4-node) elements are implemented", e + 1); return -2; }
+    if (pr->npe[e] != 4 && pr->npe[e] != 3) { snprintf(c->err, sizeof(c->err), "element %d: %d nodes (3 or 4 expected)", e + 1, pr->npe[e]); return -2; }
   if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   bem_qp_prepare(pr->qp, &c->qp);
@@ -283,6 +298,10 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   c->dom_off.assign(nd, 0);
   int tot = 0;
   for (int d = 0; d < nd; ++d) { c->dom_off[d] = tot; tot += c->dom_ne[d]; }
+  c->dom_tri.assign(nd, 0);
+  for (int d = 0; d < nd; ++d)
+    for (int s2 = 0; s2 < c->dom_ne[d]; ++s2)
+      if (pr->npe[abs(pr->sid[c->dom_off[d] + s2]) - 1] == 3) c->dom_tri[d] = 1;
   c->k0.assign(pr->k0, pr->k0 + nd);
   c->c0.assign(pr->c0, pr->c0 + nd);
   c->rho0.assign(pr->rho0, pr->rho0 + nd);
@@ -353,6 +372,18 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     const size_t N = 4 * (size_t)c->dom_ne[d];
     CK(dalloc(&c->Wd[d], 2 * N * N), "dpv factors");
     CK(dalloc(&c->ipd[d], N), "dpv pivots");
+    c->cn[d] = (int)N;
+    if (c->dom_tri[d]) {
+      std::vector<int> inv;
+      for (int s2 = 0; s2 < c->dom_ne[d]; ++s2) {
+        const int npe = pr->npe[abs(pr->sid[c->dom_off[d] + s2]) - 1];
+        for (int l = 0; l < npe; ++l) inv.push_back(4 * s2 + l);
+      }
+      c->cn[d] = (int)inv.size();
+      if (upload(c, &c->cinv[d], inv.data(), inv.size(), "dpv index")) return -1;
+      CK(dalloc(&c->Gc[d], 2 * inv.size() * inv.size()), "dpv matrix");
+      if (!c->B3c) CK(dalloc(&c->B3c, 6 * (size_t)maxN), "dpv rhs");
+    }
   }
   CK(dalloc(&c->B3, 6 * (size_t)maxN), "B3");
   CK(dalloc(&c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
@@ -427,14 +458,13 @@ extern "C" int bemgpu_unload(bemgpu_ctx *c) {
   return 0;
 }
 
+static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
+
 extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
   c->factored = false;
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   for (int d = 0; d <= c->MN; ++d) {
-    bem_dom_dev D;
-    D.ne = c->dom_ne[d];
-    D.sid = c->sid + c->dom_off[d];
-    D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane;
+    bem_dom_dev D = dom_view(c, d);
     const int periodic = d == 0;
     cudaEvent_t *ev = c->prof && d < 2 ? c->ev + 6 * d : nullptr;
     if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], &c->scr, c->G[d], c->H[d], c->dG[d], c->dH[d], c->dF[d],
@@ -527,7 +557,7 @@ static int check_side_factors(bemgpu_ctx *c) {
       }
     } else if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
       c->st_fallback[slot] = 1;
-      const int r = dense_factor_fp64(c, slot, c->G[d], 4 * (int64_t)c->dom_ne[d], "dpv LU");
+      const int r = dense_factor_fp64(c, slot, c->dom_tri[d] ? c->Gc[d] : c->G[d], c->cn[d], "dpv LU");
       if (r) return r;
     }
   }
@@ -604,8 +634,15 @@ static int solve_tail(bemgpu_ctx *c) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
     if (Nd == 0) continue;
     if (bem_launch_dpv_rhs((int)Nd, c->H[d], c->pv[d], c->B3, c->stream)) return fail(c, "dpv rhs", cudaGetLastError());
-    const int rc = dense_apply(c, 1 + d, c->G[d], Nd, 3, c->B3, c->B3s, "dpv solve");
-    if (rc) return rc;
+    if (c->dom_tri[d]) {
+      if (bem_launch_rows(c->B3, c->B3c, (int)Nd, c->cinv[d], c->cn[d], 3, 0, c->stream)) return fail(c, "dpv", cudaGetLastError());
+      const int rc = dense_apply(c, 1 + d, c->Gc[d], c->cn[d], 3, c->B3c, c->B3s, "dpv solve");
+      if (rc) return rc;
+      if (bem_launch_rows(c->B3c, c->B3, (int)Nd, c->cinv[d], c->cn[d], 3, 1, c->stream)) return fail(c, "dpv", cudaGetLastError());
+    } else {
+      const int rc = dense_apply(c, 1 + d, c->G[d], Nd, 3, c->B3, c->B3s, "dpv solve");
+      if (rc) return rc;
+    }
     if (bem_launch_dpv_store((int)Nd, c->B3, c->dpv[d], c->stream)) return fail(c, "dpv store", cudaGetLastError());
   }
   if (c->prof) cudaEventRecord(c->ev[16], c->stream);
@@ -645,7 +682,12 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   for (int d = 0; d <= c->MN; ++d) {
     const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
     if (Nd == 0) continue;
-    const int r = dense_factor(c, 1 + d, c->G[d], Nd, "dpv LU", 1);
+    double *M = c->G[d];
+    if (c->dom_tri[d]) {
+      if (bem_launch_compress(c->G[d], (int)Nd, c->cinv[d], c->cn[d], c->Gc[d], c->side)) return fail(c, "dpv", cudaGetLastError());
+      M = c->Gc[d];
+    }
+    const int r = dense_factor(c, 1 + d, M, c->cn[d], "dpv LU", 1);
     if (r) return r;
   }
   CK(cudaEventRecord(c->ev_join, c->side), "join");
@@ -773,15 +815,31 @@ extern "C" int bemgpu_get_matrix(bemgpu_ctx *c, int d, int which, double *dst) {
 }
 
 static int ensure_force_targets(bemgpu_ctx *c);
+static int ensure_centres(bemgpu_ctx *c);
 static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
 
 extern "C" int bemgpu_force(bemgpu_ctx *c, int type, const double *rc, double *F, double *N) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   CK(cudaMemcpyAsync(c->rc_d, rc, 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "rc");
   if (type == 0) {
-    if (bem_launch_force0(&c->sys, c->P[0], c->pv[0], c->rc_d, c->c0[0], c->rho0[0], c->fout, c->stream))
+    const int *ctr = nullptr;
+    if (c->dom_tri[0]) {
+      // boundary values at the centres of the domain-0 triangles (lit_force_4p's 4th point)
+      if (ensure_centres(c)) return -1;
+      bem_dom_dev D = dom_view(c, 0);
+      if (bem_launch_bdval(&D, &c->qp, 1, c->k0[0], 0, c->nctr, c->ctr_t, c->ctr_ze, c->P[0], c->dP[0], c->pv[0],
+                           c->dpv[0], c->ctr_bdv, c->status, c->stream))
+        return fail(c, "force", cudaGetLastError());
+      ctr = c->ctr_idx;
+    }
+    if (bem_launch_force0(&c->sys, c->P[0], c->pv[0], c->rc_d, c->c0[0], c->rho0[0], ctr, c->ctr_bdv, c->pw_d, c->fout,
+                          c->stream))
       return fail(c, "force", cudaGetLastError());
   } else {
+    if (c->dom_tri[0]) {
+      snprintf(c->err, sizeof(c->err), "force type %d: the 7-point rule on triangles (lit_force_7p) is not implemented", type);
+      return -2;
+    }
     // boundary values at the 9 rule points of every domain-0 element, then the stress integral
     if (ensure_force_targets(c)) return -1;
     bem_dom_dev D = dom_view(c, 0);
@@ -803,6 +861,8 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d) {
   D.ne = c->dom_ne[d];
   D.sid = c->sid + c->dom_off[d];
   D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane; D.wen = c->wen;
+  D.npe = c->npe;
+  D.has_tri = c->dom_tri[d];
   return D;
 }
 
@@ -835,6 +895,7 @@ static int ensure_points(bemgpu_ctx *c, int n) {
 extern "C" int bemgpu_field(bemgpu_ctx *c, int d, int type, int n, const double *r, double *out) {
   if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain %d", d); return -2; }
   if (type < 0 || type > 3) { snprintf(c->err, sizeof(c->err), "field rule type %d not available (0..3)", type); return -2; }
+  if (c->dom_tri[d]) { snprintf(c->err, sizeof(c->err), "field sums over triangles are not implemented"); return -2; }
   if (n <= 0) return 0;
   if (ensure_points(c, n)) return -1;
   bem_dom_dev D = dom_view(c, d);
@@ -866,6 +927,25 @@ extern "C" int bemgpu_boundary_field(bemgpu_ctx *c, int d, int type, int n, cons
     return fail(c, "boundary field", cudaGetLastError());
   CK(cudaMemcpyAsync(out, c->pt_out, 9 * sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream), "boundary field");
   CK(cudaStreamSynchronize(c->stream), "boundary field");
+  return 0;
+}
+
+// centres of the domain-0 triangles: targets (t, 0, 0) and the element -> target map
+static int ensure_centres(bemgpu_ctx *c) {
+  if (c->nctr) return 0;
+  const int ne = c->dom_ne[0];
+  std::vector<int> sid(ne), npe(c->Ne), t, idx(ne, -1);
+  CK(cudaMemcpy(sid.data(), c->sid, sizeof(int) * ne, cudaMemcpyDeviceToHost), "centres");
+  CK(cudaMemcpy(npe.data(), c->npe, sizeof(int) * c->Ne, cudaMemcpyDeviceToHost), "centres");
+  for (int s = 0; s < ne; ++s)
+    if (npe[abs(sid[s]) - 1] == 3) { idx[s] = (int)t.size(); t.push_back(s); }
+  std::vector<double> ze(2 * t.size(), 0.0);
+  if (t.empty()) return 0;
+  if (upload(c, &c->ctr_t, t.data(), t.size(), "centres") || upload(c, &c->ctr_idx, idx.data(), idx.size(), "centres") ||
+      upload(c, &c->ctr_ze, ze.data(), ze.size(), "centres"))
+    return -1;
+  CK(dalloc(&c->ctr_bdv, 9 * t.size()), "centres");
+  c->nctr = (int)t.size();
   return 0;
 }
 

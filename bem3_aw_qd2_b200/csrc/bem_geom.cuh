@@ -70,6 +70,87 @@ __device__ __forceinline__ void bem_rw_ref(const bem_el &el, double z, double e,
   }
 }
 
+// ---- linear triangles (d3qd2_elem.c:1035-1162): reference triangle with corners
+// (-1/2, -sqrt3/2), (1, 0), (-1/2, sqrt3/2); r(z,e) = cr0 + cr1 z + cr2 e
+// (cr3 = 0), W = cw0 constant (cw1 = cw2 = 0), so bem_rw, bem_K serve both types.
+#define BEM_SQ3 1.732050807568877293528
+#define BEM_P34_N0 0.2                       // collocation nodes (-N0,-N1), (2 N0, 0), (-N0, N1)
+#define BEM_P34_N1 0.3464101615137754587055
+
+// interpolation functions N_n(z,e), n = 0..2; N[3] = 0 (lit_Nn, d3qd2_elem.c:1047)
+__device__ __forceinline__ void bem_Nn3(double z, double e, double N[4]) {
+  const double ia = 0.5 / BEM_P34_N0;
+  N[0] = (1.0 / 3.0) * (1.0 - ia * (z + BEM_SQ3 * e));
+  N[1] = (1.0 / 3.0) * (1.0 + 2.0 * ia * z);
+  N[2] = (1.0 / 3.0) * (1.0 - ia * (z - BEM_SQ3 * e));
+  N[3] = 0.0;
+}
+__device__ __forceinline__ void bem_Nn(bool tri, double z, double e, double N[4]) {
+  if (tri) bem_Nn3(z, e, N);
+  else bem_Nn4(z, e, N);
+}
+// twice the derivative of N_n along the direction (c, s), the radial factor of the
+// principal-value D-eps integrals (lit_dNn_pr_cs, lit_dcoef.c:845)
+__device__ __forceinline__ void bem_dNn3(double c, double s, double dN[4]) {
+  const double ia = 0.5 / BEM_P34_N0;
+  dN[0] = -2.0 / 3.0 * ia * (c + BEM_SQ3 * s);
+  dN[1] = 4.0 / 3.0 * ia * c;
+  dN[2] = -2.0 / 3.0 * ia * (c - BEM_SQ3 * s);
+  dN[3] = 0.0;
+}
+// The triangle's product Gauss rule (q0_lit_dcoef_v2_cc_GL, q0_lit_dcoef_v2_cc.c:191-219): the
+// triangle is cut into 3 quadrilaterals (a vertex, two edge midpoints, the centroid), each
+// mapped from [-1,1]^2; point (a, b) of part `part`, Jacobian factor 1 + a/4 + b/4.
+__device__ __forceinline__ void bem_tri_point(int part, double a, double b, double &z, double &e) {
+  if (part == 0) {
+    z = 0.125 * (3.0 + 2.0 * a + 2.0 * b + a * b);
+    e = 0.125 * BEM_SQ3 * (-a + b);
+  } else if (part == 1) {
+    z = 0.0625 * (-3.0 + a - 5.0 * b - a * b);
+    e = 0.0625 * BEM_SQ3 * (3.0 + 3.0 * a + b + a * b);
+  } else {
+    z = 0.0625 * (-3.0 - 5.0 * a + b - a * b);
+    e = 0.0625 * BEM_SQ3 * (-3.0 - a - 3.0 * b - a * b);
+  }
+}
+// The same point rounded as the reference rounds it (each operation separately, in
+// its order), for the periodic sums whose lattice-plane stopping depends on exact zeros
+__device__ __forceinline__ void bem_tri_point_ref(int part, double a, double b, double &z, double &e) {
+  const double ab = __dmul_rn(a, b);
+  if (part == 0) {
+    z = __dmul_rn(0.125, __dadd_rn(__dadd_rn(__dadd_rn(3.0, __dmul_rn(2.0, a)), __dmul_rn(2.0, b)), ab));
+    e = __dmul_rn(0.125 * BEM_SQ3, __dadd_rn(-a, b));
+  } else if (part == 1) {
+    z = __dmul_rn(0.0625, __dadd_rn(__dadd_rn(__dadd_rn(-3.0, a), -__dmul_rn(5.0, b)), -ab));
+    e = __dmul_rn(0.0625 * BEM_SQ3, __dadd_rn(__dadd_rn(__dadd_rn(3.0, __dmul_rn(3.0, a)), b), ab));
+  } else {
+    z = __dmul_rn(0.0625, __dadd_rn(__dadd_rn(__dadd_rn(-3.0, -__dmul_rn(5.0, a)), b), -ab));
+    e = __dmul_rn(0.0625 * BEM_SQ3, __dadd_rn(__dadd_rn(__dadd_rn(-3.0, -a), -__dmul_rn(3.0, b)), -ab));
+  }
+}
+// weight of point (a, b) relative to wl_a wl_b with W = cw0: the rule's total is
+// |cw0| / 2, the triangle's area (the reference's 1/24 aW normalisation)
+__device__ __forceinline__ double bem_tri_wfac(double a, double b) { return (1.0 + 0.25 * a + 0.25 * b) * (1.0 / 24.0); }
+// collocation node tn of a triangle (zt_34, et_34)
+__device__ __forceinline__ void bem_tri_node(int tn, double &z, double &e) {
+  z = tn == 1 ? 2.0 * BEM_P34_N0 : -BEM_P34_N0;
+  e = tn == 0 ? -BEM_P34_N1 : (tn == 2 ? BEM_P34_N1 : 0.0);
+}
+// corner distances and angles seen from (zt, et) (lit_calc_node_r_th, d3qd2_elem.c:1149)
+__device__ __forceinline__ void bem_tri_node_r_th(double zt, double et, double r[5], double th[5]) {
+  const double ztp = 1.0 - zt, ztm = -0.5 - zt, etp = 0.5 * BEM_SQ3 - et, etm = -0.5 * BEM_SQ3 - et;
+  r[0] = sqrt(ztm * ztm + etm * etm);
+  r[1] = sqrt(ztp * ztp + et * et);
+  r[2] = sqrt(ztm * ztm + etp * etp);
+  r[3] = r[0];
+  r[4] = r[0];
+  th[0] = atan2(etm, ztm);
+  th[1] = atan2(-et, ztp);
+  th[2] = atan2(etp, ztm);
+  th[3] = th[0] + 2.0 * CUDART_PI;
+  th[4] = th[3];
+}
+
 // corner distances and angles seen from (zt,et) (bil_calc_node_r_th, d3qd2_elem.c:1014)
 __device__ __forceinline__ void bem_node_r_th(double zt, double et, double r[5], double th[5]) {
   const double ztp = 1.0 - zt, ztm = -1.0 - zt, etp = 1.0 - et, etm = -1.0 - et;

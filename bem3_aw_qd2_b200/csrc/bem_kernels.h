@@ -11,6 +11,8 @@ struct bem_dom_dev {
   const double *cr, *cw, *ren;  // element tables, see bem_types.h
   const double *wen;            // normal vectors at the collocation nodes (field rule 0)
   const uint8_t *plane;         // 1 if the element is plane (bil_check_plane)
+  const int *npe;               // nodes per element: 4 bilinear quad, 3 linear triangle
+  int has_tri;                  // any triangle among the domain's elements
 };
 
 // Scratch used by one domain assembly (sized for N = 4 ne rows).

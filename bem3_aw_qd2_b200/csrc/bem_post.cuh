@@ -33,16 +33,46 @@ __device__ __forceinline__ void rule_point(int type, int i, double &z, double &e
   else { z = c_q.xh[i / BEM_GHN]; e = c_q.xh[i % BEM_GHN]; w = c_q.wh[i / BEM_GHN] * c_q.wh[i % BEM_GHN]; }
 }
 
+// Rules on a triangle source (q0_lit_coef_4p / _7p / _GL / _GH, q0_lit_coef.c:10-250):
+// type 0: the 3 nodes and the centre (weights 25/48 x 3, -27/48), 1: 7-point rule,
+// 2, 3: the 3-part 12 x 12 / 64 x 64 rules.  w multiplies W = cw0 (twice the area).
+__device__ __forceinline__ int tri_rule_points(int type) {
+  return type == 0 ? 4 : (type == 1 ? 7 : 3 * (type == 2 ? BEM_GLN * BEM_GLN : BEM_GHN * BEM_GHN));
+}
+__device__ __forceinline__ void tri_rule_point(int type, int i, double &z, double &e, double &w) {
+  if (type == 0) {
+    if (i < 3) bem_tri_node(i, z, e);
+    else z = e = 0.0;
+    w = 0.5 * (i < 3 ? 25.0 / 48.0 : -27.0 / 48.0);
+  } else if (type == 1) {
+    // the 7-point rule (zt_37, et_37, wt_37, bem3_aw_qd2.c:1012-1021)
+    const double n0 = 0.3480702390148154917985, n1 = 0.2052130961576726346557;
+    const double n2 = 0.6028753385763033130539, n3 = 0.3554395089236065568357;
+    const double v0 = 0.1259391805448271525957, v1 = 0.1323941527885061807376, v2 = 0.225;
+    const double zz[7] = {-n0, 2.0 * n0, -n0, n1, -2.0 * n1, n1, 0.0}, ee[7] = {-n2, 0.0, n2, n3, 0.0, -n3, 0.0};
+    z = zz[i];
+    e = ee[i];
+    w = 0.5 * (i < 3 ? v0 : (i < 6 ? v1 : v2));
+  } else {
+    const int n = type == 2 ? BEM_GLN : BEM_GHN;
+    const double *x = type == 2 ? c_q.xl : c_q.xh, *wq = type == 2 ? c_q.wl : c_q.wh;
+    const int part = i / (n * n), ij = i % (n * n), a = ij / n, b = ij % n;
+    bem_tri_point(part, x[a], x[b], z, e);
+    w = wq[a] * wq[b] * bem_tri_wfac(x[a], x[b]);
+  }
+}
+
 // boundary values of source element s interpolated at (z,e); type 0 uses the
-// node value itself (the 4-point rule sits on the nodes)
+// node value itself (the 4-point rule sits on the nodes; the triangle's centre
+// point takes the mean of its 3 nodes)
 __device__ __forceinline__ void interp_bv(int type, int i, double z, double e, int s, const double *P, const double *dP,
                                           const double *pv, const double *dpv, cplx &Pn, cplx &dPn, cplx pvn[3],
-                                          cplx dpvn[3]) {
+                                          cplx dpvn[3], bool tri = false) {
   double N[4];
-  if (type == 0) {
+  if (type == 0 && !(tri && i == 3)) {
     for (int a = 0; a < 4; ++a) N[a] = a == i ? 1.0 : 0.0;
   } else {
-    bem_Nn4(z, e, N);
+    bem_Nn(tri, z, e, N);
   }
   Pn = dPn = cmk(0, 0);
   for (int c = 0; c < 3; ++c) pvn[c] = dpvn[c] = cmk(0, 0);
@@ -79,7 +109,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm /* NV*(FIE
 }
 
 // one block per field point; threads over (source element, rule point)
-__global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, bem_qp q, int periodic, double k, int type,
+__global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, const __grid_constant__ bem_qp q, int periodic, double k, int type,
                                                          const double *__restrict__ pts, const double *__restrict__ P,
                                                          const double *__restrict__ dP, const double *__restrict__ pv,
                                                          const double *__restrict__ dpv, double *__restrict__ out,
@@ -174,7 +204,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, bem_qp q
 // d3qd2_elem.c:684, self pair q0_bil_coef_bd); 0: an interior domain in free
 // space with wave number k (coef_bd, d3qd2_elem.c:187, self pair bil_coef_bd,
 // bil_coef.c:244-342).  out per target: S0 (2), S2 (6), F.
-__global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q, int periodic, double k, int type,
+__global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, const __grid_constant__ bem_qp q, int periodic, double k, int type,
                                                          const int *__restrict__ tgt_t,
                                                          const double *__restrict__ tgt_ze, const double *__restrict__ P,
                                                          const double *__restrict__ dP, const double *__restrict__ pv,
@@ -188,7 +218,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
   bem_load_el(D.cr, D.cw, te, elt);
   double rt[3], wt_[3];
   bem_rw_ref(elt, zt, et, rt, wt_);
-  const int nr = rule_points(type);
+  const int nr = D.has_tri ? max(rule_points(type), tri_rule_points(type)) : rule_points(type);
   double a[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) a[c] = 0.0;
@@ -198,10 +228,13 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
     const int s = (int)(it / nr), i = (int)(it % nr);
     const int se = abs(D.sid[s]) - 1;
     if (s == t) continue;
+    const bool stri = D.has_tri && D.npe[se] == 3;
+    if (i >= (stri ? tri_rule_points(type) : rule_points(type))) continue;
     const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
     double z, e, w, vR[3], vW[3];
-    rule_point(type, i, z, e, w);
-    if (type == 0) {
+    if (stri) tri_rule_point(type, i, z, e, w);
+    else rule_point(type, i, z, e, w);
+    if (type == 0 && !(stri && i == 3)) {
       for (int d = 0; d < 3; ++d) {
         vR[d] = __ldg(D.ren + (size_t)se * 12 + i * 3 + d);
         vW[d] = __ldg(D.wen + (size_t)se * 12 + i * 3 + d);
@@ -229,7 +262,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
       H = cscale(cmul(cmk(-1.0, k * aR), ce), sg * BEM_I_FP * tD);
     }
     cplx Pn, dPn, pvn[3], dpvn[3];
-    interp_bv(type, i, z, e, s, P, dP, pv, dpv, Pn, dPn, pvn, dpvn);
+    interp_bv(type, i, z, e, s, P, dP, pv, dpv, Pn, dPn, pvn, dpvn, stri);
     const cplx t0 = csub(cmul(G, dPn), cmul(H, Pn));
     a[0] += w * t0.re;
     a[1] += w * t0.im;
@@ -240,12 +273,15 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
     }
     a[8] += sg * w * tD * BEM_I_FP;
   }
-  // the element itself: polar rule around (zt, et)
+  // the element itself: polar rule around (zt, et); a triangle has 3 sub-triangles
+  // and the constant Jacobian vector cw0 2 / (3 sqrt3) (q0_lit_coef_bd, lit_coef_bd)
+  const bool ttri = D.has_tri && D.npe[te] == 3;
   double r[5], th[5];
-  bem_node_r_th(zt, et, r, th);
+  if (ttri) bem_tri_node_r_th(zt, et, r, th);
+  else bem_node_r_th(zt, et, r, th);
   const bool plane = D.plane[te] != 0;
   const double sgt = D.sid[t] < 0 ? -1.0 : 1.0, bdC = bem_bdC(elt);
-  for (int pt = threadIdx.x; pt < 512 * BEM_GLN; pt += FIELD_THREADS) {
+  for (int pt = threadIdx.x; pt < (ttri ? 384 : 512) * BEM_GLN; pt += FIELD_THREADS) {
     const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
     const polar_pt tp = polar_theta(th, idx);
     const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
@@ -259,7 +295,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
     bem_K(elt, rr, cth, sth, zt, et, K);
     for (int d = 0; d < 3; ++d) {
       vR[d] = rr * K[d];
-      vW[d] = elt.cw[d][0] + elt.cw[d][1] * z + elt.cw[d][2] * e;
+      vW[d] = ttri ? elt.cw[d][0] * (2.0 / (3.0 * BEM_SQ3)) : elt.cw[d][0] + elt.cw[d][1] * z + elt.cw[d][2] * e;
     }
     const double aW = sqrt(dot3(vW, vW));
     cplx G, H;
@@ -270,7 +306,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
       G = cscale(gv.g, aW);
       H = cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2]));
     } else {
-      // bil_sG_r, bil_sH_r with the Jacobian rr of the polar map taken out of w
+      // bil_sG_r, bil_sH_r (lit_sG_r) with the Jacobian rr of the polar map taken out of w
       const double aK = sqrt(dot3(K, K)), kR = k * aK * rr;
       const cplx ce = cexpi(kR);
       G = cscale(ce, BEM_I_FP * aW / (aK * rr));
@@ -278,7 +314,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_bdval(bem_dom_dev D, bem_qp q
                 : cscale(cmul(cmk(-1.0, kR), ce), sgt * BEM_I_FP * bdC * cth * sth / (aK * aK * aK * rr));
     }
     cplx Pn, dPn, pvn[3], dpvn[3];
-    interp_bv(1, 0, z, e, t, P, dP, pv, dpv, Pn, dPn, pvn, dpvn);
+    interp_bv(1, 0, z, e, t, P, dP, pv, dpv, Pn, dPn, pvn, dpvn, ttri);
     const cplx t0 = csub(cmul(G, dPn), cmul(H, Pn));
     a[0] += w * t0.re;
     a[1] += w * t0.im;

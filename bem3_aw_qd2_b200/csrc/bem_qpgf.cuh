@@ -31,6 +31,10 @@
 #define BEM_EW_LIMIT 100       // d3_qpgf_d2.h:25
 #define BEM_FD_LIMIT 100       // d3_qpgf_d2.h:22
 #define BEM_EW_EXPM 3.0        // d3_qpgf_d2.h:26
+// |z| below which the spectral rows' stopping tests can meet an exact zero of
+// the z-derivative terms (e^{bn z} rounds to 1 for |bn z| < 2^-54): there the
+// terms are formed with the reference's rounding and eta0
+#define BEM_PLANE_NEAR 1.0e-13
 #define BEM_S_LIMIT 15         // d3_qpgf_d2.h:19
 #define BEM_W_TAB 48           // exp(-a^2 n^2) table length
 #define BEM_FD_MAX_TERMS 250.0 // spectral-only sum used when it needs fewer terms than this
@@ -62,7 +66,13 @@ __device__ __forceinline__ double bem_sinc(double x, double sinx) {
 }
 
 // w(z) for z = xr + i yi.
-__device__ __noinline__ cplx bem_faddeeva(double xr, double yi) {
+#ifndef BEM_FADDEEVA_ATTR
+#define BEM_FADDEEVA_ATTR __noinline__
+#endif
+#ifndef BEM_QPGF_ATTR
+#define BEM_QPGF_ATTR
+#endif
+__device__ BEM_FADDEEVA_ATTR cplx bem_faddeeva(double xr, double yi) {
   if (xr == 0.0) return cmk(erfcx(yi), xr);  // w(iy) = erfcx(y), keep the sign of 0
   const double x = fabs(xr), ya = fabs(yi);
   if (ya >= 7.0 || (x >= 6.0 && ya >= 0.1)) {
@@ -249,11 +259,12 @@ __device__ __forceinline__ double bem_an(double mk, int n1, double g1, int n2, d
   return __dadd_rn(__dadd_rn(mk, __dmul_rn((double)n1, g1)), __dmul_rn((double)n2, g2));
 }
 // Ewald parameter, capped where k^2 eta^2 - r^2 / 4 eta^2 > EW_EXPM (d3_qpgf_d2.c:1684-1697).
-// On the lattice plane the reference's eta0 (its truncation there depends on it),
-// elsewhere eta_run (eta0 unless a tuned value is set: both sums converge).
+// On and next to the lattice plane the reference's eta0 (its truncation there
+// depends on it), elsewhere eta_run (eta0 unless a tuned value is set: both
+// sums converge).
 __device__ __forceinline__ double bem_ewald_eta(const bem_qp &q, double rx, double ry, double rz) {
   const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
-  const double ve = rz == 0.0 ? q.eta0 : q.eta_run, kk = __dmul_rn(q.k, q.k);
+  const double ve = fabs(rz) < BEM_PLANE_NEAR ? q.eta0 : q.eta_run, kk = __dmul_rn(q.k, q.k);
   const double lhs = __dadd_rn(__dmul_rn(__dmul_rn(kk, ve), ve), -__ddiv_rn(r2, __dmul_rn(__dmul_rn(4.0, ve), ve)));
   if (lhs > BEM_EW_EXPM)
     return __ddiv_rn(__dsqrt_rn(__dadd_rn(BEM_EW_EXPM, __dsqrt_rn(__dadd_rn(__dmul_rn(kk, r2), BEM_EW_EXPM * BEM_EW_EXPM)))),
@@ -298,11 +309,21 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     return 0;
   } else if (bn2 < 0.0) {
     // f1 = e^{bn z} erfc(bn ve + z/2ve), f2 = e^{-bn z} erfc(bn ve - z/2ve)
-    // = e^{-Q} erfcx(bn ve +- z/2ve) with Q = bn^2 ve^2 + (z/2ve)^2: one exp
     const double bn = sqrt(-bn2), bv = bn * ve;
-    const double eq = exp(-(bv * bv + azve * azve));
-    const double f1 = eq * erfcx(bv + azve);
-    const double f2 = eq * erfcx(bv - azve);
+    double f1, f2;
+    if (fabs(rz) < BEM_PLANE_NEAR) {
+      // Next to the lattice plane f1 - f2 is zero, or not, by rounding alone,
+      // and the rows' stopping tests see that zero: form both exactly as the
+      // reference does (ebz = exp(bn z), f2 with 1/ebz; d3_qpgf_d2.c:2003-2007).
+      const double ebz = bem_exp_cr(__dmul_rn(bn, rz)), bvr = __dmul_rn(bn, ve);
+      f1 = __dmul_rn(ebz, erfc(__dadd_rn(bvr, azve)));
+      f2 = __dmul_rn(__ddiv_rn(1.0, ebz), erfc(__dadd_rn(bvr, -azve)));
+    } else {
+      // = e^{-Q} erfcx(bn ve +- z/2ve) with Q = bn^2 ve^2 + (z/2ve)^2: one exp
+      const double eq = exp(-(bv * bv + azve * azve));
+      f1 = eq * erfcx(bv + azve);
+      f2 = eq * erfcx(bv - azve);
+    }
     // Fn = ce / (i bn) (f1 + f2)
     Fn = cmul(ce, cmk(0.0, -(f1 + f2) / bn));
     dF0 = cscale(Fn, anx);
@@ -320,7 +341,7 @@ __device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.re, -a.im); }
 // The lattice rows are walked exactly as in the reference (centre, then up,
 // then down, each stopped by the reference's tests); the Bloch phases along a
 // row are advanced by a unit complex factor, so a row costs one sincos.
-__device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
+__device__ BEM_QPGF_ATTR int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
   const double ve = bem_ewald_eta(q, rx, ry, rz);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
   const bool tab = q.wt != nullptr && ve == q.eta_run;  // table built for x = k eta_run
@@ -422,7 +443,7 @@ __device__ int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, 
 }
 
 // Pure spectral sum in the home cell (d3hm_qpgf_d2v1_fd_sd, d3_qpgf_d2.c:745-885).
-__device__ int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
+__device__ BEM_QPGF_ATTR int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
   if (rz == 0.0) return -14;
   const double eps = BEM_MEPS, az = fabs(rz);
   int cc = 0;
@@ -487,7 +508,7 @@ __device__ int bem_qpgf_spectral(const bem_qp &q, double rx, double ry, double r
 
 // G_qp and grad G_qp at r (d3hm_qpgf_d2_v1, d3_qpgf_d2.c:124-176 and the cell
 // reduction of :409-438).  Returns #terms (> 0) or the reference's negative code.
-__device__ int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
+__device__ BEM_QPGF_ATTR int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
   bool spectral = false;
   if (!q.ewald_only) {
     const double az = fabs(rz);

@@ -235,9 +235,42 @@ __global__ void k_dpv_store(int Nd, const double *__restrict__ B, double *__rest
   for (int i = 0; i < 3; ++i) zst(dpv + 2 * (3 * j + i), zld(B + 2 * ((size_t)i * Nd + j)));
 }
 
-// radiation force and torque with node values (bil_force_4p): one block
+// Domains with triangles: the dpv system keeps only real nodes (solve_dpv_bv,
+// bem3_aw_qd2_solve_bieq.c:556-600 skips row and column 3 of each triangle).
+// inv[r] = full index of compact index r.
+__global__ void k_compress_mat(const double *__restrict__ G, int N, const int *__restrict__ inv, int nn,
+                               double *__restrict__ Gc) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)nn * nn) return;
+  const int r = (int)(idx / nn), c = (int)(idx % nn);
+  zst(Gc + 2 * idx, zld(G + 2 * ((size_t)inv[r] * N + inv[c])));
+}
+// column-major right-hand sides: to = 0 compact <- full, 1 full <- compact (padding rows 0)
+__global__ void k_move_rows(const double *__restrict__ src, double *__restrict__ dst, int N, const int *__restrict__ inv,
+                            int nn, int nrhs, int to_full) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (to_full) {
+    if (r >= N) return;
+    for (int i = 0; i < nrhs; ++i) zst(dst + 2 * ((size_t)i * N + r), zmk(0, 0));
+    return;
+  }
+  if (r >= nn) return;
+  for (int i = 0; i < nrhs; ++i) zst(dst + 2 * ((size_t)i * nn + r), zld(src + 2 * ((size_t)i * N + inv[r])));
+}
+__global__ void k_scatter_rows(const double *__restrict__ src, double *__restrict__ dst, int N, const int *__restrict__ inv,
+                               int nn, int nrhs) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  for (int i = 0; i < nrhs; ++i) zst(dst + 2 * ((size_t)i * N + inv[r]), zld(src + 2 * ((size_t)i * nn + r)));
+}
+
+// radiation force and torque with node values (bil_force_4p, bem3_aw_qd2_force.c:73-120): one block.
+// Triangles (lit_force_4p, :167-228): the 3 nodes with weight 25/96 and the centre with
+// weight -27/96, whose p and v are boundary values (ctr: per domain-0 element, the
+// centre's S0, S2, F from k_bdval, or -1; pw: the incident plane wave).
 __global__ void k_force0(bem_sys_dev S, const double *__restrict__ P0, const double *__restrict__ pv0, const double *rc,
-                         double c0, double rho0, double *__restrict__ out) {
+                         double c0, double rho0, const int *__restrict__ ctr, const double *__restrict__ cbd,
+                         const double *__restrict__ pw, double *__restrict__ out) {
   const double c1 = 0.25 / (c0 * c0 * rho0), c2 = 0.25 * rho0, c3 = 0.5 * rho0;
   const zc k2 = zld(S.k2);
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -245,19 +278,39 @@ __global__ void k_force0(bem_sys_dev S, const double *__restrict__ P0, const dou
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const int t = i >> 2, tn = i & 3;
     const int asd = abs(S.sid[t]) - 1;
-    if (tn >= S.npe[asd]) continue;
-    const double *r = S.ren + (size_t)asd * 12 + tn * 3;
-    const double *w = S.wen + (size_t)asd * 12 + tn * 3;
-    zc p = zsub(zld(S.p_inc + 2 * (asd * 4 + tn)), zmul(zld(P0 + 2 * i), k2));
-    zc v[3];
-    for (int l = 0; l < 3; ++l) v[l] = zadd(zld(S.v_inc + 2 * (3 * (asd * 4 + tn) + l)), zld(pv0 + 2 * (3 * i + l)));
+    const bool tri = S.npe[asd] == 3;
+    zc p, v[3];
+    double rb[3], wb[3], wt = 1.0;  // 4-point rule weights (wt_44) are all 1
+    if (tri && tn == 3) {
+      if (!ctr) continue;
+      // centre of the triangle: r = cr0, W = cw0, boundary values from k_bdval
+      const double *b = cbd + 9 * (size_t)ctr[t];
+      const double cf = 1.0 / (1.0 + b[8]);
+      const double *crp = S.cr + (size_t)asd * 12;
+      for (int d = 0; d < 3; ++d) { rb[d] = crp[d * 4]; wb[d] = S.wen[(size_t)asd * 12 + d]; }
+      const double *R = pw + 2;
+      const double r0z = -R[6] * (rb[0] - pw[11]) - R[7] * (rb[1] - pw[12]) + R[8] * (rb[2] - pw[13]);
+      double sz, cz;
+      sincos(pw[14] * r0z, &sz, &cz);
+      const zc pinc = zmul(zmk(pw[0], pw[1]), zmk(cz, sz));
+      const zc vz = zmk(pinc.re / pw[15], pinc.im / pw[15]);
+      p = zadd(zmk(-(k2.re * b[0] - k2.im * b[1]) * cf, -(k2.re * b[1] + k2.im * b[0]) * cf), pinc);
+      for (int l = 0; l < 3; ++l) v[l] = zadd(zmk(b[2 + 2 * l] * cf, b[3 + 2 * l] * cf), zmk(vz.re * R[l * 3 + 2], vz.im * R[l * 3 + 2]));
+      wt = 0.5 * (-27.0 / 48.0);
+    } else {
+      if (tn >= S.npe[asd]) continue;
+      for (int d = 0; d < 3; ++d) { rb[d] = S.ren[(size_t)asd * 12 + tn * 3 + d]; wb[d] = S.wen[(size_t)asd * 12 + tn * 3 + d]; }
+      p = zsub(zld(S.p_inc + 2 * (asd * 4 + tn)), zmul(zld(P0 + 2 * i), k2));
+      for (int l = 0; l < 3; ++l) v[l] = zadd(zld(S.v_inc + 2 * (3 * (asd * 4 + tn) + l)), zld(pv0 + 2 * (3 * i + l)));
+      if (tri) wt = 0.5 * (25.0 / 48.0);
+    }
+    const double *r = rb, *w = wb;
     const double t1 = c1 * (p.re * p.re + p.im * p.im) - c2 * (v[0].re * v[0].re + v[0].im * v[0].im + v[1].re * v[1].re +
                                                                v[1].im * v[1].im + v[2].re * v[2].re + v[2].im * v[2].im);
     double T[9];
     for (int l = 0; l < 3; ++l)
       for (int m = 0; m < 3; ++m) T[l * 3 + m] = c3 * (v[l].re * v[m].re + v[l].im * v[m].im);
     T[0] += t1; T[4] += t1; T[8] += t1;
-    const double wt = 1.0;  // 4-point rule weights (wt_44) are all 1
     double Tw[3];
     for (int l = 0; l < 3; ++l) Tw[l] = T[l * 3] * w[0] + T[l * 3 + 1] * w[1] + T[l * 3 + 2] * w[2];
     for (int l = 0; l < 3; ++l) acc[l] += Tw[l] * wt;
@@ -316,8 +369,27 @@ extern "C" int bem_launch_dpv_store(int Nd, const double *B, double *dpv, cudaSt
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
+extern "C" int bem_launch_compress(const double *G, int N, const int *inv, int nn, double *Gc, cudaStream_t st) {
+  const long long n2 = (long long)nn * nn;
+  if (n2 == 0) return 0;
+  k_compress_mat<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(G, N, inv, nn, Gc);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bem_launch_rows(const double *src, double *dst, int N, const int *inv, int nn, int nrhs, int to_full,
+                               cudaStream_t st) {
+  if (to_full) {
+    k_move_rows<<<(N + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs, 1);
+    k_scatter_rows<<<(nn + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs);
+  } else {
+    k_move_rows<<<(nn + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs, 0);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int bem_launch_force0(const bem_sys_dev *S, const double *P0, const double *pv0, const double *rc, double c0,
-                                 double rho0, double *out, cudaStream_t st) {
-  k_force0<<<1, 256, 0, st>>>(*S, P0, pv0, rc, c0, rho0, out);
+                                 double rho0, const int *ctr, const double *cbd, const double *pw, double *out,
+                                 cudaStream_t st) {
+  k_force0<<<1, 256, 0, st>>>(*S, P0, pv0, rc, c0, rho0, ctr, cbd, pw, out);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }

@@ -32,6 +32,10 @@ int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, const double *d
                   const double *dP, double *pv, double *tpv, cudaStream_t st);
 int bem_launch_dpv_rhs(int Nd, const double *H, const double *pv, double *B, cudaStream_t st);
 int bem_launch_dpv_store(int Nd, const double *B, double *dpv, cudaStream_t st);
+// domains with triangles: dpv system without the padding rows / columns
+int bem_launch_compress(const double *G, int N, const int *inv, int nn, double *Gc, cudaStream_t st);
+int bem_launch_rows(const double *src, double *dst, int N, const int *inv, int nn, int nrhs, int to_full, cudaStream_t st);
+// ctr / cbd / pw: triangle centres (see k_force0); NULL when domain 0 has no triangles
 int bem_launch_force0(const bem_sys_dev *S, const double *P0, const double *pv0, const double *rc, double c0, double rho0,
-                      double *out, cudaStream_t st);
+                      const int *ctr, const double *cbd, const double *pw, double *out, cudaStream_t st);
 }

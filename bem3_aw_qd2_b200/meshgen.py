@@ -66,23 +66,69 @@ def cube_sphere(n, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, center=(0.0, 0.0, 0
     return nodes, quads
 
 
-def write_msh(path, nodes, quads, inner_tag=1, open_tag=99):
+def icosphere(level, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, center=(0.0, 0.0, 0.0)):
+    """Icosahedron subdivided `level` times (20 4^level triangles), projected to
+    the unit sphere and mapped to an ellipsoid.  Returns (nodes [Nn,3],
+    triangles [Ne,3] of 0-based node indices) with (r1-r0) x (r2-r0) pointing
+    out of the body."""
+    g = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, g, 0), (1, g, 0), (-1, -g, 0), (1, -g, 0), (0, -1, g), (0, 1, g), (0, -1, -g), (0, 1, -g),
+             (g, 0, -1), (g, 0, 1), (-g, 0, -1), (-g, 0, 1)]
+    verts = [np.array(v, float) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+             (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+             (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                mid[key] = len(verts) - 1
+            return mid[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    nodes = np.array(verts) * np.array(semi_axes)
+    th = math.radians(rot_y_deg)
+    R = np.array([[math.cos(th), 0, math.sin(th)], [0, 1, 0], [-math.sin(th), 0, math.cos(th)]])
+    nodes = nodes @ R.T + np.array(center)
+    tris = np.array(faces, dtype=int)
+    c = nodes.mean(axis=0)
+    for t in tris:
+        r = nodes[t]
+        if np.dot(np.cross(r[1] - r[0], r[2] - r[0]), r.mean(axis=0) - c) < 0:
+            t[[1, 2]] = t[[2, 1]]
+    return nodes, tris
+
+
+def write_msh(path, nodes, elems, inner_tag=1, open_tag=99):
+    """gmsh 2.2 ASCII: every element twice (the body side, then the open side
+    with the reversed orientation); quads are type 3, triangles type 2."""
     lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$Nodes", str(len(nodes))]
     for i, x in enumerate(nodes):
         lines.append("%d %.17g %.17g %.17g" % (i + 1, x[0], x[1], x[2]))
-    lines += ["$EndNodes", "$Elements", str(2 * len(quads))]
-    for e, q in enumerate(quads):
-        n0, n1, n2, n3 = (int(v) + 1 for v in q)
-        lines.append("%d 3 2 %d %d %d %d %d %d" % (2 * e + 1, inner_tag, 1, n0, n1, n2, n3))
-        lines.append("%d 3 2 %d %d %d %d %d %d" % (2 * e + 2, open_tag, 1, n0, n3, n2, n1))
+    lines += ["$EndNodes", "$Elements", str(2 * len(elems))]
+    for e, q in enumerate(elems):
+        v = [int(x) + 1 for x in q]
+        et = 3 if len(v) == 4 else 2
+        rev = [v[0]] + v[:0:-1]
+        lines.append("%d %d 2 %d %d %s" % (2 * e + 1, et, inner_tag, 1, " ".join(map(str, v))))
+        lines.append("%d %d 2 %d %d %s" % (2 * e + 2, et, open_tag, 1, " ".join(map(str, rev))))
     lines.append("$EndElements")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 
 
 def write_inputs(dirname, *, n=6, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, lattice=((0.8, 0.0), (0.0, 0.8)),
-                 theta_deg=20.0, phi_deg=30.0, rho_in=1.2 * RHO0, c_in=1.5 * C0, wavelength=1.0, amp=(1.0, 0.0)):
-    """Write pw.txt, periodicity.txt, medium.txt and body.msh; returns the 4 paths."""
+                 theta_deg=20.0, phi_deg=30.0, rho_in=1.2 * RHO0, c_in=1.5 * C0, wavelength=1.0, amp=(1.0, 0.0),
+                 ico=None):
+    """Write pw.txt, periodicity.txt, medium.txt and body.msh; returns the 4 paths.
+    ico: icosphere subdivision level (triangles) instead of the cube-sphere."""
     os.makedirs(dirname, exist_ok=True)
     f = C0 / wavelength
     pw = os.path.join(dirname, "pw.txt")
@@ -98,8 +144,11 @@ def write_inputs(dirname, *, n=6, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, latt
     with open(med, "w") as fp:
         fp.write("## medium\n# number of medium\n1\n# rho0 c0\n%.17g %.17g\n" % (rho_in, c_in))
     msh = os.path.join(dirname, "body.msh")
-    nodes, quads = cube_sphere(n, semi_axes, rot_y_deg)
-    write_msh(msh, nodes, quads)
+    if ico is not None:
+        nodes, elems = icosphere(ico, semi_axes, rot_y_deg)
+    else:
+        nodes, elems = cube_sphere(n, semi_axes, rot_y_deg)
+    write_msh(msh, nodes, elems)
     return pw, per, med, msh
 
 
@@ -107,6 +156,11 @@ def write_inputs(dirname, *, n=6, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, latt
 CONFIGS = {
     # one sphere r = 0.3, 216 quads, square lattice 0.8, theta 20 deg, phi 30 deg
     "sphere216": dict(n=6, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
+    # triangles: icosphere r = 0.3 with 80 triangles (fixtures) and 1280 triangles, triangular lattice 0.8
+    "tri80": dict(ico=1, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
+                  theta_deg=20.0, phi_deg=30.0),
+    "tri1280": dict(ico=3, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
+                    theta_deg=20.0, phi_deg=30.0),
     # small case for fixtures and smoke tests: 24 quads, same physics
     "sphere24": dict(n=2, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
     # 1536 quads (the batched-sweep mesh), one incidence

@@ -14,14 +14,17 @@ outputs as compressed .npz files:
   qpgf_plane.npz d3hm_qpgf_d2_v1 on points of the lattice plane (z = 0
                  exactly), where the reference's spectral rows stop on an
                  identically zero z-derivative sum
+  tri80.npz      a full solve of the 80-triangle icosphere (triangular
+                 lattice): matrices of both domains, P, dP, pv, dpv, force
+                 and torque (type 0)
   fields24.npz   on the same solved system: force and torque with the
                  9-point rule (type 1), field values (phi_s, p_t, pv_s, pv_t)
                  at points in the home cell, in shifted lattice cells, inside
                  the sphere and next to the boundary with rules 0-3, and
                  boundary values (phi_s_bd, pv_t_bd) on elements of both domains
 
-Usage: python tests/golden/make_golden.py [fields|plane]  (needs oracle/_ref; a
-few minutes; "fields" / "plane" regenerate fields24.npz / qpgf_plane.npz only)
+Usage: python tests/golden/make_golden.py [fields|plane|tri]  (needs oracle/_ref;
+a few minutes; the argument regenerates fields24.npz / qpgf_plane.npz / tri80.npz only)
 """
 import math
 import os
@@ -75,7 +78,31 @@ def make_plane():
         r = np.column_stack([rng.uniform(-0.9, 0.9, (200, 2)), np.zeros(200)])
         G, dG, ret = refwrap.qpgf(qp, r, 0)
         out.update({name + "_qp": qp, name + "_r": r, name + "_G": G, name + "_dG": dG, name + "_ret": ret})
+    # next to the plane (|z| from 1e-19 to 1e-12) on the triangular lattice of
+    # the 80-triangle icosphere, whose quadrature points meet such z
+    qp = qp_of(2 * math.pi, 20.0, 30.0, (0.8, 0.0), (0.4, 0.69282032302755091741))
+    zs = [1e-19, -1e-19, 1e-18, -1e-18, 2.6e-18, -3.5e-18, 5e-18, 7e-18, -7e-18, 1e-17, -1e-17, 3e-17,
+          1e-16, -1e-16, 1e-15, 1e-14, 1e-13, 1e-12]
+    xy = rng.uniform(-0.6, 0.6, (40, 2))
+    r = np.array([(x, y, z) for x, y in xy for z in zs])
+    G, dG, ret = refwrap.qpgf(qp, r, 0)
+    out.update({"near_qp": qp, "near_r": r, "near_G": G, "near_dG": dG, "near_ret": ret})
     np.savez_compressed(os.path.join(OUT, "qpgf_plane.npz"), **out)
+
+
+def make_solve(name, out_name):
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    files = meshgen.write_inputs(tmp, **meshgen.CONFIGS[name])
+    case = refwrap.RefCase(*files)
+    mats = case.solve(tmp)
+    sol = {}
+    for d in range(case.MN + 1):
+        P, dP, pv, dpv = case.solution(d)
+        sol.update({"P%d" % d: P, "dP%d" % d: dP, "pv%d" % d: pv, "dpv%d" % d: dpv})
+    F0, N0 = case.force(0)
+    keep = {k: v for k, v in mats.items() if not (k.startswith("dG0") or k.startswith("dH0"))}
+    np.savez_compressed(os.path.join(OUT, out_name), F0=F0, N0=N0, **keep, **sol)
+    return case
 
 
 def make_fields(case):
@@ -112,6 +139,10 @@ def make_fields(case):
 
 def main():
     rng = np.random.default_rng(20241203)
+    if sys.argv[1:] == ["tri"]:
+        make_solve("tri80", "tri80.npz")
+        print("tri80.npz written to", OUT)
+        return
     if sys.argv[1:] == ["plane"]:
         make_plane()
         print("qpgf_plane.npz written to", OUT)

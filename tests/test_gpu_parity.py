@@ -123,3 +123,23 @@ def test_sphere24_force(sphere24):
     assert np.linalg.norm(F - g["F0"]) < 1e-9 * np.linalg.norm(g["F0"])
     assert np.linalg.norm(N - g["N0"]) < 1e-9 * max(np.linalg.norm(g["N0"]), 1e-30) + 1e-9 * np.linalg.norm(g["F0"]) * 0.3
     assert case.status() == 0
+
+
+def test_qpgf_next_to_lattice_plane_matches_reference():
+    """0 < |z| <= 1e-12: whether e^{bn z} erfc(bn eta + z/2eta) and
+    e^{-bn z} erfc(bn eta - z/2eta) coincide is decided by rounding, and the
+    reference's spectral rows stop on that zero as on the plane itself.  The
+    device forms those terms with the reference's rounding and Ewald parameter
+    below |z| = 1e-13; G and its gradient agree to 1e-12 at every point, and
+    the term count wherever the reference's rows stop on the zero (|z| up to
+    3.5e-18 here, the sum as truncated as on the plane)."""
+    from bem3_aw_qd2_b200 import api
+    g = np.load(os.path.join(GOLD, "qpgf_plane.npz"))
+    r = g["near_r"]
+    G, dG, ret = api.qpgf(g["near_qp"], r)
+    eG = np.abs(G - g["near_G"]) / np.abs(g["near_G"])
+    edG = np.linalg.norm(dG - g["near_dG"], axis=1) / np.linalg.norm(g["near_dG"], axis=1)
+    assert eG.max() < 1e-12
+    assert edG.max() < 1e-12
+    flat = np.abs(r[:, 2]) <= 3.5e-18
+    assert np.array_equal(ret[flat], g["near_ret"][flat])
