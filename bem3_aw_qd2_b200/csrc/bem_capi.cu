@@ -836,11 +836,7 @@ extern "C" int bemgpu_force(bemgpu_ctx *c, int type, const double *rc, double *F
                           c->stream))
       return fail(c, "force", cudaGetLastError());
   } else {
-    if (c->dom_tri[0]) {
-      snprintf(c->err, sizeof(c->err), "force type %d: the 7-point rule on triangles (lit_force_7p) is not implemented", type);
-      return -2;
-    }
-    // boundary values at the 9 rule points of every domain-0 element, then the stress integral
+    // boundary values at the rule points of every domain-0 element, then the stress integral
     if (ensure_force_targets(c)) return -1;
     bem_dom_dev D = dom_view(c, 0);
     if (bem_launch_bdval(&D, &c->qp, 1, c->k0[0], 1, c->ntgt, c->tgt_t, c->tgt_ze, c->P[0], c->dP[0], c->pv[0], c->dpv[0], c->bdv,
@@ -894,13 +890,14 @@ static int ensure_points(bemgpu_ctx *c, int n) {
 
 extern "C" int bemgpu_field(bemgpu_ctx *c, int d, int type, int n, const double *r, double *out) {
   if (!c->loaded || d < 0 || d > c->MN) { snprintf(c->err, sizeof(c->err), "bad domain %d", d); return -2; }
+  const int grad = !(type & BEMGPU_FIELD_POTENTIAL);
+  type &= ~BEMGPU_FIELD_POTENTIAL;
   if (type < 0 || type > 3) { snprintf(c->err, sizeof(c->err), "field rule type %d not available (0..3)", type); return -2; }
-  if (c->dom_tri[d]) { snprintf(c->err, sizeof(c->err), "field sums over triangles are not implemented"); return -2; }
   if (n <= 0) return 0;
   if (ensure_points(c, n)) return -1;
   bem_dom_dev D = dom_view(c, d);
   CK(cudaMemcpyAsync(c->pt_in, r, 3 * sizeof(double) * n, cudaMemcpyHostToDevice, c->stream), "field points");
-  if (bem_launch_field(&D, &c->qp, d == 0, c->k0[d], type, n, c->pt_in, c->P[d], c->dP[d], c->pv[d], c->dpv[d],
+  if (bem_launch_field(&D, &c->qp, d == 0, grad, c->k0[d], type, n, c->pt_in, c->P[d], c->dP[d], c->pv[d], c->dpv[d],
                        c->pt_out, c->status, c->stream))
     return fail(c, "field", cudaGetLastError());
   CK(cudaMemcpyAsync(out, c->pt_out, 18 * sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream), "field");
@@ -949,22 +946,35 @@ static int ensure_centres(bemgpu_ctx *c) {
   return 0;
 }
 
-// targets of the 9-point force rule: every domain-0 element x 9 rule points
+// targets of the type-1 force rule: the 9 rule points of every domain-0 quad
+// (bil_force_9p) and the 7 of every triangle (lit_force_7p, whose element sum
+// is halved: the weight carries the 1/2)
 static int ensure_force_targets(bemgpu_ctx *c) {
   if (c->ntgt) return 0;
-  const int ne = c->dom_ne[0], n = 9 * ne;
+  const int ne = c->dom_ne[0];
   const double b = 0.7745966692414833770359, w0 = 25.0 / 81.0, w1 = 40.0 / 81.0, w2 = 64.0 / 81.0;
   const double z9[9] = {-b, b, b, -b, 0.0, b, 0.0, -b, 0.0}, e9[9] = {-b, -b, b, b, -b, 0.0, b, 0.0, 0.0};
   const double w9[9] = {w0, w0, w0, w0, w1, w1, w1, w1, w2};
-  std::vector<int> t(n);
-  std::vector<double> ze(2 * (size_t)n), w(n);
-  for (int s = 0; s < ne; ++s)
-    for (int i = 0; i < 9; ++i) {
-      t[9 * s + i] = s;
-      ze[2 * (9 * s + i)] = z9[i];
-      ze[2 * (9 * s + i) + 1] = e9[i];
-      w[9 * s + i] = w9[i];
+  const double n0 = 0.3480702390148154917985, n1 = 0.2052130961576726346557;
+  const double n2 = 0.6028753385763033130539, n3 = 0.3554395089236065568357;
+  const double v0 = 0.1259391805448271525957, v1 = 0.1323941527885061807376, v2 = 0.225;
+  const double z7[7] = {-n0, 2.0 * n0, -n0, n1, -2.0 * n1, n1, 0.0}, e7[7] = {-n2, 0.0, n2, n3, 0.0, -n3, 0.0};
+  const double w7[7] = {v0, v0, v0, v1, v1, v1, v2};
+  std::vector<int> sid(ne), npe(c->Ne);
+  CK(cudaMemcpy(sid.data(), c->sid, sizeof(int) * ne, cudaMemcpyDeviceToHost), "targets");
+  CK(cudaMemcpy(npe.data(), c->npe, sizeof(int) * c->Ne, cudaMemcpyDeviceToHost), "targets");
+  std::vector<int> t;
+  std::vector<double> ze, w;
+  for (int s = 0; s < ne; ++s) {
+    const bool tri = npe[abs(sid[s]) - 1] == 3;
+    for (int i = 0; i < (tri ? 7 : 9); ++i) {
+      t.push_back(s);
+      ze.push_back(tri ? z7[i] : z9[i]);
+      ze.push_back(tri ? e7[i] : e9[i]);
+      w.push_back(tri ? 0.5 * w7[i] : w9[i]);
     }
+  }
+  const int n = (int)t.size();
   if (upload(c, &c->tgt_t, t.data(), t.size(), "targets") || upload(c, &c->tgt_ze, ze.data(), ze.size(), "targets") ||
       upload(c, &c->tgt_w, w.data(), w.size(), "targets"))
     return -1;

@@ -33,9 +33,9 @@ int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 // table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)
 int bem_launch_wtab(double x, double *out, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
-int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int npts, const double *pts,
-                     const double *P, const double *dP, const double *pv, const double *dpv, double *out,
-                     unsigned *status, cudaStream_t st);
+int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, int grad, double k, int type, int npts,
+                     const double *pts, const double *P, const double *dP, const double *pv, const double *dpv,
+                     double *out, unsigned *status, cudaStream_t st);
 int bem_launch_bdval(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int ntgt, const int *tgt_t,
                      const double *tgt_ze,
                      const double *P, const double *dP, const double *pv, const double *dpv, double *out,

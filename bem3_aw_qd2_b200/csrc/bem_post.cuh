@@ -109,14 +109,19 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm /* NV*(FIE
 }
 
 // one block per field point; threads over (source element, rule point)
-__global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, const __grid_constant__ bem_qp q, int periodic, double k, int type,
+// grad = 1: S1 and dF with the second-derivative Green's function (q0_dcoef_rt_grad,
+// d3hm_qpgf_d2_v2); 0: the potential sums S0, S2, F alone with the
+// first-derivative one (q0_coef_rt, d3hm_qpgf_d2_v1), as phi_s_aqd2 and
+// pv_s_bieq_aqd2 form them: the two lattice sums stop differently next to
+// the lattice plane, so each caller gets the one the reference uses.
+__global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, const __grid_constant__ bem_qp q, int periodic, int grad, double k, int type,
                                                          const double *__restrict__ pts, const double *__restrict__ P,
                                                          const double *__restrict__ dP, const double *__restrict__ pv,
                                                          const double *__restrict__ dpv, double *__restrict__ out,
                                                          unsigned *status) {
   const int ip = blockIdx.x;
   const double rt[3] = {pts[3 * ip], pts[3 * ip + 1], pts[3 * ip + 2]};
-  const int nr = rule_points(type);
+  const int nr = D.has_tri ? max(rule_points(type), tri_rule_points(type)) : rule_points(type);
   double a[18];
 #pragma unroll
   for (int c = 0; c < 18; ++c) a[c] = 0.0;
@@ -124,10 +129,14 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, const __
   for (long long it = threadIdx.x; it < (long long)D.ne * nr; it += FIELD_THREADS) {
     const int s = (int)(it / nr), i = (int)(it % nr);
     const int se = abs(D.sid[s]) - 1;
+    // triangle sources: q0_lit_dcoef_grad_* / lit_dcoef_grad_* (q0_lit_dcoef_grad.c, lit_dcoef_grad.c)
+    const bool stri = D.has_tri && D.npe[se] == 3;
+    if (i >= (stri ? tri_rule_points(type) : rule_points(type))) continue;
     const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
     double z, e, w, vR[3], vW[3];
-    rule_point(type, i, z, e, w);
-    if (type == 0) {
+    if (stri) tri_rule_point(type, i, z, e, w);
+    else rule_point(type, i, z, e, w);
+    if (type == 0) {  // the rule's points are the ren entries (a triangle's centre is its 4th)
       for (int d = 0; d < 3; ++d) {
         vR[d] = __ldg(D.ren + (size_t)se * 12 + i * 3 + d);
         vW[d] = __ldg(D.wen + (size_t)se * 12 + i * 3 + d);
@@ -142,9 +151,16 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_field(bem_dom_dev D, const __
     const double aW = sqrt(dot3(vW, vW));
     const double rdW = dot3(vR, vW) * iR;
     cplx Pn, dPn, pvn[3], dpvn[3];
-    interp_bv(type, i, z, e, s, P, dP, pv, dpv, Pn, dPn, pvn, dpvn);
+    interp_bv(type, i, z, e, s, P, dP, pv, dpv, Pn, dPn, pvn, dpvn, stri);
     cplx G, H, dG[3], dH[3];
-    if (periodic) {
+    if (periodic && !grad) {
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+      if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      G = cscale(gv.g, aW);
+      H = cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2]));
+      for (int j = 0; j < 3; ++j) dG[j] = dH[j] = cmk(0.0, 0.0);
+    } else if (periodic) {
       bem_gval2 gv;
       const int rc = bem_qpgf2(q, vR[0], vR[1], vR[2], gv);
       if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
@@ -386,11 +402,11 @@ __global__ void k_force_bd(bem_dom_dev D, int ntgt, const int *__restrict__ tgt_
     for (int c = 0; c < 6; ++c) out[c] = sm[c][0];
 }
 
-extern "C" int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, double k, int type, int npts,
-                                const double *pts, const double *P, const double *dP, const double *pv,
+extern "C" int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, int grad, double k, int type,
+                                int npts, const double *pts, const double *P, const double *dP, const double *pv,
                                 const double *dpv, double *out, unsigned *status, cudaStream_t st) {
   if (npts <= 0) return 0;
-  k_field<<<npts, FIELD_THREADS, 0, st>>>(*D, *q, periodic, k, type, pts, P, dP, pv, dpv, out, status);
+  k_field<<<npts, FIELD_THREADS, 0, st>>>(*D, *q, periodic, grad, k, type, pts, P, dP, pv, dpv, out, status);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 

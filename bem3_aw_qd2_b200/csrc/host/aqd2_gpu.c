@@ -315,8 +315,8 @@ static int domain_id_home(double *rt, AQD2 *qd);
  * point is moved to the home lattice cell (domain_id_l_aqd2), its domain found
  * by the solid-angle test, and the sums of that domain evaluated on the
  * device.  Returns the domain id; o = bemgpu_field's 18 values, ce the Bloch
- * phase of the cell shift. */
-static int field_sums(double o[18], double complex *ce, double *rt, int type, AQD2 *qd)
+ * phase of the cell shift.  flags: 0 or BEMGPU_FIELD_POTENTIAL. */
+static int field_sums(double o[18], double complex *ce, double *rt, int type, int flags, AQD2 *qd)
 {
   int l1 = 0, l2 = 0;
   double r0[3] = {rt[0], rt[1], rt[2]};
@@ -335,7 +335,7 @@ static int field_sums(double o[18], double complex *ce, double *rt, int type, AQ
     exit(1);
   }
   bemgpu_ctx *c = ready_ctx(qd);
-  gpu_check(c, bemgpu_field(c, did, type, 1, r0, o), "field");
+  gpu_check(c, bemgpu_field(c, did, type | flags, 1, r0, o), "field");
   status_check(c, "field");
   *ce = 1.0;
   if (l1 != 0 || l2 != 0) {
@@ -354,7 +354,7 @@ int phi_s_aqd2(double complex *phi, double *rt, int type, AQD2 *qd)
 {
   double o[18];
   double complex ce;
-  int did = field_sums(o, &ce, rt, type, qd);
+  int did = field_sums(o, &ce, rt, type, BEMGPU_FIELD_POTENTIAL, qd);
   *phi = FS_S0(o) / (did == 0 ? 1.0 + o[8] : o[8]) * ce;
   return did;
 }
@@ -390,10 +390,14 @@ int pv_s_aqd2(double complex *p, double complex *pv, double *rt, int type, AQD2 
 {
   double o[18];
   double complex ce;
-  int did = field_sums(o, &ce, rt, type, qd);
+  int did = field_sums(o, &ce, rt, type, 0, qd);
   double iC = 1.0 / (did == 0 ? 1.0 + o[8] : o[8]);
   double complex P = FS_S0(o);
   if (fabs(o[9]) > AQD2_CBD_CDF || fabs(o[10]) > AQD2_CBD_CDF || fabs(o[11]) > AQD2_CBD_CDF) {
+    /* pv_s_bieq_aqd2: the potential sums with the first-derivative Green's function */
+    field_sums(o, &ce, rt, type, BEMGPU_FIELD_POTENTIAL, qd);
+    iC = 1.0 / (did == 0 ? 1.0 + o[8] : o[8]);
+    P = FS_S0(o);
     *p = -qd->k2[did] * P * iC;
     for (int i = 0; i < 3; i++) pv[i] = FS_S2(o, i) * iC;
   } else {

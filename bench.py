@@ -226,13 +226,27 @@ def stream_requests(count, rng):
 def run_stream(args, rank, world):
     """Serving: the request stream through the native server (continuous
     batching, factorisation reuse, HBM admission), plain FP64 and mixed."""
-    from bem3_aw_qd2_b200 import api, meshgen
+    from bem3_aw_qd2_b200 import api, meshgen, replicas
     h, g = api.libs()
     h.aqd2_set_verbose(0)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        # replicas: one stream of world x count requests at world x rate, each
+        # rank serving its round-robin share (count requests at the given rate)
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     rng = np.random.default_rng(2024)
-    count = max(args.steps, 8) * 8
-    reqs = stream_requests(count, rng)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, count))
+    per_rank = max(args.steps, 8) * 8
+    total = per_rank * world
+    all_reqs = stream_requests(total, rng)
+    all_arrivals = np.cumsum(rng.exponential(1.0 / (args.rate * world), total))
+    mine = replicas.shard(total, rank, world)
+    reqs = [all_reqs[i] for i in mine]
+    arrivals = all_arrivals[mine]
+    count = len(reqs)
     # requests are built (mesh, element tables, incident field) before the clock starts
     cases, probs = [], []
     for i, (r, key) in enumerate(reqs):
@@ -242,7 +256,7 @@ def run_stream(args, rank, world):
         probs.append(c.problem())
     out = {}
     for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 3)):
-        srv = api.Server(device=0, hbm_budget=int(args.hbm_gb * (1 << 30)), slots=args.slots)
+        srv = api.Server(device=local, hbm_budget=int(args.hbm_gb * (1 << 30)), slots=args.slots)
         # warm-up: one request per mesh size
         for i, n in enumerate(sorted({r["n"] for r, _ in reqs})):
             j = next(k for k, (r, _) in enumerate(reqs) if r["n"] == n)
@@ -251,6 +265,8 @@ def run_stream(args, rank, world):
         while got < len({r["n"] for r, _ in reqs}):
             got += len(srv.poll(timeout_ms=1000))
         done, t_sub = {}, {}
+        if world > 1:
+            dist.barrier()
         t0 = time.perf_counter()
         for i in range(count):
             while time.perf_counter() - t0 < arrivals[i]:
@@ -266,10 +282,13 @@ def run_stream(args, rank, world):
         srv.close()
         lat = [(done[i][1] - t_sub[i]) * 1000.0 for i in range(count)]
         bad = [done[i][0].error.decode() for i in range(count) if done[i][0].status != 0]
-        out[tag] = {"value": count / (t1 - t0), "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                                                               "p99": float(np.percentile(lat, 99))},
-                    "reused": int(st["reused"]), "evictions": int(st["evictions"]),
-                    "bytes_peak": st["bytes_peak"], "failed": len(bad),
+        # slowest rank's wall time and latency percentiles, all ranks' requests
+        (el, p50, p99), (n_all, n_bad, n_reused) = replicas.reduce_timing(
+            [t1 - t0, np.percentile(lat, 50), np.percentile(lat, 99)], [count, len(bad), st["reused"]],
+            device="cuda" if world > 1 else "cpu")
+        out[tag] = {"value": n_all / el, "latency_ms": {"p50": p50, "p99": p99},
+                    "reused": int(n_reused), "evictions": int(st["evictions"]),
+                    "bytes_peak": st["bytes_peak"], "failed": int(n_bad),
                     "F": {i: list(done[i][0].F[:]) for i in range(count)}}
     errs = []
     for i in range(count):
@@ -281,15 +300,19 @@ def run_stream(args, rank, world):
         c.free_problem(p)
         c.close()
     mixed = out["mixed"]
-    line = {"metric": "solves/s", "value": mixed["value"], "unit": "solves/s", "n_gpus": 1, "steps": count,
+    (emax,), _ = replicas.reduce_timing([max(errs)], [], device="cuda" if world > 1 else "cpu")
+    line = {"metric": "solves/s", "value": mixed["value"], "unit": "solves/s", "n_gpus": world, "steps": total,
             "warmup": 3, "ms_per_step": 1000.0 / mixed["value"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 assembly, complex-FP32 LU + FP64 refinement", "data": "synthetic",
-            "config": {"workload": "stream", "requests": count, "rate_per_s": args.rate, "slots": args.slots,
+            "config": {"workload": "stream", "requests": total, "rate_per_s": args.rate * world,
+                       "requests_per_gpu": per_rank, "slots": args.slots,
                        "hbm_budget_gb": args.hbm_gb, "stream": STREAM_DESC},
             "latency_ms": mixed["latency_ms"], "fp64": out["fp64"], "mixed": mixed,
-            "force_rel_err_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
+            "force_rel_err_mixed_vs_fp64": {"max": emax, "median": float(np.median(errs))}}
     if rank == 0:
         print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def workload_desc(name):
@@ -322,7 +345,7 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from bem3_aw_qd2_b200 import api, meshgen
+    from bem3_aw_qd2_b200 import api, meshgen, replicas
     h, g = api.libs()
     h.aqd2_set_device(local)
     h.aqd2_set_verbose(0)
@@ -425,13 +448,8 @@ def main():
         Fh, Nh = case.force(0)
         e2e_times.append(time.perf_counter() - t0)
     clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms, sum(e2e_times)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = float(t[0]), float(t[1])
-    else:
-        e2e_total = sum(e2e_times)
+    (total_ms, e2e_total), _ = replicas.reduce_timing([total_ms, sum(e2e_times)], [],
+                                                      device="cuda" if world > 1 else "cpu")
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1000.0)
     e2e_value = world * args.steps / e2e_total

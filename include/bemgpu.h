@@ -137,7 +137,12 @@ int bemgpu_set_solution(bemgpu_ctx *ctx, int d, const double *P, const double *d
  * bem3_aw_qd2_field.c:3-297).  type: 0 4-point, 1 9-point, 2 12x12, 3 64x64
  * rule.  out[n][18] = S0 (complex) = sum(G dP - H P), S1[3] (complex) its
  * gradient with respect to r, F, dF[3], S2[3] (complex) = sum(G dpv - H pv);
- * the caller applies the normalisation 1/(1+F) (domain 0) or 1/F. */
+ * the caller applies the normalisation 1/(1+F) (domain 0) or 1/F.
+ * type | BEMGPU_FIELD_POTENTIAL: S0, S2 and F alone (S1, dF zero), with the
+ * first-derivative Green's function as phi_s_aqd2 and pv_s_bieq_aqd2 use it
+ * (q0_coef_rt, d3qd2_elem.c:574); without the flag the sums use the
+ * second-derivative one as pv_s_dbieq_aqd2 does (q0_dcoef_rt_grad, :650). */
+#define BEMGPU_FIELD_POTENTIAL 0x100
 int bemgpu_field(bemgpu_ctx *ctx, int d, int type, int n, const double *r, double *out);
 
 /* Boundary sums of domain d at parameter points ze[n][2] = (zeta, eta) of its

@@ -105,7 +105,13 @@ def make_solve(name, out_name):
     return case
 
 
-def make_fields(case):
+TRI_BOUNDARY_POINTS = [  # on triangles: (zeta, eta) inside the reference triangle
+    (0, 1, 0.1, -0.2, 1), (0, 7, 0.0, 0.0, 1), (0, 18, -0.3480702390148154917985, -0.6028753385763033130539, 1),
+    (0, 33, 0.25, 0.1, 2), (0, 11, -0.2, 0.3, 0), (1, 2, 0.1, -0.2, 1), (1, 49, 0.0, 0.0, 2), (1, 70, -0.3, -0.1, 3),
+]
+
+
+def make_fields(case, out_name="fields24.npz", boundary_points=BOUNDARY_POINTS):
     out = {}
     out["F1"], out["N1"] = case.force(1)
     out["F1c"], out["N1c"] = case.force(1, (0.05, -0.02, 0.1))
@@ -125,23 +131,24 @@ def make_fields(case):
         res["pv_t_v"].append(v)
     out["pts"], out["types"] = pts, types
     out.update({k: np.array(v) for k, v in res.items()})
-    bd = np.array([b[:4] for b in BOUNDARY_POINTS], np.float64)
-    btypes = np.array([b[4] for b in BOUNDARY_POINTS], np.int32)
+    bd = np.array([b[:4] for b in boundary_points], np.float64)
+    btypes = np.array([b[4] for b in boundary_points], np.int32)
     phib, pb, vb = [], [], []
-    for did, t, z, e, ty in BOUNDARY_POINTS:
+    for did, t, z, e, ty in boundary_points:
         phib.append(case.boundary("phi_s_bd", did, t, z, e, ty)[0])
         a, v = case.boundary("pv_t_bd", did, t, z, e, ty)
         pb.append(a)
         vb.append(v)
     out.update(bd=bd, btypes=btypes, phi_s_bd=np.array(phib), pv_t_bd_p=np.array(pb), pv_t_bd_v=np.array(vb))
-    np.savez_compressed(os.path.join(OUT, "fields24.npz"), **out)
+    np.savez_compressed(os.path.join(OUT, out_name), **out)
 
 
 def main():
     rng = np.random.default_rng(20241203)
     if sys.argv[1:] == ["tri"]:
-        make_solve("tri80", "tri80.npz")
-        print("tri80.npz written to", OUT)
+        case = make_solve("tri80", "tri80.npz")
+        make_fields(case, "fields_tri80.npz", TRI_BOUNDARY_POINTS)
+        print("tri80.npz, fields_tri80.npz written to", OUT)
         return
     if sys.argv[1:] == ["plane"]:
         make_plane()

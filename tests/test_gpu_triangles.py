@@ -6,7 +6,11 @@ Tolerances (stated here, used below): the same as the quad sphere's
   coefficient matrices G, H, dG, dH   1e-10 relative to the row maximum
   dF                                  1e-10 (column 0), 1e-11 absolute (columns 1, 2)
   P, dP, pv, dpv                      1e-9 relative to the array maximum
-  force / torque (type 0)             1e-9 relative to |F|
+  force / torque (types 0 and 1)      1e-9 relative to |F| (torque x 0.3, the radius)
+  field values, boundary values       1e-9 relative to the largest value of the
+                                      same kind (boundary values per domain)
+Fixtures: tri80.npz (matrices, solution, type-0 force) and fields_tri80.npz
+(type-1 force, field and boundary values), both `make_golden.py tri`.
 """
 import os
 import tempfile
@@ -66,3 +70,53 @@ def test_tri80_solution_and_force(tri80):
     assert np.linalg.norm(F - g["F0"]) < 1e-9 * s
     assert np.linalg.norm(N - g["N0"]) < 1e-9 * s * 0.3
     assert case.status() == 0
+
+
+@pytest.fixture(scope="module")
+def tri80_fields(tri80):
+    case, _ = tri80
+    return case, np.load(os.path.join(GOLD, "fields_tri80.npz"))
+
+
+def test_tri80_force_type1(tri80_fields):
+    """lit_force_7p: the 7-point rule's boundary values and stress integral."""
+    case, g = tri80_fields
+    for tag, rc in (("", (0.0, 0.0, 0.0)), ("c", (0.05, -0.02, 0.1))):
+        F, N = case.force(1, rc)
+        sF = np.linalg.norm(g["F1" + tag])
+        assert np.linalg.norm(F - g["F1" + tag]) < 1e-9 * sF, (F, g["F1" + tag])
+        assert np.linalg.norm(N - g["N1" + tag]) < 1e-9 * sF * 0.3
+
+
+def test_tri80_field_values(tri80_fields):
+    """phi_s / p_t / pv_s / pv_t off the boundary with rules 0-3 on triangles
+    (q0_lit_dcoef_grad_* / lit_dcoef_grad_*): 1e-9 relative to the largest value
+    of the same kind."""
+    case, g = tri80_fields
+    pts, types = g["pts"], g["types"]
+    for name, keys in (("phi_s", ("phi_s",)), ("p_t", ("p_t",)), ("pv_s", ("pv_s_p", "pv_s_v")),
+                       ("pv_t", ("pv_t_p", "pv_t_v"))):
+        got = [case.field(name, tuple(p), int(t)) for p, t in zip(pts, types)]
+        assert [r[0] for r in got] == list(g["did"])
+        for j, key in enumerate(keys):
+            a = np.array([r[1 + j] for r in got])
+            ref = g[key]
+            assert np.max(np.abs(a - ref)) <= 1e-9 * np.max(np.abs(ref)), (name, key)
+
+
+def test_tri80_boundary_values(tri80_fields):
+    case, g = tri80_fields
+    phi, p, v = [], [], []
+    for (did, t, z, e), ty in zip(g["bd"], g["btypes"]):
+        phi.append(case.boundary("phi_s_bd", int(did), int(t), z, e, int(ty))[0])
+        a, b = case.boundary("pv_t_bd", int(did), int(t), z, e, int(ty))
+        p.append(a)
+        v.append(b)
+    # domain 0 and domain 1 values differ in scale; compare each domain on its own
+    dom = g["bd"][:, 0].astype(int)
+    for d in (0, 1):
+        m = dom == d
+        for a, key in ((phi, "phi_s_bd"), (p, "pv_t_bd_p"), (v, "pv_t_bd_v")):
+            ref = g[key]
+            err = np.abs(np.array(a) - ref).reshape(len(ref), -1).max(axis=1)
+            assert np.all(err[m] <= 1e-9 * np.max(np.abs(ref[m]))), (key, d, err[m] / np.max(np.abs(ref[m])))
