@@ -159,8 +159,9 @@ CONFIGS = {
     # triangles: icosphere r = 0.3 with 80 triangles (fixtures) and 1280 triangles, triangular lattice 0.8
     "tri80": dict(ico=1, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
                   theta_deg=20.0, phi_deg=30.0),
+    # near-normal incidence (the reference rejects an in-plane wave vector of exactly 0)
     "tri1280": dict(ico=3, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
-                    theta_deg=20.0, phi_deg=30.0),
+                    theta_deg=1e-6, phi_deg=0.0),
     # small case for fixtures and smoke tests: 24 quads, same physics
     "sphere24": dict(n=2, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
     # 1536 quads (the batched-sweep mesh), one incidence
@@ -169,3 +170,14 @@ CONFIGS = {
     "spheroid6144": dict(n=32, semi_axes=(0.2, 0.2, 0.4), rot_y_deg=30.0, lattice=((1.0, 0.0), (0.3, 0.9)),
                          theta_deg=35.0, phi_deg=15.0),
 }
+
+
+def describe(name):
+    """Element count and kind, unknowns and parameters of a configuration."""
+    c = CONFIGS[name]
+    if c.get("ico") is not None:
+        ne, npe, kind = 20 * 4 ** c["ico"], 3, "linear triangles (icosphere)"
+    else:
+        ne, npe, kind = 6 * c["n"] ** 2, 4, "bilinear quads (cube-sphere)"
+    return {"elements": ne, "element_kind": kind, "unknowns": 2 * npe * ne, "semi_axes": list(c["semi_axes"]),
+            "lattice": [list(v) for v in c["lattice"]], "theta_deg": c["theta_deg"], "phi_deg": c["phi_deg"]}

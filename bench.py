@@ -317,11 +317,7 @@ def run_stream(args, rank, world):
 
 def workload_desc(name):
     from bem3_aw_qd2_b200 import meshgen
-    c = meshgen.CONFIGS[name]
-    n = c["n"]
-    return {"quads": 6 * n * n, "unknowns": 2 * 4 * 6 * n * n, "semi_axes": list(c["semi_axes"]),
-            "lattice": [list(v) for v in c["lattice"]], "theta_deg": c["theta_deg"], "phi_deg": c["phi_deg"],
-            "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
+    return {**meshgen.describe(name), "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
             "l2": "256 MB flush between timed steps"}
 
 
@@ -399,6 +395,8 @@ def main():
     g.bemgpu_work_counters(ctx, cnt, 1)
     total_ms = sum(times)
     F_fp64, N_fp64 = F.copy(), N.copy()
+    ne = meshgen.describe(args.workload)["elements"]
+    sol_fp64 = [case.solution(dd, ne) for dd in (0, 1)]
     mixed = None
     if args.mixed_mode:
         # the mixed-precision form on the same workload: FP32 LU (tensor-core
@@ -425,6 +423,10 @@ def main():
             mph.append([ph[i] for i in range(k)])
         it, rcorr, fb = case.solve_stats()
         eff_mode = case.precision()
+        # surface coefficients P, dP, pv, dpv of both domains against the FP64 path
+        sol_m = [case.solution(dd, ne) for dd in (0, 1)]
+        coef_err = max(float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+                       for sm, s6 in zip(sol_m, sol_fp64) for a, b in zip(sm, s6))
         F1m, N1m = case.force(1)
         case.set_precision(0)
         case.run_device()
@@ -435,6 +437,7 @@ def main():
                  "latency_ms": {"p50": float(np.percentile(mt, 50)), "p99": float(np.percentile(mt, 99))},
                  "force_rel_err_vs_fp64": {"type0": float(np.linalg.norm(F - F_fp64) / np.linalg.norm(F_fp64)),
                                            "type1": float(np.linalg.norm(F1m - F1d) / np.linalg.norm(F1d))},
+                 "surface_coef_rel_err_vs_fp64": coef_err,
                  "refine_iters": [int(x) for x in it], "refine_rel_corr": [float(x) for x in rcorr],
                  "fp64_fallbacks": int(np.sum(fb)),
                  "lu_solve_ms": float(mp[11]) if len(mp) > 11 else None,
@@ -460,8 +463,6 @@ def main():
     terms_reg = cnt[0] / args.steps
     t_reg = phase_ms.get("d0_regular", float("nan")) / 1000.0
     achieved = terms_reg * C_TERM_FLOPS / t_reg / 1e12 if t_reg > 0 else None
-    nq = meshgen.CONFIGS[args.workload]["n"]
-    ne = 6 * nq * nq
     h2d = ne * (12 + 9 + 12 + 12 + 8 + 8 + 8 + 24 + 2) * 8 + ne * (1 + 4 + 1 + 2 + 8) * 4 + ne
     d2h = 2 * (4 * ne) * (2 + 2 + 6 + 6) * 8 + 48 + 4
     lat = sorted(times)

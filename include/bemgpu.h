@@ -219,6 +219,8 @@ int bemgpu_work_counters(bemgpu_ctx *ctx, unsigned long long *out6, int reset);
  * periodic = 1: the host domain 0 with the quasi-periodic Green's function
  * (H gets 1 + F on its diagonal); 0: an interior domain in free space with
  * wave number k (H gets F).  The layouts are those of bemgpu_get_matrix.
+ * Every element is taken as a bilinear quad (4 nodes); meshes with linear
+ * triangles go through bemgpu_load + bemgpu_assemble.
  *
  * The scratch the assembly needs lives in one fixed array inside the library
  * (about 21 MB on every GPU that loads it, kept until the process exits), so
