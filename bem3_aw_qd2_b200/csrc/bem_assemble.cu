@@ -272,30 +272,39 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   const int p = valid ? (int)(pair / D.ne) : 0;
   const int s = valid ? (int)(pair % D.ne) : 0;
   const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
-  double v[16];
+  // the 3 parts accumulate in this thread's shared-memory column, so that no
+  // accumulator stays live in registers across the Green's-function calls
 #pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
   unsigned long long nterm = 0, npt = 0;
   if (work) {
-    bem_node nd;
-    int t, te;
-    bem_load_node(D, p, nd, t, te);
-    bem_el el;
-    bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
     const int i = pt / BEM_GLN, j = pt % BEM_GLN;
-    const double a = c_q.xl[i], b = c_q.xl[j];
-    const double wt = c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(a, b);
+    const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
     unsigned st = 0;
     for (int part = 0; part < 3; ++part) {
+      // geometry is re-read (L1) per part rather than kept in registers
+      // across the Green's-function calls
       double z, e, vR[3], vW[3];
-      bem_tri_point_ref(part, a, b, z, e);
-      bem_rw_ref(el, z, e, vR, vW);
-      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
+      {
+        const double a = c_q.xl[i], b = c_q.xl[j];
+        bem_el el;
+        bem_load_el(D.cr, D.cw, se, el);
+        bem_tri_point_ref(part, a, b, z, e);
+        bem_rw_ref(el, z, e, vR, vW);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d));
       bem_gval gv;
       const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
       if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
       nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
       ++npt;
+      // a triangle's W is the constant cw[.][0]
+#pragma unroll
+      for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
+      const double a2 = c_q.xl[i], b2 = c_q.xl[j];
+      bem_tri_point_ref(part, a2, b2, z, e);  // recomputed: not kept across the call
+      const double wt = c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(a2, b2);
       const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
       const cplx g = cscale(gv.g, aW * wt);
       const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
@@ -303,17 +312,15 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
       bem_Nn3(z, e, N);
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
-        v[2 * n] += g.re * N[n];
-        v[2 * n + 1] += g.im * N[n];
-        v[8 + 2 * n] += h.re * N[n];
-        v[8 + 2 * n + 1] += h.im * N[n];
+        acc[2 * n][threadIdx.x] += g.re * N[n];
+        acc[2 * n + 1][threadIdx.x] += g.im * N[n];
+        acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
+        acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
       }
     }
     set_status(status, st);
   }
   count_work(terms + 0, nterm, npt);
-#pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
   __syncthreads();
   if (threadIdx.x < 32) {
     const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
@@ -1332,8 +1339,13 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
   for (int c = 0; c < nchunk; ++c) {
     const long long p0 = npairs * c / nchunk;
     const long long np = p0 + len <= npairs ? len : npairs - p0;
-    if (np > 0)
+    if (np > 0) {
+      // the kernels of the assembly itself: quad sources, and triangle sources when there are any
       k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+      if (D->has_tri)
+        k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+                                                                          p0, np);
+    }
   }
   cudaEventRecord(e1, st);
   int rc = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(ms, e0, e1) == cudaSuccess ? 0 : -1;

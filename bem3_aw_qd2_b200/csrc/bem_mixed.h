@@ -23,6 +23,10 @@ struct bem_mixed {
   size_t R32_cap = 0;
   double2 *X = nullptr, *R = nullptr, *D = nullptr;
   size_t X_cap = 0, R_cap = 0, D_cap = 0;
+  int *ts_i = nullptr;                 // panel scratch: candidate rows, displaced positions
+  size_t ts_i_cap = 0;
+  cuComplex *ts_c = nullptr;           // panel scratch: factored top block, displaced rows
+  size_t ts_c_cap = 0;
   unsigned *status = nullptr;          // 0x20: zero pivot
   unsigned long long *norms = nullptr; // max |d|, max |x| of the last refinement step
   char err[256] = {0};                 // the failing call of the last error
