@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--workload", default="sphere216")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="bracket the first timed mixed-precision step with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--rate", type=float, default=10.0, help="stream workload: mean arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="stream workload: server slots")
     ap.add_argument("--hbm-gb", type=float, default=64.0, help="stream workload: device-memory budget")
@@ -408,15 +411,19 @@ def main():
             device_step()
         torch.cuda.synchronize()
         mt, mph = [], []
-        for _ in range(args.steps):
+        for step in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
+            if args.profile_mixed and step == 0:
+                torch.cuda.cudart().cudaProfilerStart()
             device_step()
             e1.record(stream)
             e1.synchronize()
+            if args.profile_mixed and step == 0:
+                torch.cuda.cudart().cudaProfilerStop()
             mt.append(e0.elapsed_time(e1))
             ph = (api.ctypes.c_double * 16)()
             k = g.bemgpu_phase_times(ctx, ph, 16)
