@@ -405,6 +405,14 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
 }
 
 extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
+  if (scale == BEMGPU_EWALD_RULE) {
+    // k^2 eta^2 just below the cap EW_EXPM (eta = sqrt(EW_EXPM) / k): the real-space
+    // terms keep their table and the split moves as far to the spectral side
+    // as that allows
+    if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+    const double s = 0.98 * sqrt(3.0 /* EW_EXPM, d3_qpgf_d2.h:26 */) / (c->qp.k * c->qp.eta0);
+    scale = s < 1.0 ? 1.0 : (s > 1.3 ? 1.3 : s);
+  }
   if (!(scale >= 0.25 && scale <= 4.0)) { snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale); return -2; }
   c->eta_scale = scale;
   c->factored = false;

@@ -233,7 +233,7 @@ __device__ __forceinline__ bem_dd dd_mul(bem_dd x, bem_dd y) {
 __device__ __forceinline__ bem_dd dd_scale(bem_dd x, double s) {  // s a power of two
   return {x.hi * s, x.lo * s};
 }
-__device__ double bem_exp_cr(double a) {
+__device__ __noinline__ double bem_exp_cr(double a) {
   if (!(a > -700.0 && a < 700.0)) return exp(a);
   const double ln2_hi = 0.69314718055994528623, ln2_lo = 2.3190468138462995584e-17;
   const double n = rint(a * 1.4426950408889634074);
@@ -272,6 +272,32 @@ __device__ __forceinline__ double bem_ewald_eta(const bem_qp &q, double rx, doub
   return ve;
 }
 
+// The lattice-plane forms below run for a few points of a mesh only; they are
+// kept out of line so that the hot loops' code stays small.
+// Propagating order on the plane: 2 (ef Re w(bn ve) - 1) as the reference rounds it.
+__device__ __noinline__ double ew_plane_residue(const bem_qp &q, int n1, int n2, double bn2, double bn, double ve) {
+  // On the lattice plane ef Re w(bn ve) - 1 is zero up to rounding; the
+  // reference's rows stop on an identically zero z-derivative sum, so the
+  // residue must be the reference's rounded value: the host's table at
+  // eta0, else formed as the reference forms it (Faddeeva_w on the real
+  // axis is exp(-x^2), Faddeeva.cc:684; ef = exp(bn2 ve ve)).
+  if (ve == q.eta0)
+    for (int i = 0; i < q.pz_n; ++i)
+      if (q.pz_n1[i] == n1 && q.pz_n2[i] == n2) return q.pz_d[i];
+  const double x = __dmul_rn(bn, ve);
+  return __dadd_rn(__dmul_rn(bem_exp_cr(__dmul_rn(__dmul_rn(bn2, ve), ve)), bem_exp_cr(-__dmul_rn(x, x))), -1.0);
+}
+// Evanescent order next to the plane: f1 = e^{bn z} erfc(bn ve + z/2ve),
+// f2 = e^{-bn z} erfc(bn ve - z/2ve), whose difference is zero, or not, by
+// rounding alone; the rows' stopping tests see that zero, so both are formed
+// exactly as the reference forms them (ebz = exp(bn z), f2 with 1/ebz;
+// d3_qpgf_d2.c:2003-2007).
+__device__ __noinline__ double2 ew_plane_evanescent(double bn, double ve, double rz, double azve) {
+  const double ebz = bem_exp_cr(__dmul_rn(bn, rz)), bvr = __dmul_rn(bn, ve);
+  return make_double2(__dmul_rn(ebz, erfc(__dadd_rn(bvr, azve))),
+                      __dmul_rn(__ddiv_rn(1.0, ebz), erfc(__dadd_rn(bvr, -azve))));
+}
+
 __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, double anx, double any, double rz, cplx ce,
                                             double ve, cplx &Fn, cplx &dF0, cplx &dF1, cplx &dF2) {
   const double bn2 = __dadd_rn(__dadd_rn(__dmul_rn(q.k, q.k), -__dmul_rn(anx, anx)), -__dmul_rn(any, any));
@@ -286,23 +312,7 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     dF0 = cscale(Fn, anx);
     dF1 = cscale(Fn, any);
     if (rz == 0.0) {
-      // On the lattice plane ef Re w(bn ve) - 1 is zero up to rounding; the
-      // reference's rows stop on an identically zero z-derivative sum, so the
-      // residue must be the reference's rounded value: the host's table at
-      // eta0, else formed as the reference forms it (Faddeeva_w on the real
-      // axis is exp(-x^2), Faddeeva.cc:684; ef = exp(bn2 ve ve)).
-      double d = 0.0;
-      int hit = -1;
-      if (ve == q.eta0)
-        for (int i = 0; i < q.pz_n; ++i)
-          if (q.pz_n1[i] == n1 && q.pz_n2[i] == n2) { hit = i; break; }
-      if (hit >= 0) {
-        d = q.pz_d[hit];
-      } else {
-        const double x = __dmul_rn(bn, ve);
-        d = __dadd_rn(__dmul_rn(bem_exp_cr(__dmul_rn(__dmul_rn(bn2, ve), ve)), bem_exp_cr(-__dmul_rn(x, x))), -1.0);
-      }
-      dF2 = cscale(ce, 2.0 * d);
+      dF2 = cscale(ce, 2.0 * ew_plane_residue(q, n1, n2, bn2, bn, ve));
     } else {
       dF2 = cscale(cmul(ce, cmk(ef * w.re - ff.re, -ff.im)), 2.0);
     }
@@ -312,12 +322,9 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     const double bn = sqrt(-bn2), bv = bn * ve;
     double f1, f2;
     if (fabs(rz) < BEM_PLANE_NEAR) {
-      // Next to the lattice plane f1 - f2 is zero, or not, by rounding alone,
-      // and the rows' stopping tests see that zero: form both exactly as the
-      // reference does (ebz = exp(bn z), f2 with 1/ebz; d3_qpgf_d2.c:2003-2007).
-      const double ebz = bem_exp_cr(__dmul_rn(bn, rz)), bvr = __dmul_rn(bn, ve);
-      f1 = __dmul_rn(ebz, erfc(__dadd_rn(bvr, azve)));
-      f2 = __dmul_rn(__ddiv_rn(1.0, ebz), erfc(__dadd_rn(bvr, -azve)));
+      const double2 f = ew_plane_evanescent(bn, ve, rz, azve);
+      f1 = f.x;
+      f2 = f.y;
     } else {
       // = e^{-Q} erfcx(bn ve +- z/2ve) with Q = bn^2 ve^2 + (z/2ve)^2: one exp
       const double eq = exp(-(bv * bv + azve * azve));
