@@ -289,8 +289,8 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   c->qp.eta_run = c->qp.eta0 * c->eta_scale;
   if (bem_launch_wtab(c->qp.k * c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
-  c->qp.wt_h = 0.125;
-  c->qp.wt_n = 64;
+  c->qp.wt_h = BEM_WT_H;
+  c->qp.wt_n = BEM_WT_N;
   memcpy(c->pw, pr->pw, sizeof(c->pw));
   if (upload(c, &c->pw_d, c->pw, 16, "pw")) return -1;
   const int nd = pr->MN + 1;
@@ -1015,8 +1015,8 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   if (cudaMalloc(&wt, BEM_WT_SIZE * sizeof(double)) != cudaSuccess) return -1;
   if (bem_launch_wtab(q.k * q.eta_run, wt, 0) != 0) { cudaFree(wt); return -1; }
   q.wt = wt;
-  q.wt_h = 0.125;
-  q.wt_n = 64;
+  q.wt_h = BEM_WT_H;
+  q.wt_n = BEM_WT_N;
   double *dr = nullptr, *dg = nullptr, *ddg = nullptr;
   int *dret = nullptr;
   int rc = -1;

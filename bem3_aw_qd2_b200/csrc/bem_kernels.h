@@ -54,4 +54,3 @@ int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int
 #define BEM_GLN_H 12
 #define BEM_GHN_H 64
 #define BEM_MAXNEAR_H 64
-#define BEM_WT_SIZE (2 * 11 * 64)  // doubles in the w table (BEM_WT_DEG x BEM_WT_N complex)

@@ -38,9 +38,6 @@
 #define BEM_S_LIMIT 15         // d3_qpgf_d2.h:19
 #define BEM_W_TAB 48           // exp(-a^2 n^2) table length
 #define BEM_FD_MAX_TERMS 250.0 // spectral-only sum used when it needs fewer terms than this
-#define BEM_WT_DEG 11          // Chebyshev terms per interval of the w(x + i y) table: truncation below 2e-19 relative (checked for 0.05 <= x <= 6 against 30-digit w)
-#define BEM_WT_H 0.125         // interval width in y
-#define BEM_WT_N 64            // intervals: y in [0, 8)
 
 // Algorithm 916 constants for relerr = 1e-15: a = pi / sqrt(-ln(relerr/2)),
 // c = 2a/pi, tab[n-1] = exp(-a^2 n^2).  Filled once by bem_device_init().
