@@ -1213,32 +1213,33 @@ __global__ void __launch_bounds__(128) k_qpgf_points(const __grid_constant__ bem
   dG[6 * i + 4] = v.gz.re; dG[6 * i + 5] = v.gz.im;
 }
 
-// ------------------------------------------------------------------ w(x + i y) table
-// One block per interval j of width BEM_WT_H: w at the BEM_WT_DEG Chebyshev
-// nodes of the interval, then the Chebyshev coefficients (discrete cosine sums).
-__global__ void k_wtab_build(double x, double *__restrict__ out) {
-  __shared__ double fr[BEM_WT_DEG], fi[BEM_WT_DEG];
+// ------------------------------------------------------------------ real-space term table
+// One block per interval j of width BEM_WT_H: A(y), B(y) (ew_real_ab) at the
+// BEM_WT_DEG Chebyshev nodes of the interval, then the Chebyshev coefficients
+// (discrete cosine sums).
+__global__ void k_wtab_build(double k, double ve, double *__restrict__ out) {
+  __shared__ double fa[BEM_WT_DEG], fb[BEM_WT_DEG];
   const int j = blockIdx.x, m = threadIdx.x;
   const double n = BEM_WT_DEG;
   const double tm = cos(CUDART_PI * (m + 0.5) / n);
-  const cplx w = bem_faddeeva(x, (j + 0.5 * (1.0 + tm)) * BEM_WT_H);
-  fr[m] = w.re;
-  fi[m] = w.im;
+  const double2 ab = ew_real_ab(k, ve, k * ve, (j + 0.5 * (1.0 + tm)) * BEM_WT_H);
+  fa[m] = ab.x;
+  fb[m] = ab.y;
   __syncthreads();
-  double sr = 0.0, si = 0.0;
+  double sa = 0.0, sb = 0.0;
   for (int mm = 0; mm < BEM_WT_DEG; ++mm) {
     const double c = cos(CUDART_PI * m * (mm + 0.5) / n);
-    sr += fr[mm] * c;
-    si += fi[mm] * c;
+    sa += fa[mm] * c;
+    sb += fb[mm] * c;
   }
   const double f = (m == 0 ? 1.0 : 2.0) / n;
-  out[2 * ((size_t)j * BEM_WT_DEG + m)] = sr * f;
-  out[2 * ((size_t)j * BEM_WT_DEG + m) + 1] = si * f;
+  out[2 * ((size_t)j * BEM_WT_DEG + m)] = sa * f;
+  out[2 * ((size_t)j * BEM_WT_DEG + m) + 1] = sb * f;
 }
 
 // ------------------------------------------------------------------ host launchers
-extern "C" int bem_launch_wtab(double x, double *out, cudaStream_t st) {
-  k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(x, out);
+extern "C" int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st) {
+  k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(k, ve, out);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -45,7 +45,7 @@ struct bemgpu_ctx {
   size_t dwork_sz = 0;
   std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
-  double *wtab = nullptr;  // w(k eta0 + i y) table of the Ewald real-space sums
+  double *wtab = nullptr;  // real-space term table of the Ewald sums (A, B at eta_run)
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
   double eta_scale = 1.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale
   double *pw_d = nullptr;
@@ -287,7 +287,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   bem_qp_prepare(pr->qp, &c->qp);
   CK(dalloc(&c->wtab, BEM_WT_SIZE), "w table");
   c->qp.eta_run = c->qp.eta0 * c->eta_scale;
-  if (bem_launch_wtab(c->qp.k * c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
+  if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
   c->qp.wt_h = BEM_WT_H;
   c->qp.wt_n = BEM_WT_N;
@@ -418,7 +418,7 @@ extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
   c->factored = false;
   if (!c->loaded) return 0;
   c->qp.eta_run = c->qp.eta0 * scale;
-  if (bem_launch_wtab(c->qp.k * c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
+  if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   return 0;
 }
 
@@ -441,7 +441,7 @@ extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
     bem_qp q = c->qp;
     q.eta_run = q.eta0 * cand[i];
     q.wt = tab;
-    if (bem_launch_wtab(q.k * q.eta_run, tab, c->stream)) { rc = fail(c, "autotune", cudaGetLastError()); break; }
+    if (bem_launch_wtab(q.k, q.eta_run, tab, c->stream)) { rc = fail(c, "autotune", cudaGetLastError()); break; }
     float t = 0.f, tmin = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       if (bem_time_regular(&D, &q, &c->scr, c->G[0], c->H[0], 0.125, 4, c->stream, &t)) {
@@ -1013,7 +1013,7 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   bem_qp_prepare(qpar, &q);
   double *wt = nullptr;
   if (cudaMalloc(&wt, BEM_WT_SIZE * sizeof(double)) != cudaSuccess) return -1;
-  if (bem_launch_wtab(q.k * q.eta_run, wt, 0) != 0) { cudaFree(wt); return -1; }
+  if (bem_launch_wtab(q.k, q.eta_run, wt, 0) != 0) { cudaFree(wt); return -1; }
   q.wt = wt;
   q.wt_h = BEM_WT_H;
   q.wt_n = BEM_WT_N;

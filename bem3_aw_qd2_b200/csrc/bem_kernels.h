@@ -31,7 +31,8 @@ extern "C" {
 int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh);
 int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 // table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)
-int bem_launch_wtab(double x, double *out, cudaStream_t st);
+// the real-space term table of the problem with wave number k and Ewald parameter ve
+int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
 int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, int grad, double k, int type, int npts,
                      const double *pts, const double *P, const double *dP, const double *pv, const double *dpv,

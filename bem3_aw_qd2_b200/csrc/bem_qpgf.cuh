@@ -159,40 +159,59 @@ __device__ __forceinline__ bool bem_small(cplx t, cplx s, double eps) {
 
 struct bem_gval { cplx g, gx, gy, gz; };
 
-// w(x + i y) from the per-problem table (x = k eta_run, 0 <= y < 8): Clenshaw
-// recurrence on the interval's Chebyshev series.  Terms with y >= 8 are below
-// 1e-27 of the leading one and never reached by the stopping rule; they fall
-// back to the direct evaluation.
-__device__ __forceinline__ cplx bem_wtab(const bem_qp &q, double x, double y) {
+// The real-space Ewald term of a lattice point at distance rl from the
+// evaluation point, with x = k ve and y = rl / (2 ve), needs
+//   A(y) = e^{x^2 - y^2} Re w(x + i y)
+//   B(y) = e^{x^2 - y^2} (Re w / (2 ve) - k y Im w + y / (ve sqrt(pi)))
+// (term = A / rl, its radial factor = 2 ve B / rl^3).  Both are functions of y
+// alone for a problem's k and ve = eta_run, so they are tabulated once per
+// problem (piecewise Chebyshev on [0, 8), coefficients built on the device from
+// the Faddeeva function): one Clenshaw recurrence replaces a Faddeeva value and
+// an exp per term.  Truncation is below 5e-17 of the largest value (checked
+// against 30-digit arithmetic); y >= 8 (terms below 1e-27 of the leading one,
+// never reached by the stopping rule) falls back to the direct forms.
+__device__ __forceinline__ double2 ew_real_ab(double k, double ve, double x, double y) {
+  const cplx w = bem_faddeeva(x, y);
+  const double ef = exp(x * x - y * y);
+  return make_double2(ef * w.re, ef * (w.re * (0.5 / ve) - k * y * w.im + y * (0.56418958354775628695 / ve)));
+}
+__device__ __forceinline__ double2 bem_wtab(const bem_qp &q, double ve, double x, double y) {
   const double u = y * (1.0 / BEM_WT_H);
   const int j = (int)u;
-  if (j >= q.wt_n) return bem_faddeeva(x, y);
+  if (j >= q.wt_n) return ew_real_ab(q.k, ve, x, y);
   const double t = 2.0 * (u - j) - 1.0, t2 = 2.0 * t;
   const double2 *c = reinterpret_cast<const double2 *>(q.wt) + (size_t)j * BEM_WT_DEG;
-  double br = 0.0, bi = 0.0, b1r = 0.0, b1i = 0.0;
+  double ba = 0.0, bb = 0.0, b1a = 0.0, b1b = 0.0;
 #pragma unroll
   for (int k = BEM_WT_DEG - 1; k >= 1; --k) {
     const double2 ck = __ldg(c + k);
-    const double nr = ck.x + t2 * br - b1r, ni = ck.y + t2 * bi - b1i;
-    b1r = br; b1i = bi;
-    br = nr; bi = ni;
+    const double na = ck.x + t2 * ba - b1a, nb = ck.y + t2 * bb - b1b;
+    b1a = ba; b1b = bb;
+    ba = na; bb = nb;
   }
   const double2 c0 = __ldg(c);
-  return cmk(c0.x + t * br - b1r, c0.y + t * bi - b1i);
+  return make_double2(c0.x + t * ba - b1a, c0.y + t * bb - b1b);
 }
 
 // Ewald real-space term for lattice point (l1,l2)  (ew_qG1_v1_cFl, d3_qpgf_d2.c:1814).
 // ce = exp(i k_par . R_l) is supplied by the caller, which advances it along the
 // row by one complex multiplication per term instead of a sincos.
 __device__ __forceinline__ void ew_real_term(const bem_qp &q, double px, double py, double rz, cplx ce,
-                                             double ke, double ke2, double ive, bool tab, cplx &F, cplx &cf) {
+                                             double ke, double ke2, double ve, double ive, bool tab, cplx &F,
+                                             cplx &cf) {
   const double rl = sqrt(px * px + py * py + rz * rz);
   const double irl = 1.0 / rl;
   const double rl2e = rl * 0.5 * ive;
-  const double ef = exp(ke2 - rl2e * rl2e);
-  const cplx w = tab ? bem_wtab(q, ke, rl2e) : bem_faddeeva(ke, rl2e);
-  F = cscale(ce, irl * ef * w.re);
-  cf = cscale(ce, irl * irl * ef * (irl * w.re - q.k * w.im + ive * 0.56418958354775628695));
+  if (tab) {
+    const double2 ab = bem_wtab(q, ve, ke, rl2e);
+    F = cscale(ce, irl * ab.x);
+    cf = cscale(ce, 2.0 * ve * irl * irl * irl * ab.y);
+  } else {
+    const double ef = exp(ke2 - rl2e * rl2e);
+    const cplx w = bem_faddeeva(ke, rl2e);
+    F = cscale(ce, irl * ef * w.re);
+    cf = cscale(ce, irl * irl * ef * (irl * w.re - q.k * w.im + ive * 0.56418958354775628695));
+  }
 }
 
 // Ewald spectral term for reciprocal point (n1,n2) (ew_qG2_v1_cFn, d3_qpgf_d2.c:1965);
@@ -375,7 +394,7 @@ __device__ BEM_QPGF_ATTR int bem_qpgf_ewald(const bem_qp &q, double rx, double r
         for (; k < nmax; ++k, l2 += st) {
           const double px = rx + l1 * q.d1x + l2 * q.d2x, py = ry + l1 * q.d1y + l2 * q.d2y;
           cplx F, cf;
-          ew_real_term(q, px, py, rz, ce, ke, ke2, ive, tab, F, cf);
+          ew_real_term(q, px, py, rz, ce, ke, ke2, ve, ive, tab, F, cf);
           ++cc;
           s = cadd(s, F);
           sx = cadd(sx, cscale(cf, px));
@@ -578,13 +597,22 @@ __device__ int bem_qpgf2_ewald(const bem_qp &q, double rx, double ry, double rz,
           const double irl = 1.0 / rl, irl2 = irl * irl;
           const double rl2e = rl * 0.5 * ive;
           const double ef = exp(ke2 - rl2e * rl2e);
-          const cplx w = tab ? bem_wtab(q, ke, rl2e) : bem_faddeeva(ke, rl2e);
-          const cplx cef = cscale(ce, ef);
-          const cplx cf1 = cscale(cef, irl2 * (irl * w.re - q.k * w.im + ive * isp));
-          const cplx cf2 = cscale(cef, irl2 * (q.k * q.k * irl * 2.0 * w.re - ive * ive * ive * isp));
+          // A = ef Re w and the first-derivative factor from the table when it applies
+          double A, B1;
+          if (tab) {
+            const double2 ab = bem_wtab(q, ve, ke, rl2e);
+            A = ab.x;
+            B1 = 2.0 * ve * irl * irl * irl * ab.y;
+          } else {
+            const cplx w = bem_faddeeva(ke, rl2e);
+            A = ef * w.re;
+            B1 = irl2 * ef * (irl * w.re - q.k * w.im + ive * isp);
+          }
+          const cplx cf1 = cscale(ce, B1);
+          const cplx cf2 = cscale(ce, irl2 * (q.k * q.k * irl * 2.0 * A - ive * ive * ive * isp * ef));
           const cplx cf3 = cadd(cscale(cf1, -6.0 * irl2), cf2);
           ++cc;
-          s = cadd(s, cscale(cef, irl * w.re));
+          s = cadd(s, cscale(ce, irl * A));
           sd[0] = cadd(sd[0], cscale(cf1, px));
           sd[1] = cadd(sd[1], cscale(cf1, py));
           sd[2] = cadd(sd[2], cf1);

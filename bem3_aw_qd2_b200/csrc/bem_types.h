@@ -12,10 +12,11 @@
 #ifndef BEM_TYPES_H
 #define BEM_TYPES_H
 
-/* geometry of the per-problem w(x + i y) table (real-space Ewald terms): 9
- * Chebyshev terms on each of 128 intervals of width 1/16 in y in [0, 8);
- * truncation below 2e-18 relative (checked for 0.05 <= x <= 2.5 against a
- * 30-digit w), so the table adds nothing to the double rounding */
+/* geometry of the per-problem table of the real-space Ewald term factors
+ * A(y), B(y) (bem_qpgf.cuh): 9 Chebyshev terms on each of 128 intervals of
+ * width 1/16 in y in [0, 8); truncation below 5e-17 of the largest value
+ * (checked against 30-digit arithmetic), so the table adds nothing to the
+ * double rounding */
 #define BEM_WT_DEG 9
 #define BEM_WT_H 0.0625
 #define BEM_WT_N 128
@@ -42,9 +43,9 @@ typedef struct bem_qp {
   double sel_cm, sel_bm;        /*                     bN/bNm, bNm  */
   int nc1;                      /* round(k_par . d1 / 2 pi) */
   int ewald_only;               /* 1: always use the Ewald sum */
-  /* optional table of w(x + i y) for the Ewald real-space terms at
+  /* optional table of the real-space term factors (A, B) at ve = eta_run,
      x = k eta_run: piecewise Chebyshev, wt_n intervals of width wt_h on
-     y in [0, wt_n wt_h), BEM_WT_DEG (re, im) coefficients each; NULL: none */
+     y in [0, wt_n wt_h), BEM_WT_DEG (A, B) coefficients each; NULL: none */
   const double *wt;
   double wt_h;
   int wt_n;
