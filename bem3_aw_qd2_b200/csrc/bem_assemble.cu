@@ -1237,7 +1237,53 @@ __global__ void k_wtab_build(double k, double ve, double *__restrict__ out) {
   out[2 * ((size_t)j * BEM_WT_DEG + m) + 1] = sb * f;
 }
 
+// ------------------------------------------------------------------ evanescent spectral order table
+// Block (order, interval j), thread m: P and M (ew_spec_tab) at the m-th
+// Chebyshev node of the interval, then the Chebyshev coefficients.  M = (f1 -
+// f2) / d is the mean of erfcx' over [bv - d, bv + d] (64-point Gauss-Legendre;
+// erfcx' < 0 everywhere, so no cancellation) times e^{-bv^2 - d^2}.
+__global__ void k_stab_build(const __grid_constant__ bem_qp q, double ve, double *__restrict__ out) {
+  __shared__ double fp[BEM_ST_DEG], fm[BEM_ST_DEG];
+  const int ord = blockIdx.x, j = blockIdx.y, m = threadIdx.x;
+  const int n1 = q.st_n1lo + ord / q.st_n2cnt, n2 = q.st_n2lo + ord % q.st_n2cnt;
+  const double anx = bem_an(-q.kx, n1, q.g1x, n2, q.g2x), any = bem_an(-q.ky, n1, q.g1y, n2, q.g2y);
+  const double bn2 = __dadd_rn(__dadd_rn(__dmul_rn(q.k, q.k), -__dmul_rn(anx, anx)), -__dmul_rn(any, any));
+  double P = 0.0, M = 0.0;
+  if (bn2 < 0.0) {
+    const double bn = sqrt(-bn2), bv = bn * ve;
+    const double tm = cos(CUDART_PI * (m + 0.5) / BEM_ST_DEG);
+    const double d = (j + 0.5 * (1.0 + tm)) * BEM_ST_H;
+    const double e0 = exp(-(bv * bv + d * d));
+    P = e0 * (erfcx(bv + d) + erfcx(bv - d)) / bn;
+    double sg = 0.0;
+    for (int k = 0; k < BEM_GHN; ++k) {
+      const double x = bv + d * c_q.xh[k];
+      sg += c_q.wh[k] * (2.0 * x * erfcx(x) - 1.1283791670955125739);  // erfcx'(x); 2/sqrt(pi)
+    }
+    M = e0 * sg;
+  }
+  fp[m] = P;
+  fm[m] = M;
+  __syncthreads();
+  double sp = 0.0, sm = 0.0;
+  for (int mm = 0; mm < BEM_ST_DEG; ++mm) {
+    const double c = cos(CUDART_PI * m * (mm + 0.5) / BEM_ST_DEG);
+    sp += fp[mm] * c;
+    sm += fm[mm] * c;
+  }
+  const double f = (m == 0 ? 1.0 : 2.0) / BEM_ST_DEG;
+  double *o = out + 2 * (((size_t)ord * q.st_nint + j) * BEM_ST_DEG + m);
+  o[0] = sp * f;
+  o[1] = sm * f;
+}
+
 // ------------------------------------------------------------------ host launchers
+extern "C" int bem_launch_stab(const bem_qp *q, double *out, cudaStream_t st) {
+  if (q->st_n1cnt <= 0 || q->st_n2cnt <= 0 || q->st_nint <= 0) return 0;
+  k_stab_build<<<dim3(q->st_n1cnt * q->st_n2cnt, q->st_nint), BEM_ST_DEG, 0, st>>>(*q, q->eta_run, out);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st) {
   k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(k, ve, out);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;

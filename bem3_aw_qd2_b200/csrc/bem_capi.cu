@@ -46,6 +46,8 @@ struct bemgpu_ctx {
   std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
   double *wtab = nullptr;  // real-space term table of the Ewald sums (A, B at eta_run)
+  double *stab = nullptr;  // evanescent spectral order table (at eta_run)
+  double zspan = 0.0;      // height of the mesh (z extent of all elements)
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
   double eta_scale = 1.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale
   double *pw_d = nullptr;
@@ -136,7 +138,7 @@ static void free_problem(bemgpu_ctx *c) {
     dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
   }
   dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
-  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->b0); dfree(c->B3s);
+  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
   for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
     dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]);
     c->cn[d] = 0;
@@ -275,6 +277,44 @@ static int upload(bemgpu_ctx *c, T **dst, const T *src, size_t count, const char
   return 0;
 }
 
+// Window of the evanescent spectral order table for q: n1 within BEM_ST_W of
+// nc1, n2 within BEM_ST_W of every such row's centre, |d| = |z| / (2 eta_run)
+// up to zspan / (2 eta_run).  Returns the table's doubles (0: no table, when
+// it would exceed 64 MB).
+static size_t stab_window(bem_qp *q, double zspan) {
+  q->st = nullptr;
+  q->st_n1lo = q->nc1 - BEM_ST_W;
+  q->st_n1cnt = 2 * BEM_ST_W + 1;
+  int lo = 0, hi = 0;
+  for (int i = 0; i < q->st_n1cnt; ++i) {
+    const int n1 = q->st_n1lo + i;
+    const int nc = (int)round(-((-q->kx + n1 * q->g1x) * q->g2x + (-q->ky + n1 * q->g1y) * q->g2y) / q->g2sq);
+    if (i == 0 || nc < lo) lo = nc;
+    if (i == 0 || nc > hi) hi = nc;
+  }
+  q->st_n2lo = lo - BEM_ST_W;
+  q->st_n2cnt = hi - lo + 2 * BEM_ST_W + 1;
+  q->st_nint = (int)ceil(zspan / (2.0 * q->eta_run) / BEM_ST_H) + 1;
+  const size_t cnt = (size_t)q->st_n1cnt * q->st_n2cnt * q->st_nint * BEM_ST_DEG * 2;
+  if (cnt > ((size_t)64 << 20) / sizeof(double)) {
+    q->st_n1cnt = q->st_n2cnt = q->st_nint = 0;
+    return 0;
+  }
+  return cnt;
+}
+
+// (re)build the context's evanescent order table for its eta_run
+static int build_stab(bemgpu_ctx *c) {
+  dfree(c->stab);
+  c->stab = nullptr;
+  const size_t cnt = stab_window(&c->qp, c->zspan);
+  if (!cnt) return 0;
+  CK(dalloc(&c->stab, cnt), "spectral table");
+  if (bem_launch_stab(&c->qp, c->stab, c->stream) != 0) return fail(c, "spectral table", cudaGetLastError());
+  c->qp.st = c->stab;
+  return 0;
+}
+
 extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   CK(cudaSetDevice(c->device), "set device");
   free_problem(c);
@@ -291,6 +331,17 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   c->qp.wt = c->wtab;
   c->qp.wt_h = BEM_WT_H;
   c->qp.wt_n = BEM_WT_N;
+  {  // z extent of the mesh: every element within cr0 -+ (|cr1| + |cr2| + |cr3|)
+    double zlo = 0.0, zhi = 0.0;
+    for (int e = 0; e < pr->Ne; ++e) {
+      const double *z = pr->cr + (size_t)e * 12 + 8;
+      const double hw = fabs(z[1]) + fabs(z[2]) + fabs(z[3]);
+      if (e == 0 || z[0] - hw < zlo) zlo = z[0] - hw;
+      if (e == 0 || z[0] + hw > zhi) zhi = z[0] + hw;
+    }
+    c->zspan = zhi - zlo;
+  }
+  if (build_stab(c)) return -1;
   memcpy(c->pw, pr->pw, sizeof(c->pw));
   if (upload(c, &c->pw_d, c->pw, 16, "pw")) return -1;
   const int nd = pr->MN + 1;
@@ -419,7 +470,7 @@ extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
   if (!c->loaded) return 0;
   c->qp.eta_run = c->qp.eta0 * scale;
   if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
-  return 0;
+  return build_stab(c);
 }
 
 static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
@@ -431,7 +482,7 @@ extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   bem_dom_dev D = dom_view(c, 0);
   if (bem_launch_classify(&D, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
-  double *tab = nullptr;
+  double *tab = nullptr, *stab = nullptr;
   CK(dalloc(&tab, BEM_WT_SIZE), "autotune");
   const double cand[4] = {1.0, 1.1, 1.2, 1.3};
   double best = 1.0;
@@ -442,6 +493,17 @@ extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
     q.eta_run = q.eta0 * cand[i];
     q.wt = tab;
     if (bem_launch_wtab(q.k, q.eta_run, tab, c->stream)) { rc = fail(c, "autotune", cudaGetLastError()); break; }
+    // the candidate's own evanescent order table, as the assembly would use it
+    dfree(stab);
+    stab = nullptr;
+    const size_t scnt = stab_window(&q, c->zspan);
+    if (scnt) {
+      if (dalloc(&stab, scnt) != cudaSuccess || bem_launch_stab(&q, stab, c->stream)) {
+        rc = fail(c, "autotune", cudaGetLastError());
+        break;
+      }
+      q.st = stab;
+    }
     float t = 0.f, tmin = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       if (bem_time_regular(&D, &q, &c->scr, c->G[0], c->H[0], 0.125, 4, c->stream, &t)) {
@@ -454,6 +516,7 @@ extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
   }
   cudaStreamSynchronize(c->stream);
   cudaFree(tab);
+  dfree(stab);
   if (rc) return rc;
   if (best_scale) *best_scale = best;
   return bemgpu_set_ewald_scale(c, best);
@@ -1017,6 +1080,16 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
   q.wt = wt;
   q.wt_h = BEM_WT_H;
   q.wt_n = BEM_WT_N;
+  // evanescent order table reaching the points' |z|
+  double zmax = 0.0;
+  for (int i = 0; i < n; ++i) zmax = fabs(r[3 * i + 2]) > zmax ? fabs(r[3 * i + 2]) : zmax;
+  double *stb = nullptr;
+  const size_t scnt = stab_window(&q, 2.0 * zmax);
+  if (scnt) {
+    if (cudaMalloc(&stb, scnt * sizeof(double)) != cudaSuccess) { cudaFree(wt); return -1; }
+    if (bem_launch_stab(&q, stb, 0) != 0) { cudaFree(wt); cudaFree(stb); return -1; }
+    q.st = stb;
+  }
   double *dr = nullptr, *dg = nullptr, *ddg = nullptr;
   int *dret = nullptr;
   int rc = -1;
@@ -1031,6 +1104,6 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
         rc = -1;
     }
   }
-  cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret); cudaFree(wt);
+  cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret); cudaFree(wt); cudaFree(stb);
   return rc;
 }

@@ -33,6 +33,9 @@ int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 // table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)
 // the real-space term table of the problem with wave number k and Ewald parameter ve
 int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st);
+// the evanescent spectral order table of q (window and interval count set in q,
+// out: st_n1cnt x st_n2cnt x st_nint x BEM_ST_DEG (P, M) pairs)
+int bem_launch_stab(const bem_qp *q, double *out, cudaStream_t st);
 int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st);
 int bem_launch_field(const bem_dom_dev *D, const bem_qp *q, int periodic, int grad, double k, int type, int npts,
                      const double *pts, const double *P, const double *dP, const double *pv, const double *dpv,

@@ -314,6 +314,39 @@ __device__ __noinline__ double2 ew_plane_evanescent(double bn, double ve, double
                       __dmul_rn(__ddiv_rn(1.0, ebz), erfc(__dadd_rn(bvr, -azve))));
 }
 
+// Evanescent order n (beta_n^2 < 0, bv = |beta_n| ve) at d = z / (2 ve):
+//   f1 + f2 = e^{-bv^2 - d^2} (erfcx(bv + d) + erfcx(bv - d))   (even in d)
+//   f1 - f2 = d e^{-bv^2 - d^2} int_{-1}^{1} erfcx'(bv + d s) ds  (odd in d)
+// For a problem's k, k_par, lattice and ve = eta_run both depend on the point
+// only through d, so the per-problem table holds, per order of a window and
+// per interval of |d|, the Chebyshev series of P = (f1 + f2) / |beta_n| and
+// M = (f1 - f2) / d (no cancellation next to d = 0): one Clenshaw recurrence
+// replaces two erfcx, an exp, a square root and a division per term.
+// Truncation below 1e-16 of each interval's scale (checked against 30-digit
+// arithmetic).  Returns false where the table does not reach (order or |d|
+// outside it): the caller evaluates directly.
+__device__ __forceinline__ bool ew_spec_tab(const bem_qp &q, int n1, int n2, double d, double &P, double &M) {
+  const int i1 = n1 - q.st_n1lo, i2 = n2 - q.st_n2lo;
+  const double u = fabs(d) * (1.0 / BEM_ST_H);
+  const int j = (int)u;
+  if ((unsigned)i1 >= (unsigned)q.st_n1cnt || (unsigned)i2 >= (unsigned)q.st_n2cnt || j >= q.st_nint) return false;
+  const double t = 2.0 * (u - j) - 1.0, t2 = 2.0 * t;
+  const double2 *c = reinterpret_cast<const double2 *>(q.st) +
+                     ((size_t)(i1 * q.st_n2cnt + i2) * q.st_nint + j) * BEM_ST_DEG;
+  double bp = 0.0, bm = 0.0, b1p = 0.0, b1m = 0.0;
+#pragma unroll
+  for (int k = BEM_ST_DEG - 1; k >= 1; --k) {
+    const double2 ck = __ldg(c + k);
+    const double np = ck.x + t2 * bp - b1p, nm = ck.y + t2 * bm - b1m;
+    b1p = bp; b1m = bm;
+    bp = np; bm = nm;
+  }
+  const double2 c0 = __ldg(c);
+  P = c0.x + t * bp - b1p;
+  M = d * (c0.y + t * bm - b1m);
+  return true;
+}
+
 __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, double anx, double any, double rz, cplx ce,
                                             double ve, cplx &Fn, cplx &dF0, cplx &dF1, cplx &dF2) {
   const double bn2 = __dadd_rn(__dadd_rn(__dmul_rn(q.k, q.k), -__dmul_rn(anx, anx)), -__dmul_rn(any, any));
@@ -335,6 +368,15 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     return 0;
   } else if (bn2 < 0.0) {
     // f1 = e^{bn z} erfc(bn ve + z/2ve), f2 = e^{-bn z} erfc(bn ve - z/2ve)
+    double P, M;
+    if (q.st != nullptr && ve == q.eta_run && fabs(rz) >= BEM_PLANE_NEAR && ew_spec_tab(q, n1, n2, azve, P, M)) {
+      // Fn = ce / (i bn) (f1 + f2) = -i ce P
+      Fn = cmul(ce, cmk(0.0, -P));
+      dF0 = cscale(Fn, anx);
+      dF1 = cscale(Fn, any);
+      dF2 = cscale(ce, M);
+      return 1;
+    }
     const double bn = sqrt(-bn2), bv = bn * ve;
     double f1, f2;
     if (fabs(rz) < BEM_PLANE_NEAR) {
