@@ -1237,11 +1237,12 @@ __global__ void k_wtab_build(double k, double ve, double *__restrict__ out) {
   out[2 * ((size_t)j * BEM_WT_DEG + m) + 1] = sb * f;
 }
 
-// ------------------------------------------------------------------ evanescent spectral order table
-// Block (order, interval j), thread m: P and M (ew_spec_tab) at the m-th
-// Chebyshev node of the interval, then the Chebyshev coefficients.  M = (f1 -
-// f2) / d is the mean of erfcx' over [bv - d, bv + d] (64-point Gauss-Legendre;
-// erfcx' < 0 everywhere, so no cancellation) times e^{-bv^2 - d^2}.
+// ------------------------------------------------------------------ spectral order table
+// Block (order, interval j), thread m: the two channels of ew_spec_tab at the
+// m-th Chebyshev node of the interval, then the Chebyshev coefficients.  For an
+// evanescent order M = (f1 - f2) / d is twice the mean of erfcx' over
+// [bv - |d|, bv + |d|] (64-point Gauss-Legendre; erfcx' < 0 everywhere, so no
+// cancellation) times e^{-bv^2 - d^2}.
 __global__ void k_stab_build(const __grid_constant__ bem_qp q, double ve, double *__restrict__ out) {
   __shared__ double fp[BEM_ST_DEG], fm[BEM_ST_DEG];
   const int ord = blockIdx.x, j = blockIdx.y, m = threadIdx.x;
@@ -1249,10 +1250,17 @@ __global__ void k_stab_build(const __grid_constant__ bem_qp q, double ve, double
   const double anx = bem_an(-q.kx, n1, q.g1x, n2, q.g2x), any = bem_an(-q.ky, n1, q.g1y, n2, q.g2y);
   const double bn2 = __dadd_rn(__dadd_rn(__dmul_rn(q.k, q.k), -__dmul_rn(anx, anx)), -__dmul_rn(any, any));
   double P = 0.0, M = 0.0;
-  if (bn2 < 0.0) {
+  const double tm = cos(CUDART_PI * (m + 0.5) / BEM_ST_DEG);
+  const double d = (j - 0.5 * q.st_nint + 0.5 * (1.0 + tm)) * BEM_ST_H;  // intervals cover [-D, D)
+  if (bn2 > 0.0) {
+    // propagating: Q = e^{bv^2 - d^2} w(bv + i d)
+    const double bv = sqrt(bn2) * ve;
+    const cplx w = bem_faddeeva(bv, d);
+    const double ef = exp(bv * bv - d * d);
+    P = ef * w.re;
+    M = ef * w.im;
+  } else if (bn2 < 0.0) {
     const double bn = sqrt(-bn2), bv = bn * ve;
-    const double tm = cos(CUDART_PI * (m + 0.5) / BEM_ST_DEG);
-    const double d = (j + 0.5 * (1.0 + tm)) * BEM_ST_H;
     const double e0 = exp(-(bv * bv + d * d));
     P = e0 * (erfcx(bv + d) + erfcx(bv - d)) / bn;
     double sg = 0.0;

@@ -277,9 +277,9 @@ static int upload(bemgpu_ctx *c, T **dst, const T *src, size_t count, const char
   return 0;
 }
 
-// Window of the evanescent spectral order table for q: n1 within BEM_ST_W of
-// nc1, n2 within BEM_ST_W of every such row's centre, |d| = |z| / (2 eta_run)
-// up to zspan / (2 eta_run).  Returns the table's doubles (0: no table, when
+// Window of the spectral order table for q: n1 within BEM_ST_W of nc1, n2
+// within BEM_ST_W of every such row's centre, d = z / (2 eta_run) within
+// +-zspan / (2 eta_run).  Returns the table's doubles (0: no table, when
 // it would exceed 64 MB).
 static size_t stab_window(bem_qp *q, double zspan) {
   q->st = nullptr;
@@ -294,7 +294,7 @@ static size_t stab_window(bem_qp *q, double zspan) {
   }
   q->st_n2lo = lo - BEM_ST_W;
   q->st_n2cnt = hi - lo + 2 * BEM_ST_W + 1;
-  q->st_nint = (int)ceil(zspan / (2.0 * q->eta_run) / BEM_ST_H) + 1;
+  q->st_nint = 2 * ((int)ceil(zspan / (2.0 * q->eta_run) / BEM_ST_H) + 1);  // d in [-D, D)
   const size_t cnt = (size_t)q->st_n1cnt * q->st_n2cnt * q->st_nint * BEM_ST_DEG * 2;
   if (cnt > ((size_t)64 << 20) / sizeof(double)) {
     q->st_n1cnt = q->st_n2cnt = q->st_nint = 0;

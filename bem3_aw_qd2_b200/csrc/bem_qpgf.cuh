@@ -199,8 +199,8 @@ __device__ __forceinline__ double2 bem_wtab(const bem_qp &q, double ve, double x
 __device__ __forceinline__ void ew_real_term(const bem_qp &q, double px, double py, double rz, cplx ce,
                                              double ke, double ke2, double ve, double ive, bool tab, cplx &F,
                                              cplx &cf) {
-  const double rl = sqrt(px * px + py * py + rz * rz);
-  const double irl = 1.0 / rl;
+  const double r2 = px * px + py * py + rz * rz;
+  const double irl = rsqrt(r2), rl = r2 * irl;  // one reciprocal square root for both
   const double rl2e = rl * 0.5 * ive;
   if (tab) {
     const double2 ab = bem_wtab(q, ve, ke, rl2e);
@@ -314,37 +314,46 @@ __device__ __noinline__ double2 ew_plane_evanescent(double bn, double ve, double
                       __dmul_rn(__ddiv_rn(1.0, ebz), erfc(__dadd_rn(bvr, -azve))));
 }
 
-// Evanescent order n (beta_n^2 < 0, bv = |beta_n| ve) at d = z / (2 ve):
-//   f1 + f2 = e^{-bv^2 - d^2} (erfcx(bv + d) + erfcx(bv - d))   (even in d)
-//   f1 - f2 = d e^{-bv^2 - d^2} int_{-1}^{1} erfcx'(bv + d s) ds  (odd in d)
-// For a problem's k, k_par, lattice and ve = eta_run both depend on the point
-// only through d, so the per-problem table holds, per order of a window and
-// per interval of |d|, the Chebyshev series of P = (f1 + f2) / |beta_n| and
-// M = (f1 - f2) / d (no cancellation next to d = 0): one Clenshaw recurrence
-// replaces two erfcx, an exp, a square root and a division per term.
-// Truncation below 1e-16 of each interval's scale (checked against 30-digit
-// arithmetic).  Returns false where the table does not reach (order or |d|
-// outside it): the caller evaluates directly.
-__device__ __forceinline__ bool ew_spec_tab(const bem_qp &q, int n1, int n2, double d, double &P, double &M) {
+// A spectral order n at d = z / (2 ve), bv = |beta_n| ve, depends on the
+// point only through d once k, k_par, the lattice and ve = eta_run are fixed:
+//   evanescent (beta_n^2 < 0): f1 + f2 = e^{-bv^2 - d^2} (erfcx(bv + d) + erfcx(bv - d)),
+//     f1 - f2 = d e^{-bv^2 - d^2} int_{-1}^{1} erfcx'(bv + d s) ds;
+//     tabulated: P = (f1 + f2) / |beta_n| and M = (f1 - f2) / d (no
+//     cancellation next to d = 0);
+//   propagating (beta_n^2 > 0): Q = e^{bv^2 - d^2} w(bv + i d) = e^{-2 i bv d} erfc(d - i bv);
+//     tabulated: Re Q, Im Q.
+// The per-problem table holds, per order of a window and per interval of d in
+// [-D, D), the Chebyshev series of both channels: one Clenshaw recurrence
+// replaces two erfcx, an exp, a square root and a division per evanescent
+// term, and a Faddeeva value and an exp per propagating one.  Truncation below
+// 1e-16 of each interval's scale (checked against 30-digit arithmetic).
+// Returns false where the table does not reach (order or d outside it): the
+// caller evaluates directly.
+__device__ __forceinline__ bool ew_spec_tab(const bem_qp &q, int n1, int n2, double d, double &c0v, double &c1v) {
   const int i1 = n1 - q.st_n1lo, i2 = n2 - q.st_n2lo;
-  const double u = fabs(d) * (1.0 / BEM_ST_H);
+  const double u = d * (1.0 / BEM_ST_H) + 0.5 * q.st_nint;
+  if (!(u >= 0.0)) return false;
   const int j = (int)u;
   if ((unsigned)i1 >= (unsigned)q.st_n1cnt || (unsigned)i2 >= (unsigned)q.st_n2cnt || j >= q.st_nint) return false;
   const double t = 2.0 * (u - j) - 1.0, t2 = 2.0 * t;
   const double2 *c = reinterpret_cast<const double2 *>(q.st) +
                      ((size_t)(i1 * q.st_n2cnt + i2) * q.st_nint + j) * BEM_ST_DEG;
-  double bp = 0.0, bm = 0.0, b1p = 0.0, b1m = 0.0;
+  double b0 = 0.0, b1 = 0.0, b10 = 0.0, b11 = 0.0;
 #pragma unroll
   for (int k = BEM_ST_DEG - 1; k >= 1; --k) {
     const double2 ck = __ldg(c + k);
-    const double np = ck.x + t2 * bp - b1p, nm = ck.y + t2 * bm - b1m;
-    b1p = bp; b1m = bm;
-    bp = np; bm = nm;
+    const double n0 = ck.x + t2 * b0 - b10, n1v = ck.y + t2 * b1 - b11;
+    b10 = b0; b11 = b1;
+    b0 = n0; b1 = n1v;
   }
-  const double2 c0 = __ldg(c);
-  P = c0.x + t * bp - b1p;
-  M = d * (c0.y + t * bm - b1m);
+  const double2 cz = __ldg(c);
+  c0v = cz.x + t * b0 - b10;
+  c1v = cz.y + t * b1 - b11;
   return true;
+}
+// the table applies: built for this ve, and away from the lattice plane
+__device__ __forceinline__ bool ew_spec_tab_ok(const bem_qp &q, double ve, double rz) {
+  return q.st != nullptr && ve == q.eta_run && fabs(rz) >= BEM_PLANE_NEAR;
 }
 
 __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, double anx, double any, double rz, cplx ce,
@@ -353,8 +362,16 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
   const double azve = rz / (2.0 * ve);
   if (bn2 > 0.0) {
     const double bn = __dsqrt_rn(bn2);
-    const double ef = exp(bn2 * ve * ve - azve * azve);
     const cplx ff = cexpi(bn * rz);
+    double qr, qi;
+    if (ew_spec_tab_ok(q, ve, rz) && ew_spec_tab(q, n1, n2, azve, qr, qi)) {
+      Fn = cscale(cmul(ce, cmk(ff.re, qi + ff.im)), 2.0 / bn);
+      dF0 = cscale(Fn, anx);
+      dF1 = cscale(Fn, any);
+      dF2 = cscale(cmul(ce, cmk(qr - ff.re, -ff.im)), 2.0);
+      return 0;
+    }
+    const double ef = exp(bn2 * ve * ve - azve * azve);
     const cplx w = bem_faddeeva(bn * ve, azve);
     // Fn = 2 ce / bn (i ef Im w + ff)
     Fn = cscale(cmul(ce, cmk(ff.re, ef * w.im + ff.im)), 2.0 / bn);
@@ -368,13 +385,13 @@ __device__ __forceinline__ int ew_spec_term(const bem_qp &q, int n1, int n2, dou
     return 0;
   } else if (bn2 < 0.0) {
     // f1 = e^{bn z} erfc(bn ve + z/2ve), f2 = e^{-bn z} erfc(bn ve - z/2ve)
-    double P, M;
-    if (q.st != nullptr && ve == q.eta_run && fabs(rz) >= BEM_PLANE_NEAR && ew_spec_tab(q, n1, n2, azve, P, M)) {
-      // Fn = ce / (i bn) (f1 + f2) = -i ce P
+    double P, Mt;
+    if (ew_spec_tab_ok(q, ve, rz) && ew_spec_tab(q, n1, n2, azve, P, Mt)) {
+      // Fn = ce / (i bn) (f1 + f2) = -i ce P;  f1 - f2 = d M
       Fn = cmul(ce, cmk(0.0, -P));
       dF0 = cscale(Fn, anx);
       dF1 = cscale(Fn, any);
-      dF2 = cscale(ce, M);
+      dF2 = cscale(ce, azve * Mt);
       return 1;
     }
     const double bn = sqrt(-bn2), bv = bn * ve;

@@ -21,9 +21,9 @@
 #define BEM_WT_H 0.0625
 #define BEM_WT_N 128
 #define BEM_WT_SIZE (2 * BEM_WT_DEG * BEM_WT_N) /* doubles: BEM_WT_DEG x BEM_WT_N complex */
-/* per-problem table of the evanescent spectral orders (bem_qpgf.cuh): for
- * each order (n1, n2) of a window around the row centres, 10 Chebyshev terms
- * on intervals of width 1/8 in |z| / (2 eta_run), two channels */
+/* per-problem table of the spectral orders (bem_qpgf.cuh): for each order
+ * (n1, n2) of a window around the row centres, 10 Chebyshev terms on
+ * intervals of width 1/8 in z / (2 eta_run), two channels */
 #define BEM_ST_DEG 10
 #define BEM_ST_H 0.125
 #define BEM_ST_W 8  /* orders n1 - nc1 and n2 - (row centre) in [-8, 8] */
@@ -55,10 +55,11 @@ typedef struct bem_qp {
   const double *wt;
   double wt_h;
   int wt_n;
-  /* optional table of the evanescent spectral orders at ve = eta_run: orders
-     n1 in [st_n1lo, st_n1lo + st_n1cnt), n2 in [st_n2lo, st_n2lo + st_n2cnt),
-     st_nint intervals of width BEM_ST_H in |d| = |z| / (2 eta_run),
-     BEM_ST_DEG (P, M) coefficient pairs each; NULL: none */
+  /* optional table of the spectral orders at ve = eta_run: orders n1 in
+     [st_n1lo, st_n1lo + st_n1cnt), n2 in [st_n2lo, st_n2lo + st_n2cnt),
+     st_nint intervals of width BEM_ST_H covering d = z / (2 eta_run) in
+     [-st_nint BEM_ST_H / 2, st_nint BEM_ST_H / 2), BEM_ST_DEG coefficient
+     pairs each (two channels per order); NULL: none */
   const double *st;
   int st_n1lo, st_n1cnt, st_n2lo, st_n2cnt, st_nint;
   /* residues ef Re w - 1 of the propagating spectral orders (pz_n1, pz_n2) on
