@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <math.h>
+#include <unordered_map>
 #include <vector>
 #include "../../include/bemgpu.h"
 #include "bem_kernels.h"
@@ -24,6 +25,10 @@ struct bemgpu_ctx {
   char err[512] = {0};
   // problem
   bool loaded = false;
+  // bytes allocated behind each device-pointer field that a problem load sizes:
+  // a new load reuses an allocation that is large enough instead of freeing
+  // and allocating again (cudaFree waits for the device)
+  std::unordered_map<const void *, size_t> cap;
   int Ne = 0, NN = 0, MN = 0, n = 0;
   bem_qp qp;
   std::vector<int> dom_ne, dom_off, dom_tri;
@@ -125,36 +130,52 @@ static void dfree(T *&p) {
   if (p) cudaFree(p);
   p = nullptr;
 }
+// a problem-sized field of the context: reuses its allocation when it is large enough
+template <class T>
+static cudaError_t falloc(bemgpu_ctx *c, T **p, size_t count) {
+  const size_t bytes = (count ? count : 1) * sizeof(T);
+  auto it = c->cap.find((const void *)p);
+  if (*p && it != c->cap.end() && it->second >= bytes) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  c->cap.erase((const void *)p);
+  const cudaError_t e = cudaMalloc((void **)p, bytes);
+  if (e == cudaSuccess) c->cap[(const void *)p] = bytes;
+  return e;
+}
 
 // Gauss-Legendre tables and Faddeeva constants are uploaded once per device.
 static int g_const_dev = -1;
 
-static void free_problem(bemgpu_ctx *c) {
-  dfree(c->cr); dfree(c->cw); dfree(c->ren); dfree(c->wen); dfree(c->plane);
-  dfree(c->sid); dfree(c->rowidx); dfree(c->npe); dfree(c->eni); dfree(c->md); dfree(c->dom_ne_d); dfree(c->dom_off_d);
-  dfree(c->hk2); dfree(c->Pi); dfree(c->dPi); dfree(c->p_inc); dfree(c->v_inc); dfree(c->rho0_d); dfree(c->k2_d);
-  for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
-    dfree(c->G[d]); dfree(c->H[d]); dfree(c->dG[d]); dfree(c->dH[d]); dfree(c->dF[d]);
-    dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
+// release: give every problem buffer back (unload, destroy); otherwise a new
+// load follows and reuses the allocations that are large enough (falloc)
+static void free_problem(bemgpu_ctx *c, bool release) {
+  if (release) {
+    dfree(c->cr); dfree(c->cw); dfree(c->ren); dfree(c->wen); dfree(c->plane);
+    dfree(c->sid); dfree(c->rowidx); dfree(c->npe); dfree(c->eni); dfree(c->md); dfree(c->dom_ne_d); dfree(c->dom_off_d);
+    dfree(c->hk2); dfree(c->Pi); dfree(c->dPi); dfree(c->p_inc); dfree(c->v_inc); dfree(c->rho0_d); dfree(c->k2_d);
+    for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
+      dfree(c->G[d]); dfree(c->H[d]); dfree(c->dG[d]); dfree(c->dH[d]); dfree(c->dF[d]);
+      dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
+    }
+    dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
+    dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
+    for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
+    dfree(c->B3c);
+    dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
+    dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
+    c->cap.clear();
+    if (c->dwork) cudaFree(c->dwork);
+    c->dwork = nullptr;
+    c->dwork_sz = 0;
+    if (c->dwork2) cudaFree(c->dwork2);
+    c->dwork2 = nullptr;
+    c->dwork2_sz = 0;
   }
-  dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
-  dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
-  for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
-    dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]);
-    c->cn[d] = 0;
-  }
-  dfree(c->B3c);
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->cn[d] = 0;
   c->factored = false;
-  dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
-  dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
   c->nctr = 0;
   c->ntgt = 0;
-  if (c->dwork) cudaFree(c->dwork);
-  c->dwork = nullptr;
-  c->dwork_sz = 0;
-  if (c->dwork2) cudaFree(c->dwork2);
-  c->dwork2 = nullptr;
-  c->dwork2_sz = 0;
   c->loaded = false;
 }
 
@@ -200,7 +221,7 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  free_problem(c);
+  free_problem(c, true);
   dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
   dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
   for (int i = 0; i <= BEMGPU_MAXDOM; ++i)
@@ -272,7 +293,7 @@ static int ensure_constants(bemgpu_ctx *c, const double *xl, const double *wl, c
 
 template <class T>
 static int upload(bemgpu_ctx *c, T **dst, const T *src, size_t count, const char *what) {
-  CK(dalloc(dst, count), what);
+  CK(falloc(c, dst, count), what);
   if (src && count) CK(cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
   return 0;
 }
@@ -305,11 +326,9 @@ static size_t stab_window(bem_qp *q, double zspan) {
 
 // (re)build the context's evanescent order table for its eta_run
 static int build_stab(bemgpu_ctx *c) {
-  dfree(c->stab);
-  c->stab = nullptr;
   const size_t cnt = stab_window(&c->qp, c->zspan);
   if (!cnt) return 0;
-  CK(dalloc(&c->stab, cnt), "spectral table");
+  CK(falloc(c, &c->stab, cnt), "spectral table");
   if (bem_launch_stab(&c->qp, c->stab, c->stream) != 0) return fail(c, "spectral table", cudaGetLastError());
   c->qp.st = c->stab;
   return 0;
@@ -317,7 +336,10 @@ static int build_stab(bemgpu_ctx *c) {
 
 extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   CK(cudaSetDevice(c->device), "set device");
-  free_problem(c);
+  // the previous problem's work ends before its buffers are reused
+  if (c->stream) CK(cudaStreamSynchronize(c->stream), "load");
+  if (c->side) CK(cudaStreamSynchronize(c->side), "load");
+  free_problem(c, false);
   if (pr->MN + 1 > BEMGPU_MAXDOM) { snprintf(c->err, sizeof(c->err), "at most %d domains", BEMGPU_MAXDOM); return -2; }
   if (pr->ps != 1) { snprintf(c->err, sizeof(c->err), "only the quasi-periodic problem (ps=1) is implemented"); return -2; }
   for (int e = 0; e < pr->Ne; ++e)
@@ -325,7 +347,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   bem_qp_prepare(pr->qp, &c->qp);
-  CK(dalloc(&c->wtab, BEM_WT_SIZE), "w table");
+  CK(falloc(c, &c->wtab, BEM_WT_SIZE), "w table");
   c->qp.eta_run = c->qp.eta0 * c->eta_scale;
   if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
@@ -391,38 +413,38 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   for (int d = 0; d < nd; ++d) {
     const size_t N = 4 * (size_t)c->dom_ne[d];
     if ((int)N > maxN) maxN = (int)N;
-    CK(dalloc(&c->G[d], 2 * N * N), "G");
-    CK(dalloc(&c->H[d], 2 * N * N), "H");
+    CK(falloc(c, &c->G[d], 2 * N * N), "G");
+    CK(falloc(c, &c->H[d], 2 * N * N), "H");
     if (d > 0) {
-      CK(dalloc(&c->dG[d], 4 * N * N), "dG");
-      CK(dalloc(&c->dH[d], 4 * N * N), "dH");
+      CK(falloc(c, &c->dG[d], 4 * N * N), "dG");
+      CK(falloc(c, &c->dH[d], 4 * N * N), "dH");
     }
-    CK(dalloc(&c->dF[d], 3 * N), "dF");
-    CK(dalloc(&c->P[d], 2 * N), "P");
-    CK(dalloc(&c->dP[d], 2 * N), "dP");
-    CK(dalloc(&c->pv[d], 6 * N), "pv");
-    CK(dalloc(&c->dpv[d], 6 * N), "dpv");
+    CK(falloc(c, &c->dF[d], 3 * N), "dF");
+    CK(falloc(c, &c->P[d], 2 * N), "P");
+    CK(falloc(c, &c->dP[d], 2 * N), "dP");
+    CK(falloc(c, &c->pv[d], 6 * N), "pv");
+    CK(falloc(c, &c->dpv[d], 6 * N), "dpv");
     CK(cudaMemsetAsync(c->pv[d], 0, 6 * N * sizeof(double), c->stream), "pv");
   }
   int maxNe = 0;
   for (int d = 0; d < nd; ++d) maxNe = c->dom_ne[d] > maxNe ? c->dom_ne[d] : maxNe;
-  CK(dalloc(&c->scr.rowF, 3 * (size_t)maxN), "rowF");
-  CK(dalloc(&c->scr.near_s, (size_t)maxN * BEM_MAXNEAR_H), "near_s");
-  CK(dalloc(&c->scr.near_n, (size_t)maxN), "near_n");
-  CK(dalloc(&c->scr.nearF, (size_t)maxN * BEM_MAXNEAR_H * 3), "nearF");
-  CK(dalloc(&c->scr.selfF, 3 * (size_t)maxN), "selfF");
-  CK(dalloc(&c->scr.flag, (size_t)maxN * maxNe), "flag");
+  CK(falloc(c, &c->scr.rowF, 3 * (size_t)maxN), "rowF");
+  CK(falloc(c, &c->scr.near_s, (size_t)maxN * BEM_MAXNEAR_H), "near_s");
+  CK(falloc(c, &c->scr.near_n, (size_t)maxN), "near_n");
+  CK(falloc(c, &c->scr.nearF, (size_t)maxN * BEM_MAXNEAR_H * 3), "nearF");
+  CK(falloc(c, &c->scr.selfF, 3 * (size_t)maxN), "selfF");
+  CK(falloc(c, &c->scr.flag, (size_t)maxN * maxNe), "flag");
   c->scr.status = c->status;
   c->scr.terms = c->terms;
   CK(cudaMemsetAsync(c->terms, 0, 6 * sizeof(unsigned long long), c->stream), "counters");
   const size_t n = c->n;
-  CK(dalloc(&c->A, 2 * n * n), "A");
-  CK(dalloc(&c->b, 2 * n), "b");
-  CK(dalloc(&c->tpv, 6 * (size_t)c->NN), "tpv");
+  CK(falloc(c, &c->A, 2 * n * n), "A");
+  CK(falloc(c, &c->b, 2 * n), "b");
+  CK(falloc(c, &c->tpv, 6 * (size_t)c->NN), "tpv");
   for (int d = 0; d < nd; ++d) {
     const size_t N = 4 * (size_t)c->dom_ne[d];
-    CK(dalloc(&c->Wd[d], 2 * N * N), "dpv factors");
-    CK(dalloc(&c->ipd[d], N), "dpv pivots");
+    CK(falloc(c, &c->Wd[d], 2 * N * N), "dpv factors");
+    CK(falloc(c, &c->ipd[d], N), "dpv pivots");
     c->cn[d] = (int)N;
     if (c->dom_tri[d]) {
       std::vector<int> inv;
@@ -432,12 +454,12 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
       }
       c->cn[d] = (int)inv.size();
       if (upload(c, &c->cinv[d], inv.data(), inv.size(), "dpv index")) return -1;
-      CK(dalloc(&c->Gc[d], 2 * inv.size() * inv.size()), "dpv matrix");
-      if (!c->B3c) CK(dalloc(&c->B3c, 6 * (size_t)maxN), "dpv rhs");
+      CK(falloc(c, &c->Gc[d], 2 * inv.size() * inv.size()), "dpv matrix");
+      CK(falloc(c, &c->B3c, 6 * (size_t)maxN), "dpv rhs");
     }
   }
-  CK(dalloc(&c->B3, 6 * (size_t)maxN), "B3");
-  CK(dalloc(&c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
+  CK(falloc(c, &c->B3, 6 * (size_t)maxN), "B3");
+  CK(falloc(c, &c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "status");
   // device view of the system
   bem_sys_dev &S = c->sys;
@@ -525,7 +547,8 @@ extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
 extern "C" int bemgpu_unload(bemgpu_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  free_problem(c);
+  if (c->side) cudaStreamSynchronize(c->side);
+  free_problem(c, true);
   return 0;
 }
 
@@ -721,9 +744,9 @@ static int solve_tail(bemgpu_ctx *c) {
 }
 
 static int ensure_saves(bemgpu_ctx *c) {
-  if (c->precision != 0 && !c->b0) {
-    CK(dalloc(&c->b0, 2 * (size_t)c->n), "b copy");
-    CK(dalloc(&c->B3s, 6 * (size_t)c->NN), "B3 copy");
+  if (c->precision != 0) {
+    CK(falloc(c, &c->b0, 2 * (size_t)c->n), "b copy");
+    CK(falloc(c, &c->B3s, 6 * (size_t)c->NN), "B3 copy");
   }
   // mixed-precision state of every dense system, set up before any lane uses it
   for (int slot = 0; c->precision != 0 && slot <= c->MN + 1; ++slot)
@@ -1012,7 +1035,7 @@ static int ensure_centres(bemgpu_ctx *c) {
   if (upload(c, &c->ctr_t, t.data(), t.size(), "centres") || upload(c, &c->ctr_idx, idx.data(), idx.size(), "centres") ||
       upload(c, &c->ctr_ze, ze.data(), ze.size(), "centres"))
     return -1;
-  CK(dalloc(&c->ctr_bdv, 9 * t.size()), "centres");
+  CK(falloc(c, &c->ctr_bdv, 9 * t.size()), "centres");
   c->nctr = (int)t.size();
   return 0;
 }
@@ -1049,7 +1072,7 @@ static int ensure_force_targets(bemgpu_ctx *c) {
   if (upload(c, &c->tgt_t, t.data(), t.size(), "targets") || upload(c, &c->tgt_ze, ze.data(), ze.size(), "targets") ||
       upload(c, &c->tgt_w, w.data(), w.size(), "targets"))
     return -1;
-  CK(dalloc(&c->bdv, 9 * (size_t)n), "boundary values");
+  CK(falloc(c, &c->bdv, 9 * (size_t)n), "boundary values");
   c->ntgt = n;
   return 0;
 }

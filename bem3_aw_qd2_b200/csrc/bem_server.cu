@@ -237,7 +237,10 @@ static void worker(bemgpu_server *s, int idx) {
     }
     if (!reuse) {
       sl.resident = false;
-      rc = bemgpu_set_precision(sl.ctx, r->precision);
+      // the slot's device memory is what admission counted for this problem:
+      // give back the previous problem's buffers instead of reusing them
+      rc = bemgpu_unload(sl.ctx);
+      if (!rc) rc = bemgpu_set_precision(sl.ctx, r->precision);
       if (!rc) rc = bemgpu_load(sl.ctx, &r->prob.p);
       if (!rc) rc = bemgpu_set_ewald_scale(sl.ctx, BEMGPU_EWALD_RULE);
       if (!rc) rc = bemgpu_run(sl.ctx);

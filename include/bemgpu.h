@@ -70,7 +70,9 @@ const char *bemgpu_error(const bemgpu_ctx *ctx);
 unsigned bemgpu_status(bemgpu_ctx *ctx); /* BEMGPU_ST_* bits accumulated since load */
 
 /* Copy a problem from host memory to the device (replaces the state that
- * read_aqd2/initialize_aqd2 build, bem3_aw_qd2.c:3-109). */
+ * read_aqd2/initialize_aqd2 build, bem3_aw_qd2.c:3-109).  Device buffers of a
+ * previously loaded problem that are large enough are reused (no free and
+ * allocate per load); bemgpu_unload gives them back. */
 int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
 
 /* Ewald splitting parameter used off the lattice plane: eta0 x scale, where

@@ -120,3 +120,49 @@ def test_tri80_boundary_values(tri80_fields):
             ref = g[key]
             err = np.abs(np.array(a) - ref).reshape(len(ref), -1).max(axis=1)
             assert np.all(err[m] <= 1e-9 * np.max(np.abs(ref[m]))), (key, d, err[m] / np.max(np.abs(ref[m])))
+
+
+def test_context_reuse_across_problems():
+    """One context loads a 24-quad sphere, the 80-triangle sphere, the quad
+    sphere again, and the triangles again: device buffers of an earlier
+    problem are reused when large enough, grown when not, and every force
+    equals the one of a fresh context to 1e-12 of |F| (the same arithmetic
+    runs; only the order of floating-point atomics may differ)."""
+    import ctypes
+    from bem3_aw_qd2_b200 import api, meshgen
+    g = api.libs()[1]
+    g.bemgpu_load.argtypes = [ctypes.c_void_p, ctypes.POINTER(api.Problem)]
+    g.bemgpu_unload.argtypes = [ctypes.c_void_p]
+    cases = []
+    for name in ("sphere24", "tri80"):
+        d = tempfile.mkdtemp(prefix="reuse_%s_" % name)
+        cases.append(api.Case.from_files(*meshgen.write_inputs(d, **meshgen.CONFIGS[name])))
+    probs = [c.problem() for c in cases]
+
+    def forces(ctx, pr):
+        assert g.bemgpu_load(ctx, ctypes.byref(pr)) == 0, g.bemgpu_error(ctx)
+        assert g.bemgpu_run(ctx) == 0, g.bemgpu_error(ctx)
+        F, N, rc = np.zeros(3), np.zeros(3), np.zeros(3)
+        assert g.bemgpu_force(ctx, 0, api._p(rc), api._p(F), api._p(N)) == 0, g.bemgpu_error(ctx)
+        assert g.bemgpu_status(ctx) == 0
+        return np.concatenate([F, N])
+
+    fresh = []
+    for pr in probs:
+        ctx = ctypes.c_void_p()
+        assert g.bemgpu_create(0, None, ctypes.byref(ctx)) == 0
+        fresh.append(forces(ctx, pr))
+        g.bemgpu_destroy(ctx)
+    ctx = ctypes.c_void_p()
+    assert g.bemgpu_create(0, None, ctypes.byref(ctx)) == 0
+    try:
+        def same(a, b):
+            return np.max(np.abs(a - b)) <= 1e-12 * np.linalg.norm(b[:3])
+        for i in (0, 1, 0, 1):
+            assert same(forces(ctx, probs[i]), fresh[i]), i
+        assert g.bemgpu_unload(ctx) == 0
+        assert same(forces(ctx, probs[0]), fresh[0])
+    finally:
+        g.bemgpu_destroy(ctx)
+        for c, pr in zip(cases, probs):
+            c.free_problem(pr)
