@@ -73,8 +73,8 @@ __global__ void k_axpy_norms(double2 *__restrict__ x, const double2 *__restrict_
 // the solves use.  With the FP64 refinement behind it the weaker growth bound
 // of tournament pivoting costs nothing measurable; a refinement that does not
 // converge falls back to FP64.
-#define TS_ROWS 512
-#define TS_THREADS 512
+#define TS_ROWS 256
+#define TS_THREADS 256
 #define TS_NP (2 * LEAF_W)          // touched positions of one panel, at most
 #define TS_LIST (1 + 2 * TS_NP)     // count, positions, source positions
 
