@@ -63,13 +63,16 @@ def _write_dat(libpath, files, out):
     return open(out, "rb").read()
 
 
-def test_host_setup_matches_reference():
+@pytest.mark.parametrize("config", ["sphere24", "tri80"])
+def test_host_setup_matches_reference(config):
+    """read_aqd2 + initialize_aqd2 of this library against the reference's on
+    the same input files, for bilinear quads and linear triangles."""
     from oracle import refwrap
     from bem3_aw_qd2_b200 import meshgen
     if not refwrap.available():
         pytest.skip("oracle/_ref not built")
     d = tempfile.mkdtemp()
-    files = meshgen.write_inputs(d, **meshgen.CONFIGS["sphere24"])
+    files = meshgen.write_inputs(d, **meshgen.CONFIGS[config])
     mine = _write_dat(os.path.join(LIB, "libbem3_aw_qd2.so"), files, os.path.join(d, "mine.dat"))
     ref = _write_dat(refwrap.LIBPATH, files, os.path.join(d, "ref.dat"))
     assert len(mine) == len(ref)
