@@ -89,74 +89,77 @@ struct ts_shared {
   cuComplex prow[2][LEAF_W], krow[2][LEAF_W];
   int pid[2], kid[2];
 };
-// One elimination step K (a template parameter: every column index is a
-// compile-time constant, so the row stays in registers).
-template <int K>
-__device__ __forceinline__ void ts_step(cuComplex (&v)[LEAF_W], int &id, int rr, unsigned *status, ts_shared &sh) {
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
-  const int b = K & 1;
-  float val = -1.f;
-  if (t >= K && t < rr) val = fabsf(v[K].x) + fabsf(v[K].y);
-  int bi = t;
-  for (int o = 16; o > 0; o >>= 1) {
-    const float ov = __shfl_down_sync(0xffffffffu, val, o);
-    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-    if (ov > val || (ov == val && oi < bi)) { val = ov; bi = oi; }
-  }
-  if (lane == 0) { sh.wv[b][wid] = val; sh.wi[b][wid] = bi; }
-  __syncthreads();
-  float best = sh.wv[b][0];
-  int p = sh.wi[b][0];
-  for (int q = 1; q < nw; ++q) {
-    const float ov = sh.wv[b][q];
-    const int oi = sh.wi[b][q];
-    if (ov > best || (ov == best && oi < p)) { best = ov; p = oi; }
-  }
-  if (!(best > 0.f)) {
-    if (status && t == 0) atomicOr(status, 0x20u);
-    p = K;
-  }
-  if (t == p) {
+// The row of each thread is kept rotated: at step k its register 0 holds
+// column k, registers 1 .. 31 - k the columns still to be updated and the
+// registers after them the finished columns (multipliers, or U for a pivot
+// row).  Each step rotates every row left by one, so all register indices are
+// compile-time constants while the step stays one short loop body (fully
+// unrolled steps, each executed once per launch, stalled on instruction fetch:
+// twice the time); after the last step the rows are rotated back.
+__device__ __forceinline__ void ts_rotate(cuComplex (&v)[LEAF_W]) {
+  const cuComplex f = v[0];
 #pragma unroll
-    for (int c = 0; c < LEAF_W; ++c) sh.prow[b][c] = v[c];
-    sh.pid[b] = id;
-  }
-  if (t == K) {
-#pragma unroll
-    for (int c = 0; c < LEAF_W; ++c) sh.krow[b][c] = v[c];
-    sh.kid[b] = id;
-  }
-  __syncthreads();
-  if (t == K) {
-#pragma unroll
-    for (int c = 0; c < LEAF_W; ++c) v[c] = sh.prow[b][c];
-    id = sh.pid[b];
-  } else if (t == p) {
-#pragma unroll
-    for (int c = 0; c < LEAF_W; ++c) v[c] = sh.krow[b][c];
-    id = sh.kid[b];
-  }
-  const cuComplex d = sh.prow[b][K];
-  const float dn = d.x * d.x + d.y * d.y;
-  if (t > K && t < rr && dn > 0.f) {
-    const cuComplex l = cuCmulf(v[K], make_cuComplex(d.x / dn, -d.y / dn));
-    v[K] = l;
-#pragma unroll
-    for (int c = K + 1; c < LEAF_W; ++c) v[c] = cuCsubf(v[c], cuCmulf(l, sh.prow[b][c]));
-  }
-}
-template <int K>
-__device__ __forceinline__ void ts_steps(cuComplex (&v)[LEAF_W], int &id, int rr, int kmax, unsigned *status,
-                                         ts_shared &sh) {
-  if constexpr (K < LEAF_W) {
-    if (K < kmax) {
-      ts_step<K>(v, id, rr, status, sh);
-      ts_steps<K + 1>(v, id, rr, kmax, status, sh);
-    }
-  }
+  for (int c = 0; c < LEAF_W - 1; ++c) v[c] = v[c + 1];
+  v[LEAF_W - 1] = f;
 }
 __device__ void ts_gepp(cuComplex (&v)[LEAF_W], int &id, int rr, int w, unsigned *status, ts_shared &sh) {
-  ts_steps<0>(v, id, rr, min(w, rr), status, sh);
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
+  const int kmax = min(w, rr);
+  for (int k = 0; k < kmax; ++k) {
+    const int b = k & 1;
+    float val = -1.f;
+    if (t >= k && t < rr) val = fabsf(v[0].x) + fabsf(v[0].y);
+    int bi = t;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_down_sync(0xffffffffu, val, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > val || (ov == val && oi < bi)) { val = ov; bi = oi; }
+    }
+    if (lane == 0) { sh.wv[b][wid] = val; sh.wi[b][wid] = bi; }
+    __syncthreads();
+    float best = sh.wv[b][0];
+    int p = sh.wi[b][0];
+    for (int q = 1; q < nw; ++q) {
+      const float ov = sh.wv[b][q];
+      const int oi = sh.wi[b][q];
+      if (ov > best || (ov == best && oi < p)) { best = ov; p = oi; }
+    }
+    if (!(best > 0.f)) {
+      if (status && t == 0) atomicOr(status, 0x20u);
+      p = k;
+    }
+    if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LEAF_W; ++c) sh.prow[b][c] = v[c];
+      sh.pid[b] = id;
+    }
+    if (t == k) {
+#pragma unroll
+      for (int c = 0; c < LEAF_W; ++c) sh.krow[b][c] = v[c];
+      sh.kid[b] = id;
+    }
+    __syncthreads();
+    if (t == k) {
+#pragma unroll
+      for (int c = 0; c < LEAF_W; ++c) v[c] = sh.prow[b][c];
+      id = sh.pid[b];
+    } else if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LEAF_W; ++c) v[c] = sh.krow[b][c];
+      id = sh.kid[b];
+    }
+    const cuComplex d = sh.prow[b][0];
+    const float dn = d.x * d.x + d.y * d.y;
+    if (t > k && t < rr && dn > 0.f) {
+      const cuComplex l = cuCmulf(v[0], make_cuComplex(d.x / dn, -d.y / dn));
+      v[0] = l;
+#pragma unroll
+      for (int c = 1; c < LEAF_W; ++c)
+        if (c < LEAF_W - k) v[c] = cuCsubf(v[c], cuCmulf(l, sh.prow[b][c]));
+    }
+    ts_rotate(v);
+  }
+  for (int k = kmax; k < LEAF_W; ++k) ts_rotate(v);
   __syncthreads();
 }
 
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_ts_chunk(const cuComplex *__rest
   __shared__ ts_shared sh;
   const int row0 = j0 + blockIdx.x * TS_ROWS;
   const int rr = min(TS_ROWS, n - row0);
-  int id = threadIdx.x < rr ? row0 + threadIdx.x : -1;
+  int id = (int)threadIdx.x < rr ? row0 + (int)threadIdx.x : -1;
   cuComplex v[LEAF_W];
   ts_load_row(M, n, j0, w, id, v);
   ts_gepp(v, id, rr, w, nullptr, sh);
@@ -485,6 +488,9 @@ extern "C" int bem_mixed_init(bem_mixed *m, int mode, cudaStream_t st) {
   m->mode = mode;
   if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) return -1;
   CKB(cublasSetStream(m->blas, st));
+  // cuBLAS gets its workspace up front: a captured factorisation may not allocate
+  CKC(cudaMalloc(&m->blas_ws, BEM_MIXED_BLAS_WS));
+  CKB(cublasSetWorkspace(m->blas, m->blas_ws, BEM_MIXED_BLAS_WS));
   CKC(cudaMalloc(&m->status, sizeof(unsigned)));
   CKC(cudaMalloc(&m->norms, 2 * sizeof(unsigned long long)));
   CKC(cudaMemsetAsync(m->status, 0, sizeof(unsigned), st));
@@ -492,9 +498,11 @@ extern "C" int bem_mixed_init(bem_mixed *m, int mode, cudaStream_t st) {
 }
 
 extern "C" void bem_mixed_free(bem_mixed *m) {
+  if (m->gexec) cudaGraphExecDestroy(m->gexec);
+  if (m->graph) cudaGraphDestroy(m->graph);
   if (m->blas) cublasDestroy(m->blas);
   cudaFree(m->M); cudaFree(m->piv); cudaFree(m->R32); cudaFree(m->X); cudaFree(m->R); cudaFree(m->D);
-  cudaFree(m->ts_i); cudaFree(m->ts_c);
+  cudaFree(m->ts_i); cudaFree(m->ts_c); cudaFree(m->blas_ws);
   cudaFree(m->status); cudaFree(m->norms);
   *m = bem_mixed();
 }
@@ -505,11 +513,43 @@ extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream
       grow(m, &m->ts_i, &m->ts_i_cap, ts_ints(n)) ||
       grow(m, &m->ts_c, &m->ts_c_cap, (size_t)2 * LEAF_W * LEAF_W))
     return -1;
-  const size_t count = (size_t)n * n;
-  k_round_c32<<<grid_for(count), 256, 0, st>>>((const double2 *)A, m->M, count);
-  k_iota<<<(n + 255) / 256, 256, 0, st>>>(ts_gid(m, n), n);
-  CKC(cudaGetLastError());
-  return rec_lu(m, n, 0, n, st);
+  // The factorisation of a size is a fixed sequence of several hundred short
+  // launches (panels, TRSM, GEMM); it is captured once as a CUDA graph per
+  // (size, matrix and buffer addresses, arithmetic) and replayed, which takes
+  // the per-launch cost off the critical path.
+  const bool same = m->gexec && m->g_n == n && m->g_A == (const void *)A && m->g_M == (const void *)m->M &&
+                    m->g_ts == (const void *)m->ts_i && m->g_mode == m->mode;
+  if (!same) {
+    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->gexec = nullptr;
+    m->graph = nullptr;
+    CKC(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const size_t count = (size_t)n * n;
+    k_round_c32<<<grid_for(count), 256, 0, st>>>((const double2 *)A, m->M, count);
+    k_iota<<<(n + 255) / 256, 256, 0, st>>>(ts_gid(m, n), n);
+    int rc = cudaGetLastError() == cudaSuccess ? rec_lu(m, n, 0, n, st) : -1;
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(st, &g);
+    if (rc == 0 && ec != cudaSuccess) {
+      snprintf(m->err, sizeof(m->err), "capture of the factorisation: %s", cudaGetErrorString(ec));
+      rc = -1;
+    }
+    if (rc != 0) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return -1;
+    }
+    m->graph = g;
+    CKC(cudaGraphInstantiate(&m->gexec, m->graph, 0));
+    m->g_n = n;
+    m->g_A = A;
+    m->g_M = m->M;
+    m->g_ts = m->ts_i;
+    m->g_mode = m->mode;
+  }
+  CKC(cudaGraphLaunch(m->gexec, st));
+  return 0;
 }
 
 // B (n x nrhs, column-major complex FP64): right-hand sides in, solutions out

@@ -11,6 +11,7 @@
 #define BEM_MIXED_TF32 2    // TF32 tensor cores, FP32 accumulation
 #define BEM_MIXED_BF16X9 3  // FP32 emulated by three BF16 products on the tensor cores
 #define BEM_MIXED_BF16 4    // BF16 tensor cores, FP32 accumulation
+#define BEM_MIXED_BLAS_WS (32u << 20)  // cuBLAS workspace bytes per dense system
 
 struct bem_mixed {
   cublasHandle_t blas = nullptr;
@@ -27,6 +28,14 @@ struct bem_mixed {
   size_t ts_i_cap = 0;
   cuComplex *ts_c = nullptr;           // panel scratch: factored top block, displaced rows
   size_t ts_c_cap = 0;
+  // the factorisation as a CUDA graph, captured on the first call for a size
+  // and its buffers and replayed while they stay the same
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int g_n = 0, g_mode = 0;
+  const void *g_A = nullptr;
+  const void *g_M = nullptr, *g_ts = nullptr;
+  void *blas_ws = nullptr;             // cuBLAS workspace (no allocation inside a capture)
   unsigned *status = nullptr;          // 0x20: zero pivot
   unsigned long long *norms = nullptr; // max |d|, max |x| of the last refinement step
   char err[256] = {0};                 // the failing call of the last error
