@@ -54,7 +54,7 @@ struct bemgpu_ctx {
   double *stab = nullptr;  // evanescent spectral order table (at eta_run)
   double zspan = 0.0;      // height of the mesh (z extent of all elements)
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
-  double eta_scale = 1.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale
+  double eta_scale = 0.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale; 0: by rule per problem
   double *pw_d = nullptr;
   // 9-point targets on the domain-0 elements for the type-1 force
   int ntgt = 0;
@@ -324,6 +324,16 @@ static size_t stab_window(bem_qp *q, double zspan) {
   return cnt;
 }
 
+// The Ewald parameter by rule: k^2 eta^2 just below the reference's cap
+// EW_EXPM = 3 (d3_qpgf_d2.h:26, 1684-1697), so that no point needs its own
+// capped parameter (such points miss the per-problem term tables) and the
+// split leans as far to the cheaper spectral side as the cap allows; clamped
+// to [0.5, 1.3] x eta0.  Results agree with any other scale to round-off.
+static double ewald_rule_scale(const bem_qp &q) {
+  const double s = 0.98 * sqrt(3.0) / (q.k * q.eta0);
+  return s < 0.5 ? 0.5 : (s > 1.3 ? 1.3 : s);
+}
+
 // (re)build the context's evanescent order table for its eta_run
 static int build_stab(bemgpu_ctx *c) {
   const size_t cnt = stab_window(&c->qp, c->zspan);
@@ -348,7 +358,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   bem_qp_prepare(pr->qp, &c->qp);
   CK(falloc(c, &c->wtab, BEM_WT_SIZE), "w table");
-  c->qp.eta_run = c->qp.eta0 * c->eta_scale;
+  c->qp.eta_run = c->qp.eta0 * (c->eta_scale > 0.0 ? c->eta_scale : ewald_rule_scale(c->qp));
   if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   c->qp.wt = c->wtab;
   c->qp.wt_h = BEM_WT_H;
@@ -478,19 +488,14 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
 }
 
 extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
-  if (scale == BEMGPU_EWALD_RULE) {
-    // k^2 eta^2 just below the cap EW_EXPM (eta = sqrt(EW_EXPM) / k): the real-space
-    // terms keep their table and the split moves as far to the spectral side
-    // as that allows
-    if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
-    const double s = 0.98 * sqrt(3.0 /* EW_EXPM, d3_qpgf_d2.h:26 */) / (c->qp.k * c->qp.eta0);
-    scale = s < 1.0 ? 1.0 : (s > 1.3 ? 1.3 : s);
+  if (scale != BEMGPU_EWALD_RULE && !(scale >= 0.25 && scale <= 4.0)) {
+    snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale);
+    return -2;
   }
-  if (!(scale >= 0.25 && scale <= 4.0)) { snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale); return -2; }
-  c->eta_scale = scale;
+  c->eta_scale = scale;  // 0 (the rule) is applied to every problem loaded from now on
   c->factored = false;
   if (!c->loaded) return 0;
-  c->qp.eta_run = c->qp.eta0 * scale;
+  c->qp.eta_run = c->qp.eta0 * (scale > 0.0 ? scale : ewald_rule_scale(c->qp));
   if (bem_launch_wtab(c->qp.k, c->qp.eta_run, c->wtab, c->stream) != 0) return fail(c, "w table", cudaGetLastError());
   return build_stab(c);
 }
@@ -498,16 +503,19 @@ extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
 static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
 
 // Ewald-parameter autotuner: time the periodic regular-pair kernel on a
-// sample of the pairs for eta0 x {1.0, 1.1, 1.2, 1.3} (larger factors meet the
-// per-point cap and lose the tabulated real-space terms) and keep the fastest.
+// sample of the pairs for the rule's scale and three neighbours (larger
+// factors meet the per-point cap and lose the tabulated terms) and keep the
+// fastest.
 extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   bem_dom_dev D = dom_view(c, 0);
   if (bem_launch_classify(&D, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
   double *tab = nullptr, *stab = nullptr;
   CK(dalloc(&tab, BEM_WT_SIZE), "autotune");
-  const double cand[4] = {1.0, 1.1, 1.2, 1.3};
-  double best = 1.0;
+  // the rule's scale and its neighbours
+  const double r0 = ewald_rule_scale(c->qp);
+  const double cand[4] = {r0, 0.9 * r0, 0.8 * r0, r0 < 1.0 ? 1.0 : 1.1 * r0};
+  double best = r0;
   float tbest = 1e30f;
   int rc = 0;
   for (int i = 0; i < 4 && !rc; ++i) {

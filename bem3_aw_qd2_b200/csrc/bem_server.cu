@@ -242,7 +242,6 @@ static void worker(bemgpu_server *s, int idx) {
       rc = bemgpu_unload(sl.ctx);
       if (!rc) rc = bemgpu_set_precision(sl.ctx, r->precision);
       if (!rc) rc = bemgpu_load(sl.ctx, &r->prob.p);
-      if (!rc) rc = bemgpu_set_ewald_scale(sl.ctx, BEMGPU_EWALD_RULE);
       if (!rc) rc = bemgpu_run(sl.ctx);
     }
     if (!rc) rc = bemgpu_force(sl.ctx, r->force_type, r->rc, res.F, res.N);

@@ -80,17 +80,18 @@ int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
  * applies).  Both lattice sums converge to the reference's 1e-15 tolerance for
  * any scale, so the results agree to round-off while the split of the terms
  * between the real-space and spectral sums, and so the cost, changes.  On the
- * lattice plane (z = 0) eta0 is always used.  Default 1; kept across loads.
- * scale = BEMGPU_EWALD_RULE (0): the loaded problem's scale by rule, the
- * largest for which k^2 eta^2 stays below the cap (0.98 sqrt(3) / (k eta0),
- * clamped to [1, 1.3]: the autotuner's choice on the problems measured),
- * recomputed for this problem only. */
+ * lattice plane (z = 0) eta0 is always used.  scale = BEMGPU_EWALD_RULE (0,
+ * the default): each loaded problem's scale by rule, the largest for which
+ * k^2 eta^2 stays below the cap (0.98 sqrt(3) / (k eta0), clamped to
+ * [0.5, 1.3]; points past the cap would need their own parameter and miss the
+ * per-problem term tables); a scale in [0.25, 4] is used for every problem
+ * loaded until changed. */
 #define BEMGPU_EWALD_RULE 0.0
 int bemgpu_set_ewald_scale(bemgpu_ctx *ctx, double scale);
 
 /* Autotuner of the Ewald parameter for the loaded problem: times the periodic
- * regular-pair kernel on an eighth of the pairs for scales 1.0, 1.1, 1.2, 1.3
- * of eta0 and sets the fastest (bemgpu_set_ewald_scale); *best_scale gets it.
+ * regular-pair kernel on an eighth of the pairs for the rule's scale and three
+ * neighbours and sets the fastest (bemgpu_set_ewald_scale); *best_scale gets it.
  * Costs about half of one regular-pair launch. */
 int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
 
