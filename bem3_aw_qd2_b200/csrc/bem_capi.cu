@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <math.h>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 #include "../../include/bemgpu.h"
@@ -781,18 +782,42 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   CK(cudaEventRecord(c->ev_fork, c->stream), "fork");
   CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "fork");
   CK(cudaMemsetAsync(c->info2, 0, sizeof(int) * BEMGPU_MAXDOM, c->side), "fork");
-  for (int d = 0; d <= c->MN; ++d) {
-    const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
-    if (Nd == 0) continue;
-    double *M = c->G[d];
-    if (c->dom_tri[d]) {
-      if (bem_launch_compress(c->G[d], (int)Nd, c->cinv[d], c->cn[d], c->Gc[d], c->side)) return fail(c, "dpv", cudaGetLastError());
-      M = c->Gc[d];
+  auto side_lane = [c]() -> int {
+    for (int d = 0; d <= c->MN; ++d) {
+      const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
+      if (Nd == 0) continue;
+      double *M = c->G[d];
+      if (c->dom_tri[d]) {
+        if (bem_launch_compress(c->G[d], (int)Nd, c->cinv[d], c->cn[d], c->Gc[d], c->side))
+          return fail(c, "dpv", cudaGetLastError());
+        M = c->Gc[d];
+      }
+      const int r = dense_factor(c, 1 + d, M, c->cn[d], "dpv LU", 1);
+      if (r) return r;
     }
-    const int r = dense_factor(c, 1 + d, M, c->cn[d], "dpv LU", 1);
-    if (r) return r;
+    CK(cudaEventRecord(c->ev_join, c->side), "join");
+    return 0;
+  };
+  // A large FP64 factorisation holds the calling thread until it is done, so
+  // large dpv systems are factored from a second host thread: the global LU
+  // below then runs beside them instead of after them.
+  int max_nd = 0;
+  for (int d = 0; d <= c->MN; ++d) max_nd = 4 * c->dom_ne[d] > max_nd ? 4 * c->dom_ne[d] : max_nd;
+  int side_rc = 0;
+  std::thread side_thread;
+  if (max_nd >= 2048) {
+    side_thread = std::thread([c, &side_rc, &side_lane]() {
+      if (cudaSetDevice(c->device) != cudaSuccess) { side_rc = -1; return; }
+      side_rc = side_lane();
+    });
+  } else {
+    side_rc = side_lane();
+    if (side_rc) return side_rc;
   }
-  CK(cudaEventRecord(c->ev_join, c->side), "join");
+  struct joiner {
+    std::thread &t;
+    ~joiner() { if (t.joinable()) t.join(); }
+  } join_side{side_thread};
   CK(cudaMemsetAsync(c->A, 0, 2 * n * n * sizeof(double), c->stream), "A clear");
   CK(cudaMemsetAsync(c->b, 0, 2 * n * sizeof(double), c->stream), "b clear");
   for (int d = 0; d <= c->MN; ++d)
@@ -801,6 +826,9 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   int rc = dense_factor(c, 0, c->A, (int64_t)n, "global LU");
   if (!rc) rc = dense_apply(c, 0, c->A, (int64_t)n, 1, c->b, c->b0, "global solve");
   // join the side lane before anything reads the dpv factors
+  if (side_thread.joinable()) side_thread.join();
+  if (!rc) rc = side_rc;
+  if (rc) return rc;
   const cudaError_t je = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
   if (!rc && je != cudaSuccess) rc = fail(c, "join", je);
   if (!rc) rc = check_side_factors(c);
