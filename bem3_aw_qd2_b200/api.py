@@ -56,6 +56,7 @@ def libs():
         g.bemgpu_set_precision.argtypes = [vp, ctypes.c_int]
         g.bemgpu_get_precision.argtypes = [vp]
         g.bemgpu_set_ewald_scale.argtypes = [vp, ctypes.c_double]
+        g.bemgpu_set_far_rule.argtypes = [vp, ctypes.c_int]
         g.bemgpu_autotune.argtypes = [vp, _d]
         g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
         h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
@@ -228,6 +229,10 @@ class Case:
 
     def set_ewald_scale(self, scale):
         self._check(libs()[1].bemgpu_set_ewald_scale(self.ctx, float(scale)), "set_ewald_scale")
+
+    def set_far_rule(self, on):
+        """1 (default): 8 x 8 Gauss rule for far regular quad pairs of the periodic domain; 0: 12 x 12 everywhere."""
+        self._check(libs()[1].bemgpu_set_far_rule(self.ctx, int(bool(on))), "set_far_rule")
 
     def precision(self):
         """The precision mode in effect (see bemgpu.h)."""

@@ -55,6 +55,7 @@ struct bemgpu_ctx {
   double *stab = nullptr;  // evanescent spectral order table (at eta_run)
   double zspan = 0.0;      // height of the mesh (z extent of all elements)
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
+  int far_rule = 1;        // 8 x 8 rule for far quad pairs of the periodic domain (bemgpu_set_far_rule)
   double eta_scale = 0.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale; 0: by rule per problem
   double *pw_d = nullptr;
   // 9-point targets on the domain-0 elements for the type-1 force
@@ -488,6 +489,12 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   return 0;
 }
 
+extern "C" int bemgpu_set_far_rule(bemgpu_ctx *c, int on) {
+  c->far_rule = on ? 1 : 0;
+  c->factored = false;
+  return 0;
+}
+
 extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
   if (scale != BEMGPU_EWALD_RULE && !(scale >= 0.25 && scale <= 4.0)) {
     snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale);
@@ -510,7 +517,7 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
 extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   bem_dom_dev D = dom_view(c, 0);
-  if (bem_launch_classify(&D, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
+  if (bem_launch_classify(&D, &c->qp, 1, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
   double *tab = nullptr, *stab = nullptr;
   CK(dalloc(&tab, BEM_WT_SIZE), "autotune");
   // the rule's scale and its neighbours
@@ -989,6 +996,7 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d) {
   D.cr = c->cr; D.cw = c->cw; D.ren = c->ren; D.plane = c->plane; D.wen = c->wen;
   D.npe = c->npe;
   D.has_tri = c->dom_tri[d];
+  D.far_rule = c->far_rule;
   return D;
 }
 

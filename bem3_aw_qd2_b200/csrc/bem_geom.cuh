@@ -15,8 +15,10 @@
 #define BEM_P44 0.5773502691896257645091     // 1/sqrt(3)
 #define BEM_MAXNEAR 64         // near-singular sources kept per collocation node
 
+#define BEM_GFN 8              // far-pair rule (k_q0_far)
 struct bem_quad {
   double xl[BEM_GLN], wl[BEM_GLN];
+  double xf[BEM_GFN], wf[BEM_GFN];
   double xh[BEM_GHN], wh[BEM_GHN];
   double zt[4], et[4];        // collocation node parameters (zt_44, et_44)
   double z9[9], e9[9], w9[9]; // 9-point rule (zt_49, et_49, wt_49)

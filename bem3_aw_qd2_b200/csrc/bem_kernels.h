@@ -13,6 +13,7 @@ struct bem_dom_dev {
   const uint8_t *plane;         // 1 if the element is plane (bil_check_plane)
   const int *npe;               // nodes per element: 4 bilinear quad, 3 linear triangle
   int has_tri;                  // any triangle among the domain's elements
+  int far_rule;                 // periodic domain: 8 x 8 rule for far quad pairs (k_q0_far)
 };
 
 // Scratch used by one domain assembly (sized for N = 4 ne rows).
@@ -47,7 +48,7 @@ int bem_launch_bdval(const bem_dom_dev *D, const bem_qp *q, int periodic, double
 int bem_launch_force_bd(const bem_dom_dev *D, int ntgt, const int *tgt_t, const double *tgt_ze, const double *wts,
                         const double *bdv, const double *pw, double k2r, double k2i, const double *rc, double c0,
                         double rho0, double *out, cudaStream_t st);
-int bem_launch_classify(const bem_dom_dev *D, bem_scratch *S, cudaStream_t st);
+int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int periodic, bem_scratch *S, cudaStream_t st);
 int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, double frac,
                      int nchunk, cudaStream_t st, float *ms);
 int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,

@@ -113,6 +113,7 @@ extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw,
   bem_dom_dev D;
   D.ne = ne; D.sid = sid; D.cr = cr; D.cw = cw; D.ren = ren; D.plane = plane;
   D.wen = nullptr; D.npe = nullptr; D.has_tri = 0;  // bilinear elements only
+  D.far_rule = 0;                                   // the reference's 12 x 12 rule for every regular pair
   bem_qp q;
   bem_qp_prepare(qp, &q);
   if (bem_launch_assemble(&D, &q, periodic != 0, periodic != 0, k, &S, G, H, dG, dH, dF, st, nullptr) != 0) return -4;

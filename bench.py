@@ -483,14 +483,14 @@ def main():
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "solve_bieq_aqd2 + force_FN_aqd2 (C ABI, host buffers)"},
         "phase_ms": phase_ms,
-        "roofline": {"bound": "fp64", "kernel": "k_q0_regular", "achieved": achieved, "peak": FP64_PEAK_TFLOPS,
+        "roofline": {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far (regular pairs)", "achieved": achieved, "peak": FP64_PEAK_TFLOPS,
                      "unit": "TFLOP/s", "frac": (achieved / FP64_PEAK_TFLOPS) if achieved else None, "traffic": None,
                      "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
                      "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
                      "mean_terms_per_point": cnt[0] / max(cnt[3], 1)},
         "clocks": clk,
         "mixed": mixed,
-        "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1),
+        "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1 + 1),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)

@@ -111,6 +111,43 @@ TRI_BOUNDARY_POINTS = [  # on triangles: (zeta, eta) inside the reference triang
 ]
 
 
+def make_far_pairs():
+    """Reference coefficients G_i, H_i (q0_dcoef_bd_node_t2_cc) of 400 regular
+    pairs of the 216-quad sphere, most of them at least 5 element radii from
+    the nearest lattice image of the target (where the device may use a
+    shorter rule), the rest nearer."""
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    cfg = meshgen.CONFIGS["sphere216"]
+    files = meshgen.write_inputs(tmp, **cfg)
+    case = refwrap.RefCase(*files)
+    nodes, el = meshgen.cube_sphere(cfg["n"], cfg["semi_axes"])
+    P = nodes[el]
+    cen = P.mean(axis=1)
+    rad = np.max(np.linalg.norm(P - cen[:, None, :], axis=2), axis=1)
+    d1 = np.array(list(cfg["lattice"][0]) + [0.0])
+    d2 = np.array(list(cfg["lattice"][1]) + [0.0])
+    rng = np.random.default_rng(20241205)
+    ne = len(el)
+    picks = []
+    while len(picks) < 400:
+        t, s = int(rng.integers(ne)), int(rng.integers(ne))
+        if t == s:
+            continue
+        v = cen[t] - cen[s]
+        dmin = min(np.linalg.norm(v + a * d1 + b * d2) for a in (-1, 0, 1) for b in (-1, 0, 1))
+        far = dmin >= 5.5 * rad[s]
+        if not far and (dmin < 2.0 * rad[s] or sum(1 for x in picks if not x[3]) >= 80):
+            continue
+        picks.append((t + 1, int(rng.integers(4)), s + 1, far))
+    G = np.zeros((len(picks), 4), np.complex128)
+    H = np.zeros((len(picks), 4), np.complex128)
+    for i, (t, tn, s, _) in enumerate(picks):
+        cc = case.pair(0, t, tn, s)[0]
+        G[i], H[i] = cc[:4], cc[4:8]
+    idx = np.array([p[:3] for p in picks], np.int32)
+    np.savez_compressed(os.path.join(OUT, "far216.npz"), idx=idx, far=np.array([p[3] for p in picks]), G=G, H=H)
+
+
 def make_fields(case, out_name="fields24.npz", boundary_points=BOUNDARY_POINTS):
     out = {}
     out["F1"], out["N1"] = case.force(1)
@@ -149,6 +186,10 @@ def main():
         case = make_solve("tri80", "tri80.npz")
         make_fields(case, "fields_tri80.npz", TRI_BOUNDARY_POINTS)
         print("tri80.npz, fields_tri80.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["far"]:
+        make_far_pairs()
+        print("far216.npz written to", OUT)
         return
     if sys.argv[1:] == ["plane"]:
         make_plane()
