@@ -97,11 +97,17 @@ __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], co
 // gives the reference's 12 x 12 integrals to below 4e-14 of the entry
 // (checked against 40 x 40 on curved elements, k 2R up to 2.1).
 struct bem_far { int on; double d1x, d1y, d2x, d2y, idet, k; };
-__device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, const double rt[3]) {
+__device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
+  // squared circumradius about cr0 (the centre of a quad, the centroid of a
+  // triangle): corners (+-1, +-1), or (1, 0), (-1/2, +-sqrt3/2)
   double R2 = 0.0;
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const double sz = (c == 1 || c == 2) ? 1.0 : -1.0, se = c >= 2 ? 1.0 : -1.0;
+    double sz = (c == 1 || c == 2) ? 1.0 : -1.0, se = c >= 2 ? 1.0 : -1.0;
+    if (tri) {
+      sz = c == 0 ? 1.0 : -0.5;
+      se = c == 0 ? 0.0 : (c == 1 ? 0.5 * BEM_SQ3 : -0.5 * BEM_SQ3);
+    }
     double v2 = 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -184,7 +190,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
         if (k < BEM_MAXNEAR) list[k] = s;
       } else {
         sF += F; sFz += Fz; sFe += Fe;
-        if (fr.on && !tri && far_pair(fr, el, nd.rt)) fl = 3;
+        if (fr.on && far_pair(fr, el, nd.rt, tri)) fl = 3;
       }
     }
     flag[(size_t)p * D.ne + s] = fl;
@@ -373,8 +379,10 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   }
 }
 
-// Far quad pairs (flag 3, far_pair): the 8 x 8 Gauss rule, one thread per
-// point, 4 pairs per 256-thread block; otherwise as k_q0_regular.
+// Far pairs (flag 3, far_pair): the 8 x 8 Gauss rule on a quad, on each of
+// the 3 parts of a triangle; one thread per (a, b) point, 4 pairs per
+// 256-thread block, contributions accumulated in the thread's shared-memory
+// column; otherwise as k_q0_regular / k_q0_regular_tri.
 #define FP_THREADS 256
 __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
                                                         const uint8_t *__restrict__ flag, double *__restrict__ G,
@@ -387,43 +395,61 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
   const int p = valid ? (int)(pair / D.ne) : 0;
   const int s = valid ? (int)(pair % D.ne) : 0;
   const bool work = valid && flag[(size_t)p * D.ne + s] == 3;
-  double v[16];
 #pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
   unsigned long long nterm = 0, npt = 0;
   if (work) {
-    bem_node nd;
-    int t, te;
-    bem_load_node(D, p, nd, t, te);
-    bem_el el;
-    bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+    const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
+    const bool tri = bem_is_tri(D, se);
     const int i = pt >> 3, j = pt & 7;
-    const double z = c_q.xf[i], e = c_q.xf[j];
-    double vR[3], vW[3];
-    bem_rw(el, z, e, vR, vW);
-    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
-    bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
-    if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
-    nterm = rc > 0 ? (unsigned long long)rc : 0ULL;
-    npt = 1;
-    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-    const double wt = c_q.wf[i] * c_q.wf[j];
-    const cplx g = cscale(gv.g, aW * wt);
-    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-    double N[4];
-    bem_Nn4(z, e, N);
+    unsigned st = 0;
+    for (int part = 0; part < (tri ? 3 : 1); ++part) {
+      double z, e, vR[3], vW[3];
+      {
+        bem_el el;
+        bem_load_el(D.cr, D.cw, se, el);
+        if (tri) bem_tri_point_ref(part, c_q.xf[i], c_q.xf[j], z, e);
+        else { z = c_q.xf[i]; e = c_q.xf[j]; }
+        bem_rw(el, z, e, vR, vW);
+      }
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      v[2 * a] = g.re * N[a];
-      v[2 * a + 1] = g.im * N[a];
-      v[8 + 2 * a] = h.re * N[a];
-      v[8 + 2 * a + 1] = h.im * N[a];
+      for (int d = 0; d < 3; ++d) vR[d] -= __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d);
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+      if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      // re-derived after the call rather than kept live across it
+      double wt = c_q.wf[i] * c_q.wf[j];
+      if (tri) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
+        bem_tri_point_ref(part, c_q.xf[i], c_q.xf[j], z, e);
+        wt *= bem_tri_wfac(c_q.xf[i], c_q.xf[j]);
+      } else {
+        bem_el el;
+        bem_load_el(D.cr, D.cw, se, el);
+        z = c_q.xf[i]; e = c_q.xf[j];
+        double r[3];
+        bem_rw(el, z, e, r, vW);
+      }
+      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+      const cplx g = cscale(gv.g, aW * wt);
+      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+      double N[4];
+      if (tri) bem_Nn3(z, e, N);
+      else bem_Nn4(z, e, N);
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        acc[2 * n][threadIdx.x] += g.re * N[n];
+        acc[2 * n + 1][threadIdx.x] += g.im * N[n];
+        acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
+        acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
+      }
     }
+    set_status(status, st);
   }
   count_work(terms + 0, nterm, npt);
-#pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
   __syncthreads();
   if (threadIdx.x < 64) {
     const int q4 = threadIdx.x >> 4, c = threadIdx.x & 15;

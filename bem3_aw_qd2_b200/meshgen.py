@@ -160,6 +160,8 @@ CONFIGS = {
     "tri80": dict(ico=1, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
                   theta_deg=20.0, phi_deg=30.0),
     # near-normal incidence (the reference rejects kx = 0 or ky = 0)
+    "tri320": dict(ico=2, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
+                   theta_deg=20.0, phi_deg=30.0),
     "tri1280": dict(ico=3, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.4, 0.69282032302755091741)),
                     theta_deg=1e-6, phi_deg=45.0),
     # small case for fixtures and smoke tests: 24 quads, same physics

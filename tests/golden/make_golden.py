@@ -111,41 +111,44 @@ TRI_BOUNDARY_POINTS = [  # on triangles: (zeta, eta) inside the reference triang
 ]
 
 
-def make_far_pairs():
-    """Reference coefficients G_i, H_i (q0_dcoef_bd_node_t2_cc) of 400 regular
-    pairs of the 216-quad sphere, most of them at least 5 element radii from
-    the nearest lattice image of the target (where the device may use a
-    shorter rule), the rest nearer."""
+def make_far_pairs(name="sphere216", out_name="far216.npz", n_pairs=400, n_near=80):
+    """Reference coefficients G_i, H_i (q0_dcoef_bd_node_t2_cc) of n_pairs
+    regular pairs of the mesh, most of them at least 5 element circumradii
+    from the nearest lattice image of the target (where the device may use a
+    shorter rule), n_near of them nearer."""
     tmp = tempfile.mkdtemp(prefix="golden_")
-    cfg = meshgen.CONFIGS["sphere216"]
+    cfg = meshgen.CONFIGS[name]
     files = meshgen.write_inputs(tmp, **cfg)
     case = refwrap.RefCase(*files)
-    nodes, el = meshgen.cube_sphere(cfg["n"], cfg["semi_axes"])
+    if "ico" in cfg:
+        nodes, el = meshgen.icosphere(cfg["ico"], cfg["semi_axes"])
+    else:
+        nodes, el = meshgen.cube_sphere(cfg["n"], cfg["semi_axes"])
     P = nodes[el]
     cen = P.mean(axis=1)
     rad = np.max(np.linalg.norm(P - cen[:, None, :], axis=2), axis=1)
     d1 = np.array(list(cfg["lattice"][0]) + [0.0])
     d2 = np.array(list(cfg["lattice"][1]) + [0.0])
     rng = np.random.default_rng(20241205)
-    ne = len(el)
+    ne, nodes_per = len(el), el.shape[1]
     picks = []
-    while len(picks) < 400:
+    while len(picks) < n_pairs:
         t, s = int(rng.integers(ne)), int(rng.integers(ne))
         if t == s:
             continue
         v = cen[t] - cen[s]
         dmin = min(np.linalg.norm(v + a * d1 + b * d2) for a in (-1, 0, 1) for b in (-1, 0, 1))
         far = dmin >= 5.5 * rad[s]
-        if not far and (dmin < 2.0 * rad[s] or sum(1 for x in picks if not x[3]) >= 80):
+        if not far and (dmin < 2.0 * rad[s] or sum(1 for x in picks if not x[3]) >= n_near):
             continue
-        picks.append((t + 1, int(rng.integers(4)), s + 1, far))
+        picks.append((t + 1, int(rng.integers(nodes_per)), s + 1, far))
     G = np.zeros((len(picks), 4), np.complex128)
     H = np.zeros((len(picks), 4), np.complex128)
     for i, (t, tn, s, _) in enumerate(picks):
         cc = case.pair(0, t, tn, s)[0]
         G[i], H[i] = cc[:4], cc[4:8]
     idx = np.array([p[:3] for p in picks], np.int32)
-    np.savez_compressed(os.path.join(OUT, "far216.npz"), idx=idx, far=np.array([p[3] for p in picks]), G=G, H=H)
+    np.savez_compressed(os.path.join(OUT, out_name), idx=idx, far=np.array([p[3] for p in picks]), G=G, H=H)
 
 
 def make_fields(case, out_name="fields24.npz", boundary_points=BOUNDARY_POINTS):
@@ -189,7 +192,8 @@ def main():
         return
     if sys.argv[1:] == ["far"]:
         make_far_pairs()
-        print("far216.npz written to", OUT)
+        make_far_pairs("tri320", "far_tri320.npz", 300, 60)
+        print("far216.npz, far_tri320.npz written to", OUT)
         return
     if sys.argv[1:] == ["plane"]:
         make_plane()
