@@ -129,9 +129,27 @@ __device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, co
   return dmin2 >= 25.0 * R2;
 }
 
+// Compacted pair lists written by k_classify: regular pairs (flag 0) from the
+// front of one buffer, far pairs (flag 3) from its back, as p * ne + s.  A
+// kernel given a list runs a fixed grid over it; given none, it covers the
+// pair range [pair0, pair0 + npairs) one block per unit group and checks flags.
+struct bem_plist {
+  const unsigned *e;  // entry u is e[stride * u]
+  const unsigned *n;  // number of entries
+  long long stride;
+};
+__device__ __forceinline__ long long plist_units(const bem_plist &L, long long npairs) {
+  return L.e ? (long long)*L.n : npairs;
+}
+__device__ __forceinline__ long long plist_pair(const bem_plist &L, long long pair0, long long u) {
+  return L.e ? (long long)L.e[L.stride * u] : pair0 + u;
+}
+
 __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, double *__restrict__ rowF,
                                                    int *__restrict__ near_s, int *__restrict__ near_n,
-                                                   uint8_t *__restrict__ flag, unsigned *status) {
+                                                   uint8_t *__restrict__ flag, unsigned *status,
+                                                   unsigned *__restrict__ lst, unsigned *__restrict__ lcnt,
+                                                   unsigned long long lcap) {
   const int p = blockIdx.x;
   if (bem_pad_row(D, p)) {
     for (int s = threadIdx.x; s < D.ne; s += blockDim.x) flag[(size_t)p * D.ne + s] = 0;
@@ -220,6 +238,35 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
     rowF[3 * p + 1] = red[1][0];
     rowF[3 * p + 2] = red[2][0];
   }
+  if (!lst) return;
+  // this row's regular and far pairs into the lists (flags written above by
+  // this block; order within a row is immaterial: each pair writes its own entries)
+  __shared__ unsigned nreg, nfar, breg, bfar;
+  if (threadIdx.x == 0) nreg = nfar = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
+    const uint8_t fl = flag[(size_t)p * D.ne + s];
+    if (fl == 0) atomicAdd(&nreg, 1u);
+    else if (fl == 3) atomicAdd(&nfar, 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    breg = atomicAdd(lcnt, nreg);
+    bfar = atomicAdd(lcnt + 1, nfar);
+    nreg = nfar = 0;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
+    const uint8_t fl = flag[(size_t)p * D.ne + s];
+    const unsigned e = (unsigned)((size_t)p * D.ne + s);
+    if (fl == 0) {
+      const unsigned long long u = (unsigned long long)breg + atomicAdd(&nreg, 1u);
+      if (u < lcap) lst[u] = e;
+    } else if (fl == 3) {
+      const unsigned long long u = (unsigned long long)bfar + atomicAdd(&nfar, 1u);
+      if (u < lcap) lst[lcap - 1 - u] = e;
+    }
+  }
 }
 
 // ------------------------------------------------------------------ periodic regular pairs
@@ -233,19 +280,21 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
 __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, const __grid_constant__ bem_qp q, const uint8_t *__restrict__ flag,
                                                            double *__restrict__ G, double *__restrict__ H,
                                                            unsigned *status, unsigned long long *terms, long long pair0,
-                                                           long long npairs) {
+                                                           long long npairs, bem_plist L) {
   __shared__ double acc[16][RP_THREADS + 1];
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
-  const long long pair = pair0 + 2LL * blockIdx.x + lp;
-  const bool valid = pair < pair0 + npairs;
-  const int p = valid ? (int)(pair / D.ne) : 0;
-  const int s = valid ? (int)(pair % D.ne) : 0;
+  const long long nu = plist_units(L, npairs);
+  unsigned long long nterm = 0, npt = 0;
+  for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
+  const bool valid = u0 + lp < nu;
+  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+  const int p = (int)(pair / D.ne);
+  const int s = (int)(pair % D.ne);
   // triangle sources are k_q0_regular_tri's; padded rows keep their zeros
   const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && !bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
   double v[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c) v[c] = 0.0;
-  unsigned long long nterm = 0, npt = 0;
   if (work) {
     bem_node nd;
     int t, te;
@@ -260,8 +309,8 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
     bem_gval gv;
     const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
     if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
-    nterm = rc > 0 ? (unsigned long long)rc : 0ULL;
-    npt = 1;
+    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+    ++npt;
     const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
     const double wt = c_q.wl[i] * c_q.wl[j];
     const cplx g = cscale(gv.g, aW * wt);
@@ -276,14 +325,13 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
       v[8 + 2 * a + 1] = h.im * N[a];
     }
   }
-  count_work(terms + 0, nterm, npt);
 #pragma unroll
   for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
   __syncthreads();
   if (threadIdx.x < 32) {
     const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    const long long pr = pair0 + 2LL * blockIdx.x + q2;
-    if (pr < pair0 + npairs) {
+    if (u0 + q2 < nu) {
+      const long long pr = plist_pair(L, pair0, u0 + q2);
       const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
       if (flag[(size_t)pp * D.ne + ss] == 0 && !bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
         double sum = 0.0;
@@ -295,6 +343,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
       }
     }
   }
+  __syncthreads();  // acc is rewritten by the next unit group
+  }
+  count_work(terms + 0, nterm, npt);
 }
 
 // Triangle sources (q0_lit_dcoef_v2_cc_GL, q0_lit_dcoef_v2_cc.c:156-237 with
@@ -304,19 +355,21 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
                                                                const uint8_t *__restrict__ flag, double *__restrict__ G,
                                                                double *__restrict__ H, unsigned *status,
                                                                unsigned long long *terms, long long pair0,
-                                                               long long npairs) {
+                                                               long long npairs, bem_plist L) {
   __shared__ double acc[16][RP_THREADS + 1];
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
-  const long long pair = pair0 + 2LL * blockIdx.x + lp;
-  const bool valid = pair < pair0 + npairs;
-  const int p = valid ? (int)(pair / D.ne) : 0;
-  const int s = valid ? (int)(pair % D.ne) : 0;
+  const long long nu = plist_units(L, npairs);
+  unsigned long long nterm = 0, npt = 0;
+  for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
+  const bool valid = u0 + lp < nu;
+  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+  const int p = (int)(pair / D.ne);
+  const int s = (int)(pair % D.ne);
   const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
   // the 3 parts accumulate in this thread's shared-memory column, so that no
   // accumulator stays live in registers across the Green's-function calls
 #pragma unroll
   for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
-  unsigned long long nterm = 0, npt = 0;
   if (work) {
     const int i = pt / BEM_GLN, j = pt % BEM_GLN;
     const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
@@ -360,12 +413,11 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
     }
     set_status(status, st);
   }
-  count_work(terms + 0, nterm, npt);
   __syncthreads();
   if (threadIdx.x < 32) {
     const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    const long long pr = pair0 + 2LL * blockIdx.x + q2;
-    if (pr < pair0 + npairs) {
+    if (u0 + q2 < nu) {
+      const long long pr = plist_pair(L, pair0, u0 + q2);
       const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
       if (flag[(size_t)pp * D.ne + ss] == 0 && bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
         double sum = 0.0;
@@ -377,6 +429,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
       }
     }
   }
+  __syncthreads();  // acc is rewritten by the next unit group
+  }
+  count_work(terms + 0, nterm, npt);
 }
 
 // Far pairs (flag 3, far_pair): the 8 x 8 Gauss rule on a quad, on each of
@@ -387,17 +442,20 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
 __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
                                                         const uint8_t *__restrict__ flag, double *__restrict__ G,
                                                         double *__restrict__ H, unsigned *status,
-                                                        unsigned long long *terms, long long pair0, long long npairs) {
+                                                        unsigned long long *terms, long long pair0, long long npairs,
+                                                        bem_plist L) {
   __shared__ double acc[16][FP_THREADS + 1];
   const int lp = threadIdx.x >> 6, pt = threadIdx.x & 63;
-  const long long pair = pair0 + 4LL * blockIdx.x + lp;
-  const bool valid = pair < pair0 + npairs;
-  const int p = valid ? (int)(pair / D.ne) : 0;
-  const int s = valid ? (int)(pair % D.ne) : 0;
+  const long long nu = plist_units(L, npairs);
+  unsigned long long nterm = 0, npt = 0;
+  for (long long u0 = 4LL * blockIdx.x; u0 < nu; u0 += 4LL * gridDim.x) {
+  const bool valid = u0 + lp < nu;
+  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+  const int p = (int)(pair / D.ne);
+  const int s = (int)(pair % D.ne);
   const bool work = valid && flag[(size_t)p * D.ne + s] == 3;
 #pragma unroll
   for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
-  unsigned long long nterm = 0, npt = 0;
   if (work) {
     const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
     const bool tri = bem_is_tri(D, se);
@@ -449,12 +507,11 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
     }
     set_status(status, st);
   }
-  count_work(terms + 0, nterm, npt);
   __syncthreads();
   if (threadIdx.x < 64) {
     const int q4 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    const long long pr = pair0 + 4LL * blockIdx.x + q4;
-    if (pr < pair0 + npairs) {
+    if (u0 + q4 < nu) {
+      const long long pr = plist_pair(L, pair0, u0 + q4);
       const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
       if (flag[(size_t)pp * D.ne + ss] == 3) {
         double sum = 0.0;
@@ -466,6 +523,9 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
       }
     }
   }
+  __syncthreads();  // acc is rewritten by the next unit group
+  }
+  count_work(terms + 0, nterm, npt);
 }
 
 // ------------------------------------------------------------------ periodic near-singular pairs
@@ -1496,20 +1556,47 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
                cudaMemsetAsync(dH, 0, 4 * nn * sizeof(double), st) != cudaSuccess))
       return -1;
   }
-  if (ev) cudaEventRecord(ev[0], st);
-  k_classify<<<N, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status);
-  if (ev) cudaEventRecord(ev[1], st);
   const long long npairs = (long long)N * D->ne;
+  // compacted pair lists for the periodic domain when the scratch holds them
+  const bool lists = periodic && S->plist && S->pcount && (unsigned long long)npairs <= S->pcap &&
+                     npairs <= 0xffffffffLL;
+  if (lists && cudaMemsetAsync(S->pcount, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return -1;
+  if (ev) cudaEventRecord(ev[0], st);
+  k_classify<<<N, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
+                                lists ? S->plist : nullptr, S->pcount, S->pcap);
+  if (ev) cudaEventRecord(ev[1], st);
   if (periodic) {
-    const long long chunk = 1LL << 26;  // keep grid.x well inside limits
-    for (long long p0 = 0; p0 < npairs; p0 += chunk) {
-      const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
-      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+    if (lists) {
+      // one resident wave (2 blocks per SM) striding over each list
+      static int nsm = 0;
+      if (!nsm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+          nsm = 148;
+      }
+      const unsigned grid = 2u * (unsigned)nsm;
+      const bem_plist Lreg = {S->plist, S->pcount, 1};
+      const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
+      k_q0_regular<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
       if (D->far_rule)
-        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+        k_q0_far<<<grid, FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lfar);
       if (D->has_tri)
-        k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0,
-                                                                          np);
+        k_q0_regular_tri<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
+    } else {
+      const bem_plist L0 = {nullptr, nullptr, 0};
+      const long long chunk = 1LL << 26;  // keep grid.x well inside limits
+      for (long long p0 = 0; p0 < npairs; p0 += chunk) {
+        const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
+        k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+                                                                      L0);
+        if (D->far_rule)
+          k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+                                                                    L0);
+        if (D->has_tri)
+          k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+                                                                            p0, np, L0);
+      }
     }
     if (ev) cudaEventRecord(ev[2], st);
     k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
@@ -1544,13 +1631,17 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
     const long long p0 = npairs * c / nchunk;
     const long long np = p0 + len <= npairs ? len : npairs - p0;
     if (np > 0) {
-      // the kernels of the assembly itself: quad sources, and triangle sources when there are any
-      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+      // the kernels of the assembly itself (over pair ranges, not lists):
+      // quad sources, far pairs, and triangle sources when there are any
+      const bem_plist L0 = {nullptr, nullptr, 0};
+      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+                                                                    L0);
       if (D->far_rule)
-        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np);
+        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+                                                                  L0);
       if (D->has_tri)
         k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
-                                                                          p0, np);
+                                                                          p0, np, L0);
     }
   }
   cudaEventRecord(e1, st);
@@ -1563,7 +1654,8 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
 
 extern "C" int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int periodic, bem_scratch *S, cudaStream_t st) {
   if (D->ne <= 0) return 0;
-  k_classify<<<D->ne * 4, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status);
+  k_classify<<<D->ne * 4, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
+                                        nullptr, nullptr, 0);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 

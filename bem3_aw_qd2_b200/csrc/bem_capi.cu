@@ -161,6 +161,7 @@ static void free_problem(bemgpu_ctx *c, bool release) {
       dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
     }
     dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
+    dfree(c->scr.plist); dfree(c->scr.pcount);
     dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
     for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
     dfree(c->B3c);
@@ -446,6 +447,15 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   CK(falloc(c, &c->scr.nearF, (size_t)maxN * BEM_MAXNEAR_H * 3), "nearF");
   CK(falloc(c, &c->scr.selfF, 3 * (size_t)maxN), "selfF");
   CK(falloc(c, &c->scr.flag, (size_t)maxN * maxNe), "flag");
+  // pair lists of the periodic domain (32-bit entries: up to 2^32 pairs)
+  const size_t npair = (size_t)4 * c->dom_ne[0] * c->dom_ne[0];
+  if (npair > 0 && npair <= 0xffffffffull) {
+    CK(falloc(c, &c->scr.plist, npair), "pair lists");
+    CK(falloc(c, &c->scr.pcount, 2), "pair lists");
+    c->scr.pcap = npair;
+  } else {
+    c->scr.pcap = 0;
+  }
   c->scr.status = c->status;
   c->scr.terms = c->terms;
   CK(cudaMemsetAsync(c->terms, 0, 6 * sizeof(unsigned long long), c->stream), "counters");

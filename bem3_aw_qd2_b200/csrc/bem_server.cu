@@ -75,7 +75,8 @@ size_t problem_bytes(const bemgpu_problem *p, int precision) {
   size_t b = n * n * 16, f32 = n * n * 8;
   for (int d = 0; d <= p->MN; ++d) {
     const size_t N = 4 * (size_t)p->dom_ne[d];
-    b += 3 * N * N * 16 + (d > 0 ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] + N * 64 * 40;
+    // matrices, pair flags (and the periodic domain's 4-byte pair lists), near-singular tables
+    b += 3 * N * N * 16 + (d > 0 ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] * (d == 0 ? 5 : 1) + N * 64 * 40;
     f32 += N * N * 8;
   }
   if (precision) b += f32;

@@ -106,6 +106,9 @@ extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw,
   S.flag = (uint8_t *)(base + OFF_FLAG);
   S.status = (unsigned *)(base + OFF_STATUS);
   S.terms = (unsigned long long *)(base + OFF_TERMS);
+  S.plist = nullptr;  // no pair lists: the regular-pair kernels cover the pair range
+  S.pcount = nullptr;
+  S.pcap = 0;
   // the previous call's contents stay in the array: the status word and the
   // work counters must start at zero; every other table is fully rewritten
   if (cudaMemsetAsync(base + OFF_STATUS, 0, OFF_TERMS + 6 * sizeof(unsigned long long) - OFF_STATUS, st) != cudaSuccess)
