@@ -434,11 +434,23 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   count_work(terms + 0, nterm, npt);
 }
 
-// Far pairs (flag 3, far_pair): the 8 x 8 Gauss rule on a quad, on each of
-// the 3 parts of a triangle; one thread per (a, b) point, 4 pairs per
-// 256-thread block, contributions accumulated in the thread's shared-memory
-// column; otherwise as k_q0_regular / k_q0_regular_tri.
+// Far pairs (flag 3, far_pair): the 8 x 8 Gauss rule on a quad; on a
+// triangle the 8 x 8 collapsed (Duffy) rule over the whole reference triangle,
+// (z, e) = (1 - 3u/2, sqrt3/2 u (1 - 2v)) for (u, v) in [0, 1]^2, weight
+// u w_u w_v (the weights total 1/2, as the 3-part rule's do).  One thread per
+// point, 4 pairs per 256-thread block, contributions accumulated in the
+// thread's shared-memory column; otherwise as k_q0_regular / k_q0_regular_tri.
 #define FP_THREADS 256
+__device__ __forceinline__ void far_point(bool tri, int i, int j, double &z, double &e) {
+  if (tri) {
+    const double u = 0.5 * (c_q.xf[i] + 1.0), v = 0.5 * (c_q.xf[j] + 1.0);
+    z = 1.0 - 1.5 * u;
+    e = 0.5 * BEM_SQ3 * u * (1.0 - 2.0 * v);
+  } else {
+    z = c_q.xf[i];
+    e = c_q.xf[j];
+  }
+}
 __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
                                                         const uint8_t *__restrict__ flag, double *__restrict__ G,
                                                         double *__restrict__ H, unsigned *status,
@@ -461,13 +473,12 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
     const bool tri = bem_is_tri(D, se);
     const int i = pt >> 3, j = pt & 7;
     unsigned st = 0;
-    for (int part = 0; part < (tri ? 3 : 1); ++part) {
+    {
       double z, e, vR[3], vW[3];
       {
         bem_el el;
         bem_load_el(D.cr, D.cw, se, el);
-        if (tri) bem_tri_point_ref(part, c_q.xf[i], c_q.xf[j], z, e);
-        else { z = c_q.xf[i]; e = c_q.xf[j]; }
+        far_point(tri, i, j, z, e);
         bem_rw(el, z, e, vR, vW);
       }
 #pragma unroll
@@ -479,15 +490,14 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
       ++npt;
       // re-derived after the call rather than kept live across it
       double wt = c_q.wf[i] * c_q.wf[j];
+      far_point(tri, i, j, z, e);
       if (tri) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
-        bem_tri_point_ref(part, c_q.xf[i], c_q.xf[j], z, e);
-        wt *= bem_tri_wfac(c_q.xf[i], c_q.xf[j]);
+        wt *= 0.125 * (c_q.xf[i] + 1.0);  // u w_u w_v with u = (x + 1) / 2, w_u = w / 2
       } else {
         bem_el el;
         bem_load_el(D.cr, D.cw, se, el);
-        z = c_q.xf[i]; e = c_q.xf[j];
         double r[3];
         bem_rw(el, z, e, r, vW);
       }

@@ -151,9 +151,10 @@ def test_far_pairs_match_reference(mesh, fixture, far_rule):
     """Regular pairs against the reference's 12 x 12 rule per quad or triangle
     part (q0_dcoef_bd_node_t2_cc): 216-quad sphere, 320 far pairs (centre
     distance >= 5.5 element circumradii from every lattice image of the node,
-    where the device's default uses an 8 x 8 rule) and 80 nearer ones;
-    320-triangle icosphere, 240 far and 60 nearer.  Entry-wise relative 1e-12
-    (the triangles' fourth entry is zero in both)."""
+    where the device's default uses the 8 x 8 Gauss rule) and 80 nearer ones;
+    320-triangle icosphere, 240 far (8 x 8 collapsed rule over the triangle)
+    and 60 nearer.  Entry-wise relative 1e-12 (the triangles' fourth entry is
+    zero in both)."""
     from bem3_aw_qd2_b200 import api, meshgen
     g = np.load(os.path.join(GOLD, fixture))
     d = tempfile.mkdtemp(prefix="bemfar_")
