@@ -90,12 +90,14 @@ int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
 int bemgpu_set_ewald_scale(bemgpu_ctx *ctx, double scale);
 
 /* Quadrature of far regular pairs of the periodic domain (no counterpart in
- * the reference, which uses its 12 x 12 Gauss rule for every regular pair):
- * on = 1 (the default) uses an 8 x 8 rule where the source element's centre
- * is at least 5 circumradii R from the nearest lattice image of the
- * collocation node and k 2R <= 2, which reproduces the 12 x 12 integrals to
- * below 4e-14 of the entry with 2.25 times fewer Green's-function values;
- * on = 0 keeps the 12 x 12 rule everywhere.  Applies from the next assembly. */
+ * the reference, which uses its 12 x 12 Gauss rule for every regular pair,
+ * on each of 3 parts of a triangle): on = 1 (the default) uses an 8 x 8 rule
+ * (Gauss on a quad, collapsed over a whole triangle) where the source
+ * element's centre is at least 5 circumradii R from the nearest lattice image
+ * of the collocation node and k 2R <= 2, which reproduces the reference's
+ * integrals to below 1e-13 of the entry with 2.25 (quads) or 6.75 (triangles)
+ * times fewer Green's-function values; on = 0 keeps the reference's rules
+ * everywhere.  Applies from the next assembly. */
 int bemgpu_set_far_rule(bemgpu_ctx *ctx, int on);
 
 /* Autotuner of the Ewald parameter for the loaded problem: times the periodic
