@@ -97,9 +97,11 @@ __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], co
 // gives the reference's 12 x 12 integrals to below 4e-14 of the entry
 // (checked against 40 x 40 on curved elements, k 2R up to 2.1).
 struct bem_far { int on; double d1x, d1y, d2x, d2y, idet, k; };
-__device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
-  // squared circumradius about cr0 (the centre of a quad, the centroid of a
-  // triangle): corners (+-1, +-1), or (1, 0), (-1/2, +-sqrt3/2)
+// (distance from the element's centre (a triangle's centroid) to the nearest
+// lattice image of rt) / (the element's circumradius R about that centre),
+// squared; -1 where k 2R > 2.
+__device__ __forceinline__ double pair_ratio2(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
+  // corners (+-1, +-1) of a quad, (1, 0), (-1/2, +-sqrt3/2) of a triangle
   double R2 = 0.0;
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
@@ -116,8 +118,9 @@ __device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, co
     }
     R2 = fmax(R2, v2);
   }
-  if (4.0 * fr.k * fr.k * R2 > 4.0) return false;
-  const double vx = rt[0] - el.cr[0][0], vy = rt[1] - el.cr[1][0], vz = rt[2] - el.cr[2][0];
+  if (4.0 * fr.k * fr.k * R2 > 4.0) return -1.0;
+  const double vz = rt[2] - el.cr[2][0];
+  const double vx = rt[0] - el.cr[0][0], vy = rt[1] - el.cr[1][0];
   const double l1 = floor((vx * fr.d2y - vy * fr.d2x) * fr.idet + 0.5);
   const double l2 = floor(-(vx * fr.d1y - vy * fr.d1x) * fr.idet + 0.5);
   double dmin2 = 1e300;
@@ -126,7 +129,26 @@ __device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, co
       const double x = vx - (l1 + a) * fr.d1x - (l2 + b) * fr.d2x, y = vy - (l1 + a) * fr.d1y - (l2 + b) * fr.d2y;
       dmin2 = fmin(dmin2, x * x + y * y + vz * vz);
     }
-  return dmin2 >= 25.0 * R2;
+  return dmin2 / R2;
+}
+// Quadrature points closer than this to the lattice plane through the node
+// keep a pair on the reference's rule: there the reference's lattice sums
+// stop on rounding-decided zeros, so its values at its own points are not a
+// smooth function that another rule could reproduce.
+#define BEM_FAR_PLANE_TOL 1e-10
+__device__ __forceinline__ void far_point(bool tri, int i, int j, double &z, double &e);
+// far pair: centre at least 5 circumradii from every lattice image of rt, and
+// none of the far rule's points within BEM_FAR_PLANE_TOL of rt's lattice plane
+// (the reference rule's points are checked by the caller)
+__device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
+  if (pair_ratio2(fr, el, rt, tri) < 25.0) return false;
+  for (int ij = 0; ij < BEM_GFN * BEM_GFN; ++ij) {
+    double z, e, r[3], w[3];
+    far_point(tri, ij / BEM_GFN, ij % BEM_GFN, z, e);
+    bem_rw(el, z, e, r, w);
+    if (fabs(r[2] - rt[2]) < BEM_FAR_PLANE_TOL) return false;
+  }
+  return true;
 }
 
 // Compacted pair lists written by k_classify: regular pairs (flag 0) from the
@@ -177,7 +199,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
       bem_el el;
       bem_load_el(D.cr, D.cw, se, el);
       const bool tri = bem_is_tri(D, se);
-      double F = 0, Fz = 0, Fe = 0;
+      double F = 0, Fz = 0, Fe = 0, rzmin = 1e300;
       for (int part = 0; part < (tri ? 3 : 1); ++part)
         for (int i = 0; i < BEM_GLN; ++i) {
           double f = 0, fz = 0, fe = 0;
@@ -190,6 +212,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
             double vR[3], vW[3];
             bem_rw(el, z, e, vR, vW);
             for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+            rzmin = fmin(rzmin, fabs(vR[2]));
             double a, b, c;
             geomF(vR, vW, nd, a, b, c);
             f += c_q.wl[j] * wf * a;
@@ -208,7 +231,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
         if (k < BEM_MAXNEAR) list[k] = s;
       } else {
         sF += F; sFz += Fz; sFe += Fe;
-        if (fr.on && far_pair(fr, el, nd.rt, tri)) fl = 3;
+        if (fr.on && rzmin >= BEM_FAR_PLANE_TOL && far_pair(fr, el, nd.rt, tri)) fl = 3;
       }
     }
     flag[(size_t)p * D.ne + s] = fl;

@@ -151,6 +151,42 @@ def make_far_pairs(name="sphere216", out_name="far216.npz", n_pairs=400, n_near=
     np.savez_compressed(os.path.join(OUT, out_name), idx=idx, far=np.array([p[3] for p in picks]), G=G, H=H)
 
 
+def make_near_pairs(n_pairs=240):
+    """Reference coefficients of node-element pairs of the 216-quad sphere at
+    1 to 3 element circumradii (centre distance from the node's nearest
+    lattice image): the pairs the reference integrates with its 64 x 64 rule
+    (|dF/dt| > 0.5) and the nearest of its 12 x 12 ones."""
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    cfg = meshgen.CONFIGS["sphere216"]
+    files = meshgen.write_inputs(tmp, **cfg)
+    case = refwrap.RefCase(*files)
+    nodes, el = meshgen.cube_sphere(cfg["n"], cfg["semi_axes"])
+    P = nodes[el]
+    cen = P.mean(axis=1)
+    rad = np.max(np.linalg.norm(P - cen[:, None, :], axis=2), axis=1)
+    d1 = np.array(list(cfg["lattice"][0]) + [0.0])
+    d2 = np.array(list(cfg["lattice"][1]) + [0.0])
+    rng = np.random.default_rng(20241206)
+    ne = len(el)
+    picks = []
+    while len(picks) < n_pairs:
+        t, s, tn = int(rng.integers(ne)), int(rng.integers(ne)), int(rng.integers(4))
+        if t == s:
+            continue
+        # the node lies inside element t, near its corner tn
+        node = cen[t] + 0.58 * (P[t, tn] - cen[t])
+        v = node - cen[s]
+        dmin = min(np.linalg.norm(v + a * d1 + b * d2) for a in (-1, 0, 1) for b in (-1, 0, 1))
+        if 1.0 * rad[s] <= dmin < 3.0 * rad[s]:
+            picks.append((t + 1, tn, s + 1))
+    G = np.zeros((len(picks), 4), np.complex128)
+    H = np.zeros((len(picks), 4), np.complex128)
+    for i, (t, tn, s) in enumerate(picks):
+        cc = case.pair(0, t, tn, s)[0]
+        G[i], H[i] = cc[:4], cc[4:8]
+    np.savez_compressed(os.path.join(OUT, "near216.npz"), idx=np.array(picks, np.int32), G=G, H=H)
+
+
 def make_fields(case, out_name="fields24.npz", boundary_points=BOUNDARY_POINTS):
     out = {}
     out["F1"], out["N1"] = case.force(1)
@@ -194,6 +230,10 @@ def main():
         make_far_pairs()
         make_far_pairs("tri320", "far_tri320.npz", 300, 60)
         print("far216.npz, far_tri320.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["near"]:
+        make_near_pairs()
+        print("near216.npz written to", OUT)
         return
     if sys.argv[1:] == ["plane"]:
         make_plane()
