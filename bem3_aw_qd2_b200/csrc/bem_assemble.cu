@@ -1601,13 +1601,10 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   if (periodic) {
     if (lists) {
       // one resident wave (2 blocks per SM) striding over each list
-      static int nsm = 0;
-      if (!nsm) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
-          nsm = 148;
-      }
+      int dev = 0, nsm = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+        return -1;
       const unsigned grid = 2u * (unsigned)nsm;
       const bem_plist Lreg = {S->plist, S->pcount, 1};
       const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
