@@ -42,7 +42,8 @@ struct bemgpu_ctx {
   // per-domain matrices and boundary values
   double *G[BEMGPU_MAXDOM] = {}, *H[BEMGPU_MAXDOM] = {}, *dG[BEMGPU_MAXDOM] = {}, *dH[BEMGPU_MAXDOM] = {}, *dF[BEMGPU_MAXDOM] = {};
   double *P[BEMGPU_MAXDOM] = {}, *dP[BEMGPU_MAXDOM] = {}, *pv[BEMGPU_MAXDOM] = {}, *dpv[BEMGPU_MAXDOM] = {};
-  bem_scratch scr = {};
+  bem_scratch scr = {};   // periodic domain (context stream)
+  bem_scratch scr1 = {};  // domains 1.. (side stream, beside the periodic domain)
   // solve work
   double *A = nullptr, *b = nullptr, *tpv = nullptr, *B3 = nullptr;
   int64_t *ipiv = nullptr;
@@ -160,7 +161,9 @@ static void free_problem(bemgpu_ctx *c, bool release) {
       dfree(c->G[d]); dfree(c->H[d]); dfree(c->dG[d]); dfree(c->dH[d]); dfree(c->dF[d]);
       dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
     }
-    dfree(c->scr.rowF); dfree(c->scr.near_s); dfree(c->scr.near_n); dfree(c->scr.nearF); dfree(c->scr.selfF); dfree(c->scr.flag);
+    for (bem_scratch *S : {&c->scr, &c->scr1}) {
+      dfree(S->rowF); dfree(S->near_s); dfree(S->near_n); dfree(S->nearF); dfree(S->selfF); dfree(S->flag);
+    }
     dfree(c->scr.plist); dfree(c->scr.pcount);
     dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
     for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
@@ -439,14 +442,24 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     CK(falloc(c, &c->dpv[d], 6 * N), "dpv");
     CK(cudaMemsetAsync(c->pv[d], 0, 6 * N * sizeof(double), c->stream), "pv");
   }
-  int maxNe = 0;
-  for (int d = 0; d < nd; ++d) maxNe = c->dom_ne[d] > maxNe ? c->dom_ne[d] : maxNe;
-  CK(falloc(c, &c->scr.rowF, 3 * (size_t)maxN), "rowF");
-  CK(falloc(c, &c->scr.near_s, (size_t)maxN * BEM_MAXNEAR_H), "near_s");
-  CK(falloc(c, &c->scr.near_n, (size_t)maxN), "near_n");
-  CK(falloc(c, &c->scr.nearF, (size_t)maxN * BEM_MAXNEAR_H * 3), "nearF");
-  CK(falloc(c, &c->scr.selfF, 3 * (size_t)maxN), "selfF");
-  CK(falloc(c, &c->scr.flag, (size_t)maxN * maxNe), "flag");
+  // scratch of the periodic domain and, apart, of the free-space domains (they
+  // are assembled on the side stream while the periodic domain is)
+  for (int g = 0; g < 2; ++g) {
+    bem_scratch &S = g == 0 ? c->scr : c->scr1;
+    size_t sN = 0, sNe = 0;
+    for (int d = g; d < (g == 0 ? 1 : nd); ++d) {
+      sN = 4 * (size_t)c->dom_ne[d] > sN ? 4 * (size_t)c->dom_ne[d] : sN;
+      sNe = (size_t)c->dom_ne[d] > sNe ? (size_t)c->dom_ne[d] : sNe;
+    }
+    CK(falloc(c, &S.rowF, 3 * sN), "rowF");
+    CK(falloc(c, &S.near_s, sN * BEM_MAXNEAR_H), "near_s");
+    CK(falloc(c, &S.near_n, sN), "near_n");
+    CK(falloc(c, &S.nearF, sN * BEM_MAXNEAR_H * 3), "nearF");
+    CK(falloc(c, &S.selfF, 3 * sN), "selfF");
+    CK(falloc(c, &S.flag, sN * sNe), "flag");
+    S.status = c->status;
+    S.terms = c->terms;
+  }
   // pair lists of the periodic domain (32-bit entries: up to 2^32 pairs)
   const size_t npair = (size_t)4 * c->dom_ne[0] * c->dom_ne[0];
   if (npair > 0 && npair <= 0xffffffffull) {
@@ -456,8 +469,6 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   } else {
     c->scr.pcap = 0;
   }
-  c->scr.status = c->status;
-  c->scr.terms = c->terms;
   CK(cudaMemsetAsync(c->terms, 0, 6 * sizeof(unsigned long long), c->stream), "counters");
   const size_t n = c->n;
   CK(falloc(c, &c->A, 2 * n * n), "A");
@@ -583,13 +594,22 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
 extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
   c->factored = false;
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  // the free-space domains on the side stream, beside the periodic domain
+  if (c->MN >= 1) {
+    CK(cudaEventRecord(c->ev_fork, c->stream), "assembly fork");
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "assembly fork");
+  }
   for (int d = 0; d <= c->MN; ++d) {
     bem_dom_dev D = dom_view(c, d);
     const int periodic = d == 0;
     cudaEvent_t *ev = c->prof && d < 2 ? c->ev + 6 * d : nullptr;
-    if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], &c->scr, c->G[d], c->H[d], c->dG[d], c->dH[d], c->dF[d],
-                            c->stream, ev) != 0)
+    if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], d == 0 ? &c->scr : &c->scr1, c->G[d], c->H[d],
+                            c->dG[d], c->dH[d], c->dF[d], d == 0 ? c->stream : c->side, ev) != 0)
       return fail(c, "assembly launch", cudaGetLastError());
+  }
+  if (c->MN >= 1) {
+    CK(cudaEventRecord(c->ev_join, c->side), "assembly join");
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0), "assembly join");
   }
   return 0;
 }
