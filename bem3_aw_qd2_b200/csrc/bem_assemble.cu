@@ -90,12 +90,13 @@ __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], co
 
 // ------------------------------------------------------------------ classify
 // One block per collocation node p; threads stride over source elements.
-// Far pairs of the periodic domain (flag 3): a quad source whose centre is at
-// least 5 circumradii R from the nearest lattice image of the collocation
+// Far pairs of the periodic domain (flag 3): a source element whose centre is
+// at least 5 circumradii R from the nearest lattice image of the collocation
 // node, with k 2R <= 2.  There the integrand is analytic well beyond the
-// element (its nearest singularity is that image) and an 8 x 8 Gauss rule
-// gives the reference's 12 x 12 integrals to below 4e-14 of the entry
-// (checked against 40 x 40 on curved elements, k 2R up to 2.1).
+// element (its nearest singularity is that image) and an 8 x 8 rule (Gauss on
+// a quad, collapsed Gauss over a triangle) gives the reference's 12 x 12
+// integrals to below 1e-13 of the entry (checked against 40 x 40 on curved
+// quads and on triangles, k 2R up to 2).
 struct bem_far { int on; double d1x, d1y, d2x, d2y, idet, k; };
 // (distance from the element's centre (a triangle's centroid) to the nearest
 // lattice image of rt) / (the element's circumradius R about that centre),
