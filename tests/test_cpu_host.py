@@ -135,7 +135,38 @@ print(repr(F.tolist()), repr(N.tolist()), repr(p.tolist()), repr(v.tolist()))
 
 
 def test_golden_fixtures_present(golden_dir):
-    for f in ("faddeeva.npz", "qpgf.npz", "sphere24.npz"):
+    for f in ("faddeeva.npz", "qpgf.npz", "sphere24.npz", "far216.npz", "far_tri320.npz", "near216.npz"):
         assert os.path.exists(os.path.join(golden_dir, f))
     g = np.load(os.path.join(golden_dir, "sphere24.npz"))
     assert g["G0"].shape == (96, 96) and g["dG1"].shape == (192, 96)
+
+
+_PAIRS = r"""
+import sys, os, tempfile
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle import refwrap
+from bem3_aw_qd2_b200 import meshgen
+gold = os.path.join(sys.argv[1], "tests", "golden")
+worst = 0.0
+for mesh, fixture in (("sphere216", "far216.npz"), ("tri320", "far_tri320.npz"), ("sphere216", "near216.npz")):
+    g = np.load(os.path.join(gold, fixture))
+    d = tempfile.mkdtemp()
+    case = refwrap.RefCase(*meshgen.write_inputs(d, **meshgen.CONFIGS[mesh]))
+    for k in range(0, len(g["idx"]), max(1, len(g["idx"]) // 8)):
+        t, tn, s = (int(x) for x in g["idx"][k])
+        cc = case.pair(0, t, tn, s)[0]
+        worst = max(worst, float(np.max(np.abs(cc[:4] - g["G"][k]))), float(np.max(np.abs(cc[4:8] - g["H"][k]))))
+print(worst)
+"""
+
+
+def test_pair_fixtures_reproduced_by_oracle():
+    """The single-pair fixtures (far216, far_tri320, near216) are the
+    reference's q0_dcoef_bd_node_t2_cc values: a sample of each recomputed by
+    the reference build here agrees exactly."""
+    from oracle import refwrap
+    if not refwrap.available():
+        pytest.skip("oracle/_ref not built")
+    out = subprocess.check_output([sys.executable, "-c", _PAIRS, ROOT], timeout=600).decode().split()
+    assert float(out[-1]) == 0.0
