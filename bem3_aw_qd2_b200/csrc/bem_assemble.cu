@@ -310,64 +310,64 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
-  const bool valid = u0 + lp < nu;
-  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
-  const int p = (int)(pair / D.ne);
-  const int s = (int)(pair % D.ne);
-  // triangle sources are k_q0_regular_tri's; padded rows keep their zeros
-  const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && !bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
-  double v[16];
+    const bool valid = u0 + lp < nu;
+    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+    const int p = (int)(pair / D.ne);
+    const int s = (int)(pair % D.ne);
+    // triangle sources are k_q0_regular_tri's; padded rows keep their zeros
+    const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && !bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
+    double v[16];
 #pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = 0.0;
-  if (work) {
-    bem_node nd;
-    int t, te;
-    bem_load_node(D, p, nd, t, te);
-    bem_el el;
-    bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
-    const int i = pt / BEM_GLN, j = pt % BEM_GLN;
-    const double z = c_q.xl[i], e = c_q.xl[j];
-    double vR[3], vW[3];
-    bem_rw(el, z, e, vR, vW);
-    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
-    bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
-    if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
-    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-    ++npt;
-    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-    const double wt = c_q.wl[i] * c_q.wl[j];
-    const cplx g = cscale(gv.g, aW * wt);
-    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-    double N[4];
-    bem_Nn4(z, e, N);
+    for (int c = 0; c < 16; ++c) v[c] = 0.0;
+    if (work) {
+      bem_node nd;
+      int t, te;
+      bem_load_node(D, p, nd, t, te);
+      bem_el el;
+      bem_load_el(D.cr, D.cw, abs(D.sid[s]) - 1, el);
+      const int i = pt / BEM_GLN, j = pt % BEM_GLN;
+      const double z = c_q.xl[i], e = c_q.xl[j];
+      double vR[3], vW[3];
+      bem_rw(el, z, e, vR, vW);
+      for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+      if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+      const double wt = c_q.wl[i] * c_q.wl[j];
+      const cplx g = cscale(gv.g, aW * wt);
+      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+      double N[4];
+      bem_Nn4(z, e, N);
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      v[2 * a] = g.re * N[a];
-      v[2 * a + 1] = g.im * N[a];
-      v[8 + 2 * a] = h.re * N[a];
-      v[8 + 2 * a + 1] = h.im * N[a];
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    if (u0 + q2 < nu) {
-      const long long pr = plist_pair(L, pair0, u0 + q2);
-      const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
-      if (flag[(size_t)pp * D.ne + ss] == 0 && !bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
-        double sum = 0.0;
-        for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
-        const size_t N = (size_t)D.ne * 4;
-        double *dst = c < 8 ? G : H;
-        const int a = (c & 7) >> 1, part = c & 1;
-        dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+      for (int a = 0; a < 4; ++a) {
+        v[2 * a] = g.re * N[a];
+        v[2 * a + 1] = g.im * N[a];
+        v[8 + 2 * a] = h.re * N[a];
+        v[8 + 2 * a + 1] = h.im * N[a];
       }
     }
-  }
-  __syncthreads();  // acc is rewritten by the next unit group
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = v[c];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
+      if (u0 + q2 < nu) {
+        const long long pr = plist_pair(L, pair0, u0 + q2);
+        const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
+        if (flag[(size_t)pp * D.ne + ss] == 0 && !bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
+          double sum = 0.0;
+          for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
+          const size_t N = (size_t)D.ne * 4;
+          double *dst = c < 8 ? G : H;
+          const int a = (c & 7) >> 1, part = c & 1;
+          dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+        }
+      }
+    }
+    __syncthreads();  // acc is rewritten by the next unit group
   }
   count_work(terms + 0, nterm, npt);
 }
@@ -385,75 +385,75 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
-  const bool valid = u0 + lp < nu;
-  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
-  const int p = (int)(pair / D.ne);
-  const int s = (int)(pair % D.ne);
-  const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
-  // the 3 parts accumulate in this thread's shared-memory column, so that no
-  // accumulator stays live in registers across the Green's-function calls
+    const bool valid = u0 + lp < nu;
+    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+    const int p = (int)(pair / D.ne);
+    const int s = (int)(pair % D.ne);
+    const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
+    // the 3 parts accumulate in this thread's shared-memory column, so that no
+    // accumulator stays live in registers across the Green's-function calls
 #pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
-  if (work) {
-    const int i = pt / BEM_GLN, j = pt % BEM_GLN;
-    const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
-    unsigned st = 0;
-    for (int part = 0; part < 3; ++part) {
-      // geometry is re-read (L1) per part rather than kept in registers
-      // across the Green's-function calls
-      double z, e, vR[3], vW[3];
-      {
-        const double a = c_q.xl[i], b = c_q.xl[j];
-        bem_el el;
-        bem_load_el(D.cr, D.cw, se, el);
-        bem_tri_point_ref(part, a, b, z, e);
-        bem_rw_ref(el, z, e, vR, vW);
+    for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
+    if (work) {
+      const int i = pt / BEM_GLN, j = pt % BEM_GLN;
+      const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
+      unsigned st = 0;
+      for (int part = 0; part < 3; ++part) {
+        // geometry is re-read (L1) per part rather than kept in registers
+        // across the Green's-function calls
+        double z, e, vR[3], vW[3];
+        {
+          const double a = c_q.xl[i], b = c_q.xl[j];
+          bem_el el;
+          bem_load_el(D.cr, D.cw, se, el);
+          bem_tri_point_ref(part, a, b, z, e);
+          bem_rw_ref(el, z, e, vR, vW);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d));
+        bem_gval gv;
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+        if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+        nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+        ++npt;
+        // a triangle's W is the constant cw[.][0]
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
+        const double a2 = c_q.xl[i], b2 = c_q.xl[j];
+        bem_tri_point_ref(part, a2, b2, z, e);  // recomputed: not kept across the call
+        const double wt = c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(a2, b2);
+        const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+        const cplx g = cscale(gv.g, aW * wt);
+        const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+        double N[4];
+        bem_Nn3(z, e, N);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          acc[2 * n][threadIdx.x] += g.re * N[n];
+          acc[2 * n + 1][threadIdx.x] += g.im * N[n];
+          acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
+          acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
+        }
       }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d));
-      bem_gval gv;
-      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
-      if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
-      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-      ++npt;
-      // a triangle's W is the constant cw[.][0]
-#pragma unroll
-      for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
-      const double a2 = c_q.xl[i], b2 = c_q.xl[j];
-      bem_tri_point_ref(part, a2, b2, z, e);  // recomputed: not kept across the call
-      const double wt = c_q.wl[i] * c_q.wl[j] * bem_tri_wfac(a2, b2);
-      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-      const cplx g = cscale(gv.g, aW * wt);
-      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-      double N[4];
-      bem_Nn3(z, e, N);
-#pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        acc[2 * n][threadIdx.x] += g.re * N[n];
-        acc[2 * n + 1][threadIdx.x] += g.im * N[n];
-        acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
-        acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
+      set_status(status, st);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
+      if (u0 + q2 < nu) {
+        const long long pr = plist_pair(L, pair0, u0 + q2);
+        const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
+        if (flag[(size_t)pp * D.ne + ss] == 0 && bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
+          double sum = 0.0;
+          for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
+          const size_t N = (size_t)D.ne * 4;
+          double *dst = c < 8 ? G : H;
+          const int a = (c & 7) >> 1, part = c & 1;
+          dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+        }
       }
     }
-    set_status(status, st);
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    if (u0 + q2 < nu) {
-      const long long pr = plist_pair(L, pair0, u0 + q2);
-      const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
-      if (flag[(size_t)pp * D.ne + ss] == 0 && bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
-        double sum = 0.0;
-        for (int k = 0; k < 144; ++k) sum += acc[c][q2 * 144 + k];
-        const size_t N = (size_t)D.ne * 4;
-        double *dst = c < 8 ? G : H;
-        const int a = (c & 7) >> 1, part = c & 1;
-        dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
-      }
-    }
-  }
-  __syncthreads();  // acc is rewritten by the next unit group
+    __syncthreads();  // acc is rewritten by the next unit group
   }
   count_work(terms + 0, nterm, npt);
 }
@@ -485,79 +485,79 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
   for (long long u0 = 4LL * blockIdx.x; u0 < nu; u0 += 4LL * gridDim.x) {
-  const bool valid = u0 + lp < nu;
-  const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
-  const int p = (int)(pair / D.ne);
-  const int s = (int)(pair % D.ne);
-  const bool work = valid && flag[(size_t)p * D.ne + s] == 3;
+    const bool valid = u0 + lp < nu;
+    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+    const int p = (int)(pair / D.ne);
+    const int s = (int)(pair % D.ne);
+    const bool work = valid && flag[(size_t)p * D.ne + s] == 3;
 #pragma unroll
-  for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
-  if (work) {
-    const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
-    const bool tri = bem_is_tri(D, se);
-    const int i = pt >> 3, j = pt & 7;
-    unsigned st = 0;
-    {
-      double z, e, vR[3], vW[3];
+    for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
+    if (work) {
+      const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
+      const bool tri = bem_is_tri(D, se);
+      const int i = pt >> 3, j = pt & 7;
+      unsigned st = 0;
       {
-        bem_el el;
-        bem_load_el(D.cr, D.cw, se, el);
+        double z, e, vR[3], vW[3];
+        {
+          bem_el el;
+          bem_load_el(D.cr, D.cw, se, el);
+          far_point(tri, i, j, z, e);
+          bem_rw(el, z, e, vR, vW);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vR[d] -= __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d);
+        bem_gval gv;
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+        if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+        nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+        ++npt;
+        // re-derived after the call rather than kept live across it
+        double wt = c_q.wf[i] * c_q.wf[j];
         far_point(tri, i, j, z, e);
-        bem_rw(el, z, e, vR, vW);
+        if (tri) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
+          wt *= 0.125 * (c_q.xf[i] + 1.0);  // u w_u w_v with u = (x + 1) / 2, w_u = w / 2
+        } else {
+          bem_el el;
+          bem_load_el(D.cr, D.cw, se, el);
+          double r[3];
+          bem_rw(el, z, e, r, vW);
+        }
+        const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+        const cplx g = cscale(gv.g, aW * wt);
+        const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+        double N[4];
+        if (tri) bem_Nn3(z, e, N);
+        else bem_Nn4(z, e, N);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          acc[2 * n][threadIdx.x] += g.re * N[n];
+          acc[2 * n + 1][threadIdx.x] += g.im * N[n];
+          acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
+          acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
+        }
       }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) vR[d] -= __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d);
-      bem_gval gv;
-      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
-      if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
-      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-      ++npt;
-      // re-derived after the call rather than kept live across it
-      double wt = c_q.wf[i] * c_q.wf[j];
-      far_point(tri, i, j, z, e);
-      if (tri) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
-        wt *= 0.125 * (c_q.xf[i] + 1.0);  // u w_u w_v with u = (x + 1) / 2, w_u = w / 2
-      } else {
-        bem_el el;
-        bem_load_el(D.cr, D.cw, se, el);
-        double r[3];
-        bem_rw(el, z, e, r, vW);
-      }
-      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-      const cplx g = cscale(gv.g, aW * wt);
-      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-      double N[4];
-      if (tri) bem_Nn3(z, e, N);
-      else bem_Nn4(z, e, N);
-#pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        acc[2 * n][threadIdx.x] += g.re * N[n];
-        acc[2 * n + 1][threadIdx.x] += g.im * N[n];
-        acc[8 + 2 * n][threadIdx.x] += h.re * N[n];
-        acc[8 + 2 * n + 1][threadIdx.x] += h.im * N[n];
+      set_status(status, st);
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      const int q4 = threadIdx.x >> 4, c = threadIdx.x & 15;
+      if (u0 + q4 < nu) {
+        const long long pr = plist_pair(L, pair0, u0 + q4);
+        const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
+        if (flag[(size_t)pp * D.ne + ss] == 3) {
+          double sum = 0.0;
+          for (int k = 0; k < 64; ++k) sum += acc[c][q4 * 64 + k];
+          const size_t N = (size_t)D.ne * 4;
+          double *dst = c < 8 ? G : H;
+          const int a = (c & 7) >> 1, part = c & 1;
+          dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
+        }
       }
     }
-    set_status(status, st);
-  }
-  __syncthreads();
-  if (threadIdx.x < 64) {
-    const int q4 = threadIdx.x >> 4, c = threadIdx.x & 15;
-    if (u0 + q4 < nu) {
-      const long long pr = plist_pair(L, pair0, u0 + q4);
-      const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
-      if (flag[(size_t)pp * D.ne + ss] == 3) {
-        double sum = 0.0;
-        for (int k = 0; k < 64; ++k) sum += acc[c][q4 * 64 + k];
-        const size_t N = (size_t)D.ne * 4;
-        double *dst = c < 8 ? G : H;
-        const int a = (c & 7) >> 1, part = c & 1;
-        dst[2 * ((size_t)pp * N + 4 * ss + a) + part] = sum;
-      }
-    }
-  }
-  __syncthreads();  // acc is rewritten by the next unit group
+    __syncthreads();  // acc is rewritten by the next unit group
   }
   count_work(terms + 0, nterm, npt);
 }
