@@ -1,7 +1,6 @@
 // C ABI (include/bemgpu.h): device buffers, problem upload, the assembly /
-// solve sequence and the cuSOLVER factorisations.
+// solve sequence and the dense factorisations (bem_lu.cu, bem_mixed.cu).
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -14,6 +13,7 @@
 #include "bem_solve.h"
 #include "bem_lattice.h"
 #include "bem_mixed.h"
+#include "bem_lu.h"
 
 #define BEMGPU_MAXDOM 8
 
@@ -21,8 +21,6 @@ struct bemgpu_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  cusolverDnHandle_t solver = nullptr;
-  cusolverDnParams_t params = nullptr;
   char err[512] = {0};
   // problem
   bool loaded = false;
@@ -46,11 +44,6 @@ struct bemgpu_ctx {
   bem_scratch scr1 = {};  // domains 1.. (side stream, beside the periodic domain)
   // solve work
   double *A = nullptr, *b = nullptr, *tpv = nullptr, *B3 = nullptr;
-  int64_t *ipiv = nullptr;
-  int *info = nullptr;
-  void *dwork = nullptr;
-  size_t dwork_sz = 0;
-  std::vector<char> hwork;
   double *fout = nullptr, *rc_d = nullptr;
   double *wtab = nullptr;  // real-space term table of the Ewald sums (A, B at eta_run)
   double *stab = nullptr;  // evanescent spectral order table (at eta_run)
@@ -81,24 +74,21 @@ struct bemgpu_ctx {
   int precision = 0;
   bem_mixed mxs[BEMGPU_MAXDOM + 1];  // FP32 factors per dense system (0 global, 1 + d dpv of domain d)
   bool mx_ready[BEMGPU_MAXDOM + 1] = {};
-  // FP64 factors: the global system in A (ipiv), domain d's dpv system in Wd[d] (ipd[d])
+  // FP64 factors: the global system in A, domain d's dpv system in Wd[d]; the
+  // row pivoting and the scratch of each in lus[slot] (0 global, 1 + d dpv)
   double *Wd[BEMGPU_MAXDOM] = {};
+  bem_lu lus[BEMGPU_MAXDOM + 1];
+  bool lu_ready[BEMGPU_MAXDOM + 1] = {};
   // domains with triangles: the dpv system without padding (compact -> full index, size, matrix)
   int *cinv[BEMGPU_MAXDOM] = {};
   int cn[BEMGPU_MAXDOM] = {};
   double *Gc[BEMGPU_MAXDOM] = {};
   double *B3c = nullptr;
-  int64_t *ipd[BEMGPU_MAXDOM] = {};
   bool fac_fp64[BEMGPU_MAXDOM + 1] = {};
   bool factored = false;  // factors of the current matrices are held (bemgpu_solve_rhs may run)
   double *b0 = nullptr, *B3s = nullptr;  // saved right-hand sides (FP64 fallback)
   // side lane: the dpv factorisations run there, overlapping the global system
   cudaStream_t side = nullptr;
-  cusolverDnHandle_t solver2 = nullptr;
-  void *dwork2 = nullptr;
-  size_t dwork2_sz = 0;
-  std::vector<char> hwork2;
-  int *info2 = nullptr;  // [BEMGPU_MAXDOM] getrf info of the dpv systems
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
   double st_corr[BEMGPU_MAXDOM + 1] = {};
@@ -112,14 +102,6 @@ static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
   do {                                           \
     cudaError_t _e = (call);                     \
     if (_e != cudaSuccess) return fail(c, what, _e); \
-  } while (0)
-#define CKS(call, what)                                                         \
-  do {                                                                          \
-    cusolverStatus_t _s = (call);                                               \
-    if (_s != CUSOLVER_STATUS_SUCCESS) {                                        \
-      snprintf(c->err, sizeof(c->err), "%s: cusolver status %d", what, (int)_s); \
-      return -1;                                                                \
-    }                                                                           \
   } while (0)
 
 template <class T>
@@ -165,18 +147,12 @@ static void free_problem(bemgpu_ctx *c, bool release) {
       dfree(S->rowF); dfree(S->near_s); dfree(S->near_n); dfree(S->nearF); dfree(S->selfF); dfree(S->flag);
     }
     dfree(c->scr.plist); dfree(c->scr.pcount);
-    dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->ipiv); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
-    for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->ipd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
+    dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
+    for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
     dfree(c->B3c);
     dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
     dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
     c->cap.clear();
-    if (c->dwork) cudaFree(c->dwork);
-    c->dwork = nullptr;
-    c->dwork_sz = 0;
-    if (c->dwork2) cudaFree(c->dwork2);
-    c->dwork2 = nullptr;
-    c->dwork2_sz = 0;
   }
   for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->cn[d] = 0;
   c->factored = false;
@@ -197,20 +173,21 @@ extern "C" int bemgpu_create(int device, void *stream, bemgpu_ctx **out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return -1; }
     c->own_stream = true;
   }
-  if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS || cusolverDnSetStream(c->solver, c->stream) != CUSOLVER_STATUS_SUCCESS ||
-      cusolverDnCreateParams(&c->params) != CUSOLVER_STATUS_SUCCESS) {
-    delete c;
-    return -1;
-  }
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
-      cusolverDnCreate(&c->solver2) != CUSOLVER_STATUS_SUCCESS ||
-      cusolverDnSetStream(c->solver2, c->side) != CUSOLVER_STATUS_SUCCESS ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess || dalloc(&c->info2, BEMGPU_MAXDOM) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
     return -1;
   }
-  if (dalloc(&c->info, 1) != cudaSuccess || dalloc(&c->status, 1) != cudaSuccess || dalloc(&c->fout, 8) != cudaSuccess ||
+  for (int i = 0; i <= BEMGPU_MAXDOM; ++i) {
+    if (bem_lu_init(&c->lus[i], device) != 0) {
+      for (int j = 0; j < i; ++j) bem_lu_free(&c->lus[j]);
+      delete c;
+      return -1;
+    }
+    c->lu_ready[i] = true;
+  }
+  if (dalloc(&c->status, 1) != cudaSuccess || dalloc(&c->fout, 8) != cudaSuccess ||
       dalloc(&c->rc_d, 4) != cudaSuccess || dalloc(&c->terms, 6) != cudaSuccess) {
     delete c;
     return -1;
@@ -228,19 +205,17 @@ extern "C" void bemgpu_destroy(bemgpu_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_problem(c, true);
-  dfree(c->info); dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
+  dfree(c->status); dfree(c->fout); dfree(c->rc_d); dfree(c->terms);
   dfree(c->pt_in); dfree(c->pt_out); dfree(c->pt_t);
   for (int i = 0; i <= BEMGPU_MAXDOM; ++i)
     if (c->mx_ready[i]) { bem_mixed_free(&c->mxs[i]); c->mx_ready[i] = false; }
+  for (int i = 0; i <= BEMGPU_MAXDOM; ++i)
+    if (c->lu_ready[i]) { bem_lu_free(&c->lus[i]); c->lu_ready[i] = false; }
   for (int i = 0; i < 17; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
-  if (c->params) cusolverDnDestroyParams(c->params);
-  if (c->solver) cusolverDnDestroy(c->solver);
-  if (c->solver2) cusolverDnDestroy(c->solver2);
   if (c->side) { cudaStreamSynchronize(c->side); cudaStreamDestroy(c->side); }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
-  dfree(c->info2);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -477,7 +452,6 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   for (int d = 0; d < nd; ++d) {
     const size_t N = 4 * (size_t)c->dom_ne[d];
     CK(falloc(c, &c->Wd[d], 2 * N * N), "dpv factors");
-    CK(falloc(c, &c->ipd[d], N), "dpv pivots");
     c->cn[d] = (int)N;
     if (c->dom_tri[d]) {
       std::vector<int> inv;
@@ -492,7 +466,6 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     }
   }
   CK(falloc(c, &c->B3, 6 * (size_t)maxN), "B3");
-  CK(falloc(c, &c->ipiv, n > (size_t)maxN ? n : (size_t)maxN), "ipiv");
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "status");
   // device view of the system
   bem_sys_dev &S = c->sys;
@@ -614,52 +587,40 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
   return 0;
 }
 
-// LU factorisation of the row-major n x n complex matrix M in place; cuSOLVER
-// sees the column-major transpose, so solves below use op = T.
-static int check_info(bemgpu_ctx *c, const char *what) {
-  int info = 0;
-  CK(cudaMemcpyAsync(&info, c->info, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
-  CK(cudaStreamSynchronize(c->stream), what);
-  if (info != 0) {
-    snprintf(c->err, sizeof(c->err), "%s: factorisation info %d", what, info);
+// Dense systems M X = B with M row-major FP64 (n x n), B column-major (n x nrhs).
+// slot 0 is the global system (factors in place of A), slot 1 + d the dpv
+// system of domain d (M = G[d], FP64 factors in Wd[d]).  FP64: the device LU
+// of bem_lu.cu (P M = L U, row pivoting).  Mixed precision: FP32 factors +
+// FP64 refinement against M, which stays intact; a system with a zero FP32
+// pivot, or whose refinement does not reach 1e-12, switches to FP64 factors
+// (then kept for later right-hand sides).
+// lane 0: the context's stream (checked at once); lane 1: the side stream
+// (dpv systems, checked after the join in bemgpu_solve)
+static int lu_status_check(bemgpu_ctx *c, int slot, const char *what) {
+  const unsigned st = bem_lu_status(&c->lus[slot], c->stream);
+  if (st == 0xffffffffu) return fail(c, what, cudaGetLastError());
+  if (st & BEM_LU_ST_ZERO) {
+    snprintf(c->err, sizeof(c->err), "%s: zero pivot (singular matrix)", what);
     return -3;
+  }
+  if (st & (BEM_LU_ST_WAIT | BEM_LU_ST_INTERNAL)) {
+    snprintf(c->err, sizeof(c->err), "%s: %s", what,
+             (st & BEM_LU_ST_WAIT) ? "a triangular-solve wait gave up" : "a row move out of range");
+    return -1;
   }
   return 0;
 }
 
-// Dense systems M X = B with M row-major FP64 (n x n), B column-major (n x nrhs).
-// slot 0 is the global system (factors in place of A), slot 1 + d the dpv
-// system of domain d (M = G[d], FP64 factors in Wd[d]).  Mixed precision: FP32
-// factors + FP64 refinement against M, which stays intact; a system with a
-// zero FP32 pivot, or whose refinement does not reach 1e-12, switches to FP64
-// factors (then kept for later right-hand sides).
-// lane 0: the context's stream (checked at once); lane 1: the side stream
-// (dpv systems, checked after the join in bemgpu_solve)
 static int dense_factor_fp64(bemgpu_ctx *c, int slot, double *M, int64_t n, const char *what, int lane = 0) {
   double *F = slot == 0 ? M : c->Wd[slot - 1];
-  int64_t *ip = slot == 0 ? c->ipiv : c->ipd[slot - 1];
   cudaStream_t st = lane ? c->side : c->stream;
-  cusolverDnHandle_t sv = lane ? c->solver2 : c->solver;
-  void **dw = lane ? &c->dwork2 : &c->dwork;
-  size_t *dws = lane ? &c->dwork2_sz : &c->dwork_sz;
-  std::vector<char> &hw = lane ? c->hwork2 : c->hwork;
-  int *info = lane ? c->info2 + (slot - 1) : c->info;
   if (F != M) CK(cudaMemcpyAsync(F, M, 2 * n * n * sizeof(double), cudaMemcpyDeviceToDevice, st), what);
-  size_t dsz = 0, hsz = 0;
-  CKS(cusolverDnXgetrf_bufferSize(sv, c->params, n, n, CUDA_C_64F, F, n, CUDA_C_64F, &dsz, &hsz), what);
-  if (dsz > *dws) {
-    // the lane's stream may still use the old workspace
-    CK(cudaStreamSynchronize(st), what);
-    if (*dw) cudaFree(*dw);
-    CK(cudaMalloc(dw, dsz), what);
-    *dws = dsz;
+  if (bem_lu_factor_z(&c->lus[slot], F, (int)n, st)) {
+    snprintf(c->err, sizeof(c->err), "%s: %s", what, c->lus[slot].err);
+    return -1;
   }
-  if (hsz > hw.size()) hw.resize(hsz);
-  CKS(cusolverDnXgetrf(sv, c->params, n, n, CUDA_C_64F, F, n, ip, CUDA_C_64F, *dw, *dws, hsz ? hw.data() : nullptr, hsz,
-                       info),
-      what);
   c->fac_fp64[slot] = true;
-  if (lane == 0 && check_info(c, what)) return -3;
+  if (lane == 0) return lu_status_check(c, slot, what);
   return 0;
 }
 
@@ -685,15 +646,15 @@ static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const cha
 
 // After the side lane joined: the dpv factorisations' outcome (zero pivots).
 static int check_side_factors(bemgpu_ctx *c) {
-  int info[BEMGPU_MAXDOM] = {};
-  CK(cudaMemcpyAsync(info, c->info2, sizeof(int) * (c->MN + 1), cudaMemcpyDeviceToHost, c->stream), "dpv LU");
-  CK(cudaStreamSynchronize(c->stream), "dpv LU");
   for (int d = 0; d <= c->MN; ++d) {
     const int slot = 1 + d;
     if (c->fac_fp64[slot]) {
-      if (info[d] != 0) {
-        snprintf(c->err, sizeof(c->err), "dpv LU of domain %d: factorisation info %d", d, info[d]);
-        return -3;
+      const int r = lu_status_check(c, slot, "dpv LU");
+      if (r) {
+        char tmp[512];
+        snprintf(tmp, sizeof(tmp), "domain %d: %s", d, c->err);
+        snprintf(c->err, sizeof(c->err), "%s", tmp);
+        return r;
       }
     } else if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
       c->st_fallback[slot] = 1;
@@ -727,8 +688,10 @@ static int dense_apply(bemgpu_ctx *c, int slot, double *M, int64_t n, int64_t nr
     if (r) return r;
   }
   double *F = slot == 0 ? M : c->Wd[slot - 1];
-  int64_t *ip = slot == 0 ? c->ipiv : c->ipd[slot - 1];
-  CKS(cusolverDnXgetrs(c->solver, c->params, CUBLAS_OP_T, n, nrhs, CUDA_C_64F, F, n, ip, CUDA_C_64F, B, n, c->info), what);
+  if (bem_lu_solve_z(&c->lus[slot], F, (int)n, (int)nrhs, B, c->stream)) {
+    snprintf(c->err, sizeof(c->err), "%s: %s", what, c->lus[slot].err);
+    return -1;
+  }
   return 0;
 }
 
@@ -789,6 +752,16 @@ static int solve_tail(bemgpu_ctx *c) {
   return 0;
 }
 
+// The triangular solves' waits of every FP64 system (one synchronisation).
+static int check_solve_waits(bemgpu_ctx *c) {
+  for (int slot = 0; slot <= c->MN + 1; ++slot)
+    if (c->fac_fp64[slot]) {
+      const int r = lu_status_check(c, slot, slot ? "dpv solve" : "global solve");
+      if (r) return r;
+    }
+  return 0;
+}
+
 static int ensure_saves(bemgpu_ctx *c) {
   if (c->precision != 0) {
     CK(falloc(c, &c->b0, 2 * (size_t)c->n), "b copy");
@@ -818,7 +791,6 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   // global system is gathered, factored and solved here
   CK(cudaEventRecord(c->ev_fork, c->stream), "fork");
   CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "fork");
-  CK(cudaMemsetAsync(c->info2, 0, sizeof(int) * BEMGPU_MAXDOM, c->side), "fork");
   auto side_lane = [c]() -> int {
     for (int d = 0; d <= c->MN; ++d) {
       const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
@@ -870,6 +842,7 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
   if (!rc && je != cudaSuccess) rc = fail(c, "join", je);
   if (!rc) rc = check_side_factors(c);
   if (!rc) rc = solve_tail(c);
+  if (!rc) rc = check_solve_waits(c);
   if (rc) return rc;
   c->factored = true;
   return 0;
@@ -888,6 +861,7 @@ extern "C" int bemgpu_solve_rhs(bemgpu_ctx *c) {
   if (c->prof) cudaEventRecord(c->ev[13], c->stream);
   int rc = dense_apply(c, 0, c->A, (int64_t)c->n, 1, c->b, c->b0, "global solve");
   if (!rc) rc = solve_tail(c);
+  if (!rc) rc = check_solve_waits(c);
   return rc;
 }
 
@@ -1202,5 +1176,30 @@ extern "C" int bemgpu_qpgf(const double *qpar, const double *r, int n, double *G
     }
   }
   cudaFree(dr); cudaFree(dg); cudaFree(ddg); cudaFree(dret); cudaFree(wt); cudaFree(stb);
+  return rc;
+}
+
+extern "C" int bemgpu_zgesv(int device, int n, int nrhs, const double *A, double *B) {
+  if (n <= 0 || nrhs < 1 || nrhs > 4) return -2;
+  if (cudaSetDevice(device) != cudaSuccess) return -1;
+  bem_lu w;
+  if (bem_lu_init(&w, device)) return -1;
+  cudaStream_t st = nullptr;
+  double *dA = nullptr, *dB = nullptr;
+  int rc = -1;
+  const size_t an = 2 * (size_t)n * n * sizeof(double), bn = 2 * (size_t)n * nrhs * sizeof(double);
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess && cudaMalloc(&dA, an) == cudaSuccess &&
+      cudaMalloc(&dB, bn) == cudaSuccess && cudaMemcpyAsync(dA, A, an, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+      cudaMemcpyAsync(dB, B, bn, cudaMemcpyHostToDevice, st) == cudaSuccess && bem_lu_factor_z(&w, dA, n, st) == 0 &&
+      bem_lu_solve_z(&w, dA, n, nrhs, dB, st) == 0 &&
+      cudaMemcpyAsync(B, dB, bn, cudaMemcpyDeviceToHost, st) == cudaSuccess) {
+    const unsigned s = bem_lu_status(&w, st);
+    rc = s == 0 ? 0 : (s & BEM_LU_ST_ZERO) ? -3 : -1;
+  }
+  if (st) cudaStreamSynchronize(st);
+  cudaFree(dA);
+  cudaFree(dB);
+  bem_lu_free(&w);
+  if (st) cudaStreamDestroy(st);
   return rc;
 }

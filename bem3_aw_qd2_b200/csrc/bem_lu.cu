@@ -1,0 +1,767 @@
+// Dense complex FP64 LU factorisation with row pivoting, and the triangular
+// solves, written for B200 with no library: the device replacement of the
+// reference's dense solves (PARDISO mtype 13 on the global system,
+// b_mkl_solver_pardiso_d, d3qd2_mkl_solver.c:18-148, called at
+// bem3_aw_qd2_solve_bieq.c:347-368; LAPACKE_zgesv on each domain's dpv system,
+// solve_dpv_bv, bem3_aw_qd2_solve_bieq.c:533-653).
+//
+// The matrix is row-major (the layout the assembly writes), factored in place
+// as P A = L U, right-looking, 32 columns per panel.  Per panel three kernels:
+//
+//  k_lu_panel   one thread-block cluster of 8 CTAs picks the panel's 32 pivot
+//               rows by tournament pivoting (communication-avoiding LU): each
+//               CTA runs partial pivoting on its slice of rows, one row per
+//               thread in registers, and passes its winners on; CTA 0 runs
+//               partial pivoting on the winners, which gives the pivot order
+//               and the packed L11\U11, inverts U11 and L11, and lists the row
+//               moves (at most 64 touched positions).  The matrix is not
+//               written here.
+//  k_lu_apply   all SMs: L21 = A21 U11^-1 for every row below the panel,
+//               the row moves on the columns outside the panel, and
+//               U12 = L11^-1 A12 on the pivot rows.
+//  k_lu_update  all SMs: A22 -= L21 U12 on the FP64 tensor cores
+//               (mma.sync m8n8k4 f64; Blackwell's tcgen05 has no FP64 kind),
+//               64 x 64 complex tiles, the complex product as four real ones.
+//
+// The sequence of a size and matrix is captured once as a CUDA graph and
+// replayed.  Solves: forward substitution L y = P b and back substitution
+// U x = y in one launch each, one CTA per 32-row block; a block waits for the
+// blocks it needs through flags in global memory (bounded waits: a wait that
+// gives up sets BEM_LU_ST_WAIT and the call reports it; nothing hangs).  The
+// launches are cooperative, so every CTA is resident and blocks are taken in
+// order: the waits cannot deadlock.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include "bem_lu.h"
+
+#define LU_W BEM_LU_W
+#define LU_TH 256        // threads of a panel CTA: one row each
+#define LU_CL 8          // CTAs of the panel cluster
+#define LU_MAXP (2 * LU_W)
+#define FULL 0xffffffffu
+
+// integer scratch (bem_lu.piv)
+#define PV_CAND 0                    // [LU_CL][LU_W] candidate rows of each leaf
+#define PV_CCNT (LU_CL * LU_W)       // [LU_CL] candidates per leaf
+#define PV_SEL (PV_CCNT + LU_CL)     // [LU_W] pivot rows in order
+#define PV_PERM (PV_SEL + LU_W)      // count, then (dst, src) pairs of the row moves
+#define PV_INTS (PV_PERM + 1 + 2 * LU_MAXP)
+// complex scratch (bem_lu.u11)
+#define U_LU 0                       // [LU_W][LU_W] packed L11\U11, row i = pivot row i
+#define U_UINV (LU_W * LU_W)         // U11^-1 (upper)
+#define U_LINV (2 * LU_W * LU_W)     // L11^-1 (unit lower)
+#define U_STAGE (3 * LU_W * LU_W)    // panel values of the rows moved out of the pivot block
+#define U_COUNT (4 * LU_W * LU_W)
+
+// ---------------------------------------------------------------- complex helpers
+__device__ __forceinline__ double2 cz() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// c + a b
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+// c - a b
+__device__ __forceinline__ double2 cfms(double2 a, double2 b, double2 c) {
+  return make_double2(fma(-a.x, b.x, fma(a.y, b.y, c.x)), fma(-a.x, b.y, fma(-a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 crcp(double2 a) {
+  const double d = 1.0 / fma(a.x, a.x, a.y * a.y);
+  return make_double2(a.x * d, -a.y * d);
+}
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+
+// ---------------------------------------------------------------- partial pivoting in one CTA
+struct gepp_sh {
+  double wv[2][LU_TH / 32];
+  int wi[2][LU_TH / 32];
+  double2 prow[2][LU_W], krow[2][LU_W];
+  int pid[2], kid[2];
+};
+
+__device__ __forceinline__ void rot1(double2 (&v)[LU_W]) {
+  const double2 f = v[0];
+#pragma unroll
+  for (int c = 0; c < LU_W - 1; ++c) v[c] = v[c + 1];
+  v[LU_W - 1] = f;
+}
+
+// Partial pivoting (|re| + |im| as LAPACK's izamax, lowest row on ties) over
+// the rr <= LU_TH rows held one per thread (thread t < rr: values v, matrix
+// row id), w columns.  Afterwards thread i < min(w, rr) holds the i-th pivot
+// row and its id, its values packed (multipliers left of column i, U from i
+// on), columns in order.  A row is kept rotated while it is eliminated: at
+// step j its register 0 holds column j, registers 1 .. 31 - j the columns
+// still to update and the rest the finished ones, so that every register
+// index is a compile-time constant inside one short loop body.
+__device__ void gepp(double2 (&v)[LU_W], int &id, int rr, int w, gepp_sh &sh, unsigned *status) {
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int steps = min(w, rr);
+  for (int j = 0; j < steps; ++j) {
+    const int b = j & 1;
+    double val = (t >= j && t < rr) ? cabs1(v[0]) : -1.0;
+    int bi = t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_down_sync(FULL, val, o);
+      const int oi = __shfl_down_sync(FULL, bi, o);
+      if (ov > val || (ov == val && oi < bi)) { val = ov; bi = oi; }
+    }
+    if (lane == 0) { sh.wv[b][wid] = val; sh.wi[b][wid] = bi; }
+    __syncthreads();
+    double best = sh.wv[b][0];
+    int p = sh.wi[b][0];
+#pragma unroll
+    for (int q = 1; q < LU_TH / 32; ++q) {
+      const double ov = sh.wv[b][q];
+      const int oi = sh.wi[b][q];
+      if (ov > best || (ov == best && oi < p)) { best = ov; p = oi; }
+    }
+    if (!(best > 0.0)) {
+      if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
+      p = j;
+    }
+    if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) sh.prow[b][c] = v[c];
+      sh.pid[b] = id;
+    }
+    if (t == j) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) sh.krow[b][c] = v[c];
+      sh.kid[b] = id;
+    }
+    __syncthreads();
+    if (t == j) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) v[c] = sh.prow[b][c];
+      id = sh.pid[b];
+    } else if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) v[c] = sh.krow[b][c];
+      id = sh.kid[b];
+    }
+    if (t > j && t < rr) {
+      const double2 l = cmul(v[0], crcp(sh.prow[b][0]));
+      v[0] = l;
+#pragma unroll
+      for (int c = 1; c < LU_W; ++c)
+        if (c < LU_W - j) v[c] = cfms(l, sh.prow[b][c], v[c]);
+    }
+    rot1(v);
+  }
+  for (int s = steps; s < LU_W; ++s) rot1(v);  // LU_W rotations in all: columns back in order
+}
+
+__device__ __forceinline__ void load_row(double2 (&v)[LU_W], const double2 *A, long lda, int row, int k, int w) {
+  const double2 *p = A + (size_t)(row < 0 ? 0 : row) * lda + k;
+#pragma unroll
+  for (int c = 0; c < LU_W; ++c) v[c] = (row >= 0 && c < w) ? p[c] : cz();
+}
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// all threads of all CTAs of the cluster; orders global-memory writes before it
+// with reads after it (release / acquire at cluster scope)
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------- panel
+struct panel_sh {
+  gepp_sh g;
+  double2 lu[LU_W][LU_W + 1];
+  double2 ui[LU_W][LU_W + 1];
+  double2 li[LU_W][LU_W + 1];
+  int sel[LU_W], la[LU_W], lb[LU_W];
+};
+
+__global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
+    k_lu_panel(double2 *A, long lda, int n, int k, int *pv, double2 *u, unsigned *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  panel_sh &S = *reinterpret_cast<panel_sh *>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int crank = (int)cluster_rank();
+  const int w = min(LU_W, n - k), m = n - k;
+  double2 v[LU_W];
+  int id = -1;
+  if (m > LU_TH) {
+    // leaves: each CTA a contiguous slice of the panel's rows, in rounds of
+    // LU_TH rows: the winners of a round stay, fresh rows fill the other slots
+    const int q = (m + LU_CL - 1) / LU_CL;
+    const int lo = k + crank * q, hi = min(n, lo + q);
+    int ncand = 0, next = lo;
+    while (next < hi) {
+      const int fresh = min(LU_TH - ncand, hi - next);
+      int row = -1;
+      if (t < ncand) row = id;
+      else if (t < ncand + fresh) row = next + (t - ncand);
+      next += fresh;
+      id = row;
+      load_row(v, A, lda, row, k, w);
+      const int rr = ncand + fresh;
+      gepp(v, id, rr, w, S.g, nullptr);
+      ncand = min(w, rr);
+      __syncthreads();
+    }
+    if (t < ncand) pv[PV_CAND + crank * LU_W + t] = id;
+    if (t == 0) pv[PV_CCNT + crank] = ncand;
+    __threadfence();
+  }
+  cluster_sync_all();
+  if (crank != 0) return;
+  // root: partial pivoting over the leaves' winners (or over all rows of a
+  // short panel), with the values kept: the pivot order and L11\U11
+  int rr;
+  if (m > LU_TH) {
+    int total = 0, mine = -1;
+    for (int cc = 0; cc < LU_CL; ++cc) {
+      const int cnt = __ldcg(pv + PV_CCNT + cc);
+      if (t >= total && t < total + cnt) mine = __ldcg(pv + PV_CAND + cc * LU_W + (t - total));
+      total += cnt;
+    }
+    rr = total;
+    id = mine;
+  } else {
+    rr = m;
+    id = t < m ? k + t : -1;
+  }
+  load_row(v, A, lda, id, k, w);
+  gepp(v, id, rr, w, S.g, status);
+  if (t < LU_W) {
+#pragma unroll
+    for (int c = 0; c < LU_W; ++c) {
+      const double2 x = (t < w) ? v[c] : cz();
+      S.lu[t][c] = x;
+      u[U_LU + t * LU_W + c] = x;
+    }
+    S.sel[t] = t < w ? id : -1;
+    if (t < w) pv[PV_SEL + t] = id;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    // U11^-1, column j = lane: x_j = 1 / u_jj, x_i = -(sum_{i<l<=j} u_il x_l) / u_ii
+    const int j = lane;
+    for (int i = 0; i < LU_W; ++i) S.ui[i][j] = cz();
+    if (j < w) {
+      S.ui[j][j] = crcp(S.lu[j][j]);
+      for (int i = j - 1; i >= 0; --i) {
+        double2 s = cz();
+        for (int l = i + 1; l <= j; ++l) s = cfma(S.lu[i][l], S.ui[l][j], s);
+        const double2 x = cmul(s, crcp(S.lu[i][i]));
+        S.ui[i][j] = make_double2(-x.x, -x.y);
+      }
+    }
+    __syncwarp();
+    for (int i = 0; i < LU_W; ++i) u[U_UINV + i * LU_W + j] = S.ui[i][j];
+  } else if (wid == 1) {
+    // L11^-1 (unit lower), column j = lane: x_j = 1, x_i = -sum_{j<=l<i} l_il x_l
+    const int j = lane;
+    for (int i = 0; i < LU_W; ++i) S.li[i][j] = cz();
+    if (j < w) {
+      S.li[j][j] = make_double2(1.0, 0.0);
+      for (int i = j + 1; i < w; ++i) {
+        double2 s = cz();
+        for (int l = j; l < i; ++l) s = cfma(S.lu[i][l], S.li[l][j], s);
+        S.li[i][j] = make_double2(-s.x, -s.y);
+      }
+    }
+    __syncwarp();
+    for (int i = 0; i < LU_W; ++i) u[U_LINV + i * LU_W + j] = S.li[i][j];
+  } else if (wid == 2) {
+    // row moves: pivot row i goes to position k + i; the rows of the pivot
+    // block that were not picked (displaced) go to the positions the pivot
+    // rows from below left, paired in lane order
+    const int i = lane;
+    const int p = (i < w) ? S.sel[i] : -1;
+    const bool below = (i < w) && (p >= k + w);
+    bool picked = false;
+    for (int jj = 0; jj < w; ++jj) picked |= (S.sel[jj] == k + i);
+    const bool displaced = (i < w) && !picked;
+    const unsigned ba = __ballot_sync(FULL, below), bb = __ballot_sync(FULL, displaced);
+    const unsigned lt = (1u << lane) - 1u;
+    if (below) S.la[__popc(ba & lt)] = p;
+    if (displaced) S.lb[__popc(bb & lt)] = k + i;
+    __syncwarp();
+    const int cnt = __popc(ba);
+    int *perm = pv + PV_PERM;
+    if (lane == 0) perm[0] = w + cnt;
+    if (i < w) { perm[1 + 2 * i] = k + i; perm[2 + 2 * i] = p; }
+    if (lane < cnt) { perm[1 + 2 * (w + lane)] = S.la[lane]; perm[2 + 2 * (w + lane)] = S.lb[lane]; }
+    // the displaced rows' panel values, before anything overwrites them
+    for (int r = 0; r < cnt; ++r)
+      u[U_STAGE + r * LU_W + lane] = lane < w ? A[(size_t)S.lb[r] * lda + k + lane] : cz();
+  }
+}
+
+// ---------------------------------------------------------------- row moves, L21, U12
+#define AP_TH 128
+#define AP_ROWS 32   // rows of an L21 block (4 threads per row)
+#define AP_COLS 16   // columns of a row-move block
+
+__global__ void __launch_bounds__(AP_TH) k_lu_apply(double2 *A, long lda, int n, int k, const int *pv,
+                                                    const double2 *u, int *rowmap, unsigned *status) {
+  __shared__ double2 sm[LU_W][LU_W + 1];
+  __shared__ double2 srow[LU_MAXP][AP_COLS + 1];
+  __shared__ int sdst[LU_MAXP], ssrc[LU_MAXP];
+  const int t = threadIdx.x;
+  const int w = min(LU_W, n - k);
+  const int r0 = k + w;
+  int nperm = __ldcg(pv + PV_PERM);
+  if (nperm < 0 || nperm > LU_MAXP) {
+    if (t == 0) atomicOr(status, BEM_LU_ST_INTERNAL);
+    nperm = 0;
+  }
+  for (int e = t; e < nperm; e += AP_TH) {
+    int d = __ldcg(pv + PV_PERM + 1 + 2 * e), sr = __ldcg(pv + PV_PERM + 2 + 2 * e);
+    if (d < k || d >= n || sr < k || sr >= n) {  // a row move out of range: report, keep the row
+      if (blockIdx.x == 0) atomicOr(status, BEM_LU_ST_INTERNAL);
+      d = sr = k + (e < w ? e : 0);
+    }
+    sdst[e] = d;
+    ssrc[e] = sr;
+  }
+  const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
+  const int nCl = (k + AP_COLS - 1) / AP_COLS, nCr = (n - r0 + AP_COLS - 1) / AP_COLS;
+  const int b = blockIdx.x;
+  if (b < nL) {
+    // L21 = A21 U11^-1 in place, for the rows below the pivot block that no move touches
+    for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(u + U_UINV + e);
+    __syncthreads();
+    const int row = r0 + b * AP_ROWS + (t >> 2), part = t & 3;
+    bool live = row < n;
+    for (int e = w; e < nperm && live; ++e) live = sdst[e] != row;
+    double2 x[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x[c] = cz();
+    if (live) {
+      const double2 *a = A + (size_t)row * lda + k;
+      for (int l = 0; l < w; ++l) {
+        const double2 al = a[l];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
+      }
+    }
+    __syncthreads();  // every read of the row before any write to it
+    if (live) {
+      double2 *a = A + (size_t)row * lda + k;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (part * 8 + c < w) a[part * 8 + c] = x[c];
+    }
+    return;
+  }
+  if (b < nL + nCl + nCr) {
+    // the row moves on AP_COLS columns outside the panel; right of the panel
+    // also U12 = L11^-1 A12 on the pivot block
+    const int i = b - nL;
+    const bool right = i >= nCl;
+    const int c0 = right ? r0 + (i - nCl) * AP_COLS : i * AP_COLS;
+    const int c1 = min(right ? n : k, c0 + AP_COLS);
+    const int nc = c1 - c0;
+    if (right)
+      for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(u + U_LINV + e);
+    __syncthreads();  // sdst / ssrc
+    for (int e = t; e < nperm * AP_COLS; e += AP_TH) {
+      const int pr = e / AP_COLS, cc = e % AP_COLS;
+      srow[pr][cc] = cc < nc ? A[(size_t)ssrc[pr] * lda + c0 + cc] : cz();
+    }
+    __syncthreads();
+    const int cc = t % AP_COLS, grp = t / AP_COLS;  // 8 groups of 16 columns
+    if (cc < nc) {
+      if (right) {
+        for (int ii = grp; ii < w; ii += AP_TH / AP_COLS) {
+          double2 s = cz();
+          for (int l = 0; l <= ii; ++l) s = cfma(sm[ii][l], srow[l][cc], s);
+          A[(size_t)(k + ii) * lda + c0 + cc] = s;
+        }
+        for (int e = w + grp; e < nperm; e += AP_TH / AP_COLS) A[(size_t)sdst[e] * lda + c0 + cc] = srow[e][cc];
+      } else {
+        for (int e = grp; e < nperm; e += AP_TH / AP_COLS) A[(size_t)sdst[e] * lda + c0 + cc] = srow[e][cc];
+      }
+    }
+    return;
+  }
+  // last block: the panel columns of the moved rows (the pivot block gets
+  // L11\U11, a row moved below it its L21), and the row map
+  for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(u + U_UINV + e);
+  __syncthreads();
+  for (int e = t; e < w * LU_W; e += AP_TH) {
+    const int ii = e / LU_W, c = e % LU_W;
+    if (c < w) A[(size_t)(k + ii) * lda + k + c] = __ldcg(u + U_LU + ii * LU_W + c);
+  }
+  {
+    const int r = t >> 2, part = t & 3, e = w + r;
+    if (e < nperm) {
+      double2 x[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = cz();
+      for (int l = 0; l < w; ++l) {
+        const double2 al = __ldcg(u + U_STAGE + r * LU_W + l);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
+      }
+      double2 *a = A + (size_t)sdst[e] * lda + k;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (part * 8 + c < w) a[part * 8 + c] = x[c];
+    }
+  }
+  int old = 0;
+  if (t < nperm) old = rowmap[ssrc[t]];
+  __syncthreads();
+  if (t < nperm) rowmap[sdst[t]] = old;
+}
+
+// ---------------------------------------------------------------- trailing update
+#define UP_BM 64
+#define UP_BN 64
+#define UP_TH 256
+#define UP_LDA 36   // shared-memory row strides (doubles) of the L21 and U12 tiles:
+#define UP_LDB 68   // conflict-free fragment loads
+#define UP_SMEM ((2 * UP_BM * UP_LDA + 2 * LU_W * UP_LDB) * sizeof(double))
+
+// d = a b + d on an 8 x 8 x 4 FP64 tile: a (8 x 4, row) holds a[g][q], b (4 x 8,
+// col) b[q][g], d (8 x 8) d[g][2 q .. 2 q + 1], with g = lane / 4, q = lane % 4
+__device__ __forceinline__ void dmma(double a, double b, double (&d)[2]) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, int n, int k) {
+  extern __shared__ __align__(16) double up_smem[];
+  double *Ar = up_smem, *Ai = Ar + UP_BM * UP_LDA, *Br = Ai + UP_BM * UP_LDA, *Bi = Br + LU_W * UP_LDB;
+  const int t = threadIdx.x;
+  const int w = min(LU_W, n - k);
+  const int r0 = k + w;
+  const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
+  for (int e = t; e < UP_BM * LU_W; e += UP_TH) {
+    const int r = e / LU_W, c = e % LU_W;
+    const double2 x = (rb + r < n && c < w) ? A[(size_t)(rb + r) * lda + k + c] : cz();
+    Ar[r * UP_LDA + c] = x.x;
+    Ai[r * UP_LDA + c] = x.y;
+  }
+  for (int e = t; e < LU_W * UP_BN; e += UP_TH) {
+    const int r = e / UP_BN, c = e % UP_BN;
+    const double2 x = (r < w && cb + c < n) ? A[(size_t)(k + r) * lda + cb + c] : cz();
+    Br[r * UP_LDB + c] = x.x;
+    Bi[r * UP_LDB + c] = x.y;
+  }
+  __syncthreads();
+  const int lane = t & 31, wid = t >> 5, g = lane >> 2, q = lane & 3;
+  const int wm = wid & 1, wn = wid >> 1;  // warp tile: 32 rows x 16 columns
+  double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      const int row = rb + wm * 32 + mt * 8 + g, col = cb + wn * 16 + nt * 8 + 2 * q;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double2 x = (row < n && col + i < n) ? A[(size_t)row * lda + col + i] : cz();
+        cr[mt][nt][i] = x.x;
+        ci[mt][nt][i] = x.y;
+      }
+    }
+#pragma unroll
+  for (int kk = 0; kk < LU_W; kk += 4) {
+    double ar[4], ai[4], br[2], bi[2];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      ar[mt] = Ar[(wm * 32 + mt * 8 + g) * UP_LDA + kk + q];
+      ai[mt] = Ai[(wm * 32 + mt * 8 + g) * UP_LDA + kk + q];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      br[nt] = Br[(kk + q) * UP_LDB + wn * 16 + nt * 8 + g];
+      bi[nt] = Bi[(kk + q) * UP_LDB + wn * 16 + nt * 8 + g];
+    }
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        // (cr, ci) -= (ar + i ai)(br + i bi)
+        dmma(-ar[mt], br[nt], cr[mt][nt]);
+        dmma(ai[mt], bi[nt], cr[mt][nt]);
+        dmma(-ar[mt], bi[nt], ci[mt][nt]);
+        dmma(-ai[mt], br[nt], ci[mt][nt]);
+      }
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      const int row = rb + wm * 32 + mt * 8 + g, col = cb + wn * 16 + nt * 8 + 2 * q;
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+        if (row < n && col + i < n) A[(size_t)row * lda + col + i] = make_double2(cr[mt][nt][i], ci[mt][nt][i]);
+    }
+}
+
+__global__ void k_lu_iota(int *rowmap, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rowmap[i] = i;
+}
+
+// ---------------------------------------------------------------- triangular solves
+#define TS_TH 128
+#define TS_SPIN_LIMIT (1L << 24)
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// wait until *f != 0, at most TS_SPIN_LIMIT polls (about a second), then give up
+// with BEM_LU_ST_WAIT set; once any wait has given up, later waits return at once
+__device__ __forceinline__ void wait_flag(const unsigned *f, unsigned *status) {
+  for (long it = 0; !ld_acquire(f); ++it) {
+    if (it >= TS_SPIN_LIMIT || ((it & 255) == 255 && (ld_acquire(status) & BEM_LU_ST_WAIT))) {
+      atomicOr(status, BEM_LU_ST_WAIT);
+      return;
+    }
+    __nanosleep(64);
+  }
+}
+
+// lower = 1: out = L^-1 (P in), in read through rowmap (unit lower L);
+// lower = 0: out = U^-1 in.  in / out are n x NR column-major; block b of out
+// is published through flags[b] once written.
+template <int NR>
+__global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, int n, const int *rowmap,
+                                                   const double2 *in, double2 *out, unsigned *flags, int lower,
+                                                   unsigned *status) {
+  __shared__ double2 sd[32][33];
+  __shared__ double2 sacc[4][32][NR];
+  const int nb = (n + 31) / 32;
+  const int t = threadIdx.x, r = t & 31, s = t >> 5;
+  for (int it = blockIdx.x; it < nb; it += gridDim.x) {
+    const int b = lower ? it : nb - 1 - it;
+    const int r0 = b * 32, rows = min(32, n - r0);
+    for (int e = t; e < 32 * 32; e += TS_TH) {
+      const int i = e >> 5, j = e & 31;
+      sd[i][j] = (i < rows && j < rows) ? LU[(size_t)(r0 + i) * lda + r0 + j] : cz();
+    }
+    const int row = r0 + r;
+    double2 acc[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = cz();
+    if (s == 0 && r < rows) {
+      const int src = lower ? rowmap[row] : row;
+#pragma unroll
+      for (int q = 0; q < NR; ++q) acc[q] = in[(size_t)q * n + src];
+    }
+    const int jlo = lower ? 0 : b + 1, jhi = lower ? b : nb;
+    for (int jb = jlo; jb < jhi; ++jb) {
+      wait_flag(flags + jb, status);
+      const int c0 = jb * 32 + s * 8;
+      if (r < rows) {
+        const double2 *a = LU + (size_t)row * lda;
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+          const int col = c0 + cc;
+          if (col < n) {
+            const double2 av = a[col];
+#pragma unroll
+            for (int q = 0; q < NR; ++q) acc[q] = cfms(av, __ldcg(out + (size_t)q * n + col), acc[q]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NR; ++q) sacc[s][r][q] = acc[q];
+    __syncthreads();
+    if (s == 0) {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        double2 x = sacc[0][r][q];
+        for (int ss = 1; ss < 4; ++ss) x = make_double2(x.x + sacc[ss][r][q].x, x.y + sacc[ss][r][q].y);
+        acc[q] = x;
+      }
+      if (lower) {
+        for (int i = 0; i < rows; ++i) {
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            const double2 yi = make_double2(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
+            if (r > i && r < rows) acc[q] = cfms(sd[r][i], yi, acc[q]);
+          }
+        }
+      } else {
+        for (int i = rows - 1; i >= 0; --i) {
+          if (r == i) {
+            const double2 d = crcp(sd[i][i]);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) acc[q] = cmul(acc[q], d);
+          }
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            const double2 xi = make_double2(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
+            if (r < i) acc[q] = cfms(sd[r][i], xi, acc[q]);
+          }
+        }
+      }
+      if (r < rows)
+#pragma unroll
+        for (int q = 0; q < NR; ++q) out[(size_t)q * n + row] = acc[q];
+      __threadfence();
+      __syncwarp();
+      if (r == 0) st_release(flags + b, 1u);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- host side
+#define CKL(call, what)                                                                     \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      snprintf(w->err, sizeof(w->err), "%s: %s", what, cudaGetErrorString(_e));            \
+      return -1;                                                                           \
+    }                                                                                      \
+  } while (0)
+
+extern "C" int bem_lu_init(bem_lu *w, int device) {
+  CKL(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  CKL(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(panel_sh)), "panel smem");
+  CKL(cudaFuncSetAttribute(k_lu_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UP_SMEM), "update smem");
+  int per_sm = 0;
+  CKL(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_trsv<4>, TS_TH, 0), "solve occupancy");
+  w->coop_blocks = per_sm * w->sms;
+  if (w->coop_blocks <= 0) {
+    snprintf(w->err, sizeof(w->err), "triangular solve: no resident block");
+    return -1;
+  }
+  CKL(cudaMalloc(&w->piv, PV_INTS * sizeof(int)), "LU scratch");
+  CKL(cudaMalloc(&w->u11, U_COUNT * sizeof(double2)), "LU scratch");
+  CKL(cudaMalloc(&w->status, sizeof(unsigned)), "LU status");
+  CKL(cudaMemset(w->status, 0, sizeof(unsigned)), "LU status");
+  return 0;
+}
+
+extern "C" void bem_lu_free(bem_lu *w) {
+  if (w->gexec) cudaGraphExecDestroy(w->gexec);
+  if (w->graph) cudaGraphDestroy(w->graph);
+  cudaFree(w->rowmap);
+  cudaFree(w->piv);
+  cudaFree(w->u11);
+  cudaFree(w->status);
+  cudaFree(w->flags);
+  cudaFree(w->y);
+  *w = bem_lu();
+}
+
+static int grow_bytes(bem_lu *w, void **p, size_t *cap, size_t bytes, const char *what) {
+  if (*cap >= bytes) return 0;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  CKL(cudaMalloc(p, bytes), what);
+  *cap = bytes;
+  return 0;
+}
+
+// the launches of one factorisation, in order (captured into the graph)
+static int factor_launches(bem_lu *w, double2 *A, int n, cudaStream_t st) {
+  k_lu_iota<<<(n + 255) / 256, 256, 0, st>>>(w->rowmap, n);
+  for (int k = 0; k < n; k += LU_W) {
+    const int wd = n - k < LU_W ? n - k : LU_W;
+    const int r0 = k + wd;
+    k_lu_panel<<<LU_CL, LU_TH, sizeof(panel_sh), st>>>(A, n, n, k, w->piv, (double2 *)w->u11, w->status);
+    const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
+    const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
+    k_lu_apply<<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, w->piv, (const double2 *)w->u11, w->rowmap, w->status);
+    if (r0 < n) {
+      const int tiles = (n - r0 + UP_BM - 1) / UP_BM;
+      k_lu_update<<<dim3(tiles, tiles), UP_TH, UP_SMEM, st>>>(A, n, n, k);
+    }
+  }
+  CKL(cudaGetLastError(), "LU launch");
+  return 0;
+}
+
+extern "C" int bem_lu_factor_z(bem_lu *w, double *Ad, int n, cudaStream_t st) {
+  if (n <= 0) return 0;
+  double2 *A = (double2 *)Ad;
+  if (grow_bytes(w, (void **)&w->rowmap, &w->rowmap_cap, (size_t)n * sizeof(int), "row map")) return -1;
+  if (!(w->gexec && w->g_A == Ad && w->g_n == n)) {
+    if (w->gexec) cudaGraphExecDestroy(w->gexec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    w->gexec = nullptr;
+    w->graph = nullptr;
+    CKL(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "LU capture");
+    const int rc = factor_launches(w, A, n, st);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CKL(ce, "LU capture");
+    w->graph = g;
+    CKL(cudaGraphInstantiate(&w->gexec, g, 0), "LU graph");
+    w->g_A = Ad;
+    w->g_n = n;
+  }
+  CKL(cudaGraphLaunch(w->gexec, st), "LU graph launch");
+  return 0;
+}
+
+template <int NR>
+static int launch_trsv(bem_lu *w, const double2 *LU, int n, const double2 *in, double2 *out, unsigned *flags,
+                       int lower, cudaStream_t st) {
+  const int nb = (n + 31) / 32;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb < w->coop_blocks ? nb : w->coop_blocks);
+  cfg.blockDim = dim3(TS_TH);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CKL(cudaLaunchKernelEx(&cfg, k_lu_trsv<NR>, LU, (long)n, n, (const int *)w->rowmap, in, out, flags, lower,
+                         w->status),
+      "triangular solve");
+  return 0;
+}
+
+extern "C" int bem_lu_solve_z(bem_lu *w, const double *LUd, int n, int nrhs, double *Bd, cudaStream_t st) {
+  if (n <= 0) return 0;
+  if (nrhs < 1 || nrhs > 4) {
+    snprintf(w->err, sizeof(w->err), "LU solve: %d right-hand sides (1..4)", nrhs);
+    return -1;
+  }
+  const int nb = (n + 31) / 32;
+  if (grow_bytes(w, (void **)&w->flags, &w->flags_cap, 2 * (size_t)nb * sizeof(unsigned), "solve flags") ||
+      grow_bytes(w, &w->y, &w->y_cap, (size_t)n * nrhs * sizeof(double2), "solve scratch"))
+    return -1;
+  const double2 *LU = (const double2 *)LUd;
+  double2 *B = (double2 *)Bd, *Y = (double2 *)w->y;
+  CKL(cudaMemsetAsync(w->flags, 0, 2 * (size_t)nb * sizeof(unsigned), st), "solve flags");
+  int rc = 0;
+  switch (nrhs) {
+    case 1: rc = launch_trsv<1>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<1>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 2: rc = launch_trsv<2>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<2>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 3: rc = launch_trsv<3>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<3>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    default: rc = launch_trsv<4>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<4>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+  }
+  return rc ? -1 : 0;
+}
+
+extern "C" unsigned bem_lu_status(bem_lu *w, cudaStream_t st) {
+  unsigned s = 0;
+  if (cudaMemcpyAsync(&s, w->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess) return 0xffffffffu;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return 0xffffffffu;
+  cudaMemsetAsync(w->status, 0, sizeof(unsigned), st);
+  return s;
+}

@@ -1,0 +1,45 @@
+// Dense complex LU factorisation and solves on the device (no library): the
+// FP64 path of the global boundary-integral system and of the per-domain dpv
+// systems, replacing the reference's PARDISO (b_mkl_solver_pardiso_d,
+// d3qd2_mkl_solver.c:18-148) and LAPACKE_zgesv (solve_dpv_bv,
+// bem3_aw_qd2_solve_bieq.c:533-653).  See bem_lu.cu for the algorithm.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#define BEM_LU_W 32            // panel width (columns factored per panel)
+#define BEM_LU_ST_ZERO 0x20u   // a zero pivot (singular matrix), as BEMGPU_ST_SOLVE
+#define BEM_LU_ST_WAIT 0x40u   // a triangular-solve wait gave up (no hang; result invalid)
+#define BEM_LU_ST_INTERNAL 0x80u  // a row move out of range (skipped; result invalid)
+
+struct bem_lu {
+  int *rowmap = nullptr;    // [n] original row of each position after pivoting
+  size_t rowmap_cap = 0;
+  int *piv = nullptr;       // panel scratch: selected pivot rows, candidates, permutation list
+  void *u11 = nullptr;      // panel scratch: packed L11\U11, inverse of U11, inverse of L11, staged rows
+  unsigned *status = nullptr;
+  unsigned *flags = nullptr;  // triangular-solve readiness flags, 2 x ceil(n / 32)
+  size_t flags_cap = 0;
+  void *y = nullptr;          // triangular-solve intermediate (n x nrhs complex)
+  size_t y_cap = 0;
+  // the factorisation of one (matrix, size) as a CUDA graph, replayed while both stay the same
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  const void *g_A = nullptr;
+  int g_n = 0;
+  int sms = 0, coop_blocks = 0;  // device facts for the launches
+  char err[200] = {0};
+};
+
+extern "C" {
+int bem_lu_init(bem_lu *w, int device);
+void bem_lu_free(bem_lu *w);
+// In-place LU with row pivoting of the row-major n x n complex FP64 matrix A:
+// P A = L U (L unit lower, U upper, both in A; w->rowmap holds P).
+int bem_lu_factor_z(bem_lu *w, double *A, int n, cudaStream_t st);
+// Solve A X = B with the factors of bem_lu_factor_z; B is n x nrhs complex,
+// column-major (ld n), overwritten by X; nrhs <= 4.
+int bem_lu_solve_z(bem_lu *w, const double *LU, int n, int nrhs, double *B, cudaStream_t st);
+// Status bits (BEM_LU_ST_*) accumulated since the last call; waits for st.
+unsigned bem_lu_status(bem_lu *w, cudaStream_t st);
+}

@@ -24,6 +24,7 @@
 #include <stdio.h>
 #include <string.h>
 #include "bem_mixed.h"
+#include "bem_refine.h"
 
 #define LEAF_W 32
 
@@ -35,8 +36,10 @@ __global__ void k_round_c32(const double2 *__restrict__ a, cuComplex *__restrict
   }
 }
 
-// x += d (FP64); norms[0] = max |d|, norms[1] = max |x| (|re| + |im|).
-// Non-negative doubles order as their bit patterns, so atomicMax on the bits works.
+// x += d (FP64); norms[0] = max |d|, norms[1] = max |x| (|re| + |im|), +inf in
+// norms[0] if any entry is not finite (bem_refine_norms).  Non-negative
+// doubles, +inf included, order as their bit patterns, so atomicMax on the
+// bits works.
 __global__ void k_axpy_norms(double2 *__restrict__ x, const double2 *__restrict__ d, size_t count,
                              unsigned long long *norms) {
   double md = 0.0, mx = 0.0;
@@ -46,8 +49,7 @@ __global__ void k_axpy_norms(double2 *__restrict__ x, const double2 *__restrict_
     v.x += a.x;
     v.y += a.y;
     x[i] = v;
-    md = fmax(md, fabs(a.x) + fabs(a.y));
-    mx = fmax(mx, fabs(v.x) + fabs(v.y));
+    bem_refine_norms(a.x, a.y, v.x, v.y, &md, &mx);
   }
   for (int o = 16; o > 0; o >>= 1) {
     md = fmax(md, __shfl_down_sync(0xffffffffu, md, o));
@@ -588,7 +590,7 @@ extern "C" int bem_mixed_solve(bem_mixed *m, const double *A, int n, int nrhs, d
     double dn, xn;
     memcpy(&dn, &nb[0], sizeof(double));
     memcpy(&xn, &nb[1], sizeof(double));
-    rc = xn > 0.0 ? dn / xn : 0.0;
+    rc = bem_refine_rel(dn, xn);
     // stop when converged, when the corrections no longer shrink fourfold
     // (the FP64 residual's own accuracy is reached), or when they grow
     // (divergence: the caller falls back to FP64)

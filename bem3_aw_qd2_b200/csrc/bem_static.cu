@@ -68,17 +68,33 @@ static void gl_nodes(int n, double *x, double *w) {
 }
 
 
-// Once per device, with that device current: the device address of the
-// scratch array and the quadrature / Faddeeva constant tables.
-static unsigned char *device_setup(int dev) {
+// Set-up marker in device memory: zero when the module is loaded on a device
+// (also after a cudaDeviceReset reloads it), SETUP_MAGIC once the constant
+// tables are uploaded and the scratch address is known.
+#define SETUP_MAGIC 0x42454d53u
+static __device__ unsigned g_static_ready;
+
+// With the device current: the device address of the scratch array, and the
+// quadrature / Faddeeva constant tables uploaded when the device-side marker
+// says they are not (first call on the device, or after a device reset).
+// The address is looked up on every call, so a stale one is never used.
+static unsigned char *device_setup(int dev, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (g_addr[dev]) return g_addr[dev];
   unsigned char *p = nullptr;
   if (cudaGetSymbolAddress((void **)&p, g_static_scratch) != cudaSuccess || p == nullptr) return nullptr;
+  unsigned ready = 0;
+  if (cudaMemcpyFromSymbolAsync(&ready, g_static_ready, sizeof(ready), 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return nullptr;
+  if (ready == SETUP_MAGIC && p == g_addr[dev]) return p;
   double xl[BEM_GLN_H], wl[BEM_GLN_H], xh[BEM_GHN_H], wh[BEM_GHN_H];
   gl_nodes(BEM_GLN_H, xl, wl);
   gl_nodes(BEM_GHN_H, xh, wh);
   if (bem_set_constants(xl, wl, xh, wh) != 0) return nullptr;
+  ready = SETUP_MAGIC;
+  if (cudaMemcpyToSymbolAsync(g_static_ready, &ready, sizeof(ready), 0, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return nullptr;
   g_addr[dev] = p;
   return p;
 }
@@ -92,11 +108,17 @@ extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw,
             ne, BEMGPU_STATIC_MAX_NE);
     return -2;
   }
+  // every pointer the kernels dereference must be given (an interior domain
+  // also writes dG and dH): a missing one is an error return, not a fault
+  if (!cr || !cw || !ren || !plane || !sid || !qp || !G || !H || !dF || (!periodic && (!dG || !dH))) {
+    fprintf(stderr, "bemgpu_assemble_domain_static: a required input or output pointer is NULL\n");
+    return -2;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return -3;
-  unsigned char *base = device_setup(dev);
-  if (!base) return -3;
   cudaStream_t st = (cudaStream_t)stream;
+  unsigned char *base = device_setup(dev, st);
+  if (!base) return -3;
   bem_scratch S;
   S.rowF = (double *)(base + OFF_ROWF);
   S.near_s = (int *)(base + OFF_NEARS);

@@ -38,14 +38,6 @@ void setup_apw(Apw *pw)
   w->kz = w->R[8] * w->k0;
 }
 
-/* point in the frame where the wave travels along +z */
-static void to_wave_frame(const double *R, const double *v, double *o)
-{
-  o[0] = R[0] * v[0] + R[3] * v[1] - R[6] * v[2];
-  o[1] = R[1] * v[0] + R[4] * v[1] - R[7] * v[2];
-  o[2] = -R[2] * v[0] - R[5] * v[1] + R[8] * v[2];
-}
-
 void calc_apw_pv(double complex *p, double complex *v, double *r, Apw *pw)
 {
   const double *R = pw->wd.R;
@@ -60,7 +52,6 @@ void calc_apw_pv(double complex *p, double complex *v, double *r, Apw *pw)
   double complex vz = pp / (pw->rho0 * pw->c0);
   *p = pp;
   for (int i = 0; i < 3; i++) v[i] = R[i * 3 + 2] * vz;
-  (void)to_wave_frame;
 }
 
 void calc_apw_dpdn(double complex *p, double complex *dpdn, double *r, double *n, Apw *pw)

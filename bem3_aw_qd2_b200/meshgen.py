@@ -19,9 +19,21 @@ import numpy as np
 RHO0, C0 = 1000.0, 1500.0
 
 
-def cube_sphere(n, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, center=(0.0, 0.0, 0.0)):
+def rotation_matrix(axis, deg):
+    """Rotation by deg degrees about axis (Rodrigues' formula)."""
+    a = np.asarray(axis, dtype=float)
+    a = a / np.linalg.norm(a)
+    th = math.radians(deg)
+    K = np.array([[0.0, -a[2], a[1]], [a[2], 0.0, -a[0]], [-a[1], a[0], 0.0]])
+    return np.eye(3) + math.sin(th) * K + (1.0 - math.cos(th)) * (K @ K)
+
+
+def cube_sphere(n, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, center=(0.0, 0.0, 0.0), rot=None):
     """Equiangular cube-sphere with 6 n^2 quads mapped to an ellipsoid.
 
+    rot = (axis, degrees): a further rotation after the one about y, e.g. about
+    a generic axis so that no mirror plane of the mesh is vertical and no two
+    quadrature points of different elements share a height by symmetry.
     Returns (nodes [Nn,3], quads [Ne,4] of 0-based node indices) with every
     quad ordered so that (r1-r0) x (r3-r0) points out of the body."""
     a = np.linspace(-math.pi / 4, math.pi / 4, n + 1)
@@ -55,6 +67,8 @@ def cube_sphere(n, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, center=(0.0, 0.0, 0
         th = math.radians(rot_y_deg)
         R = np.array([[math.cos(th), 0.0, math.sin(th)], [0.0, 1.0, 0.0], [-math.sin(th), 0.0, math.cos(th)]])
         nodes = nodes @ R.T
+    if rot is not None:
+        nodes = nodes @ rotation_matrix(*rot).T
     nodes = nodes + np.array(center, dtype=float)
     quads = np.array(quads, dtype=np.int64)
     c = nodes.mean(axis=0)
@@ -126,9 +140,10 @@ def write_msh(path, nodes, elems, inner_tag=1, open_tag=99):
 
 def write_inputs(dirname, *, n=6, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, lattice=((0.8, 0.0), (0.0, 0.8)),
                  theta_deg=20.0, phi_deg=30.0, rho_in=1.2 * RHO0, c_in=1.5 * C0, wavelength=1.0, amp=(1.0, 0.0),
-                 ico=None):
+                 ico=None, rot=None, center=(0.0, 0.0, 0.0)):
     """Write pw.txt, periodicity.txt, medium.txt and body.msh; returns the 4 paths.
-    ico: icosphere subdivision level (triangles) instead of the cube-sphere."""
+    ico: icosphere subdivision level (triangles) instead of the cube-sphere;
+    rot, center: see cube_sphere (quads only)."""
     os.makedirs(dirname, exist_ok=True)
     f = C0 / wavelength
     pw = os.path.join(dirname, "pw.txt")
@@ -147,7 +162,7 @@ def write_inputs(dirname, *, n=6, semi_axes=(0.3, 0.3, 0.3), rot_y_deg=0.0, latt
     if ico is not None:
         nodes, elems = icosphere(ico, semi_axes, rot_y_deg)
     else:
-        nodes, elems = cube_sphere(n, semi_axes, rot_y_deg)
+        nodes, elems = cube_sphere(n, semi_axes, rot_y_deg, center, rot)
     write_msh(msh, nodes, elems)
     return pw, per, med, msh
 
@@ -166,6 +181,12 @@ CONFIGS = {
                     theta_deg=1e-6, phi_deg=45.0),
     # small case for fixtures and smoke tests: 24 quads, same physics
     "sphere24": dict(n=2, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
+    # 54 quads turned about a generic axis and moved off the lattice plane: no
+    # quadrature point shares its height with another element's point by
+    # symmetry, so the reference's lattice sums never stop on an exactly zero
+    # derivative row there
+    "sphere54_rot": dict(n=3, semi_axes=(0.3, 0.3, 0.3), rot=((1.0, 2.0, 3.0), 37.0), center=(0.0, 0.0, 0.013),
+                         lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
     # 1536 quads (the batched-sweep mesh), one incidence
     "sphere1536": dict(n=16, semi_axes=(0.3, 0.3, 0.3), lattice=((0.8, 0.0), (0.0, 0.8)), theta_deg=20.0, phi_deg=30.0),
     # prolate spheroid 0.2/0.2/0.4 rotated 30 deg about y, 6144 quads, oblique lattice

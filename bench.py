@@ -45,9 +45,40 @@ sys.path.insert(0, ROOT)
 # implementation of the periodic regular-pair kernel on the 216-quad sphere
 # (1.88e12 flop / 6.727e9 terms); frozen, never re-tuned.
 C_TERM_FLOPS = 280.0
-# nominal FP64 peak of B200 (148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz): no
-# measured FP64 peak is available on this pool
-FP64_PEAK_TFLOPS = 37.2
+# nominal FP64 peak of B200 (148 SMs x 64 FP64 FMA/clk x 2 x 1.965 GHz), for
+# context; the roofline divides by the FP64 rate measured in the run
+# (measured_fp64_peak), as the bf16 and HBM peaks of this pool are measured
+FP64_NOMINAL_TFLOPS = 37.2
+# The regular-pair kernels' hardware readings from one ncu capture of the
+# 216-quad workload (profiles/k_q0_regular_sphere216.md and
+# profiles/k_q0_far_sphere216.md, command given there): FP64 pipe busy
+# fraction (sm__pipe_fp64_cycles_active over elapsed cycles) and DRAM bytes
+# read + written per launch.
+NCU_REGULAR = {"k_q0_regular": {"fp64_pipe": None, "dram_bytes": None},
+               "k_q0_far": {"fp64_pipe": None, "dram_bytes": None}}
+
+
+def measured_fp64_peak():
+    """FP64 rate of a dense cuBLAS DGEMM (torch float64 matmul, 8192^3,
+    2 n^3 flop, best of 3 with CUDA events): the measured FP64 ceiling of this
+    GPU, in TFLOP/s."""
+    import torch
+    n = 8192
+    g = torch.Generator(device="cuda").manual_seed(0)
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1000.0)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
 
 
 def parse():
@@ -59,6 +90,8 @@ def parse():
     ap.add_argument("--workload", default="sphere216")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="reference arm: host seconds of complete reference solves (at least one is timed)")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="bracket the first timed mixed-precision step with cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off)")
@@ -121,26 +154,29 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(files, budget_s, threads=None):
-    """The reference's own assembly (oracle/_ref) on a sample of collocation
-    elements, extrapolated to the full assembly, plus the dense solves."""
+def cpu_baseline(files, budget_s, threads=None, seed=20241209):
+    """The reference's own assembly loop (oracle/_ref) on a seeded random
+    sample of collocation elements of each domain, extrapolated linearly to
+    all of them, plus the dense solves: a bounded sample (about budget_s of
+    host time) of one solve, labelled as extrapolated."""
     from oracle import refwrap
     if not refwrap.available():
         return None
     threads = threads or os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(threads)
     case = refwrap.RefCase(*files)
+    rng = np.random.default_rng(seed)
     ne0, ne1 = case.dom_ne[0], case.dom_ne[1]
-    # one collocation element per thread of each domain (the reference's
-    # OpenMP loop runs over collocation elements, dynamic schedule)
-    m0 = min(ne0, threads)
-    t0 = time.perf_counter(); case.assemble_rows(0, 1, 1 + m0); s0 = time.perf_counter() - t0
-    m1 = min(ne1, threads)
-    t0 = time.perf_counter(); case.assemble_rows(1, 1, 1 + m1); s1 = time.perf_counter() - t0
+    # as many elements per domain as host threads (the reference's OpenMP loop
+    # runs over collocation elements, dynamic schedule), drawn at random
+    m0, m1 = min(ne0, threads), min(ne1, threads)
+    rows0 = np.sort(rng.choice(ne0, m0, replace=False)) + 1
+    rows1 = np.sort(rng.choice(ne1, m1, replace=False)) + 1
+    t0 = time.perf_counter(); case.assemble_list(0, rows0); s0 = time.perf_counter() - t0
+    t0 = time.perf_counter(); case.assemble_list(1, rows1); s1 = time.perf_counter() - t0
     t_asm = s0 * ne0 / m0 + s1 * ne1 / m1
     # dense solves with the same OpenBLAS the reference build links (n = 2 NN; dpv: NN with 3 rhs per domain)
     n = 8 * ne0
-    rng = np.random.default_rng(0)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     b = rng.standard_normal(n) + 0j
     t0 = time.perf_counter(); np.linalg.solve(A, b); ts = time.perf_counter() - t0
@@ -149,11 +185,44 @@ def cpu_baseline(files, budget_s, threads=None):
     t0 = time.perf_counter(); np.linalg.solve(A2, B2); np.linalg.solve(A2, B2); td = time.perf_counter() - t0
     total = t_asm + ts + td
     return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "reference",
-            "sample": "reference create_cmatrix_domain loop on %d of %d collocation elements (domain 0) and %d of %d "
-                      "(domain 1), %d OpenMP threads, extrapolated linearly (%.1f s measured); dense solves timed "
-                      "at n=%d (OpenBLAS zgesv, as linked by the reference build)" % (m0, ne0, m1, ne1, threads,
-                                                                                        s0 + s1, n),
+            "sample": "extrapolated: reference create_cmatrix_domain loop on %d of %d collocation elements (domain 0) "
+                      "and %d of %d (domain 1), drawn with numpy default_rng(%d), %d OpenMP threads, scaled linearly "
+                      "in elements (%.1f s measured); dense solves timed at n=%d (OpenBLAS zgesv, as linked by the "
+                      "reference build)" % (m0, ne0, m1, ne1, seed, threads, s0 + s1, n),
             "seconds_per_solve": total, "assembly_seconds_extrapolated": t_asm}
+
+
+# Workloads whose full reference solve fits a bench run (about 3 minutes on
+# 16 host threads for the 216-quad sphere): the reference arm times complete
+# solves of these; larger ones are sampled and extrapolated (cpu_baseline).
+FULL_REFERENCE_SOLVE = {"sphere216"}
+
+
+def reference_full_solves(files, budget_s, max_steps, threads):
+    """Complete solves by the reference's own solver program
+    (oracle/_ref/aw_d3qd2_bv_solver: read, assemble, PARDISO stand-in, pv,
+    dpv, .dat write) plus its type-0 force (force_FN_aqd2), each timed on the
+    host clock; repeated while the budget lasts (at least one)."""
+    from oracle import refwrap
+    exe = os.path.join(ROOT, "oracle", "_ref", "aw_d3qd2_bv_solver")
+    wd = os.path.dirname(files[0])
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_steps:
+        t0 = time.perf_counter()
+        r = subprocess.run([exe] + [os.path.basename(f) for f in files] + ["ref_out.dat"], cwd=wd, env=env,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("reference solver failed: " + r.stderr[-500:])
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        case = refwrap.RefCase.from_dat(os.path.join(wd, "ref_out.dat"))
+        case.force(0)
+        times.append(time.perf_counter() - t0)
+        elapsed = time.perf_counter() - t_start
+        if elapsed + times[-1] > budget_s:
+            break
+    return times
 
 
 def run_reference(args, rank, world):
@@ -166,21 +235,40 @@ def run_reference(args, rank, world):
     if not refwrap.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference build) is missing"}))
         return
-    warm = refwrap.RefCase(*files)
-    for _ in range(args.warmup):  # warm-up: one interior collocation element (pages in code and data)
-        warm.assemble_rows(1, 1, 2)
-    vals = []
-    for _ in range(args.steps):
-        cb = cpu_baseline(files, args.cpu_seconds)
-        vals.append(cb["value"])
-    v = statistics.mean(vals)
-    cb["value"] = v
-    print(json.dumps({"impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": args.workload, **workload_desc(args.workload)},
-                      "cpu_baseline": cb, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                                                  "d2h_bytes_per_step": 0}}))
+    threads = os.cpu_count()
+    base = {"impl": "reference", "metric": "solves/s", "unit": "solves/s", "n_gpus": args.gpus,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, **workload_desc(args.workload)}, "steps_requested": args.steps,
+            "warmup_requested": args.warmup}
+    if args.workload in FULL_REFERENCE_SOLVE:
+        # complete solves, as many as fit the budget: steps = solves timed
+        times = reference_full_solves(files, args.ref_budget_s, args.steps, threads)
+        v = len(times) / sum(times)
+        cb = {"value": v, "unit": "solves/s", "cores": threads, "kind": "reference",
+              "sample": "%d complete solve(s) of the workload by the reference's own aw_d3qd2_bv_solver "
+                        "(oracle/_ref, OpenMP on %d host threads, dense LU stand-in for PARDISO on OpenBLAS) plus "
+                        "force_FN_aqd2 type 0, host clock per solve; no warm-up solve (CPU code)" % (len(times),
+                                                                                                 threads),
+              "seconds_per_solve": [float(t) for t in times]}
+        line = dict(base, value=v, steps=len(times), warmup=0, ms_per_step=1000.0 * sum(times) / len(times))
+    else:
+        warm = refwrap.RefCase(*files)
+        for _ in range(args.warmup):  # warm-up: one interior collocation element (pages in code and data)
+            warm.assemble_rows(1, 1, 2)
+        vals, walls = [], []
+        for step in range(args.steps):
+            t0 = time.perf_counter()
+            cb = cpu_baseline(files, args.cpu_seconds, threads, seed=20241209 + step)
+            walls.append(time.perf_counter() - t0)
+            vals.append(cb["value"])
+        v = statistics.mean(vals)
+        cb["value"] = v
+        cb["sample"] += "; mean of %d seeded samples" % args.steps
+        line = dict(base, value=v, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=1000.0 * sum(walls) / len(walls), extrapolated=True)
+    line["cpu_baseline"] = cb
+    line["e2e"] = {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
 
 
 STREAM_DESC = ("seeded Poisson request stream (numpy default_rng(2024)), scaled down from the 216-6144-quad "
@@ -318,6 +406,25 @@ def run_stream(args, rank, world):
         dist.destroy_process_group()
 
 
+def roofline_record(achieved, fp64_peak, terms_reg, cnt):
+    """The dominant kernels' roofline: periodic regular-pair assembly
+    (k_q0_regular on near-ish pairs, k_q0_far on far ones, one phase), FP64
+    work = lattice terms counted by the kernels x the frozen per-term count,
+    over the phase's CUDA-event time; beside it the FP64 pipe fraction and DRAM
+    traffic ncu read on the same kernels."""
+    reg, far = NCU_REGULAR["k_q0_regular"], NCU_REGULAR["k_q0_far"]
+    traffic = None
+    if reg["dram_bytes"] is not None and far["dram_bytes"] is not None:
+        traffic = reg["dram_bytes"] + far["dram_bytes"]
+    return {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far (regular pairs)", "achieved": achieved,
+            "peak": fp64_peak, "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
+            "traffic": traffic, "traffic_unit": "bytes per launch pair (ncu dram__bytes_read.sum + write.sum)",
+            "peak_source": "of measured: cuBLAS DGEMM 8192^3 in this run (nominal %.1f TFLOP/s)" % FP64_NOMINAL_TFLOPS,
+            "fp64_pipe_frac_ncu": {"k_q0_regular": reg["fp64_pipe"], "k_q0_far": far["fp64_pipe"]},
+            "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
+            "mean_terms_per_point": cnt[0] / max(cnt[3], 1)}
+
+
 def workload_desc(name):
     from bem3_aw_qd2_b200 import meshgen
     return {**meshgen.describe(name), "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
@@ -356,6 +463,7 @@ def main():
     stream = torch.cuda.ExternalStream(int(g.bemgpu_stream(ctx)))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     ewald_scale = case.autotune()  # Ewald parameter for this problem (kept for every later solve)
+    fp64_peak = measured_fp64_peak()
     g.bemgpu_set_profiling(ctx, 1)
     rc = np.zeros(3)
     F = np.zeros(3)
@@ -483,11 +591,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "solve_bieq_aqd2 + force_FN_aqd2 (C ABI, host buffers)"},
         "phase_ms": phase_ms,
-        "roofline": {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far (regular pairs)", "achieved": achieved, "peak": FP64_PEAK_TFLOPS,
-                     "unit": "TFLOP/s", "frac": (achieved / FP64_PEAK_TFLOPS) if achieved else None, "traffic": None,
-                     "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
-                     "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
-                     "mean_terms_per_point": cnt[0] / max(cnt[3], 1)},
+        "roofline": roofline_record(achieved, fp64_peak, terms_reg, cnt),
         "clocks": clk,
         "mixed": mixed,
         "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1 + 1),

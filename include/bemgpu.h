@@ -239,18 +239,23 @@ int bemgpu_work_counters(bemgpu_ctx *ctx, unsigned long long *out6, int reset);
  * (H gets 1 + F on its diagonal); 0: an interior domain in free space with
  * wave number k (H gets F).  The layouts are those of bemgpu_get_matrix.
  * Every element is taken as a bilinear quad (4 nodes); meshes with linear
- * triangles go through bemgpu_load + bemgpu_assemble.
+ * triangles go through bemgpu_load + bemgpu_assemble.  Every regular pair is
+ * integrated with the reference's 12 x 12 rule (as a context after
+ * bemgpu_set_far_rule(ctx, 0)) and the Ewald parameter is the reference's.
  *
  * The scratch the assembly needs lives in one fixed array inside the library
  * (about 21 MB on every GPU that loads it, kept until the process exits), so
  * a domain may have at most BEMGPU_STATIC_MAX_NE elements; more is rejected
  * with -2 and a message on stderr.  The first call on each device sets the
  * array up (finds its device address, uploads the quadrature tables); make
- * that first call before any stream capture.  Every call reuses the array and
+ * that first call before any stream capture.  Each call checks a marker in
+ * device memory and repeats the set-up when the device lost it (a
+ * cudaDeviceReset), and looks the array's address up again.  Every call reuses the array and
  * finds the previous call's contents in it (the status word is cleared at
  * the start of each call); calls that overlap on the GPU race on it, so the
  * caller must not run two at once.  The call returns after its work on
- * stream has finished.  Returns 0; -2 size out of range; -3 device set-up
+ * stream has finished.  Returns 0; -2 size out of range or a required
+ * pointer NULL (dG, dH may be NULL only when periodic = 1); -3 device set-up
  * failed; -4 launch or copy failed; -5 a BEMGPU_ST_* status bit was set. */
 #define BEMGPU_STATIC_MAX_NE 1536
 int bemgpu_assemble_domain_static(const double *cr, const double *cw, const double *ren, const unsigned char *plane,
@@ -295,6 +300,15 @@ int bemgpu_server_poll(bemgpu_server *srv, bemgpu_result *out, int max, int time
 /* out8: submitted, completed, solved by reuse, running, queued, device bytes resident, peak, evictions */
 int bemgpu_server_stats(bemgpu_server *srv, double *out8);
 void bemgpu_server_destroy(bemgpu_server *srv);
+
+/* Dense complex solve A X = B on the device (the FP64 factorisation and
+ * solves the context uses for the global and dpv systems, bem_lu.cu),
+ * replacing LAPACKE_zgesv (solve_dpv_bv, bem3_aw_qd2_solve_bieq.c:617) and
+ * the dense PARDISO solve (b_mkl_solver_pardiso_d, d3qd2_mkl_solver.c:18):
+ * A row-major n x n complex (host), B column-major n x nrhs complex (host,
+ * nrhs <= 4), overwritten by X.  Allocates its own device buffers for the
+ * call.  Returns 0; -2 bad size; -3 singular (zero pivot); -1 CUDA error. */
+int bemgpu_zgesv(int device, int n, int nrhs, const double *A, double *B);
 
 /* Faddeeva w(z) at n points (host arrays of (re, im) pairs), relative error
  * 1e-15 (Faddeeva_w, qgf2_src/Faddeeva.cc:679, called with MEPS). */

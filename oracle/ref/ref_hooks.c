@@ -131,6 +131,32 @@ double ref_assemble_rows(AQD2 *qd, int did, int t0, int t1)
   return chk;
 }
 
+/* The same loop on a list of collocation elements ts[0..n) (1-based), e.g. a
+ * seeded random sample of the domain's rows. */
+double ref_assemble_list(AQD2 *qd, int did, const int *ts, int n)
+{
+  double chk = 0.0;
+  int Ne = qd->bd.sb[did].Ne;
+  double complex kc = (double complex)qd->k0[did];
+  #pragma omp parallel for schedule(dynamic) reduction(+:chk)
+  for (int i = 0; i < n; i++) {
+    double complex CC[9], dCz[9], dCe[9];
+    double vtz[3], vte[3];
+    int td = qd->bd.sb[did].sid[ts[i]];
+    int tl = (ELT3 == check_element_type(td, &(qd->bd))) ? 3 : 4;
+    for (int tn = 0; tn < tl; tn++) {
+      tz_te_bd_node(vtz, vte, td, tn, &(qd->bd));
+      for (int s = 1; s <= Ne; s++) {
+        int sd = qd->bd.sb[did].sid[s];
+        if (did == 0 && qd->bd.ps == 1) q0_dcoef_bd_node_t2_cc(CC, dCz, dCe, td, tn, vtz, vte, sd, kc, 2, &(qd->bd));
+        else dcoef_bd_node_t2(CC, dCz, dCe, td, tn, vtz, vte, sd, kc, 2, &(qd->bd));
+        chk += creal(CC[0]) + cimag(CC[4]);
+      }
+    }
+  }
+  return chk;
+}
+
 /* One element-pair coefficient call, for unit tests of the per-pair kernels.
  * out: CC[9], dCdtz[9], dCdte[9] as interleaved (re, im). */
 void ref_pair_coef(AQD2 *qd, int did, int t, int tn, int s, double *out)

@@ -36,11 +36,14 @@ def lib():
         L.ref_assemble_domain_files.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_assemble_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.ref_assemble_rows.restype = ctypes.c_double
+        L.ref_assemble_list.argtypes = [ctypes.c_void_p, ctypes.c_int, i, ctypes.c_int]
+        L.ref_assemble_list.restype = ctypes.c_double
         L.ref_pair_coef.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, d]
         L.ref_domain_ne.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_get_solution.argtypes = [ctypes.c_void_p, ctypes.c_int, d, d, d, d]
         L.force_FN_aqd2.argtypes = [d, d, d, ctypes.c_int, ctypes.c_void_p]
         L.finalize_aqd2.argtypes = [ctypes.c_void_p]
+        L.dat_read_aqd2.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -79,6 +82,19 @@ class RefCase:
         L.ref_load(self.qd, pw.encode(), per.encode(), med.encode(), msh.encode())
         self.MN = L.ref_mn(self.qd)
         self.dom_ne = [L.ref_domain_ne(self.qd, d) for d in range(self.MN + 1)]
+
+    @classmethod
+    def from_dat(cls, path):
+        """dat_read_aqd2 (bem3_aw_qd2.c:226) of a solved system, e.g. one the
+        reference ships with its results."""
+        L = lib()
+        c = cls.__new__(cls)
+        c.buf = ctypes.create_string_buffer(L.ref_sizeof_aqd2())
+        c.qd = ctypes.cast(c.buf, ctypes.c_void_p)
+        L.dat_read_aqd2(path.encode(), c.qd)
+        c.MN = L.ref_mn(c.qd)
+        c.dom_ne = [L.ref_domain_ne(c.qd, d) for d in range(c.MN + 1)]
+        return c
 
     def solve(self, workdir=None):
         """Full solve; returns the coefficient matrices read from the temp files."""
@@ -148,6 +164,11 @@ class RefCase:
     def assemble_rows(self, did, t0, t1):
         """Time the reference's own assembly loop on collocation elements [t0, t1) (1-based)."""
         return lib().ref_assemble_rows(self.qd, did, t0, t1)
+
+    def assemble_list(self, did, rows):
+        """The reference's assembly loop on the listed collocation elements (1-based)."""
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        return lib().ref_assemble_list(self.qd, did, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(rows))
 
     def pair(self, did, t, tn, s):
         out = np.zeros(54)

@@ -23,8 +23,19 @@ outputs as compressed .npz files:
                  the sphere and next to the boundary with rules 0-3, and
                  boundary values (phi_s_bd, pv_t_bd) on elements of both domains
 
-Usage: python tests/golden/make_golden.py [fields|plane|tri]  (needs oracle/_ref;
-a few minutes; the argument regenerates fields24.npz / qpgf_plane.npz / tri80.npz only)
+  sphere216.npz  the 216-quad benchmark configuration solved by the reference
+                 (sampled matrix rows, products with a random-phase vector,
+                 absolute row sums, P, dP, pv, dpv, forces of both rules)
+  sphere54_rot.npz, fields54_rot.npz
+                 a full solve, forces, fields and boundary values of a 54-quad
+                 sphere turned about a generic axis (no lattice-plane ties)
+  shipped_*.npz  the reference's own shipped solved systems (ex.dat,
+                 verification/, analysis_sample1/ex1.dat, analysis_sample2/ex2.dat):
+                 their input files, the values their example1.log prints and
+                 the solutions stored in the .dat files
+
+Usage: python tests/golden/make_golden.py [fields|plane|tri|far|near|sphere216|rot|shipped [dir]]
+(needs oracle/_ref; a few minutes; an argument regenerates only that fixture)
 """
 import math
 import os
@@ -219,6 +230,110 @@ def make_fields(case, out_name="fields24.npz", boundary_points=BOUNDARY_POINTS):
     np.savez_compressed(os.path.join(OUT, out_name), **out)
 
 
+def checksum_weights(n):
+    """Fixed weights of the array checksums (the tests rebuild them the same way)."""
+    return np.cos(0.7 * np.arange(n) + 0.3)
+
+
+def make_sphere216():
+    """The 216-quad configuration (the benchmark's workload) solved by the
+    reference: sampled rows, a random-phase product and the absolute row sums
+    of every coefficient matrix, the full P, dP, pv, dpv of both domains and
+    the forces of both rules.  Takes several minutes on a few host threads."""
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    files = meshgen.write_inputs(tmp, **meshgen.CONFIGS["sphere216"])
+    case = refwrap.RefCase(*files)
+    mats = case.solve(tmp)
+    rng = np.random.default_rng(20241207)
+    out = {}
+    for d in range(case.MN + 1):
+        N = 4 * case.dom_ne[d]
+        x = np.exp(2j * np.pi * rng.random(N))
+        out["x%d" % d] = x
+        for name in ("G", "H") + (("dG", "dH") if d > 0 else ()):
+            M = mats["%s%d" % (name, d)]
+            rows = np.sort(rng.choice(M.shape[0], 6, replace=False))
+            out["%s%d_rows" % (name, d)] = rows
+            out["%s%d_sample" % (name, d)] = M[rows]
+            out["%s%d_Mx" % (name, d)] = M @ x
+            out["%s%d_abs" % (name, d)] = np.abs(M).sum(axis=1)
+        out["dF%d" % d] = mats["dF%d" % d]
+        P, dP, pv, dpv = case.solution(d)
+        out.update({"P%d" % d: P, "dP%d" % d: dP, "pv%d" % d: pv, "dpv%d" % d: dpv})
+    out["F0"], out["N0"] = case.force(0)
+    out["F1"], out["N1"] = case.force(1)
+    np.savez_compressed(os.path.join(OUT, "sphere216.npz"), **out)
+
+
+def make_rot():
+    """54 quads turned about a generic axis (no point of one element shares its
+    height with another's by symmetry): P, dP, pv, dpv, both force rules and
+    the field and boundary values of fields24.npz's point lists (the matrices
+    are left out: the 24-quad fixtures cover them)."""
+    case = make_solve("sphere54_rot", "sphere54_rot.npz")
+    g = dict(np.load(os.path.join(OUT, "sphere54_rot.npz")))
+    np.savez_compressed(os.path.join(OUT, "sphere54_rot.npz"),
+                        **{k: v for k, v in g.items() if not k.startswith(("G", "H", "dG", "dH", "dF"))})
+    make_fields(case, "fields54_rot.npz")
+
+
+# The solved systems the reference ships: (name, directory, .dat file or None, mesh)
+SHIPPED = [("ex", "", "ex.dat", "sphere_m1.msh"), ("veri", "verification", None, "sphere_m1.msh"),
+           ("ex1", "analysis_sample1", "ex1.dat", "sphere_m1.msh"), ("ex2", "analysis_sample2", "ex2.dat", "sphere_m3.msh")]
+
+
+def parse_example1_log(path):
+    """p, v (type 0 and 1) at r = (-0.03, 0.01, 0.002) and F, N (type 0 and 1)
+    as printed by the reference's example1.c."""
+    import re
+    cplx = []
+    vecs = []
+    for line in open(path):
+        m = re.match(r"\s*(p|vx|vy|vz)\s*=\s*(\S+)\s*([+-]\S+)\s*I", line)
+        if m:
+            cplx.append(complex(float(m.group(2)), float(m.group(3))))
+        m = re.match(r"\s*[FN] = \(([^)]*)\)", line)
+        if m:
+            vecs.append([float(v) for v in m.group(1).split(",")])
+    assert len(cplx) == 8 and len(vecs) == 4, path
+    return {"p_t0": cplx[0], "v_t0": np.array(cplx[1:4]), "p_t1": cplx[4], "v_t1": np.array(cplx[5:8]),
+            "F0": np.array(vecs[0]), "N0": np.array(vecs[1]), "F1": np.array(vecs[2]), "N1": np.array(vecs[3])}
+
+
+def make_shipped(ref_dir):
+    """Fixtures of the reference's shipped solved systems: the four input files
+    as text (the mesh zlib-compressed), the values its example1.log prints and,
+    where the .dat ships, the stored solution: P, dP of every domain in full,
+    pv, dpv on 48 seeded elements per domain plus weighted sums over all
+    elements (checksum_weights) and the matching sums of absolute values."""
+    import zlib
+    for name, sub, dat, msh in SHIPPED:
+        base = os.path.join(ref_dir, sub)
+        out = {"name": name}
+        for f in ("pw.txt", "periodicity.txt", "medium.txt"):
+            out[f.split(".")[0]] = open(os.path.join(base, f)).read()
+        out["mesh_name"] = msh
+        out["mesh_z"] = np.frombuffer(zlib.compress(open(os.path.join(base, msh), "rb").read(), 9), np.uint8)
+        out.update(parse_example1_log(os.path.join(base, "example1.log")))
+        if dat is not None:
+            case = refwrap.RefCase.from_dat(os.path.join(base, dat))
+            rng = np.random.default_rng(20241208)
+            out["MN"] = case.MN
+            out["dom_ne"] = np.array(case.dom_ne)
+            for d in range(case.MN + 1):
+                P, dP, pv, dpv = case.solution(d)
+                out["P%d" % d], out["dP%d" % d] = P, dP
+                idx = np.sort(rng.choice(case.dom_ne[d], 48, replace=False))
+                out["idx%d" % d] = idx
+                out["pv%d" % d], out["dpv%d" % d] = pv[idx], dpv[idx]
+                w = checksum_weights(pv.size)
+                for k, a in (("pv", pv), ("dpv", dpv)):
+                    out["%s%d_sum" % (k, d)] = np.dot(w, a.ravel())
+                    out["%s%d_abs" % (k, d)] = np.dot(np.abs(w), np.abs(a.ravel()))
+        np.savez_compressed(os.path.join(OUT, "shipped_%s.npz" % name), **out)
+        print("shipped_%s.npz" % name)
+
+
 def main():
     rng = np.random.default_rng(20241203)
     if sys.argv[1:] == ["tri"]:
@@ -234,6 +349,17 @@ def main():
     if sys.argv[1:] == ["near"]:
         make_near_pairs()
         print("near216.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["sphere216"]:
+        make_sphere216()
+        print("sphere216.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["rot"]:
+        make_rot()
+        print("sphere54_rot.npz, fields54_rot.npz written to", OUT)
+        return
+    if sys.argv[1:2] == ["shipped"]:
+        make_shipped(sys.argv[2] if len(sys.argv) > 2 else os.environ.get("BEM_REFERENCE_DIR", "/root/reference"))
         return
     if sys.argv[1:] == ["plane"]:
         make_plane()

@@ -104,7 +104,7 @@ def test_oracle_reproduces_reference_example1_log():
     """Pins the reference build: force (type 0) and field (type 0) on the
     reference's own shipped ex.dat must equal example1.log."""
     from oracle import refwrap
-    exdat = "/root/reference/ex.dat"
+    exdat = os.path.join(os.environ.get("BEM_REFERENCE_DIR", "/root/reference"), "ex.dat")
     if not (refwrap.available() and os.path.exists(exdat)):
         pytest.skip("needs oracle/_ref and the reference sources")
     code = r"""

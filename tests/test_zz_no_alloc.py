@@ -80,54 +80,123 @@ def _entry():
     return fn
 
 
-def test_static_assembly_matches_context_path_twice():
+def _static_matrices(fn, t, dom, stream, dev, outs=None):
+    """One call of the entry point for domain dom of the parsed case t into
+    caller-owned torch buffers (made once and passed back in as outs)."""
+    import torch
+    sid = torch.tensor(t["sids"][dom], dtype=torch.int32, device=dev)
+    ne = len(t["sids"][dom])
+    N = 4 * ne
+    if outs is None:
+        outs = dict(G=torch.empty((N, N), dtype=torch.complex128, device=dev),
+                    H=torch.empty((N, N), dtype=torch.complex128, device=dev),
+                    dF=torch.empty((N, 3), dtype=torch.float64, device=dev),
+                    dG=torch.empty((2 * N, N), dtype=torch.complex128, device=dev) if dom else None,
+                    dH=torch.empty((2 * N, N), dtype=torch.complex128, device=dev) if dom else None,
+                    sid=sid)
+    for k in ("G", "H", "dF", "dG", "dH"):
+        if outs[k] is not None:
+            outs[k].fill_(float("nan"))
+    torch.cuda.synchronize()
+    qp = np.ascontiguousarray(t["qp"])
+    rc = fn(t["cr_d"].data_ptr(), t["cw_d"].data_ptr(), t["ren_d"].data_ptr(), t["plane_d"].data_ptr(),
+            outs["sid"].data_ptr(), ne, qp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1 if dom == 0 else 0,
+            float(t["k0"][dom]), outs["G"].data_ptr(), outs["H"].data_ptr(),
+            outs["dG"].data_ptr() if outs["dG"] is not None else None,
+            outs["dH"].data_ptr() if outs["dH"] is not None else None, outs["dF"].data_ptr(), stream.cuda_stream)
+    assert rc == 0, "domain %d returned %d" % (dom, rc)
+    torch.cuda.synchronize()
+    return outs
+
+
+def _case_tables(config):
     import torch
     from bem3_aw_qd2_b200 import api, meshgen
     h, _ = api.libs()
     h.aqd2_set_verbose(0)
     d = tempfile.mkdtemp(prefix="bem_static_")
-    files = meshgen.write_inputs(d, **meshgen.CONFIGS["sphere24"])
-    case = api.Case.from_files(*files)
+    case = api.Case.from_files(*meshgen.write_inputs(d, **meshgen.CONFIGS[config]))
     case.solve()
     datp = os.path.join(d, "case.dat")
     case.dat_write(datp)
     t = parse_dat(datp)
     dev = torch.device("cuda:0")
-    cr = torch.tensor(t["cr"], device=dev)
-    cw = torch.tensor(t["cw"], device=dev)
-    ren = torch.tensor(t["ren"], device=dev)
-    plane = torch.tensor(t["plane"], device=dev)
+    for k in ("cr", "cw", "ren", "plane"):
+        t[k + "_d"] = torch.tensor(t[k], device=dev)
+    return case, t, dev
+
+
+def test_static_assembly_matches_context_path_twice():
+    """24 quads: the same matrices as the context path and as the reference's
+    own (tests/golden/sphere24.npz), on two calls in a row."""
+    import torch
+    case, t, dev = _case_tables("sphere24")
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "sphere24.npz"))
     fn = _entry()
     stream = torch.cuda.Stream(device=dev)
-    qp = np.ascontiguousarray(t["qp"])
     for call in range(2):
         for dom in (0, 1):
-            sid = torch.tensor(t["sids"][dom], dtype=torch.int32, device=dev)
-            ne = len(t["sids"][dom])
-            N = 4 * ne
-            G = torch.full((N, N), float("nan"), dtype=torch.complex128, device=dev)
-            H = torch.full((N, N), float("nan"), dtype=torch.complex128, device=dev)
-            dF = torch.full((N, 3), float("nan"), dtype=torch.float64, device=dev)
-            dG = torch.zeros((2 * N, N), dtype=torch.complex128, device=dev) if dom else None
-            dH = torch.zeros((2 * N, N), dtype=torch.complex128, device=dev) if dom else None
-            torch.cuda.synchronize()
-            rc = fn(cr.data_ptr(), cw.data_ptr(), ren.data_ptr(), plane.data_ptr(), sid.data_ptr(), ne,
-                    qp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1 if dom == 0 else 0, float(t["k0"][dom]),
-                    G.data_ptr(), H.data_ptr(), dG.data_ptr() if dG is not None else None,
-                    dH.data_ptr() if dH is not None else None, dF.data_ptr(), stream.cuda_stream)
-            assert rc == 0, "call %d domain %d returned %d" % (call, dom, rc)
-            torch.cuda.synchronize()
-            assert rel_rows(G.cpu().numpy(), case.matrix(dom, "G", N)) < 1e-10
-            assert rel_rows(H.cpu().numpy(), case.matrix(dom, "H", N)) < 1e-10
-            assert np.max(np.abs(dF.cpu().numpy() - case.matrix(dom, "dF", N))) < 1e-10
-            if dom:
-                assert rel_rows(dG.cpu().numpy(), case.matrix(dom, "dG", N)) < 1e-10
-                assert rel_rows(dH.cpu().numpy(), case.matrix(dom, "dH", N)) < 1e-10
+            N = 4 * len(t["sids"][dom])
+            o = _static_matrices(fn, t, dom, stream, dev)
+            for k in ("G", "H") + (("dG", "dH") if dom else ()):
+                got = o[k].cpu().numpy()
+                assert rel_rows(got, case.matrix(dom, k, N)) < 1e-10, (call, dom, k)
+                assert rel_rows(got, gold["%s%d" % (k, dom)]) < 1e-10, (call, dom, k)
+            dF = o["dF"].cpu().numpy()
+            assert np.max(np.abs(dF - case.matrix(dom, "dF", N))) < 1e-10
+            ref = gold["dF%d" % dom]
+            assert np.max(np.abs(dF[:, 0] - ref[:, 0])) < 1e-10 * np.max(np.abs(ref[:, 0]))
+            assert np.max(np.abs(dF[:, 1:] - ref[:, 1:])) < 1e-11
+    case.close()
 
 
-def test_static_assembly_rejects_oversized_domain():
+def test_static_assembly_with_far_pairs_allocates_nothing():
+    """216 quads, where most regular pairs are far: the entry point keeps the
+    reference's 12 x 12 rule on every pair, so it is compared with a context
+    set to that rule (bemgpu_set_far_rule(ctx, 0)).  The second call runs with
+    the device's free memory unchanged: nothing is allocated."""
+    import torch
+    case, t, dev = _case_tables("sphere216")
+    case.set_far_rule(0)
+    case.run_device()
+    fn = _entry()
+    stream = torch.cuda.Stream(device=dev)
+    outs = {dom: _static_matrices(fn, t, dom, stream, dev) for dom in (0, 1)}  # warm: loads the kernels
+    free_before = torch.cuda.mem_get_info(dev)[0]
+    for dom in (0, 1):
+        _static_matrices(fn, t, dom, stream, dev, outs[dom])
+    free_after = torch.cuda.mem_get_info(dev)[0]
+    assert free_after == free_before, (free_before, free_after)
+    for dom in (0, 1):
+        N = 4 * len(t["sids"][dom])
+        for k in ("G", "H") + (("dG", "dH") if dom else ()):
+            assert rel_rows(outs[dom][k].cpu().numpy(), case.matrix(dom, k, N)) < 1e-10, (dom, k)
+        assert np.max(np.abs(outs[dom]["dF"].cpu().numpy() - case.matrix(dom, "dF", N))) < 1e-10
+    case.close()
+
+
+def test_static_assembly_rejects_bad_arguments():
+    """Sizes beyond the limit and missing pointers are error returns (-2),
+    checked on the host before any device work."""
+    import torch
     fn = _entry()
     qp = np.zeros(8)
-    rc = fn(None, None, None, None, None, 1537, qp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1, 1.0,
-            None, None, None, None, None, None)
+    qpp = qp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rc = fn(None, None, None, None, None, 1537, qpp, 1, 1.0, None, None, None, None, None, None)
+    assert rc == -2
+    rc = fn(None, None, None, None, None, 4, qpp, 1, 1.0, None, None, None, None, None, None)
+    assert rc == -2
+    dev = torch.device("cuda:0")
+    ne, N = 1, 4
+    buf = {k: torch.zeros(n, dtype=torch.float64, device=dev) for k, n in
+           (("cr", 12), ("cw", 9), ("ren", 12), ("G", 2 * N * N), ("H", 2 * N * N), ("dF", 3 * N))}
+    plane = torch.zeros(1, dtype=torch.uint8, device=dev)
+    sid = torch.ones(1, dtype=torch.int32, device=dev)
+    args = [buf["cr"].data_ptr(), buf["cw"].data_ptr(), buf["ren"].data_ptr(), plane.data_ptr(), sid.data_ptr(), ne,
+            qpp]
+    # an interior domain (periodic = 0) without its dG / dH outputs
+    rc = fn(*args, 0, 1.0, buf["G"].data_ptr(), buf["H"].data_ptr(), None, None, buf["dF"].data_ptr(), None)
+    assert rc == -2
+    # a periodic domain without H
+    rc = fn(*args, 1, 1.0, buf["G"].data_ptr(), None, None, None, buf["dF"].data_ptr(), None)
     assert rc == -2
