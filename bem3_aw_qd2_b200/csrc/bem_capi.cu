@@ -92,6 +92,17 @@ struct bemgpu_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
   double st_corr[BEMGPU_MAXDOM + 1] = {};
+  // Free-space (interior) domains: their matrices depend on the mesh, the
+  // media and the frequency only, not on the in-plane Bloch wave vector or the
+  // incident field.  int_data is what defines them for the loaded problem;
+  // int_valid: G, H, dG, dH, dF of domains >= 1 hold that problem's matrices;
+  // int_factored[d]: domain d's dpv factors are those of these matrices in the
+  // current precision; int_reuse: this load found the same data, so assembly
+  // and dpv factorisation of the interior domains are skipped.
+  std::vector<unsigned char> int_data;
+  bool int_valid = false, int_reuse = false;
+  bool int_factored[BEMGPU_MAXDOM] = {};
+  long long int_reused_loads = 0;
 };
 
 static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
@@ -153,6 +164,9 @@ static void free_problem(bemgpu_ctx *c, bool release) {
     dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
     dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
     c->cap.clear();
+    c->int_valid = false;  // the interior matrices went with the buffers
+    c->int_data.clear();
+    for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
   }
   for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->cn[d] = 0;
   c->factored = false;
@@ -336,6 +350,32 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   for (int e = 0; e < pr->Ne; ++e)
     if (pr->npe[e] != 4 && pr->npe[e] != 3) { snprintf(c->err, sizeof(c->err), "element %d: %d nodes (3 or 4 expected)", e + 1, pr->npe[e]); return -2; }
   if (ensure_constants(c, pr->xl, pr->wl, pr->xh, pr->wh) != 0) return -1;
+  {
+    // what the interior domains' matrices depend on: the element tables, the
+    // domain lists and the interior wave numbers (quadrature rules are fixed)
+    std::vector<unsigned char> idata;
+    auto put = [&idata](const void *p, size_t bytes) {
+      const unsigned char *b = (const unsigned char *)p;
+      idata.insert(idata.end(), b, b + bytes);
+    };
+    const size_t ne = pr->Ne;
+    int tot = 0;
+    for (int d = 0; d <= pr->MN; ++d) tot += pr->dom_ne[d];
+    put(&pr->Ne, sizeof(int)); put(&pr->MN, sizeof(int));
+    put(pr->dom_ne, sizeof(int) * (pr->MN + 1)); put(pr->sid, sizeof(int) * (size_t)tot);
+    put(pr->cr, sizeof(double) * 12 * ne); put(pr->cw, sizeof(double) * 9 * ne);
+    put(pr->ren, sizeof(double) * 12 * ne); put(pr->wen, sizeof(double) * 12 * ne);
+    put(pr->npe, sizeof(int) * ne); put(pr->plane, ne);
+    put(pr->k0 + 1, sizeof(double) * pr->MN);
+    c->int_reuse = pr->MN >= 1 && c->int_valid && idata == c->int_data;
+    if (!c->int_reuse) {
+      c->int_valid = false;
+      for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
+      c->int_data.swap(idata);
+    } else {
+      ++c->int_reused_loads;
+    }
+  }
   c->Ne = pr->Ne; c->NN = pr->NN; c->MN = pr->MN; c->n = 2 * pr->NN;
   bem_qp_prepare(pr->qp, &c->qp);
   CK(falloc(c, &c->wtab, BEM_WT_SIZE), "w table");
@@ -572,10 +612,17 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
     CK(cudaEventRecord(c->ev_fork, c->stream), "assembly fork");
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "assembly fork");
   }
+  // interior matrices of the same mesh, media and frequency are kept (int_reuse)
+  const bool skip_interior = c->int_reuse && c->int_valid;
   for (int d = 0; d <= c->MN; ++d) {
+    cudaEvent_t *ev = c->prof && d < 2 ? c->ev + 6 * d : nullptr;
+    if (d > 0 && skip_interior) {
+      if (ev)
+        for (int i = 0; i < 6; ++i) CK(cudaEventRecord(ev[i], c->side), "phase events");
+      continue;
+    }
     bem_dom_dev D = dom_view(c, d);
     const int periodic = d == 0;
-    cudaEvent_t *ev = c->prof && d < 2 ? c->ev + 6 * d : nullptr;
     if (bem_launch_assemble(&D, &c->qp, periodic, d == 0, c->k0[d], d == 0 ? &c->scr : &c->scr1, c->G[d], c->H[d],
                             c->dG[d], c->dH[d], c->dF[d], d == 0 ? c->stream : c->side, ev) != 0)
       return fail(c, "assembly launch", cudaGetLastError());
@@ -584,6 +631,7 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
     CK(cudaEventRecord(c->ev_join, c->side), "assembly join");
     CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0), "assembly join");
   }
+  c->int_valid = c->MN >= 1;
   return 0;
 }
 
@@ -628,7 +676,7 @@ static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const cha
   c->fac_fp64[slot] = false;
   if (c->precision == 0) return dense_factor_fp64(c, slot, M, n, what, lane);
   if (!c->mx_ready[slot]) {
-    if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) { snprintf(c->err, sizeof(c->err), "%s: cuBLAS set-up", what); return -1; }
+    if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) { snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err); return -1; }
     c->mx_ready[slot] = true;
   }
   c->mxs[slot].mode = c->precision;
@@ -661,6 +709,7 @@ static int check_side_factors(bemgpu_ctx *c) {
       const int r = dense_factor_fp64(c, slot, c->dom_tri[d] ? c->Gc[d] : c->G[d], c->cn[d], "dpv LU");
       if (r) return r;
     }
+    if (d > 0) c->int_factored[d] = true;
   }
   return 0;
 }
@@ -699,6 +748,7 @@ extern "C" int bemgpu_set_precision(bemgpu_ctx *c, int mode) {
   if (mode < 0 || mode > BEM_MIXED_BF16) { snprintf(c->err, sizeof(c->err), "precision mode %d (0..4)", mode); return -2; }
   c->precision = mode;
   c->factored = false;  // factors of the other precision are not reused
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
   return 0;
 }
 
@@ -771,7 +821,7 @@ static int ensure_saves(bemgpu_ctx *c) {
   for (int slot = 0; c->precision != 0 && slot <= c->MN + 1; ++slot)
     if (!c->mx_ready[slot]) {
       if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) {
-        snprintf(c->err, sizeof(c->err), "cuBLAS set-up failed");
+        snprintf(c->err, sizeof(c->err), "mixed-precision set-up: %s", c->mxs[slot].err);
         return -1;
       }
       c->mx_ready[slot] = true;
@@ -795,6 +845,8 @@ extern "C" int bemgpu_solve(bemgpu_ctx *c) {
     for (int d = 0; d <= c->MN; ++d) {
       const int64_t Nd = 4 * (int64_t)c->dom_ne[d];
       if (Nd == 0) continue;
+      if (d > 0 && c->int_reuse && c->int_factored[d]) continue;  // factors of the same interior matrices held
+      c->int_factored[d] = false;
       double *M = c->G[d];
       if (c->dom_tri[d]) {
         if (bem_launch_compress(c->G[d], (int)Nd, c->cinv[d], c->cn[d], c->Gc[d], c->side))
@@ -1202,4 +1254,37 @@ extern "C" int bemgpu_zgesv(int device, int n, int nrhs, const double *A, double
   bem_lu_free(&w);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+extern "C" long long bemgpu_interior_reuses(bemgpu_ctx *c) { return c ? c->int_reused_loads : -1; }
+
+extern "C" cudaError_t bem_launch_transform(int ne, const double *rv, double th, const double *tv, double *cr,
+                                            double *cw, double *ren, double *wen, double *Pi, double *dPi,
+                                            double *p_inc, double *v_inc, const double *pw_d, const double *k2,
+                                            cudaStream_t st);
+
+extern "C" int bemgpu_transform_mesh(bemgpu_ctx *c, const double *rv, double th, const double *tv) {
+  if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
+  CK(bem_launch_transform(c->Ne, rv, th, tv, c->cr, c->cw, c->ren, c->wen, c->Pi, c->dPi, c->p_inc, c->v_inc,
+                          c->pw_d, c->k2.data(), c->stream),
+     "mesh transform");
+  // the z extent of the moved mesh sets the spectral table's window
+  std::vector<double> cr(12 * (size_t)c->Ne);
+  CK(cudaMemcpyAsync(cr.data(), c->cr, cr.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "mesh transform");
+  CK(cudaStreamSynchronize(c->stream), "mesh transform");
+  double zlo = 0.0, zhi = 0.0;
+  for (int e = 0; e < c->Ne; ++e) {
+    const double *z = cr.data() + (size_t)e * 12 + 8;
+    const double hw = fabs(z[1]) + fabs(z[2]) + fabs(z[3]);
+    if (e == 0 || z[0] - hw < zlo) zlo = z[0] - hw;
+    if (e == 0 || z[0] + hw > zhi) zhi = z[0] + hw;
+  }
+  c->zspan = zhi - zlo;
+  if (build_stab(c)) return -1;
+  // every matrix and factor belongs to the old placement
+  c->factored = false;
+  c->int_valid = false;
+  c->int_data.clear();
+  for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
+  return 0;
 }

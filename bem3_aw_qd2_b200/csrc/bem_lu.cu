@@ -56,6 +56,20 @@
 #define U_COUNT (4 * LU_W * LU_W)
 
 // ---------------------------------------------------------------- complex helpers
+// complex double (double2) and complex float (float2): the same code in both
+// precisions
+template <class C2> struct cx;
+template <> struct cx<double2> {
+  using R = double;
+  static __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+};
+template <> struct cx<float2> {
+  using R = float;
+  static __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+};
+template <class C2> __device__ __forceinline__ C2 czero() { return cx<C2>::mk(0, 0); }
+template <class C2> __device__ __forceinline__ C2 cone() { return cx<C2>::mk(1, 0); }
+template <class C2> __device__ __forceinline__ C2 cneg(C2 a) { return cx<C2>::mk(-a.x, -a.y); }
 __device__ __forceinline__ double2 cz() { return make_double2(0.0, 0.0); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -73,17 +87,33 @@ __device__ __forceinline__ double2 crcp(double2 a) {
   return make_double2(a.x * d, -a.y * d);
 }
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 cfms(float2 a, float2 b, float2 c) {
+  return make_float2(fmaf(-a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(-a.x, b.y, fmaf(-a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 crcp(float2 a) {
+  const float d = 1.0f / fmaf(a.x, a.x, a.y * a.y);
+  return make_float2(a.x * d, -a.y * d);
+}
+__device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y); }
 
 // ---------------------------------------------------------------- partial pivoting in one CTA
+template <class C2>
 struct gepp_sh {
-  double wv[2][LU_TH / 32];
+  typename cx<C2>::R wv[2][LU_TH / 32];
   int wi[2][LU_TH / 32];
-  double2 prow[2][LU_W], krow[2][LU_W];
+  C2 prow[2][LU_W], krow[2][LU_W];
   int pid[2], kid[2];
 };
 
-__device__ __forceinline__ void rot1(double2 (&v)[LU_W]) {
-  const double2 f = v[0];
+template <class C2>
+__device__ __forceinline__ void rot1(C2 (&v)[LU_W]) {
+  const C2 f = v[0];
 #pragma unroll
   for (int c = 0; c < LU_W - 1; ++c) v[c] = v[c + 1];
   v[LU_W - 1] = f;
@@ -97,30 +127,32 @@ __device__ __forceinline__ void rot1(double2 (&v)[LU_W]) {
 // step j its register 0 holds column j, registers 1 .. 31 - j the columns
 // still to update and the rest the finished ones, so that every register
 // index is a compile-time constant inside one short loop body.
-__device__ void gepp(double2 (&v)[LU_W], int &id, int rr, int w, gepp_sh &sh, unsigned *status) {
+template <class C2>
+__device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, unsigned *status) {
+  using R = typename cx<C2>::R;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int steps = min(w, rr);
   for (int j = 0; j < steps; ++j) {
     const int b = j & 1;
-    double val = (t >= j && t < rr) ? cabs1(v[0]) : -1.0;
+    R val = (t >= j && t < rr) ? cabs1(v[0]) : (R)-1;
     int bi = t;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_down_sync(FULL, val, o);
+      const R ov = __shfl_down_sync(FULL, val, o);
       const int oi = __shfl_down_sync(FULL, bi, o);
       if (ov > val || (ov == val && oi < bi)) { val = ov; bi = oi; }
     }
     if (lane == 0) { sh.wv[b][wid] = val; sh.wi[b][wid] = bi; }
     __syncthreads();
-    double best = sh.wv[b][0];
+    R best = sh.wv[b][0];
     int p = sh.wi[b][0];
 #pragma unroll
     for (int q = 1; q < LU_TH / 32; ++q) {
-      const double ov = sh.wv[b][q];
+      const R ov = sh.wv[b][q];
       const int oi = sh.wi[b][q];
       if (ov > best || (ov == best && oi < p)) { best = ov; p = oi; }
     }
-    if (!(best > 0.0)) {
+    if (!(best > (R)0)) {
       if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
       p = j;
     }
@@ -145,7 +177,7 @@ __device__ void gepp(double2 (&v)[LU_W], int &id, int rr, int w, gepp_sh &sh, un
       id = sh.kid[b];
     }
     if (t > j && t < rr) {
-      const double2 l = cmul(v[0], crcp(sh.prow[b][0]));
+      const C2 l = cmul(v[0], crcp(sh.prow[b][0]));
       v[0] = l;
 #pragma unroll
       for (int c = 1; c < LU_W; ++c)
@@ -156,10 +188,11 @@ __device__ void gepp(double2 (&v)[LU_W], int &id, int rr, int w, gepp_sh &sh, un
   for (int s = steps; s < LU_W; ++s) rot1(v);  // LU_W rotations in all: columns back in order
 }
 
-__device__ __forceinline__ void load_row(double2 (&v)[LU_W], const double2 *A, long lda, int row, int k, int w) {
-  const double2 *p = A + (size_t)(row < 0 ? 0 : row) * lda + k;
+template <class C2>
+__device__ __forceinline__ void load_row(C2 (&v)[LU_W], const C2 *A, long lda, int row, int k, int w) {
+  const C2 *p = A + (size_t)(row < 0 ? 0 : row) * lda + k;
 #pragma unroll
-  for (int c = 0; c < LU_W; ++c) v[c] = (row >= 0 && c < w) ? p[c] : cz();
+  for (int c = 0; c < LU_W; ++c) v[c] = (row >= 0 && c < w) ? p[c] : czero<C2>();
 }
 
 __device__ __forceinline__ unsigned cluster_rank() {
@@ -174,22 +207,24 @@ __device__ __forceinline__ void cluster_sync_all() {
 }
 
 // ---------------------------------------------------------------- panel
+template <class C2>
 struct panel_sh {
-  gepp_sh g;
-  double2 lu[LU_W][LU_W + 1];
-  double2 ui[LU_W][LU_W + 1];
-  double2 li[LU_W][LU_W + 1];
+  gepp_sh<C2> g;
+  C2 lu[LU_W][LU_W + 1];
+  C2 ui[LU_W][LU_W + 1];
+  C2 li[LU_W][LU_W + 1];
   int sel[LU_W], la[LU_W], lb[LU_W];
 };
 
+template <class C2>
 __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
-    k_lu_panel(double2 *A, long lda, int n, int k, int *pv, double2 *u, unsigned *status) {
+    k_lu_panel(C2 *A, long lda, int n, int k, int *pv, C2 *u, unsigned *status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  panel_sh &S = *reinterpret_cast<panel_sh *>(smem_raw);
+  panel_sh<C2> &S = *reinterpret_cast<panel_sh<C2> *>(smem_raw);
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int crank = (int)cluster_rank();
   const int w = min(LU_W, n - k), m = n - k;
-  double2 v[LU_W];
+  C2 v[LU_W];
   int id = -1;
   if (m > LU_TH) {
     // leaves: each CTA a contiguous slice of the panel's rows, in rounds of
@@ -237,7 +272,7 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
   if (t < LU_W) {
 #pragma unroll
     for (int c = 0; c < LU_W; ++c) {
-      const double2 x = (t < w) ? v[c] : cz();
+      const C2 x = (t < w) ? v[c] : czero<C2>();
       S.lu[t][c] = x;
       u[U_LU + t * LU_W + c] = x;
     }
@@ -248,14 +283,13 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
   if (wid == 0) {
     // U11^-1, column j = lane: x_j = 1 / u_jj, x_i = -(sum_{i<l<=j} u_il x_l) / u_ii
     const int j = lane;
-    for (int i = 0; i < LU_W; ++i) S.ui[i][j] = cz();
+    for (int i = 0; i < LU_W; ++i) S.ui[i][j] = czero<C2>();
     if (j < w) {
       S.ui[j][j] = crcp(S.lu[j][j]);
       for (int i = j - 1; i >= 0; --i) {
-        double2 s = cz();
+        C2 s = czero<C2>();
         for (int l = i + 1; l <= j; ++l) s = cfma(S.lu[i][l], S.ui[l][j], s);
-        const double2 x = cmul(s, crcp(S.lu[i][i]));
-        S.ui[i][j] = make_double2(-x.x, -x.y);
+        S.ui[i][j] = cneg(cmul(s, crcp(S.lu[i][i])));
       }
     }
     __syncwarp();
@@ -263,13 +297,13 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
   } else if (wid == 1) {
     // L11^-1 (unit lower), column j = lane: x_j = 1, x_i = -sum_{j<=l<i} l_il x_l
     const int j = lane;
-    for (int i = 0; i < LU_W; ++i) S.li[i][j] = cz();
+    for (int i = 0; i < LU_W; ++i) S.li[i][j] = czero<C2>();
     if (j < w) {
-      S.li[j][j] = make_double2(1.0, 0.0);
+      S.li[j][j] = cone<C2>();
       for (int i = j + 1; i < w; ++i) {
-        double2 s = cz();
+        C2 s = czero<C2>();
         for (int l = j; l < i; ++l) s = cfma(S.lu[i][l], S.li[l][j], s);
-        S.li[i][j] = make_double2(-s.x, -s.y);
+        S.li[i][j] = cneg(s);
       }
     }
     __syncwarp();
@@ -296,7 +330,7 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
     if (lane < cnt) { perm[1 + 2 * (w + lane)] = S.la[lane]; perm[2 + 2 * (w + lane)] = S.lb[lane]; }
     // the displaced rows' panel values, before anything overwrites them
     for (int r = 0; r < cnt; ++r)
-      u[U_STAGE + r * LU_W + lane] = lane < w ? A[(size_t)S.lb[r] * lda + k + lane] : cz();
+      u[U_STAGE + r * LU_W + lane] = lane < w ? A[(size_t)S.lb[r] * lda + k + lane] : czero<C2>();
   }
 }
 
@@ -305,10 +339,11 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
 #define AP_ROWS 32   // rows of an L21 block (4 threads per row)
 #define AP_COLS 16   // columns of a row-move block
 
-__global__ void __launch_bounds__(AP_TH) k_lu_apply(double2 *A, long lda, int n, int k, const int *pv,
-                                                    const double2 *u, int *rowmap, unsigned *status) {
-  __shared__ double2 sm[LU_W][LU_W + 1];
-  __shared__ double2 srow[LU_MAXP][AP_COLS + 1];
+template <class C2>
+__global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int k, const int *pv, const C2 *u,
+                                                    int *rowmap, unsigned *status) {
+  __shared__ C2 sm[LU_W][LU_W + 1];
+  __shared__ C2 srow[LU_MAXP][AP_COLS + 1];
   __shared__ int sdst[LU_MAXP], ssrc[LU_MAXP];
   const int t = threadIdx.x;
   const int w = min(LU_W, n - k);
@@ -337,20 +372,20 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(double2 *A, long lda, int n,
     const int row = r0 + b * AP_ROWS + (t >> 2), part = t & 3;
     bool live = row < n;
     for (int e = w; e < nperm && live; ++e) live = sdst[e] != row;
-    double2 x[8];
+    C2 x[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) x[c] = cz();
+    for (int c = 0; c < 8; ++c) x[c] = czero<C2>();
     if (live) {
-      const double2 *a = A + (size_t)row * lda + k;
+      const C2 *a = A + (size_t)row * lda + k;
       for (int l = 0; l < w; ++l) {
-        const double2 al = a[l];
+        const C2 al = a[l];
 #pragma unroll
         for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
       }
     }
     __syncthreads();  // every read of the row before any write to it
     if (live) {
-      double2 *a = A + (size_t)row * lda + k;
+      C2 *a = A + (size_t)row * lda + k;
 #pragma unroll
       for (int c = 0; c < 8; ++c)
         if (part * 8 + c < w) a[part * 8 + c] = x[c];
@@ -370,14 +405,14 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(double2 *A, long lda, int n,
     __syncthreads();  // sdst / ssrc
     for (int e = t; e < nperm * AP_COLS; e += AP_TH) {
       const int pr = e / AP_COLS, cc = e % AP_COLS;
-      srow[pr][cc] = cc < nc ? A[(size_t)ssrc[pr] * lda + c0 + cc] : cz();
+      srow[pr][cc] = cc < nc ? A[(size_t)ssrc[pr] * lda + c0 + cc] : czero<C2>();
     }
     __syncthreads();
     const int cc = t % AP_COLS, grp = t / AP_COLS;  // 8 groups of 16 columns
     if (cc < nc) {
       if (right) {
         for (int ii = grp; ii < w; ii += AP_TH / AP_COLS) {
-          double2 s = cz();
+          C2 s = czero<C2>();
           for (int l = 0; l <= ii; ++l) s = cfma(sm[ii][l], srow[l][cc], s);
           A[(size_t)(k + ii) * lda + c0 + cc] = s;
         }
@@ -399,15 +434,15 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(double2 *A, long lda, int n,
   {
     const int r = t >> 2, part = t & 3, e = w + r;
     if (e < nperm) {
-      double2 x[8];
+      C2 x[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) x[c] = cz();
+      for (int c = 0; c < 8; ++c) x[c] = czero<C2>();
       for (int l = 0; l < w; ++l) {
-        const double2 al = __ldcg(u + U_STAGE + r * LU_W + l);
+        const C2 al = __ldcg(u + U_STAGE + r * LU_W + l);
 #pragma unroll
         for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
       }
-      double2 *a = A + (size_t)sdst[e] * lda + k;
+      C2 *a = A + (size_t)sdst[e] * lda + k;
 #pragma unroll
       for (int c = 0; c < 8; ++c)
         if (part * 8 + c < w) a[part * 8 + c] = x[c];
@@ -505,6 +540,87 @@ __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, in
     }
 }
 
+// complex FP32: the same update on the CUDA cores, 64 x 64 tiles, 4 x 4
+// outputs per thread (rows ty*4 + i, columns tx + 16 j: conflict-free shared
+// loads and 128-byte runs of C per 16 threads)
+#define UF_TH 256
+__global__ void __launch_bounds__(UF_TH) k_lu_update_c32(float2 *A, long lda, int n, int k) {
+  __shared__ float2 As[UP_BM][LU_W + 1];
+  __shared__ float2 Bs[LU_W][UP_BN + 1];
+  const int t = threadIdx.x;
+  const int w = min(LU_W, n - k);
+  const int r0 = k + w;
+  const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
+  for (int e = t; e < UP_BM * LU_W; e += UF_TH) {
+    const int r = e / LU_W, c = e % LU_W;
+    As[r][c] = (rb + r < n && c < w) ? A[(size_t)(rb + r) * lda + k + c] : make_float2(0.f, 0.f);
+  }
+  for (int e = t; e < LU_W * UP_BN; e += UF_TH) {
+    const int r = e / UP_BN, c = e % UP_BN;
+    Bs[r][c] = (r < w && cb + c < n) ? A[(size_t)(k + r) * lda + cb + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int ty = t >> 4, tx = t & 15;
+  float2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int row = rb + ty * 4 + i, col = cb + tx + 16 * j;
+      acc[i][j] = (row < n && col < n) ? A[(size_t)row * lda + col] : make_float2(0.f, 0.f);
+    }
+  for (int kk = 0; kk < w; ++kk) {
+    float2 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][kk];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = cfms(a[i], b[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int row = rb + ty * 4 + i, col = cb + tx + 16 * j;
+      if (row < n && col < n) A[(size_t)row * lda + col] = acc[i][j];
+    }
+}
+
+// R = B - A X in FP64 (refinement residual): A row-major n x n, X, B, R
+// column-major n x NR; one warp per row
+template <int NR>
+__global__ void __launch_bounds__(256) k_resid_z(const double2 *A, int n, const double2 *X, const double2 *B,
+                                                 double2 *R) {
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= n) return;
+  double2 acc[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) acc[q] = cz();
+  const double2 *a = A + (size_t)row * n;
+  for (int col = lane; col < n; col += 32) {
+    const double2 av = a[col];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = cfma(av, X[(size_t)q * n + col], acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < NR; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      acc[q].x += __shfl_down_sync(FULL, acc[q].x, o);
+      acc[q].y += __shfl_down_sync(FULL, acc[q].y, o);
+    }
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+      const double2 b = B[(size_t)q * n + row];
+      R[(size_t)q * n + row] = make_double2(b.x - acc[q].x, b.y - acc[q].y);
+    }
+}
+
 __global__ void k_lu_iota(int *rowmap, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rowmap[i] = i;
 }
@@ -536,12 +652,11 @@ __device__ __forceinline__ void wait_flag(const unsigned *f, unsigned *status) {
 // lower = 1: out = L^-1 (P in), in read through rowmap (unit lower L);
 // lower = 0: out = U^-1 in.  in / out are n x NR column-major; block b of out
 // is published through flags[b] once written.
-template <int NR>
-__global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, int n, const int *rowmap,
-                                                   const double2 *in, double2 *out, unsigned *flags, int lower,
-                                                   unsigned *status) {
-  __shared__ double2 sd[32][33];
-  __shared__ double2 sacc[4][32][NR];
+template <class C2, int NR>
+__global__ void __launch_bounds__(TS_TH) k_lu_trsv(const C2 *LU, long lda, int n, const int *rowmap, const C2 *in,
+                                                   C2 *out, unsigned *flags, int lower, unsigned *status) {
+  __shared__ C2 sd[32][33];
+  __shared__ C2 sacc[4][32][NR];
   const int nb = (n + 31) / 32;
   const int t = threadIdx.x, r = t & 31, s = t >> 5;
   for (int it = blockIdx.x; it < nb; it += gridDim.x) {
@@ -549,12 +664,12 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, 
     const int r0 = b * 32, rows = min(32, n - r0);
     for (int e = t; e < 32 * 32; e += TS_TH) {
       const int i = e >> 5, j = e & 31;
-      sd[i][j] = (i < rows && j < rows) ? LU[(size_t)(r0 + i) * lda + r0 + j] : cz();
+      sd[i][j] = (i < rows && j < rows) ? LU[(size_t)(r0 + i) * lda + r0 + j] : czero<C2>();
     }
     const int row = r0 + r;
-    double2 acc[NR];
+    C2 acc[NR];
 #pragma unroll
-    for (int q = 0; q < NR; ++q) acc[q] = cz();
+    for (int q = 0; q < NR; ++q) acc[q] = czero<C2>();
     if (s == 0 && r < rows) {
       const int src = lower ? rowmap[row] : row;
 #pragma unroll
@@ -565,12 +680,12 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, 
       wait_flag(flags + jb, status);
       const int c0 = jb * 32 + s * 8;
       if (r < rows) {
-        const double2 *a = LU + (size_t)row * lda;
+        const C2 *a = LU + (size_t)row * lda;
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
           const int col = c0 + cc;
           if (col < n) {
-            const double2 av = a[col];
+            const C2 av = a[col];
 #pragma unroll
             for (int q = 0; q < NR; ++q) acc[q] = cfms(av, __ldcg(out + (size_t)q * n + col), acc[q]);
           }
@@ -583,28 +698,28 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, 
     if (s == 0) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
-        double2 x = sacc[0][r][q];
-        for (int ss = 1; ss < 4; ++ss) x = make_double2(x.x + sacc[ss][r][q].x, x.y + sacc[ss][r][q].y);
+        C2 x = sacc[0][r][q];
+        for (int ss = 1; ss < 4; ++ss) x = cx<C2>::mk(x.x + sacc[ss][r][q].x, x.y + sacc[ss][r][q].y);
         acc[q] = x;
       }
       if (lower) {
         for (int i = 0; i < rows; ++i) {
 #pragma unroll
           for (int q = 0; q < NR; ++q) {
-            const double2 yi = make_double2(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
+            const C2 yi = cx<C2>::mk(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
             if (r > i && r < rows) acc[q] = cfms(sd[r][i], yi, acc[q]);
           }
         }
       } else {
         for (int i = rows - 1; i >= 0; --i) {
           if (r == i) {
-            const double2 d = crcp(sd[i][i]);
+            const C2 d = crcp(sd[i][i]);
 #pragma unroll
             for (int q = 0; q < NR; ++q) acc[q] = cmul(acc[q], d);
           }
 #pragma unroll
           for (int q = 0; q < NR; ++q) {
-            const double2 xi = make_double2(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
+            const C2 xi = cx<C2>::mk(__shfl_sync(FULL, acc[q].x, i), __shfl_sync(FULL, acc[q].y, i));
             if (r < i) acc[q] = cfms(sd[r][i], xi, acc[q]);
           }
         }
@@ -632,10 +747,15 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const double2 *LU, long lda, 
 
 extern "C" int bem_lu_init(bem_lu *w, int device) {
   CKL(cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-  CKL(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(panel_sh)), "panel smem");
+  CKL(cudaFuncSetAttribute(k_lu_panel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(panel_sh<double2>)),
+      "panel smem");
+  CKL(cudaFuncSetAttribute(k_lu_panel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(panel_sh<float2>)),
+      "panel smem");
   CKL(cudaFuncSetAttribute(k_lu_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UP_SMEM), "update smem");
   int per_sm = 0;
-  CKL(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_trsv<4>, TS_TH, 0), "solve occupancy");
+  CKL(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_trsv<double2, 4>, TS_TH, 0), "solve occupancy");
   w->coop_blocks = per_sm * w->sms;
   if (w->coop_blocks <= 0) {
     snprintf(w->err, sizeof(w->err), "triangular solve: no resident block");
@@ -670,30 +790,36 @@ static int grow_bytes(bem_lu *w, void **p, size_t *cap, size_t bytes, const char
   return 0;
 }
 
+static void launch_update(double2 *A, int n, int k, int tiles, cudaStream_t st) {
+  k_lu_update<<<dim3(tiles, tiles), UP_TH, UP_SMEM, st>>>(A, n, n, k);
+}
+static void launch_update(float2 *A, int n, int k, int tiles, cudaStream_t st) {
+  k_lu_update_c32<<<dim3(tiles, tiles), UF_TH, 0, st>>>(A, n, n, k);
+}
+
 // the launches of one factorisation, in order (captured into the graph)
-static int factor_launches(bem_lu *w, double2 *A, int n, cudaStream_t st) {
+template <class C2>
+static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
   k_lu_iota<<<(n + 255) / 256, 256, 0, st>>>(w->rowmap, n);
   for (int k = 0; k < n; k += LU_W) {
     const int wd = n - k < LU_W ? n - k : LU_W;
     const int r0 = k + wd;
-    k_lu_panel<<<LU_CL, LU_TH, sizeof(panel_sh), st>>>(A, n, n, k, w->piv, (double2 *)w->u11, w->status);
+    k_lu_panel<C2><<<LU_CL, LU_TH, sizeof(panel_sh<C2>), st>>>(A, n, n, k, w->piv, (C2 *)w->u11, w->status);
     const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
     const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
-    k_lu_apply<<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, w->piv, (const double2 *)w->u11, w->rowmap, w->status);
-    if (r0 < n) {
-      const int tiles = (n - r0 + UP_BM - 1) / UP_BM;
-      k_lu_update<<<dim3(tiles, tiles), UP_TH, UP_SMEM, st>>>(A, n, n, k);
-    }
+    k_lu_apply<C2><<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, w->piv, (const C2 *)w->u11, w->rowmap, w->status);
+    if (r0 < n) launch_update(A, n, k, (n - r0 + UP_BM - 1) / UP_BM, st);
   }
   CKL(cudaGetLastError(), "LU launch");
   return 0;
 }
 
-extern "C" int bem_lu_factor_z(bem_lu *w, double *Ad, int n, cudaStream_t st) {
+template <class C2>
+static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
   if (n <= 0) return 0;
-  double2 *A = (double2 *)Ad;
+  C2 *A = (C2 *)Av;
   if (grow_bytes(w, (void **)&w->rowmap, &w->rowmap_cap, (size_t)n * sizeof(int), "row map")) return -1;
-  if (!(w->gexec && w->g_A == Ad && w->g_n == n)) {
+  if (!(w->gexec && w->g_A == Av && w->g_n == n)) {
     if (w->gexec) cudaGraphExecDestroy(w->gexec);
     if (w->graph) cudaGraphDestroy(w->graph);
     w->gexec = nullptr;
@@ -709,16 +835,19 @@ extern "C" int bem_lu_factor_z(bem_lu *w, double *Ad, int n, cudaStream_t st) {
     CKL(ce, "LU capture");
     w->graph = g;
     CKL(cudaGraphInstantiate(&w->gexec, g, 0), "LU graph");
-    w->g_A = Ad;
+    w->g_A = Av;
     w->g_n = n;
   }
   CKL(cudaGraphLaunch(w->gexec, st), "LU graph launch");
   return 0;
 }
 
-template <int NR>
-static int launch_trsv(bem_lu *w, const double2 *LU, int n, const double2 *in, double2 *out, unsigned *flags,
-                       int lower, cudaStream_t st) {
+extern "C" int bem_lu_factor_z(bem_lu *w, double *A, int n, cudaStream_t st) { return lu_factor<double2>(w, A, n, st); }
+extern "C" int bem_lu_factor_c(bem_lu *w, float *A, int n, cudaStream_t st) { return lu_factor<float2>(w, A, n, st); }
+
+template <class C2, int NR>
+static int launch_trsv(bem_lu *w, const C2 *LU, int n, const C2 *in, C2 *out, unsigned *flags, int lower,
+                       cudaStream_t st) {
   const int nb = (n + 31) / 32;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb < w->coop_blocks ? nb : w->coop_blocks);
@@ -729,13 +858,14 @@ static int launch_trsv(bem_lu *w, const double2 *LU, int n, const double2 *in, d
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  CKL(cudaLaunchKernelEx(&cfg, k_lu_trsv<NR>, LU, (long)n, n, (const int *)w->rowmap, in, out, flags, lower,
+  CKL(cudaLaunchKernelEx(&cfg, k_lu_trsv<C2, NR>, LU, (long)n, n, (const int *)w->rowmap, in, out, flags, lower,
                          w->status),
       "triangular solve");
   return 0;
 }
 
-extern "C" int bem_lu_solve_z(bem_lu *w, const double *LUd, int n, int nrhs, double *Bd, cudaStream_t st) {
+template <class C2>
+static int lu_solve(bem_lu *w, const void *LUv, int n, int nrhs, void *Bv, cudaStream_t st) {
   if (n <= 0) return 0;
   if (nrhs < 1 || nrhs > 4) {
     snprintf(w->err, sizeof(w->err), "LU solve: %d right-hand sides (1..4)", nrhs);
@@ -743,19 +873,41 @@ extern "C" int bem_lu_solve_z(bem_lu *w, const double *LUd, int n, int nrhs, dou
   }
   const int nb = (n + 31) / 32;
   if (grow_bytes(w, (void **)&w->flags, &w->flags_cap, 2 * (size_t)nb * sizeof(unsigned), "solve flags") ||
-      grow_bytes(w, &w->y, &w->y_cap, (size_t)n * nrhs * sizeof(double2), "solve scratch"))
+      grow_bytes(w, &w->y, &w->y_cap, (size_t)n * nrhs * sizeof(C2), "solve scratch"))
     return -1;
-  const double2 *LU = (const double2 *)LUd;
-  double2 *B = (double2 *)Bd, *Y = (double2 *)w->y;
+  const C2 *LU = (const C2 *)LUv;
+  C2 *B = (C2 *)Bv, *Y = (C2 *)w->y;
   CKL(cudaMemsetAsync(w->flags, 0, 2 * (size_t)nb * sizeof(unsigned), st), "solve flags");
   int rc = 0;
   switch (nrhs) {
-    case 1: rc = launch_trsv<1>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<1>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    case 2: rc = launch_trsv<2>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<2>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    case 3: rc = launch_trsv<3>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<3>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    default: rc = launch_trsv<4>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<4>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 1: rc = launch_trsv<C2, 1>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 1>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 2: rc = launch_trsv<C2, 2>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 2>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 3: rc = launch_trsv<C2, 3>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 3>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    default: rc = launch_trsv<C2, 4>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 4>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
   }
   return rc ? -1 : 0;
+}
+
+extern "C" int bem_lu_solve_z(bem_lu *w, const double *LU, int n, int nrhs, double *B, cudaStream_t st) {
+  return lu_solve<double2>(w, LU, n, nrhs, B, st);
+}
+extern "C" int bem_lu_solve_c(bem_lu *w, const float *LU, int n, int nrhs, float *B, cudaStream_t st) {
+  return lu_solve<float2>(w, LU, n, nrhs, B, st);
+}
+
+extern "C" int bem_lu_resid_z(const double *A, int n, int nrhs, const double *X, const double *B, double *R,
+                              cudaStream_t st) {
+  const int blocks = (n + 7) / 8;
+  const double2 *a = (const double2 *)A, *x = (const double2 *)X, *b = (const double2 *)B;
+  double2 *r = (double2 *)R;
+  switch (nrhs) {
+    case 1: k_resid_z<1><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
+    case 2: k_resid_z<2><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
+    case 3: k_resid_z<3><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
+    case 4: k_resid_z<4><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
+    default: return -1;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" unsigned bem_lu_status(bem_lu *w, cudaStream_t st) {

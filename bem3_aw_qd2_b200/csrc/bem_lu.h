@@ -40,6 +40,13 @@ int bem_lu_factor_z(bem_lu *w, double *A, int n, cudaStream_t st);
 // Solve A X = B with the factors of bem_lu_factor_z; B is n x nrhs complex,
 // column-major (ld n), overwritten by X; nrhs <= 4.
 int bem_lu_solve_z(bem_lu *w, const double *LU, int n, int nrhs, double *B, cudaStream_t st);
+// The same in complex FP32 (interleaved re/im floats): the factors of the
+// mixed-precision solves.
+int bem_lu_factor_c(bem_lu *w, float *A, int n, cudaStream_t st);
+int bem_lu_solve_c(bem_lu *w, const float *LU, int n, int nrhs, float *B, cudaStream_t st);
+// R = B - A X in FP64 (A row-major n x n, X, B, R column-major n x nrhs,
+// nrhs <= 4): the refinement residual.
+int bem_lu_resid_z(const double *A, int n, int nrhs, const double *X, const double *B, double *R, cudaStream_t st);
 // Status bits (BEM_LU_ST_*) accumulated since the last call; waits for st.
 unsigned bem_lu_status(bem_lu *w, cudaStream_t st);
 }

@@ -2,12 +2,15 @@
 //
 // Requests (a bemgpu_problem: mesh, media, lattice, frequency, incidence) are
 // queued on submit and admitted to solver slots as slots and device memory
-// free up.  Each slot owns a context (its own CUDA stream and cuSOLVER /
-// cuBLAS handles) and a host worker thread, so the assemblies and solves of
+// free up.  Each slot owns a context (its own CUDA streams and solver
+// scratch) and a host worker thread, so the assemblies and solves of
 // admitted requests overlap on the device.  A slot keeps its last problem's
 // matrices and factors; a request whose reuse key (mesh, media, lattice,
 // frequency, in-plane Bloch wave vector, precision) matches an idle slot's is
-// routed there and only its right-hand side is solved.  Admission keeps the
+// routed there and only its right-hand side is solved; a request on the same
+// body, media and frequency as a slot's resident problem (another Bloch wave
+// vector) is preferred there, and the context keeps the free-space domains'
+// matrices and dpv factors (bemgpu_interior_reuses).  Admission keeps the
 // sum of the resident problems' device bytes (N^2 16 B per matrix plus
 // workspace, see problem_bytes) within the budget; idle slots' problems are
 // evicted, least recently used first, to make room.  Later requests that fit
@@ -83,16 +86,38 @@ size_t problem_bytes(const bemgpu_problem *p, int precision) {
   return b + (size_t)p->Ne * 512 + (64u << 20);  // tables, workspace of the solvers
 }
 
+// FNV-1a over what the free-space (interior) domains' matrices depend on (the
+// element tables, domain lists and interior wave numbers; the context itself
+// compares the data exactly before it keeps anything)
+unsigned long long interior_key(const bemgpu_problem *p) {
+  unsigned long long h = 1469598103934665603ull;
+  auto put = [&h](const void *src, size_t bytes) {
+    const unsigned char *b = (const unsigned char *)src;
+    for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  };
+  const size_t ne = p->Ne;
+  size_t tot = 0;
+  for (int d = 0; d <= p->MN; ++d) tot += p->dom_ne[d];
+  put(&p->Ne, sizeof(int)); put(&p->MN, sizeof(int));
+  put(p->dom_ne, sizeof(int) * (p->MN + 1)); put(p->sid, sizeof(int) * tot);
+  put(p->cr, sizeof(double) * 12 * ne); put(p->cw, sizeof(double) * 9 * ne);
+  put(p->ren, sizeof(double) * 12 * ne); put(p->wen, sizeof(double) * 12 * ne);
+  put(p->npe, sizeof(int) * ne); put(p->plane, ne);
+  put(p->k0 + 1, sizeof(double) * p->MN);
+  return h;
+}
+
 struct request {
   long long id;
   owned_problem prob;
-  unsigned long long key;
+  unsigned long long key, ikey;
   int precision, force_type;
   double rc[3];
   size_t bytes;
   double t_submit, t_start = 0;
   request(const bemgpu_problem *p, unsigned long long k, int prec, int ft, const double *r, long long i)
-      : id(i), prob(p), key(k), precision(prec), force_type(ft), bytes(problem_bytes(p, prec)), t_submit(now_ms()) {
+      : id(i), prob(p), key(k), ikey(interior_key(p)), precision(prec), force_type(ft), bytes(problem_bytes(p, prec)),
+        t_submit(now_ms()) {
     for (int j = 0; j < 3; ++j) rc[j] = r ? r[j] : 0.0;
   }
 };
@@ -102,6 +127,7 @@ struct slot {
   std::thread th;
   request *cur = nullptr;        // assigned request (owned by the slot while running)
   unsigned long long key = 0;    // reuse key of the resident problem
+  unsigned long long ikey = 0;   // interior key of the resident problem
   int precision = -1;
   bool resident = false;         // a problem (and its factors) is loaded
   bool evict = false;            // free the resident problem before the next request
@@ -151,8 +177,12 @@ static void dispatch_locked(bemgpu_server *s) {
       for (size_t i = 0; i < s->slots.size(); ++i)
         if (!s->slots[i].cur) idle.push_back((int)i);
       if (!idle.empty()) {
-        // replace first: empty slots, then slots whose factors no queued
-        // request wants, least recently used first
+        // replace first: a slot with this request's interior matrices, then
+        // empty slots, then slots whose factors no queued request wants,
+        // least recently used first
+        auto same_interior = [&](const slot &x) {
+          return x.resident && x.ikey == r->ikey && x.precision == r->precision;
+        };
         auto wanted = [&](const slot &x) {
           if (!x.resident) return false;
           for (request *q : s->queue)
@@ -161,6 +191,8 @@ static void dispatch_locked(bemgpu_server *s) {
         };
         std::sort(idle.begin(), idle.end(), [&](int a, int b) {
           const slot &x = s->slots[a], &y = s->slots[b];
+          const bool ix = same_interior(x), iy = same_interior(y);
+          if (ix != iy) return ix;
           if (x.resident != y.resident) return !x.resident;
           const bool wx = wanted(x), wy = wanted(y);
           if (wx != wy) return !wx;
@@ -237,11 +269,15 @@ static void worker(bemgpu_server *s, int idx) {
       if (rc == -2) reuse = false;  // factors no longer held: full solve below
     }
     if (!reuse) {
-      sl.resident = false;
       // the slot's device memory is what admission counted for this problem:
-      // give back the previous problem's buffers instead of reusing them
-      rc = bemgpu_unload(sl.ctx);
-      if (!rc) rc = bemgpu_set_precision(sl.ctx, r->precision);
+      // give back the previous problem's buffers instead of reusing them,
+      // unless the problem is on the same body at the same frequency, whose
+      // buffers have this problem's sizes and whose interior matrices and
+      // factors the context keeps
+      const bool same_interior = sl.resident && sl.ikey == r->ikey && sl.precision == r->precision;
+      sl.resident = false;
+      rc = same_interior ? 0 : bemgpu_unload(sl.ctx);
+      if (!rc && !same_interior) rc = bemgpu_set_precision(sl.ctx, r->precision);
       if (!rc) rc = bemgpu_load(sl.ctx, &r->prob.p);
       if (!rc) rc = bemgpu_run(sl.ctx);
     }
@@ -268,6 +304,7 @@ static void worker(bemgpu_server *s, int idx) {
       } else {
         sl.resident = true;
         sl.key = r->key;
+        sl.ikey = r->ikey;
         sl.precision = r->precision;
         if (reuse) ++s->reused;
       }

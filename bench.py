@@ -97,7 +97,12 @@ def parse():
                          "(for ncu --profile-from-start off)")
     ap.add_argument("--rate", type=float, default=10.0, help="stream workload: mean arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="stream workload: server slots")
-    ap.add_argument("--hbm-gb", type=float, default=64.0, help="stream workload: device-memory budget")
+    ap.add_argument("--hbm-gb", type=float, default=170.0, help="stream: device-memory budget of the server")
+    ap.add_argument("--stream-sizes", default="6,10", help="--workload stream: cube-sphere n (6 n^2 quads)")
+    ap.add_argument("--sweep-freqs", type=int, default=2, help="--workload sweep: frequencies (of 8)")
+    ap.add_argument("--sweep-dirs", type=int, default=8, help="--workload sweep: incidence directions (of 64)")
+    ap.add_argument("--stream-requests", type=int, default=STREAM_REQUESTS,
+                    help="requests of the headline stream in the default line (0: leave it out)")
     ap.add_argument("--mixed-mode", type=int, default=3,
                     help="precision of the mixed form: 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates; 0: skip it")
     return ap.parse_args()
@@ -271,14 +276,18 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
-STREAM_DESC = ("seeded Poisson request stream (numpy default_rng(2024)), scaled down from the 216-6144-quad "
-               "stream to 216/384/600-quad cube-spheres and spheroids (radius 0.2-0.3), square or triangular "
-               "lattice of period 0.7-1.1, k.a in [1, 2.5], theta 0-60 deg, phi 0-360 deg, 30% repeats of an "
-               "earlier (mesh, k, in-plane wave vector) with a new amplitude or the mirrored polar angle; draws "
-               "within 2% of a Rayleigh anomaly are redrawn")
+STREAM_DESC = ("seeded Poisson request stream (numpy default_rng(2024)) at the given rate: cube-spheres and spheroids "
+               "of {sizes} quads (sizes drawn uniformly), radius 0.2-0.35 wavelengths (spheroids 0.85/0.85/1.15 of "
+               "it), square or triangular lattice of period 0.7-1.1 wavelengths (redrawn when the body's horizontal "
+               "extent exceeds 0.9 of the period), k.a in [1, 2.5], theta 0-60 deg, phi 0-360 deg; 30% of requests "
+               "repeat an earlier (mesh, k, in-plane wave vector) with a new amplitude or the mirrored polar angle; "
+               "draws within 2% of a Rayleigh anomaly are redrawn")
+# the headline request stream: its mesh sizes (6 n^2 quads) and request count
+STREAM_SIZES = (6, 16, 24, 32)
+STREAM_REQUESTS = 16
 
 
-def stream_requests(count, rng):
+def stream_requests(count, rng, sizes=STREAM_SIZES, radius=(0.2, 0.35)):
     """The request stream: (meshgen arguments, reuse key) per request."""
     import math
     reqs, seen = [], []
@@ -291,10 +300,12 @@ def stream_requests(count, rng):
             r["amp"] = (float(rng.uniform(0.5, 1.5)), float(rng.uniform(-1, 1)))
             reqs.append((r, base[1]))
             continue
-        n = int(rng.choice([6, 8, 10]))
-        rad = float(rng.uniform(0.2, 0.3))
+        n = int(rng.choice(list(sizes)))
+        rad = float(rng.uniform(*radius))
         axes = (rad, rad, rad) if rng.random() < 0.5 else (0.85 * rad, 0.85 * rad, 1.15 * rad)
         a = float(rng.uniform(0.7, 1.1))
+        if 2.0 * axes[0] > 0.9 * a:  # the body must fit its lattice cell with a gap
+            continue
         lat = ((a, 0.0), (0.0, a)) if rng.random() < 0.5 else ((a, 0.0), (0.5 * a, 0.5 * math.sqrt(3.0) * a))
         k = float(rng.uniform(1.0, 2.5)) / a
         th, ph = float(rng.uniform(0.0, 60.0)), float(rng.uniform(0.0, 360.0))
@@ -312,6 +323,80 @@ def stream_requests(count, rng):
         seen.append((r, key))
         reqs.append((r, key))
     return reqs
+
+
+def stream_compare(count, rate, slots, hbm_gb, mixed_mode, sizes=STREAM_SIZES, seed=2024, device=0):
+    """The headline comparison on one GPU: a seeded request stream served by
+    the native server in mixed precision (continuous batching, factorisation
+    and interior reuse, admission by device memory) against the plain FP64
+    drop-in path, one solve_bieq_aqd2 + force_FN_aqd2 per request in arrival
+    order with no reuse.  Both see the same arrival times; latency is arrival
+    to result.  Returns the sub-record of the bench line."""
+    from bem3_aw_qd2_b200 import api, meshgen
+    h, g = api.libs()
+    h.aqd2_set_verbose(0)
+    rng = np.random.default_rng(seed)
+    reqs = stream_requests(count, rng, sizes)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    files = [meshgen.write_inputs(tempfile.mkdtemp(prefix="stream_"), **r) for r, _ in reqs]
+    # plain FP64 drop-in path: requests in arrival order, one context each
+    # (read + initialisation from the input files happen before the clock)
+    cases = [api.Case.from_files(*f) for f in files]
+    F_plain, lat_plain = [], []
+    t0 = time.perf_counter()
+    for i, c in enumerate(cases):
+        while time.perf_counter() - t0 < arrivals[i]:
+            time.sleep(0.0005)
+        c.solve()
+        F_plain.append(c.force(0)[0])
+        c.close()
+        lat_plain.append((time.perf_counter() - t0 - arrivals[i]) * 1000.0)
+    el_plain = time.perf_counter() - t0
+    # served, mixed precision
+    cases = [api.Case.from_files(*f) for f in files]
+    probs = [c.problem() for c in cases]
+    srv = api.Server(device=device, hbm_budget=int(hbm_gb * (1 << 30)), slots=slots)
+    done, t_sub = {}, {}
+    t0 = time.perf_counter()
+    for i in range(count):
+        while time.perf_counter() - t0 < arrivals[i]:
+            for r in srv.poll(timeout_ms=1):
+                done[r.id] = (r, time.perf_counter())
+        t_sub[i] = time.perf_counter()
+        srv.submit(probs[i], reqs[i][1], i, precision=mixed_mode)
+    while len(done) < count:
+        for r in srv.poll(timeout_ms=100):
+            done[r.id] = (r, time.perf_counter())
+    el_served = max(t for _, t in done.values()) - t0
+    st = srv.stats()
+    srv.close()
+    lat_served = [(done[i][1] - t0 - arrivals[i]) * 1000.0 for i in range(count)]
+    bad = [done[i][0].error.decode() for i in range(count) if done[i][0].status != 0]
+    errs = [float(np.linalg.norm(np.array(done[i][0].F[:]) - F_plain[i]) / np.linalg.norm(F_plain[i]))
+            for i in range(count) if done[i][0].status == 0]
+    for c, p in zip(cases, probs):
+        c.free_problem(p)
+        c.close()
+    sizes_drawn = [6 * r["n"] ** 2 for r, _ in reqs]
+    return {"requests": count, "rate_per_s": rate, "mesh_quads": sizes_drawn,
+            "repeats": int(count - len({k for _, k in reqs})),
+            "plain_fp64": {"value": count / el_plain, "unit": "solves/s", "path": "solve_bieq_aqd2 + force_FN_aqd2 "
+                           "per request (C ABI, host buffers), arrival order, no reuse",
+                           "latency_ms": {"p50": float(np.percentile(lat_plain, 50)),
+                                          "p99": float(np.percentile(lat_plain, 99))}},
+            "served_mixed": {"value": count / el_served, "unit": "solves/s",
+                             "mode": {1: "FP32", 2: "TF32", 3: "BF16x9", 4: "BF16"}.get(mixed_mode, "?") +
+                                     " LU updates + FP64 refinement",
+                             "slots": slots, "hbm_budget_gb": hbm_gb,
+                             "latency_ms": {"p50": float(np.percentile(lat_served, 50)),
+                                            "p99": float(np.percentile(lat_served, 99))},
+                             "reused": int(st["reused"]), "evictions": int(st["evictions"]),
+                             "bytes_peak": st["bytes_peak"], "failed": len(bad), "errors": bad[:3]},
+            "served_over_plain": (count / el_served) / (count / el_plain),
+            "target": ">= 3x served mixed over plain FP64 at force rel. err <= 1e-8",
+            "force_rel_err_vs_plain_fp64": {"max": max(errs) if errs else None,
+                                            "median": float(np.median(errs)) if errs else None},
+            "stream": STREAM_DESC.format(sizes="/".join(str(6 * n * n) for n in sizes))}
 
 
 def run_stream(args, rank, world):
@@ -332,7 +417,7 @@ def run_stream(args, rank, world):
     rng = np.random.default_rng(2024)
     per_rank = max(args.steps, 8) * 8
     total = per_rank * world
-    all_reqs = stream_requests(total, rng)
+    all_reqs = stream_requests(total, rng, sizes=tuple(int(x) for x in args.stream_sizes.split(",")))
     all_arrivals = np.cumsum(rng.exponential(1.0 / (args.rate * world), total))
     mine = replicas.shard(total, rank, world)
     reqs = [all_reqs[i] for i in mine]
@@ -397,7 +482,9 @@ def run_stream(args, rank, world):
             "vs_baseline": None, "dtype": "f64 assembly, complex-FP32 LU + FP64 refinement", "data": "synthetic",
             "config": {"workload": "stream", "requests": total, "rate_per_s": args.rate * world,
                        "requests_per_gpu": per_rank, "slots": args.slots,
-                       "hbm_budget_gb": args.hbm_gb, "stream": STREAM_DESC},
+                       "hbm_budget_gb": args.hbm_gb,
+                       "stream": STREAM_DESC.format(sizes="/".join(str(6 * int(x) ** 2)
+                                                                  for x in args.stream_sizes.split(",")))},
             "latency_ms": mixed["latency_ms"], "fp64": out["fp64"], "mixed": mixed,
             "force_rel_err_mixed_vs_fp64": {"max": emax, "median": float(np.median(errs))}}
     if rank == 0:
@@ -425,6 +512,90 @@ def roofline_record(achieved, fp64_peak, terms_reg, cnt):
             "mean_terms_per_point": cnt[0] / max(cnt[3], 1)}
 
 
+def sweep_instances(freqs, dirs, n=16, a=0.8):
+    """Config-2 style sweep: the 1536-quad (n = 16) sphere of radius 0.3 in the
+    square lattice of period a, k a in [1.2, 2.4] (freqs values), theta uniform
+    in [0, 60] deg (dirs values; 0 becomes the reference's tiny tilt), phi = 0
+    (the reference rejects ky = 0: phi = 1e-6 deg); an instance within 2% of a
+    Rayleigh anomaly is left out.  Returns [(frequency index, meshgen args)]."""
+    import math
+    out = []
+    for fi, ka in enumerate(np.linspace(1.2, 2.4, freqs)):
+        k = ka / a
+        g = 2 * math.pi / a
+        for th in np.linspace(0.0, 60.0, dirs):
+            th = max(float(th), 1e-6)
+            kx = k * math.sin(math.radians(th))
+            if any(abs(math.hypot(kx + i * g, j * g) - k) < 0.02 * k for i in range(-6, 7) for j in range(-6, 7)):
+                continue
+            out.append((fi, dict(n=n, semi_axes=(0.3, 0.3, 0.3), lattice=((a, 0.0), (0.0, a)), theta_deg=th,
+                                 phi_deg=1e-6, wavelength=2 * math.pi / k)))
+    return out
+
+
+def run_sweep(args, rank, world):
+    """Batched sweep (config 2, reduced to --sweep-freqs x --sweep-dirs
+    instances): one context solves the instances in frequency order, so that
+    instances at the same frequency keep the free-space domain's matrices and
+    dpv factors (bemgpu_interior_reuses); FP64, then the mixed form, with the
+    mixed form's force error against FP64 per instance."""
+    import ctypes
+    from bem3_aw_qd2_b200 import api, meshgen
+    h, g = api.libs()
+    h.aqd2_set_verbose(0)
+    g.bemgpu_load.argtypes = [ctypes.c_void_p, ctypes.POINTER(api.Problem)]
+    g.bemgpu_interior_reuses.argtypes = [ctypes.c_void_p]
+    g.bemgpu_interior_reuses.restype = ctypes.c_longlong
+    inst = sweep_instances(args.sweep_freqs, args.sweep_dirs)
+    cases = [api.Case.from_files(*meshgen.write_inputs(tempfile.mkdtemp(prefix="sweep_"), **r)) for _, r in inst]
+    probs = [c.problem() for c in cases]
+    ctx = ctypes.c_void_p()
+    if g.bemgpu_create(0, None, ctypes.byref(ctx)) != 0:
+        raise RuntimeError("bemgpu_create failed")
+    rc3 = np.zeros(3)
+    res = {}
+    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 3)):
+        g.bemgpu_set_precision(ctx, prec)
+        # warm-up: the first instance (kernels loaded, graphs captured)
+        g.bemgpu_load(ctx, ctypes.byref(probs[0]))
+        g.bemgpu_run(ctx)
+        g.bemgpu_sync(ctx)
+        r0 = g.bemgpu_interior_reuses(ctx)
+        F = []
+        t0 = time.perf_counter()
+        for p in probs:
+            if g.bemgpu_load(ctx, ctypes.byref(p)) or g.bemgpu_run(ctx):
+                raise RuntimeError(g.bemgpu_error(ctx).decode())
+            Fv, Nv = np.zeros(3), np.zeros(3)
+            g.bemgpu_force(ctx, 0, api._p(rc3), api._p(Fv), api._p(Nv))
+            F.append(Fv)
+        g.bemgpu_sync(ctx)
+        el = time.perf_counter() - t0
+        res[tag] = {"value": len(probs) / el, "unit": "solves/s", "seconds": el,
+                    "interior_reuses": int(g.bemgpu_interior_reuses(ctx) - r0), "F": F}
+        if prec:
+            res[tag]["mode"] = {1: "FP32", 2: "TF32", 3: "BF16x9", 4: "BF16"}.get(g.bemgpu_get_precision(ctx), "?")
+    errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(res["mixed"]["F"], res["fp64"]["F"])]
+    for tag in res:
+        del res[tag]["F"]
+    g.bemgpu_destroy(ctx)
+    for c, p in zip(cases, probs):
+        c.free_problem(p)
+        c.close()
+    v = res["mixed"]["value"]
+    line = {"metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": 1, "steps": len(probs), "warmup": 1,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 assembly, complex-FP32 LU + FP64 refinement", "data": "synthetic",
+            "config": {"workload": "sweep", "instances": len(probs), "frequencies": args.sweep_freqs,
+                       "directions": args.sweep_dirs, "full_sweep": "64 directions x 8 frequencies (reduced here)",
+                       "mesh": "1536-quad cube-sphere r = 0.3, square lattice 0.8",
+                       "order": "frequency-major: instances at one frequency share the interior domain"},
+            "fp64": res["fp64"], "mixed": res["mixed"],
+            "force_rel_err_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def workload_desc(name):
     from bem3_aw_qd2_b200 import meshgen
     return {**meshgen.describe(name), "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
@@ -436,13 +607,18 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference" and args.workload != "stream":
         return run_reference(args, rank, world)
+    if args.workload == "sweep":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the sweep's reference time is the sphere1536 "
+                                                                  "reference line times the instance count"}))
+            return
+        return run_sweep(args, rank, world)
     if args.workload == "stream":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; its per-solve "
                                                                   "time is the sphere216 reference line"}))
             return
         return run_stream(args, rank, world)
-    # load the library (and the CUDA 12.9 cuBLAS it links) before torch brings its own
     from bem3_aw_qd2_b200 import api
     api.libs()
     import torch
@@ -596,6 +772,13 @@ def main():
         "mixed": mixed,
         "gpu_launches": args.steps * (10 + 4 + 2 + 2 + 2 + 2 + 1 + 1),
     }
+    if rank == 0 and world == 1 and args.stream_requests > 0 and args.workload == "sphere216":
+        # the headline metric on one GPU: the config-4 request stream, served
+        # mixed precision against the plain FP64 drop-in path
+        case.close()
+        torch.cuda.empty_cache()
+        out["stream"] = stream_compare(args.stream_requests, 200.0, args.slots, args.hbm_gb, args.mixed_mode or 3,
+                                       device=local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)
     if rank == 0:

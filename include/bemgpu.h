@@ -106,6 +106,31 @@ int bemgpu_set_far_rule(bemgpu_ctx *ctx, int on);
  * Costs about half of one regular-pair launch. */
 int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
 
+/* Interior-domain reuse (no counterpart in the reference, which assembles
+ * every domain for every solve): the free-space domains' matrices (G, H, dG,
+ * dH, dF of domains >= 1, create_cmatrix_domain with did >= 1,
+ * bem3_aw_qd2_solve_bieq.c:133-218) and their dpv factors depend only on the
+ * mesh, the media and the frequency.  bemgpu_load compares the new problem's
+ * element tables, domain lists and interior wave numbers with the previous
+ * load's; when they are the same (a new in-plane Bloch wave vector or
+ * incident field on the same body at the same frequency) the context keeps
+ * those matrices and factors and the next bemgpu_assemble / bemgpu_solve skip
+ * them.  Returns the number of loads that did so. */
+long long bemgpu_interior_reuses(bemgpu_ctx *ctx);
+
+/* Rotation and translation of the loaded body on the device (the
+ * reference's Rodrigues options of read_aqd2, bem3_aw_qd2.c:16-24, 395-422:
+ * rotation about the axis rv[3] by th radians, then translation by tv[3]),
+ * for requests that differ from a resident problem only in the body's
+ * placement: the element constants, collocation nodes and normals are turned
+ * and moved, and the incident field at the new nodes is evaluated on the
+ * device (init_boundary_data, bem3_aw_qd2.c:1104-1146), so nothing is
+ * uploaded again.  The lattice and the incident wave stay.  The next
+ * bemgpu_run assembles and solves the moved body.  Transforms compose: each
+ * applies to the current placement.  A host AQD2 the problem came from is not
+ * changed. */
+int bemgpu_transform_mesh(bemgpu_ctx *ctx, const double *rv, double th, const double *tv);
+
 /* Free the loaded problem's device memory (the context stays usable). */
 int bemgpu_unload(bemgpu_ctx *ctx);
 
@@ -178,23 +203,23 @@ int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t,
  * d3qd2_mkl_solver.c:18-148, bem3_aw_qd2_solve_bieq.c:533-653).  Assembly,
  * residuals and the force integral stay FP64 in every mode.
  *   0 BEMGPU_FP64      FP64 LU (default; the drop-in)
- *   1 BEMGPU_MIXED_FP32   complex FP32 LU, FP32 CUDA-core GEMM updates
- *   2 BEMGPU_MIXED_TF32   complex FP32 LU, TF32 tensor-core GEMM updates
- *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, GEMM updates as three BF16 products
- *                         on the tensor cores (FP32-accurate)
- *   4 BEMGPU_MIXED_BF16   complex FP32 LU, BF16 tensor-core GEMM updates
+ *   1 BEMGPU_MIXED_FP32   complex FP32 LU, FP32 CUDA-core trailing updates
+ *   2 BEMGPU_MIXED_TF32   complex FP32 LU, TF32 tensor-core trailing updates
+ *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, trailing updates as split-BF16
+ *                         products on the tensor cores (FP32-accurate)
+ *   4 BEMGPU_MIXED_BF16   complex FP32 LU, BF16 tensor-core trailing updates
  * Modes 1-4 refine in FP64 against the FP64 matrix until the correction is
  * below 1e-15 of the solution; a system that does not get below 1e-12 is
- * solved again in FP64 (reported by bemgpu_solve_stats). */
+ * solved again in FP64 (reported by bemgpu_solve_stats).  A mode whose
+ * tensor-core update this build does not have runs as mode 1;
+ * bemgpu_get_precision reports the mode in effect. */
 #define BEMGPU_FP64 0
 #define BEMGPU_MIXED_FP32 1
 #define BEMGPU_MIXED_TF32 2
 #define BEMGPU_MIXED_BF16X9 3
 #define BEMGPU_MIXED_BF16 4
 int bemgpu_set_precision(bemgpu_ctx *ctx, int mode);
-/* The mode in effect: BF16X9 needs cuBLAS 12.9 or later in the process and
- * becomes TF32 with an older one (for example when another library loaded
- * its own cuBLAS first). */
+/* The mode in effect (see bemgpu_set_precision). */
 int bemgpu_get_precision(bemgpu_ctx *ctx);
 
 /* Refinement record of the last bemgpu_solve, one entry per dense system
