@@ -95,7 +95,7 @@ class Problem(ctypes.Structure):
 class Result(ctypes.Structure):
     """bemgpu_result (include/bemgpu.h)."""
     _fields_ = [("id", ctypes.c_longlong), ("status", ctypes.c_int), ("reused", ctypes.c_int),
-                ("F", ctypes.c_double * 3), ("N", ctypes.c_double * 3), ("queue_ms", ctypes.c_double),
+                ("precision", ctypes.c_int), ("F", ctypes.c_double * 3), ("N", ctypes.c_double * 3), ("queue_ms", ctypes.c_double),
                 ("service_ms", ctypes.c_double), ("error", ctypes.c_char * 160)]
 
 

@@ -21,7 +21,7 @@ LIB = os.path.join(HERE, "lib")
 INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["bem_assemble.cu", "bem_solve.cu", "bem_lu.cu", "bem_capi.cu", "bem_static.cu", "bem_mixed.cu",
-                "bem_server.cu", "bem_transform.cu"]
+                "bem_server.cu", "bem_transform.cu", "bem_gmres.cu", "bem_tc.cu"]
 HOST_SOURCES = ["host/aqd2_io.c", "host/aqd2_init.c", "host/aqd2_gpu.c"]
 REFERENCE = os.environ.get("BEM_REFERENCE_DIR", "/root/reference")
 

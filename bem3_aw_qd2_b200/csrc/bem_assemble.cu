@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
       if (fabs(Fz) > BEM_CBD_SDF || fabs(Fe) > BEM_CBD_SDF) {
         fl = 1;
         const int k = atomicAdd(&cnt, 1);
-        if (k < BEM_MAXNEAR) list[k] = s;
+        if (k < D.near_cap) list[k] = s;
       } else {
         sF += F; sFz += Fz; sFe += Fe;
         if (fr.on && rzmin >= BEM_FAR_PLANE_TOL && far_pair(fr, el, nd.rt, tri)) fl = 3;
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
   }
   if (threadIdx.x == 0) {
     int n = cnt;
-    if (n > BEM_MAXNEAR) { set_status(status, BEM_ST_NEAR_OVERFLOW); n = BEM_MAXNEAR; }
+    if (n > D.near_cap) { set_status(status, BEM_ST_NEAR_OVERFLOW); n = D.near_cap; }
     // deterministic order: sort the row's near-singular sources by index
     for (int a = 1; a < n; ++a) {
       const int v = list[a];
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
       while (b >= 0 && list[b] > v) { list[b + 1] = list[b]; --b; }
       list[b + 1] = v;
     }
-    for (int a = 0; a < n; ++a) near_s[(size_t)p * BEM_MAXNEAR + a] = list[a];
+    for (int a = 0; a < n; ++a) near_s[(size_t)p * D.near_cap + a] = list[a];
     near_n[p] = n;
     rowF[3 * p + 0] = red[0][0];
     rowF[3 * p + 1] = red[1][0];
@@ -601,7 +601,7 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
                                                         unsigned long long *terms) {
   const int p = blockIdx.x, k = blockIdx.y;
   if (k >= near_n[p]) return;
-  const int s = near_s[(size_t)p * BEM_MAXNEAR + k];
+  const int s = near_s[(size_t)p * D.near_cap + k];
   bem_node nd;
   int t, te;
   bem_load_node(D, p, nd, t, te);
@@ -662,7 +662,7 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
     const int a = (c & 7) >> 1, part = c & 1;
     dst[2 * ((size_t)p * N + 4 * s + a) + part] = v[c];
   } else if (threadIdx.x < 19) {
-    nearF[((size_t)p * BEM_MAXNEAR + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
+    nearF[((size_t)p * D.near_cap + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
   }
 }
 
@@ -920,7 +920,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k,
                                                         double *__restrict__ dH, double *__restrict__ nearF) {
   const int p = blockIdx.x, kk = blockIdx.y;
   if (kk >= near_n[p]) return;
-  const int s = near_s[(size_t)p * BEM_MAXNEAR + kk];
+  const int s = near_s[(size_t)p * D.near_cap + kk];
   bem_node nd;
   int t, te;
   bem_load_node(D, p, nd, t, te);
@@ -952,7 +952,7 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k,
     for (int c = 0; c < 51; ++c) av[c] = v[c];
     fs_store(D, p, s, a, G, H, dG, dH);
     const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
-    double *nf = nearF + ((size_t)p * BEM_MAXNEAR + kk) * 3;
+    double *nf = nearF + ((size_t)p * D.near_cap + kk) * 3;
     nf[0] = sg * a.f * BEM_I_FP;
     nf[1] = sg * a.fz * BEM_I_FP;
     nf[2] = sg * a.fe * BEM_I_FP;
@@ -1401,7 +1401,7 @@ __global__ void k_diag(bem_dom_dev D, int exterior, const double *__restrict__ r
   double F = rowF[3 * p], Fz = rowF[3 * p + 1], Fe = rowF[3 * p + 2];
   const int n = near_n[p];
   for (int k = 0; k < n; ++k) {
-    const double *nf = nearF + ((size_t)p * BEM_MAXNEAR + k) * 3;
+    const double *nf = nearF + ((size_t)p * D.near_cap + k) * 3;
     F += nf[0]; Fz += nf[1]; Fe += nf[2];
   }
   F += selfF[3 * p]; Fz += selfF[3 * p + 1]; Fe += selfF[3 * p + 2];
@@ -1630,14 +1630,14 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    k_q0_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
+    k_q0_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
     if (ev) cudaEventRecord(ev[3], st);
     k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
     if (D->has_tri) k_q0_self_tri<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
   } else {
     k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
     if (ev) cudaEventRecord(ev[2], st);
-    k_fs_near<<<dim3(N, BEM_MAXNEAR), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
+    k_fs_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
     if (ev) cudaEventRecord(ev[3], st);
     k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
     if (D->has_tri) k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);

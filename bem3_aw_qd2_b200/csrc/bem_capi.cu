@@ -73,6 +73,7 @@ struct bemgpu_ctx {
   // precision of the dense solves: 0 FP64 LU; BEM_MIXED_* complex FP32 LU + FP64 refinement
   int precision = 0;
   bem_mixed mxs[BEMGPU_MAXDOM + 1];  // FP32 factors per dense system (0 global, 1 + d dpv of domain d)
+  int refine = 0;  // refinement of the mixed solves: 0 IR then GMRES-IR, 1 IR only, 2 GMRES-IR only
   bool mx_ready[BEMGPU_MAXDOM + 1] = {};
   // FP64 factors: the global system in A, domain d's dpv system in Wd[d]; the
   // row pivoting and the scratch of each in lus[slot] (0 global, 1 + d dpv)
@@ -90,7 +91,7 @@ struct bemgpu_ctx {
   // side lane: the dpv factorisations run there, overlapping the global system
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {};
+  int st_n = 0, st_iters[BEMGPU_MAXDOM + 1] = {}, st_fallback[BEMGPU_MAXDOM + 1] = {}, st_gmres[BEMGPU_MAXDOM + 1] = {};
   double st_corr[BEMGPU_MAXDOM + 1] = {};
   // Free-space (interior) domains: their matrices depend on the mesh, the
   // media and the frequency only, not on the in-plane Bloch wave vector or the
@@ -679,7 +680,7 @@ static int dense_factor(bemgpu_ctx *c, int slot, double *M, int64_t n, const cha
     if (bem_mixed_init(&c->mxs[slot], c->precision, c->stream)) { snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err); return -1; }
     c->mx_ready[slot] = true;
   }
-  c->mxs[slot].mode = c->precision;
+  c->mxs[slot].req_mode = c->precision;
   cudaStream_t st = lane ? c->side : c->stream;
   if (bem_mixed_factor(&c->mxs[slot], M, (int)n, st)) {
     snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
@@ -697,13 +698,10 @@ static int check_side_factors(bemgpu_ctx *c) {
   for (int d = 0; d <= c->MN; ++d) {
     const int slot = 1 + d;
     if (c->fac_fp64[slot]) {
-      const int r = lu_status_check(c, slot, "dpv LU");
-      if (r) {
-        char tmp[512];
-        snprintf(tmp, sizeof(tmp), "domain %d: %s", d, c->err);
-        snprintf(c->err, sizeof(c->err), "%s", tmp);
-        return r;
-      }
+      char what[48];
+      snprintf(what, sizeof(what), "dpv LU of domain %d", d);
+      const int r = lu_status_check(c, slot, what);
+      if (r) return r;
     } else if (bem_mixed_status(&c->mxs[slot], c->stream) & 0x20u) {
       c->st_fallback[slot] = 1;
       const int r = dense_factor_fp64(c, slot, c->dom_tri[d] ? c->Gc[d] : c->G[d], c->cn[d], "dpv LU");
@@ -722,14 +720,29 @@ static int dense_apply(bemgpu_ctx *c, int slot, double *M, int64_t n, int64_t nr
     CK(cudaMemcpyAsync(Bsave, B, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
     int it = 0;
     double rc = 1.0;
-    if (bem_mixed_solve(&c->mxs[slot], M, (int)n, (int)nrhs, B, 30, 4.0 * 1.1102230246251565e-16, &it, &rc,
-                        c->stream)) {
-      snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
-      return -1;
+    if (c->refine != 2) {
+      if (bem_mixed_solve(&c->mxs[slot], M, (int)n, (int)nrhs, B, 30, 4.0 * 1.1102230246251565e-16, &it, &rc,
+                          c->stream)) {
+        snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
+        return -1;
+      }
+      c->st_iters[slot] = it;
+      c->st_corr[slot] = rc;
+      if (rc <= 1e-12) return 0;
     }
-    c->st_iters[slot] = it;
-    c->st_corr[slot] = rc;
-    if (rc <= 1e-12) return 0;
+    if (c->refine != 1) {
+      // GMRES-IR with the same FP32 factors as the preconditioner, from the
+      // saved right-hand sides; success: relative residual <= 1e-12
+      CK(cudaMemcpyAsync(B, Bsave, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
+      if (bem_mixed_solve_gmres(&c->mxs[slot], M, (int)n, (int)nrhs, B, 1e-14, &it, &rc, c->stream)) {
+        snprintf(c->err, sizeof(c->err), "%s: %s", what, c->mxs[slot].err);
+        return -1;
+      }
+      c->st_iters[slot] = it;
+      c->st_corr[slot] = rc;
+      c->st_gmres[slot] = 1;
+      if (rc <= 1e-12) return 0;
+    }
     // not refined to FP64 accuracy: FP64 factors from the intact M
     c->st_fallback[slot] = 1;
     CK(cudaMemcpyAsync(B, Bsave, 2 * n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), what);
@@ -827,7 +840,7 @@ static int ensure_saves(bemgpu_ctx *c) {
       c->mx_ready[slot] = true;
     }
   c->st_n = c->MN + 2;
-  for (int i = 0; i < c->st_n; ++i) c->st_fallback[i] = 0;
+  for (int i = 0; i < c->st_n; ++i) c->st_fallback[i] = c->st_gmres[i] = 0;
   return 0;
 }
 
@@ -1053,6 +1066,7 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d) {
   D.npe = c->npe;
   D.has_tri = c->dom_tri[d];
   D.far_rule = c->far_rule;
+  D.near_cap = BEM_MAXNEAR_H;
   return D;
 }
 
@@ -1287,4 +1301,16 @@ extern "C" int bemgpu_transform_mesh(bemgpu_ctx *c, const double *rv, double th,
   c->int_data.clear();
   for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
   return 0;
+}
+
+extern "C" int bemgpu_set_refinement(bemgpu_ctx *c, int method) {
+  if (method < 0 || method > 2) { snprintf(c->err, sizeof(c->err), "refinement method %d (0..2)", method); return -2; }
+  c->refine = method;
+  return 0;
+}
+
+extern "C" int bemgpu_refinement_used(bemgpu_ctx *c, int *gmres, int max) {
+  int k = 0;
+  for (; k < c->st_n && k < max; ++k) gmres[k] = c->st_gmres[k];
+  return k;
 }

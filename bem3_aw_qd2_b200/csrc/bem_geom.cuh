@@ -13,7 +13,7 @@
 #define BEM_DEPS 0.1           // radius of the PV disc D_eps        (d3qd2_const.h:34)
 #define BEM_I_FP 7.957747154594766788444e-2  // 1/(4 pi)
 #define BEM_P44 0.5773502691896257645091     // 1/sqrt(3)
-#define BEM_MAXNEAR 64         // near-singular sources kept per collocation node
+#define BEM_MAXNEAR 256        // most near-singular sources a collocation node can hold (bem_dom_dev.near_cap)
 
 #define BEM_GFN 8              // far-pair rule (k_q0_far)
 struct bem_quad {

@@ -14,14 +14,16 @@ struct bem_dom_dev {
   const int *npe;               // nodes per element: 4 bilinear quad, 3 linear triangle
   int has_tri;                  // any triangle among the domain's elements
   int far_rule;                 // periodic domain: 8 x 8 rule for far quad pairs (k_q0_far)
+  int near_cap;                 // near-singular sources one collocation node can hold (<= 256):
+                                // the stride of bem_scratch.near_s / nearF
 };
 
 // Scratch used by one domain assembly (sized for N = 4 ne rows).
 struct bem_scratch {
   double *rowF;     // [N][3] geometric F, dF/dtz, dF/dte summed over regular sources
-  int *near_s;      // [N][BEM_MAXNEAR] near-singular source indices, sorted
+  int *near_s;      // [N][near_cap] near-singular source indices, sorted
   int *near_n;      // [N]
-  double *nearF;    // [N][BEM_MAXNEAR][3]
+  double *nearF;    // [N][near_cap][3]
   double *selfF;    // [N][3]
   uint8_t *flag;    // [N][ne] 0 regular, 1 near-singular, 2 self, 3 far (regular, shorter rule)
   unsigned *plist;  // [pcap] periodic-domain pair lists p * ne + s: regular from the front, far from the back (optional)
@@ -61,4 +63,5 @@ int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int
 // host-side copies of the table sizes
 #define BEM_GLN_H 12
 #define BEM_GHN_H 64
-#define BEM_MAXNEAR_H 64
+#define BEM_MAXNEAR_H 256      // near-singular table of a context (bodies a millimetre apart need ~90)
+#define BEM_MAXNEAR_STATIC 64  // near-singular table of the allocation-free entry point

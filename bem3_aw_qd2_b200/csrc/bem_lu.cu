@@ -105,11 +105,19 @@ __device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y
 // ---------------------------------------------------------------- partial pivoting in one CTA
 template <class C2>
 struct gepp_sh {
-  typename cx<C2>::R wv[2][LU_TH / 32];
-  int wi[2][LU_TH / 32];
+  unsigned wk[2][LU_TH / 32];  // each warp's pivot key
   C2 prow[2][LU_W], krow[2][LU_W];
+  C2 prcp[2];                  // reciprocal of the pivot
   int pid[2], kid[2];
 };
+
+// Pivot key of a candidate: the float bits of |re| + |im| (non-negative floats
+// order as their bits) with the low 8 bits replaced by 255 - t, so that one
+// integer maximum gives the largest value and, among values equal to 2^-15,
+// the lowest row; 0 for a row that takes no part.
+__device__ __forceinline__ unsigned pivot_key(float a, int t) {
+  return (__float_as_uint(a) & 0xFFFFFF00u) | (unsigned)(255 - t);
+}
 
 template <class C2>
 __device__ __forceinline__ void rot1(C2 (&v)[LU_W]) {
@@ -129,30 +137,21 @@ __device__ __forceinline__ void rot1(C2 (&v)[LU_W]) {
 // index is a compile-time constant inside one short loop body.
 template <class C2>
 __device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, unsigned *status) {
-  using R = typename cx<C2>::R;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int steps = min(w, rr);
   for (int j = 0; j < steps; ++j) {
     const int b = j & 1;
-    R val = (t >= j && t < rr) ? cabs1(v[0]) : (R)-1;
-    int bi = t;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const R ov = __shfl_down_sync(FULL, val, o);
-      const int oi = __shfl_down_sync(FULL, bi, o);
-      if (ov > val || (ov == val && oi < bi)) { val = ov; bi = oi; }
-    }
-    if (lane == 0) { sh.wv[b][wid] = val; sh.wi[b][wid] = bi; }
+    // the pivot: one integer maximum per warp, then over the warps (the
+    // 2^-15 resolution of the key only picks among rows within that much of
+    // the largest, which keeps partial pivoting's growth bound)
+    const unsigned key = __reduce_max_sync(FULL, (t >= j && t < rr) ? pivot_key((float)cabs1(v[0]), t) : 0u);
+    if (lane == 0) sh.wk[b][wid] = key;
     __syncthreads();
-    R best = sh.wv[b][0];
-    int p = sh.wi[b][0];
+    unsigned best = sh.wk[b][0];
 #pragma unroll
-    for (int q = 1; q < LU_TH / 32; ++q) {
-      const R ov = sh.wv[b][q];
-      const int oi = sh.wi[b][q];
-      if (ov > best || (ov == best && oi < p)) { best = ov; p = oi; }
-    }
-    if (!(best > (R)0)) {
+    for (int q = 1; q < LU_TH / 32; ++q) best = max(best, sh.wk[b][q]);
+    int p = 255 - (int)(best & 255u);
+    if ((best >> 8) == 0u) {  // no non-zero entry left in the column
       if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
       p = j;
     }
@@ -160,6 +159,7 @@ __device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, uns
 #pragma unroll
       for (int c = 0; c < LU_W; ++c) sh.prow[b][c] = v[c];
       sh.pid[b] = id;
+      sh.prcp[b] = crcp(v[0]);
     }
     if (t == j) {
 #pragma unroll
@@ -177,7 +177,7 @@ __device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, uns
       id = sh.kid[b];
     }
     if (t > j && t < rr) {
-      const C2 l = cmul(v[0], crcp(sh.prow[b][0]));
+      const C2 l = cmul(v[0], sh.prcp[b]);
       v[0] = l;
 #pragma unroll
       for (int c = 1; c < LU_W; ++c)
@@ -207,12 +207,31 @@ __device__ __forceinline__ void cluster_sync_all() {
 }
 
 // ---------------------------------------------------------------- panel
+// the leaves' partial pivoting only selects candidate rows (the root factors
+// the winners from their stored values), so it runs in complex FP32 for
+// either precision of the factorisation
+template <class C2> struct leaf_of { using T = float2; };
+
+__device__ __forceinline__ void load_row_leaf(float2 (&v)[LU_W], const double2 *A, long lda, int row, int k, int w) {
+  const double2 *p = A + (size_t)(row < 0 ? 0 : row) * lda + k;
+#pragma unroll
+  for (int c = 0; c < LU_W; ++c) {
+    const double2 x = (row >= 0 && c < w) ? p[c] : make_double2(0.0, 0.0);
+    v[c] = make_float2((float)x.x, (float)x.y);
+  }
+}
+__device__ __forceinline__ void load_row_leaf(float2 (&v)[LU_W], const float2 *A, long lda, int row, int k, int w) {
+  load_row(v, A, lda, row, k, w);
+}
+
 template <class C2>
 struct panel_sh {
   gepp_sh<C2> g;
+  gepp_sh<float2> gl;
   C2 lu[LU_W][LU_W + 1];
   C2 ui[LU_W][LU_W + 1];
   C2 li[LU_W][LU_W + 1];
+  C2 rd[LU_W];  // reciprocals of U11's diagonal
   int sel[LU_W], la[LU_W], lb[LU_W];
 };
 
@@ -224,7 +243,6 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int crank = (int)cluster_rank();
   const int w = min(LU_W, n - k), m = n - k;
-  C2 v[LU_W];
   int id = -1;
   if (m > LU_TH) {
     // leaves: each CTA a contiguous slice of the panel's rows, in rounds of
@@ -239,9 +257,10 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
       else if (t < ncand + fresh) row = next + (t - ncand);
       next += fresh;
       id = row;
-      load_row(v, A, lda, row, k, w);
+      float2 vl[LU_W];
+      load_row_leaf(vl, A, lda, row, k, w);
       const int rr = ncand + fresh;
-      gepp(v, id, rr, w, S.g, nullptr);
+      gepp(vl, id, rr, w, S.gl, nullptr);
       ncand = min(w, rr);
       __syncthreads();
     }
@@ -267,6 +286,7 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
     rr = m;
     id = t < m ? k + t : -1;
   }
+  C2 v[LU_W];
   load_row(v, A, lda, id, k, w);
   gepp(v, id, rr, w, S.g, status);
   if (t < LU_W) {
@@ -279,17 +299,27 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
     S.sel[t] = t < w ? id : -1;
     if (t < w) pv[PV_SEL + t] = id;
   }
+  if (t < LU_W) S.rd[t] = t < w ? crcp(S.lu[t][t]) : czero<C2>();
   __syncthreads();
   if (wid == 0) {
     // U11^-1, column j = lane: x_j = 1 / u_jj, x_i = -(sum_{i<l<=j} u_il x_l) / u_ii
+    // (four partial sums: the dependent chain is the critical path)
     const int j = lane;
     for (int i = 0; i < LU_W; ++i) S.ui[i][j] = czero<C2>();
     if (j < w) {
-      S.ui[j][j] = crcp(S.lu[j][j]);
+      S.ui[j][j] = S.rd[j];
       for (int i = j - 1; i >= 0; --i) {
-        C2 s = czero<C2>();
-        for (int l = i + 1; l <= j; ++l) s = cfma(S.lu[i][l], S.ui[l][j], s);
-        S.ui[i][j] = cneg(cmul(s, crcp(S.lu[i][i])));
+        C2 s0 = czero<C2>(), s1 = czero<C2>(), s2 = czero<C2>(), s3 = czero<C2>();
+        int l = i + 1;
+        for (; l + 3 <= j; l += 4) {
+          s0 = cfma(S.lu[i][l], S.ui[l][j], s0);
+          s1 = cfma(S.lu[i][l + 1], S.ui[l + 1][j], s1);
+          s2 = cfma(S.lu[i][l + 2], S.ui[l + 2][j], s2);
+          s3 = cfma(S.lu[i][l + 3], S.ui[l + 3][j], s3);
+        }
+        for (; l <= j; ++l) s0 = cfma(S.lu[i][l], S.ui[l][j], s0);
+        const C2 s = cx<C2>::mk(s0.x + s1.x + s2.x + s3.x, s0.y + s1.y + s2.y + s3.y);
+        S.ui[i][j] = cneg(cmul(s, S.rd[i]));
       }
     }
     __syncwarp();
@@ -301,9 +331,16 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
     if (j < w) {
       S.li[j][j] = cone<C2>();
       for (int i = j + 1; i < w; ++i) {
-        C2 s = czero<C2>();
-        for (int l = j; l < i; ++l) s = cfma(S.lu[i][l], S.li[l][j], s);
-        S.li[i][j] = cneg(s);
+        C2 s0 = czero<C2>(), s1 = czero<C2>(), s2 = czero<C2>(), s3 = czero<C2>();
+        int l = j;
+        for (; l + 3 < i; l += 4) {
+          s0 = cfma(S.lu[i][l], S.li[l][j], s0);
+          s1 = cfma(S.lu[i][l + 1], S.li[l + 1][j], s1);
+          s2 = cfma(S.lu[i][l + 2], S.li[l + 2][j], s2);
+          s3 = cfma(S.lu[i][l + 3], S.li[l + 3][j], s3);
+        }
+        for (; l < i; ++l) s0 = cfma(S.lu[i][l], S.li[l][j], s0);
+        S.li[i][j] = cx<C2>::mk(-(s0.x + s1.x + s2.x + s3.x), -(s0.y + s1.y + s2.y + s3.y));
       }
     }
     __syncwarp();
@@ -627,7 +664,7 @@ __global__ void k_lu_iota(int *rowmap, int n) {
 
 // ---------------------------------------------------------------- triangular solves
 #define TS_TH 128
-#define TS_SPIN_LIMIT (1L << 24)
+#define TS_WAIT_NS 1000000000ull  // one second
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   unsigned v;
@@ -637,15 +674,28 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// wait until *f != 0, at most TS_SPIN_LIMIT polls (about a second), then give up
-// with BEM_LU_ST_WAIT set; once any wait has given up, later waits return at once
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// wait until *f != 0: a tight spin for the first 20 us (a flag normally
+// arrives within a few), then polls with short sleeps; after one second it
+// gives up with BEM_LU_ST_WAIT set, and once any wait has given up later
+// waits return at once
 __device__ __forceinline__ void wait_flag(const unsigned *f, unsigned *status) {
-  for (long it = 0; !ld_acquire(f); ++it) {
-    if (it >= TS_SPIN_LIMIT || ((it & 255) == 255 && (ld_acquire(status) & BEM_LU_ST_WAIT))) {
-      atomicOr(status, BEM_LU_ST_WAIT);
-      return;
+  if (ld_acquire(f)) return;
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 1;; ++it) {
+    if (ld_acquire(f)) return;
+    if ((it & 63) == 0) {
+      const unsigned long long dt = gtimer() - t0;
+      if (dt > TS_WAIT_NS || (ld_acquire(status) & BEM_LU_ST_WAIT)) {
+        atomicOr(status, BEM_LU_ST_WAIT);
+        return;
+      }
+      if (dt > 20000ull) __nanosleep(256);
     }
-    __nanosleep(64);
   }
 }
 
@@ -676,20 +726,30 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const C2 *LU, long lda, int n
       for (int q = 0; q < NR; ++q) acc[q] = in[(size_t)q * n + src];
     }
     const int jlo = lower ? 0 : b + 1, jhi = lower ? b : nb;
+    // the factor's entries do not depend on the other blocks: the next
+    // block's eight are loaded before the wait for the current one's flag
+    const C2 *arow = LU + (size_t)(r < rows ? row : r0) * lda;
+    C2 ac[8], an[8];
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) {
+      const int col = jlo * 32 + s * 8 + cc;
+      ac[cc] = (jlo < jhi && r < rows && col < n) ? arow[col] : czero<C2>();
+    }
     for (int jb = jlo; jb < jhi; ++jb) {
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) {
+        const int col = (jb + 1) * 32 + s * 8 + cc;
+        an[cc] = (jb + 1 < jhi && r < rows && col < n) ? arow[col] : czero<C2>();
+      }
       wait_flag(flags + jb, status);
       const int c0 = jb * 32 + s * 8;
-      if (r < rows) {
-        const C2 *a = LU + (size_t)row * lda;
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-          const int col = c0 + cc;
-          if (col < n) {
-            const C2 av = a[col];
+      for (int cc = 0; cc < 8; ++cc) {
+        const int col = c0 + cc;
+        if (col < n)
 #pragma unroll
-            for (int q = 0; q < NR; ++q) acc[q] = cfms(av, __ldcg(out + (size_t)q * n + col), acc[q]);
-          }
-        }
+          for (int q = 0; q < NR; ++q) acc[q] = cfms(ac[cc], __ldcg(out + (size_t)q * n + col), acc[q]);
+        ac[cc] = an[cc];
       }
     }
 #pragma unroll
@@ -797,6 +857,15 @@ static void launch_update(float2 *A, int n, int k, int tiles, cudaStream_t st) {
   k_lu_update_c32<<<dim3(tiles, tiles), UF_TH, 0, st>>>(A, n, n, k);
 }
 
+// the tensor-core update of a complex FP32 panel when the LU has one
+// (returns 1 when launched)
+static int tc_update(bem_lu *w, double2 *, int, int, int, cudaStream_t) { (void)w; return 0; }
+static int tc_update(bem_lu *w, float2 *A, int n, int k, int wd, cudaStream_t st) {
+  if (!w->tc || !w->tc->ready) return 0;
+  bem_tc_launch(w->tc, A, n, n, k, wd, w->status, st);
+  return 1;
+}
+
 // the launches of one factorisation, in order (captured into the graph)
 template <class C2>
 static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
@@ -808,7 +877,9 @@ static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
     const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
     const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
     k_lu_apply<C2><<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, w->piv, (const C2 *)w->u11, w->rowmap, w->status);
-    if (r0 < n) launch_update(A, n, k, (n - r0 + UP_BM - 1) / UP_BM, st);
+    if (r0 < n) {
+      if (tc_update(w, A, n, k, wd, st) == 0) launch_update(A, n, k, (n - r0 + UP_BM - 1) / UP_BM, st);
+    }
   }
   CKL(cudaGetLastError(), "LU launch");
   return 0;
@@ -819,7 +890,8 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
   if (n <= 0) return 0;
   C2 *A = (C2 *)Av;
   if (grow_bytes(w, (void **)&w->rowmap, &w->rowmap_cap, (size_t)n * sizeof(int), "row map")) return -1;
-  if (!(w->gexec && w->g_A == Av && w->g_n == n)) {
+  const int tcmode = (sizeof(C2) == sizeof(float2) && w->tc && w->tc->ready) ? w->tc->nprod : 0;
+  if (!(w->gexec && w->g_A == Av && w->g_n == n && w->g_tc == tcmode)) {
     if (w->gexec) cudaGraphExecDestroy(w->gexec);
     if (w->graph) cudaGraphDestroy(w->graph);
     w->gexec = nullptr;
@@ -837,6 +909,7 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
     CKL(cudaGraphInstantiate(&w->gexec, g, 0), "LU graph");
     w->g_A = Av;
     w->g_n = n;
+    w->g_tc = tcmode;
   }
   CKL(cudaGraphLaunch(w->gexec, st), "LU graph launch");
   return 0;

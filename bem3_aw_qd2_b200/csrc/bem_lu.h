@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include "bem_tc.h"
 
 #define BEM_LU_W 32            // panel width (columns factored per panel)
 #define BEM_LU_ST_ZERO 0x20u   // a zero pivot (singular matrix), as BEMGPU_ST_SOLVE
@@ -26,7 +27,8 @@ struct bem_lu {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   const void *g_A = nullptr;
-  int g_n = 0;
+  int g_n = 0, g_tc = -1;
+  bem_tc *tc = nullptr;       // complex FP32 only: trailing updates on the tensor cores when set
   int sms = 0, coop_blocks = 0;  // device facts for the launches
   char err[200] = {0};
 };

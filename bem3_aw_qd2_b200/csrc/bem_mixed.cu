@@ -79,8 +79,8 @@ static int grow(bem_mixed *m, T **p, size_t *cap, size_t count) {
 }
 
 extern "C" int bem_mixed_init(bem_mixed *m, int mode, cudaStream_t st) {
-  (void)mode;  // every mode runs its trailing updates in FP32 on the CUDA cores
   *m = bem_mixed();
+  m->req_mode = mode;
   m->mode = BEM_MIXED_FP32;
   int dev = 0;
   CKC(cudaGetDevice(&dev));
@@ -96,6 +96,8 @@ extern "C" int bem_mixed_init(bem_mixed *m, int mode, cudaStream_t st) {
 
 extern "C" void bem_mixed_free(bem_mixed *m) {
   if (m->lu_ready) bem_lu_free(&m->lu);
+  bem_gmres_free(&m->gm);
+  bem_tc_free(&m->tc);
   cudaFree(m->M); cudaFree(m->R32); cudaFree(m->X); cudaFree(m->R); cudaFree(m->norms);
   *m = bem_mixed();
 }
@@ -105,6 +107,18 @@ extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream
   if (grow(m, &m->M, &m->M_cap, count)) return -1;
   k_round_c32<<<grid_for(count), 256, 0, st>>>((const double2 *)A, m->M, count);
   CKC(cudaGetLastError());
+  // trailing updates: mode 1 on the CUDA cores; 2 and 4 one TF32 product, 3
+  // three split products on the tensor cores (buffers and TMA maps prepared
+  // here, outside any capture); a failed set-up leaves the CUDA cores
+  m->lu.tc = nullptr;
+  m->mode = BEM_MIXED_FP32;
+  if (m->req_mode >= BEM_MIXED_TF32) {
+    const int nprod = m->req_mode == BEM_MIXED_BF16X9 ? 3 : 1;
+    if (bem_tc_prepare(&m->tc, n, nprod) == 0) {
+      m->lu.tc = &m->tc;
+      m->mode = nprod == 3 ? BEM_MIXED_BF16X9 : BEM_MIXED_TF32;
+    }
+  }
   if (bem_lu_factor_c(&m->lu, (float *)m->M, n, st)) {
     snprintf(m->err, sizeof(m->err), "%s", m->lu.err);
     return -1;
@@ -152,6 +166,45 @@ extern "C" int bem_mixed_solve(bem_mixed *m, const double *A, int n, int nrhs, d
   *iters = it;
   *rel_corr = rc;
   CKC(cudaMemcpyAsync(B, m->X, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  return 0;
+}
+
+__global__ void k_widen(const float2 *__restrict__ a, double2 *__restrict__ b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = make_double2((double)a[i].x, (double)a[i].y);
+}
+
+// the GMRES-IR preconditioner: z = M^-1 r with the FP32 factors
+static int mixed_precond(void *pctx, const double2 *r, double2 *z, cudaStream_t st) {
+  bem_mixed *m = (bem_mixed *)pctx;
+  const int n = m->gm_n;
+  k_round_c32<<<grid_for((size_t)n), 256, 0, st>>>(r, m->R32, (size_t)n);
+  if (bem_lu_solve_c(&m->lu, (const float *)m->M, n, 1, (float *)m->R32, st)) return -1;
+  k_widen<<<grid_for((size_t)n), 256, 0, st>>>(m->R32, z, n);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bem_mixed_solve_gmres(bem_mixed *m, const double *A, int n, int nrhs, double *B, double tol, int *iters,
+                                     double *rel_res, cudaStream_t st) {
+  if (grow(m, &m->R32, &m->R32_cap, (size_t)n) || grow(m, &m->X, &m->X_cap, (size_t)n)) return -1;
+  m->gm_n = n;
+  int total = 0;
+  double worst = 0.0;
+  for (int q = 0; q < nrhs; ++q) {
+    double *b = B + 2 * (size_t)q * n;
+    CKC(cudaMemsetAsync(m->X, 0, (size_t)n * sizeof(double2), st));
+    int outer = 0, inner = 0;
+    double rr = 0.0;
+    if (bem_gmres_ir(&m->gm, A, n, b, (double *)m->X, 20, tol, 10, mixed_precond, m, &outer, &inner, &rr, st)) {
+      snprintf(m->err, sizeof(m->err), "%s", m->gm.err);
+      return -1;
+    }
+    CKC(cudaMemcpyAsync(b, m->X, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    total += inner;
+    worst = !(rr <= worst) ? rr : worst;
+  }
+  *iters = total;
+  *rel_res = worst;
   return 0;
 }
 

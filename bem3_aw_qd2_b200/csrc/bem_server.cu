@@ -79,7 +79,7 @@ size_t problem_bytes(const bemgpu_problem *p, int precision) {
   for (int d = 0; d <= p->MN; ++d) {
     const size_t N = 4 * (size_t)p->dom_ne[d];
     // matrices, pair flags (and the periodic domain's 4-byte pair lists), near-singular tables
-    b += 3 * N * N * 16 + (d > 0 ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] * (d == 0 ? 5 : 1) + N * 64 * 40;
+    b += 3 * N * N * 16 + (d > 0 ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] * (d == 0 ? 5 : 1) + N * 256 * 28;
     f32 += N * N * 8;
   }
   if (precision) b += f32;
@@ -287,6 +287,7 @@ static void worker(bemgpu_server *s, int idx) {
     const double t_end = now_ms();
     res.status = rc;
     res.reused = reuse ? 1 : 0;
+    res.precision = r->precision;
     res.queue_ms = r->t_start - r->t_submit;
     res.service_ms = t_end - r->t_start;
     if (rc) snprintf(res.error, sizeof(res.error), "%s", bemgpu_error(sl.ctx));
@@ -339,6 +340,11 @@ extern "C" int bemgpu_server_submit(bemgpu_server *s, const bemgpu_problem *p, u
                                     int precision, int force_type, const double *rc, long long id) {
   request *r = new request(p, reuse_key, precision, force_type, rc, id);
   std::lock_guard<std::mutex> lk(s->mu);
+  if (r->bytes > s->budget && r->precision != 0) {
+    // the FP32 factors do not fit beside the FP64 matrices: run it in FP64
+    r->precision = 0;
+    r->bytes = problem_bytes(p, 0);
+  }
   if (r->bytes > s->budget) { delete r; return -2; }  // can never be admitted
   s->queue.push_back(r);
   ++s->submitted;

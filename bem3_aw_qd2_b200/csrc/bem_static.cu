@@ -30,9 +30,9 @@
 // scratch carve-up for N = 4 ne <= SMAX_N rows
 #define OFF_ROWF 0
 #define OFF_NEARS ALIGN256(OFF_ROWF + sizeof(double) * 3 * (size_t)SMAX_N)
-#define OFF_NEARN ALIGN256(OFF_NEARS + sizeof(int) * (size_t)SMAX_N * BEM_MAXNEAR_H)
+#define OFF_NEARN ALIGN256(OFF_NEARS + sizeof(int) * (size_t)SMAX_N * BEM_MAXNEAR_STATIC)
 #define OFF_NEARF ALIGN256(OFF_NEARN + sizeof(int) * (size_t)SMAX_N)
-#define OFF_SELFF ALIGN256(OFF_NEARF + sizeof(double) * 3 * (size_t)SMAX_N * BEM_MAXNEAR_H)
+#define OFF_SELFF ALIGN256(OFF_NEARF + sizeof(double) * 3 * (size_t)SMAX_N * BEM_MAXNEAR_STATIC)
 #define OFF_FLAG ALIGN256(OFF_SELFF + sizeof(double) * 3 * (size_t)SMAX_N)
 #define OFF_STATUS ALIGN256(OFF_FLAG + (size_t)SMAX_N * BEMGPU_STATIC_MAX_NE)
 #define OFF_TERMS ALIGN256(OFF_STATUS + sizeof(unsigned))
@@ -139,6 +139,7 @@ extern "C" int bemgpu_assemble_domain_static(const double *cr, const double *cw,
   D.ne = ne; D.sid = sid; D.cr = cr; D.cw = cw; D.ren = ren; D.plane = plane;
   D.wen = nullptr; D.npe = nullptr; D.has_tri = 0;  // bilinear elements only
   D.far_rule = 0;                                   // the reference's 12 x 12 rule for every regular pair
+  D.near_cap = BEM_MAXNEAR_STATIC;                  // at most 64 near-singular sources per node (status bit 0x04 beyond)
   bem_qp q;
   bem_qp_prepare(qp, &q);
   if (bem_launch_assemble(&D, &q, periodic != 0, periodic != 0, k, &S, G, H, dG, dH, dF, st, nullptr) != 0) return -4;

@@ -97,7 +97,7 @@ def parse():
                          "(for ncu --profile-from-start off)")
     ap.add_argument("--rate", type=float, default=10.0, help="stream workload: mean arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="stream workload: server slots")
-    ap.add_argument("--hbm-gb", type=float, default=170.0, help="stream: device-memory budget of the server")
+    ap.add_argument("--hbm-gb", type=float, default=150.0, help="stream: device-memory budget of the server (GiB)")
     ap.add_argument("--stream-sizes", default="6,10", help="--workload stream: cube-sphere n (6 n^2 quads)")
     ap.add_argument("--sweep-freqs", type=int, default=2, help="--workload sweep: frequencies (of 8)")
     ap.add_argument("--sweep-dirs", type=int, default=8, help="--workload sweep: incidence directions (of 64)")
@@ -284,7 +284,7 @@ STREAM_DESC = ("seeded Poisson request stream (numpy default_rng(2024)) at the g
                "draws within 2% of a Rayleigh anomaly are redrawn")
 # the headline request stream: its mesh sizes (6 n^2 quads) and request count
 STREAM_SIZES = (6, 16, 24, 32)
-STREAM_REQUESTS = 16
+STREAM_REQUESTS = 12
 
 
 def stream_requests(count, rng, sizes=STREAM_SIZES, radius=(0.2, 0.35)):
@@ -372,6 +372,7 @@ def stream_compare(count, rate, slots, hbm_gb, mixed_mode, sizes=STREAM_SIZES, s
     srv.close()
     lat_served = [(done[i][1] - t0 - arrivals[i]) * 1000.0 for i in range(count)]
     bad = [done[i][0].error.decode() for i in range(count) if done[i][0].status != 0]
+    fp64_run = sum(1 for i in range(count) if done[i][0].precision == 0)
     errs = [float(np.linalg.norm(np.array(done[i][0].F[:]) - F_plain[i]) / np.linalg.norm(F_plain[i]))
             for i in range(count) if done[i][0].status == 0]
     for c, p in zip(cases, probs):
@@ -391,6 +392,7 @@ def stream_compare(count, rate, slots, hbm_gb, mixed_mode, sizes=STREAM_SIZES, s
                              "latency_ms": {"p50": float(np.percentile(lat_served, 50)),
                                             "p99": float(np.percentile(lat_served, 99))},
                              "reused": int(st["reused"]), "evictions": int(st["evictions"]),
+                             "ran_fp64_for_memory": fp64_run,
                              "bytes_peak": st["bytes_peak"], "failed": len(bad), "errors": bad[:3]},
             "served_over_plain": (count / el_served) / (count / el_plain),
             "target": ">= 3x served mixed over plain FP64 at force rel. err <= 1e-8",

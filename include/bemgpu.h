@@ -204,10 +204,11 @@ int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t,
  * residuals and the force integral stay FP64 in every mode.
  *   0 BEMGPU_FP64      FP64 LU (default; the drop-in)
  *   1 BEMGPU_MIXED_FP32   complex FP32 LU, FP32 CUDA-core trailing updates
- *   2 BEMGPU_MIXED_TF32   complex FP32 LU, TF32 tensor-core trailing updates
- *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, trailing updates as split-BF16
- *                         products on the tensor cores (FP32-accurate)
- *   4 BEMGPU_MIXED_BF16   complex FP32 LU, BF16 tensor-core trailing updates
+ *   2 BEMGPU_MIXED_TF32   complex FP32 LU, trailing updates as one TF32
+ *                         product on the tensor cores (tcgen05)
+ *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, trailing updates as three split
+ *                         TF32 products on the tensor cores (FP32-accurate)
+ *   4 BEMGPU_MIXED_BF16   a single low-precision tensor-core product: mode 2
  * Modes 1-4 refine in FP64 against the FP64 matrix until the correction is
  * below 1e-15 of the solution; a system that does not get below 1e-12 is
  * solved again in FP64 (reported by bemgpu_solve_stats).  A mode whose
@@ -221,6 +222,19 @@ int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t,
 int bemgpu_set_precision(bemgpu_ctx *ctx, int mode);
 /* The mode in effect (see bemgpu_set_precision). */
 int bemgpu_get_precision(bemgpu_ctx *ctx);
+
+/* Refinement of the mixed-precision solves (no counterpart in the reference):
+ *   0 (default) iterative refinement; a system it does not bring below 1e-12
+ *     is solved by GMRES-IR before any FP64 fallback
+ *   1 iterative refinement only
+ *   2 GMRES-IR only: GMRES(20) on the system preconditioned by the FP32
+ *     factors, FP64 residuals and Krylov vectors, to a relative residual of
+ *     1e-14 (success: 1e-12)
+ * bemgpu_refinement_used gives, per dense system of the last solve, 1 if
+ * GMRES-IR ran (bemgpu_solve_stats then reports its Krylov steps and the
+ * relative residual ||b - A x|| / ||b||). */
+int bemgpu_set_refinement(bemgpu_ctx *ctx, int method);
+int bemgpu_refinement_used(bemgpu_ctx *ctx, int *gmres, int max);
 
 /* Refinement record of the last bemgpu_solve, one entry per dense system
  * (0: global system, 1 + d: dpv system of domain d): refinement steps, final
@@ -311,13 +325,15 @@ typedef struct bemgpu_result {
   long long id;        /* the id given to bemgpu_server_submit */
   int status;          /* 0, or the failing call's return code */
   int reused;          /* 1: solved with a resident factorisation (right-hand side only) */
+  int precision;       /* precision the request ran in (a mixed request whose footprint
+                          exceeds the budget runs in BEMGPU_FP64 when that fits) */
   double F[3], N[3];   /* force and torque */
   double queue_ms;     /* submit -> admitted to a slot */
   double service_ms;   /* admitted -> result */
   char error[160];
 } bemgpu_result;
 int bemgpu_server_create(int device, size_t hbm_budget, int slots, bemgpu_server **out);
-/* 0 queued; -2 the problem needs more than the whole budget */
+/* 0 queued; -2 the problem needs more than the whole budget (in FP64 too) */
 int bemgpu_server_submit(bemgpu_server *srv, const bemgpu_problem *prob, unsigned long long reuse_key, int precision,
                          int force_type, const double *rc, long long id);
 /* Up to max finished results; waits up to timeout_ms for the first one.  Returns the count. */

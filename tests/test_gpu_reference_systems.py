@@ -22,11 +22,17 @@ Tolerances (stated here, used below):
                                row's absolute sum
   P, dP, pv, dpv               1e-9 of the array maximum; weighted sums over all
                                elements 1e-9 of the weighted absolute sum
-  force, torque, field values  1e-9 relative (torque: of |N|, which carries the
-                               non-zero component; the near-zero components are
-                               covered by it)
-  9-point force on the mirror-symmetric meshes  TOL_RULE = 1e-7 (the reference's
-                               own lattice-plane rounding noise, test_gpu_fields.py)
+  field values, type-0 force   1e-9 relative
+  torque                       1e-9 of |F| times the body's radius (the torque
+                               is a small difference of large moments: its own
+                               relative error means nothing)
+  9-point force on the mirror-symmetric meshes (the cube-spheres, and the
+                               shipped gmsh spheres, whose 9-point targets share
+                               heights with other elements' points)
+                               TOL_RULE = 1e-7: the reference's own lattice-plane
+                               rounding noise (test_gpu_fields.py); measured on
+                               the shipped systems 3e-11 (ex), 9e-8 (verification),
+                               7e-12 (ex1)
 """
 import os
 import re
@@ -87,9 +93,10 @@ def parse_example1(text):
             "F0": np.array(vecs[0]), "N0": np.array(vecs[1]), "F1": np.array(vecs[2]), "N1": np.array(vecs[3])}
 
 
-def check_log_values(got, g, tol_force1=TOL, tol_print=0.0):
-    """got: dict as parse_example1 returns; g: the fixture.  tol_print adds the
-    rounding of 15 printed digits when got comes from printed text."""
+def check_log_values(got, g, radius, tol_force1=TOL_RULE, tol_print=0.0):
+    """got: dict as parse_example1 returns; g: the fixture; radius: the body's
+    size (torque scale).  tol_print adds the rounding of 15 printed digits when
+    got comes from printed text."""
     t = TOL + tol_print
     for k in ("p_t0", "p_t1"):
         assert abs(got[k] - g[k]) <= t * abs(g[k]), (k, got[k], g[k])
@@ -98,7 +105,15 @@ def check_log_values(got, g, tol_force1=TOL, tol_print=0.0):
     for ty, tf in (("0", t), ("1", tol_force1 + tol_print)):
         F, Fr, N, Nr = got["F" + ty], g["F" + ty], got["N" + ty], g["N" + ty]
         assert np.linalg.norm(F - Fr) <= tf * np.linalg.norm(Fr), ("F" + ty, F, Fr)
-        assert np.linalg.norm(N - Nr) <= tf * np.linalg.norm(Nr), ("N" + ty, N, Nr)
+        assert np.linalg.norm(N - Nr) <= tf * np.linalg.norm(Fr) * radius, ("N" + ty, N, Nr)
+
+
+def mesh_radius(g):
+    """Largest distance of a mesh node from the origin (the torque centre)."""
+    text = zlib.decompress(g["mesh_z"].tobytes()).decode().split("\n")
+    i = text.index("$Nodes")
+    pts = np.array([[float(x) for x in line.split()[1:4]] for line in text[i + 2:i + 2 + int(text[i + 1])]])
+    return float(np.max(np.linalg.norm(pts, axis=1)))
 
 
 def case_log_values(case):
@@ -148,7 +163,7 @@ def test_shipped_example1_values(shipped):
     """Field at example1.c's point and force / torque of both rules against
     the reference's example1.log of the same system."""
     name, case, g = shipped
-    check_log_values(case_log_values(case), g, tol_force1=TOL)
+    check_log_values(case_log_values(case), g, mesh_radius(g))
 
 
 # ---- the 216-quad benchmark configuration, solved by the reference
@@ -283,7 +298,7 @@ def test_reference_drivers_on_shipped_inputs():
     files = [os.path.basename(p) for p in write_shipped_inputs(g, d)]
     _run([solver] + files + ["out.dat"], d)
     got = parse_example1(_run([ex1, "out.dat"], d))
-    check_log_values(got, g, tol_force1=TOL, tol_print=1e-14)
+    check_log_values(got, g, mesh_radius(g), tol_print=1e-14)
 
 
 def test_dat_from_library_read_by_reference():
@@ -305,4 +320,4 @@ def test_dat_from_library_read_by_reference():
     theirs = parse_example1(env_out.stdout)
     # the reference's 9-point force on this mirror-symmetric mesh carries its
     # lattice-plane rounding noise (TOL_RULE)
-    check_log_values(ours, theirs, tol_force1=TOL_RULE, tol_print=1e-14)
+    check_log_values(ours, theirs, 0.3, tol_print=1e-14)
