@@ -59,6 +59,11 @@ def libs():
         g.bemgpu_set_far_rule.argtypes = [vp, ctypes.c_int]
         g.bemgpu_autotune.argtypes = [vp, _d]
         g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
+        g.bemgpu_set_interior_reuse.argtypes = [vp, ctypes.c_int]
+        g.bemgpu_interior_reuses.argtypes = [vp]
+        g.bemgpu_interior_reuses.restype = ctypes.c_longlong
+        g.bemgpu_kernel_launches.argtypes = []
+        g.bemgpu_kernel_launches.restype = ctypes.c_ulonglong
         h.read_aqd2.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), vp]
         for name in ("print_aqd2", "initialize_aqd2", "finalize_aqd2", "solve_bieq_aqd2"):
             getattr(h, name).argtypes = [vp]
@@ -218,7 +223,7 @@ class Case:
         self._check(libs()[1].bemgpu_run(self.ctx), "bemgpu_run")
 
     def set_precision(self, mode):
-        """0 FP64 LU; 1 FP32, 2 TF32, 3 BF16x9, 4 BF16 LU updates with FP64 refinement."""
+        """0 FP64 LU; 1 FP32, 2 TF32, 3 TF32x3 (three split TF32 products), 4 as 2 with FP64 refinement."""
         self._check(libs()[1].bemgpu_set_precision(self.ctx, int(mode)), "set_precision")
 
     def autotune(self):

@@ -17,6 +17,7 @@
 //   self      singular polar quadrature on the collocation element, one block
 //             per collocation node
 //   diag      adds (1+)F to the diagonal of H and writes dF
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "bem_qpgf.cuh"
@@ -1512,11 +1513,13 @@ __global__ void k_stab_build(const __grid_constant__ bem_qp q, double ve, double
 extern "C" int bem_launch_stab(const bem_qp *q, double *out, cudaStream_t st) {
   if (q->st_n1cnt <= 0 || q->st_n2cnt <= 0 || q->st_nint <= 0) return 0;
   k_stab_build<<<dim3(q->st_n1cnt * q->st_n2cnt, q->st_nint), BEM_ST_DEG, 0, st>>>(*q, q->eta_run, out);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st) {
   k_wtab_build<<<BEM_WT_N, BEM_WT_DEG, 0, st>>>(k, ve, out);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -1555,12 +1558,14 @@ extern "C" int bem_set_constants(const double *xl, const double *wl, const doubl
 extern "C" int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st) {
   if (n <= 0) return 0;
   k_faddeeva<<<(n + 127) / 128, 128, 0, st>>>(z, n, w);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_qpgf(const bem_qp *q, const double *r, int n, double *G, double *dG, int *ret, cudaStream_t st) {
   if (n <= 0) return 0;
   k_qpgf_points<<<(n + 127) / 128, 128, 0, st>>>(*q, r, n, G, dG, ret);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -1598,6 +1603,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   if (ev) cudaEventRecord(ev[0], st);
   k_classify<<<N, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
                                 lists ? S->plist : nullptr, S->pcount, S->pcap);
+  bem_count_launches(1);
   if (ev) cudaEventRecord(ev[1], st);
   if (periodic) {
     if (lists) {
@@ -1610,10 +1616,15 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       const bem_plist Lreg = {S->plist, S->pcount, 1};
       const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
       k_q0_regular<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
-      if (D->far_rule)
+      bem_count_launches(1);
+      if (D->far_rule) {
         k_q0_far<<<grid, FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lfar);
-      if (D->has_tri)
+        bem_count_launches(1);
+      }
+      if (D->has_tri) {
         k_q0_regular_tri<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
+        bem_count_launches(1);
+      }
     } else {
       const bem_plist L0 = {nullptr, nullptr, 0};
       const long long chunk = 1LL << 26;  // keep grid.x well inside limits
@@ -1621,29 +1632,46 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
         const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
         k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                       L0);
-        if (D->far_rule)
+        bem_count_launches(1);
+        if (D->far_rule) {
           k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                     L0);
-        if (D->has_tri)
+          bem_count_launches(1);
+        }
+        if (D->has_tri) {
           k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                             p0, np, L0);
+          bem_count_launches(1);
+        }
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
     k_q0_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
+    bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
     k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
-    if (D->has_tri) k_q0_self_tri<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+    bem_count_launches(1);
+    if (D->has_tri) {
+      k_q0_self_tri<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+      bem_count_launches(1);
+    }
   } else {
     k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
+    bem_count_launches(1);
     if (ev) cudaEventRecord(ev[2], st);
     k_fs_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
+    bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
     k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
-    if (D->has_tri) k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+    bem_count_launches(1);
+    if (D->has_tri) {
+      k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+      bem_count_launches(1);
+    }
   }
   if (ev) cudaEventRecord(ev[4], st);
   k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, exterior, S->rowF, S->near_n, S->nearF, S->selfF, H, dF, S->status);
+  bem_count_launches(1);
   if (ev) cudaEventRecord(ev[5], st);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1667,12 +1695,17 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
       const bem_plist L0 = {nullptr, nullptr, 0};
       k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                     L0);
-      if (D->far_rule)
+      bem_count_launches(1);
+      if (D->far_rule) {
         k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                   L0);
-      if (D->has_tri)
+        bem_count_launches(1);
+      }
+      if (D->has_tri) {
         k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                           p0, np, L0);
+        bem_count_launches(1);
+      }
     }
   }
   cudaEventRecord(e1, st);
@@ -1687,6 +1720,7 @@ extern "C" int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int pe
   if (D->ne <= 0) return 0;
   k_classify<<<D->ne * 4, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
                                         nullptr, nullptr, 0);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 

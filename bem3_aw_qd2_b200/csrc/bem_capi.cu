@@ -14,6 +14,8 @@
 #include "bem_lattice.h"
 #include "bem_mixed.h"
 #include "bem_lu.h"
+#include "bem_count.h"
+#include <atomic>
 
 #define BEMGPU_MAXDOM 8
 
@@ -102,6 +104,7 @@ struct bemgpu_ctx {
   // and dpv factorisation of the interior domains are skipped.
   std::vector<unsigned char> int_data;
   bool int_valid = false, int_reuse = false;
+  bool int_reuse_on = true;  // bemgpu_set_interior_reuse
   bool int_factored[BEMGPU_MAXDOM] = {};
   long long int_reused_loads = 0;
 };
@@ -368,7 +371,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     put(pr->ren, sizeof(double) * 12 * ne); put(pr->wen, sizeof(double) * 12 * ne);
     put(pr->npe, sizeof(int) * ne); put(pr->plane, ne);
     put(pr->k0 + 1, sizeof(double) * pr->MN);
-    c->int_reuse = pr->MN >= 1 && c->int_valid && idata == c->int_data;
+    c->int_reuse = c->int_reuse_on && pr->MN >= 1 && c->int_valid && idata == c->int_data;
     if (!c->int_reuse) {
       c->int_valid = false;
       for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
@@ -758,7 +761,7 @@ static int dense_apply(bemgpu_ctx *c, int slot, double *M, int64_t n, int64_t nr
 }
 
 extern "C" int bemgpu_set_precision(bemgpu_ctx *c, int mode) {
-  if (mode < 0 || mode > BEM_MIXED_BF16) { snprintf(c->err, sizeof(c->err), "precision mode %d (0..4)", mode); return -2; }
+  if (mode < 0 || mode > BEM_MIXED_FAST) { snprintf(c->err, sizeof(c->err), "precision mode %d (0..4)", mode); return -2; }
   c->precision = mode;
   c->factored = false;  // factors of the other precision are not reused
   for (int d = 0; d < BEMGPU_MAXDOM; ++d) c->int_factored[d] = false;
@@ -1271,6 +1274,22 @@ extern "C" int bemgpu_zgesv(int device, int n, int nrhs, const double *A, double
 }
 
 extern "C" long long bemgpu_interior_reuses(bemgpu_ctx *c) { return c ? c->int_reused_loads : -1; }
+
+extern "C" int bemgpu_set_interior_reuse(bemgpu_ctx *c, int on) {
+  if (!c) return -2;
+  c->int_reuse_on = on != 0;
+  if (!c->int_reuse_on) {
+    // the next load assembles and factors every domain
+    c->int_valid = false;
+    c->int_reuse = false;
+    c->int_data.clear();
+  }
+  return 0;
+}
+
+static std::atomic<unsigned long long> g_launches{0};
+extern "C" void bem_count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+extern "C" unsigned long long bemgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 extern "C" cudaError_t bem_launch_transform(int ne, const double *rv, double th, const double *tv, double *cr,
                                             double *cw, double *ren, double *wen, double *Pi, double *dPi,

@@ -1,7 +1,7 @@
 // GMRES-based iterative refinement (GMRES-IR) of a dense complex system with
 // low-precision LU factors as the preconditioner: the FP64 accuracy of the
 // mixed-precision solves when plain refinement converges slowly or not at all
-// (factors of a TF32 or BF16 trailing update, or an ill-conditioned system).
+// (factors of a TF32 trailing update, or an ill-conditioned system).
 // No counterpart in the reference, whose solves are FP64 throughout
 // (b_mkl_solver_pardiso_d, d3qd2_mkl_solver.c:18-148).
 //
@@ -11,6 +11,7 @@
 // Gram-Schmidt, applied twice); x += d.  Each Krylov step is one FP64 matvec
 // with A, one FP32 solve with the factors, and two projection passes; the
 // small least-squares problem (Givens rotations) is solved on the host.
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>
@@ -162,6 +163,7 @@ static int gm_grow(bem_gmres *g, int n) {
 static int gm_norm2(bem_gmres *g, const double2 *a, int n, double *out, cudaStream_t st) {
   CKG(cudaMemsetAsync(g->h, 0, 2 * sizeof(double), st));
   k_gm_dots<<<blocks_for(n), GM_TH, 0, st>>>(a, n, 1, a, g->h);
+  bem_count_launches(1);
   double hv[2];
   CKG(cudaMemcpyAsync(hv, g->h, sizeof(hv), cudaMemcpyDeviceToHost, st));
   CKG(cudaStreamSynchronize(st));
@@ -188,6 +190,7 @@ extern "C" int bem_gmres_ir(bem_gmres *g, const double *Ad, int n, const double 
   for (; outer < max_outer; ++outer) {
     // r = b - A x, its size against b
     k_gm_resid<<<rows_b, 256, 0, st>>>(A, n, x, b, g->r);
+    bem_count_launches(1);
     CKG(cudaGetLastError());
     double rn2 = 0.0;
     if (gm_norm2(g, g->r, n, &rn2, st)) return -1;
@@ -204,12 +207,14 @@ extern "C" int bem_gmres_ir(bem_gmres *g, const double *Ad, int n, const double 
     const double beta = sqrt(z2);
     if (!(beta > 0.0) || !(beta <= DBL_MAX)) break;
     k_gm_scale<<<nb, GM_TH, 0, st>>>(g->V, g->w, n, 1.0 / beta);
+    bem_count_launches(1);
     std::vector<zc> H((size_t)(m + 1) * m), cs(m), sn(m), e(m + 1);
     e[0] = beta;
     int j = 0;
     for (; j < m; ++j) {
       // w = M^-1 A v_j
       k_gm_matvec<<<rows_b, 256, 0, st>>>(A, n, g->V + (size_t)j * n, g->r);
+      bem_count_launches(1);
       if (precond(pctx, g->r, g->w, st)) {
         snprintf(g->err, sizeof(g->err), "GMRES-IR: preconditioner solve failed");
         return -1;
@@ -219,7 +224,9 @@ extern "C" int bem_gmres_ir(bem_gmres *g, const double *Ad, int n, const double 
       for (int pass = 0; pass < 2; ++pass) {
         CKG(cudaMemsetAsync(g->h, 0, 2 * (j + 1) * sizeof(double), st));
         k_gm_dots<<<nb, GM_TH, 0, st>>>(g->V, n, j + 1, g->w, g->h);
+        bem_count_launches(1);
         k_gm_project<<<nb, GM_TH, 0, st>>>(g->V, n, j + 1, g->h, g->w);
+        bem_count_launches(1);
         std::vector<double> hv(2 * (j + 1));
         CKG(cudaMemcpyAsync(hv.data(), g->h, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CKG(cudaStreamSynchronize(st));
@@ -248,7 +255,10 @@ extern "C" int bem_gmres_ir(bem_gmres *g, const double *Ad, int n, const double 
       e[j + 1] = -std::conj(sn[j]) * e[j];
       e[j] = cs[j] * e[j];
       const bool done = std::abs(e[j + 1]) <= 0.01 * tol * beta || !(hj1 > 0.0);
-      if (j + 1 < m && hj1 > 0.0) k_gm_scale<<<nb, GM_TH, 0, st>>>(g->V + (size_t)(j + 1) * n, g->w, n, 1.0 / hj1);
+      if (j + 1 < m && hj1 > 0.0) {
+        k_gm_scale<<<nb, GM_TH, 0, st>>>(g->V + (size_t)(j + 1) * n, g->w, n, 1.0 / hj1);
+        bem_count_launches(1);
+      }
       if (done) { ++j; break; }
     }
     // y = R^-1 e (back substitution), x += V y
@@ -262,6 +272,7 @@ extern "C" int bem_gmres_ir(bem_gmres *g, const double *Ad, int n, const double 
     for (int i = 0; i < j; ++i) { yh[2 * i] = yv[i].real(); yh[2 * i + 1] = yv[i].imag(); }
     CKG(cudaMemcpyAsync(g->y, yh.data(), yh.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     k_gm_combine<<<nb, GM_TH, 0, st>>>(g->V, n, j, g->y, x);
+    bem_count_launches(1);
     CKG(cudaGetLastError());
   }
   *outer_steps = outer;

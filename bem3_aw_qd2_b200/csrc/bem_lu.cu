@@ -25,11 +25,13 @@
 //
 // The sequence of a size and matrix is captured once as a CUDA graph and
 // replayed.  Solves: forward substitution L y = P b and back substitution
-// U x = y in one launch each, one CTA per 32-row block; a block waits for the
-// blocks it needs through flags in global memory (bounded waits: a wait that
+// U x = y in one launch each, one CTA per 32-row block; blocks are written in
+// dependency order and a block folds in each block it needs as soon as a
+// progress counter in global memory has passed it (bounded waits: a wait that
 // gives up sets BEM_LU_ST_WAIT and the call reports it; nothing hangs).  The
 // launches are cooperative, so every CTA is resident and blocks are taken in
 // order: the waits cannot deadlock.
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -679,36 +681,49 @@ __device__ __forceinline__ unsigned long long gtimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// wait until *f != 0: a tight spin for the first 20 us (a flag normally
-// arrives within a few), then polls with short sleeps; after one second it
-// gives up with BEM_LU_ST_WAIT set, and once any wait has given up later
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// the two counters (lower, upper solve) sit 128 bytes apart
+#define TS_FSTRIDE 32
+// wait until *cnt > k and return the count seen: a spin of relaxed loads with
+// an acquire fence once it has moved past k; after one second it gives up with
+// BEM_LU_ST_WAIT set (and returns k + 1), and once any wait has given up later
 // waits return at once
-__device__ __forceinline__ void wait_flag(const unsigned *f, unsigned *status) {
-  if (ld_acquire(f)) return;
+__device__ __forceinline__ unsigned wait_count(const unsigned *cnt, unsigned k, unsigned *status) {
+  unsigned c = ld_acquire(cnt);
+  if (c > k) return c;
   const unsigned long long t0 = gtimer();
   for (unsigned it = 1;; ++it) {
-    if (ld_acquire(f)) return;
-    if ((it & 63) == 0) {
-      const unsigned long long dt = gtimer() - t0;
-      if (dt > TS_WAIT_NS || (ld_acquire(status) & BEM_LU_ST_WAIT)) {
-        atomicOr(status, BEM_LU_ST_WAIT);
-        return;
-      }
-      if (dt > 20000ull) __nanosleep(256);
+    c = ld_relaxed(cnt);
+    if (c > k) {
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      return c;
+    }
+    if ((it & 255) == 0 && (gtimer() - t0 > TS_WAIT_NS || (ld_relaxed(status) & BEM_LU_ST_WAIT))) {
+      atomicOr(status, BEM_LU_ST_WAIT);
+      return k + 1;
     }
   }
 }
 
 // lower = 1: out = L^-1 (P in), in read through rowmap (unit lower L);
-// lower = 0: out = U^-1 in.  in / out are n x NR column-major; block b of out
-// is published through flags[b] once written.
+// lower = 0: out = U^-1 in.  in / out are n x NR column-major.  The 32-row
+// blocks are solved in dependency order (top down for L, bottom up for U): the
+// block of position it needs the blocks of positions 0 .. it-1, each of which
+// it folds in as soon as *cnt (the number of blocks written so far, which
+// grows in position order) has passed it.
 template <class C2, int NR>
 __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const C2 *LU, long lda, int n, const int *rowmap, const C2 *in,
-                                                   C2 *out, unsigned *flags, int lower, unsigned *status) {
+                                                   C2 *out, unsigned *cnt, int lower, unsigned *status) {
   __shared__ C2 sd[32][33];
   __shared__ C2 sacc[4][32][NR];
+  __shared__ unsigned sready[2];
   const int nb = (n + 31) / 32;
   const int t = threadIdx.x, r = t & 31, s = t >> 5;
+  unsigned nwait = 0;
   for (int it = blockIdx.x; it < nb; it += gridDim.x) {
     const int b = lower ? it : nb - 1 - it;
     const int r0 = b * 32, rows = min(32, n - r0);
@@ -725,23 +740,38 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const C2 *LU, long lda, int n
 #pragma unroll
       for (int q = 0; q < NR; ++q) acc[q] = in[(size_t)q * n + src];
     }
-    const int jlo = lower ? 0 : b + 1, jhi = lower ? b : nb;
-    // the factor's entries do not depend on the other blocks: the next
-    // block's eight are loaded before the wait for the current one's flag
+    // dependency k is the block of position k: rows/columns jb * 32 ..
+    // jb * 32 + 31 with jb = k (lower) or nb - 1 - k (upper).  The factor's
+    // entries do not depend on the other blocks, so dependency k + 1's eight
+    // are loaded before the wait for dependency k.
     const C2 *arow = LU + (size_t)(r < rows ? row : r0) * lda;
     C2 ac[8], an[8];
-#pragma unroll
-    for (int cc = 0; cc < 8; ++cc) {
-      const int col = jlo * 32 + s * 8 + cc;
-      ac[cc] = (jlo < jhi && r < rows && col < n) ? arow[col] : czero<C2>();
-    }
-    for (int jb = jlo; jb < jhi; ++jb) {
+    {
+      const int jb = lower ? 0 : nb - 1;
 #pragma unroll
       for (int cc = 0; cc < 8; ++cc) {
-        const int col = (jb + 1) * 32 + s * 8 + cc;
-        an[cc] = (jb + 1 < jhi && r < rows && col < n) ? arow[col] : czero<C2>();
+        const int col = jb * 32 + s * 8 + cc;
+        ac[cc] = (it > 0 && r < rows && col < n) ? arow[col] : czero<C2>();
       }
-      wait_flag(flags + jb, status);
+    }
+    unsigned ready = 0;
+    for (int k = 0; k < it; ++k) {
+      const int jb = lower ? k : nb - 1 - k, jn = lower ? k + 1 : nb - 2 - k;
+#pragma unroll
+      for (int cc = 0; cc < 8; ++cc) {
+        const int col = jn * 32 + s * 8 + cc;
+        an[cc] = (k + 1 < it && r < rows && col < n) ? arow[col] : czero<C2>();
+      }
+      if ((unsigned)k >= ready) {
+        // one thread polls (all threads polling one line starve the block
+        // that publishes it); the barrier passes its acquire on.  The two
+        // slots alternate so a slot is rewritten only after every thread has
+        // passed the barrier that follows its read.
+        if (t == 0) sready[nwait & 1] = wait_count(cnt, (unsigned)k, status);
+        __syncthreads();
+        ready = sready[nwait & 1];
+        ++nwait;
+      }
       const int c0 = jb * 32 + s * 8;
 #pragma unroll
       for (int cc = 0; cc < 8; ++cc) {
@@ -789,7 +819,7 @@ __global__ void __launch_bounds__(TS_TH) k_lu_trsv(const C2 *LU, long lda, int n
         for (int q = 0; q < NR; ++q) out[(size_t)q * n + row] = acc[q];
       __threadfence();
       __syncwarp();
-      if (r == 0) st_release(flags + b, 1u);
+      if (r == 0) st_release(cnt, (unsigned)it + 1u);
     }
     __syncthreads();
   }
@@ -866,7 +896,8 @@ static int tc_update(bem_lu *w, float2 *A, int n, int k, int wd, cudaStream_t st
   return 1;
 }
 
-// the launches of one factorisation, in order (captured into the graph)
+// the launches of one factorisation, in order (captured into the graph, whose
+// replays count them)
 template <class C2>
 static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
   k_lu_iota<<<(n + 255) / 256, 256, 0, st>>>(w->rowmap, n);
@@ -907,11 +938,15 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
     CKL(ce, "LU capture");
     w->graph = g;
     CKL(cudaGraphInstantiate(&w->gexec, g, 0), "LU graph");
+    size_t nodes = 0;
+    CKL(cudaGraphGetNodes(g, nullptr, &nodes), "LU graph");
+    w->g_nodes = nodes;
     w->g_A = Av;
     w->g_n = n;
     w->g_tc = tcmode;
   }
   CKL(cudaGraphLaunch(w->gexec, st), "LU graph launch");
+  bem_count_launches(w->g_nodes);
   return 0;
 }
 
@@ -934,6 +969,7 @@ static int launch_trsv(bem_lu *w, const C2 *LU, int n, const C2 *in, C2 *out, un
   CKL(cudaLaunchKernelEx(&cfg, k_lu_trsv<C2, NR>, LU, (long)n, n, (const int *)w->rowmap, in, out, flags, lower,
                          w->status),
       "triangular solve");
+  bem_count_launches(1);
   return 0;
 }
 
@@ -944,19 +980,18 @@ static int lu_solve(bem_lu *w, const void *LUv, int n, int nrhs, void *Bv, cudaS
     snprintf(w->err, sizeof(w->err), "LU solve: %d right-hand sides (1..4)", nrhs);
     return -1;
   }
-  const int nb = (n + 31) / 32;
-  if (grow_bytes(w, (void **)&w->flags, &w->flags_cap, 2 * (size_t)nb * sizeof(unsigned), "solve flags") ||
+  if (grow_bytes(w, (void **)&w->flags, &w->flags_cap, 2 * TS_FSTRIDE * sizeof(unsigned), "solve flags") ||
       grow_bytes(w, &w->y, &w->y_cap, (size_t)n * nrhs * sizeof(C2), "solve scratch"))
     return -1;
   const C2 *LU = (const C2 *)LUv;
   C2 *B = (C2 *)Bv, *Y = (C2 *)w->y;
-  CKL(cudaMemsetAsync(w->flags, 0, 2 * (size_t)nb * sizeof(unsigned), st), "solve flags");
+  CKL(cudaMemsetAsync(w->flags, 0, 2 * TS_FSTRIDE * sizeof(unsigned), st), "solve flags");
   int rc = 0;
   switch (nrhs) {
-    case 1: rc = launch_trsv<C2, 1>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 1>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    case 2: rc = launch_trsv<C2, 2>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 2>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    case 3: rc = launch_trsv<C2, 3>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 3>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
-    default: rc = launch_trsv<C2, 4>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 4>(w, LU, n, Y, B, w->flags + nb, 0, st); break;
+    case 1: rc = launch_trsv<C2, 1>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 1>(w, LU, n, Y, B, w->flags + TS_FSTRIDE, 0, st); break;
+    case 2: rc = launch_trsv<C2, 2>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 2>(w, LU, n, Y, B, w->flags + TS_FSTRIDE, 0, st); break;
+    case 3: rc = launch_trsv<C2, 3>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 3>(w, LU, n, Y, B, w->flags + TS_FSTRIDE, 0, st); break;
+    default: rc = launch_trsv<C2, 4>(w, LU, n, B, Y, w->flags, 1, st) || launch_trsv<C2, 4>(w, LU, n, Y, B, w->flags + TS_FSTRIDE, 0, st); break;
   }
   return rc ? -1 : 0;
 }
@@ -974,10 +1009,10 @@ extern "C" int bem_lu_resid_z(const double *A, int n, int nrhs, const double *X,
   const double2 *a = (const double2 *)A, *x = (const double2 *)X, *b = (const double2 *)B;
   double2 *r = (double2 *)R;
   switch (nrhs) {
-    case 1: k_resid_z<1><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
-    case 2: k_resid_z<2><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
-    case 3: k_resid_z<3><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
-    case 4: k_resid_z<4><<<blocks, 256, 0, st>>>(a, n, x, b, r); break;
+    case 1: k_resid_z<1><<<blocks, 256, 0, st>>>(a, n, x, b, r); bem_count_launches(1); break;
+    case 2: k_resid_z<2><<<blocks, 256, 0, st>>>(a, n, x, b, r); bem_count_launches(1); break;
+    case 3: k_resid_z<3><<<blocks, 256, 0, st>>>(a, n, x, b, r); bem_count_launches(1); break;
+    case 4: k_resid_z<4><<<blocks, 256, 0, st>>>(a, n, x, b, r); bem_count_launches(1); break;
     default: return -1;
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;

@@ -19,7 +19,7 @@ struct bem_lu {
   int *piv = nullptr;       // panel scratch: selected pivot rows, candidates, permutation list
   void *u11 = nullptr;      // panel scratch: packed L11\U11, inverse of U11, inverse of L11, staged rows
   unsigned *status = nullptr;
-  unsigned *flags = nullptr;  // triangular-solve readiness flags, 2 x ceil(n / 32)
+  unsigned *flags = nullptr;  // triangular-solve progress counters (lower, upper), 128 bytes apart
   size_t flags_cap = 0;
   void *y = nullptr;          // triangular-solve intermediate (n x nrhs complex)
   size_t y_cap = 0;
@@ -28,6 +28,7 @@ struct bem_lu {
   cudaGraphExec_t gexec = nullptr;
   const void *g_A = nullptr;
   int g_n = 0, g_tc = -1;
+  size_t g_nodes = 0;   // kernels in the captured graph (launch count per replay)
   bem_tc *tc = nullptr;       // complex FP32 only: trailing updates on the tensor cores when set
   int sms = 0, coop_blocks = 0;  // device facts for the launches
   char err[200] = {0};

@@ -13,6 +13,7 @@
 // is below the tolerance, stops shrinking, or grows (the caller then falls
 // back to FP64 factors).  FP64 stays in the assembly, the residuals and the
 // updates.
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -106,6 +107,7 @@ extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream
   const size_t count = (size_t)n * n;
   if (grow(m, &m->M, &m->M_cap, count)) return -1;
   k_round_c32<<<grid_for(count), 256, 0, st>>>((const double2 *)A, m->M, count);
+  bem_count_launches(1);
   CKC(cudaGetLastError());
   // trailing updates: mode 1 on the CUDA cores; 2 and 4 one TF32 product, 3
   // three split products on the tensor cores (buffers and TMA maps prepared
@@ -113,10 +115,10 @@ extern "C" int bem_mixed_factor(bem_mixed *m, const double *A, int n, cudaStream
   m->lu.tc = nullptr;
   m->mode = BEM_MIXED_FP32;
   if (m->req_mode >= BEM_MIXED_TF32) {
-    const int nprod = m->req_mode == BEM_MIXED_BF16X9 ? 3 : 1;
+    const int nprod = m->req_mode == BEM_MIXED_TF32X3 ? 3 : 1;
     if (bem_tc_prepare(&m->tc, n, nprod) == 0) {
       m->lu.tc = &m->tc;
-      m->mode = nprod == 3 ? BEM_MIXED_BF16X9 : BEM_MIXED_TF32;
+      m->mode = nprod == 3 ? BEM_MIXED_TF32X3 : BEM_MIXED_TF32;
     }
   }
   if (bem_lu_factor_c(&m->lu, (float *)m->M, n, st)) {
@@ -137,6 +139,7 @@ extern "C" int bem_mixed_solve(bem_mixed *m, const double *A, int n, int nrhs, d
   for (; it < max_iter; ++it) {
     // correction d = A^-1 r from the FP32 factors
     k_round_c32<<<grid_for(cnt), 256, 0, st>>>(m->R, m->R32, cnt);
+    bem_count_launches(1);
     CKC(cudaGetLastError());
     if (bem_lu_solve_c(&m->lu, (const float *)m->M, n, nrhs, (float *)m->R32, st)) {
       snprintf(m->err, sizeof(m->err), "%s", m->lu.err);
@@ -144,6 +147,7 @@ extern "C" int bem_mixed_solve(bem_mixed *m, const double *A, int n, int nrhs, d
     }
     CKC(cudaMemsetAsync(m->norms, 0, 2 * sizeof(unsigned long long), st));
     k_axpy_norms<<<grid_for(cnt), 256, 0, st>>>(m->X, m->R32, cnt, m->norms);
+    bem_count_launches(1);
     CKC(cudaGetLastError());
     // r = b - A x in FP64
     if (bem_lu_resid_z(A, n, nrhs, (const double *)m->X, B, (double *)m->R, st)) {
@@ -179,8 +183,10 @@ static int mixed_precond(void *pctx, const double2 *r, double2 *z, cudaStream_t 
   bem_mixed *m = (bem_mixed *)pctx;
   const int n = m->gm_n;
   k_round_c32<<<grid_for((size_t)n), 256, 0, st>>>(r, m->R32, (size_t)n);
+  bem_count_launches(1);
   if (bem_lu_solve_c(&m->lu, (const float *)m->M, n, 1, (float *)m->R32, st)) return -1;
   k_widen<<<grid_for((size_t)n), 256, 0, st>>>(m->R32, z, n);
+  bem_count_launches(1);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

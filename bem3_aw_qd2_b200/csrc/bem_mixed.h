@@ -10,8 +10,8 @@
 // mode in effect is in bem_mixed.mode
 #define BEM_MIXED_FP32 1    // FP32 CUDA cores
 #define BEM_MIXED_TF32 2    // one TF32 product on the tensor cores (tcgen05), FP32 accumulation
-#define BEM_MIXED_BF16X9 3  // FP32-accurate: three split TF32 products on the tensor cores
-#define BEM_MIXED_BF16 4    // a single low-precision product: runs as mode 2
+#define BEM_MIXED_TF32X3 3  // FP32-accurate: three split TF32 products on the tensor cores
+#define BEM_MIXED_FAST 4    // a single low-precision product: runs as mode 2
 
 struct bem_mixed {
   int req_mode = 0;          // arithmetic asked for (bemgpu_set_precision)

@@ -15,6 +15,7 @@
 //   k_force0       radiation force and torque, 4-point rule at the element
 //                  nodes (force_FN_aqd2 + bil_force_4p, bem3_aw_qd2_force.c:4-120)
 // The LU factorisations themselves run in cuSOLVER (bem_capi.cu).
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "bem_solve.h"
@@ -336,8 +337,12 @@ extern "C" int bem_launch_gather(const bem_sys_dev *S, int d, const double *G, c
                                  cudaStream_t st) {
   const long long Nd = (long long)S->dom_ne_h[d] * 4;
   if (Nd == 0) return 0;
-  if (A) k_gather<<<(unsigned)((Nd * Nd + 255) / 256), 256, 0, st>>>(*S, d, G, H, A);
+  if (A) {
+    k_gather<<<(unsigned)((Nd * Nd + 255) / 256), 256, 0, st>>>(*S, d, G, H, A);
+    bem_count_launches(1);
+  }
   k_rhs<<<(unsigned)((Nd + 7) / 8), 256, 0, st>>>(*S, d, G, H, b);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -345,6 +350,7 @@ extern "C" int bem_launch_store(const bem_sys_dev *S, int d, const double *X, do
   const int n = S->dom_ne_h[d] * 4;
   if (n == 0) return 0;
   k_store<<<(n + 127) / 128, 128, 0, st>>>(*S, d, X, P, dP);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -352,20 +358,27 @@ extern "C" int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, cons
                              const double *P, const double *dP, double *pv, double *tpv, cudaStream_t st) {
   const int n = S->dom_ne_h[d] * 4;
   if (n == 0) return 0;
-  if (d == 0) k_pv_exterior<<<(n + 127) / 128, 128, 0, st>>>(*S, tpv, pv);
-  else k_pv_interior<<<(n + 7) / 8, 256, 0, st>>>(*S, d, dG, dH, dF, P, dP, pv, tpv);
+  if (d == 0) {
+    k_pv_exterior<<<(n + 127) / 128, 128, 0, st>>>(*S, tpv, pv);
+    bem_count_launches(1);
+  } else {
+    k_pv_interior<<<(n + 7) / 8, 256, 0, st>>>(*S, d, dG, dH, dF, P, dP, pv, tpv);
+    bem_count_launches(1);
+  }
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_dpv_rhs(int Nd, const double *H, const double *pv, double *B, cudaStream_t st) {
   if (Nd == 0) return 0;
   k_dpv_rhs<<<(Nd + 7) / 8, 256, 0, st>>>(Nd, H, pv, B);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_dpv_store(int Nd, const double *B, double *dpv, cudaStream_t st) {
   if (Nd == 0) return 0;
   k_dpv_store<<<(Nd + 127) / 128, 128, 0, st>>>(Nd, B, dpv);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -373,6 +386,7 @@ extern "C" int bem_launch_compress(const double *G, int N, const int *inv, int n
   const long long n2 = (long long)nn * nn;
   if (n2 == 0) return 0;
   k_compress_mat<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(G, N, inv, nn, Gc);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -380,9 +394,12 @@ extern "C" int bem_launch_rows(const double *src, double *dst, int N, const int 
                                cudaStream_t st) {
   if (to_full) {
     k_move_rows<<<(N + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs, 1);
+    bem_count_launches(1);
     k_scatter_rows<<<(nn + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs);
+    bem_count_launches(1);
   } else {
     k_move_rows<<<(nn + 127) / 128, 128, 0, st>>>(src, dst, N, inv, nn, nrhs, 0);
+    bem_count_launches(1);
   }
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
@@ -391,5 +408,6 @@ extern "C" int bem_launch_force0(const bem_sys_dev *S, const double *P0, const d
                                  double rho0, const int *ctr, const double *cbd, const double *pw, double *out,
                                  cudaStream_t st) {
   k_force0<<<1, 256, 0, st>>>(*S, P0, pv0, rc, c0, rho0, ctr, cbd, pw, out);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }

@@ -14,6 +14,7 @@
 // rounding, and evaluates the incident plane wave at the new collocation
 // nodes with the formulas of calc_apw_pv / calc_apw_dpdn.  Whether an element
 // is plane does not change under a rotation.
+#include "bem_count.h"
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -117,5 +118,6 @@ extern "C" cudaError_t bem_launch_transform(int ne, const double *rv, double th,
   const double den = k2[0] * k2[0] + k2[1] * k2[1];
   const double2 cp = make_double2(-k2[0] / den, k2[1] / den);
   k_transform<<<(ne + 127) / 128, 128, 0, st>>>(ne, X, cr, cw, ren, wen, Pi, dPi, p_inc, v_inc, pw_d, cp);
+  bem_count_launches(1);
   return cudaGetLastError();
 }

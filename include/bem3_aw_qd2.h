@@ -150,7 +150,7 @@ void calc_apw_dpdn(double complex *p, double complex *dpdn, double *r, double *n
 /* GPU device used by solve_bieq_aqd2 / force_FN_aqd2 (default 0). */
 void aqd2_set_device(int device);
 /* Precision of the dense solves of contexts created afterwards (bemgpu.h
- * BEMGPU_FP64 .. BEMGPU_MIXED_BF16; default 0, or the AQD2_PRECISION
+ * BEMGPU_FP64 .. BEMGPU_MIXED_FAST; default 0, or the AQD2_PRECISION
  * environment variable). */
 void aqd2_set_precision(int mode);
 /* 0: solve_bieq_aqd2 prints nothing (default 1: the reference's progress lines). */

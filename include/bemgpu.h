@@ -117,6 +117,14 @@ int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
  * those matrices and factors and the next bemgpu_assemble / bemgpu_solve skip
  * them.  Returns the number of loads that did so. */
 long long bemgpu_interior_reuses(bemgpu_ctx *ctx);
+/* Interior-domain reuse on (1, the default) or off (0: every load assembles
+ * and factors every domain, as the reference does). */
+int bemgpu_set_interior_reuse(bemgpu_ctx *ctx, int on);
+
+/* Kernel launches of this library in this process so far, all contexts and
+ * threads (no counterpart in the reference): every launch counts one, a
+ * replay of a captured factorisation counts its kernels. */
+unsigned long long bemgpu_kernel_launches(void);
 
 /* Rotation and translation of the loaded body on the device (the
  * reference's Rodrigues options of read_aqd2, bem3_aw_qd2.c:16-24, 395-422:
@@ -206,9 +214,9 @@ int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t,
  *   1 BEMGPU_MIXED_FP32   complex FP32 LU, FP32 CUDA-core trailing updates
  *   2 BEMGPU_MIXED_TF32   complex FP32 LU, trailing updates as one TF32
  *                         product on the tensor cores (tcgen05)
- *   3 BEMGPU_MIXED_BF16X9 complex FP32 LU, trailing updates as three split
+ *   3 BEMGPU_MIXED_TF32X3 complex FP32 LU, trailing updates as three split
  *                         TF32 products on the tensor cores (FP32-accurate)
- *   4 BEMGPU_MIXED_BF16   a single low-precision tensor-core product: mode 2
+ *   4 BEMGPU_MIXED_FAST   a single low-precision tensor-core product: mode 2
  * Modes 1-4 refine in FP64 against the FP64 matrix until the correction is
  * below 1e-15 of the solution; a system that does not get below 1e-12 is
  * solved again in FP64 (reported by bemgpu_solve_stats).  A mode whose
@@ -217,8 +225,8 @@ int bemgpu_boundary_field(bemgpu_ctx *ctx, int d, int type, int n, const int *t,
 #define BEMGPU_FP64 0
 #define BEMGPU_MIXED_FP32 1
 #define BEMGPU_MIXED_TF32 2
-#define BEMGPU_MIXED_BF16X9 3
-#define BEMGPU_MIXED_BF16 4
+#define BEMGPU_MIXED_TF32X3 3
+#define BEMGPU_MIXED_FAST 4
 int bemgpu_set_precision(bemgpu_ctx *ctx, int mode);
 /* The mode in effect (see bemgpu_set_precision). */
 int bemgpu_get_precision(bemgpu_ctx *ctx);

@@ -124,7 +124,7 @@ def test_dat_file_postprocessing(solved):
 
 @pytest.mark.parametrize("mode", [1, 2, 3, 4])
 def test_mixed_precision_matches_fp64(solved, mode):
-    """Complex FP32 LU (FP32 / TF32 / BF16x9 / BF16 trailing updates) with FP64
+    """Complex FP32 LU (FP32 / TF32 / TF32x3 trailing updates) with FP64
     refinement: surface values to 1e-11 of the FP64 solve, force and torque of
     both rules to 1e-8 (the radiation-force tolerance of the mixed form)."""
     case, g, _ = solved

@@ -62,6 +62,18 @@ def test_interior_matrices_kept_across_bloch_vectors():
         got = _solve(g, ctx, pb, 24)          # back to b after c: reassembled, same result
         for x, y in zip(got, ref):
             assert np.max(np.abs(x - y)) <= TOL * np.max(np.abs(y))
+        # reuse switched off: the same problem again is assembled in full
+        assert g.bemgpu_set_interior_reuse(ctx, 0) == 0
+        n0 = g.bemgpu_kernel_launches()
+        got = _solve(g, ctx, pb, 24)
+        assert g.bemgpu_interior_reuses(ctx) == 1
+        assert g.bemgpu_kernel_launches() > n0
+        for x, y in zip(got, ref):
+            assert np.max(np.abs(x - y)) <= TOL * np.max(np.abs(y))
+        assert g.bemgpu_set_interior_reuse(ctx, 1) == 0
+        _solve(g, ctx, pb, 24)
+        _solve(g, ctx, pb, 24)
+        assert g.bemgpu_interior_reuses(ctx) == 2
     finally:
         g.bemgpu_destroy(ctx)
         g.bemgpu_destroy(fresh)
