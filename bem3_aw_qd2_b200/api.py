@@ -60,6 +60,7 @@ def libs():
         g.bemgpu_autotune.argtypes = [vp, _d]
         g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
         g.bemgpu_set_interior_reuse.argtypes = [vp, ctypes.c_int]
+        g.bemgpu_set_interior_derivatives.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         g.bemgpu_interior_reuses.argtypes = [vp]
         g.bemgpu_interior_reuses.restype = ctypes.c_longlong
         g.bemgpu_kernel_launches.argtypes = []

@@ -858,35 +858,45 @@ __device__ __forceinline__ void fs_point(const bem_el &el, const bem_node &nd, d
 }
 
 // write one pair's 24 complex coefficients with the reference's scale factors
-// (1/4pi, -1/4pi for dG) and the sign flip for negative element ids
+// (1/4pi, -1/4pi for dG) and the sign flip for negative element ids.  G, H
+// (and dG, dH) may be null: a pass that only recomputes the derivative rows
+// writes dG, dH alone, row 2 (p - p0) of a block of rows starting at p0.
 __device__ __forceinline__ void fs_store(const bem_dom_dev &D, int p, int s, const fs_acc &a, double *G, double *H,
-                                         double *dG, double *dH) {
+                                         double *dG, double *dH, int p0) {
   const size_t N = (size_t)D.ne * 4;
   const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
   const double c = BEM_I_FP;
-  double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * s));
-  double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * s));
-  double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * s));
-  double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * s));
-  double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * s));
-  double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * s));
+  if (G) {
+    double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * s));
+    double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * s));
 #pragma unroll
-  for (int n = 0; n < 4; ++n) {
-    g2[n] = make_double2(a.g[2 * n] * c, a.g[2 * n + 1] * c);
-    h2[n] = make_double2(sg * a.h[2 * n] * c, sg * a.h[2 * n + 1] * c);
-    gz[n] = make_double2(-a.gz[2 * n] * c, -a.gz[2 * n + 1] * c);
-    ge[n] = make_double2(-a.ge[2 * n] * c, -a.ge[2 * n + 1] * c);
-    hz[n] = make_double2(sg * a.hz[2 * n] * c, sg * a.hz[2 * n + 1] * c);
-    he[n] = make_double2(sg * a.he[2 * n] * c, sg * a.he[2 * n + 1] * c);
+    for (int n = 0; n < 4; ++n) {
+      g2[n] = make_double2(a.g[2 * n] * c, a.g[2 * n + 1] * c);
+      h2[n] = make_double2(sg * a.h[2 * n] * c, sg * a.h[2 * n + 1] * c);
+    }
+  }
+  if (dG) {
+    const size_t r = 2 * (size_t)(p - p0);
+    double2 *gz = reinterpret_cast<double2 *>(dG + 2 * (r * N + 4 * s));
+    double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((r + 1) * N + 4 * s));
+    double2 *hz = reinterpret_cast<double2 *>(dH + 2 * (r * N + 4 * s));
+    double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((r + 1) * N + 4 * s));
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      gz[n] = make_double2(-a.gz[2 * n] * c, -a.gz[2 * n + 1] * c);
+      ge[n] = make_double2(-a.ge[2 * n] * c, -a.ge[2 * n + 1] * c);
+      hz[n] = make_double2(sg * a.hz[2 * n] * c, sg * a.hz[2 * n + 1] * c);
+      he[n] = make_double2(sg * a.he[2 * n] * c, sg * a.he[2 * n + 1] * c);
+    }
   }
 }
 
-// one thread per (p, s) pair, 12x12 points
+// one thread per (p, s) pair, 12x12 points; rows p0 .. p0 + np - 1
 __global__ void __launch_bounds__(128) k_fs_regular(bem_dom_dev D, double k, const uint8_t *__restrict__ flag,
                                                     double *__restrict__ G, double *__restrict__ H,
-                                                    double *__restrict__ dG, double *__restrict__ dH) {
-  const long long pair = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)D.ne * 4 * D.ne;
+                                                    double *__restrict__ dG, double *__restrict__ dH, int p0, int np) {
+  const long long pair = (long long)p0 * D.ne + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)(p0 + np) * D.ne;
   if (pair >= total) return;
   const int p = (int)(pair / D.ne), s = (int)(pair % D.ne);
   if (flag[pair] != 0 || bem_pad_row(D, p)) return;
@@ -911,15 +921,15 @@ __global__ void __launch_bounds__(128) k_fs_regular(bem_dom_dev D, double k, con
     for (int i = 0; i < BEM_GLN; ++i)
       for (int j = 0; j < BEM_GLN; ++j) fs_point(el, nd, k, c_q.xl[i], c_q.xl[j], c_q.wl[i] * c_q.wl[j], a);
   }
-  fs_store(D, p, s, a, G, H, dG, dH);
+  fs_store(D, p, s, a, G, H, dG, dH, p0);
 }
 
 // one block per flagged pair, 64x64 points
 __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k, const int *__restrict__ near_s,
                                                         const int *__restrict__ near_n, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ dG,
-                                                        double *__restrict__ dH, double *__restrict__ nearF) {
-  const int p = blockIdx.x, kk = blockIdx.y;
+                                                        double *__restrict__ dH, double *__restrict__ nearF, int p0) {
+  const int p = p0 + blockIdx.x, kk = blockIdx.y;
   if (kk >= near_n[p]) return;
   const int s = near_s[(size_t)p * D.near_cap + kk];
   bem_node nd;
@@ -951,12 +961,14 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k,
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int c = 0; c < 51; ++c) av[c] = v[c];
-    fs_store(D, p, s, a, G, H, dG, dH);
-    const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
-    double *nf = nearF + ((size_t)p * D.near_cap + kk) * 3;
-    nf[0] = sg * a.f * BEM_I_FP;
-    nf[1] = sg * a.fz * BEM_I_FP;
-    nf[2] = sg * a.fe * BEM_I_FP;
+    fs_store(D, p, s, a, G, H, dG, dH, p0);
+    if (G) {
+      const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
+      double *nf = nearF + ((size_t)p * D.near_cap + kk) * 3;
+      nf[0] = sg * a.f * BEM_I_FP;
+      nf[1] = sg * a.fz * BEM_I_FP;
+      nf[2] = sg * a.fe * BEM_I_FP;
+    }
   }
 }
 
@@ -977,8 +989,8 @@ struct self_acc {
 __global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ dG,
                                                         double *__restrict__ dH, double *__restrict__ selfF,
-                                                        unsigned *status) {
-  const int p = blockIdx.x;
+                                                        unsigned *status, int p0) {
+  const int p = p0 + blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (bem_is_tri(D, te)) return;  // k_fs_self_tri
@@ -1169,26 +1181,33 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k,
     const double bdC = bem_bdC(el);
     const double iTz = 1.0 / sqrt(dot3(vz, vz)), iTe = 1.0 / sqrt(dot3(ve, ve));
     const double c = BEM_I_FP;
-    double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
-    double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
-    double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * t));
-    double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
-    double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * t));
-    double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
-    for (int n = 0; n < 4; ++n) {
-      g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
-      const double hs = plane ? 0.0 : sg * bdC * c;
-      h2[n] = make_double2(v[8 + 2 * n] * hs, v[8 + 2 * n + 1] * hs);
-      // dG: times -1/4pi/|T|; not affected by the element orientation
-      gz[n] = make_double2(-c * iTz * v[16 + 2 * n], -c * iTz * v[16 + 2 * n + 1]);
-      ge[n] = make_double2(-c * iTe * v[24 + 2 * n], -c * iTe * v[24 + 2 * n + 1]);
-      const double hzs = plane ? 0.0 : sg * bdC * c * iTz, hes = plane ? 0.0 : sg * bdC * c * iTe;
-      hz[n] = make_double2(v[32 + 2 * n] * hzs, v[32 + 2 * n + 1] * hzs);
-      he[n] = make_double2(v[40 + 2 * n] * hes, v[40 + 2 * n + 1] * hes);
+    if (G) {
+      double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
+      double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
+      for (int n = 0; n < 4; ++n) {
+        g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
+        const double hs = plane ? 0.0 : sg * bdC * c;
+        h2[n] = make_double2(v[8 + 2 * n] * hs, v[8 + 2 * n + 1] * hs);
+      }
+      selfF[3 * p + 0] = plane ? 0.0 : sg * v[48] * bdC * c;
+      selfF[3 * p + 1] = plane ? 0.0 : sg * v[49] * bdC * c * iTz;
+      selfF[3 * p + 2] = plane ? 0.0 : sg * v[50] * bdC * c * iTe;
     }
-    selfF[3 * p + 0] = plane ? 0.0 : sg * v[48] * bdC * c;
-    selfF[3 * p + 1] = plane ? 0.0 : sg * v[49] * bdC * c * iTz;
-    selfF[3 * p + 2] = plane ? 0.0 : sg * v[50] * bdC * c * iTe;
+    if (dG) {
+      const size_t r = 2 * (size_t)(p - p0);
+      double2 *gz = reinterpret_cast<double2 *>(dG + 2 * (r * N + 4 * t));
+      double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((r + 1) * N + 4 * t));
+      double2 *hz = reinterpret_cast<double2 *>(dH + 2 * (r * N + 4 * t));
+      double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((r + 1) * N + 4 * t));
+      for (int n = 0; n < 4; ++n) {
+        // dG: times -1/4pi/|T|; not affected by the element orientation
+        gz[n] = make_double2(-c * iTz * v[16 + 2 * n], -c * iTz * v[16 + 2 * n + 1]);
+        ge[n] = make_double2(-c * iTe * v[24 + 2 * n], -c * iTe * v[24 + 2 * n + 1]);
+        const double hzs = plane ? 0.0 : sg * bdC * c * iTz, hes = plane ? 0.0 : sg * bdC * c * iTe;
+        hz[n] = make_double2(v[32 + 2 * n] * hzs, v[32 + 2 * n + 1] * hzs);
+        he[n] = make_double2(v[40 + 2 * n] * hes, v[40 + 2 * n + 1] * hes);
+      }
+    }
   }
 }
 
@@ -1269,8 +1288,8 @@ __global__ void NP_BOUNDS k_q0_self_tri(bem_dom_dev D, const __grid_constant__ b
 __global__ void __launch_bounds__(NP_THREADS) k_fs_self_tri(bem_dom_dev D, double k, double *__restrict__ G,
                                                             double *__restrict__ H, double *__restrict__ dG,
                                                             double *__restrict__ dH, double *__restrict__ selfF,
-                                                            unsigned *status) {
-  const int p = blockIdx.x;
+                                                            unsigned *status, int p0) {
+  const int p = p0 + blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (!bem_is_tri(D, te) || tn == 3) return;
@@ -1375,21 +1394,28 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_self_tri(bem_dom_dev D, doubl
     const size_t N = (size_t)D.ne * 4;
     const double c = BEM_I_FP * aJ;
     const double iTz = 1.0 / sqrt(dot3(vz, vz)), iTe = 1.0 / sqrt(dot3(ve, ve));
-    double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
-    double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
-    double2 *gz = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p) * N + 4 * t));
-    double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
-    double2 *hz = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p) * N + 4 * t));
-    double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((size_t)(2 * p + 1) * N + 4 * t));
-    for (int n = 0; n < 4; ++n) {
-      g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
-      h2[n] = make_double2(0.0, 0.0);
-      gz[n] = make_double2(-c * iTz * v[8 + 2 * n], -c * iTz * v[8 + 2 * n + 1]);
-      ge[n] = make_double2(-c * iTe * v[16 + 2 * n], -c * iTe * v[16 + 2 * n + 1]);
-      hz[n] = make_double2(0.0, 0.0);
-      he[n] = make_double2(0.0, 0.0);
+    if (G) {
+      double2 *g2 = reinterpret_cast<double2 *>(G + 2 * ((size_t)p * N + 4 * t));
+      double2 *h2 = reinterpret_cast<double2 *>(H + 2 * ((size_t)p * N + 4 * t));
+      for (int n = 0; n < 4; ++n) {
+        g2[n] = make_double2(v[2 * n] * c, v[2 * n + 1] * c);
+        h2[n] = make_double2(0.0, 0.0);
+      }
+      selfF[3 * p] = selfF[3 * p + 1] = selfF[3 * p + 2] = 0.0;
     }
-    selfF[3 * p] = selfF[3 * p + 1] = selfF[3 * p + 2] = 0.0;
+    if (dG) {
+      const size_t r = 2 * (size_t)(p - p0);
+      double2 *gz = reinterpret_cast<double2 *>(dG + 2 * (r * N + 4 * t));
+      double2 *ge = reinterpret_cast<double2 *>(dG + 2 * ((r + 1) * N + 4 * t));
+      double2 *hz = reinterpret_cast<double2 *>(dH + 2 * (r * N + 4 * t));
+      double2 *he = reinterpret_cast<double2 *>(dH + 2 * ((r + 1) * N + 4 * t));
+      for (int n = 0; n < 4; ++n) {
+        gz[n] = make_double2(-c * iTz * v[8 + 2 * n], -c * iTz * v[8 + 2 * n + 1]);
+        ge[n] = make_double2(-c * iTe * v[16 + 2 * n], -c * iTe * v[16 + 2 * n + 1]);
+        hz[n] = make_double2(0.0, 0.0);
+        he[n] = make_double2(0.0, 0.0);
+      }
+    }
   }
 }
 
@@ -1656,16 +1682,16 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       bem_count_launches(1);
     }
   } else {
-    k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH);
+    k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH, 0, N);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[2], st);
-    k_fs_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF);
+    k_fs_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF, 0);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
-    k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+    k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status, 0);
     bem_count_launches(1);
     if (D->has_tri) {
-      k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status);
+      k_fs_self_tri<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status, 0);
       bem_count_launches(1);
     }
   }
@@ -1714,6 +1740,29 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
   cudaEventDestroy(e1);
   if (cudaPeekAtLastError() != cudaSuccess) rc = -1;
   return rc;
+}
+
+// The free-space kernels over the rows p0 .. p0 + np - 1 writing only dG and
+// dH (row 2 (p - p0) of each): the derivative rows of an interior domain
+// recomputed a block of rows at a time for the particle velocity, instead of
+// kept (2 x 2N x N complex).  The pair flags and near lists must be current
+// (bem_launch_classify).
+extern "C" int bem_launch_fs_deriv(const bem_dom_dev *D, double k, bem_scratch *S, int p0, int np, double *dG,
+                                   double *dH, cudaStream_t st) {
+  if (np <= 0 || D->ne <= 0) return 0;
+  const long long npairs = (long long)np * D->ne;
+  k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, nullptr, nullptr, dG, dH, p0, np);
+  bem_count_launches(1);
+  k_fs_near<<<dim3(np, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, nullptr, nullptr, dG, dH,
+                                                          S->nearF, p0);
+  bem_count_launches(1);
+  k_fs_self<<<np, NP_THREADS, 0, st>>>(*D, k, nullptr, nullptr, dG, dH, S->selfF, S->status, p0);
+  bem_count_launches(1);
+  if (D->has_tri) {
+    k_fs_self_tri<<<np, NP_THREADS, 0, st>>>(*D, k, nullptr, nullptr, dG, dH, S->selfF, S->status, p0);
+    bem_count_launches(1);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int periodic, bem_scratch *S, cudaStream_t st) {

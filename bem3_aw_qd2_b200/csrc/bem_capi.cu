@@ -105,6 +105,13 @@ struct bemgpu_ctx {
   std::vector<unsigned char> int_data;
   bool int_valid = false, int_reuse = false;
   bool int_reuse_on = true;  // bemgpu_set_interior_reuse
+  // interior derivative rows dG, dH: kept (default) or recomputed a block of
+  // rows at a time in the particle-velocity step (bemgpu_set_interior_derivatives;
+  // dgh_keep_req takes effect at the next load)
+  bool dgh_keep = true, dgh_keep_req = true;
+  double *dGc = nullptr, *dHc = nullptr;  // one block of recomputed rows
+  int dgh_rows = 0;                       // rows a block holds
+  int dgh_rows_req = 0;                   // asked for (0: 256 MiB of each)
   bool int_factored[BEMGPU_MAXDOM] = {};
   long long int_reused_loads = 0;
 };
@@ -156,6 +163,8 @@ static void free_problem(bemgpu_ctx *c, bool release) {
     dfree(c->hk2); dfree(c->Pi); dfree(c->dPi); dfree(c->p_inc); dfree(c->v_inc); dfree(c->rho0_d); dfree(c->k2_d);
     for (int d = 0; d < BEMGPU_MAXDOM; ++d) {
       dfree(c->G[d]); dfree(c->H[d]); dfree(c->dG[d]); dfree(c->dH[d]); dfree(c->dF[d]);
+      c->cap.erase((const void *)&c->dG[d]);
+      c->cap.erase((const void *)&c->dH[d]);
       dfree(c->P[d]); dfree(c->dP[d]); dfree(c->pv[d]); dfree(c->dpv[d]);
     }
     for (bem_scratch *S : {&c->scr, &c->scr1}) {
@@ -165,6 +174,7 @@ static void free_problem(bemgpu_ctx *c, bool release) {
     dfree(c->A); dfree(c->b); dfree(c->tpv); dfree(c->B3); dfree(c->wtab); dfree(c->stab); dfree(c->b0); dfree(c->B3s);
     for (int d = 0; d < BEMGPU_MAXDOM; ++d) { dfree(c->Wd[d]); dfree(c->cinv[d]); dfree(c->Gc[d]); }
     dfree(c->B3c);
+    dfree(c->dGc); dfree(c->dHc);
     dfree(c->pw_d); dfree(c->tgt_t); dfree(c->tgt_ze); dfree(c->tgt_w); dfree(c->bdv);
     dfree(c->ctr_t); dfree(c->ctr_idx); dfree(c->ctr_ze); dfree(c->ctr_bdv);
     c->cap.clear();
@@ -450,9 +460,15 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     if ((int)N > maxN) maxN = (int)N;
     CK(falloc(c, &c->G[d], 2 * N * N), "G");
     CK(falloc(c, &c->H[d], 2 * N * N), "H");
-    if (d > 0) {
+    if (d > 0 && c->dgh_keep_req) {
       CK(falloc(c, &c->dG[d], 4 * N * N), "dG");
       CK(falloc(c, &c->dH[d], 4 * N * N), "dH");
+    } else if (d > 0) {
+      // recomputed per block of rows: the full-size rows are not kept
+      dfree(c->dG[d]);
+      dfree(c->dH[d]);
+      c->cap.erase((const void *)&c->dG[d]);
+      c->cap.erase((const void *)&c->dH[d]);
     }
     CK(falloc(c, &c->dF[d], 3 * N), "dF");
     CK(falloc(c, &c->P[d], 2 * N), "P");
@@ -510,6 +526,21 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
     }
   }
   CK(falloc(c, &c->B3, 6 * (size_t)maxN), "B3");
+  c->dgh_keep = c->dgh_keep_req;
+  if (!c->dgh_keep && nd > 1) {
+    // a block of recomputed derivative rows: 256 MiB for each of dG, dH (at
+    // least 32 rows), rows a multiple of 4 (one element's nodes)
+    int maxNi = 0;
+    for (int d = 1; d < nd; ++d) maxNi = 4 * c->dom_ne[d] > maxNi ? 4 * c->dom_ne[d] : maxNi;
+    size_t rows = ((size_t)256 << 20) / (64 * (size_t)(maxNi ? maxNi : 1));
+    rows = rows < 32 ? 32 : rows;
+    if (c->dgh_rows_req > 0) rows = (size_t)c->dgh_rows_req;
+    rows = rows > (size_t)maxNi ? (size_t)maxNi : rows;
+    rows -= rows % 4;
+    c->dgh_rows = (int)(rows ? rows : 4);
+    CK(falloc(c, &c->dGc, 4 * (size_t)c->dgh_rows * maxNi), "dG rows");
+    CK(falloc(c, &c->dHc, 4 * (size_t)c->dgh_rows * maxNi), "dH rows");
+  }
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "status");
   // device view of the system
   bem_sys_dev &S = c->sys;
@@ -792,9 +823,25 @@ static int solve_tail(bemgpu_ctx *c) {
   if (c->prof) cudaEventRecord(c->ev[14], c->stream);
   // particle velocity: interior domains first, then domain 0 from the interface condition
   CK(cudaMemsetAsync(c->tpv, 0, 6 * (size_t)c->NN * sizeof(double), c->stream), "tpv");
-  for (int d = 1; d <= c->MN; ++d)
-    if (bem_launch_pv(&c->sys, d, c->dG[d], c->dH[d], c->dF[d], c->P[d], c->dP[d], c->pv[d], c->tpv, c->stream))
-      return fail(c, "pv", cudaGetLastError());
+  for (int d = 1; d <= c->MN; ++d) {
+    if (c->dgh_keep) {
+      if (bem_launch_pv(&c->sys, d, c->dG[d], c->dH[d], c->dF[d], c->P[d], c->dP[d], c->pv[d], c->tpv, c->stream))
+        return fail(c, "pv", cudaGetLastError());
+      continue;
+    }
+    // derivative rows recomputed a block at a time (pair flags and near lists
+    // of this domain first: the free-space scratch may hold another domain's)
+    bem_dom_dev D = dom_view(c, d);
+    const int N = 4 * c->dom_ne[d];
+    if (bem_launch_classify(&D, &c->qp, 0, &c->scr1, c->stream)) return fail(c, "classify", cudaGetLastError());
+    for (int p0 = 0; p0 < N; p0 += c->dgh_rows) {
+      const int np = N - p0 < c->dgh_rows ? N - p0 : c->dgh_rows;
+      if (bem_launch_fs_deriv(&D, c->k0[d], &c->scr1, p0, np, c->dGc, c->dHc, c->stream) ||
+          bem_launch_pv_rows(&c->sys, d, c->dGc, c->dHc, c->dF[d], c->P[d], c->dP[d], c->pv[d], c->tpv, p0, np,
+                             c->stream))
+        return fail(c, "pv", cudaGetLastError());
+    }
+  }
   if (bem_launch_pv(&c->sys, 0, nullptr, nullptr, nullptr, nullptr, nullptr, c->pv[0], c->tpv, c->stream))
     return fail(c, "pv0", cudaGetLastError());
   if (c->prof) cudaEventRecord(c->ev[15], c->stream);
@@ -1274,6 +1321,13 @@ extern "C" int bemgpu_zgesv(int device, int n, int nrhs, const double *A, double
 }
 
 extern "C" long long bemgpu_interior_reuses(bemgpu_ctx *c) { return c ? c->int_reused_loads : -1; }
+
+extern "C" int bemgpu_set_interior_derivatives(bemgpu_ctx *c, int keep, int block_rows) {
+  if (!c || block_rows < 0) return -2;
+  c->dgh_keep_req = keep != 0;
+  c->dgh_rows_req = block_rows;
+  return 0;
+}
 
 extern "C" int bemgpu_set_interior_reuse(bemgpu_ctx *c, int on) {
   if (!c) return -2;

@@ -54,6 +54,9 @@ int bem_launch_force_bd(const bem_dom_dev *D, int ntgt, const int *tgt_t, const 
                         const double *bdv, const double *pw, double k2r, double k2i, const double *rc, double c0,
                         double rho0, double *out, cudaStream_t st);
 int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int periodic, bem_scratch *S, cudaStream_t st);
+// free-space derivative rows dG, dH of rows p0 .. p0 + np - 1 only (row 2 (p - p0))
+int bem_launch_fs_deriv(const bem_dom_dev *D, double k, bem_scratch *S, int p0, int np, double *dG, double *dH,
+                        cudaStream_t st);
 int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, double frac,
                      int nchunk, cudaStream_t st, float *ms);
 int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k, bem_scratch *S,

@@ -39,6 +39,10 @@
 #include "bem_lu.h"
 
 #define LU_W BEM_LU_W
+#define LU_OB BEM_LU_OB  // outer block: panels whose updates right of it are delayed and applied at once
+#define LU_NSLOT (LU_OB / LU_W)
+#define LU_ONE_BLOCK_N 2048  // default of bem_lu.one_block_max
+static_assert(LU_OB == LU_OUTER_W, "the tensor-core update depth is the outer block");
 #define LU_TH 256        // threads of a panel CTA: one row each
 #define LU_CL 8          // CTAs of the panel cluster
 #define LU_MAXP (2 * LU_W)
@@ -53,9 +57,9 @@
 // complex scratch (bem_lu.u11)
 #define U_LU 0                       // [LU_W][LU_W] packed L11\U11, row i = pivot row i
 #define U_UINV (LU_W * LU_W)         // U11^-1 (upper)
-#define U_LINV (2 * LU_W * LU_W)     // L11^-1 (unit lower)
-#define U_STAGE (3 * LU_W * LU_W)    // panel values of the rows moved out of the pivot block
-#define U_COUNT (4 * LU_W * LU_W)
+#define U_STAGE (2 * LU_W * LU_W)    // panel values of the rows moved out of the pivot block
+#define U_LINV (3 * LU_W * LU_W)     // [LU_NSLOT] L11^-1 (unit lower) of each panel of the outer block
+#define U_COUNT ((3 + LU_NSLOT) * LU_W * LU_W)
 
 // ---------------------------------------------------------------- complex helpers
 // complex double (double2) and complex float (float2): the same code in both
@@ -107,10 +111,12 @@ __device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y
 // ---------------------------------------------------------------- partial pivoting in one CTA
 template <class C2>
 struct gepp_sh {
-  unsigned wk[2][LU_TH / 32];  // each warp's pivot key
-  C2 prow[2][LU_W], krow[2][LU_W];
-  C2 prcp[2];                  // reciprocal of the pivot
-  int pid[2], kid[2];
+  unsigned wk[2][LU_TH / 32];        // each warp's best pivot key
+  C2 cand[2][LU_TH / 32][LU_W];      // each warp's best row, as its owner holds it
+  C2 crcp[2][LU_TH / 32];            // reciprocal of that row's pivot entry
+  int cid[2][LU_TH / 32];            // its matrix row
+  C2 krow[2][LU_W];                  // the row at position j
+  int kid[2];
 };
 
 // Pivot key of a candidate: the float bits of |re| + |im| (non-negative floats
@@ -143,47 +149,58 @@ __device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, uns
   const int steps = min(w, rr);
   for (int j = 0; j < steps; ++j) {
     const int b = j & 1;
-    // the pivot: one integer maximum per warp, then over the warps (the
-    // 2^-15 resolution of the key only picks among rows within that much of
-    // the largest, which keeps partial pivoting's growth bound)
-    const unsigned key = __reduce_max_sync(FULL, (t >= j && t < rr) ? pivot_key((float)cabs1(v[0]), t) : 0u);
+    // the pivot: one integer maximum per warp, whose owner publishes its row
+    // and reciprocal at once; after the one barrier every thread takes the
+    // maximum over the warps (the 2^-15 resolution of the key only picks
+    // among rows within that much of the largest, which keeps partial
+    // pivoting's growth bound).  The buffers alternate between steps, so a
+    // step's writes never meet the previous step's reads.
+    const unsigned mykey = (t >= j && t < rr) ? pivot_key((float)cabs1(v[0]), t) : 0u;
+    const unsigned key = __reduce_max_sync(FULL, mykey);
+    if (mykey == key && key != 0u) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) sh.cand[b][wid][c] = v[c];
+      sh.crcp[b][wid] = crcp(v[0]);
+      sh.cid[b][wid] = id;
+    }
     if (lane == 0) sh.wk[b][wid] = key;
-    __syncthreads();
-    unsigned best = sh.wk[b][0];
-#pragma unroll
-    for (int q = 1; q < LU_TH / 32; ++q) best = max(best, sh.wk[b][q]);
-    int p = 255 - (int)(best & 255u);
-    if ((best >> 8) == 0u) {  // no non-zero entry left in the column
-      if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
-      p = j;
-    }
-    if (t == p) {
-#pragma unroll
-      for (int c = 0; c < LU_W; ++c) sh.prow[b][c] = v[c];
-      sh.pid[b] = id;
-      sh.prcp[b] = crcp(v[0]);
-    }
     if (t == j) {
 #pragma unroll
       for (int c = 0; c < LU_W; ++c) sh.krow[b][c] = v[c];
       sh.kid[b] = id;
     }
     __syncthreads();
-    if (t == j) {
+    unsigned best = sh.wk[b][0];
+    int bw = 0;
 #pragma unroll
-      for (int c = 0; c < LU_W; ++c) v[c] = sh.prow[b][c];
-      id = sh.pid[b];
+    for (int q = 1; q < LU_TH / 32; ++q) {
+      const unsigned kq = sh.wk[b][q];
+      if (kq > best) { best = kq; bw = q; }
+    }
+    int p = 255 - (int)(best & 255u);
+    const bool zero = (best >> 8) == 0u;  // no non-zero entry left in the column
+    if (zero) {
+      if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
+      p = j;
+    }
+    const C2 *prow = zero ? sh.krow[b] : sh.cand[b][bw];
+    if (t == j) {
+      if (!zero) {
+#pragma unroll
+        for (int c = 0; c < LU_W; ++c) v[c] = prow[c];
+        id = sh.cid[b][bw];
+      }
     } else if (t == p) {
 #pragma unroll
       for (int c = 0; c < LU_W; ++c) v[c] = sh.krow[b][c];
       id = sh.kid[b];
     }
     if (t > j && t < rr) {
-      const C2 l = cmul(v[0], sh.prcp[b]);
+      const C2 l = zero ? czero<C2>() : cmul(v[0], sh.crcp[b][bw]);
       v[0] = l;
 #pragma unroll
       for (int c = 1; c < LU_W; ++c)
-        if (c < LU_W - j) v[c] = cfms(l, sh.prow[b][c], v[c]);
+        if (c < LU_W - j) v[c] = cfms(l, prow[c], v[c]);
     }
     rot1(v);
   }
@@ -231,8 +248,6 @@ struct panel_sh {
   gepp_sh<C2> g;
   gepp_sh<float2> gl;
   C2 lu[LU_W][LU_W + 1];
-  C2 ui[LU_W][LU_W + 1];
-  C2 li[LU_W][LU_W + 1];
   C2 rd[LU_W];  // reciprocals of U11's diagonal
   int sel[LU_W], la[LU_W], lb[LU_W];
 };
@@ -303,51 +318,49 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
   }
   if (t < LU_W) S.rd[t] = t < w ? crcp(S.lu[t][t]) : czero<C2>();
   __syncthreads();
-  if (wid == 0) {
-    // U11^-1, column j = lane: x_j = 1 / u_jj, x_i = -(sum_{i<l<=j} u_il x_l) / u_ii
-    // (four partial sums: the dependent chain is the critical path)
-    const int j = lane;
-    for (int i = 0; i < LU_W; ++i) S.ui[i][j] = czero<C2>();
-    if (j < w) {
-      S.ui[j][j] = S.rd[j];
-      for (int i = j - 1; i >= 0; --i) {
-        C2 s0 = czero<C2>(), s1 = czero<C2>(), s2 = czero<C2>(), s3 = czero<C2>();
-        int l = i + 1;
-        for (; l + 3 <= j; l += 4) {
-          s0 = cfma(S.lu[i][l], S.ui[l][j], s0);
-          s1 = cfma(S.lu[i][l + 1], S.ui[l + 1][j], s1);
-          s2 = cfma(S.lu[i][l + 2], S.ui[l + 2][j], s2);
-          s3 = cfma(S.lu[i][l + 3], S.ui[l + 3][j], s3);
+  // U11^-1 (warps 0-3) and L11^-1 (warps 4-7), 8 columns a warp, 4 at a
+  // time, column-oriented substitution with lane = row: at step l lane l
+  // finishes x_l, a shuffle hands it to the other lanes, and each lane
+  // removes its u_il x_l (l_il x_l): one short dependent step per row, all
+  // rows of four columns at once
+  {
+    const int i = lane;
+    const bool upper = wid < 4;
+    const int jb = (wid & 3) * 8;
+    for (int half = 0; half < 2; ++half) {
+      C2 x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = (i == jb + half * 4 + q && i < w) ? cone<C2>() : czero<C2>();
+      if (upper) {
+        for (int l = LU_W - 1; l >= 0; --l) {
+          const C2 a = S.lu[i][l], d = S.rd[l];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (i == l) x[q] = cmul(x[q], d);
+            const C2 xl = cx<C2>::mk(__shfl_sync(FULL, x[q].x, l), __shfl_sync(FULL, x[q].y, l));
+            if (i < l) x[q] = cfms(a, xl, x[q]);
+          }
         }
-        for (; l <= j; ++l) s0 = cfma(S.lu[i][l], S.ui[l][j], s0);
-        const C2 s = cx<C2>::mk(s0.x + s1.x + s2.x + s3.x, s0.y + s1.y + s2.y + s3.y);
-        S.ui[i][j] = cneg(cmul(s, S.rd[i]));
+      } else {
+        for (int l = 0; l < LU_W; ++l) {
+          const C2 a = S.lu[i][l];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const C2 xl = cx<C2>::mk(__shfl_sync(FULL, x[q].x, l), __shfl_sync(FULL, x[q].y, l));
+            if (i > l) x[q] = cfms(a, xl, x[q]);
+          }
+        }
+      }
+      C2 *dst = upper ? u + U_UINV : u + U_LINV + (k % LU_OB) / LU_W * (LU_W * LU_W);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = jb + half * 4 + q;
+        // entries outside a short panel (w < 32) are zero
+        dst[i * LU_W + j] = (i < w && j < w) ? x[q] : czero<C2>();
       }
     }
-    __syncwarp();
-    for (int i = 0; i < LU_W; ++i) u[U_UINV + i * LU_W + j] = S.ui[i][j];
-  } else if (wid == 1) {
-    // L11^-1 (unit lower), column j = lane: x_j = 1, x_i = -sum_{j<=l<i} l_il x_l
-    const int j = lane;
-    for (int i = 0; i < LU_W; ++i) S.li[i][j] = czero<C2>();
-    if (j < w) {
-      S.li[j][j] = cone<C2>();
-      for (int i = j + 1; i < w; ++i) {
-        C2 s0 = czero<C2>(), s1 = czero<C2>(), s2 = czero<C2>(), s3 = czero<C2>();
-        int l = j;
-        for (; l + 3 < i; l += 4) {
-          s0 = cfma(S.lu[i][l], S.li[l][j], s0);
-          s1 = cfma(S.lu[i][l + 1], S.li[l + 1][j], s1);
-          s2 = cfma(S.lu[i][l + 2], S.li[l + 2][j], s2);
-          s3 = cfma(S.lu[i][l + 3], S.li[l + 3][j], s3);
-        }
-        for (; l < i; ++l) s0 = cfma(S.lu[i][l], S.li[l][j], s0);
-        S.li[i][j] = cx<C2>::mk(-(s0.x + s1.x + s2.x + s3.x), -(s0.y + s1.y + s2.y + s3.y));
-      }
-    }
-    __syncwarp();
-    for (int i = 0; i < LU_W; ++i) u[U_LINV + i * LU_W + j] = S.li[i][j];
-  } else if (wid == 2) {
+  }
+  if (wid == 2) {
     // row moves: pivot row i goes to position k + i; the rows of the pivot
     // block that were not picked (displaced) go to the positions the pivot
     // rows from below left, paired in lane order
@@ -379,7 +392,7 @@ __global__ void __cluster_dims__(LU_CL, 1, 1) __launch_bounds__(LU_TH, 1)
 #define AP_COLS 16   // columns of a row-move block
 
 template <class C2>
-__global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int k, const int *pv, const C2 *u,
+__global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int k, int cend, const int *pv, const C2 *u,
                                                     int *rowmap, unsigned *status) {
   __shared__ C2 sm[LU_W][LU_W + 1];
   __shared__ C2 srow[LU_MAXP][AP_COLS + 1];
@@ -407,40 +420,48 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int 
   if (b < nL) {
     // L21 = A21 U11^-1 in place, for the rows below the pivot block that no move touches
     for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(u + U_UINV + e);
-    __syncthreads();
     const int row = r0 + b * AP_ROWS + (t >> 2), part = t & 3;
+    // the row's panel values, loaded at once (independent loads, not a chain)
+    C2 a[LU_W];
+    {
+      const C2 *ap = A + (size_t)(row < n ? row : r0) * lda + k;
+#pragma unroll
+      for (int l = 0; l < LU_W; ++l) a[l] = (row < n && l < w) ? ap[l] : czero<C2>();
+    }
+    __syncthreads();
     bool live = row < n;
     for (int e = w; e < nperm && live; ++e) live = sdst[e] != row;
     C2 x[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) x[c] = czero<C2>();
-    if (live) {
-      const C2 *a = A + (size_t)row * lda + k;
-      for (int l = 0; l < w; ++l) {
-        const C2 al = a[l];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
-      }
-    }
+    for (int l = 0; l < LU_W; ++l)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) x[c] = cfma(a[l], sm[l][part * 8 + c], x[c]);
     __syncthreads();  // every read of the row before any write to it
     if (live) {
-      C2 *a = A + (size_t)row * lda + k;
+      C2 *ap = A + (size_t)row * lda + k;
 #pragma unroll
       for (int c = 0; c < 8; ++c)
-        if (part * 8 + c < w) a[part * 8 + c] = x[c];
+        if (part * 8 + c < w) ap[part * 8 + c] = x[c];
     }
     return;
   }
   if (b < nL + nCl + nCr) {
     // the row moves on AP_COLS columns outside the panel; right of the panel
-    // also U12 = L11^-1 A12 on the pivot block
+    // and left of cend (the end of the outer block) also U12 = L11^-1 A12 on
+    // the pivot block; right of cend the moves alone (U12 there is formed for
+    // the whole outer block at once, k_lu_trsm)
     const int i = b - nL;
     const bool right = i >= nCl;
     const int c0 = right ? r0 + (i - nCl) * AP_COLS : i * AP_COLS;
     const int c1 = min(right ? n : k, c0 + AP_COLS);
     const int nc = c1 - c0;
-    if (right)
-      for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(u + U_LINV + e);
+    const bool u12 = right && c0 < cend;
+    if (u12) {
+      const C2 *linv = u + U_LINV + (k % LU_OB) / LU_W * (LU_W * LU_W);
+      for (int e = t; e < LU_W * LU_W; e += AP_TH) sm[e / LU_W][e % LU_W] = __ldcg(linv + e);
+    }
     __syncthreads();  // sdst / ssrc
     for (int e = t; e < nperm * AP_COLS; e += AP_TH) {
       const int pr = e / AP_COLS, cc = e % AP_COLS;
@@ -449,7 +470,7 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int 
     __syncthreads();
     const int cc = t % AP_COLS, grp = t / AP_COLS;  // 8 groups of 16 columns
     if (cc < nc) {
-      if (right) {
+      if (u12) {
         for (int ii = grp; ii < w; ii += AP_TH / AP_COLS) {
           C2 s = czero<C2>();
           for (int l = 0; l <= ii; ++l) s = cfma(sm[ii][l], srow[l][cc], s);
@@ -473,18 +494,20 @@ __global__ void __launch_bounds__(AP_TH) k_lu_apply(C2 *A, long lda, int n, int 
   {
     const int r = t >> 2, part = t & 3, e = w + r;
     if (e < nperm) {
+      C2 a[LU_W];
+#pragma unroll
+      for (int l = 0; l < LU_W; ++l) a[l] = l < w ? __ldcg(u + U_STAGE + r * LU_W + l) : czero<C2>();
       C2 x[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) x[c] = czero<C2>();
-      for (int l = 0; l < w; ++l) {
-        const C2 al = __ldcg(u + U_STAGE + r * LU_W + l);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) x[c] = cfma(al, sm[l][part * 8 + c], x[c]);
-      }
-      C2 *a = A + (size_t)sdst[e] * lda + k;
+      for (int l = 0; l < LU_W; ++l)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) x[c] = cfma(a[l], sm[l][part * 8 + c], x[c]);
+      C2 *ap = A + (size_t)sdst[e] * lda + k;
 #pragma unroll
       for (int c = 0; c < 8; ++c)
-        if (part * 8 + c < w) a[part * 8 + c] = x[c];
+        if (part * 8 + c < w) ap[part * 8 + c] = x[c];
     }
   }
   int old = 0;
@@ -509,26 +532,16 @@ __device__ __forceinline__ void dmma(double a, double b, double (&d)[2]) {
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, int n, int k) {
+// C -= L U on the FP64 tensor cores: C = A[r0:n, r0:cend), L = A[r0:n, kk:kk+kw),
+// U = A[kk:kk+kw, r0:cend); kw in steps of LU_W staged through shared memory.
+// A panel's update (kk = k, kw = 32, cend = the end of its outer block) and an
+// outer block's (kk = its first column, kw = LU_OB, cend = n) alike.
+__global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, int n, int kk, int kw, int r0,
+                                                        int cend) {
   extern __shared__ __align__(16) double up_smem[];
   double *Ar = up_smem, *Ai = Ar + UP_BM * UP_LDA, *Br = Ai + UP_BM * UP_LDA, *Bi = Br + LU_W * UP_LDB;
   const int t = threadIdx.x;
-  const int w = min(LU_W, n - k);
-  const int r0 = k + w;
   const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
-  for (int e = t; e < UP_BM * LU_W; e += UP_TH) {
-    const int r = e / LU_W, c = e % LU_W;
-    const double2 x = (rb + r < n && c < w) ? A[(size_t)(rb + r) * lda + k + c] : cz();
-    Ar[r * UP_LDA + c] = x.x;
-    Ai[r * UP_LDA + c] = x.y;
-  }
-  for (int e = t; e < LU_W * UP_BN; e += UP_TH) {
-    const int r = e / UP_BN, c = e % UP_BN;
-    const double2 x = (r < w && cb + c < n) ? A[(size_t)(k + r) * lda + cb + c] : cz();
-    Br[r * UP_LDB + c] = x.x;
-    Bi[r * UP_LDB + c] = x.y;
-  }
-  __syncthreads();
   const int lane = t & 31, wid = t >> 5, g = lane >> 2, q = lane & 3;
   const int wm = wid & 1, wn = wid >> 1;  // warp tile: 32 rows x 16 columns
   double cr[4][2][2], ci[4][2][2];
@@ -539,34 +552,51 @@ __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, in
       const int row = rb + wm * 32 + mt * 8 + g, col = cb + wn * 16 + nt * 8 + 2 * q;
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
-        const double2 x = (row < n && col + i < n) ? A[(size_t)row * lda + col + i] : cz();
+        const double2 x = (row < n && col + i < cend) ? A[(size_t)row * lda + col + i] : cz();
         cr[mt][nt][i] = x.x;
         ci[mt][nt][i] = x.y;
       }
     }
-#pragma unroll
-  for (int kk = 0; kk < LU_W; kk += 4) {
-    double ar[4], ai[4], br[2], bi[2];
-#pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-      ar[mt] = Ar[(wm * 32 + mt * 8 + g) * UP_LDA + kk + q];
-      ai[mt] = Ai[(wm * 32 + mt * 8 + g) * UP_LDA + kk + q];
+  for (int q0 = 0; q0 < kw; q0 += LU_W) {
+    const int wq = min(LU_W, kw - q0), kc = kk + q0;
+    if (q0) __syncthreads();  // the previous chunk's fragment loads are done
+    for (int e = t; e < UP_BM * LU_W; e += UP_TH) {
+      const int r = e / LU_W, c = e % LU_W;
+      const double2 x = (rb + r < n && c < wq) ? A[(size_t)(rb + r) * lda + kc + c] : cz();
+      Ar[r * UP_LDA + c] = x.x;
+      Ai[r * UP_LDA + c] = x.y;
     }
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-      br[nt] = Br[(kk + q) * UP_LDB + wn * 16 + nt * 8 + g];
-      bi[nt] = Bi[(kk + q) * UP_LDB + wn * 16 + nt * 8 + g];
+    for (int e = t; e < LU_W * UP_BN; e += UP_TH) {
+      const int r = e / UP_BN, c = e % UP_BN;
+      const double2 x = (r < wq && cb + c < cend) ? A[(size_t)(kc + r) * lda + cb + c] : cz();
+      Br[r * UP_LDB + c] = x.x;
+      Bi[r * UP_LDB + c] = x.y;
     }
+    __syncthreads();
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
+    for (int k4 = 0; k4 < LU_W; k4 += 4) {
+      double ar[4], ai[4], br[2], bi[2];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        ar[mt] = Ar[(wm * 32 + mt * 8 + g) * UP_LDA + k4 + q];
+        ai[mt] = Ai[(wm * 32 + mt * 8 + g) * UP_LDA + k4 + q];
+      }
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
-        // (cr, ci) -= (ar + i ai)(br + i bi)
-        dmma(-ar[mt], br[nt], cr[mt][nt]);
-        dmma(ai[mt], bi[nt], cr[mt][nt]);
-        dmma(-ar[mt], bi[nt], ci[mt][nt]);
-        dmma(-ai[mt], br[nt], ci[mt][nt]);
+        br[nt] = Br[(k4 + q) * UP_LDB + wn * 16 + nt * 8 + g];
+        bi[nt] = Bi[(k4 + q) * UP_LDB + wn * 16 + nt * 8 + g];
       }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          // (cr, ci) -= (ar + i ai)(br + i bi)
+          dmma(-ar[mt], br[nt], cr[mt][nt]);
+          dmma(ai[mt], bi[nt], cr[mt][nt]);
+          dmma(-ar[mt], bi[nt], ci[mt][nt]);
+          dmma(-ai[mt], br[nt], ci[mt][nt]);
+        }
+    }
   }
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
@@ -575,7 +605,7 @@ __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, in
       const int row = rb + wm * 32 + mt * 8 + g, col = cb + wn * 16 + nt * 8 + 2 * q;
 #pragma unroll
       for (int i = 0; i < 2; ++i)
-        if (row < n && col + i < n) A[(size_t)row * lda + col + i] = make_double2(cr[mt][nt][i], ci[mt][nt][i]);
+        if (row < n && col + i < cend) A[(size_t)row * lda + col + i] = make_double2(cr[mt][nt][i], ci[mt][nt][i]);
     }
 }
 
@@ -583,22 +613,12 @@ __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, in
 // outputs per thread (rows ty*4 + i, columns tx + 16 j: conflict-free shared
 // loads and 128-byte runs of C per 16 threads)
 #define UF_TH 256
-__global__ void __launch_bounds__(UF_TH) k_lu_update_c32(float2 *A, long lda, int n, int k) {
+__global__ void __launch_bounds__(UF_TH) k_lu_update_c32(float2 *A, long lda, int n, int kk, int kw, int r0,
+                                                         int cend) {
   __shared__ float2 As[UP_BM][LU_W + 1];
   __shared__ float2 Bs[LU_W][UP_BN + 1];
   const int t = threadIdx.x;
-  const int w = min(LU_W, n - k);
-  const int r0 = k + w;
   const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
-  for (int e = t; e < UP_BM * LU_W; e += UF_TH) {
-    const int r = e / LU_W, c = e % LU_W;
-    As[r][c] = (rb + r < n && c < w) ? A[(size_t)(rb + r) * lda + k + c] : make_float2(0.f, 0.f);
-  }
-  for (int e = t; e < LU_W * UP_BN; e += UF_TH) {
-    const int r = e / UP_BN, c = e % UP_BN;
-    Bs[r][c] = (r < w && cb + c < n) ? A[(size_t)(k + r) * lda + cb + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
   const int ty = t >> 4, tx = t & 15;
   float2 acc[4][4];
 #pragma unroll
@@ -606,26 +626,111 @@ __global__ void __launch_bounds__(UF_TH) k_lu_update_c32(float2 *A, long lda, in
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int row = rb + ty * 4 + i, col = cb + tx + 16 * j;
-      acc[i][j] = (row < n && col < n) ? A[(size_t)row * lda + col] : make_float2(0.f, 0.f);
+      acc[i][j] = (row < n && col < cend) ? A[(size_t)row * lda + col] : make_float2(0.f, 0.f);
     }
-  for (int kk = 0; kk < w; ++kk) {
-    float2 a[4], b[4];
+  for (int q0 = 0; q0 < kw; q0 += LU_W) {
+    const int wq = min(LU_W, kw - q0), kc = kk + q0;
+    if (q0) __syncthreads();
+    for (int e = t; e < UP_BM * LU_W; e += UF_TH) {
+      const int r = e / LU_W, c = e % LU_W;
+      As[r][c] = (rb + r < n && c < wq) ? A[(size_t)(rb + r) * lda + kc + c] : make_float2(0.f, 0.f);
+    }
+    for (int e = t; e < LU_W * UP_BN; e += UF_TH) {
+      const int r = e / UP_BN, c = e % UP_BN;
+      Bs[r][c] = (r < wq && cb + c < cend) ? A[(size_t)(kc + r) * lda + cb + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k1 = 0; k1 < LU_W; ++k1) {
+      float2 a[4], b[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][kk];
+      for (int i = 0; i < 4; ++i) a[i] = As[ty * 4 + i][k1];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k1][tx + 16 * j];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = cfms(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; ++j) acc[i][j] = cfms(a[i], b[j], acc[i][j]);
+    }
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int row = rb + ty * 4 + i, col = cb + tx + 16 * j;
-      if (row < n && col < n) A[(size_t)row * lda + col] = acc[i][j];
+      if (row < n && col < cend) A[(size_t)row * lda + col] = acc[i][j];
     }
+}
+
+// ---------------------------------------------------------------- U12 of an outer block
+// U12 = L11^-1 A12 in place for the outer block's rows K .. K + ob - 1 and the
+// columns right of it (L11 unit lower, in A's strictly lower part, its
+// diagonal blocks' inverses in the LINV slots): block row ib gets
+// Linv_ib (A12_ib - sum_{jb < ib} L_ib,jb U12_jb).  One CTA per TR_NC
+// columns; thread (i, c) holds row i of a block row and columns c, c + 4,
+// c + 8, c + 12 (conflict-free shared-memory reads: a warp reads 8 rows of L
+// at one column and 4 consecutive columns of X).
+#define TR_TH 128
+#define TR_NC 16
+template <class C2>
+struct trsm_sh {
+  C2 X[LU_OB][TR_NC + 1];
+  C2 L[LU_W][LU_W + 1];
+  C2 Y[LU_W][TR_NC + 1];
+};
+template <class C2>
+__global__ void __launch_bounds__(TR_TH) k_lu_trsm(C2 *A, long lda, int n, int K, int ob, const C2 *u) {
+  extern __shared__ __align__(16) unsigned char tr_raw[];
+  trsm_sh<C2> &S = *reinterpret_cast<trsm_sh<C2> *>(tr_raw);
+  const int t = threadIdx.x;
+  const int c0 = K + ob + blockIdx.x * TR_NC;
+  const int nbk = ob / LU_W;
+  for (int e = t; e < ob * TR_NC; e += TR_TH) {
+    const int r = e / TR_NC, c = e % TR_NC;
+    S.X[r][c] = c0 + c < n ? A[(size_t)(K + r) * lda + c0 + c] : czero<C2>();
+  }
+  const int i = t >> 2, cq = t & 3;  // row i of a block row, columns cq + 4 j
+  for (int ib = 0; ib < nbk; ++ib) {
+    C2 acc[4];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = S.X[ib * LU_W + i][cq + 4 * j];
+    for (int jb = 0; jb < ib; ++jb) {
+      for (int e = t; e < LU_W * LU_W; e += TR_TH) {
+        const int r = e / LU_W, c = e % LU_W;
+        S.L[r][c] = A[(size_t)(K + ib * LU_W + r) * lda + K + jb * LU_W + c];
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int l = 0; l < LU_W; ++l) {
+        const C2 lv = S.L[i][l];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] = cfms(lv, S.X[jb * LU_W + l][cq + 4 * j], acc[j]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) S.Y[i][cq + 4 * j] = acc[j];
+    const C2 *linv = u + U_LINV + ib * (LU_W * LU_W);
+    for (int e = t; e < LU_W * LU_W; e += TR_TH) S.L[e / LU_W][e % LU_W] = __ldcg(linv + e);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = czero<C2>();
+#pragma unroll 8
+    for (int l = 0; l < LU_W; ++l) {
+      const C2 lv = S.L[i][l];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[j] = cfma(lv, S.Y[l][cq + 4 * j], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) S.X[ib * LU_W + i][cq + 4 * j] = acc[j];
+    __syncthreads();  // Y and L are rewritten by the next block row
+  }
+  __syncthreads();
+  for (int e = t; e < ob * TR_NC; e += TR_TH) {
+    const int r = e / TR_NC, c = e % TR_NC;
+    if (c0 + c < n) A[(size_t)(K + r) * lda + c0 + c] = S.X[r][c];
+  }
 }
 
 // R = B - A X in FP64 (refinement residual): A row-major n x n, X, B, R
@@ -844,6 +949,12 @@ extern "C" int bem_lu_init(bem_lu *w, int device) {
                            (int)sizeof(panel_sh<float2>)),
       "panel smem");
   CKL(cudaFuncSetAttribute(k_lu_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UP_SMEM), "update smem");
+  CKL(cudaFuncSetAttribute(k_lu_trsm<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(trsm_sh<double2>)),
+      "U12 smem");
+  CKL(cudaFuncSetAttribute(k_lu_trsm<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(trsm_sh<float2>)),
+      "U12 smem");
   int per_sm = 0;
   CKL(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_trsv<double2, 4>, TS_TH, 0), "solve occupancy");
   w->coop_blocks = per_sm * w->sms;
@@ -880,36 +991,55 @@ static int grow_bytes(bem_lu *w, void **p, size_t *cap, size_t bytes, const char
   return 0;
 }
 
-static void launch_update(double2 *A, int n, int k, int tiles, cudaStream_t st) {
-  k_lu_update<<<dim3(tiles, tiles), UP_TH, UP_SMEM, st>>>(A, n, n, k);
+// C = A[r0:n, r0:cend) -= A[r0:n, kk:kk+kw) A[kk:kk+kw, r0:cend)
+static void launch_update(double2 *A, int n, int kk, int kw, int r0, int cend, cudaStream_t st) {
+  const dim3 grid((cend - r0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
+  k_lu_update<<<grid, UP_TH, UP_SMEM, st>>>(A, n, n, kk, kw, r0, cend);
 }
-static void launch_update(float2 *A, int n, int k, int tiles, cudaStream_t st) {
-  k_lu_update_c32<<<dim3(tiles, tiles), UF_TH, 0, st>>>(A, n, n, k);
+static void launch_update(float2 *A, int n, int kk, int kw, int r0, int cend, cudaStream_t st) {
+  const dim3 grid((cend - r0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
+  k_lu_update_c32<<<grid, UF_TH, 0, st>>>(A, n, n, kk, kw, r0, cend);
 }
 
-// the tensor-core update of a complex FP32 panel when the LU has one
-// (returns 1 when launched)
-static int tc_update(bem_lu *w, double2 *, int, int, int, cudaStream_t) { (void)w; return 0; }
-static int tc_update(bem_lu *w, float2 *A, int n, int k, int wd, cudaStream_t st) {
+// an outer block's update of a complex FP32 factorisation on the tensor cores
+// when the LU has them (returns 1 when launched)
+static int tc_update(bem_lu *w, double2 *, int, int, cudaStream_t) { (void)w; return 0; }
+static int tc_update(bem_lu *w, float2 *A, int n, int K, cudaStream_t st) {
   if (!w->tc || !w->tc->ready) return 0;
-  bem_tc_launch(w->tc, A, n, n, k, wd, w->status, st);
+  bem_tc_launch(w->tc, A, n, n, K, w->status, st);
   return 1;
 }
 
 // the launches of one factorisation, in order (captured into the graph, whose
-// replays count them)
+// replays count them).  Outer blocks of LU_OB columns: each panel's update
+// covers only the rest of its outer block; the columns right of the block get
+// the row moves as the panels go, then U12 (k_lu_trsm) and one rank-LU_OB
+// update, so the trailing matrix is read and written once per outer block
+// instead of once per panel.
 template <class C2>
 static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
   k_lu_iota<<<(n + 255) / 256, 256, 0, st>>>(w->rowmap, n);
-  for (int k = 0; k < n; k += LU_W) {
-    const int wd = n - k < LU_W ? n - k : LU_W;
-    const int r0 = k + wd;
-    k_lu_panel<C2><<<LU_CL, LU_TH, sizeof(panel_sh<C2>), st>>>(A, n, n, k, w->piv, (C2 *)w->u11, w->status);
-    const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
-    const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
-    k_lu_apply<C2><<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, w->piv, (const C2 *)w->u11, w->rowmap, w->status);
-    if (r0 < n) {
-      if (tc_update(w, A, n, k, wd, st) == 0) launch_update(A, n, k, (n - r0 + UP_BM - 1) / UP_BM, st);
+  // up to one_block_max the whole matrix is one outer block (every panel
+  // updates the whole trailing matrix: fewer, shorter launches on the
+  // critical path of a small factorisation)
+  const int one_block = w->one_block_max > 0 ? w->one_block_max : LU_ONE_BLOCK_N;
+  const int obw = n <= one_block ? n : LU_OB;
+  for (int K = 0; K < n; K += obw) {
+    const int cend = n - K < obw ? n : K + obw;
+    for (int k = K; k < cend; k += LU_W) {
+      const int wd = n - k < LU_W ? n - k : LU_W;
+      const int r0 = k + wd;
+      k_lu_panel<C2><<<LU_CL, LU_TH, sizeof(panel_sh<C2>), st>>>(A, n, n, k, w->piv, (C2 *)w->u11, w->status);
+      const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
+      const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
+      k_lu_apply<C2><<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, cend, w->piv, (const C2 *)w->u11, w->rowmap,
+                                                    w->status);
+      if (r0 < cend) launch_update(A, n, k, wd, r0, cend, st);
+    }
+    if (cend < n) {
+      k_lu_trsm<C2><<<(n - cend + TR_NC - 1) / TR_NC, TR_TH, sizeof(trsm_sh<C2>), st>>>(A, n, n, K, cend - K,
+                                                                                         (const C2 *)w->u11);
+      if (tc_update(w, A, n, K, st) == 0) launch_update(A, n, K, cend - K, cend, n, st);
     }
   }
   CKL(cudaGetLastError(), "LU launch");
@@ -922,7 +1052,7 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
   C2 *A = (C2 *)Av;
   if (grow_bytes(w, (void **)&w->rowmap, &w->rowmap_cap, (size_t)n * sizeof(int), "row map")) return -1;
   const int tcmode = (sizeof(C2) == sizeof(float2) && w->tc && w->tc->ready) ? w->tc->nprod : 0;
-  if (!(w->gexec && w->g_A == Av && w->g_n == n && w->g_tc == tcmode)) {
+  if (!(w->gexec && w->g_A == Av && w->g_n == n && w->g_tc == tcmode && w->g_obm == w->one_block_max)) {
     if (w->gexec) cudaGraphExecDestroy(w->gexec);
     if (w->graph) cudaGraphDestroy(w->graph);
     w->gexec = nullptr;
@@ -941,6 +1071,7 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
     size_t nodes = 0;
     CKL(cudaGraphGetNodes(g, nullptr, &nodes), "LU graph");
     w->g_nodes = nodes;
+    w->g_obm = w->one_block_max;
     w->g_A = Av;
     w->g_n = n;
     w->g_tc = tcmode;
@@ -950,6 +1081,7 @@ static int lu_factor(bem_lu *w, void *Av, int n, cudaStream_t st) {
   return 0;
 }
 
+extern "C" void bem_lu_set_one_block(bem_lu *w, int nmax) { w->one_block_max = nmax; }
 extern "C" int bem_lu_factor_z(bem_lu *w, double *A, int n, cudaStream_t st) { return lu_factor<double2>(w, A, n, st); }
 extern "C" int bem_lu_factor_c(bem_lu *w, float *A, int n, cudaStream_t st) { return lu_factor<float2>(w, A, n, st); }
 

@@ -9,6 +9,7 @@
 #include "bem_tc.h"
 
 #define BEM_LU_W 32            // panel width (columns factored per panel)
+#define BEM_LU_OB 128          // outer block: trailing updates right of it are applied once per block
 #define BEM_LU_ST_ZERO 0x20u   // a zero pivot (singular matrix), as BEMGPU_ST_SOLVE
 #define BEM_LU_ST_WAIT 0x40u   // a triangular-solve wait gave up (no hang; result invalid)
 #define BEM_LU_ST_INTERNAL 0x80u  // a row move out of range (skipped; result invalid)
@@ -27,10 +28,11 @@ struct bem_lu {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   const void *g_A = nullptr;
-  int g_n = 0, g_tc = -1;
+  int g_n = 0, g_tc = -1, g_obm = 0;
   size_t g_nodes = 0;   // kernels in the captured graph (launch count per replay)
   bem_tc *tc = nullptr;       // complex FP32 only: trailing updates on the tensor cores when set
   int sms = 0, coop_blocks = 0;  // device facts for the launches
+  int one_block_max = 0;      // largest n factored as one outer block (0: the default, 2048)
   char err[200] = {0};
 };
 
@@ -50,6 +52,8 @@ int bem_lu_solve_c(bem_lu *w, const float *LU, int n, int nrhs, float *B, cudaSt
 // R = B - A X in FP64 (A row-major n x n, X, B, R column-major n x nrhs,
 // nrhs <= 4): the refinement residual.
 int bem_lu_resid_z(const double *A, int n, int nrhs, const double *X, const double *B, double *R, cudaStream_t st);
+// Largest n factored as one outer block (bem_lu.one_block_max; 0: default).
+void bem_lu_set_one_block(bem_lu *w, int nmax);
 // Status bits (BEM_LU_ST_*) accumulated since the last call; waits for st.
 unsigned bem_lu_status(bem_lu *w, cudaStream_t st);
 }

@@ -71,18 +71,21 @@ struct owned_problem {
 };
 
 // device bytes a resident problem holds: global matrix n^2 16 B, per domain
-// G, H, dpv factors 3 N_d^2 16 B (+ dG, dH 4 N_d^2 16 B for interior domains),
-// FP32 factors in mixed precision, and element tables / scratch
-size_t problem_bytes(const bemgpu_problem *p, int precision) {
+// G, H, dpv factors 3 N_d^2 16 B (+ dG, dH 4 N_d^2 16 B for interior domains
+// when they are kept, else one 512 MiB block of recomputed rows), FP32 factors
+// in mixed precision, and element tables / scratch
+size_t problem_bytes(const bemgpu_problem *p, int precision, bool keep_dgh) {
   const size_t n = 2 * (size_t)p->NN;
   size_t b = n * n * 16, f32 = n * n * 8;
   for (int d = 0; d <= p->MN; ++d) {
     const size_t N = 4 * (size_t)p->dom_ne[d];
     // matrices, pair flags (and the periodic domain's 4-byte pair lists), near-singular tables
-    b += 3 * N * N * 16 + (d > 0 ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] * (d == 0 ? 5 : 1) + N * 256 * 28;
+    b += 3 * N * N * 16 + (d > 0 && keep_dgh ? 4 * N * N * 16 : 0) + N * (size_t)p->dom_ne[d] * (d == 0 ? 5 : 1) +
+         N * 256 * 28;
     f32 += N * N * 8;
   }
   if (precision) b += f32;
+  if (!keep_dgh && p->MN >= 1) b += (size_t)512 << 20;
   return b + (size_t)p->Ne * 512 + (64u << 20);  // tables, workspace of the solvers
 }
 
@@ -112,12 +115,13 @@ struct request {
   owned_problem prob;
   unsigned long long key, ikey;
   int precision, force_type;
+  bool keep_dgh = true;  // interior derivative rows kept (false: recomputed in blocks)
   double rc[3];
   size_t bytes;
   double t_submit, t_start = 0;
   request(const bemgpu_problem *p, unsigned long long k, int prec, int ft, const double *r, long long i)
-      : id(i), prob(p), key(k), ikey(interior_key(p)), precision(prec), force_type(ft), bytes(problem_bytes(p, prec)),
-        t_submit(now_ms()) {
+      : id(i), prob(p), key(k), ikey(interior_key(p)), precision(prec), force_type(ft),
+        bytes(problem_bytes(p, prec, true)), t_submit(now_ms()) {
     for (int j = 0; j < 3; ++j) rc[j] = r ? r[j] : 0.0;
   }
 };
@@ -129,6 +133,7 @@ struct slot {
   unsigned long long key = 0;    // reuse key of the resident problem
   unsigned long long ikey = 0;   // interior key of the resident problem
   int precision = -1;
+  bool keep_dgh = true;          // the resident problem's interior derivative rows are kept
   bool resident = false;         // a problem (and its factors) is loaded
   bool evict = false;            // free the resident problem before the next request
   size_t bytes = 0;              // device bytes of the resident problem
@@ -274,10 +279,12 @@ static void worker(bemgpu_server *s, int idx) {
       // unless the problem is on the same body at the same frequency, whose
       // buffers have this problem's sizes and whose interior matrices and
       // factors the context keeps
-      const bool same_interior = sl.resident && sl.ikey == r->ikey && sl.precision == r->precision;
+      const bool same_interior =
+          sl.resident && sl.ikey == r->ikey && sl.precision == r->precision && sl.keep_dgh == r->keep_dgh;
       sl.resident = false;
       rc = same_interior ? 0 : bemgpu_unload(sl.ctx);
       if (!rc && !same_interior) rc = bemgpu_set_precision(sl.ctx, r->precision);
+      if (!rc && !same_interior) rc = bemgpu_set_interior_derivatives(sl.ctx, r->keep_dgh ? 1 : 0, 0);
       if (!rc) rc = bemgpu_load(sl.ctx, &r->prob.p);
       if (!rc) rc = bemgpu_run(sl.ctx);
     }
@@ -307,6 +314,7 @@ static void worker(bemgpu_server *s, int idx) {
         sl.key = r->key;
         sl.ikey = r->ikey;
         sl.precision = r->precision;
+        sl.keep_dgh = r->keep_dgh;
         if (reuse) ++s->reused;
       }
       ++s->completed;
@@ -340,10 +348,18 @@ extern "C" int bemgpu_server_submit(bemgpu_server *s, const bemgpu_problem *p, u
                                     int precision, int force_type, const double *rc, long long id) {
   request *r = new request(p, reuse_key, precision, force_type, rc, id);
   std::lock_guard<std::mutex> lk(s->mu);
-  if (r->bytes > s->budget && r->precision != 0) {
-    // the FP32 factors do not fit beside the FP64 matrices: run it in FP64
-    r->precision = 0;
-    r->bytes = problem_bytes(p, 0);
+  if (r->bytes > s->budget) {
+    // too large as asked: first recompute the interior derivative rows in
+    // blocks instead of keeping them, then give up the FP32 factors (FP64
+    // with the rows kept, then recomputed)
+    const int prec = r->precision;
+    const struct { int prec; bool keep; } tries[3] = {{prec, false}, {0, true}, {0, false}};
+    for (const auto &tr : tries) {
+      r->precision = tr.prec;
+      r->keep_dgh = tr.keep;
+      r->bytes = problem_bytes(p, tr.prec, tr.keep);
+      if (r->bytes <= s->budget) break;
+    }
   }
   if (r->bytes > s->budget) { delete r; return -2; }  // can never be admitted
   s->queue.push_back(r);

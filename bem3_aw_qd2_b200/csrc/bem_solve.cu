@@ -124,20 +124,22 @@ __device__ __forceinline__ void inv33(double *ma, const double *vn, const double
 }
 
 // one warp per collocation row p of interior domain d
+// rows p0 .. p0 + np - 1; dG, dH hold rows 2 (p - p0) and 2 (p - p0) + 1
 __global__ void k_pv_interior(bem_sys_dev S, int d, const double *__restrict__ dG, const double *__restrict__ dH,
                               const double *__restrict__ dF, const double *__restrict__ P, const double *__restrict__ dP,
-                              double *__restrict__ pv, double *__restrict__ tpv) {
+                              double *__restrict__ pv, double *__restrict__ tpv, int p0, int np) {
   const int Nd = S.dom_ne[d] * 4;
-  const int p = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int p = p0 + blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
-  if (p >= Nd) return;
+  if (p >= p0 + np || p >= Nd) return;
   const int t = p >> 2, tn = p & 3;
   const int at = S.sid[S.dom_off[d] + t];
   const int atd = abs(at) - 1;
   if (tn >= S.npe[atd]) return;
   zc az = zmk(0, 0), ae = zmk(0, 0);
-  const double *rz = dG + 2 * (size_t)(2 * p) * Nd, *re = dG + 2 * (size_t)(2 * p + 1) * Nd;
-  const double *hz = dH + 2 * (size_t)(2 * p) * Nd, *he = dH + 2 * (size_t)(2 * p + 1) * Nd;
+  const size_t r2 = 2 * (size_t)(p - p0);
+  const double *rz = dG + 2 * r2 * Nd, *re = dG + 2 * (r2 + 1) * Nd;
+  const double *hz = dH + 2 * r2 * Nd, *he = dH + 2 * (r2 + 1) * Nd;
   for (int c = lane; c < Nd; c += 32) {
     const zc dp = zld(dP + 2 * c), pp = zld(P + 2 * c);
     az = zadd(az, zsub(zmul(zld(rz + 2 * c), dp), zmul(zld(hz + 2 * c), pp)));
@@ -361,10 +363,17 @@ extern "C" int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, cons
   if (d == 0) {
     k_pv_exterior<<<(n + 127) / 128, 128, 0, st>>>(*S, tpv, pv);
     bem_count_launches(1);
-  } else {
-    k_pv_interior<<<(n + 7) / 8, 256, 0, st>>>(*S, d, dG, dH, dF, P, dP, pv, tpv);
-    bem_count_launches(1);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
   }
+  return bem_launch_pv_rows(S, d, dG, dH, dF, P, dP, pv, tpv, 0, n, st);
+}
+
+extern "C" int bem_launch_pv_rows(const bem_sys_dev *S, int d, const double *dG, const double *dH, const double *dF,
+                                  const double *P, const double *dP, double *pv, double *tpv, int p0, int np,
+                                  cudaStream_t st) {
+  if (np <= 0) return 0;
+  k_pv_interior<<<(np + 7) / 8, 256, 0, st>>>(*S, d, dG, dH, dF, P, dP, pv, tpv, p0, np);
+  bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -30,6 +30,9 @@ int bem_launch_gather(const bem_sys_dev *S, int d, const double *G, const double
 int bem_launch_store(const bem_sys_dev *S, int d, const double *X, double *P, double *dP, cudaStream_t st);
 int bem_launch_pv(const bem_sys_dev *S, int d, const double *dG, const double *dH, const double *dF, const double *P,
                   const double *dP, double *pv, double *tpv, cudaStream_t st);
+// interior domain d, rows p0 .. p0 + np - 1, with dG, dH holding only those rows
+int bem_launch_pv_rows(const bem_sys_dev *S, int d, const double *dG, const double *dH, const double *dF,
+                       const double *P, const double *dP, double *pv, double *tpv, int p0, int np, cudaStream_t st);
 int bem_launch_dpv_rhs(int Nd, const double *H, const double *pv, double *B, cudaStream_t st);
 int bem_launch_dpv_store(int Nd, const double *B, double *dpv, cudaStream_t st);
 // domains with triangles: dpv system without the padding rows / columns

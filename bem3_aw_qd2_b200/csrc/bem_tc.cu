@@ -1,8 +1,9 @@
 // Trailing update of the complex FP32 LU on the fifth-generation tensor cores
-// (tcgen05, Blackwell): C -= L21 U12 for one 32-column panel of the
-// mixed-precision factorisation (bem_lu.cu), in place of the CUDA-core
-// update.  No counterpart in the reference, whose solves are FP64
-// (b_mkl_solver_pardiso_d, d3qd2_mkl_solver.c:18-148).
+// (tcgen05, Blackwell): C -= L21 U12 for one outer block (BEM_LU_OB = 128
+// columns, four 32-column panels) of the mixed-precision factorisation
+// (bem_lu.cu), in place of the CUDA-core update.  No counterpart in the
+// reference, whose solves are FP64 (b_mkl_solver_pardiso_d,
+// d3qd2_mkl_solver.c:18-148).
 //
 // The complex product is one real GEMM: a row of L21 read as 2K reals
 // (re, im interleaved) times, for output column c, the 2K reals
@@ -11,13 +12,16 @@
 // is split x = hi + lo (hi rounded to TF32) and the product is
 // hi hi + hi lo + lo hi: close to FP32 accuracy; nprod = 1 is a single TF32
 // product.  A pack kernel writes the operands K-major (A'' rows: L21 rows;
-// B'' rows: 64 real-part then 64 imaginary-part columns per tile); each CTA
-// loads its 128 x 128-row tiles with 2D TMA into 128-byte-swizzled shared
-// memory, one thread issues the MMAs into a 128 x 128 FP32 accumulator in
-// TMEM, and four warps read it back (tcgen05.ld) and subtract it from C.
-// Every wait on an mbarrier is bounded: a wait that gives up sets
-// BEM_TC_ST_WAIT, waits (bounded) for the copies in flight, frees the TMEM and
-// returns.  The TMA loads read this GPU's own memory and use no multicast.
+// B'' rows: 64 real-part then 64 imaginary-part columns per tile).  Each CTA
+// computes a 128-row x 64-complex-column tile: one thread streams the
+// 128-byte-wide K boxes of both operands with 2D TMA into a ring of
+// shared-memory stages (128-byte swizzle), another issues the MMAs into a
+// 128 x 128 FP32 accumulator in TMEM and frees each stage with
+// tcgen05.commit, and the four warps read the accumulator back (tcgen05.ld)
+// and subtract it from C.  Every wait on an mbarrier is bounded: a wait that
+// gives up sets BEM_TC_ST_WAIT, waits (bounded) for the copies and MMAs in
+// flight, frees the TMEM and returns.  The TMA loads read this GPU's own
+// memory and use no multicast.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -30,30 +34,31 @@
 #define TC_TH 128       // four warps: one TMEM lane quarter each
 #define TC_BOX_K 32     // FP32 elements per 128-byte swizzle row
 #define TC_BOX_BYTES (TC_M * 128)
+#define TC_STAGES 2     // K boxes in flight (A and B box each: 32 KB a stage)
+#define TC_KR (2 * LU_OUTER_W)  // reals of one product part of a packed row
 #define TC_WAIT_NS 1000000000ull  // one second
 
 // ---------------------------------------------------------------- packing
-// A'' [rows][64 nprod]: [hi(a) | hi(a) | lo(a)] of the 2K = 64 reals of L21's
-// row (nprod 3) or [a] (nprod 1); B'' [tile rows][64 nprod]: [hi(b) | lo(b) |
-// hi(b)] or [b] of the 64 reals of an output column (see above).
+// A'' [rows][TC_KR nprod]: [hi(a) | hi(a) | lo(a)] of the 2K reals of L21's
+// row (nprod 3) or [a] (nprod 1); B'' [tile rows][TC_KR nprod]: [hi(b) |
+// lo(b) | hi(b)] or [b] of the 2K reals of an output column (see above).
 __device__ __forceinline__ float tf32_hi(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
 }
 
-__global__ void k_tc_pack(const float2 *__restrict__ M, long lda, int n, int k, int w, int nprod,
+__global__ void k_tc_pack(const float2 *__restrict__ M, long lda, int n, int K, int r0, int nprod,
                           float *__restrict__ Ap, float *__restrict__ Bp, int rows, int ntiles) {
-  const int kp = 64 * nprod;
-  const int r0 = k + w;
+  const int kp = TC_KR * nprod;
   // A'': one thread per (row, k)
-  const long na = (long)rows * LU_PANEL_W;
-  const long nb = (long)ntiles * TC_NC * LU_PANEL_W;
+  const long na = (long)rows * LU_OUTER_W;
+  const long nb = (long)ntiles * TC_NC * LU_OUTER_W;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < na + nb; e += (long)gridDim.x * blockDim.x) {
     if (e < na) {
-      const int r = (int)(e / LU_PANEL_W), kk = (int)(e % LU_PANEL_W);
+      const int r = (int)(e / LU_OUTER_W), kk = (int)(e % LU_OUTER_W);
       const int row = r0 + r;
-      const float2 a = (row < n && kk < w) ? M[(size_t)row * lda + k + kk] : make_float2(0.f, 0.f);
+      const float2 a = row < n ? M[(size_t)row * lda + K + kk] : make_float2(0.f, 0.f);
       float *dst = Ap + (size_t)r * kp;
       if (nprod == 1) {
         dst[2 * kk] = a.x;
@@ -61,14 +66,14 @@ __global__ void k_tc_pack(const float2 *__restrict__ M, long lda, int n, int k, 
       } else {
         const float hx = tf32_hi(a.x), hy = tf32_hi(a.y);
         dst[2 * kk] = hx; dst[2 * kk + 1] = hy;
-        dst[64 + 2 * kk] = hx; dst[64 + 2 * kk + 1] = hy;
-        dst[128 + 2 * kk] = a.x - hx; dst[128 + 2 * kk + 1] = a.y - hy;
+        dst[TC_KR + 2 * kk] = hx; dst[TC_KR + 2 * kk + 1] = hy;
+        dst[2 * TC_KR + 2 * kk] = a.x - hx; dst[2 * TC_KR + 2 * kk + 1] = a.y - hy;
       }
     } else {
       const long f = e - na;
-      const int cc = (int)(f / LU_PANEL_W), kk = (int)(f % LU_PANEL_W);
+      const int cc = (int)(f / LU_OUTER_W), kk = (int)(f % LU_OUTER_W);
       const int col = r0 + cc;
-      const float2 b = (col < n && kk < w) ? M[(size_t)(k + kk) * lda + col] : make_float2(0.f, 0.f);
+      const float2 b = col < n ? M[(size_t)(K + kk) * lda + col] : make_float2(0.f, 0.f);
       const int tile = cc / TC_NC, j = cc % TC_NC;
       float *re = Bp + (size_t)(tile * 2 * TC_NC + j) * kp, *im = Bp + (size_t)(tile * 2 * TC_NC + TC_NC + j) * kp;
       // real output: (Re b, -Im b); imaginary output: (Im b, Re b)
@@ -80,11 +85,11 @@ __global__ void k_tc_pack(const float2 *__restrict__ M, long lda, int n, int k, 
         float h[4];
         for (int q = 0; q < 4; ++q) h[q] = tf32_hi(v[q]);
         re[2 * kk] = h[0]; re[2 * kk + 1] = h[1];
-        re[64 + 2 * kk] = v[0] - h[0]; re[64 + 2 * kk + 1] = v[1] - h[1];
-        re[128 + 2 * kk] = h[0]; re[128 + 2 * kk + 1] = h[1];
+        re[TC_KR + 2 * kk] = v[0] - h[0]; re[TC_KR + 2 * kk + 1] = v[1] - h[1];
+        re[2 * TC_KR + 2 * kk] = h[0]; re[2 * TC_KR + 2 * kk + 1] = h[1];
         im[2 * kk] = h[2]; im[2 * kk + 1] = h[3];
-        im[64 + 2 * kk] = v[2] - h[2]; im[64 + 2 * kk + 1] = v[3] - h[3];
-        im[128 + 2 * kk] = h[2]; im[128 + 2 * kk + 1] = h[3];
+        im[TC_KR + 2 * kk] = v[2] - h[2]; im[TC_KR + 2 * kk + 1] = v[3] - h[3];
+        im[2 * TC_KR + 2 * kk] = h[2]; im[2 * TC_KR + 2 * kk + 1] = h[3];
       }
     }
   }
@@ -164,23 +169,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 }
 
 // ---------------------------------------------------------------- the update
-// grid: (column tiles, row tiles); smem: A tile then B tile, each
-// (64 nprod / 32) swizzle boxes of TC_M rows x 128 bytes
-__global__ void __launch_bounds__(TC_TH, 1)
+// grid: (column tiles, row tiles); dynamic smem: TC_STAGES stages of an A box
+// and a B box (TC_M rows x 128 bytes each)
+__global__ void __launch_bounds__(TC_TH, 3)
     k_tc_update(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2 *C, long ldc,
-                int n, int r0, int nprod, unsigned *status) {
+                int n, int r0, int nbox, unsigned *status) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-  __shared__ __align__(8) uint64_t bar_full, bar_done;
+  __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_empty[TC_STAGES], bar_done;
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail;
   unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
-  const int nbox = 2 * nprod;  // 128-byte boxes per operand row (64 nprod FP32)
-  unsigned char *sA = sm, *sB = sm + (size_t)nbox * TC_BOX_BYTES;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int row_tile = r0 + blockIdx.y * TC_M;   // matrix row of the tile's first row
   const int col_tile = blockIdx.x;               // column tile (TC_NC complex columns)
   if (t == 0) {
-    mbar_init(&bar_full, 1);
+    for (int s = 0; s < TC_STAGES; ++s) {
+      mbar_init(&bar_full[s], 1);
+      mbar_init(&bar_empty[s], 1);
+    }
     mbar_init(&bar_done, 1);
     s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -196,43 +202,67 @@ __global__ void __launch_bounds__(TC_TH, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
-  if (t == 0) {
-    mbar_expect_tx(&bar_full, (uint32_t)(2 * nbox * TC_BOX_BYTES));
-    for (int bx = 0; bx < nbox; ++bx) {
-      tma_load_2d(sA + (size_t)bx * TC_BOX_BYTES, &tmA, bx * TC_BOX_K, row_tile - r0, &bar_full);
-      tma_load_2d(sB + (size_t)bx * TC_BOX_BYTES, &tmB, bx * TC_BOX_K, col_tile * 2 * TC_NC, &bar_full);
-    }
-    if (!mbar_wait(&bar_full, 0)) {
-      atomicOr(status, BEM_TC_ST_WAIT);
-      s_fail = 1;
-      mbar_wait(&bar_full, 0);  // the copies in flight, bounded once more
-    } else {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // K steps of 8 TF32 (32 bytes) within each 128-byte swizzle row
-      const int steps = nbox * 4;
-      for (int s = 0; s < steps; ++s) {
-        const uint32_t off = (uint32_t)(s >> 2) * TC_BOX_BYTES + (uint32_t)(s & 3) * 32u;
-        tc_mma(tmem, umma_desc(smem_u32(sA) + off), umma_desc(smem_u32(sB) + off), s > 0 ? 1u : 0u);
+  if (warp == 0 && lane == 0) {
+    // producer: box b into stage b % TC_STAGES once the MMAs of box b - TC_STAGES freed it
+    int issued = 0;
+    for (int b = 0; b < nbox; ++b) {
+      const int s = b % TC_STAGES;
+      if (b >= TC_STAGES && !mbar_wait(&bar_empty[s], (uint32_t)((b / TC_STAGES) - 1) & 1u)) {
+        atomicOr(status, BEM_TC_ST_WAIT);
+        s_fail = 1;
+        break;
       }
-      tc_commit(&bar_done);
+      unsigned char *sA = sm + (size_t)s * 2 * TC_BOX_BYTES, *sB = sA + TC_BOX_BYTES;
+      mbar_expect_tx(&bar_full[s], (uint32_t)(2 * TC_BOX_BYTES));
+      tma_load_2d(sA, &tmA, b * TC_BOX_K, row_tile - r0, &bar_full[s]);
+      tma_load_2d(sB, &tmB, b * TC_BOX_K, col_tile * 2 * TC_NC, &bar_full[s]);
+      issued = b + 1;
     }
+    // the copies still in flight land before the CTA may end (bounded)
+    for (int b = issued > TC_STAGES ? issued - TC_STAGES : 0; b < issued; ++b)
+      mbar_wait(&bar_full[b % TC_STAGES], (uint32_t)(b / TC_STAGES) & 1u);
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: K steps of 8 TF32 (32 bytes) within each 128-byte swizzle row
+    int done_boxes = 0;
+    for (int b = 0; b < nbox; ++b) {
+      const int s = b % TC_STAGES;
+      if (!mbar_wait(&bar_full[s], (uint32_t)(b / TC_STAGES) & 1u)) {
+        atomicOr(status, BEM_TC_ST_WAIT);
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(sm + (size_t)s * 2 * TC_BOX_BYTES), b0 = a0 + TC_BOX_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        tc_mma(tmem, umma_desc(a0 + 32u * ks), umma_desc(b0 + 32u * ks), (b | ks) ? 1u : 0u);
+      tc_commit(&bar_empty[s]);
+      done_boxes = b + 1;
+    }
+    tc_commit(&bar_done);  // every MMA this thread issued
+    // the last stages' releases arrive before the CTA may end (bounded)
+    for (int b = done_boxes > TC_STAGES ? done_boxes - TC_STAGES : 0; b < done_boxes; ++b)
+      mbar_wait(&bar_empty[b % TC_STAGES], (uint32_t)(b / TC_STAGES) & 1u);
   }
   __syncthreads();
   // one lane per warp waits for the MMAs; the warp reads TMEM only together
-  int ok = !s_fail;
-  if (ok) {
+  int ok = 1;
+  {
     int got = 1;
     if (lane == 0 && !mbar_wait(&bar_done, 0)) {
       atomicOr(status, BEM_TC_ST_WAIT);
       got = 0;
       mbar_wait(&bar_done, 0);
     }
-    ok = __shfl_sync(0xffffffffu, got, 0);
+    ok = __shfl_sync(0xffffffffu, got, 0) && !s_fail;
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    // warp w reads accumulator lanes 32 w .. 32 w + 31: row 32 w + lane of the tile
-    const int row = row_tile + 32 * warp + lane;
+    // warp w reads accumulator lanes 32 w .. 32 w + 31 (rows 32 w + lane of
+    // the tile), 32 columns at a time, and turns them through shared memory
+    // (the stages are free: every copy and MMA has completed) so that C is
+    // read and written a row at a time, 32 consecutive columns per warp access
+    float *tre = (float *)sm + warp * (2 * 32 * 33), *tim = tre + 32 * 33;
     const uint32_t tw = tmem + ((uint32_t)(32 * warp) << 16);
     const int col0 = r0 + col_tile * TC_NC;
 #pragma unroll
@@ -240,15 +270,27 @@ __global__ void __launch_bounds__(TC_TH, 1)
       float re[32], im[32];
       tmem_ld32(tw + (uint32_t)(32 * half), re);
       tmem_ld32(tw + (uint32_t)(TC_NC + 32 * half), im);
-      if (row < n) {
-        float2 *c = C + (size_t)row * ldc + col0 + 32 * half;
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (col0 + 32 * half + j < n) {
-            const float2 x = c[j];
-            c[j] = make_float2(x.x - re[j], x.y - im[j]);
-          }
+      for (int j = 0; j < 32; ++j) {
+        tre[lane * 33 + j] = re[j];
+        tim[lane * 33 + j] = im[j];
       }
+      __syncwarp();
+      const int col = col0 + 32 * half + lane;
+      // all 32 rows' loads in flight at once, then the stores
+      float2 x[32];
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const int row = row_tile + 32 * warp + r;
+        x[r] = (row < n && col < n) ? C[(size_t)row * ldc + col] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const int row = row_tile + 32 * warp + r;
+        if (row < n && col < n)
+          C[(size_t)row * ldc + col] = make_float2(x[r].x - tre[r * 33 + lane], x[r].y - tim[r * 33 + lane]);
+      }
+      __syncwarp();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -287,7 +329,7 @@ static int encode(bem_tc *t, CUtensorMap *tm, float *base, int cols, long rows) 
   return 0;
 }
 
-static size_t tc_smem(int nprod) { return (size_t)2 * (2 * nprod) * TC_BOX_BYTES + 1024; }
+static size_t tc_smem() { return (size_t)TC_STAGES * 2 * TC_BOX_BYTES + 1024; }
 
 extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   if (nprod != 1 && nprod != 3) nprod = 3;
@@ -296,19 +338,20 @@ extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   cudaFree(t->Bp);
   t->Ap = t->Bp = nullptr;
   t->ready = false;
-  const int kp = 64 * nprod;
+  const int kp = TC_KR * nprod;
   const long arows = n + TC_M, brows = 2L * ((n + TC_NC - 1) / TC_NC + 1) * TC_NC;
   if (cudaMalloc(&t->Ap, (size_t)arows * kp * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&t->Bp, (size_t)brows * kp * sizeof(float)) != cudaSuccess) {
     snprintf(t->err, sizeof(t->err), "tensor-core update: out of device memory");
     return -1;
   }
-  // rows a partial tile reads past the packed ones stay zero
+  // rows a partial tile reads past the packed ones: zero until a pack writes
+  // them (an accumulator row or column depends only on its own operand row)
   if (cudaMemset(t->Ap, 0, (size_t)arows * kp * sizeof(float)) != cudaSuccess ||
       cudaMemset(t->Bp, 0, (size_t)brows * kp * sizeof(float)) != cudaSuccess)
     return -1;
   if (encode(t, &t->tmA, t->Ap, kp, arows) || encode(t, &t->tmB, t->Bp, kp, brows)) return -1;
-  if (cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem(3)) != cudaSuccess) {
+  if (cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem()) != cudaSuccess) {
     snprintf(t->err, sizeof(t->err), "tensor-core update: shared memory attribute");
     return -1;
   }
@@ -318,16 +361,16 @@ extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   return 0;
 }
 
-extern "C" void bem_tc_launch(bem_tc *t, float2 *M, long lda, int n, int k, int w, unsigned *status,
-                              cudaStream_t st) {
-  const int r0 = k + w;
+extern "C" void bem_tc_launch(bem_tc *t, float2 *M, long lda, int n, int K, unsigned *status, cudaStream_t st) {
+  const int r0 = K + LU_OUTER_W;
   const int rows = n - r0;
   if (rows <= 0) return;
   const int ctiles = (rows + TC_NC - 1) / TC_NC, rtiles = (rows + TC_M - 1) / TC_M;
-  const long work = (long)rows * LU_PANEL_W + (long)ctiles * TC_NC * LU_PANEL_W;
-  const int pb = (int)((work + 255) / 256 < 4096 ? (work + 255) / 256 : 4096);
-  k_tc_pack<<<pb, 256, 0, st>>>(M, lda, n, k, w, t->nprod, t->Ap, t->Bp, rows, ctiles);
-  k_tc_update<<<dim3(ctiles, rtiles), TC_TH, tc_smem(t->nprod), st>>>(t->tmA, t->tmB, M, lda, n, r0, t->nprod, status);
+  const long work = (long)rows * LU_OUTER_W + (long)ctiles * TC_NC * LU_OUTER_W;
+  const int pb = (int)((work + 255) / 256 < 8192 ? (work + 255) / 256 : 8192);
+  k_tc_pack<<<pb, 256, 0, st>>>(M, lda, n, K, r0, t->nprod, t->Ap, t->Bp, rows, ctiles);
+  const int nbox = TC_KR * t->nprod / TC_BOX_K;
+  k_tc_update<<<dim3(ctiles, rtiles), TC_TH, tc_smem(), st>>>(t->tmA, t->tmB, M, lda, n, r0, nbox, status);
 }
 
 extern "C" void bem_tc_free(bem_tc *t) {

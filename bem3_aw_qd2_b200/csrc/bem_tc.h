@@ -3,7 +3,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
-#define LU_PANEL_W 32            // panel width of the LU (bem_lu.h BEM_LU_W)
+#define LU_OUTER_W 128           // outer block of the LU (bem_lu.h BEM_LU_OB): the update's depth
 #define BEM_TC_ST_WAIT 0x100u     // a tensor-core update wait gave up (no hang; result invalid)
 
 struct bem_tc {
@@ -19,8 +19,9 @@ extern "C" {
 // packed-operand buffers and TMA maps for systems up to n (no allocation
 // inside a stream capture: call before capturing)
 int bem_tc_prepare(bem_tc *t, int n, int nprod);
-// pack and launch the update of panel k (width w) of the row-major complex
-// FP32 matrix M: M[r0.., r0..] -= L21 U12, r0 = k + w
-void bem_tc_launch(bem_tc *t, float2 *M, long lda, int n, int k, int w, unsigned *status, cudaStream_t st);
+// pack and launch the update of the outer block starting at column K of the
+// row-major complex FP32 matrix M: M[r0:n, r0:n] -= M[r0:n, K:r0] M[K:r0, r0:n],
+// r0 = K + LU_OUTER_W
+void bem_tc_launch(bem_tc *t, float2 *M, long lda, int n, int K, unsigned *status, cudaStream_t st);
 void bem_tc_free(bem_tc *t);
 }

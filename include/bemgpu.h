@@ -121,6 +121,21 @@ long long bemgpu_interior_reuses(bemgpu_ctx *ctx);
  * and factors every domain, as the reference does). */
 int bemgpu_set_interior_reuse(bemgpu_ctx *ctx, int on);
 
+/* Interior-domain derivative rows (no counterpart in the reference, which
+ * keeps them: dG, dH of create_cmatrix_domain with did >= 1,
+ * bem3_aw_qd2_solve_bieq.c:133-218, used by dpdt_fcm in q_solve_pv_bv,
+ * :516-530, 655-750).  keep = 1 (default): dG and dH (2N x N complex each)
+ * stay on the device after the assembly.  keep = 0: they are not stored; the
+ * particle-velocity step recomputes them a block of rows at a time (about
+ * 256 MiB each) and contracts each block with P and dP at once.  This saves
+ * 64 N^2 bytes per interior domain (38.7 GB at N = 24576) for one more
+ * free-space integration per solve.  Takes effect at the next bemgpu_load;
+ * bemgpu_get_matrix then has no dG, dH (which = 2, 3) to return.  block_rows
+ * (keep = 0 only): rows recomputed at a time, rounded down to a multiple of 4;
+ * 0 chooses the 256 MiB block.  The request server chooses keep = 0 for a
+ * request that does not fit its device-memory budget otherwise. */
+int bemgpu_set_interior_derivatives(bemgpu_ctx *ctx, int keep, int block_rows);
+
 /* Kernel launches of this library in this process so far, all contexts and
  * threads (no counterpart in the reference): every launch counts one, a
  * replay of a captured factorisation counts its kernels. */
