@@ -307,6 +307,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
                                                            unsigned *status, unsigned long long *terms, long long pair0,
                                                            long long npairs, bem_plist L) {
   __shared__ double acc[16][RP_THREADS + 1];
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
       bem_rw(el, z, e, vR, vW);
       for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
       bem_gval gv;
-      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
       if (rc < 0) set_status(status, rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT);
       nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
       ++npt;
@@ -382,6 +385,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
                                                                unsigned long long *terms, long long pair0,
                                                                long long npairs, bem_plist L) {
   __shared__ double acc[16][RP_THREADS + 1];
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
@@ -413,7 +419,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
 #pragma unroll
         for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d));
         bem_gval gv;
-        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
         if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
         nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
         ++npt;
@@ -482,6 +488,9 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
                                                         unsigned long long *terms, long long pair0, long long npairs,
                                                         bem_plist L) {
   __shared__ double acc[16][FP_THREADS + 1];
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   const int lp = threadIdx.x >> 6, pt = threadIdx.x & 63;
   const long long nu = plist_units(L, npairs);
   unsigned long long nterm = 0, npt = 0;
@@ -509,7 +518,7 @@ __global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const _
 #pragma unroll
         for (int d = 0; d < 3; ++d) vR[d] -= __ldg(D.ren + (size_t)te * 12 + (p & 3) * 3 + d);
         bem_gval gv;
-        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
         if (rc < 0) st |= rc == -12 || rc == -23 ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
         nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
         ++npt;
@@ -602,6 +611,9 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
                                                         unsigned long long *terms) {
   const int p = blockIdx.x, k = blockIdx.y;
   if (k >= near_n[p]) return;
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   const int s = near_s[(size_t)p * D.near_cap + k];
   bem_node nd;
   int t, te;
@@ -630,7 +642,7 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
       for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
     }
     bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
     nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
     ++npt;
@@ -720,6 +732,9 @@ __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_q
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (bem_is_tri(D, te)) return;  // k_q0_self_tri
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   bem_el el;
   bem_load_el(D.cr, D.cw, te, el);
   const double zt = c_q.zt[tn], et = c_q.et[tn];
@@ -747,7 +762,7 @@ __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_q
       vW[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
     }
     bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv);
+    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
     nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
     ++npt;
@@ -1223,6 +1238,9 @@ __global__ void NP_BOUNDS k_q0_self_tri(bem_dom_dev D, const __grid_constant__ b
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (!bem_is_tri(D, te) || tn == 3) return;
+  extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const double2 *wts = bem_wtab_stage(q, wts_s);
+  __syncthreads();
   bem_el el;
   bem_load_el(D.cr, D.cw, te, el);
   double zt, et, r[5], th[5];
@@ -1249,7 +1267,7 @@ __global__ void NP_BOUNDS k_q0_self_tri(bem_dom_dev D, const __grid_constant__ b
     double K[3];
     bem_K(el, rr, cth, sth, zt, et, K);
     bem_gval gv;
-    const int rc = bem_qpgf(q, rr * K[0], rr * K[1], rr * K[2], gv);
+    const int rc = bem_qpgf(q, rr * K[0], rr * K[1], rr * K[2], gv, wts);
     if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
     nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
     ++npt;
@@ -1604,9 +1622,23 @@ static bem_far far_params(const bem_dom_dev *D, const bem_qp *q, int periodic) {
   return fr;
 }
 
+// The periodic kernels keep a copy of the real-space term table in dynamic
+// shared memory (BEM_WT_SMEM bytes), which takes some of them past the 48 KB
+// a block gets without asking.
+static int q0_smem_attrs() {
+  const int b = (int)BEM_WT_SMEM;
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (cudaFuncSetAttribute(k_q0_regular, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_regular_tri, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_near, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_self, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self_tri, a, b) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
                                    bem_scratch *S, double *G, double *H, double *dG, double *dH, double *dF,
                                    cudaStream_t st, cudaEvent_t *ev) {
+  if (periodic && q0_smem_attrs()) return -1;
   // ev (optional): 6 events recorded around classify | regular | near | self | diag
   const int N = D->ne * 4;
   if (D->ne <= 0) return 0;
@@ -1641,14 +1673,14 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       const unsigned grid = 2u * (unsigned)nsm;
       const bem_plist Lreg = {S->plist, S->pcount, 1};
       const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
-      k_q0_regular<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
+      k_q0_regular<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
       bem_count_launches(1);
       if (D->far_rule) {
-        k_q0_far<<<grid, FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lfar);
+        k_q0_far<<<grid, FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lfar);
         bem_count_launches(1);
       }
       if (D->has_tri) {
-        k_q0_regular_tri<<<grid, RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
+        k_q0_regular_tri<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
         bem_count_launches(1);
       }
     } else {
@@ -1656,29 +1688,29 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       const long long chunk = 1LL << 26;  // keep grid.x well inside limits
       for (long long p0 = 0; p0 < npairs; p0 += chunk) {
         const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
-        k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+        k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                       L0);
         bem_count_launches(1);
         if (D->far_rule) {
-          k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+          k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                     L0);
           bem_count_launches(1);
         }
         if (D->has_tri) {
-          k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+          k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                             p0, np, L0);
           bem_count_launches(1);
         }
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    k_q0_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
+    k_q0_near<<<dim3(N, D->near_cap), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
-    k_q0_self<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+    k_q0_self<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
     bem_count_launches(1);
     if (D->has_tri) {
-      k_q0_self_tri<<<N, NP_THREADS, 0, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+      k_q0_self_tri<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
       bem_count_launches(1);
     }
   } else {
@@ -1707,6 +1739,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
 // Ewald-parameter autotuner; the pair flags must be current (k_classify).
 extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H,
                                 double frac, int nchunk, cudaStream_t st, float *ms) {
+  if (q0_smem_attrs()) return -1;
   const long long npairs = (long long)D->ne * 4 * D->ne;
   const long long len = (long long)(npairs * frac / nchunk) + 1;
   cudaEvent_t e0, e1;
@@ -1719,16 +1752,16 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
       // the kernels of the assembly itself (over pair ranges, not lists):
       // quad sources, far pairs, and triangle sources when there are any
       const bem_plist L0 = {nullptr, nullptr, 0};
-      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                     L0);
       bem_count_launches(1);
       if (D->far_rule) {
-        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
+        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                   L0);
         bem_count_launches(1);
       }
       if (D->has_tri) {
-        k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, 0, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+        k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                           p0, np, L0);
         bem_count_launches(1);
       }

@@ -111,12 +111,10 @@ __device__ __forceinline__ float cabs1(float2 a) { return fabsf(a.x) + fabsf(a.y
 // ---------------------------------------------------------------- partial pivoting in one CTA
 template <class C2>
 struct gepp_sh {
-  unsigned wk[2][LU_TH / 32];        // each warp's best pivot key
-  C2 cand[2][LU_TH / 32][LU_W];      // each warp's best row, as its owner holds it
-  C2 crcp[2][LU_TH / 32];            // reciprocal of that row's pivot entry
-  int cid[2][LU_TH / 32];            // its matrix row
-  C2 krow[2][LU_W];                  // the row at position j
-  int kid[2];
+  unsigned wk[2][LU_TH / 32];  // each warp's pivot key
+  C2 prow[2][LU_W], krow[2][LU_W];
+  C2 prcp[2];                  // reciprocal of the pivot
+  int pid[2], kid[2];
 };
 
 // Pivot key of a candidate: the float bits of |re| + |im| (non-negative floats
@@ -127,12 +125,70 @@ __device__ __forceinline__ unsigned pivot_key(float a, int t) {
   return (__float_as_uint(a) & 0xFFFFFF00u) | (unsigned)(255 - t);
 }
 
-template <class C2>
-__device__ __forceinline__ void rot1(C2 (&v)[LU_W]) {
+// rotate the first L registers by one: v[0] (the finished pivot column)
+// goes to v[L - 1]
+template <int L, class C2>
+__device__ __forceinline__ void rotl(C2 (&v)[LU_W]) {
   const C2 f = v[0];
 #pragma unroll
-  for (int c = 0; c < LU_W - 1; ++c) v[c] = v[c + 1];
-  v[LU_W - 1] = f;
+  for (int c = 0; c < L - 1; ++c) v[c] = v[c + 1];
+  v[L - 1] = f;
+}
+
+// One elimination step j of gepp: v[0] holds column j and v[1 .. 31 - j] the
+// columns still to update; L >= 32 - j is the step's compile-time bound, so
+// that the update and the rotation touch only the live window (the finished
+// columns beyond it stay where they are).
+template <int L, class C2>
+__device__ __forceinline__ void gepp_step(C2 (&v)[LU_W], int &id, int j, int steps, int rr, gepp_sh<C2> &sh,
+                                          unsigned *status) {
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  if (j < steps) {
+    const int b = j & 1;
+    // the pivot: one integer maximum per warp, then over the warps (the
+    // 2^-15 resolution of the key only picks among rows within that much of
+    // the largest, which keeps partial pivoting's growth bound)
+    const unsigned key = __reduce_max_sync(FULL, (t >= j && t < rr) ? pivot_key((float)cabs1(v[0]), t) : 0u);
+    if (lane == 0) sh.wk[b][wid] = key;
+    __syncthreads();
+    unsigned best = sh.wk[b][0];
+#pragma unroll
+    for (int q = 1; q < LU_TH / 32; ++q) best = max(best, sh.wk[b][q]);
+    int p = 255 - (int)(best & 255u);
+    if ((best >> 8) == 0u) {  // no non-zero entry left in the column
+      if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
+      p = j;
+    }
+    if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) sh.prow[b][c] = v[c];
+      sh.pid[b] = id;
+      sh.prcp[b] = crcp(v[0]);
+    }
+    if (t == j) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) sh.krow[b][c] = v[c];
+      sh.kid[b] = id;
+    }
+    __syncthreads();
+    if (t == j) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) v[c] = sh.prow[b][c];
+      id = sh.pid[b];
+    } else if (t == p) {
+#pragma unroll
+      for (int c = 0; c < LU_W; ++c) v[c] = sh.krow[b][c];
+      id = sh.kid[b];
+    }
+    if (t > j && t < rr) {
+      const C2 l = cmul(v[0], sh.prcp[b]);
+      v[0] = l;
+#pragma unroll
+      for (int c = 1; c < L; ++c)
+        if (c < LU_W - j) v[c] = cfms(l, sh.prow[b][c], v[c]);
+    }
+  }
+  rotl<L>(v);
 }
 
 // Partial pivoting (|re| + |im| as LAPACK's izamax, lowest row on ties) over
@@ -143,68 +199,26 @@ __device__ __forceinline__ void rot1(C2 (&v)[LU_W]) {
 // step j its register 0 holds column j, registers 1 .. 31 - j the columns
 // still to update and the rest the finished ones, so that every register
 // index is a compile-time constant inside one short loop body.
+//
+// The steps run in four groups of eight with a shrinking live window of 32,
+// 24, 16 and 8 registers: each group's finished columns end up in the eight
+// registers just past the next group's window (group g's at 24 - 8 g ..
+// 31 - 8 g), which a fixed permutation puts back in order at the end.
 template <class C2>
 __device__ void gepp(C2 (&v)[LU_W], int &id, int rr, int w, gepp_sh<C2> &sh, unsigned *status) {
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int steps = min(w, rr);
-  for (int j = 0; j < steps; ++j) {
-    const int b = j & 1;
-    // the pivot: one integer maximum per warp, whose owner publishes its row
-    // and reciprocal at once; after the one barrier every thread takes the
-    // maximum over the warps (the 2^-15 resolution of the key only picks
-    // among rows within that much of the largest, which keeps partial
-    // pivoting's growth bound).  The buffers alternate between steps, so a
-    // step's writes never meet the previous step's reads.
-    const unsigned mykey = (t >= j && t < rr) ? pivot_key((float)cabs1(v[0]), t) : 0u;
-    const unsigned key = __reduce_max_sync(FULL, mykey);
-    if (mykey == key && key != 0u) {
+  for (int j = 0; j < 8; ++j) gepp_step<32>(v, id, j, steps, rr, sh, status);
+  for (int j = 8; j < 16; ++j) gepp_step<24>(v, id, j, steps, rr, sh, status);
+  for (int j = 16; j < 24; ++j) gepp_step<16>(v, id, j, steps, rr, sh, status);
+  for (int j = 24; j < 32; ++j) gepp_step<8>(v, id, j, steps, rr, sh, status);
+  // registers 24 - 8 g .. 31 - 8 g hold columns 8 g .. 8 g + 7
+  C2 o[LU_W];
 #pragma unroll
-      for (int c = 0; c < LU_W; ++c) sh.cand[b][wid][c] = v[c];
-      sh.crcp[b][wid] = crcp(v[0]);
-      sh.cid[b][wid] = id;
-    }
-    if (lane == 0) sh.wk[b][wid] = key;
-    if (t == j) {
+  for (int g = 0; g < 4; ++g)
 #pragma unroll
-      for (int c = 0; c < LU_W; ++c) sh.krow[b][c] = v[c];
-      sh.kid[b] = id;
-    }
-    __syncthreads();
-    unsigned best = sh.wk[b][0];
-    int bw = 0;
+    for (int i = 0; i < 8; ++i) o[8 * g + i] = v[24 - 8 * g + i];
 #pragma unroll
-    for (int q = 1; q < LU_TH / 32; ++q) {
-      const unsigned kq = sh.wk[b][q];
-      if (kq > best) { best = kq; bw = q; }
-    }
-    int p = 255 - (int)(best & 255u);
-    const bool zero = (best >> 8) == 0u;  // no non-zero entry left in the column
-    if (zero) {
-      if (status && t == 0) atomicOr(status, BEM_LU_ST_ZERO);
-      p = j;
-    }
-    const C2 *prow = zero ? sh.krow[b] : sh.cand[b][bw];
-    if (t == j) {
-      if (!zero) {
-#pragma unroll
-        for (int c = 0; c < LU_W; ++c) v[c] = prow[c];
-        id = sh.cid[b][bw];
-      }
-    } else if (t == p) {
-#pragma unroll
-      for (int c = 0; c < LU_W; ++c) v[c] = sh.krow[b][c];
-      id = sh.kid[b];
-    }
-    if (t > j && t < rr) {
-      const C2 l = zero ? czero<C2>() : cmul(v[0], sh.crcp[b][bw]);
-      v[0] = l;
-#pragma unroll
-      for (int c = 1; c < LU_W; ++c)
-        if (c < LU_W - j) v[c] = cfms(l, prow[c], v[c]);
-    }
-    rot1(v);
-  }
-  for (int s = steps; s < LU_W; ++s) rot1(v);  // LU_W rotations in all: columns back in order
+  for (int c = 0; c < LU_W; ++c) v[c] = o[c];
 }
 
 template <class C2>
@@ -532,16 +546,16 @@ __device__ __forceinline__ void dmma(double a, double b, double (&d)[2]) {
                : "d"(a), "d"(b));
 }
 
-// C -= L U on the FP64 tensor cores: C = A[r0:n, r0:cend), L = A[r0:n, kk:kk+kw),
-// U = A[kk:kk+kw, r0:cend); kw in steps of LU_W staged through shared memory.
+// C -= L U on the FP64 tensor cores: C = A[r0:n, c0:cend), L = A[r0:n, kk:kk+kw),
+// U = A[kk:kk+kw, c0:cend); kw in steps of LU_W staged through shared memory.
 // A panel's update (kk = k, kw = 32, cend = the end of its outer block) and an
 // outer block's (kk = its first column, kw = LU_OB, cend = n) alike.
 __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, int n, int kk, int kw, int r0,
-                                                        int cend) {
+                                                        int c0, int cend) {
   extern __shared__ __align__(16) double up_smem[];
   double *Ar = up_smem, *Ai = Ar + UP_BM * UP_LDA, *Br = Ai + UP_BM * UP_LDA, *Bi = Br + LU_W * UP_LDB;
   const int t = threadIdx.x;
-  const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
+  const int rb = r0 + blockIdx.y * UP_BM, cb = c0 + blockIdx.x * UP_BN;
   const int lane = t & 31, wid = t >> 5, g = lane >> 2, q = lane & 3;
   const int wm = wid & 1, wn = wid >> 1;  // warp tile: 32 rows x 16 columns
   double cr[4][2][2], ci[4][2][2];
@@ -614,11 +628,11 @@ __global__ void __launch_bounds__(UP_TH, 2) k_lu_update(double2 *A, long lda, in
 // loads and 128-byte runs of C per 16 threads)
 #define UF_TH 256
 __global__ void __launch_bounds__(UF_TH) k_lu_update_c32(float2 *A, long lda, int n, int kk, int kw, int r0,
-                                                         int cend) {
+                                                         int c0, int cend) {
   __shared__ float2 As[UP_BM][LU_W + 1];
   __shared__ float2 Bs[LU_W][UP_BN + 1];
   const int t = threadIdx.x;
-  const int rb = r0 + blockIdx.y * UP_BM, cb = r0 + blockIdx.x * UP_BN;
+  const int rb = r0 + blockIdx.y * UP_BM, cb = c0 + blockIdx.x * UP_BN;
   const int ty = t >> 4, tx = t & 15;
   float2 acc[4][4];
 #pragma unroll
@@ -962,6 +976,9 @@ extern "C" int bem_lu_init(bem_lu *w, int device) {
     snprintf(w->err, sizeof(w->err), "triangular solve: no resident block");
     return -1;
   }
+  CKL(cudaStreamCreateWithFlags(&w->side, cudaStreamNonBlocking), "LU side stream");
+  CKL(cudaEventCreateWithFlags(&w->ev_fork, cudaEventDisableTiming), "LU events");
+  CKL(cudaEventCreateWithFlags(&w->ev_join, cudaEventDisableTiming), "LU events");
   CKL(cudaMalloc(&w->piv, PV_INTS * sizeof(int)), "LU scratch");
   CKL(cudaMalloc(&w->u11, U_COUNT * sizeof(double2)), "LU scratch");
   CKL(cudaMalloc(&w->status, sizeof(unsigned)), "LU status");
@@ -978,6 +995,9 @@ extern "C" void bem_lu_free(bem_lu *w) {
   cudaFree(w->status);
   cudaFree(w->flags);
   cudaFree(w->y);
+  if (w->ev_fork) cudaEventDestroy(w->ev_fork);
+  if (w->ev_join) cudaEventDestroy(w->ev_join);
+  if (w->side) cudaStreamDestroy(w->side);
   *w = bem_lu();
 }
 
@@ -991,14 +1011,14 @@ static int grow_bytes(bem_lu *w, void **p, size_t *cap, size_t bytes, const char
   return 0;
 }
 
-// C = A[r0:n, r0:cend) -= A[r0:n, kk:kk+kw) A[kk:kk+kw, r0:cend)
-static void launch_update(double2 *A, int n, int kk, int kw, int r0, int cend, cudaStream_t st) {
-  const dim3 grid((cend - r0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
-  k_lu_update<<<grid, UP_TH, UP_SMEM, st>>>(A, n, n, kk, kw, r0, cend);
+// C = A[r0:n, c0:cend) -= A[r0:n, kk:kk+kw) A[kk:kk+kw, c0:cend)
+static void launch_update(double2 *A, int n, int kk, int kw, int r0, int c0, int cend, cudaStream_t st) {
+  const dim3 grid((cend - c0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
+  k_lu_update<<<grid, UP_TH, UP_SMEM, st>>>(A, n, n, kk, kw, r0, c0, cend);
 }
-static void launch_update(float2 *A, int n, int kk, int kw, int r0, int cend, cudaStream_t st) {
-  const dim3 grid((cend - r0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
-  k_lu_update_c32<<<grid, UF_TH, 0, st>>>(A, n, n, kk, kw, r0, cend);
+static void launch_update(float2 *A, int n, int kk, int kw, int r0, int c0, int cend, cudaStream_t st) {
+  const dim3 grid((cend - c0 + UP_BN - 1) / UP_BN, (n - r0 + UP_BM - 1) / UP_BM);
+  k_lu_update_c32<<<grid, UF_TH, 0, st>>>(A, n, n, kk, kw, r0, c0, cend);
 }
 
 // an outer block's update of a complex FP32 factorisation on the tensor cores
@@ -1015,7 +1035,9 @@ static int tc_update(bem_lu *w, float2 *A, int n, int K, cudaStream_t st) {
 // covers only the rest of its outer block; the columns right of the block get
 // the row moves as the panels go, then U12 (k_lu_trsm) and one rank-LU_OB
 // update, so the trailing matrix is read and written once per outer block
-// instead of once per panel.
+// instead of once per panel.  Look-ahead: a panel's update is split into the
+// next panel's 32 columns (on st, before the next panel) and the rest (on the
+// side stream, beside the next panel); the next row moves wait for the rest.
 template <class C2>
 static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
   k_lu_iota<<<(n + 255) / 256, 256, 0, st>>>(w->rowmap, n);
@@ -1024,22 +1046,41 @@ static int factor_launches(bem_lu *w, C2 *A, int n, cudaStream_t st) {
   // critical path of a small factorisation)
   const int one_block = w->one_block_max > 0 ? w->one_block_max : LU_ONE_BLOCK_N;
   const int obw = n <= one_block ? n : LU_OB;
+  bool pending = false;  // update work on the side stream not yet joined
   for (int K = 0; K < n; K += obw) {
     const int cend = n - K < obw ? n : K + obw;
     for (int k = K; k < cend; k += LU_W) {
       const int wd = n - k < LU_W ? n - k : LU_W;
       const int r0 = k + wd;
       k_lu_panel<C2><<<LU_CL, LU_TH, sizeof(panel_sh<C2>), st>>>(A, n, n, k, w->piv, (C2 *)w->u11, w->status);
+      if (pending) {
+        CKL(cudaStreamWaitEvent(st, w->ev_join, 0), "LU join");
+        pending = false;
+      }
       const int nL = (n - r0 + AP_ROWS - 1) / AP_ROWS;
       const int nC = (k + AP_COLS - 1) / AP_COLS + (n - r0 + AP_COLS - 1) / AP_COLS;
       k_lu_apply<C2><<<nL + nC + 1, AP_TH, 0, st>>>(A, n, n, k, cend, w->piv, (const C2 *)w->u11, w->rowmap,
                                                     w->status);
-      if (r0 < cend) launch_update(A, n, k, wd, r0, cend, st);
+      if (r0 < cend) {
+        const int nxt = cend - r0 < LU_W ? cend : r0 + LU_W;
+        launch_update(A, n, k, wd, r0, r0, nxt, st);
+        if (nxt < cend) {
+          CKL(cudaEventRecord(w->ev_fork, st), "LU fork");
+          CKL(cudaStreamWaitEvent(w->side, w->ev_fork, 0), "LU fork");
+          launch_update(A, n, k, wd, r0, nxt, cend, w->side);
+          CKL(cudaEventRecord(w->ev_join, w->side), "LU join");
+          pending = true;
+        }
+      }
+    }
+    if (pending) {
+      CKL(cudaStreamWaitEvent(st, w->ev_join, 0), "LU join");
+      pending = false;
     }
     if (cend < n) {
       k_lu_trsm<C2><<<(n - cend + TR_NC - 1) / TR_NC, TR_TH, sizeof(trsm_sh<C2>), st>>>(A, n, n, K, cend - K,
                                                                                          (const C2 *)w->u11);
-      if (tc_update(w, A, n, K, st) == 0) launch_update(A, n, K, cend - K, cend, n, st);
+      if (tc_update(w, A, n, K, st) == 0) launch_update(A, n, K, cend - K, cend, cend, n, st);
     }
   }
   CKL(cudaGetLastError(), "LU launch");

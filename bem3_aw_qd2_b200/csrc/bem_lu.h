@@ -31,6 +31,8 @@ struct bem_lu {
   int g_n = 0, g_tc = -1, g_obm = 0;
   size_t g_nodes = 0;   // kernels in the captured graph (launch count per replay)
   bem_tc *tc = nullptr;       // complex FP32 only: trailing updates on the tensor cores when set
+  cudaStream_t side = nullptr;  // second stream of the captured factorisation (look-ahead updates)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int sms = 0, coop_blocks = 0;  // device facts for the launches
   int one_block_max = 0;      // largest n factored as one outer block (0: the default, 2048)
   char err[200] = {0};

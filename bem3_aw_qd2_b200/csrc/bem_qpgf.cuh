@@ -175,22 +175,50 @@ __device__ __forceinline__ double2 ew_real_ab(double k, double ve, double x, dou
   const double ef = exp(x * x - y * y);
   return make_double2(ef * w.re, ef * (w.re * (0.5 / ve) - k * y * w.im + y * (0.56418958354775628695 / ve)));
 }
-__device__ __forceinline__ double2 bem_wtab(const bem_qp &q, double ve, double x, double y) {
+// wts: the kernel's shared-memory copy of the table (bem_wtab_stage), or null
+// to read q.wt through the read-only cache
+__device__ __forceinline__ double2 bem_wtab(const bem_qp &q, double ve, double x, double y,
+                                            const double2 *wts = nullptr) {
   const double u = y * (1.0 / BEM_WT_H);
   const int j = (int)u;
   if (j >= q.wt_n) return ew_real_ab(q.k, ve, x, y);
   const double t = 2.0 * (u - j) - 1.0, t2 = 2.0 * t;
-  const double2 *c = reinterpret_cast<const double2 *>(q.wt) + (size_t)j * BEM_WT_DEG;
   double ba = 0.0, bb = 0.0, b1a = 0.0, b1b = 0.0;
+  double2 c0;
+  if (wts) {
+    const double2 *c = wts + j * BEM_WT_DEG;
 #pragma unroll
-  for (int k = BEM_WT_DEG - 1; k >= 1; --k) {
-    const double2 ck = __ldg(c + k);
-    const double na = ck.x + t2 * ba - b1a, nb = ck.y + t2 * bb - b1b;
-    b1a = ba; b1b = bb;
-    ba = na; bb = nb;
+    for (int k = BEM_WT_DEG - 1; k >= 1; --k) {
+      const double2 ck = c[k];
+      const double na = ck.x + t2 * ba - b1a, nb = ck.y + t2 * bb - b1b;
+      b1a = ba; b1b = bb;
+      ba = na; bb = nb;
+    }
+    c0 = c[0];
+  } else {
+    const double2 *c = reinterpret_cast<const double2 *>(q.wt) + (size_t)j * BEM_WT_DEG;
+#pragma unroll
+    for (int k = BEM_WT_DEG - 1; k >= 1; --k) {
+      const double2 ck = __ldg(c + k);
+      const double na = ck.x + t2 * ba - b1a, nb = ck.y + t2 * bb - b1b;
+      b1a = ba; b1b = bb;
+      ba = na; bb = nb;
+    }
+    c0 = __ldg(c);
   }
-  const double2 c0 = __ldg(c);
   return make_double2(c0.x + t * ba - b1a, c0.y + t * bb - b1b);
+}
+// copy the real-space table of q into shared memory (all threads of the
+// block take part; the caller synchronises before the first use).  A block
+// that evaluates many lattice sums reads its table from there: the lanes of a
+// warp look up different intervals, which the read-only cache serves as that
+// many separate lines.
+__device__ __forceinline__ const double2 *bem_wtab_stage(const bem_qp &q, double2 *wts) {
+  if (!q.wt) return nullptr;
+  const int cnt = q.wt_n * BEM_WT_DEG;
+  const double2 *src = reinterpret_cast<const double2 *>(q.wt);
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) wts[e] = __ldg(src + e);
+  return wts;
 }
 
 // Ewald real-space term for lattice point (l1,l2)  (ew_qG1_v1_cFl, d3_qpgf_d2.c:1814).
@@ -198,12 +226,12 @@ __device__ __forceinline__ double2 bem_wtab(const bem_qp &q, double ve, double x
 // row by one complex multiplication per term instead of a sincos.
 __device__ __forceinline__ void ew_real_term(const bem_qp &q, double px, double py, double rz, cplx ce,
                                              double ke, double ke2, double ve, double ive, bool tab, cplx &F,
-                                             cplx &cf) {
+                                             cplx &cf, const double2 *wts = nullptr) {
   const double r2 = px * px + py * py + rz * rz;
   const double irl = rsqrt(r2), rl = r2 * irl;  // one reciprocal square root for both
   const double rl2e = rl * 0.5 * ive;
   if (tab) {
-    const double2 ab = bem_wtab(q, ve, ke, rl2e);
+    const double2 ab = bem_wtab(q, ve, ke, rl2e, wts);
     F = cscale(ce, irl * ab.x);
     cf = cscale(ce, 2.0 * ve * irl * irl * irl * ab.y);
   } else {
@@ -423,7 +451,8 @@ __device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.re, -a.im); }
 // The lattice rows are walked exactly as in the reference (centre, then up,
 // then down, each stopped by the reference's tests); the Bloch phases along a
 // row are advanced by a unit complex factor, so a row costs one sincos.
-__device__ BEM_QPGF_ATTR int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
+__device__ BEM_QPGF_ATTR int bem_qpgf_ewald(const bem_qp &q, double rx, double ry, double rz, bem_gval &out,
+                                            const double2 *wts = nullptr) {
   const double ve = bem_ewald_eta(q, rx, ry, rz);
   const double ke = q.k * ve, ke2 = ke * ke, ive = 1.0 / ve;
   const bool tab = q.wt != nullptr && ve == q.eta_run;  // table built for x = k eta_run
@@ -453,7 +482,7 @@ __device__ BEM_QPGF_ATTR int bem_qpgf_ewald(const bem_qp &q, double rx, double r
         for (; k < nmax; ++k, l2 += st) {
           const double px = rx + l1 * q.d1x + l2 * q.d2x, py = ry + l1 * q.d1y + l2 * q.d2y;
           cplx F, cf;
-          ew_real_term(q, px, py, rz, ce, ke, ke2, ve, ive, tab, F, cf);
+          ew_real_term(q, px, py, rz, ce, ke, ke2, ve, ive, tab, F, cf, wts);
           ++cc;
           s = cadd(s, F);
           sx = cadd(sx, cscale(cf, px));
@@ -590,7 +619,8 @@ __device__ BEM_QPGF_ATTR int bem_qpgf_spectral(const bem_qp &q, double rx, doubl
 
 // G_qp and grad G_qp at r (d3hm_qpgf_d2_v1, d3_qpgf_d2.c:124-176 and the cell
 // reduction of :409-438).  Returns #terms (> 0) or the reference's negative code.
-__device__ BEM_QPGF_ATTR int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gval &out) {
+__device__ BEM_QPGF_ATTR int bem_qpgf(const bem_qp &q, double rx, double ry, double rz, bem_gval &out,
+                                      const double2 *wts = nullptr) {
   bool spectral = false;
   if (!q.ewald_only) {
     const double az = fabs(rz);
@@ -605,7 +635,7 @@ __device__ BEM_QPGF_ATTR int bem_qpgf(const bem_qp &q, double rx, double ry, dou
   const int l2 = (int)floor(-(rx * q.d1y - ry * q.d1x) * q.idet + 0.5);
   const double hx = bem_sub2(rx, l1, q.d1x, l2, q.d2x);
   const double hy = bem_sub2(ry, l1, q.d1y, l2, q.d2y);
-  const int e = spectral ? bem_qpgf_spectral(q, hx, hy, rz, out) : bem_qpgf_ewald(q, hx, hy, rz, out);
+  const int e = spectral ? bem_qpgf_spectral(q, hx, hy, rz, out) : bem_qpgf_ewald(q, hx, hy, rz, out, wts);
   if (e > 0 && (l1 != 0 || l2 != 0)) {
     const cplx cf = cexpi(-(q.kx * (l1 * q.d1x + l2 * q.d2x) + q.ky * (l1 * q.d1y + l2 * q.d2y)));
     out.g = cmul(out.g, cf);

@@ -21,6 +21,7 @@
 #define BEM_WT_H 0.0625
 #define BEM_WT_N 128
 #define BEM_WT_SIZE (2 * BEM_WT_DEG * BEM_WT_N) /* doubles: BEM_WT_DEG x BEM_WT_N complex */
+#define BEM_WT_SMEM (BEM_WT_SIZE * 8)           /* its bytes (a kernel's shared-memory copy) */
 /* per-problem table of the spectral orders (bem_qpgf.cuh): for each order
  * (n1, n2) of a window around the row centres, 10 Chebyshev terms on
  * intervals of width 1/8 in z / (2 eta_run), two channels */
