@@ -75,6 +75,7 @@ def libs():
         h.aqd2_device_context.restype = vp
         h.aqd2_last_timing.argtypes = [_d]
         h.aqd2_set_device.argtypes = [ctypes.c_int]
+        h.aqd2_set_interior_derivatives.argtypes = [ctypes.c_int]
         h.aqd2_set_verbose.argtypes = [ctypes.c_int]
         h.aqd2_problem_build.argtypes = [vp, ctypes.POINTER(Problem)]
         h.aqd2_problem_free.argtypes = [ctypes.POINTER(Problem)]

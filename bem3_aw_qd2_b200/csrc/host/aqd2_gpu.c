@@ -22,6 +22,15 @@ void aqd2_set_verbose(int on) { g_verbose = on; }
 void aqd2_set_device(int device) { g_device = device; }
 void aqd2_set_precision(int mode) { g_precision = mode; }
 
+static int g_keep_dgh = -1; /* -1: from the environment (AQD2_INTERIOR_DERIVATIVES), else 1 */
+void aqd2_set_interior_derivatives(int keep) { g_keep_dgh = keep; }
+static int keep_dgh_mode(void)
+{
+  if (g_keep_dgh >= 0) return g_keep_dgh;
+  const char *e = getenv("AQD2_INTERIOR_DERIVATIVES");
+  return e ? atoi(e) : 1;
+}
+
 static int precision_mode(void)
 {
   if (g_precision >= 0) return g_precision;
@@ -42,7 +51,8 @@ static bemgpu_ctx *ctx_for(AQD2 *qd, int create)
         printf("bem3_aw_qd2: failed to create a CUDA context on device %d. Exit...\n", g_device);
         exit(1);
       }
-      if (bemgpu_set_precision(c, precision_mode()) != 0) {
+      if (bemgpu_set_precision(c, precision_mode()) != 0 ||
+          bemgpu_set_interior_derivatives(c, keep_dgh_mode(), 0) != 0) {
         printf("bem3_aw_qd2: %s. Exit...\n", bemgpu_error(c));
         exit(1);
       }

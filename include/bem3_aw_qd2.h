@@ -153,6 +153,10 @@ void aqd2_set_device(int device);
  * BEMGPU_FP64 .. BEMGPU_MIXED_FAST; default 0, or the AQD2_PRECISION
  * environment variable). */
 void aqd2_set_precision(int mode);
+/* Interior derivative rows of contexts created afterwards kept (1) or
+ * recomputed in blocks (0) (bemgpu.h bemgpu_set_interior_derivatives;
+ * default 1, or the AQD2_INTERIOR_DERIVATIVES environment variable). */
+void aqd2_set_interior_derivatives(int keep);
 /* 0: solve_bieq_aqd2 prints nothing (default 1: the reference's progress lines). */
 void aqd2_set_verbose(int on);
 /* Last wall time of the solve phases in seconds: [0] upload, [1] assembly,
