@@ -609,73 +609,77 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
                                                         const int *__restrict__ near_n, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ nearF, unsigned *status,
                                                         unsigned long long *terms) {
-  const int p = blockIdx.x, k = blockIdx.y;
-  if (k >= near_n[p]) return;
+  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...
+  const int p = blockIdx.x, nn = near_n[p];
+  if ((int)blockIdx.y >= nn) return;
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
-  const int s = near_s[(size_t)p * D.near_cap + k];
-  bem_node nd;
-  int t, te;
-  bem_load_node(D, p, nd, t, te);
-  bem_el el;
-  const int se = abs(D.sid[s]) - 1;
-  bem_load_el(D.cr, D.cw, se, el);
-  const bool tri = bem_is_tri(D, se);  // q0_lit_dcoef_v2_cc_GH: 3 parts x 64 x 64
-  double v[19];
-#pragma unroll
-  for (int c = 0; c < 19; ++c) v[c] = 0.0;
-  unsigned st = 0;
-  unsigned long long nterm = 0, npt = 0;
-  for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
-    const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
-    const int i = ij / BEM_GHN, j = ij % BEM_GHN;
-    double z = c_q.xh[i], e = c_q.xh[j], wt = c_q.wh[i] * c_q.wh[j];
-    double vR[3], vW[3];
-    if (tri) {
-      bem_tri_point_ref(part, c_q.xh[i], c_q.xh[j], z, e);
-      wt *= bem_tri_wfac(c_q.xh[i], c_q.xh[j]);
-      bem_rw_ref(el, z, e, vR, vW);
-      for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
-    } else {
-      bem_rw(el, z, e, vR, vW);
-      for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
-    }
-    bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
-    if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
-    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-    ++npt;
-    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-    const cplx g = cscale(gv.g, aW * wt);
-    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-    double N[4];
-    bem_Nn(tri, z, e, N);
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      v[2 * a] += g.re * N[a];
-      v[2 * a + 1] += g.im * N[a];
-      v[8 + 2 * a] += h.re * N[a];
-      v[8 + 2 * a + 1] += h.im * N[a];
-    }
-    double f, fz, fe;
-    geomF(vR, vW, nd, f, fz, fe);
-    v[16] += wt * f;
-    v[17] += wt * fz;
-    v[18] += wt * fe;
-  }
-  count_work(terms + 1, nterm, npt);
-  set_status(status, st);
   __shared__ double sm[19 * (NP_THREADS / 32) + 19];
-  block_reduce<19>(v, sm);
-  if (threadIdx.x < 16) {
-    const size_t N = (size_t)D.ne * 4;
-    const int c = threadIdx.x;
-    double *dst = c < 8 ? G : H;
-    const int a = (c & 7) >> 1, part = c & 1;
-    dst[2 * ((size_t)p * N + 4 * s + a) + part] = v[c];
-  } else if (threadIdx.x < 19) {
-    nearF[((size_t)p * D.near_cap + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
+  for (int k = blockIdx.y; k < nn; k += gridDim.y) {
+    const int s = near_s[(size_t)p * D.near_cap + k];
+    bem_node nd;
+    int t, te;
+    bem_load_node(D, p, nd, t, te);
+    bem_el el;
+    const int se = abs(D.sid[s]) - 1;
+    bem_load_el(D.cr, D.cw, se, el);
+    const bool tri = bem_is_tri(D, se);  // q0_lit_dcoef_v2_cc_GH: 3 parts x 64 x 64
+    double v[19];
+#pragma unroll
+    for (int c = 0; c < 19; ++c) v[c] = 0.0;
+    unsigned st = 0;
+    unsigned long long nterm = 0, npt = 0;
+    for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+      const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
+      const int i = ij / BEM_GHN, j = ij % BEM_GHN;
+      double z = c_q.xh[i], e = c_q.xh[j], wt = c_q.wh[i] * c_q.wh[j];
+      double vR[3], vW[3];
+      if (tri) {
+        bem_tri_point_ref(part, c_q.xh[i], c_q.xh[j], z, e);
+        wt *= bem_tri_wfac(c_q.xh[i], c_q.xh[j]);
+        bem_rw_ref(el, z, e, vR, vW);
+        for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
+      } else {
+        bem_rw(el, z, e, vR, vW);
+        for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+      }
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
+      if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
+      const cplx g = cscale(gv.g, aW * wt);
+      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
+      double N[4];
+      bem_Nn(tri, z, e, N);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        v[2 * a] += g.re * N[a];
+        v[2 * a + 1] += g.im * N[a];
+        v[8 + 2 * a] += h.re * N[a];
+        v[8 + 2 * a + 1] += h.im * N[a];
+      }
+      double f, fz, fe;
+      geomF(vR, vW, nd, f, fz, fe);
+      v[16] += wt * f;
+      v[17] += wt * fz;
+      v[18] += wt * fe;
+    }
+    count_work(terms + 1, nterm, npt);
+    set_status(status, st);
+    block_reduce<19>(v, sm);
+    if (threadIdx.x < 16) {
+      const size_t N = (size_t)D.ne * 4;
+      const int c = threadIdx.x;
+      double *dst = c < 8 ? G : H;
+      const int a = (c & 7) >> 1, part = c & 1;
+      dst[2 * ((size_t)p * N + 4 * s + a) + part] = v[c];
+    } else if (threadIdx.x < 19) {
+      nearF[((size_t)p * D.near_cap + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
+    }
+    __syncthreads();  // sm is reused by the next pair
   }
 }
 
@@ -944,46 +948,49 @@ __global__ void __launch_bounds__(NP_THREADS) k_fs_near(bem_dom_dev D, double k,
                                                         const int *__restrict__ near_n, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ dG,
                                                         double *__restrict__ dH, double *__restrict__ nearF, int p0) {
-  const int p = p0 + blockIdx.x, kk = blockIdx.y;
-  if (kk >= near_n[p]) return;
-  const int s = near_s[(size_t)p * D.near_cap + kk];
-  bem_node nd;
-  int t, te;
-  bem_load_node(D, p, nd, t, te);
-  bem_el el;
-  const int se = abs(D.sid[s]) - 1;
-  bem_load_el(D.cr, D.cw, se, el);
-  const bool tri = bem_is_tri(D, se);  // lit_dcoef_v2_GH: 3 parts x 64 x 64
-  fs_acc a;
-  fs_zero(a);
-  for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
-    const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
-    const int i = ij / BEM_GHN, j = ij % BEM_GHN;
-    if (tri) {
-      double z, e;
-      bem_tri_point(part, c_q.xh[i], c_q.xh[j], z, e);
-      fs_point(el, nd, k, z, e, c_q.wh[i] * c_q.wh[j] * bem_tri_wfac(c_q.xh[i], c_q.xh[j]), a, true);
-    } else {
-      fs_point(el, nd, k, c_q.xh[i], c_q.xh[j], c_q.wh[i] * c_q.wh[j], a);
-    }
-  }
+  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...
+  const int p = p0 + blockIdx.x, nn = near_n[p];
   __shared__ double sm[51 * (NP_THREADS / 32) + 51];
-  double *av = reinterpret_cast<double *>(&a);
-  double v[51];
-#pragma unroll
-  for (int c = 0; c < 51; ++c) v[c] = av[c];
-  block_reduce<51>(v, sm);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int c = 0; c < 51; ++c) av[c] = v[c];
-    fs_store(D, p, s, a, G, H, dG, dH, p0);
-    if (G) {
-      const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
-      double *nf = nearF + ((size_t)p * D.near_cap + kk) * 3;
-      nf[0] = sg * a.f * BEM_I_FP;
-      nf[1] = sg * a.fz * BEM_I_FP;
-      nf[2] = sg * a.fe * BEM_I_FP;
+  for (int kk = blockIdx.y; kk < nn; kk += gridDim.y) {
+    const int s = near_s[(size_t)p * D.near_cap + kk];
+    bem_node nd;
+    int t, te;
+    bem_load_node(D, p, nd, t, te);
+    bem_el el;
+    const int se = abs(D.sid[s]) - 1;
+    bem_load_el(D.cr, D.cw, se, el);
+    const bool tri = bem_is_tri(D, se);  // lit_dcoef_v2_GH: 3 parts x 64 x 64
+    fs_acc a;
+    fs_zero(a);
+    for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
+      const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
+      const int i = ij / BEM_GHN, j = ij % BEM_GHN;
+      if (tri) {
+        double z, e;
+        bem_tri_point(part, c_q.xh[i], c_q.xh[j], z, e);
+        fs_point(el, nd, k, z, e, c_q.wh[i] * c_q.wh[j] * bem_tri_wfac(c_q.xh[i], c_q.xh[j]), a, true);
+      } else {
+        fs_point(el, nd, k, c_q.xh[i], c_q.xh[j], c_q.wh[i] * c_q.wh[j], a);
+      }
     }
+    double *av = reinterpret_cast<double *>(&a);
+    double v[51];
+#pragma unroll
+    for (int c = 0; c < 51; ++c) v[c] = av[c];
+    block_reduce<51>(v, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int c = 0; c < 51; ++c) av[c] = v[c];
+      fs_store(D, p, s, a, G, H, dG, dH, p0);
+      if (G) {
+        const double sg = D.sid[s] < 0 ? -1.0 : 1.0;
+        double *nf = nearF + ((size_t)p * D.near_cap + kk) * 3;
+        nf[0] = sg * a.f * BEM_I_FP;
+        nf[1] = sg * a.fz * BEM_I_FP;
+        nf[2] = sg * a.fe * BEM_I_FP;
+      }
+    }
+    __syncthreads();  // sm is reused by the next pair
   }
 }
 
@@ -1625,6 +1632,11 @@ static bem_far far_params(const bem_dom_dev *D, const bem_qp *q, int periodic) {
 // The periodic kernels keep a copy of the real-space term table in dynamic
 // shared memory (BEM_WT_SMEM bytes), which takes some of them past the 48 KB
 // a block gets without asking.
+// blocks per node of the near-singular kernels: each strides over the node's
+// listed pairs (a grid over the table's whole capacity would start mostly
+// empty blocks)
+static int near_grid_y(const bem_dom_dev *D) { return D->near_cap < 32 ? D->near_cap : 32; }
+
 static int q0_smem_attrs() {
   const int b = (int)BEM_WT_SMEM;
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
@@ -1704,7 +1716,8 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    k_q0_near<<<dim3(N, D->near_cap), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF, S->status, S->terms);
+    k_q0_near<<<dim3(N, near_grid_y(D)), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF,
+                                                                       S->status, S->terms);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
     k_q0_self<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
@@ -1717,7 +1730,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
     k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, G, H, dG, dH, 0, N);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[2], st);
-    k_fs_near<<<dim3(N, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF, 0);
+    k_fs_near<<<dim3(N, near_grid_y(D)), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, G, H, dG, dH, S->nearF, 0);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
     k_fs_self<<<N, NP_THREADS, 0, st>>>(*D, k, G, H, dG, dH, S->selfF, S->status, 0);
@@ -1786,7 +1799,7 @@ extern "C" int bem_launch_fs_deriv(const bem_dom_dev *D, double k, bem_scratch *
   const long long npairs = (long long)np * D->ne;
   k_fs_regular<<<(unsigned)((npairs + 127) / 128), 128, 0, st>>>(*D, k, S->flag, nullptr, nullptr, dG, dH, p0, np);
   bem_count_launches(1);
-  k_fs_near<<<dim3(np, D->near_cap), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, nullptr, nullptr, dG, dH,
+  k_fs_near<<<dim3(np, near_grid_y(D)), NP_THREADS, 0, st>>>(*D, k, S->near_s, S->near_n, nullptr, nullptr, dG, dH,
                                                           S->nearF, p0);
   bem_count_launches(1);
   k_fs_self<<<np, NP_THREADS, 0, st>>>(*D, k, nullptr, nullptr, dG, dH, S->selfF, S->status, p0);

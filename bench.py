@@ -49,13 +49,14 @@ C_TERM_FLOPS = 280.0
 # context; the roofline divides by the FP64 rate measured in the run
 # (measured_fp64_peak), as the bf16 and HBM peaks of this pool are measured
 FP64_NOMINAL_TFLOPS = 37.2
-# The regular-pair kernels' hardware readings from one ncu capture of the
-# 216-quad workload (profiles/k_q0_regular_sphere216.md and
-# profiles/k_q0_far_sphere216.md, command given there): FP64 pipe busy
-# fraction (sm__pipe_fp64_cycles_active over elapsed cycles) and DRAM bytes
-# read + written per launch.
-NCU_REGULAR = {"k_q0_regular": {"fp64_pipe": None, "dram_bytes": None},
-               "k_q0_far": {"fp64_pipe": None, "dram_bytes": None}}
+# The regular-pair kernels' hardware readings from one ncu capture of a
+# timed-configuration launch on the 216-quad workload (profiles/
+# k_q0_regular_far_sphere216.md, command given there): FP64 pipe busy fraction
+# (sm__pipe_fp64_cycles_active over active cycles) and DRAM bytes read +
+# written per launch.  Reported for that workload only.
+NCU_WORKLOAD = "sphere216"
+NCU_REGULAR = {"k_q0_regular": {"fp64_pipe": 0.4304, "dram_bytes": 588288 + 28716032},
+               "k_q0_far": {"fp64_pipe": 0.4765, "dram_bytes": 1411328 + 1803520}}
 
 
 def measured_fp64_peak():
@@ -103,6 +104,10 @@ def parse():
     ap.add_argument("--sweep-dirs", type=int, default=8, help="--workload sweep: incidence directions (of 64)")
     ap.add_argument("--stream-requests", type=int, default=STREAM_REQUESTS,
                     help="requests of the headline stream in the default line (0: leave it out)")
+    ap.add_argument("--lu-sizes", default="1728,4096,12288", help="--workload lu: matrix orders")
+    ap.add_argument("--lu-arith", default="z,c,t1,t3",
+                    help="--workload lu: z FP64 (DMMA), c complex FP32 (CUDA cores), t1 / t3 complex FP32 with "
+                         "one / three split TF32 products on the tensor cores")
     ap.add_argument("--mixed-mode", type=int, default=3,
                     help="precision of the mixed form: 1 FP32, 2 TF32, 3 TF32x3 (three split TF32 products), 4 as 2; 0: skip it")
     return ap.parse_args()
@@ -495,21 +500,25 @@ def run_stream(args, rank, world):
         dist.destroy_process_group()
 
 
-def roofline_record(achieved, fp64_peak, terms_reg, cnt):
+def roofline_record(achieved, fp64_peak, terms_reg, cnt, workload, out_bytes):
     """The dominant kernels' roofline: periodic regular-pair assembly
     (k_q0_regular on near-ish pairs, k_q0_far on far ones, one phase), FP64
     work = lattice terms counted by the kernels x the frozen per-term count,
     over the phase's CUDA-event time; beside it the FP64 pipe fraction and DRAM
     traffic ncu read on the same kernels."""
     reg, far = NCU_REGULAR["k_q0_regular"], NCU_REGULAR["k_q0_far"]
-    traffic = None
-    if reg["dram_bytes"] is not None and far["dram_bytes"] is not None:
+    traffic, pipe = None, {"k_q0_regular": None, "k_q0_far": None}
+    if workload == NCU_WORKLOAD:
         traffic = reg["dram_bytes"] + far["dram_bytes"]
+        pipe = {"k_q0_regular": reg["fp64_pipe"], "k_q0_far": far["fp64_pipe"]}
     return {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far (regular pairs)", "achieved": achieved,
             "peak": fp64_peak, "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
             "traffic": traffic, "traffic_unit": "bytes per launch pair (ncu dram__bytes_read.sum + write.sum)",
+            "algorithmic_bytes": out_bytes,
+            "algorithmic_bytes_what": "G and H of the periodic domain written (the kernels' only DRAM output; "
+                                      "inputs are L2-resident)",
             "peak_source": "of measured: cuBLAS DGEMM 8192^3 in this run (nominal %.1f TFLOP/s)" % FP64_NOMINAL_TFLOPS,
-            "fp64_pipe_frac_ncu": {"k_q0_regular": reg["fp64_pipe"], "k_q0_far": far["fp64_pipe"]},
+            "fp64_pipe_frac_ncu": pipe,
             "work": "%.3e lattice terms x %.0f FP64 ops per launch" % (terms_reg, C_TERM_FLOPS),
             "mean_terms_per_point": cnt[0] / max(cnt[3], 1)}
 
@@ -598,6 +607,83 @@ def run_sweep(args, rank, world):
         print(json.dumps(line))
 
 
+def run_lu(args, rank, world):
+    """The device LU alone (bem_lu.cu): factorisation and one-right-hand-side
+    solve of a seeded random complex matrix (diagonally heavy, rows permuted
+    so that every panel moves rows), by order and arithmetic, CUDA events on
+    the factorisation's stream, best of --steps after --warmup; the relative
+    residual ||A x - b|| / (||A|| ||x||) checks each result."""
+    import ctypes
+    import torch
+    from bem3_aw_qd2_b200 import api
+    _, g = api.libs()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    vp = ctypes.c_void_p
+    g.bem_lu_init.argtypes = [vp, ctypes.c_int]
+    g.bem_lu_free.argtypes = [vp]
+    for p in ("z", "c"):
+        getattr(g, "bem_lu_factor_" + p).argtypes = [vp, vp, ctypes.c_int, vp]
+        getattr(g, "bem_lu_solve_" + p).argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    g.bem_lu_status.argtypes = [vp, vp]
+    g.bem_lu_status.restype = ctypes.c_uint
+    g.bem_lu_attach_tc.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    g.bem_lu_detach_tc.argtypes = [vp]
+    st = torch.cuda.Stream()
+    out = []
+    for arith in args.lu_arith.split(","):
+        for n in [int(x) for x in args.lu_sizes.split(",")]:
+            w = ctypes.create_string_buffer(4096)
+            wp = ctypes.addressof(w)
+            if g.bem_lu_init(wp, 0) != 0:
+                raise RuntimeError("bem_lu_init failed")
+            if arith.startswith("t") and g.bem_lu_attach_tc(wp, n, int(arith[1])) != 0:
+                raise RuntimeError("tensor-core update buffers")
+            dt = torch.complex128 if arith == "z" else torch.complex64
+            gen = torch.Generator(device="cuda").manual_seed(n)
+            A0 = torch.randn(n, n, dtype=dt, device="cuda", generator=gen) / n ** 0.5
+            A0 += (1.5 + 0.5j) * torch.eye(n, dtype=dt, device="cuda")
+            A0 = A0[torch.randperm(n, generator=gen, device="cuda")]
+            B0 = torch.randn(1, n, dtype=dt, device="cuda", generator=gen)
+            A = A0.clone()
+            p = "z" if arith == "z" else "c"
+            fac, sol = getattr(g, "bem_lu_factor_" + p), getattr(g, "bem_lu_solve_" + p)
+            tf, ts = [], []
+            with torch.cuda.stream(st):
+                for r in range(args.warmup + args.steps):
+                    A.copy_(A0)
+                    B = B0.clone()
+                    e0, e1, e2 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                    e0.record(st)
+                    if fac(wp, A.data_ptr(), n, st.cuda_stream) != 0:
+                        raise RuntimeError("factorisation failed")
+                    e1.record(st)
+                    if sol(wp, A.data_ptr(), n, 1, B.data_ptr(), st.cuda_stream) != 0:
+                        raise RuntimeError("solve failed")
+                    e2.record(st)
+                    e2.synchronize()
+                    if r >= args.warmup:
+                        tf.append(e0.elapsed_time(e1))
+                        ts.append(e1.elapsed_time(e2))
+            status = g.bem_lu_status(wp, st.cuda_stream)
+            x = B[0].to(torch.complex128)
+            Ad, bd = A0.to(torch.complex128), B0[0].to(torch.complex128)
+            res = float(torch.linalg.vector_norm(Ad @ x - bd) /
+                        (torch.linalg.matrix_norm(Ad) * torch.linalg.vector_norm(x)))
+            g.bem_lu_detach_tc(wp)
+            g.bem_lu_free(wp)
+            del A, A0, Ad
+            torch.cuda.empty_cache()
+            out.append({"n": n, "arith": arith, "factor_ms": min(tf), "solve_ms": min(ts),
+                        "tflops": 8.0 / 3.0 * n ** 3 / (min(tf) / 1e3) / 1e12, "rel_residual": res,
+                        "status": int(status)})
+    if rank == 0:
+        print(json.dumps({"metric": "complex LU factorisation time", "unit": "ms", "workload": "lu",
+                          "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+                          "data": "synthetic: seeded random complex matrices, (1.5 + 0.5i) I + N(0, 1/n), rows "
+                                  "permuted", "tflops_count": "8/3 n^3 real flop per complex LU",
+                          "results": out}))
+
+
 def workload_desc(name):
     from bem3_aw_qd2_b200 import meshgen
     return {**meshgen.describe(name), "media": "host rho 1000 c 1500 (wavelength 1); body rho 1200 c 2250",
@@ -609,6 +695,12 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference" and args.workload != "stream":
         return run_reference(args, rank, world)
+    if args.workload == "lu":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's dense solves are timed inside "
+                                                                  "its full-solve line (sphere216)"}))
+            return
+        return run_lu(args, rank, world)
     if args.workload == "sweep":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the sweep's reference time is the sphere1536 "
@@ -785,7 +877,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "solve_bieq_aqd2 + force_FN_aqd2 (C ABI, host buffers)"},
         "phase_ms": phase_ms,
-        "roofline": roofline_record(achieved, fp64_peak, terms_reg, cnt),
+        "roofline": roofline_record(achieved, fp64_peak, terms_reg, cnt, args.workload, 2 * 16 * n_dom ** 2),
         "clocks": clk,
         "mixed": mixed,
         "gpu_launches": int(launches),
