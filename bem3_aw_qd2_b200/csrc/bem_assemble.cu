@@ -482,7 +482,10 @@ __device__ __forceinline__ void far_point(bool tri, int i, int j, double &z, dou
     e = c_q.xf[j];
   }
 }
-__global__ void __launch_bounds__(FP_THREADS, 2) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
+#ifndef FP_MINB
+#define FP_MINB 2  // two blocks (16 warps) per SM: caps registers at 128
+#endif
+__global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
                                                         const uint8_t *__restrict__ flag, double *__restrict__ G,
                                                         double *__restrict__ H, unsigned *status,
                                                         unsigned long long *terms, long long pair0, long long npairs,
@@ -1677,18 +1680,19 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   if (ev) cudaEventRecord(ev[1], st);
   if (periodic) {
     if (lists) {
-      // one resident wave (2 blocks per SM) striding over each list
+      // one resident wave (RP_MINB / FP_MINB blocks per SM) striding over each list
       int dev = 0, nsm = 0;
       if (cudaGetDevice(&dev) != cudaSuccess ||
           cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
         return -1;
-      const unsigned grid = 2u * (unsigned)nsm;
+      const unsigned grid = RP_MINB * (unsigned)nsm, grid_far = FP_MINB * (unsigned)nsm;
       const bem_plist Lreg = {S->plist, S->pcount, 1};
       const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
       k_q0_regular<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
       bem_count_launches(1);
       if (D->far_rule) {
-        k_q0_far<<<grid, FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lfar);
+        k_q0_far<<<grid_far, FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs,
+                                                            Lfar);
         bem_count_launches(1);
       }
       if (D->has_tri) {

@@ -14,7 +14,7 @@
 //   k_dpv_rhs      B = H pv (3 right-hand sides) for the dpv solve (solve_dpv_bv, :533-653)
 //   k_force0       radiation force and torque, 4-point rule at the element
 //                  nodes (force_FN_aqd2 + bil_force_4p, bem3_aw_qd2_force.c:4-120)
-// The LU factorisations themselves run in cuSOLVER (bem_capi.cu).
+// The LU factorisations themselves are the device LU of bem_lu.cu (bem_capi.cu).
 #include "bem_count.h"
 #include <cuda_runtime.h>
 #include <stdint.h>

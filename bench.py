@@ -645,6 +645,7 @@ def run_lu(args, rank, world):
             A0 = A0[torch.randperm(n, generator=gen, device="cuda")]
             B0 = torch.randn(1, n, dtype=dt, device="cuda", generator=gen)
             A = A0.clone()
+            torch.cuda.synchronize()  # the inputs (default stream) before st copies them
             p = "z" if arith == "z" else "c"
             fac, sol = getattr(g, "bem_lu_factor_" + p), getattr(g, "bem_lu_solve_" + p)
             tf, ts = [], []
