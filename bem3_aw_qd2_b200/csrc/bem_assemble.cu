@@ -578,6 +578,83 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
 // ------------------------------------------------------------------ periodic near-singular pairs
 // 64x64 points (q0_bil_dcoef_v2_cc_GH, q0_bil_dcoef_v2_cc.c:206-281).
 #define NP_THREADS 256
+// The home-cell image of the quasi-periodic Green's function: the free-space
+// e^{ikR} / (4 pi R) and its gradient at r, in bem_qpgf's conventions.  The
+// near-singular and self integrals split G_qp = G0 + (G_qp - G0): G0 carries
+// the whole singularity and costs a sincos, so it is integrated on the
+// reference's own points (64 x 64 Gauss, the polar rule); the rest is smooth
+// over the element (its nearest singularities are the other lattice images)
+// and is integrated on the 12 x 12 Gauss rule of regular pairs, a lattice sum
+// at 144 points instead of 4096 or 6144.
+__device__ __forceinline__ void bem_g0(double k, const double vR[3], bem_gval &o) {
+  const double R2 = vR[0] * vR[0] + vR[1] * vR[1] + vR[2] * vR[2];
+  const double R = sqrt(R2), iR = 1.0 / R;
+  const cplx ce = cexpi(k * R);
+  const double c4 = 0.07957747154594766788 * iR;  // 1 / (4 pi R)
+  o.g = cscale(ce, c4);
+  // (i k R - 1) e^{ikR} / (4 pi R^3) times r
+  const cplx f = cscale(cmul(cmk(-1.0, k * R), ce), c4 * iR * iR);
+  o.gx = cscale(f, vR[0]);
+  o.gy = cscale(f, vR[1]);
+  o.gz = cscale(f, vR[2]);
+}
+// accumulate a point's G and H contributions: g = gv.g |W| wg, h = (grad gv . W) wh
+__device__ __forceinline__ void acc_gh(double (&v)[19], const bem_gval &gv, const double vW[3], double wg, double wh,
+                                       const double N[4]) {
+  const cplx g = cscale(gv.g, wg);
+  const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wh);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    v[2 * a] += g.re * N[a];
+    v[2 * a + 1] += g.im * N[a];
+    v[8 + 2 * a] += h.re * N[a];
+    v[8 + 2 * a + 1] += h.im * N[a];
+  }
+}
+// gv -= g0
+__device__ __forceinline__ void gval_sub(bem_gval &gv, const bem_gval &g0) {
+  gv.g = csub(gv.g, g0.g);
+  gv.gx = csub(gv.gx, g0.gx);
+  gv.gy = csub(gv.gy, g0.gy);
+  gv.gz = csub(gv.gz, g0.gz);
+}
+
+// point pt of the reference's near-singular rule (64 x 64, 3 parts of 64 x 64
+// on a triangle, with the reference's rounding there): (z, e), weight, R from
+// the node, W
+__device__ __forceinline__ void near_point(const bem_dom_dev &D, const bem_el &el, const bem_node &nd, bool tri, int pt,
+                                           double &z, double &e, double &wt, double vR[3], double vW[3]) {
+  const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
+  const int i = ij / BEM_GHN, j = ij % BEM_GHN;
+  z = c_q.xh[i];
+  e = c_q.xh[j];
+  wt = c_q.wh[i] * c_q.wh[j];
+  if (tri) {
+    bem_tri_point_ref(part, c_q.xh[i], c_q.xh[j], z, e);
+    wt *= bem_tri_wfac(c_q.xh[i], c_q.xh[j]);
+    bem_rw_ref(el, z, e, vR, vW);
+    for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
+  } else {
+    bem_rw(el, z, e, vR, vW);
+    for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+  }
+}
+// point pt of the regular-pair rule (12 x 12, 3 parts of 12 x 12 on a triangle)
+__device__ __forceinline__ void reg_point(const bem_el &el, const bem_node &nd, bool tri, int pt, double &z, double &e,
+                                          double &wt, double vR[3], double vW[3]) {
+  const int part = pt / (BEM_GLN * BEM_GLN), ij = pt % (BEM_GLN * BEM_GLN);
+  const int i = ij / BEM_GLN, j = ij % BEM_GLN;
+  z = c_q.xl[i];
+  e = c_q.xl[j];
+  wt = c_q.wl[i] * c_q.wl[j];
+  if (tri) {
+    bem_tri_point(part, c_q.xl[i], c_q.xl[j], z, e);
+    wt *= bem_tri_wfac(c_q.xl[i], c_q.xl[j]);
+  }
+  bem_rw(el, z, e, vR, vW);
+  for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
+}
+
 // register cap of the periodic near-singular and self kernels (0: compiler's choice)
 #ifndef NP_MAXREG
 #define NP_MAXREG 0
@@ -633,42 +710,63 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
     for (int c = 0; c < 19; ++c) v[c] = 0.0;
     unsigned st = 0;
     unsigned long long nterm = 0, npt = 0;
-    for (int pt = threadIdx.x; pt < (tri ? 3 : 1) * BEM_GHN * BEM_GHN; pt += NP_THREADS) {
-      const int part = pt / (BEM_GHN * BEM_GHN), ij = pt % (BEM_GHN * BEM_GHN);
-      const int i = ij / BEM_GHN, j = ij % BEM_GHN;
-      double z = c_q.xh[i], e = c_q.xh[j], wt = c_q.wh[i] * c_q.wh[j];
-      double vR[3], vW[3];
-      if (tri) {
-        bem_tri_point_ref(part, c_q.xh[i], c_q.xh[j], z, e);
-        wt *= bem_tri_wfac(c_q.xh[i], c_q.xh[j]);
-        bem_rw_ref(el, z, e, vR, vW);
-        for (int d = 0; d < 3; ++d) vR[d] = __dsub_rn(vR[d], nd.rt[d]);
-      } else {
-        bem_rw(el, z, e, vR, vW);
-        for (int d = 0; d < 3; ++d) vR[d] -= nd.rt[d];
-      }
-      bem_gval gv;
-      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
-      if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
-      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-      ++npt;
-      const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-      const cplx g = cscale(gv.g, aW * wt);
-      const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), wt);
-      double N[4];
+    const int npts = (tri ? 3 : 1) * BEM_GHN * BEM_GHN;
+    // the reference's points (q0_lit_dcoef_v2_cc_GH / q0_bil_dcoef_v2_cc_GH):
+    // the geometric F, and G0 unless a point lies on the lattice plane
+    bool on_plane = false;
+    for (int pt = threadIdx.x; pt < npts; pt += NP_THREADS) {
+      double z, e, wt, vR[3], vW[3], N[4];
+      near_point(D, el, nd, tri, pt, z, e, wt, vR, vW);
+      on_plane |= fabs(vR[2]) < BEM_FAR_PLANE_TOL;
+      bem_gval g0;
+      bem_g0(q.k, vR, g0);
       bem_Nn(tri, z, e, N);
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        v[2 * a] += g.re * N[a];
-        v[2 * a + 1] += g.im * N[a];
-        v[8 + 2 * a] += h.re * N[a];
-        v[8 + 2 * a + 1] += h.im * N[a];
-      }
+      acc_gh(v, g0, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wt, wt, N);
       double f, fz, fe;
       geomF(vR, vW, nd, f, fz, fe);
       v[16] += wt * f;
       v[17] += wt * fz;
       v[18] += wt * fe;
+    }
+    // G_qp - G0 on the regular-pair rule (12 x 12 on a quad, 3 parts of 12 x
+    // 12 on a triangle), whose points must stay off the lattice plane too
+    const int nreg = (tri ? 3 : 1) * BEM_GLN * BEM_GLN;
+    for (int pt = threadIdx.x; pt < nreg; pt += NP_THREADS) {
+      double z, e, wt, vR[3], vW[3];
+      reg_point(el, nd, tri, pt, z, e, wt, vR, vW);
+      on_plane |= fabs(vR[2]) < BEM_FAR_PLANE_TOL;
+    }
+    if (!__syncthreads_or(on_plane)) {
+      for (int pt = threadIdx.x; pt < nreg; pt += NP_THREADS) {
+        double z, e, wt, vR[3], vW[3], N[4];
+        reg_point(el, nd, tri, pt, z, e, wt, vR, vW);
+        bem_gval gv, g0;
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
+        if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+        nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+        ++npt;
+        bem_g0(q.k, vR, g0);
+        gval_sub(gv, g0);
+        bem_Nn(tri, z, e, N);
+        acc_gh(v, gv, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wt, wt, N);
+      }
+    } else {
+      // a point on the lattice plane: the reference's rule on the full
+      // quasi-periodic Green's function (its sums stop on rounding-decided
+      // zeros there, which only its own points reproduce)
+#pragma unroll
+      for (int c = 0; c < 16; ++c) v[c] = 0.0;
+      for (int pt = threadIdx.x; pt < npts; pt += NP_THREADS) {
+        double z, e, wt, vR[3], vW[3], N[4];
+        near_point(D, el, nd, tri, pt, z, e, wt, vR, vW);
+        bem_gval gv;
+        const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
+        if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+        nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+        ++npt;
+        bem_Nn(tri, z, e, N);
+        acc_gh(v, gv, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wt, wt, N);
+      }
     }
     count_work(terms + 1, nterm, npt);
     set_status(status, st);
@@ -732,6 +830,29 @@ __device__ __forceinline__ double bem_bdC(const bem_el &el) {
 }
 
 // periodic self pair: one block per collocation node p
+// point pt of the polar rule around the node (zt, et) on its own quad: (z, e),
+// the weight with the polar Jacobian, R = rr K from the node, W; false when
+// the rule's radius comes out negative (bad geometry)
+__device__ __forceinline__ bool self_point(const bem_el &el, const double th[5], const double r[5], double zt, double et,
+                                           int pt, double &z, double &e, double &wr, double vR[3], double vW[3]) {
+  const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
+  const polar_pt tp = polar_theta(th, idx);
+  const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
+  double sth, cth;
+  sincos(tp.th, &sth, &cth);
+  const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
+  wr = tp.wth * 0.5 * rm * c_q.wl[ir] * rr;
+  z = rr * cth + zt;
+  e = rr * sth + et;
+  double K[3];
+  bem_K(el, rr, cth, sth, zt, et, K);
+  for (int d = 0; d < 3; ++d) {
+    vR[d] = rr * K[d];
+    vW[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
+  }
+  return rm >= 0.0;
+}
+
 __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_qp q, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ selfF,
                                                         unsigned *status, unsigned long long *terms) {
@@ -748,42 +869,64 @@ __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_q
   double r[5], th[5];
   bem_node_r_th(zt, et, r, th);
   unsigned long long nterm = 0, npt = 0;
-  double v[16];
+  double v[19];
 #pragma unroll
-  for (int c = 0; c < 16; ++c) v[c] = 0.0;
+  for (int c = 0; c < 19; ++c) v[c] = 0.0;
   unsigned st = 0;
+  // the node on its own element
+  bem_node nd;
+  {
+    double w0[3];
+    bem_rw(el, zt, et, nd.rt, w0);
+  }
+  // the polar rule around the node (q0_bil_coef_bd, q0_bil_coef.c:246-338):
+  // G0 at every point, unless a point lies on the lattice plane
+  bool on_plane = false;
   for (int pt = threadIdx.x; pt < 512 * BEM_GLN; pt += NP_THREADS) {
-    const int idx = pt / BEM_GLN, ir = pt % BEM_GLN;
-    const polar_pt tp = polar_theta(th, idx);
-    const double rm = bem_rmax(r[tp.j], r[tp.j + 1], th[tp.j], th[tp.j + 1], tp.th);
-    if (rm < 0.0) st |= BEM_ST_GEOMETRY;
-    double sth, cth;
-    sincos(tp.th, &sth, &cth);
-    const double rr = 0.5 * rm * (c_q.xl[ir] + 1.0);
-    const double w = tp.wth * 0.5 * rm * c_q.wl[ir];
-    const double z = rr * cth + zt, e = rr * sth + et;
-    double K[3], vR[3], vW[3];
-    bem_K(el, rr, cth, sth, zt, et, K);
-    for (int d = 0; d < 3; ++d) {
-      vR[d] = rr * K[d];
-      vW[d] = el.cw[d][0] + el.cw[d][1] * z + el.cw[d][2] * e;
-    }
-    bem_gval gv;
-    const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
-    if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
-    nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
-    ++npt;
-    const double aW = sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]);
-    const cplx g = cscale(gv.g, aW * rr * w);
-    const cplx h = cscale(cadd(cadd(cscale(gv.gx, vW[0]), cscale(gv.gy, vW[1])), cscale(gv.gz, vW[2])), rr * w);
-    double N[4];
+    double z, e, wr, vR[3], vW[3], N[4];
+    if (!self_point(el, th, r, zt, et, pt, z, e, wr, vR, vW)) st |= BEM_ST_GEOMETRY;
+    on_plane |= fabs(vR[2]) < BEM_FAR_PLANE_TOL;
+    bem_gval g0;
+    bem_g0(q.k, vR, g0);
     bem_Nn4(z, e, N);
+    acc_gh(v, g0, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wr, wr, N);
+  }
+  // G_qp - G0 on the 12 x 12 Gauss rule over the element
+  for (int pt = threadIdx.x; pt < BEM_GLN * BEM_GLN; pt += NP_THREADS) {
+    double z, e, wt, vR[3], vW[3];
+    reg_point(el, nd, false, pt, z, e, wt, vR, vW);
+    on_plane |= fabs(vR[2]) < BEM_FAR_PLANE_TOL;
+  }
+  if (!__syncthreads_or(on_plane)) {
+    for (int pt = threadIdx.x; pt < BEM_GLN * BEM_GLN; pt += NP_THREADS) {
+      double z, e, wt, vR[3], vW[3], N[4];
+      reg_point(el, nd, false, pt, z, e, wt, vR, vW);
+      bem_gval gv, g0;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
+      if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      bem_g0(q.k, vR, g0);
+      gval_sub(gv, g0);
+      bem_Nn4(z, e, N);
+      acc_gh(v, gv, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wt, wt, N);
+    }
+  } else {
+    // a point on the lattice plane (a plane element, or a curved one whose
+    // points meet the node's height): the reference's polar rule on the full
+    // quasi-periodic Green's function
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      v[2 * a] += g.re * N[a];
-      v[2 * a + 1] += g.im * N[a];
-      v[8 + 2 * a] += h.re * N[a];
-      v[8 + 2 * a + 1] += h.im * N[a];
+    for (int c = 0; c < 16; ++c) v[c] = 0.0;
+    for (int pt = threadIdx.x; pt < 512 * BEM_GLN; pt += NP_THREADS) {
+      double z, e, wr, vR[3], vW[3], N[4];
+      self_point(el, th, r, zt, et, pt, z, e, wr, vR, vW);
+      bem_gval gv;
+      const int rc = bem_qpgf(q, vR[0], vR[1], vR[2], gv, wts);
+      if (rc < 0) st |= (rc == -12 || rc == -23) ? BEM_ST_RAYLEIGH : BEM_ST_QPGF_LIMIT;
+      nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
+      ++npt;
+      bem_Nn4(z, e, N);
+      acc_gh(v, gv, vW, sqrt(vW[0] * vW[0] + vW[1] * vW[1] + vW[2] * vW[2]) * wr, wr, N);
     }
   }
   count_work(terms + 2, nterm, npt);
