@@ -662,7 +662,7 @@ __device__ __forceinline__ void reg_point(const bem_el &el, const bem_node &nd, 
 #if NP_MAXREG > 0
 #define NP_BOUNDS __maxnreg__(NP_MAXREG)
 #else
-#define NP_BOUNDS __launch_bounds__(NP_THREADS)
+#define NP_BOUNDS __launch_bounds__(NP_THREADS, 2)  // two blocks (16 warps) per SM: at most 128 registers
 #endif
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*NP_THREADS */) {

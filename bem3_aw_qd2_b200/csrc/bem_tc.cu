@@ -12,13 +12,13 @@
 // is split x = hi + lo (hi rounded to TF32) and the product is
 // hi hi + hi lo + lo hi: close to FP32 accuracy; nprod = 1 is a single TF32
 // product.  A pack kernel writes the operands K-major (A'' rows: L21 rows;
-// B'' rows: 64 real-part then 64 imaginary-part columns per tile).  Each CTA
-// computes a 128-row x 64-complex-column tile: one thread streams the
-// 128-byte-wide K boxes of both operands with 2D TMA into a ring of
-// shared-memory stages (128-byte swizzle), another issues the MMAs into a
-// 128 x 128 FP32 accumulator in TMEM and frees each stage with
-// tcgen05.commit, and the four warps read the accumulator back (tcgen05.ld)
-// and subtract it from C.  Every wait on an mbarrier is bounded: a wait that
+// B'' rows: per 64-column sub-tile, 64 real-part then 64 imaginary-part
+// columns).  Each CTA computes a 128-row x 128-complex-column tile: one
+// thread streams the 128-byte-wide K boxes of both operands with 2D TMA into
+// a ring of shared-memory stages (128-byte swizzle), another issues the MMAs
+// (M = 128, N = 256) into a 128 x 256 FP32 accumulator in TMEM and frees each
+// stage with tcgen05.commit, and the four warps read the accumulator back
+// (tcgen05.ld) and subtract it from C a row at a time.  Every wait on an mbarrier is bounded: a wait that
 // gives up sets BEM_TC_ST_WAIT, waits (bounded) for the copies and MMAs in
 // flight, frees the TMEM and returns.  The TMA loads read this GPU's own
 // memory and use no multicast.
@@ -30,11 +30,15 @@
 #include "bem_tc.h"
 
 #define TC_M 128        // rows of a tile (TMEM lanes)
-#define TC_NC 64        // complex output columns of a tile (128 real accumulator columns)
+#define TC_NC 64        // complex columns of a packed sub-tile (its 64 real then 64 imaginary B'' rows)
+#define TC_NS 2         // sub-tiles of a CTA's tile: 128 complex columns
+#define TC_N (2 * TC_NC * TC_NS)  // real accumulator columns of a tile (256: the MMA's N)
 #define TC_TH 128       // four warps: one TMEM lane quarter each
 #define TC_BOX_K 32     // FP32 elements per 128-byte swizzle row
-#define TC_BOX_BYTES (TC_M * 128)
-#define TC_STAGES 2     // K boxes in flight (A and B box each: 32 KB a stage)
+#define TC_A_BYTES (TC_M * 128)   // an A box: TC_M rows x 128 bytes
+#define TC_B_BYTES (TC_N * 128)   // a B box: TC_N rows x 128 bytes
+#define TC_STAGE_BYTES (TC_A_BYTES + TC_B_BYTES)
+#define TC_STAGES 2     // K boxes in flight (48 KB a stage)
 #define TC_KR (2 * LU_OUTER_W)  // reals of one product part of a packed row
 #define TC_WAIT_NS 1000000000ull  // one second
 
@@ -139,8 +143,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 128, M = 128
-#define TC_IDESC ((1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(2 * TC_NC) >> 3 << 17) | ((uint32_t)TC_M >> 4 << 24))
+// instruction descriptor: D F32, A and B TF32, both K-major, N = 256, M = 128
+#define TC_IDESC ((1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)TC_N >> 3 << 17) | ((uint32_t)TC_M >> 4 << 24))
 
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
@@ -171,7 +175,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 // ---------------------------------------------------------------- the update
 // grid: (column tiles, row tiles); dynamic smem: TC_STAGES stages of an A box
 // and a B box (TC_M rows x 128 bytes each)
-__global__ void __launch_bounds__(TC_TH, 3)
+__global__ void __launch_bounds__(TC_TH, 2)
     k_tc_update(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2 *C, long ldc,
                 int n, int r0, int nbox, unsigned *status) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(TC_TH, 3)
   unsigned char *sm = (unsigned char *)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int row_tile = r0 + blockIdx.y * TC_M;   // matrix row of the tile's first row
-  const int col_tile = blockIdx.x;               // column tile (TC_NC complex columns)
+  const int col_tile = blockIdx.x;               // column tile (TC_NC x TC_NS complex columns)
   if (t == 0) {
     for (int s = 0; s < TC_STAGES; ++s) {
       mbar_init(&bar_full[s], 1);
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(TC_TH, 3)
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(2 * TC_NC)
+                 "r"(TC_N)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -212,10 +216,10 @@ __global__ void __launch_bounds__(TC_TH, 3)
         s_fail = 1;
         break;
       }
-      unsigned char *sA = sm + (size_t)s * 2 * TC_BOX_BYTES, *sB = sA + TC_BOX_BYTES;
-      mbar_expect_tx(&bar_full[s], (uint32_t)(2 * TC_BOX_BYTES));
+      unsigned char *sA = sm + (size_t)s * TC_STAGE_BYTES, *sB = sA + TC_A_BYTES;
+      mbar_expect_tx(&bar_full[s], (uint32_t)TC_STAGE_BYTES);
       tma_load_2d(sA, &tmA, b * TC_BOX_K, row_tile - r0, &bar_full[s]);
-      tma_load_2d(sB, &tmB, b * TC_BOX_K, col_tile * 2 * TC_NC, &bar_full[s]);
+      tma_load_2d(sB, &tmB, b * TC_BOX_K, col_tile * TC_N, &bar_full[s]);
       issued = b + 1;
     }
     // the copies still in flight land before the CTA may end (bounded)
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(TC_TH, 3)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(sm + (size_t)s * 2 * TC_BOX_BYTES), b0 = a0 + TC_BOX_BYTES;
+      const uint32_t a0 = smem_u32(sm + (size_t)s * TC_STAGE_BYTES), b0 = a0 + TC_A_BYTES;
 #pragma unroll
       for (int ks = 0; ks < 4; ++ks)
         tc_mma(tmem, umma_desc(a0 + 32u * ks), umma_desc(b0 + 32u * ks), (b | ks) ? 1u : 0u);
@@ -264,19 +268,21 @@ __global__ void __launch_bounds__(TC_TH, 3)
     // read and written a row at a time, 32 consecutive columns per warp access
     float *tre = (float *)sm + warp * (2 * 32 * 33), *tim = tre + 32 * 33;
     const uint32_t tw = tmem + ((uint32_t)(32 * warp) << 16);
-    const int col0 = r0 + col_tile * TC_NC;
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
+    // accumulator columns: per sub-tile u, 64 real-part then 64 imaginary-part columns
+#pragma unroll 1
+    for (int q = 0; q < 2 * TC_NS; ++q) {
+      const int u = q >> 1, half = q & 1;
+      const int col0 = r0 + (col_tile * TC_NS + u) * TC_NC + 32 * half;
       float re[32], im[32];
-      tmem_ld32(tw + (uint32_t)(32 * half), re);
-      tmem_ld32(tw + (uint32_t)(TC_NC + 32 * half), im);
+      tmem_ld32(tw + (uint32_t)(2 * TC_NC * u + 32 * half), re);
+      tmem_ld32(tw + (uint32_t)(2 * TC_NC * u + TC_NC + 32 * half), im);
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         tre[lane * 33 + j] = re[j];
         tim[lane * 33 + j] = im[j];
       }
       __syncwarp();
-      const int col = col0 + 32 * half + lane;
+      const int col = col0 + lane;
       // all 32 rows' loads in flight at once, then the stores
       float2 x[32];
 #pragma unroll
@@ -296,7 +302,7 @@ __global__ void __launch_bounds__(TC_TH, 3)
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_NC) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_N) : "memory");
 }
 
 // ---------------------------------------------------------------- host side
@@ -304,7 +310,7 @@ typedef CUresult (*encode_tiled_t)(CUtensorMap *, CUtensorMapDataType, cuuint32_
                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-static int encode(bem_tc *t, CUtensorMap *tm, float *base, int cols, long rows) {
+static int encode(bem_tc *t, CUtensorMap *tm, float *base, int cols, long rows, int box_rows) {
   static encode_tiled_t fn = nullptr;
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
@@ -317,7 +323,7 @@ static int encode(bem_tc *t, CUtensorMap *tm, float *base, int cols, long rows) 
   }
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(float)};
-  const cuuint32_t box[2] = {TC_BOX_K, TC_M};
+  const cuuint32_t box[2] = {TC_BOX_K, (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
   const CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -329,7 +335,7 @@ static int encode(bem_tc *t, CUtensorMap *tm, float *base, int cols, long rows) 
   return 0;
 }
 
-static size_t tc_smem() { return (size_t)TC_STAGES * 2 * TC_BOX_BYTES + 1024; }
+static size_t tc_smem() { return (size_t)TC_STAGES * TC_STAGE_BYTES + 1024; }
 
 extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   if (nprod != 1 && nprod != 3) nprod = 3;
@@ -339,7 +345,9 @@ extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   t->Ap = t->Bp = nullptr;
   t->ready = false;
   const int kp = TC_KR * nprod;
-  const long arows = n + TC_M, brows = 2L * ((n + TC_NC - 1) / TC_NC + 1) * TC_NC;
+  // rows a tile's TMA boxes may reach: A to the last row tile's end, B'' to
+  // the last column tile's TC_N rows
+  const long arows = n + TC_M, brows = (long)TC_N * ((n + TC_NC * TC_NS - 1) / (TC_NC * TC_NS) + 1);
   if (cudaMalloc(&t->Ap, (size_t)arows * kp * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&t->Bp, (size_t)brows * kp * sizeof(float)) != cudaSuccess) {
     snprintf(t->err, sizeof(t->err), "tensor-core update: out of device memory");
@@ -350,7 +358,7 @@ extern "C" int bem_tc_prepare(bem_tc *t, int n, int nprod) {
   if (cudaMemset(t->Ap, 0, (size_t)arows * kp * sizeof(float)) != cudaSuccess ||
       cudaMemset(t->Bp, 0, (size_t)brows * kp * sizeof(float)) != cudaSuccess)
     return -1;
-  if (encode(t, &t->tmA, t->Ap, kp, arows) || encode(t, &t->tmB, t->Bp, kp, brows)) return -1;
+  if (encode(t, &t->tmA, t->Ap, kp, arows, TC_M) || encode(t, &t->tmB, t->Bp, kp, brows, TC_N)) return -1;
   if (cudaFuncSetAttribute(k_tc_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem()) != cudaSuccess) {
     snprintf(t->err, sizeof(t->err), "tensor-core update: shared memory attribute");
     return -1;
@@ -365,10 +373,11 @@ extern "C" void bem_tc_launch(bem_tc *t, float2 *M, long lda, int n, int K, unsi
   const int r0 = K + LU_OUTER_W;
   const int rows = n - r0;
   if (rows <= 0) return;
-  const int ctiles = (rows + TC_NC - 1) / TC_NC, rtiles = (rows + TC_M - 1) / TC_M;
-  const long work = (long)rows * LU_OUTER_W + (long)ctiles * TC_NC * LU_OUTER_W;
+  const int ctiles = (rows + TC_NC * TC_NS - 1) / (TC_NC * TC_NS), rtiles = (rows + TC_M - 1) / TC_M;
+  const int subtiles = ctiles * TC_NS;  // 64-column sub-tiles packed (the last ones may lie past n)
+  const long work = (long)rows * LU_OUTER_W + (long)subtiles * TC_NC * LU_OUTER_W;
   const int pb = (int)((work + 255) / 256 < 8192 ? (work + 255) / 256 : 8192);
-  k_tc_pack<<<pb, 256, 0, st>>>(M, lda, n, K, r0, t->nprod, t->Ap, t->Bp, rows, ctiles);
+  k_tc_pack<<<pb, 256, 0, st>>>(M, lda, n, K, r0, t->nprod, t->Ap, t->Bp, rows, subtiles);
   const int nbox = TC_KR * t->nprod / TC_BOX_K;
   k_tc_update<<<dim3(ctiles, rtiles), TC_TH, tc_smem(), st>>>(t->tmA, t->tmB, M, lda, n, r0, nbox, status);
 }

@@ -108,8 +108,9 @@ def parse():
     ap.add_argument("--lu-arith", default="z,c,t1,t3",
                     help="--workload lu: z FP64 (DMMA), c complex FP32 (CUDA cores), t1 / t3 complex FP32 with "
                          "one / three split TF32 products on the tensor cores")
-    ap.add_argument("--mixed-mode", type=int, default=3,
-                    help="precision of the mixed form: 1 FP32, 2 TF32, 3 TF32x3 (three split TF32 products), 4 as 2; 0: skip it")
+    ap.add_argument("--mixed-mode", type=int, default=2,
+                    help="precision of the mixed form: 1 FP32, 2 TF32 (one product on the tensor cores), 3 TF32x3 "
+                         "(three split TF32 products), 4 as 2; 0: skip it")
     return ap.parse_args()
 
 
@@ -438,7 +439,7 @@ def run_stream(args, rank, world):
         cases.append(c)
         probs.append(c.problem())
     out = {}
-    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 3)):
+    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 2)):
         srv = api.Server(device=local, hbm_budget=int(args.hbm_gb * (1 << 30)), slots=args.slots)
         # warm-up: one request per mesh size
         for i, n in enumerate(sorted({r["n"] for r, _ in reqs})):
@@ -565,7 +566,7 @@ def run_sweep(args, rank, world):
         raise RuntimeError("bemgpu_create failed")
     rc3 = np.zeros(3)
     res = {}
-    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 3)):
+    for tag, prec in (("fp64", 0), ("mixed", args.mixed_mode or 2)):
         g.bemgpu_set_precision(ctx, prec)
         # warm-up: the first instance (kernels loaded, graphs captured)
         g.bemgpu_load(ctx, ctypes.byref(probs[0]))
@@ -888,7 +889,7 @@ def main():
         # mixed precision against the plain FP64 drop-in path
         case.close()
         torch.cuda.empty_cache()
-        out["stream"] = stream_compare(args.stream_requests, 200.0, args.slots, args.hbm_gb, args.mixed_mode or 3,
+        out["stream"] = stream_compare(args.stream_requests, 200.0, args.slots, args.hbm_gb, args.mixed_mode or 2,
                                        device=local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)

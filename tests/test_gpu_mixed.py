@@ -1,14 +1,14 @@
-"""The mixed-precision solve at sizes where its panel factorisation runs every
-stage (chunk selections, reductions, final selection): complex-FP32 LU with
-tensor-core updates and FP64 refinement against the plain FP64 solve of the
-same assembled system.
+"""The mixed-precision solve (complex FP32 LU, FP64 refinement) against the
+plain FP64 solve of the same assembled system, with the tensor-core
+outer-block updates as one TF32 product (mode 2) and as three split products
+(mode 3).
 
 Tolerances (stated here, used below):
   surface coefficients P, dP, pv, dpv   1e-10 relative to the array maximum
   force / torque (type 0)               1e-8 relative to |F| (the serving target)
-The 216-quad sphere (n = 1728) has 4 row chunks per panel; the 1536-quad
-sphere (n = 12288) has 24, whose 768 candidate rows need a reduction stage
-before the final selection.
+The 216-quad sphere (n = 1728) is one outer block (no tensor-core update runs);
+the 1536-quad sphere (n = 12288) has 96 outer blocks on the tensor cores and
+panels whose leaves run several rounds of candidate selection.
 """
 import tempfile
 
