@@ -57,6 +57,7 @@ def libs():
         g.bemgpu_get_precision.argtypes = [vp]
         g.bemgpu_set_ewald_scale.argtypes = [vp, ctypes.c_double]
         g.bemgpu_set_far_rule.argtypes = [vp, ctypes.c_int]
+        g.bemgpu_rule_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
         g.bemgpu_autotune.argtypes = [vp, _d]
         g.bemgpu_solve_stats.argtypes = [vp, _i, _d, _i, ctypes.c_int]
         g.bemgpu_set_interior_reuse.argtypes = [vp, ctypes.c_int]
@@ -238,8 +239,18 @@ class Case:
         self._check(libs()[1].bemgpu_set_ewald_scale(self.ctx, float(scale)), "set_ewald_scale")
 
     def set_far_rule(self, on):
-        """1 (default): 8 x 8 Gauss rule for far regular quad pairs of the periodic domain; 0: 12 x 12 everywhere."""
+        """1 (default): shorter rules (10 down to 6 points a side) for regular pairs of
+        the periodic domain far enough from every lattice image; 0: 12 x 12 everywhere."""
         self._check(libs()[1].bemgpu_set_far_rule(self.ctx, int(bool(on))), "set_far_rule")
+
+    def rule_pairs(self):
+        """Regular pairs of the periodic domain in the last assembly: on the
+        reference's 12 x 12 rule, then on the 10, 9, 8, 7 and 6-point rules
+        (None when the assembly kept no pair lists)."""
+        out = (ctypes.c_ulonglong * 6)()
+        if libs()[1].bemgpu_rule_pairs(self.ctx, out) != 0:
+            return None
+        return list(out)
 
     def precision(self):
         """The precision mode in effect (see bemgpu.h)."""

@@ -91,18 +91,46 @@ __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], co
 
 // ------------------------------------------------------------------ classify
 // One block per collocation node p; threads stride over source elements.
-// Far pairs of the periodic domain (flag 3): a source element whose centre is
-// at least 5 circumradii R from the nearest lattice image of the collocation
-// node, with k 2R <= 2.  There the integrand is analytic well beyond the
-// element (its nearest singularity is that image) and an 8 x 8 rule (Gauss on
-// a quad, collapsed Gauss over a triangle) gives the reference's 12 x 12
-// integrals to below 1e-13 of the entry (checked against 40 x 40 on curved
-// quads and on triangles, k 2R up to 2).
+// Regular pairs of the periodic domain on a shorter rule (flag 3 + t, tier t):
+// a source element whose centre is at least d_t circumradii R from the nearest
+// lattice image of the collocation node, with k R <= kR_t, is integrated with
+// the n_t x n_t Gauss rule on a quad (the collapsed rule over the whole
+// triangle on a triangle) instead of the reference's 12 x 12 per quad or
+// triangle part.  There the integrand is analytic well beyond the element (its
+// nearest singularity is that image) and turns by at most k R in phase across it:
+//    t   n_t   d_t   kR_t
+//    0   10    3     1
+//    1    9    3.5   1
+//    2    8    5     1
+//    3    7    8     0.5
+//    4    6    25    0.2
+// Each rule gives the converged integral (and so the reference's 12 x 12,
+// itself converged there) to about 1e-13 of the pair's largest entry: checked
+// against 40 x 40 on curved and on twisted quads, on triangles with angles of
+// 25 degrees and more, and on the cube-sphere and spheroid elements.  Tiers
+// 0, 1, 3 and 4 also need a quad that is nearly flat and not long: the part of
+// its twist c3 along the normal c1 x c2 at most a tenth of its shorter
+// half-side |c1| or |c2| (cube-sphere and spheroid quads: under 0.05), and the
+// longer half-side at most 3 times the shorter (a twisted quad's area element
+// |W| has complex zeros near the element, which the shorter rules feel first;
+// at a quarter the 6-point tier is off by 1e-11); other quads keep tier 2 or
+// the reference rule.
 struct bem_far { int on; double d1x, d1y, d2x, d2y, idet, k; };
+__device__ __forceinline__ bool quad_tier_shape(const bem_el &el) {
+  double c1[3], c2[3], c3[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { c1[d] = el.cr[d][1]; c2[d] = el.cr[d][2]; c3[d] = el.cr[d][3]; }
+  const double n0 = c1[1] * c2[2] - c1[2] * c2[1], n1 = c1[2] * c2[0] - c1[0] * c2[2], n2 = c1[0] * c2[1] - c1[1] * c2[0];
+  const double nn = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+  const double l1 = sqrt(dot3(c1, c1)), l2 = sqrt(dot3(c2, c2));
+  const double lmin = fmin(l1, l2), lmax = fmax(l1, l2);
+  return nn > 0.0 && fabs(c3[0] * n0 + c3[1] * n1 + c3[2] * n2) <= 0.1 * lmin * nn && lmax <= 3.0 * lmin;
+}
 // (distance from the element's centre (a triangle's centroid) to the nearest
 // lattice image of rt) / (the element's circumradius R about that centre),
-// squared; -1 where k 2R > 2.
-__device__ __forceinline__ double pair_ratio2(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
+// squared, and (k R)^2.
+__device__ __forceinline__ double pair_ratio2(const bem_far &fr, const bem_el &el, const double rt[3], bool tri,
+                                              double &kR2) {
   // corners (+-1, +-1) of a quad, (1, 0), (-1/2, +-sqrt3/2) of a triangle
   double R2 = 0.0;
 #pragma unroll
@@ -120,7 +148,7 @@ __device__ __forceinline__ double pair_ratio2(const bem_far &fr, const bem_el &e
     }
     R2 = fmax(R2, v2);
   }
-  if (4.0 * fr.k * fr.k * R2 > 4.0) return -1.0;
+  kR2 = fr.k * fr.k * R2;
   const double vz = rt[2] - el.cr[2][0];
   const double vx = rt[0] - el.cr[0][0], vy = rt[1] - el.cr[1][0];
   const double l1 = floor((vx * fr.d2y - vy * fr.d2x) * fr.idet + 0.5);
@@ -138,42 +166,73 @@ __device__ __forceinline__ double pair_ratio2(const bem_far &fr, const bem_el &e
 // stop on rounding-decided zeros, so its values at its own points are not a
 // smooth function that another rule could reproduce.
 #define BEM_FAR_PLANE_TOL 1e-10
-__device__ __forceinline__ void far_point(bool tri, int i, int j, double &z, double &e);
-// far pair: centre at least 5 circumradii from every lattice image of rt, and
-// none of the far rule's points within BEM_FAR_PLANE_TOL of rt's lattice plane
-// (the reference rule's points are checked by the caller)
-__device__ __forceinline__ bool far_pair(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
-  if (pair_ratio2(fr, el, rt, tri) < 25.0) return false;
-  for (int ij = 0; ij < BEM_GFN * BEM_GFN; ++ij) {
-    double z, e, r[3], w[3];
-    far_point(tri, ij / BEM_GFN, ij % BEM_GFN, z, e);
-    bem_rw(el, z, e, r, w);
-    if (fabs(r[2] - rt[2]) < BEM_FAR_PLANE_TOL) return false;
+// point (i, j) of tier t's rule: Gauss on a quad; on a triangle the collapsed
+// (Duffy) rule over the whole reference triangle, (z, e) = (1 - 3u/2,
+// sqrt3/2 u (1 - 2v)) for (u, v) in [0, 1]^2, weight u w_u w_v
+__device__ __forceinline__ void tier_point(int t, bool tri, int i, int j, double &z, double &e) {
+  if (tri) {
+    const double u = 0.5 * (c_q.xt[t][i] + 1.0), v = 0.5 * (c_q.xt[t][j] + 1.0);
+    z = 1.0 - 1.5 * u;
+    e = 0.5 * BEM_SQ3 * u * (1.0 - 2.0 * v);
+  } else {
+    z = c_q.xt[t][i];
+    e = c_q.xt[t][j];
   }
-  return true;
+}
+// tier of a regular pair, or -1 for the reference's rule (whose points the
+// caller has checked against the lattice plane); none of the tier's points
+// may lie within BEM_FAR_PLANE_TOL of rt's lattice plane either
+__device__ __forceinline__ int far_tier(const bem_far &fr, const bem_el &el, const double rt[3], bool tri) {
+  double kR2;
+  const double r2 = pair_ratio2(fr, el, rt, tri, kR2);
+  if (kR2 > 1.0) return -1;
+  const bool shaped = tri || quad_tier_shape(el);
+  int t;
+  if (!shaped) t = r2 >= 25.0 ? 2 : -1;
+  else t = r2 >= 625.0 && kR2 <= 0.04 ? 4 : r2 >= 64.0 && kR2 <= 0.25 ? 3 : r2 >= 25.0 ? 2 : r2 >= 12.25 ? 1 : r2 >= 9.0 ? 0 : -1;
+  if (t < 0) return -1;
+  // |z(zeta, eta) - c0z| <= |c1z| + |c2z| + |c3z| over the element
+  const double zr = fabs(el.cr[2][1]) + fabs(el.cr[2][2]) + fabs(el.cr[2][3]);
+  if (fabs(el.cr[2][0] - rt[2]) - zr > 2.0 * BEM_FAR_PLANE_TOL) return t;
+  const int n = BEM_TIER_N0 - t;
+  for (int ij = 0; ij < n * n; ++ij) {
+    double z, e, r[3], w[3];
+    tier_point(t, tri, ij / n, ij % n, z, e);
+    bem_rw(el, z, e, r, w);
+    if (fabs(r[2] - rt[2]) < BEM_FAR_PLANE_TOL) return -1;
+  }
+  return t;
 }
 
-// Compacted pair lists written by k_classify: regular pairs (flag 0) from the
-// front of one buffer, far pairs (flag 3) from its back, as p * ne + s.  A
+// Compacted pair lists: k_classify counts the regular pairs (list 0, flag 0)
+// and each tier's pairs (list 1 + t, flag 3 + t) into n[0 .. BEM_NTIER];
+// k_plist_fill writes them, as p * ne + s, list after list into one buffer.  A
 // kernel given a list runs a fixed grid over it; given none, it covers the
 // pair range [pair0, pair0 + npairs) one block per unit group and checks flags.
+#define BEM_NLIST (1 + BEM_NTIER)
 struct bem_plist {
-  const unsigned *e;  // entry u is e[stride * u]
-  const unsigned *n;  // number of entries
-  long long stride;
+  const unsigned *e;  // all lists (null: pair-range mode)
+  const unsigned *n;  // list lengths n[0 .. BEM_NLIST - 1], then BEM_NLIST fill counters
+  int type;           // this kernel's list
 };
 __device__ __forceinline__ long long plist_units(const bem_plist &L, long long npairs) {
-  return L.e ? (long long)*L.n : npairs;
+  return L.e ? (long long)L.n[L.type] : npairs;
 }
-__device__ __forceinline__ long long plist_pair(const bem_plist &L, long long pair0, long long u) {
-  return L.e ? (long long)L.e[L.stride * u] : pair0 + u;
+__device__ __forceinline__ unsigned long long plist_base(const bem_plist &L) {
+  unsigned long long b = 0;
+  if (L.e)
+    for (int t = 0; t < L.type; ++t) b += L.n[t];
+  return b;
 }
+__device__ __forceinline__ long long plist_pair(const bem_plist &L, unsigned long long base, long long pair0, long long u) {
+  return L.e ? (long long)L.e[base + u] : pair0 + u;
+}
+__device__ __forceinline__ int plist_of_flag(uint8_t fl) { return fl == 0 ? 0 : fl >= 3 ? fl - 2 : -1; }
 
 __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, double *__restrict__ rowF,
                                                    int *__restrict__ near_s, int *__restrict__ near_n,
                                                    uint8_t *__restrict__ flag, unsigned *status,
-                                                   unsigned *__restrict__ lst, unsigned *__restrict__ lcnt,
-                                                   unsigned long long lcap) {
+                                                   unsigned *__restrict__ lcnt) {
   const int p = blockIdx.x;
   if (bem_pad_row(D, p)) {
     for (int s = threadIdx.x; s < D.ne; s += blockDim.x) flag[(size_t)p * D.ne + s] = 0;
@@ -233,7 +292,10 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
         if (k < D.near_cap) list[k] = s;
       } else {
         sF += F; sFz += Fz; sFe += Fe;
-        if (fr.on && rzmin >= BEM_FAR_PLANE_TOL && far_pair(fr, el, nd.rt, tri)) fl = 3;
+        if (fr.on && rzmin >= BEM_FAR_PLANE_TOL) {
+          const int tier = far_tier(fr, el, nd.rt, tri);
+          if (tier >= 0) fl = (uint8_t)(3 + tier);
+        }
       }
     }
     flag[(size_t)p * D.ne + s] = fl;
@@ -263,34 +325,49 @@ __global__ void __launch_bounds__(128) k_classify(bem_dom_dev D, bem_far fr, dou
     rowF[3 * p + 1] = red[1][0];
     rowF[3 * p + 2] = red[2][0];
   }
-  if (!lst) return;
-  // this row's regular and far pairs into the lists (flags written above by
-  // this block; order within a row is immaterial: each pair writes its own entries)
-  __shared__ unsigned nreg, nfar, breg, bfar;
-  if (threadIdx.x == 0) nreg = nfar = 0;
+  if (!lcnt) return;
+  // this row's pairs counted into the list lengths (flags written above by this block)
+  __shared__ unsigned nl[BEM_NLIST];
+  if (threadIdx.x < BEM_NLIST) nl[threadIdx.x] = 0;
   __syncthreads();
   for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
-    const uint8_t fl = flag[(size_t)p * D.ne + s];
-    if (fl == 0) atomicAdd(&nreg, 1u);
-    else if (fl == 3) atomicAdd(&nfar, 1u);
+    const int l = plist_of_flag(flag[(size_t)p * D.ne + s]);
+    if (l >= 0) atomicAdd(&nl[l], 1u);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    breg = atomicAdd(lcnt, nreg);
-    bfar = atomicAdd(lcnt + 1, nfar);
-    nreg = nfar = 0;
+  if (threadIdx.x < BEM_NLIST && nl[threadIdx.x]) atomicAdd(lcnt + threadIdx.x, nl[threadIdx.x]);
+}
+
+// One block per row p: the row's pairs into the lists whose lengths k_classify
+// counted (lcnt[0 .. BEM_NLIST - 1]); lcnt[BEM_NLIST + l] hands out the places
+// of list l.  Order within a list is immaterial: each pair writes its own entries.
+__global__ void __launch_bounds__(128) k_plist_fill(bem_dom_dev D, const uint8_t *__restrict__ flag,
+                                                    unsigned *__restrict__ lst, unsigned *__restrict__ lcnt,
+                                                    unsigned long long lcap) {
+  const int p = blockIdx.x;
+  if (bem_pad_row(D, p)) return;  // k_classify counts no pair of a padding row
+  __shared__ unsigned nl[BEM_NLIST];
+  __shared__ unsigned long long at[BEM_NLIST];
+  if (threadIdx.x < BEM_NLIST) nl[threadIdx.x] = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
+    const int l = plist_of_flag(flag[(size_t)p * D.ne + s]);
+    if (l >= 0) atomicAdd(&nl[l], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < BEM_NLIST) {
+    const int l = threadIdx.x;
+    unsigned long long base = 0;
+    for (int m = 0; m < l; ++m) base += lcnt[m];
+    at[l] = base + (nl[l] ? atomicAdd(lcnt + BEM_NLIST + l, nl[l]) : 0u);
+    nl[l] = 0;
   }
   __syncthreads();
   for (int s = threadIdx.x; s < D.ne; s += blockDim.x) {
-    const uint8_t fl = flag[(size_t)p * D.ne + s];
-    const unsigned e = (unsigned)((size_t)p * D.ne + s);
-    if (fl == 0) {
-      const unsigned long long u = (unsigned long long)breg + atomicAdd(&nreg, 1u);
-      if (u < lcap) lst[u] = e;
-    } else if (fl == 3) {
-      const unsigned long long u = (unsigned long long)bfar + atomicAdd(&nfar, 1u);
-      if (u < lcap) lst[lcap - 1 - u] = e;
-    }
+    const int l = plist_of_flag(flag[(size_t)p * D.ne + s]);
+    if (l < 0) continue;
+    const unsigned long long u = at[l] + atomicAdd(&nl[l], 1u);
+    if (u < lcap) lst[u] = (unsigned)((size_t)p * D.ne + s);
   }
 }
 
@@ -312,10 +389,11 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
   __syncthreads();
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long nu = plist_units(L, npairs);
+  const unsigned long long lb = plist_base(L);
   unsigned long long nterm = 0, npt = 0;
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
     const bool valid = u0 + lp < nu;
-    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+    const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
     const int p = (int)(pair / D.ne);
     const int s = (int)(pair % D.ne);
     // triangle sources are k_q0_regular_tri's; padded rows keep their zeros
@@ -359,7 +437,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
     if (threadIdx.x < 32) {
       const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
       if (u0 + q2 < nu) {
-        const long long pr = plist_pair(L, pair0, u0 + q2);
+        const long long pr = plist_pair(L, lb, pair0, u0 + q2);
         const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
         if (flag[(size_t)pp * D.ne + ss] == 0 && !bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
           double sum = 0.0;
@@ -390,10 +468,11 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   __syncthreads();
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long nu = plist_units(L, npairs);
+  const unsigned long long lb = plist_base(L);
   unsigned long long nterm = 0, npt = 0;
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
     const bool valid = u0 + lp < nu;
-    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+    const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
     const int p = (int)(pair / D.ne);
     const int s = (int)(pair % D.ne);
     const bool work = valid && flag[(size_t)p * D.ne + s] == 0 && bem_is_tri(D, abs(D.sid[s]) - 1) && !bem_pad_row(D, p);
@@ -448,7 +527,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
     if (threadIdx.x < 32) {
       const int q2 = threadIdx.x >> 4, c = threadIdx.x & 15;
       if (u0 + q2 < nu) {
-        const long long pr = plist_pair(L, pair0, u0 + q2);
+        const long long pr = plist_pair(L, lb, pair0, u0 + q2);
         const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
         if (flag[(size_t)pp * D.ne + ss] == 0 && bem_is_tri(D, abs(D.sid[ss]) - 1) && !bem_pad_row(D, pp)) {
           double sum = 0.0;
@@ -465,57 +544,65 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular_tri(bem_dom_
   count_work(terms + 0, nterm, npt);
 }
 
-// Far pairs (flag 3, far_pair): the 8 x 8 Gauss rule on a quad; on a
-// triangle the 8 x 8 collapsed (Duffy) rule over the whole reference triangle,
-// (z, e) = (1 - 3u/2, sqrt3/2 u (1 - 2v)) for (u, v) in [0, 1]^2, weight
-// u w_u w_v (the weights total 1/2, as the 3-part rule's do).  One thread per
-// point, 4 pairs per 256-thread block, contributions accumulated in the
-// thread's shared-memory column; otherwise as k_q0_regular / k_q0_regular_tri.
+// Regular pairs on tier t's shorter rule (flag 3 + t, far_tier): NF x NF
+// points (NF = BEM_TIER_N0 - t), Gauss on a quad, collapsed over a triangle
+// (tier_point; the weights u w_u w_v total 1/2, as the 3-part rule's do).  One
+// thread per point, PB = FP_THREADS / NF^2 pairs per block, contributions
+// accumulated in the thread's shared-memory column; otherwise as k_q0_regular /
+// k_q0_regular_tri.
 #define FP_THREADS 256
-__device__ __forceinline__ void far_point(bool tri, int i, int j, double &z, double &e) {
-  if (tri) {
-    const double u = 0.5 * (c_q.xf[i] + 1.0), v = 0.5 * (c_q.xf[j] + 1.0);
-    z = 1.0 - 1.5 * u;
-    e = 0.5 * BEM_SQ3 * u * (1.0 - 2.0 * v);
-  } else {
-    z = c_q.xf[i];
-    e = c_q.xf[j];
-  }
-}
 #ifndef FP_MINB
 #define FP_MINB 2  // two blocks (16 warps) per SM: caps registers at 128
 #endif
+template <int NF>
+struct far_shape {
+  // TH threads hold points; the block has TB (whole warps), the rest idle
+  static constexpr int NP = NF * NF, PB = FP_THREADS / NP, TH = PB * NP, TB = (TH + 31) / 32 * 32,
+                       T = BEM_TIER_N0 - NF;
+};
+template <int NF>
 __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
                                                         const uint8_t *__restrict__ flag, double *__restrict__ G,
                                                         double *__restrict__ H, unsigned *status,
                                                         unsigned long long *terms, long long pair0, long long npairs,
                                                         bem_plist L) {
-  __shared__ double acc[16][FP_THREADS + 1];
+  using F = far_shape<NF>;
+  constexpr uint8_t FL = (uint8_t)(3 + F::T);
+  __shared__ double acc[16][F::TB + 1];
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
+  const long long nu = plist_units(L, npairs);
+  const unsigned long long lb = plist_base(L);
+  if (!L.e) {
+    // pair-range mode: a block none of whose pairs is on this tier stops
+    // before staging the table
+    bool mine = false;
+    for (long long u0 = (long long)F::PB * blockIdx.x; u0 < nu; u0 += (long long)F::PB * gridDim.x)
+      if (threadIdx.x < F::PB && u0 + threadIdx.x < nu) mine |= flag[pair0 + u0 + threadIdx.x] == FL;
+    if (!__syncthreads_or(mine)) return;
+  }
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
-  const int lp = threadIdx.x >> 6, pt = threadIdx.x & 63;
-  const long long nu = plist_units(L, npairs);
+  const int lp = threadIdx.x / F::NP, pt = threadIdx.x % F::NP;
   unsigned long long nterm = 0, npt = 0;
-  for (long long u0 = 4LL * blockIdx.x; u0 < nu; u0 += 4LL * gridDim.x) {
-    const bool valid = u0 + lp < nu;
-    const long long pair = valid ? plist_pair(L, pair0, u0 + lp) : 0;
+  for (long long u0 = (long long)F::PB * blockIdx.x; u0 < nu; u0 += (long long)F::PB * gridDim.x) {
+    const bool valid = threadIdx.x < F::TH && u0 + lp < nu;
+    const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
     const int p = (int)(pair / D.ne);
     const int s = (int)(pair % D.ne);
-    const bool work = valid && flag[(size_t)p * D.ne + s] == 3;
+    const bool work = valid && flag[(size_t)p * D.ne + s] == FL;
 #pragma unroll
     for (int c = 0; c < 16; ++c) acc[c][threadIdx.x] = 0.0;
     if (work) {
       const int se = abs(D.sid[s]) - 1, te = abs(D.sid[p >> 2]) - 1;
       const bool tri = bem_is_tri(D, se);
-      const int i = pt >> 3, j = pt & 7;
+      const int i = pt / NF, j = pt % NF;
       unsigned st = 0;
       {
         double z, e, vR[3], vW[3];
         {
           bem_el el;
           bem_load_el(D.cr, D.cw, se, el);
-          far_point(tri, i, j, z, e);
+          tier_point(F::T, tri, i, j, z, e);
           bem_rw(el, z, e, vR, vW);
         }
 #pragma unroll
@@ -526,12 +613,12 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
         nterm += rc > 0 ? (unsigned long long)rc : 0ULL;
         ++npt;
         // re-derived after the call rather than kept live across it
-        double wt = c_q.wf[i] * c_q.wf[j];
-        far_point(tri, i, j, z, e);
+        double wt = c_q.wt[F::T][i] * c_q.wt[F::T][j];
+        tier_point(F::T, tri, i, j, z, e);
         if (tri) {
 #pragma unroll
           for (int d = 0; d < 3; ++d) vW[d] = __ldg(D.cw + (size_t)se * 9 + d * 3);
-          wt *= 0.125 * (c_q.xf[i] + 1.0);  // u w_u w_v with u = (x + 1) / 2, w_u = w / 2
+          wt *= 0.125 * (c_q.xt[F::T][i] + 1.0);  // u w_u w_v with u = (x + 1) / 2, w_u = w / 2
         } else {
           bem_el el;
           bem_load_el(D.cr, D.cw, se, el);
@@ -555,14 +642,14 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
       set_status(status, st);
     }
     __syncthreads();
-    if (threadIdx.x < 64) {
-      const int q4 = threadIdx.x >> 4, c = threadIdx.x & 15;
-      if (u0 + q4 < nu) {
-        const long long pr = plist_pair(L, pair0, u0 + q4);
+    if (threadIdx.x < 16 * F::PB) {
+      const int qq = threadIdx.x >> 4, c = threadIdx.x & 15;
+      if (u0 + qq < nu) {
+        const long long pr = plist_pair(L, lb, pair0, u0 + qq);
         const int pp = (int)(pr / D.ne), ss = (int)(pr % D.ne);
-        if (flag[(size_t)pp * D.ne + ss] == 3) {
+        if (flag[(size_t)pp * D.ne + ss] == FL) {
           double sum = 0.0;
-          for (int k = 0; k < 64; ++k) sum += acc[c][q4 * 64 + k];
+          for (int k = 0; k < F::NP; ++k) sum += acc[c][qq * F::NP + k];
           const size_t N = (size_t)D.ne * 4;
           double *dst = c < 8 ? G : H;
           const int a = (c & 7) >> 1, part = c & 1;
@@ -1720,6 +1807,42 @@ extern "C" int bem_launch_wtab(double k, double ve, double *out, cudaStream_t st
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
+// n-point Gauss-Legendre rule on [-1, 1], nodes ascending: Newton's method on
+// P_n (three-term recurrence) from the Chebyshev-like guess cos(pi (i + 3/4) /
+// (n + 1/2)), weights 2 / ((1 - x^2) P_n'(x)^2); symmetric pairs are set from
+// one root so that the rule is exactly symmetric.
+static void gauss_legendre(int n, double *x, double *w) {
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = cos(CUDART_PI * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int m = 2; m <= n; ++m) {
+        const double p2 = ((2.0 * m - 1.0) * z * p1 - (m - 1.0) * p0) / m;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (fabs(dz) < 1e-17) break;
+    }
+    // derivative at the converged root
+    {
+      double p0 = 1.0, p1 = z;
+      for (int m = 2; m <= n; ++m) {
+        const double p2 = ((2.0 * m - 1.0) * z * p1 - (m - 1.0) * p0) / m;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+    }
+    const double wi = 2.0 / ((1.0 - z * z) * dp * dp);
+    x[i] = -z; w[i] = wi;           // z > 0: the i-th largest root
+    x[n - 1 - i] = z; w[n - 1 - i] = wi;
+  }
+  if (n & 1) x[n / 2] = 0.0;
+}
+
 extern "C" int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh) {
   bem_quad qq;
   for (int i = 0; i < BEM_GLN; ++i) { qq.xl[i] = xl[i]; qq.wl[i] = wl[i]; }
@@ -1729,9 +1852,19 @@ extern "C" int bem_set_constants(const double *xl, const double *wl, const doubl
                         0.9602898564975362316836};
   const double w8[4] = {0.3626837833783619829652, 0.3137066458778872873380, 0.2223810344533744705444,
                         0.1012285362903762591525};
-  for (int i = 0; i < 4; ++i) {
-    qq.xf[3 - i] = -x8[i]; qq.wf[3 - i] = w8[i];
-    qq.xf[4 + i] = x8[i]; qq.wf[4 + i] = w8[i];
+  // the tiers' n-point rules, nodes ascending: 8 points from the table above,
+  // the others by gauss_legendre
+  for (int t = 0; t < BEM_NTIER; ++t) {
+    const int n = BEM_TIER_N0 - t;
+    for (int i = 0; i < BEM_TIER_N0; ++i) qq.xt[t][i] = qq.wt[t][i] = 0.0;
+    if (n == 8) {
+      for (int i = 0; i < 4; ++i) {
+        qq.xt[t][3 - i] = -x8[i]; qq.wt[t][3 - i] = w8[i];
+        qq.xt[t][4 + i] = x8[i]; qq.wt[t][4 + i] = w8[i];
+      }
+    } else {
+      gauss_legendre(n, qq.xt[t], qq.wt[t]);
+    }
   }
   const double zt[4] = {-BEM_P44, BEM_P44, BEM_P44, -BEM_P44}, et[4] = {-BEM_P44, -BEM_P44, BEM_P44, BEM_P44};
   for (int i = 0; i < 4; ++i) { qq.zt[i] = zt[i]; qq.et[i] = et[i]; }
@@ -1786,11 +1919,36 @@ static int near_grid_y(const bem_dom_dev *D) { return D->near_cap < 32 ? D->near
 static int q0_smem_attrs() {
   const int b = (int)BEM_WT_SMEM;
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (cudaFuncSetAttribute(k_q0_regular, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far, a, b) != cudaSuccess ||
+  if (cudaFuncSetAttribute(k_q0_far<10>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<9>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<8>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<7>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<6>, a, b) != cudaSuccess)
+    return -1;
+  if (cudaFuncSetAttribute(k_q0_regular, a, b) != cudaSuccess ||
       cudaFuncSetAttribute(k_q0_regular_tri, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_near, a, b) != cudaSuccess ||
       cudaFuncSetAttribute(k_q0_self, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self_tri, a, b) != cudaSuccess)
     return -1;
   return 0;
+}
+
+// tier NF's kernel over its list (L.e set: grid_list blocks striding over it)
+// or over the pair range [p0, p0 + np)
+template <int NF>
+static void launch_far(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
+                       long long np, bem_plist L, unsigned grid_list, cudaStream_t st) {
+  using F = far_shape<NF>;
+  L.type = 1 + F::T;
+  const unsigned grid = L.e ? grid_list : (unsigned)((np + F::PB - 1) / F::PB);
+  if (grid == 0) return;
+  k_q0_far<NF><<<grid, F::TB, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np, L);
+  bem_count_launches(1);
+}
+static void launch_far_tiers(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
+                             long long np, const bem_plist &L, unsigned grid_list, cudaStream_t st) {
+  launch_far<10>(D, q, S, G, H, p0, np, L, grid_list, st);
+  launch_far<9>(D, q, S, G, H, p0, np, L, grid_list, st);
+  launch_far<8>(D, q, S, G, H, p0, np, L, grid_list, st);
+  launch_far<7>(D, q, S, G, H, p0, np, L, grid_list, st);
+  launch_far<6>(D, q, S, G, H, p0, np, L, grid_list, st);
 }
 
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
@@ -1815,11 +1973,15 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   // compacted pair lists for the periodic domain when the scratch holds them
   const bool lists = periodic && S->plist && S->pcount && (unsigned long long)npairs <= S->pcap &&
                      npairs <= 0xffffffffLL;
-  if (lists && cudaMemsetAsync(S->pcount, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return -1;
+  if (lists && cudaMemsetAsync(S->pcount, 0, 2 * BEM_NLIST * sizeof(unsigned), st) != cudaSuccess) return -1;
   if (ev) cudaEventRecord(ev[0], st);
   k_classify<<<N, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
-                                lists ? S->plist : nullptr, S->pcount, S->pcap);
+                                lists ? S->pcount : nullptr);
   bem_count_launches(1);
+  if (lists) {
+    k_plist_fill<<<N, 128, 0, st>>>(*D, S->flag, S->plist, S->pcount, S->pcap);
+    bem_count_launches(1);
+  }
   if (ev) cudaEventRecord(ev[1], st);
   if (periodic) {
     if (lists) {
@@ -1829,15 +1991,10 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
           cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
         return -1;
       const unsigned grid = RP_MINB * (unsigned)nsm, grid_far = FP_MINB * (unsigned)nsm;
-      const bem_plist Lreg = {S->plist, S->pcount, 1};
-      const bem_plist Lfar = {S->plist + (S->pcap - 1), S->pcount + 1, -1};
+      const bem_plist Lreg = {S->plist, S->pcount, 0};
       k_q0_regular<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
       bem_count_launches(1);
-      if (D->far_rule) {
-        k_q0_far<<<grid_far, FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs,
-                                                            Lfar);
-        bem_count_launches(1);
-      }
+      if (D->far_rule) launch_far_tiers(D, q, S, G, H, 0, npairs, Lreg, grid_far, st);
       if (D->has_tri) {
         k_q0_regular_tri<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
         bem_count_launches(1);
@@ -1850,11 +2007,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
         k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                       L0);
         bem_count_launches(1);
-        if (D->far_rule) {
-          k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
-                                                                    L0);
-          bem_count_launches(1);
-        }
+        if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);
         if (D->has_tri) {
           k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                             p0, np, L0);
@@ -1915,11 +2068,7 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
       k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
                                                                     L0);
       bem_count_launches(1);
-      if (D->far_rule) {
-        k_q0_far<<<(unsigned)((np + 3) / 4), FP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
-                                                                  L0);
-        bem_count_launches(1);
-      }
+      if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);
       if (D->has_tri) {
         k_q0_regular_tri<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                           p0, np, L0);
@@ -1961,7 +2110,7 @@ extern "C" int bem_launch_fs_deriv(const bem_dom_dev *D, double k, bem_scratch *
 extern "C" int bem_launch_classify(const bem_dom_dev *D, const bem_qp *q, int periodic, bem_scratch *S, cudaStream_t st) {
   if (D->ne <= 0) return 0;
   k_classify<<<D->ne * 4, 128, 0, st>>>(*D, far_params(D, q, periodic), S->rowF, S->near_s, S->near_n, S->flag, S->status,
-                                        nullptr, nullptr, 0);
+                                        nullptr);
   bem_count_launches(1);
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }

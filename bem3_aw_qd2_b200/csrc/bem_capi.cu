@@ -51,7 +51,7 @@ struct bemgpu_ctx {
   double *stab = nullptr;  // evanescent spectral order table (at eta_run)
   double zspan = 0.0;      // height of the mesh (z extent of all elements)
   double pw[16] = {};      // incident plane wave (bemgpu_problem.pw)
-  int far_rule = 1;        // 8 x 8 rule for far quad pairs of the periodic domain (bemgpu_set_far_rule)
+  int far_rule = 1;        // shorter rules for regular pairs of the periodic domain (bemgpu_set_far_rule)
   double eta_scale = 0.0;  // Ewald parameter off the lattice plane = eta0 x eta_scale; 0: by rule per problem
   double *pw_d = nullptr;
   // 9-point targets on the domain-0 elements for the type-1 force
@@ -499,7 +499,7 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
   const size_t npair = (size_t)4 * c->dom_ne[0] * c->dom_ne[0];
   if (npair > 0 && npair <= 0xffffffffull) {
     CK(falloc(c, &c->scr.plist, npair), "pair lists");
-    CK(falloc(c, &c->scr.pcount, 2), "pair lists");
+    CK(falloc(c, &c->scr.pcount, 16), "pair lists");
     c->scr.pcap = npair;
   } else {
     c->scr.pcap = 0;
@@ -561,6 +561,17 @@ extern "C" int bemgpu_load(bemgpu_ctx *c, const bemgpu_problem *pr) {
 extern "C" int bemgpu_set_far_rule(bemgpu_ctx *c, int on) {
   c->far_rule = on ? 1 : 0;
   c->factored = false;
+  return 0;
+}
+
+extern "C" int bemgpu_rule_pairs(bemgpu_ctx *c, unsigned long long counts[6]) {
+  if (!c || !counts) return -2;
+  if (!c->scr.pcount || c->scr.pcap == 0) return -2;
+  unsigned n[6];
+  if (cudaMemcpyAsync(n, c->scr.pcount, sizeof(n), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return fail(c, "rule_pairs", cudaGetLastError());
+  for (int i = 0; i < 6; ++i) counts[i] = n[i];
   return 0;
 }
 

@@ -15,10 +15,14 @@
 #define BEM_P44 0.5773502691896257645091     // 1/sqrt(3)
 #define BEM_MAXNEAR 256        // most near-singular sources a collocation node can hold (bem_dom_dev.near_cap)
 
-#define BEM_GFN 8              // far-pair rule (k_q0_far)
+// Shorter rules of the periodic domain's regular pairs (k_q0_far): tier t is
+// the (BEM_TIER_N0 - t)-point Gauss-Legendre rule, t = 0 .. BEM_NTIER - 1
+// (10, 9, 8, 7 and 6 points)
+#define BEM_NTIER 5
+#define BEM_TIER_N0 10
 struct bem_quad {
   double xl[BEM_GLN], wl[BEM_GLN];
-  double xf[BEM_GFN], wf[BEM_GFN];
+  double xt[BEM_NTIER][BEM_TIER_N0], wt[BEM_NTIER][BEM_TIER_N0];
   double xh[BEM_GHN], wh[BEM_GHN];
   double zt[4], et[4];        // collocation node parameters (zt_44, et_44)
   double z9[9], e9[9], w9[9]; // 9-point rule (zt_49, et_49, wt_49)

@@ -25,9 +25,9 @@ struct bem_scratch {
   int *near_n;      // [N]
   double *nearF;    // [N][near_cap][3]
   double *selfF;    // [N][3]
-  uint8_t *flag;    // [N][ne] 0 regular, 1 near-singular, 2 self, 3 far (regular, shorter rule)
-  unsigned *plist;  // [pcap] periodic-domain pair lists p * ne + s: regular from the front, far from the back (optional)
-  unsigned *pcount; // [2] list lengths
+  uint8_t *flag;    // [N][ne] 0 regular, 1 near-singular, 2 self, 3 + t regular on shorter-rule tier t
+  unsigned *plist;  // [pcap] periodic-domain pair lists p * ne + s: regular, then tier 0, 1, ... (optional)
+  unsigned *pcount; // [16] list lengths, then the fill counters
   unsigned long long pcap;
   unsigned *status; // BEM_ST_* bits
   unsigned long long *terms;  // [6] lattice terms of regular / near / self pairs, then point counts

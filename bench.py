@@ -50,13 +50,18 @@ C_TERM_FLOPS = 280.0
 # (measured_fp64_peak), as the bf16 and HBM peaks of this pool are measured
 FP64_NOMINAL_TFLOPS = 37.2
 # The regular-pair kernels' hardware readings from one ncu capture of a
-# timed-configuration launch on the 216-quad workload (profiles/
-# k_q0_regular_far_sphere216.md, command given there): FP64 pipe busy fraction
-# (sm__pipe_fp64_cycles_active over active cycles) and DRAM bytes read +
-# written per launch.  Reported for that workload only.
+# warm-up assembly of the timed configuration on the 216-quad workload
+# (profiles/k_q0_regular_far_sphere216.md, command given there): FP64 pipe busy
+# fraction (sm__pipe_fp64_cycles_active over active cycles) and DRAM bytes read +
+# written per launch, for k_q0_regular and each shorter-rule tier's k_q0_far<n>.
+# Reported for that workload only.
 NCU_WORKLOAD = "sphere216"
-NCU_REGULAR = {"k_q0_regular": {"fp64_pipe": 0.4304, "dram_bytes": 588288 + 28716032},
-               "k_q0_far": {"fp64_pipe": 0.4765, "dram_bytes": 1411328 + 1803520}}
+NCU_REGULAR = {"k_q0_regular": {"fp64_pipe": 0.4343, "dram_bytes": 434432 + 7126272},
+               "k_q0_far<10>": {"fp64_pipe": 0.4598, "dram_bytes": 414720 + 20992},
+               "k_q0_far<9>": {"fp64_pipe": 0.5040, "dram_bytes": 960512 + 305408},
+               "k_q0_far<8>": {"fp64_pipe": 0.5010, "dram_bytes": 817152 + 1160192},
+               "k_q0_far<7>": {"fp64_pipe": 0.4631, "dram_bytes": 1312000 + 1236480},
+               "k_q0_far<6>": {"fp64_pipe": 0.0, "dram_bytes": 85760 + 0}}
 
 
 def measured_fp64_peak():
@@ -503,18 +508,18 @@ def run_stream(args, rank, world):
 
 def roofline_record(achieved, fp64_peak, terms_reg, cnt, workload, out_bytes):
     """The dominant kernels' roofline: periodic regular-pair assembly
-    (k_q0_regular on near-ish pairs, k_q0_far on far ones, one phase), FP64
+    (k_q0_regular on the reference's rule, k_q0_far<n> on the shorter rules'
+    tiers, one phase), FP64
     work = lattice terms counted by the kernels x the frozen per-term count,
     over the phase's CUDA-event time; beside it the FP64 pipe fraction and DRAM
     traffic ncu read on the same kernels."""
-    reg, far = NCU_REGULAR["k_q0_regular"], NCU_REGULAR["k_q0_far"]
-    traffic, pipe = None, {"k_q0_regular": None, "k_q0_far": None}
+    traffic, pipe = None, {k: None for k in NCU_REGULAR}
     if workload == NCU_WORKLOAD:
-        traffic = reg["dram_bytes"] + far["dram_bytes"]
-        pipe = {"k_q0_regular": reg["fp64_pipe"], "k_q0_far": far["fp64_pipe"]}
-    return {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far (regular pairs)", "achieved": achieved,
+        traffic = sum(v["dram_bytes"] for v in NCU_REGULAR.values())
+        pipe = {k: v["fp64_pipe"] for k, v in NCU_REGULAR.items()}
+    return {"bound": "fp64", "kernel": "k_q0_regular + k_q0_far<10..6> (regular pairs)", "achieved": achieved,
             "peak": fp64_peak, "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
-            "traffic": traffic, "traffic_unit": "bytes per launch pair (ncu dram__bytes_read.sum + write.sum)",
+            "traffic": traffic, "traffic_unit": "bytes per assembly over the phase's 6 launches (ncu dram__bytes_read.sum + write.sum)",
             "algorithmic_bytes": out_bytes,
             "algorithmic_bytes_what": "G and H of the periodic domain written (the kernels' only DRAM output; "
                                       "inputs are L2-resident)",
@@ -874,6 +879,8 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "precision": "plain FP64 (assembly and LU)",
                    "ewald_scale": ewald_scale, "interior_derivative_rows": "kept" if keep_dgh else "recomputed in blocks",
+                   "regular_pairs_by_rule": dict(zip(["12x12 (reference)", "10x10", "9x9", "8x8", "7x7", "6x6"],
+                                                     case.rule_pairs() or [])),
                    **workload_desc(args.workload)},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

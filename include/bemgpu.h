@@ -89,16 +89,26 @@ int bemgpu_load(bemgpu_ctx *ctx, const bemgpu_problem *prob);
 #define BEMGPU_EWALD_RULE 0.0
 int bemgpu_set_ewald_scale(bemgpu_ctx *ctx, double scale);
 
-/* Quadrature of far regular pairs of the periodic domain (no counterpart in
+/* Quadrature of the regular pairs of the periodic domain (no counterpart in
  * the reference, which uses its 12 x 12 Gauss rule for every regular pair,
- * on each of 3 parts of a triangle): on = 1 (the default) uses an 8 x 8 rule
- * (Gauss on a quad, collapsed over a whole triangle) where the source
- * element's centre is at least 5 circumradii R from the nearest lattice image
- * of the collocation node and k 2R <= 2, which reproduces the reference's
- * integrals to below 1e-13 of the entry with 2.25 (quads) or 6.75 (triangles)
+ * on each of 3 parts of a triangle): on = 1 (the default) uses a shorter
+ * n x n rule (Gauss on a quad, collapsed over a whole triangle) where the
+ * source element's centre is at least d circumradii R from the nearest
+ * lattice image of the collocation node:
+ *     n = 10 from d = 3, 9 from 3.5, 8 from 5 (all with k R <= 1),
+ *     7 from 8 (k R <= 0.5), 6 from 25 (k R <= 0.2),
+ * the 10, 9, 7 and 6-point rules only on quads whose twist along the normal
+ * is at most a tenth of the shorter half-side and whose half-sides are within
+ * 3x (every triangle).  Each reproduces the reference's integrals to about
+ * 1e-13 of the pair's largest entry with up to 4 (quads) or 12 (triangles)
  * times fewer Green's-function values; on = 0 keeps the reference's rules
  * everywhere.  Applies from the next assembly. */
 int bemgpu_set_far_rule(bemgpu_ctx *ctx, int on);
+/* Regular pairs of the periodic domain by rule in the last assembly:
+ * counts[0] on the reference's 12 x 12 rule, counts[1 .. 5] on the 10, 9, 8,
+ * 7 and 6-point rules.  Returns 0, or -2 when the assembly kept no pair
+ * lists (no counts; domains of more than 32768 elements). */
+int bemgpu_rule_pairs(bemgpu_ctx *ctx, unsigned long long counts[6]);
 
 /* Autotuner of the Ewald parameter for the loaded problem: times the periodic
  * regular-pair kernel on an eighth of the pairs for the rule's scale and three

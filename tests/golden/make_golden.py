@@ -162,6 +162,51 @@ def make_far_pairs(name="sphere216", out_name="far216.npz", n_pairs=400, n_near=
     np.savez_compressed(os.path.join(OUT, out_name), idx=idx, far=np.array([p[3] for p in picks]), G=G, H=H)
 
 
+def make_tier_pairs(name="sphere1536", out_name="tiers1536.npz", per_band=40):
+    """Reference coefficients G_i, H_i (q0_dcoef_bd_node_t2_cc) of regular
+    pairs spread over the distance bands of the device's shorter rules:
+    (distance from the collocation node's nearest lattice image to the source
+    element's centre) / (its circumradius) in 2.2-2.9 (the reference's rule),
+    3.1-3.4 (10 points), 3.6-4.8 (9), 5.2-7.8 (8), 8.3-24 (7) and above 26 (6
+    points where k R <= 0.2), per_band pairs each.  The node is the bilinear
+    map of (+-1/sqrt3, +-1/sqrt3) on its element, as the reference places it."""
+    tmp = tempfile.mkdtemp(prefix="golden_")
+    cfg = meshgen.CONFIGS[name]
+    files = meshgen.write_inputs(tmp, **cfg)
+    case = refwrap.RefCase(*files)
+    nodes, el = meshgen.cube_sphere(cfg["n"], cfg["semi_axes"])
+    P = nodes[el]
+    cen = P.mean(axis=1)
+    rad = np.max(np.linalg.norm(P - cen[:, None, :], axis=2), axis=1)
+    a = 1.0 / np.sqrt(3.0)
+    zt, et = (-a, a, a, -a), (-a, -a, a, a)
+    d1 = np.array(list(cfg["lattice"][0]) + [0.0])
+    d2 = np.array(list(cfg["lattice"][1]) + [0.0])
+    bands = [(2.2, 2.9), (3.1, 3.4), (3.6, 4.8), (5.2, 7.8), (8.3, 24.0), (26.0, 1e9)]
+    rng = np.random.default_rng(20241209)
+    ne = len(el)
+    picks, count = [], [0] * len(bands)
+    while min(count) < per_band:
+        t, s, tn = int(rng.integers(ne)), int(rng.integers(ne)), int(rng.integers(4))
+        if t == s:
+            continue
+        z, e = zt[tn], et[tn]
+        N = np.array([(1 - z) * (1 - e), (1 + z) * (1 - e), (1 + z) * (1 + e), (1 - z) * (1 + e)]) / 4
+        rt = N @ P[t]
+        ratio = min(np.linalg.norm(rt - cen[s] + i * d1 + j * d2) for i in (-1, 0, 1) for j in (-1, 0, 1)) / rad[s]
+        for b, (lo, hi) in enumerate(bands):
+            if lo <= ratio <= hi and count[b] < per_band:
+                count[b] += 1
+                picks.append((t + 1, tn, s + 1, b))
+    G = np.zeros((len(picks), 4), np.complex128)
+    H = np.zeros((len(picks), 4), np.complex128)
+    for i, (t, tn, s, _) in enumerate(picks):
+        cc = case.pair(0, t, tn, s)[0]
+        G[i], H[i] = cc[:4], cc[4:8]
+    idx = np.array([p[:3] for p in picks], np.int32)
+    np.savez_compressed(os.path.join(OUT, out_name), idx=idx, band=np.array([p[3] for p in picks], np.int8), G=G, H=H)
+
+
 def make_near_pairs(n_pairs=240):
     """Reference coefficients of node-element pairs of the 216-quad sphere at
     1 to 3 element circumradii (centre distance from the node's nearest
@@ -345,6 +390,10 @@ def main():
         make_far_pairs()
         make_far_pairs("tri320", "far_tri320.npz", 300, 60)
         print("far216.npz, far_tri320.npz written to", OUT)
+        return
+    if sys.argv[1:] == ["tiers"]:
+        make_tier_pairs()
+        print("tiers1536.npz written to", OUT)
         return
     if sys.argv[1:] == ["near"]:
         make_near_pairs()

@@ -1,12 +1,17 @@
-"""Error model of the far-pair rule (no GPU): the device integrates far
-regular pairs of the periodic domain (element centre at least 5 circumradii
-R from the nearest lattice image of the node, k 2R <= 2) with an 8 x 8 rule
-instead of the reference's 12 x 12 per quad or triangle part.  Here the
+"""Error model of the shorter rules for regular pairs (no GPU): the device
+integrates a regular pair of the periodic domain whose element centre is at
+least d_t circumradii R from the nearest lattice image of the node, with
+k R <= kR_t, with an n_t x n_t rule instead of the reference's 12 x 12 per
+quad or triangle part (TIERS below: 10 points from 3 R, 9 from 3.5 R, 8 from
+5 R, 7 from 8 R when k R <= 0.5, 6 from 25 R when k R <= 0.2).  Here the
 integrand exp(ikr)/r and its gradient, times an interpolation function, is
-integrated over a curved quad and a flat triangle with both rules and with a
-converged 40-point rule, for targets at 5 R in every direction: the 8 x 8
-rule matches the converged integral (and so the reference's 12 x 12, itself
-converged there) to 1e-13 of the entry."""
+integrated over a curved quad and a flat triangle with each rule and with a
+converged 40-point rule, for targets in every direction: each tier matches the
+converged integral (and so the reference's 12 x 12, itself converged there) to
+1e-13 of the entry.  On bilinear quads with the surface Jacobian the bar holds
+for elements inside the device's shape guard (twist along the normal at most a
+tenth of the shorter half-side, half-sides within 3x) to 5e-13 of the pair's
+largest entry, and fails outside it."""
 import numpy as np
 
 K = 2 * np.pi
@@ -95,3 +100,74 @@ def test_closer_pairs_need_the_reference_rule():
         ref = quad_integrals(40, tgt, h, 0.2)
         worst = max(worst, np.max(np.abs(quad_integrals(8, tgt, h, 0.2) - ref) / np.abs(ref)))
     assert worst > 1e-12
+
+
+# (points, distance in circumradii, largest k R) of each tier
+TIERS = [(10, 3.0, 1.0), (9, 3.5, 1.0), (8, 5.0, 1.0), (7, 8.0, 0.5), (6, 25.0, 0.2)]
+
+
+def test_tier_rules_error():
+    for n, dR, kmax in TIERS:
+        worst = 0.0
+        for kR in [x for x in (0.05, 0.2, 0.5, 1.0) if x <= kmax]:
+            h = kR / (K * np.sqrt(2))
+            for tgt in _targets(dR * h * np.sqrt(2)):
+                ref = quad_integrals(40, tgt, h, 0.2)
+                worst = max(worst, np.max(np.abs(quad_integrals(n, tgt, h, 0.2) - ref) / np.abs(ref)))
+            R = kR / K
+            for tgt in _targets(dR * R):
+                ref = tri_parts(40, tgt, R)
+                worst = max(worst, np.max(np.abs(tri_collapsed(n, tgt, R) - ref) / np.abs(ref)))
+        assert worst < 1e-13, (n, worst)
+
+
+def _bilinear(n, C, tgt):
+    """G |W| N_i and (grad G . W) N_i over the bilinear quad c0 + c1 z + c2 e + c3 z e."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    Z, E = np.meshgrid(x, x, indexing="ij")
+    W2 = np.outer(w, w)
+    r = C[0] + C[1] * Z[..., None] + C[2] * E[..., None] + C[3] * (Z * E)[..., None]
+    Wv = np.cross(C[1] + C[3] * E[..., None], C[2] + C[3] * Z[..., None])
+    v = r - tgt
+    R = np.linalg.norm(v, axis=-1)
+    g = np.exp(1j * K * R) / R
+    h = g * (1j * K - 1 / R) / R * np.einsum("...d,...d->...", v, Wv)
+    aW = np.linalg.norm(Wv, axis=-1)
+    Ns = [0.25 * (1 + a * Z) * (1 + b * E) for a, b in ((-1, -1), (1, -1), (1, 1), (-1, 1))]
+    return np.array([np.sum(W2 * g * aW * N) for N in Ns] + [np.sum(W2 * h * N) for N in Ns])
+
+
+def _quad(kR, aspect, twist, rng):
+    P = np.array([[-1, -1 / aspect, 0], [1, -1 / aspect, 0], [1, 1 / aspect, 0], [-1, 1 / aspect, 0]], float)
+    P[:, 2] = twist * np.array([1, -1, 1, -1]) / aspect
+    P[:, :2] += 0.1 * rng.standard_normal((4, 2)) / aspect
+    C = [0.25 * (P[0] + P[1] + P[2] + P[3]), 0.25 * (-P[0] + P[1] + P[2] - P[3]),
+         0.25 * (-P[0] - P[1] + P[2] + P[3]), 0.25 * (P[0] - P[1] + P[2] - P[3])]
+    R = np.linalg.norm(P - C[0], axis=1).max()
+    return [c * (kR / K) / R for c in C], kR / K
+
+
+def _pair_max_error(n, dR, kR, aspect, twist, seed, trials=3, dirs=12):
+    rng = np.random.default_rng(seed)
+    worst = 0.0
+    for _ in range(trials):
+        C, R = _quad(kR, aspect, twist, rng)
+        for _ in range(dirs):
+            u = rng.standard_normal(3)
+            tgt = C[0] + dR * R * u / np.linalg.norm(u)
+            ref, got = _bilinear(40, C, tgt), _bilinear(n, C, tgt)
+            scale = np.r_[np.full(4, np.abs(ref[:4]).max()), np.full(4, np.abs(ref[4:]).max())]
+            worst = max(worst, np.max(np.abs(got - ref) / scale))
+    return worst
+
+
+def test_tier_rules_on_guarded_bilinear_quads():
+    """Twisted (|c3 . n| up to 1/10 of the shorter half-side) and long (3:1) quads with the Jacobian."""
+    for n, dR, kmax in TIERS:
+        for aspect, twist in ((1.0, 0.0), (1.0, 0.1), (3.0, 0.0), (2.0, 0.1), (3.0, 0.1)):
+            assert _pair_max_error(n, dR, kmax, aspect, twist, seed=n) < 5e-13, (n, aspect, twist)
+
+
+def test_twisted_quads_need_the_guard():
+    """Twist 1/4 of the half-side: the 6 x 6 tier at 25 R is off by far more than the bar."""
+    assert _pair_max_error(6, 25.0, 0.2, 1.0, 0.25, seed=6) > 1e-12
