@@ -15,7 +15,9 @@
 // workspace, see problem_bytes) within the budget; idle slots' problems are
 // evicted, least recently used first, to make room.  Later requests that fit
 // may pass a request that does not (backfilling), until the waiting request
-// is older than BACKFILL_MS.
+// is older than BACKFILL_MS.  A request whose reuse key is being solved in a
+// busy slot, or by an earlier queued request, waits for those factors without
+// a time limit, letting later requests pass.
 //
 // The reference has no server: each request is one solve_bieq_aqd2 +
 // force_FN_aqd2 (bem3_aw_qd2_solve_bieq.c:3, bem3_aw_qd2_force.c:4).
@@ -164,10 +166,12 @@ static void dispatch_locked(bemgpu_server *s) {
       slot &sl = s->slots[i];
       if (!sl.cur && sl.resident && !sl.evict && sl.key == r->key && sl.precision == r->precision) { pick = (int)i; break; }
     }
-    if (pick < 0 && t - r->t_submit <= BACKFILL_MS) {
+    if (pick < 0) {
       // a busy slot computes this request's matrices, or an earlier queued
       // request will: wait for those factors rather than assembling the same
-      // matrices a second time
+      // matrices a second time, however long that takes (the factors arrive no
+      // later than a second assembly started now would finish; if the other
+      // request fails, this one is admitted on its own at the next dispatch)
       bool pending = false;
       for (auto &sl : s->slots)
         if (sl.cur && sl.cur->key == r->key && sl.cur->precision == r->precision) pending = true;
