@@ -98,12 +98,12 @@ __device__ __forceinline__ void geomF(const double vR[3], const double vW[3], co
 // triangle on a triangle) instead of the reference's 12 x 12 per quad or
 // triangle part.  There the integrand is analytic well beyond the element (its
 // nearest singularity is that image) and turns by at most k R in phase across it:
-//    t   n_t   d_t   kR_t
+//    t   n_t   d_t   kR_t   (triangles: d_t, kR_t)
 //    0   10    3     1
 //    1    9    3.5   1
 //    2    8    5     1
-//    3    7    8     0.5
-//    4    6    25    0.2
+//    3    7    8     0.5    (6, 0.5)
+//    4    6    25    0.2    (12, 0.5)
 // Each rule gives the converged integral (and so the reference's 12 x 12,
 // itself converged there) to about 1e-13 of the pair's largest entry: checked
 // against 40 x 40 on curved and on twisted quads, on triangles with angles of
@@ -186,10 +186,13 @@ __device__ __forceinline__ int far_tier(const bem_far &fr, const bem_el &el, con
   double kR2;
   const double r2 = pair_ratio2(fr, el, rt, tri, kR2);
   if (kR2 > 1.0) return -1;
-  const bool shaped = tri || quad_tier_shape(el);
   int t;
-  if (!shaped) t = r2 >= 25.0 ? 2 : -1;
-  else t = r2 >= 625.0 && kR2 <= 0.04 ? 4 : r2 >= 64.0 && kR2 <= 0.25 ? 3 : r2 >= 25.0 ? 2 : r2 >= 12.25 ? 1 : r2 >= 9.0 ? 0 : -1;
+  if (tri)  // flat triangles converge faster: 7 points from 6 R, 6 from 12 R (k R <= 0.5)
+    t = r2 >= 144.0 && kR2 <= 0.25 ? 4 : r2 >= 36.0 && kR2 <= 0.25 ? 3 : r2 >= 25.0 ? 2 : r2 >= 12.25 ? 1 : r2 >= 9.0 ? 0 : -1;
+  else if (!quad_tier_shape(el))
+    t = r2 >= 25.0 ? 2 : -1;
+  else
+    t = r2 >= 625.0 && kR2 <= 0.04 ? 4 : r2 >= 64.0 && kR2 <= 0.25 ? 3 : r2 >= 25.0 ? 2 : r2 >= 12.25 ? 1 : r2 >= 9.0 ? 0 : -1;
   if (t < 0) return -1;
   // |z(zeta, eta) - c0z| <= |c1z| + |c2z| + |c3z| over the element
   const double zr = fabs(el.cr[2][1]) + fabs(el.cr[2][2]) + fabs(el.cr[2][3]);
@@ -1241,7 +1244,13 @@ struct self_acc {
   double f, fz, fe;
 };
 
-__global__ void __launch_bounds__(NP_THREADS) k_fs_self(bem_dom_dev D, double k, double *__restrict__ G,
+#ifndef FS_SELF_MINB
+// two blocks (16 warps) per SM: 128 registers with 520 B of spills, 1.1 % faster
+// per 216-quad solve than one block at 244 registers (it shares the SMs with
+// the periodic domain's kernels)
+#define FS_SELF_MINB 2
+#endif
+__global__ void __launch_bounds__(NP_THREADS, FS_SELF_MINB) k_fs_self(bem_dom_dev D, double k, double *__restrict__ G,
                                                         double *__restrict__ H, double *__restrict__ dG,
                                                         double *__restrict__ dH, double *__restrict__ selfF,
                                                         unsigned *status, int p0) {

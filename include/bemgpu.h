@@ -96,7 +96,8 @@ int bemgpu_set_ewald_scale(bemgpu_ctx *ctx, double scale);
  * source element's centre is at least d circumradii R from the nearest
  * lattice image of the collocation node:
  *     n = 10 from d = 3, 9 from 3.5, 8 from 5 (all with k R <= 1),
- *     7 from 8 (k R <= 0.5), 6 from 25 (k R <= 0.2),
+ *     7 from 8 (k R <= 0.5), 6 from 25 (k R <= 0.2);
+ *     on triangles 7 from 6 and 6 from 12 (k R <= 0.5);
  * the 10, 9, 7 and 6-point rules only on quads whose twist along the normal
  * is at most a tenth of the shorter half-side and whose half-sides are within
  * 3x (every triangle).  Each reproduces the reference's integrals to about

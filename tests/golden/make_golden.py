@@ -391,6 +391,10 @@ def main():
         make_far_pairs("tri320", "far_tri320.npz", 300, 60)
         print("far216.npz, far_tri320.npz written to", OUT)
         return
+    if sys.argv[1:] == ["fartri1280"]:
+        make_far_pairs("tri1280", "far_tri1280.npz", 300, 60)
+        print("far_tri1280.npz written to", OUT)
+        return
     if sys.argv[1:] == ["tiers"]:
         make_tier_pairs()
         print("tiers1536.npz written to", OUT)

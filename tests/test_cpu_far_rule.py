@@ -11,7 +11,9 @@ converged integral (and so the reference's 12 x 12, itself converged there) to
 1e-13 of the entry.  On bilinear quads with the surface Jacobian the bar holds
 for elements inside the device's shape guard (twist along the normal at most a
 tenth of the shorter half-side, half-sides within 3x) to 5e-13 of the pair's
-largest entry, and fails outside it."""
+largest entry, and fails outside it.  Flat triangles converge faster: 7 points
+from 6 R and 6 from 12 R (k R <= 0.5) meet 1e-13 of the entry, equilateral or
+with angles down to 25 degrees (TRI_TIERS)."""
 import numpy as np
 
 K = 2 * np.pi
@@ -102,8 +104,58 @@ def test_closer_pairs_need_the_reference_rule():
     assert worst > 1e-12
 
 
-# (points, distance in circumradii, largest k R) of each tier
+# (points, distance in circumradii, largest k R) of each tier; flat triangles
+# take the 7 and 6-point rules nearer in (TRI_TIERS)
 TIERS = [(10, 3.0, 1.0), (9, 3.5, 1.0), (8, 5.0, 1.0), (7, 8.0, 0.5), (6, 25.0, 0.2)]
+TRI_TIERS = [(7, 6.0, 0.5), (6, 12.0, 0.5)]
+
+
+def _tri_affine(n, V, tgt):
+    """G |W| N_i and (grad G . W) N_i over the flat triangle V[0..2] with the
+    collapsed rule (n > 30: converged), the reference triangle mapped affinely."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    u = 0.5 * (x + 1)
+    U, Vv = np.meshgrid(u, u, indexing="ij")
+    W = np.outer(0.5 * w, 0.5 * w) * U
+    z, e = 1 - 1.5 * U, 0.5 * SQ3 * U * (1 - 2 * Vv)
+    c0, c1, c2 = V.mean(0), (2 * V[0] - V[1] - V[2]) / 3, (V[1] - V[2]) / SQ3
+    r = c0 + c1 * z[..., None] + c2 * e[..., None]
+    Wv = np.cross(c1, c2)
+    v = r - tgt
+    R = np.linalg.norm(v, axis=-1)
+    g = np.exp(1j * K * R) / R
+    h = g * (1j * K - 1 / R) / R * (v @ Wv)
+    Ns = [1 / 3 + 2 / 3 * z, 1 / 3 - z / 3 + e / SQ3, 1 / 3 - z / 3 - e / SQ3]
+    return np.array([np.sum(W * g * np.linalg.norm(Wv) * N) for N in Ns] + [np.sum(W * h * N) for N in Ns])
+
+
+def test_triangle_tier_rules_error():
+    """Equilateral triangles (the model above) and triangles with angles down to 25 degrees."""
+    rng = np.random.default_rng(7)
+    for n, dR, kmax in TRI_TIERS:
+        worst = 0.0
+        for kR in (0.05, 0.2, kmax):
+            R = kR / K
+            for tgt in _targets(dR * R):
+                ref = tri_parts(40, tgt, R)
+                worst = max(worst, np.max(np.abs(tri_collapsed(n, tgt, R) - ref) / np.abs(ref)))
+            for _ in range(4):
+                while True:
+                    V = rng.standard_normal((3, 3))
+                    V[:, 2] = 0.0
+                    ang = [np.degrees(np.arccos(np.dot(V[(i + 1) % 3] - V[i], V[(i + 2) % 3] - V[i])
+                                                / np.linalg.norm(V[(i + 1) % 3] - V[i])
+                                                / np.linalg.norm(V[(i + 2) % 3] - V[i]))) for i in range(3)]
+                    if min(ang) >= 25.0:
+                        break
+                V -= V.mean(0)
+                V *= R / np.linalg.norm(V, axis=1).max()
+                for _ in range(8):
+                    u = rng.standard_normal(3)
+                    tgt = dR * R * rng.uniform(1.0, 1.5) * u / np.linalg.norm(u)
+                    ref, got = _tri_affine(60, V, tgt), _tri_affine(n, V, tgt)
+                    worst = max(worst, np.max(np.abs(got - ref) / np.abs(ref)))
+        assert worst < 1e-13, (n, worst)
 
 
 def test_tier_rules_error():

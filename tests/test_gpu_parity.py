@@ -147,14 +147,16 @@ def test_qpgf_next_to_lattice_plane_matches_reference():
 
 @pytest.mark.parametrize("mesh,fixture,far_rule", [("sphere216", "far216.npz", 1), ("sphere216", "far216.npz", 0),
                                                    ("tri320", "far_tri320.npz", 1), ("sphere216", "near216.npz", 1),
-                                                   ("sphere1536", "tiers1536.npz", 1)])
+                                                   ("sphere1536", "tiers1536.npz", 1), ("tri1280", "far_tri1280.npz", 1)])
 def test_far_pairs_match_reference(mesh, fixture, far_rule):
     """Regular pairs against the reference's 12 x 12 rule per quad or triangle
     part (q0_dcoef_bd_node_t2_cc): 216-quad sphere, 320 far pairs (centre
     distance >= 5.5 element circumradii from every lattice image of the node,
     where the device's default uses its 8 and 7-point rules) and 80 nearer
     ones (the 10 and 9-point rules from 3 R); 320-triangle icosphere, 240 far
-    (collapsed rules over the triangle) and 60 nearer; 1536-quad sphere, 40
+    (collapsed rules over the triangle) and 60 nearer; 1280-triangle icosphere
+    (k R = 0.18), 240 far (191 of them from 12 R: the triangles' 6-point rule)
+    and 60 nearer; 1536-quad sphere, 40
     pairs in each distance band of the shorter rules (k R = 0.15: the 6-point
     rule from 25 R).  Entry-wise relative 1e-12 (the triangles' fourth entry is
     zero in both).  216-quad sphere, 240 pairs at 1 to 3 circumradii, most of
@@ -179,7 +181,7 @@ def test_far_pairs_match_reference(mesh, fixture, far_rule):
     assert sum(counts) > 0
     if not far_rule:
         assert counts[1:] == [0] * 5
-    elif mesh == "sphere1536":
+    elif mesh in ("sphere1536", "tri1280"):
         assert min(counts) > 0, counts  # the reference's rule and all five shorter ones
     elif mesh == "sphere216":
         assert min(counts[:5]) > 0 and counts[5] == 0, counts  # k R = 0.37: no 6-point pairs
