@@ -374,6 +374,29 @@ __global__ void __launch_bounds__(128) k_plist_fill(bem_dom_dev D, const uint8_t
   }
 }
 
+// ------------------------------------------------------------------ batches of Bloch vectors
+// A batch: nb problems on one body, media, lattice and frequency that differ
+// only in the in-plane Bloch wave vector (and incident field).  Their pair
+// flags, pair lists, near lists and real-space term table are the same; each
+// has its own Ewald parameters (bem_qp: Bloch phases, spectral table) and its
+// own G and H.  The batched kernels (BT = true) take instance b's parameters
+// from qp[b] into shared memory and write G[b], H[b].
+struct bem_bat {
+  int nb;
+  const bem_qp *qp;   // [nb] on the device
+  double *const *G;   // [nb] device pointers
+  double *const *H;
+};
+// every thread of the block calls it; qs is complete after the barrier
+static_assert(sizeof(bem_qp) % 8 == 0, "bem_qp is copied in 8-byte words");
+__device__ __forceinline__ void bat_stage(const bem_bat &B, int b, bem_qp &qs) {
+  __syncthreads();  // the previous instance's readers are done with qs
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.qp + b);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&qs);
+  for (int i = threadIdx.x; i < (int)(sizeof(bem_qp) / 8); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
 // ------------------------------------------------------------------ periodic regular pairs
 // 2 pairs x 144 points per block; one quasi-periodic Green's function per thread
 // (q0_bil_dcoef_v2_cc_GL, q0_bil_dcoef_v2_cc.c:129-204, evaluated once per
@@ -382,18 +405,28 @@ __global__ void __launch_bounds__(128) k_plist_fill(bem_dom_dev D, const uint8_t
 #ifndef RP_MINB
 #define RP_MINB 2  // two blocks (18 warps) per SM: caps registers at 113
 #endif
-__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, const __grid_constant__ bem_qp q, const uint8_t *__restrict__ flag,
-                                                           double *__restrict__ G, double *__restrict__ H,
+template <bool BT>
+__global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, const __grid_constant__ bem_qp q0, const uint8_t *__restrict__ flag,
+                                                           double *G0, double *H0,
                                                            unsigned *status, unsigned long long *terms, long long pair0,
-                                                           long long npairs, bem_plist L) {
+                                                           long long npairs, bem_plist L, bem_bat B) {
   __shared__ double acc[16][RP_THREADS + 1];
+  __shared__ bem_qp qs;  // BT: the instance's parameters
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
-  const double2 *wts = bem_wtab_stage(q, wts_s);
+  const double2 *wts = bem_wtab_stage(q0, wts_s);  // one table for every instance of a batch
   __syncthreads();
   const int lp = threadIdx.x / 144, pt = threadIdx.x % 144;
   const long long nu = plist_units(L, npairs);
   const unsigned long long lb = plist_base(L);
   unsigned long long nterm = 0, npt = 0;
+  for (int b = 0; b < (BT ? B.nb : 1); ++b) {
+  double *__restrict__ G = G0, *__restrict__ H = H0;
+  if (BT) {
+    bat_stage(B, b, qs);
+    G = B.G[b];
+    H = B.H[b];
+  }
+  const bem_qp &q = BT ? qs : q0;
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
     const bool valid = u0 + lp < nu;
     const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
@@ -453,6 +486,7 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
       }
     }
     __syncthreads();  // acc is rewritten by the next unit group
+  }
   }
   count_work(terms + 0, nterm, npt);
 }
@@ -563,15 +597,16 @@ struct far_shape {
   static constexpr int NP = NF * NF, PB = FP_THREADS / NP, TH = PB * NP, TB = (TH + 31) / 32 * 32,
                        T = BEM_TIER_N0 - NF;
 };
-template <int NF>
-__global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q,
-                                                        const uint8_t *__restrict__ flag, double *__restrict__ G,
-                                                        double *__restrict__ H, unsigned *status,
+template <int NF, bool BT>
+__global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q0,
+                                                        const uint8_t *__restrict__ flag, double *G0,
+                                                        double *H0, unsigned *status,
                                                         unsigned long long *terms, long long pair0, long long npairs,
-                                                        bem_plist L) {
+                                                        bem_plist L, bem_bat B) {
   using F = far_shape<NF>;
   constexpr uint8_t FL = (uint8_t)(3 + F::T);
   __shared__ double acc[16][F::TB + 1];
+  __shared__ bem_qp qs;  // BT: the instance's parameters
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const long long nu = plist_units(L, npairs);
   const unsigned long long lb = plist_base(L);
@@ -583,10 +618,18 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
       if (threadIdx.x < F::PB && u0 + threadIdx.x < nu) mine |= flag[pair0 + u0 + threadIdx.x] == FL;
     if (!__syncthreads_or(mine)) return;
   }
-  const double2 *wts = bem_wtab_stage(q, wts_s);
+  const double2 *wts = bem_wtab_stage(q0, wts_s);  // one table for every instance of a batch
   __syncthreads();
   const int lp = threadIdx.x / F::NP, pt = threadIdx.x % F::NP;
   unsigned long long nterm = 0, npt = 0;
+  for (int b = 0; b < (BT ? B.nb : 1); ++b) {
+  double *__restrict__ G = G0, *__restrict__ H = H0;
+  if (BT) {
+    bat_stage(B, b, qs);
+    G = B.G[b];
+    H = B.H[b];
+  }
+  const bem_qp &q = BT ? qs : q0;
   for (long long u0 = (long long)F::PB * blockIdx.x; u0 < nu; u0 += (long long)F::PB * gridDim.x) {
     const bool valid = threadIdx.x < F::TH && u0 + lp < nu;
     const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
@@ -661,6 +704,7 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
       }
     }
     __syncthreads();  // acc is rewritten by the next unit group
+  }
   }
   count_work(terms + 0, nterm, npt);
 }
@@ -775,13 +819,24 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*N
   __syncthreads();
 }
 
-__global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_qp q, const int *__restrict__ near_s,
-                                                        const int *__restrict__ near_n, double *__restrict__ G,
-                                                        double *__restrict__ H, double *__restrict__ nearF, unsigned *status,
-                                                        unsigned long long *terms) {
-  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...
+template <bool BT>
+__global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_qp q0, const int *__restrict__ near_s,
+                                                        const int *__restrict__ near_n, double *G0,
+                                                        double *H0, double *__restrict__ nearF, unsigned *status,
+                                                        unsigned long long *terms, bem_bat B) {
+  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...; BT: block
+  // (p, y, b) those of instance b, and instance 0 alone writes the geometric sums
   const int p = blockIdx.x, nn = near_n[p];
   if ((int)blockIdx.y >= nn) return;
+  __shared__ bem_qp qs;
+  double *__restrict__ G = G0, *__restrict__ H = H0;
+  if (BT) {
+    bat_stage(B, blockIdx.z, qs);
+    G = B.G[blockIdx.z];
+    H = B.H[blockIdx.z];
+    if (blockIdx.z) nearF = nullptr;
+  }
+  const bem_qp &q = BT ? qs : q0;
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
@@ -867,7 +922,7 @@ __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_q
       double *dst = c < 8 ? G : H;
       const int a = (c & 7) >> 1, part = c & 1;
       dst[2 * ((size_t)p * N + 4 * s + a) + part] = v[c];
-    } else if (threadIdx.x < 19) {
+    } else if (threadIdx.x < 19 && nearF) {
       nearF[((size_t)p * D.near_cap + k) * 3 + (threadIdx.x - 16)] = v[threadIdx.x] * BEM_I_FP;
     }
     __syncthreads();  // sm is reused by the next pair
@@ -943,13 +998,24 @@ __device__ __forceinline__ bool self_point(const bem_el &el, const double th[5],
   return rm >= 0.0;
 }
 
-__global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_qp q, double *__restrict__ G,
-                                                        double *__restrict__ H, double *__restrict__ selfF,
-                                                        unsigned *status, unsigned long long *terms) {
+template <bool BT>
+__global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_qp q0, double *G0,
+                                                        double *H0, double *__restrict__ selfF,
+                                                        unsigned *status, unsigned long long *terms, bem_bat B) {
   const int p = blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (bem_is_tri(D, te)) return;  // k_q0_self_tri
+  // BT: block (p, 0, b) integrates instance b; instance 0 alone writes selfF
+  __shared__ bem_qp qs;
+  double *__restrict__ G = G0, *__restrict__ H = H0;
+  if (BT) {
+    bat_stage(B, blockIdx.z, qs);
+    G = B.G[blockIdx.z];
+    H = B.H[blockIdx.z];
+    if (blockIdx.z) selfF = nullptr;
+  }
+  const bem_qp &q = BT ? qs : q0;
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
@@ -1056,9 +1122,11 @@ __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_q
       Te[d] = el.cr[d][2] + el.cr[d][3] * zt;
     }
     const double iTz = 1.0 / sqrt(dot3(Tz, Tz)), iTe = 1.0 / sqrt(dot3(Te, Te));
-    selfF[3 * p + 0] = F0;
-    selfF[3 * p + 1] = plane ? 0.0 : iTz * (Fzp - Fzm) / (2.0 * BEM_CDFH);
-    selfF[3 * p + 2] = plane ? 0.0 : iTe * (Fep - Fem) / (2.0 * BEM_CDFH);
+    if (selfF) {
+      selfF[3 * p + 0] = F0;
+      selfF[3 * p + 1] = plane ? 0.0 : iTz * (Fzp - Fzm) / (2.0 * BEM_CDFH);
+      selfF[3 * p + 2] = plane ? 0.0 : iTe * (Fep - Fem) / (2.0 * BEM_CDFH);
+    }
   }
 }
 
@@ -1925,40 +1993,49 @@ static bem_far far_params(const bem_dom_dev *D, const bem_qp *q, int periodic) {
 // empty blocks)
 static int near_grid_y(const bem_dom_dev *D) { return D->near_cap < 32 ? D->near_cap : 32; }
 
+template <bool BT>
+static int q0_smem_attrs_bt() {
+  const int b = (int)BEM_WT_SMEM;
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (cudaFuncSetAttribute(k_q0_far<10, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<9, BT>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<8, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<7, BT>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<6, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_regular<BT>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_near<BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self<BT>, a, b) != cudaSuccess)
+    return -1;
+  return 0;
+}
 static int q0_smem_attrs() {
   const int b = (int)BEM_WT_SMEM;
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (cudaFuncSetAttribute(k_q0_far<10>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<9>, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_far<8>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<7>, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_far<6>, a, b) != cudaSuccess)
-    return -1;
-  if (cudaFuncSetAttribute(k_q0_regular, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_regular_tri, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_near, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_self, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self_tri, a, b) != cudaSuccess)
+  if (q0_smem_attrs_bt<false>() || q0_smem_attrs_bt<true>()) return -1;
+  if (cudaFuncSetAttribute(k_q0_regular_tri, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self_tri, a, b) != cudaSuccess)
     return -1;
   return 0;
 }
 
 // tier NF's kernel over its list (L.e set: grid_list blocks striding over it)
 // or over the pair range [p0, p0 + np)
-template <int NF>
+template <int NF, bool BT>
 static void launch_far(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
-                       long long np, bem_plist L, unsigned grid_list, cudaStream_t st) {
+                       long long np, bem_plist L, unsigned grid_list, const bem_bat &B, cudaStream_t st) {
   using F = far_shape<NF>;
   L.type = 1 + F::T;
   const unsigned grid = L.e ? grid_list : (unsigned)((np + F::PB - 1) / F::PB);
   if (grid == 0) return;
-  k_q0_far<NF><<<grid, F::TB, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np, L);
+  k_q0_far<NF, BT><<<grid, F::TB, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np, L, B);
   bem_count_launches(1);
 }
+template <bool BT = false>
 static void launch_far_tiers(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
-                             long long np, const bem_plist &L, unsigned grid_list, cudaStream_t st) {
-  launch_far<10>(D, q, S, G, H, p0, np, L, grid_list, st);
-  launch_far<9>(D, q, S, G, H, p0, np, L, grid_list, st);
-  launch_far<8>(D, q, S, G, H, p0, np, L, grid_list, st);
-  launch_far<7>(D, q, S, G, H, p0, np, L, grid_list, st);
-  launch_far<6>(D, q, S, G, H, p0, np, L, grid_list, st);
+                             long long np, const bem_plist &L, unsigned grid_list, cudaStream_t st,
+                             const bem_bat &B = bem_bat{0, nullptr, nullptr, nullptr}) {
+  launch_far<10, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<9, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<8, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<7, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<6, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
 }
+static const bem_bat k_nobat = {0, nullptr, nullptr, nullptr};
 
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
                                    bem_scratch *S, double *G, double *H, double *dG, double *dH, double *dF,
@@ -2001,7 +2078,8 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
         return -1;
       const unsigned grid = RP_MINB * (unsigned)nsm, grid_far = FP_MINB * (unsigned)nsm;
       const bem_plist Lreg = {S->plist, S->pcount, 0};
-      k_q0_regular<<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg);
+      k_q0_regular<false><<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg,
+                                                                         k_nobat);
       bem_count_launches(1);
       if (D->far_rule) launch_far_tiers(D, q, S, G, H, 0, npairs, Lreg, grid_far, st);
       if (D->has_tri) {
@@ -2013,8 +2091,8 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       const long long chunk = 1LL << 26;  // keep grid.x well inside limits
       for (long long p0 = 0; p0 < npairs; p0 += chunk) {
         const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
-        k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
-                                                                      L0);
+        k_q0_regular<false><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+                                                                             p0, np, L0, k_nobat);
         bem_count_launches(1);
         if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);
         if (D->has_tri) {
@@ -2025,11 +2103,11 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    k_q0_near<<<dim3(N, near_grid_y(D)), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF,
-                                                                       S->status, S->terms);
+    k_q0_near<false><<<dim3(N, near_grid_y(D)), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF,
+                                                                              S->status, S->terms, k_nobat);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
-    k_q0_self<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
+    k_q0_self<false><<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms, k_nobat);
     bem_count_launches(1);
     if (D->has_tri) {
       k_q0_self_tri<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
@@ -2056,6 +2134,53 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
   return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
 }
 
+// The periodic domain of a batch of nb problems on one body, media, lattice
+// and frequency (bem_bat).  One classification, with q (instance 0's
+// parameters: pair flags, rule tiers, lists and geometric sums depend on the
+// geometry, the lattice and k only), then each kernel launched once for all
+// instances: the regular-pair kernels stride over the lists instance after
+// instance, the near-singular and self kernels take the instance from
+// blockIdx.z; the diagonal per instance.  qp_d, G_d, H_d: the batch's arrays on
+// the device; Hh: the H pointers on the host.  Quad meshes with pair lists only
+// (-2 otherwise).
+extern "C" int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, int nb, const bem_qp *qp_d,
+                                         double *const *G_d, double *const *H_d, double *const *Hh, bem_scratch *S,
+                                         double *dF, cudaStream_t st) {
+  if (q0_smem_attrs()) return -1;
+  const int N = D->ne * 4;
+  if (D->ne <= 0 || nb <= 0) return 0;
+  if (D->has_tri || nb > 65535) return -2;
+  const long long npairs = (long long)N * D->ne;
+  if (!(S->plist && S->pcount && (unsigned long long)npairs <= S->pcap && npairs <= 0xffffffffLL)) return -2;
+  if (cudaMemsetAsync(S->pcount, 0, 2 * BEM_NLIST * sizeof(unsigned), st) != cudaSuccess) return -1;
+  k_classify<<<N, 128, 0, st>>>(*D, far_params(D, q, 1), S->rowF, S->near_s, S->near_n, S->flag, S->status,
+                                S->pcount);
+  bem_count_launches(1);
+  k_plist_fill<<<N, 128, 0, st>>>(*D, S->flag, S->plist, S->pcount, S->pcap);
+  bem_count_launches(1);
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
+    return -1;
+  const bem_bat B = {nb, qp_d, G_d, H_d};
+  const bem_plist Lreg = {S->plist, S->pcount, 0};
+  k_q0_regular<true><<<RP_MINB * (unsigned)nsm, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, nullptr, nullptr, S->status,
+                                                                              S->terms, 0, npairs, Lreg, B);
+  bem_count_launches(1);
+  if (D->far_rule) launch_far_tiers<true>(D, q, S, nullptr, nullptr, 0, npairs, Lreg, FP_MINB * (unsigned)nsm, st, B);
+  k_q0_near<true><<<dim3(N, near_grid_y(D), nb), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, nullptr,
+                                                                                nullptr, S->nearF, S->status, S->terms, B);
+  bem_count_launches(1);
+  k_q0_self<true><<<dim3(N, 1, nb), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, nullptr, nullptr, S->selfF, S->status,
+                                                                   S->terms, B);
+  bem_count_launches(1);
+  for (int b = 0; b < nb; ++b) {
+    k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, 1, S->rowF, S->near_n, S->nearF, S->selfF, Hh[b], dF, S->status);
+    bem_count_launches(1);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
 // Time the periodic regular-pair kernel on a sample of the pairs (nchunk
 // chunks of frac / nchunk of all pairs, spread over the node range) for the
 // Ewald-parameter autotuner; the pair flags must be current (k_classify).
@@ -2074,8 +2199,8 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
       // the kernels of the assembly itself (over pair ranges, not lists):
       // quad sources, far pairs, and triangle sources when there are any
       const bem_plist L0 = {nullptr, nullptr, 0};
-      k_q0_regular<<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np,
-                                                                    L0);
+      k_q0_regular<false><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+                                                                           p0, np, L0, k_nobat);
       bem_count_launches(1);
       if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);
       if (D->has_tri) {

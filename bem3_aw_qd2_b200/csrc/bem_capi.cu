@@ -114,7 +114,22 @@ struct bemgpu_ctx {
   int dgh_rows_req = 0;                   // asked for (0: 256 MiB of each)
   bool int_factored[BEMGPU_MAXDOM] = {};
   long long int_reused_loads = 0;
+  // batch of Bloch vectors (bemgpu_batch_load): instance b's Ewald parameters,
+  // periodic-domain G and H and incident data; instance 0's G, H and spectral
+  // table are the context's own, the others' are owned here.  G[0], H[0] and
+  // qp point at the selected instance (bemgpu_batch_select).
+  struct batch_inst {
+    bem_qp qp;
+    double *G = nullptr, *H = nullptr, *stab = nullptr;
+    std::vector<double> Pi, dPi, p_inc, v_inc;
+    double pw[16];
+  };
+  std::vector<batch_inst> bat;
+  int bat_cur = -1;
+  bem_qp *bat_qp_d = nullptr;
+  double **bat_G_d = nullptr, **bat_H_d = nullptr;
 };
+
 
 static int fail(bemgpu_ctx *c, const char *what, cudaError_t e) {
   if (c) snprintf(c->err, sizeof(c->err), "%s: %s", what, cudaGetErrorString(e));
@@ -154,9 +169,26 @@ static cudaError_t falloc(bemgpu_ctx *c, T **p, size_t count) {
 // Gauss-Legendre tables and Faddeeva constants are uploaded once per device.
 static int g_const_dev = -1;
 
+// back to a single problem: instance 0 selected again (its G, H and
+// parameters are the context's own buffers), the others' buffers freed
+static void batch_clear(bemgpu_ctx *c) {
+  if (c->bat.empty()) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->G[0] = c->bat[0].G;
+  c->H[0] = c->bat[0].H;
+  c->qp = c->bat[0].qp;
+  for (size_t b = 1; b < c->bat.size(); ++b) {
+    dfree(c->bat[b].G); dfree(c->bat[b].H); dfree(c->bat[b].stab);
+  }
+  dfree(c->bat_qp_d); dfree(c->bat_G_d); dfree(c->bat_H_d);
+  c->bat.clear();
+  c->bat_cur = -1;
+}
+
 // release: give every problem buffer back (unload, destroy); otherwise a new
 // load follows and reuses the allocations that are large enough (falloc)
 static void free_problem(bemgpu_ctx *c, bool release) {
+  batch_clear(c);
   if (release) {
     dfree(c->cr); dfree(c->cw); dfree(c->ren); dfree(c->wen); dfree(c->plane);
     dfree(c->sid); dfree(c->rowidx); dfree(c->npe); dfree(c->eni); dfree(c->md); dfree(c->dom_ne_d); dfree(c->dom_off_d);
@@ -576,6 +608,7 @@ extern "C" int bemgpu_rule_pairs(bemgpu_ctx *c, unsigned long long counts[6]) {
 }
 
 extern "C" int bemgpu_set_ewald_scale(bemgpu_ctx *c, double scale) {
+  if (!c->bat.empty()) { snprintf(c->err, sizeof(c->err), "a batch is loaded (load a single problem first)"); return -2; }
   if (scale != BEMGPU_EWALD_RULE && !(scale >= 0.25 && scale <= 4.0)) {
     snprintf(c->err, sizeof(c->err), "Ewald scale %g outside [0.25, 4]", scale);
     return -2;
@@ -595,6 +628,7 @@ static bem_dom_dev dom_view(bemgpu_ctx *c, int d);
 // factors meet the per-point cap and lose the tabulated terms) and keep the
 // fastest.
 extern "C" int bemgpu_autotune(bemgpu_ctx *c, double *best_scale) {
+  if (!c->bat.empty()) { snprintf(c->err, sizeof(c->err), "a batch is loaded (load a single problem first)"); return -2; }
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   bem_dom_dev D = dom_view(c, 0);
   if (bem_launch_classify(&D, &c->qp, 1, &c->scr, c->stream)) return fail(c, "autotune", cudaGetLastError());
@@ -679,6 +713,151 @@ extern "C" int bemgpu_assemble(bemgpu_ctx *c) {
   }
   c->int_valid = c->MN >= 1;
   return 0;
+}
+
+// ---------------------------------------------------------------- batches of Bloch vectors
+// Problems on one body, media, lattice and frequency that differ only in the
+// incidence (in-plane Bloch wave vector and incident field): the free-space
+// domains and the periodic domain's classification are the same for all of
+// them, so one batch assembles the interior domains once and the periodic
+// domain of every instance with each kernel launched once
+// (bem_launch_assemble_batch).
+static bool same_body(const bemgpu_problem *a, const bemgpu_problem *b) {
+  if (a->Ne != b->Ne || a->NN != b->NN || a->MN != b->MN || a->ps != b->ps) return false;
+  const size_t ne = a->Ne, nd = a->MN + 1;
+  size_t tot = 0;
+  for (size_t d = 0; d < nd; ++d) {
+    if (a->dom_ne[d] != b->dom_ne[d]) return false;
+    tot += a->dom_ne[d];
+  }
+  if (a->qp[0] != b->qp[0]) return false;                       // k
+  for (int i = 4; i < 8; ++i) if (a->qp[i] != b->qp[i]) return false;  // lattice
+  return !memcmp(a->sid, b->sid, tot * sizeof(int)) && !memcmp(a->cr, b->cr, ne * 12 * sizeof(double)) &&
+         !memcmp(a->cw, b->cw, ne * 9 * sizeof(double)) && !memcmp(a->ren, b->ren, ne * 12 * sizeof(double)) &&
+         !memcmp(a->wen, b->wen, ne * 12 * sizeof(double)) && !memcmp(a->npe, b->npe, ne * sizeof(int)) &&
+         !memcmp(a->eni, b->eni, ne * 4 * sizeof(int)) && !memcmp(a->plane, b->plane, ne) &&
+         !memcmp(a->k0, b->k0, nd * sizeof(double)) && !memcmp(a->k2, b->k2, 2 * nd * sizeof(double)) &&
+         !memcmp(a->rho0, b->rho0, nd * sizeof(double)) && !memcmp(a->c0, b->c0, nd * sizeof(double));
+}
+
+extern "C" int bemgpu_batch_load(bemgpu_ctx *c, int nb, const bemgpu_problem *const *probs) {
+  if (nb < 1 || !probs) { snprintf(c->err, sizeof(c->err), "batch of %d problems", nb); return -2; }
+  for (int b = 1; b < nb; ++b)
+    if (!same_body(probs[0], probs[b])) {
+      snprintf(c->err, sizeof(c->err), "batch problem %d: not the same body, media, lattice and frequency", b);
+      return -2;
+    }
+  const int rc = bemgpu_load(c, probs[0]);
+  if (rc) return rc;
+  if (c->dom_tri[0]) { snprintf(c->err, sizeof(c->err), "batches take quad meshes only"); return -2; }
+  const size_t N = 4 * (size_t)c->dom_ne[0], ne = c->Ne;
+  if (!c->scr.plist || (unsigned long long)(N * (size_t)c->dom_ne[0]) > c->scr.pcap) {
+    snprintf(c->err, sizeof(c->err), "batches need the periodic domain's pair lists (at most 32768 elements)");
+    return -2;
+  }
+  c->bat.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    bemgpu_ctx::batch_inst &I = c->bat[b];
+    const bemgpu_problem *pr = probs[b];
+    I.Pi.assign(pr->Pi, pr->Pi + ne * 8);
+    I.dPi.assign(pr->dPi, pr->dPi + ne * 8);
+    I.p_inc.assign(pr->p_inc, pr->p_inc + ne * 8);
+    I.v_inc.assign(pr->v_inc, pr->v_inc + ne * 24);
+    memcpy(I.pw, pr->pw, sizeof(I.pw));
+    if (b == 0) {
+      I.qp = c->qp;
+      I.G = c->G[0];
+      I.H = c->H[0];
+      continue;
+    }
+    bem_qp_prepare(pr->qp, &I.qp);
+    if (I.qp.eta0 != c->qp.eta0) {
+      snprintf(c->err, sizeof(c->err), "batch problem %d: another Ewald parameter", b);
+      batch_clear(c);
+      return -2;
+    }
+    I.qp.eta_run = c->qp.eta_run;  // one real-space table for the batch
+    I.qp.wt = c->qp.wt;
+    I.qp.wt_h = c->qp.wt_h;
+    I.qp.wt_n = c->qp.wt_n;
+    const size_t cnt = stab_window(&I.qp, c->zspan);
+    cudaError_t e = cudaSuccess;
+    if (cnt) {
+      e = dalloc(&I.stab, cnt);
+      if (e == cudaSuccess && bem_launch_stab(&I.qp, I.stab, c->stream) != 0) e = cudaGetLastError();
+      I.qp.st = I.stab;
+    }
+    if (e == cudaSuccess) e = dalloc(&I.G, 2 * N * N);
+    if (e == cudaSuccess) e = dalloc(&I.H, 2 * N * N);
+    if (e != cudaSuccess) {
+      batch_clear(c);
+      return fail(c, "batch buffers", e);
+    }
+  }
+  std::vector<bem_qp> qps(nb);
+  std::vector<double *> gs(nb), hs(nb);
+  for (int b = 0; b < nb; ++b) { qps[b] = c->bat[b].qp; gs[b] = c->bat[b].G; hs[b] = c->bat[b].H; }
+  cudaError_t e = dalloc(&c->bat_qp_d, (size_t)nb);
+  if (e == cudaSuccess) e = dalloc(&c->bat_G_d, (size_t)nb);
+  if (e == cudaSuccess) e = dalloc(&c->bat_H_d, (size_t)nb);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_qp_d, qps.data(), nb * sizeof(bem_qp), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_G_d, gs.data(), nb * sizeof(double *), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_H_d, hs.data(), nb * sizeof(double *), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // the host arrays go out of scope
+  if (e != cudaSuccess) {
+    batch_clear(c);
+    return fail(c, "batch tables", e);
+  }
+  c->bat_cur = 0;
+  return 0;
+}
+
+extern "C" int bemgpu_batch_assemble(bemgpu_ctx *c) {
+  if (!c->loaded || c->bat.empty()) { snprintf(c->err, sizeof(c->err), "no batch loaded"); return -2; }
+  c->factored = false;
+  if (c->MN >= 1) {
+    CK(cudaEventRecord(c->ev_fork, c->stream), "assembly fork");
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "assembly fork");
+  }
+  const bool skip_interior = c->int_reuse && c->int_valid;
+  for (int d = 1; d <= c->MN && !skip_interior; ++d) {
+    bem_dom_dev D = dom_view(c, d);
+    if (bem_launch_assemble(&D, &c->qp, 0, 0, c->k0[d], &c->scr1, c->G[d], c->H[d], c->dG[d], c->dH[d], c->dF[d],
+                            c->side, nullptr) != 0)
+      return fail(c, "assembly launch", cudaGetLastError());
+  }
+  const int nb = (int)c->bat.size();
+  std::vector<double *> hs(nb);
+  for (int b = 0; b < nb; ++b) hs[b] = c->bat[b].H;
+  bem_dom_dev D = dom_view(c, 0);
+  const int r = bem_launch_assemble_batch(&D, &c->bat[0].qp, nb, c->bat_qp_d, c->bat_G_d, c->bat_H_d, hs.data(),
+                                          &c->scr, c->dF[0], c->stream);
+  if (r == -2) { snprintf(c->err, sizeof(c->err), "batch assembly: quad meshes with pair lists only"); return -2; }
+  if (r) return fail(c, "batch assembly launch", cudaGetLastError());
+  if (c->MN >= 1) {
+    CK(cudaEventRecord(c->ev_join, c->side), "assembly join");
+    CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0), "assembly join");
+  }
+  c->int_valid = c->MN >= 1;
+  return 0;
+}
+
+extern "C" int bemgpu_batch_select(bemgpu_ctx *c, int b) {
+  if (!c->loaded || c->bat.empty() || b < 0 || b >= (int)c->bat.size()) {
+    snprintf(c->err, sizeof(c->err), "no batch instance %d", b);
+    return -2;
+  }
+  bemgpu_ctx::batch_inst &I = c->bat[b];
+  CK(cudaStreamSynchronize(c->stream), "batch select");
+  c->G[0] = I.G;
+  c->H[0] = I.H;
+  c->qp = I.qp;
+  c->bat_cur = b;
+  c->factored = false;
+  // the interior domains' matrices are the batch's: their dpv factors, once
+  // made by a solve, serve every instance
+  if (b > 0) c->int_reuse = c->int_reuse_on;
+  return bemgpu_set_incident(c, I.Pi.data(), I.dPi.data(), I.p_inc.data(), I.v_inc.data(), I.pw);
 }
 
 // Dense systems M X = B with M row-major FP64 (n x n), B column-major (n x nrhs).
@@ -1362,6 +1541,7 @@ extern "C" cudaError_t bem_launch_transform(int ne, const double *rv, double th,
                                             cudaStream_t st);
 
 extern "C" int bemgpu_transform_mesh(bemgpu_ctx *c, const double *rv, double th, const double *tv) {
+  if (!c->bat.empty()) { snprintf(c->err, sizeof(c->err), "a batch is loaded (load a single problem first)"); return -2; }
   if (!c->loaded) { snprintf(c->err, sizeof(c->err), "no problem loaded"); return -2; }
   CK(bem_launch_transform(c->Ne, rv, th, tv, c->cr, c->cw, c->ren, c->wen, c->Pi, c->dPi, c->p_inc, c->v_inc,
                           c->pw_d, c->k2.data(), c->stream),

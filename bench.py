@@ -555,7 +555,9 @@ def run_sweep(args, rank, world):
     instances): one context solves the instances in frequency order, so that
     instances at the same frequency keep the free-space domain's matrices and
     dpv factors (bemgpu_interior_reuses); FP64, then the mixed form, with the
-    mixed form's force error against FP64 per instance."""
+    mixed form's force error against FP64 per instance; then the mixed form
+    with one batch per frequency (bemgpu_batch_load / _assemble / _select),
+    its forces against the unbatched ones."""
     import ctypes
     from bem3_aw_qd2_b200 import api, meshgen
     h, g = api.libs()
@@ -593,7 +595,42 @@ def run_sweep(args, rank, world):
         if prec:
             res[tag]["mode"] = {1: "FP32", 2: "TF32", 3: "TF32x3", 4: "TF32"}.get(g.bemgpu_get_precision(ctx), "?")
     errs = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(res["mixed"]["F"], res["fp64"]["F"])]
-    for tag in res:
+    # the mixed form again, one batch per frequency (bemgpu_batch_*): the
+    # interior domains once, the periodic domain of all the frequency's
+    # directions with each kernel launched once, then a solve per instance
+    PP = ctypes.POINTER(api.Problem)
+    g.bemgpu_batch_load.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(PP)]
+    g.bemgpu_batch_assemble.argtypes = [ctypes.c_void_p]
+    g.bemgpu_batch_select.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    groups = {}
+    for i, (fi, _) in enumerate(inst):
+        groups.setdefault(fi, []).append(i)
+
+    def batch_pass(sel):
+        Fb = {}
+        for fi, idx in sel.items():
+            arr = (PP * len(idx))(*[ctypes.pointer(probs[i]) for i in idx])
+            if g.bemgpu_batch_load(ctx, len(idx), arr) or g.bemgpu_batch_assemble(ctx):
+                raise RuntimeError(g.bemgpu_error(ctx).decode())
+            for j, i in enumerate(idx):
+                if g.bemgpu_batch_select(ctx, j) or g.bemgpu_solve(ctx):
+                    raise RuntimeError(g.bemgpu_error(ctx).decode())
+                Fv, Nv = np.zeros(3), np.zeros(3)
+                g.bemgpu_force(ctx, 0, api._p(rc3), api._p(Fv), api._p(Nv))
+                Fb[i] = Fv
+        g.bemgpu_sync(ctx)
+        return Fb
+    g.bemgpu_set_precision(ctx, args.mixed_mode or 2)
+    batch_pass({0: [0]})  # warm-up: the batched kernels' first launch
+    t0 = time.perf_counter()
+    Fb = batch_pass(groups)
+    el = time.perf_counter() - t0
+    res["mixed_batched"] = {"value": len(probs) / el, "unit": "solves/s", "seconds": el,
+                            "batches": len(groups), "instances_per_batch": [len(v) for v in groups.values()],
+                            "force_rel_diff_vs_unbatched": max(float(np.linalg.norm(Fb[i] - res["mixed"]["F"][i])
+                                                                     / np.linalg.norm(res["mixed"]["F"][i]))
+                                                               for i in range(len(probs)))}
+    for tag in ("fp64", "mixed"):
         del res[tag]["F"]
     g.bemgpu_destroy(ctx)
     for c, p in zip(cases, probs):
@@ -607,7 +644,7 @@ def run_sweep(args, rank, world):
                        "directions": args.sweep_dirs, "full_sweep": "64 directions x 8 frequencies (reduced here)",
                        "mesh": "1536-quad cube-sphere r = 0.3, square lattice 0.8",
                        "order": "frequency-major: instances at one frequency share the interior domain"},
-            "fp64": res["fp64"], "mixed": res["mixed"],
+            "fp64": res["fp64"], "mixed": res["mixed"], "mixed_batched": res["mixed_batched"],
             "force_rel_err_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
     if rank == 0:
         print(json.dumps(line))

@@ -117,6 +117,29 @@ int bemgpu_rule_pairs(bemgpu_ctx *ctx, unsigned long long counts[6]);
  * Costs about half of one regular-pair launch. */
 int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
 
+/* Batches of Bloch vectors (form 2; no counterpart in the reference, which
+ * assembles every problem on its own): nb problems on one body, media,
+ * lattice and frequency that differ only in the incidence (in-plane Bloch
+ * wave vector and incident field).  bemgpu_batch_load checks that, loads
+ * probs[0] as bemgpu_load does and keeps every instance's Ewald parameters
+ * (its own spectral table) and incident data, with device room for its
+ * periodic-domain G and H (32 N_0^2 bytes each); quad meshes of at most 32768
+ * elements.  bemgpu_batch_assemble assembles the free-space domains once and
+ * the periodic domain of all instances with each kernel launched once (one
+ * classification and one set of pair lists; the regular-pair kernels stride
+ * over the lists instance after instance, the near-singular and self kernels
+ * take the instance from the grid).  bemgpu_batch_select(ctx, b) makes
+ * instance b the context's problem: bemgpu_solve, bemgpu_force,
+ * bemgpu_get_solution, bemgpu_get_matrix and the field functions then act on
+ * it (the interior domains' dpv factors made by the first solve serve every
+ * instance).  Results equal those of loading and running each problem alone
+ * (same kernels and order of sums).  The batch ends at the next load; the
+ * Ewald scale, the autotuner and mesh transforms are refused while it is
+ * loaded.  Returns 0, -2 for bad input, -1 on a CUDA error. */
+int bemgpu_batch_load(bemgpu_ctx *ctx, int nb, const bemgpu_problem *const *probs);
+int bemgpu_batch_assemble(bemgpu_ctx *ctx);
+int bemgpu_batch_select(bemgpu_ctx *ctx, int b);
+
 /* Interior-domain reuse (no counterpart in the reference, which assembles
  * every domain for every solve): the free-space domains' matrices (G, H, dG,
  * dH, dF of domains >= 1, create_cmatrix_domain with did >= 1,
