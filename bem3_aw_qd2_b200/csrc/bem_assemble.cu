@@ -379,23 +379,27 @@ __global__ void __launch_bounds__(128) k_plist_fill(bem_dom_dev D, const uint8_t
 // only in the in-plane Bloch wave vector (and incident field).  Their pair
 // flags, pair lists, near lists and real-space term table are the same; each
 // has its own Ewald parameters (bem_qp: Bloch phases, spectral table) and its
-// own G and H.  The batched kernels (BT = true) take instance b's parameters
-// from qp[b] into shared memory and write G[b], H[b].
+// own G and H.  The batched kernels (BA = bem_bat) read instance b's
+// parameters from the argument block (qp[b], like a single problem's q0) and
+// write G[b], H[b].
+#define BEM_BAT_MAX 32  // instances per launch (the parameters travel in the kernel's argument block)
 struct bem_bat {
   int nb;
-  const bem_qp *qp;   // [nb] on the device
-  double *const *G;   // [nb] device pointers
-  double *const *H;
+  bem_qp qp[BEM_BAT_MAX];
+  double *G[BEM_BAT_MAX];
+  double *H[BEM_BAT_MAX];
 };
-// every thread of the block calls it; qs is complete after the barrier
-static_assert(sizeof(bem_qp) % 8 == 0, "bem_qp is copied in 8-byte words");
-__device__ __forceinline__ void bat_stage(const bem_bat &B, int b, bem_qp &qs) {
-  __syncthreads();  // the previous instance's readers are done with qs
-  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.qp + b);
-  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&qs);
-  for (int i = threadIdx.x; i < (int)(sizeof(bem_qp) / 8); i += blockDim.x) dst[i] = src[i];
-  __syncthreads();
-}
+struct bat_none {};  // a single problem: the kernel's own q0, G0, H0
+__device__ __forceinline__ int bat_n(const bat_none &) { return 1; }
+__device__ __forceinline__ int bat_n(const bem_bat &B) { return B.nb; }
+__device__ __forceinline__ const bem_qp &bat_q(const bat_none &, int, const bem_qp &q0) { return q0; }
+__device__ __forceinline__ const bem_qp &bat_q(const bem_bat &B, int b, const bem_qp &) { return B.qp[b]; }
+__device__ __forceinline__ double *bat_G(const bat_none &, int, double *G0) { return G0; }
+__device__ __forceinline__ double *bat_G(const bem_bat &B, int b, double *) { return B.G[b]; }
+__device__ __forceinline__ double *bat_H(const bat_none &, int, double *H0) { return H0; }
+__device__ __forceinline__ double *bat_H(const bem_bat &B, int b, double *) { return B.H[b]; }
+template <class BA> struct bat_is { static constexpr bool on = false; };
+template <> struct bat_is<bem_bat> { static constexpr bool on = true; };
 
 // ------------------------------------------------------------------ periodic regular pairs
 // 2 pairs x 144 points per block; one quasi-periodic Green's function per thread
@@ -405,13 +409,12 @@ __device__ __forceinline__ void bat_stage(const bem_bat &B, int b, bem_qp &qs) {
 #ifndef RP_MINB
 #define RP_MINB 2  // two blocks (18 warps) per SM: caps registers at 113
 #endif
-template <bool BT>
+template <class BA>
 __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev D, const __grid_constant__ bem_qp q0, const uint8_t *__restrict__ flag,
                                                            double *G0, double *H0,
                                                            unsigned *status, unsigned long long *terms, long long pair0,
-                                                           long long npairs, bem_plist L, bem_bat B) {
+                                                           long long npairs, bem_plist L, const __grid_constant__ BA B) {
   __shared__ double acc[16][RP_THREADS + 1];
-  __shared__ bem_qp qs;  // BT: the instance's parameters
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q0, wts_s);  // one table for every instance of a batch
   __syncthreads();
@@ -419,14 +422,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
   const long long nu = plist_units(L, npairs);
   const unsigned long long lb = plist_base(L);
   unsigned long long nterm = 0, npt = 0;
-  for (int b = 0; b < (BT ? B.nb : 1); ++b) {
-  double *__restrict__ G = G0, *__restrict__ H = H0;
-  if (BT) {
-    bat_stage(B, b, qs);
-    G = B.G[b];
-    H = B.H[b];
-  }
-  const bem_qp &q = BT ? qs : q0;
+  for (int b = 0; b < bat_n(B); ++b) {
+  double *__restrict__ G = bat_G(B, b, G0), *__restrict__ H = bat_H(B, b, H0);
+  const bem_qp &q = bat_q(B, b, q0);
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
     const bool valid = u0 + lp < nu;
     const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
@@ -597,16 +595,15 @@ struct far_shape {
   static constexpr int NP = NF * NF, PB = FP_THREADS / NP, TH = PB * NP, TB = (TH + 31) / 32 * 32,
                        T = BEM_TIER_N0 - NF;
 };
-template <int NF, bool BT>
+template <int NF, class BA>
 __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, const __grid_constant__ bem_qp q0,
                                                         const uint8_t *__restrict__ flag, double *G0,
                                                         double *H0, unsigned *status,
                                                         unsigned long long *terms, long long pair0, long long npairs,
-                                                        bem_plist L, bem_bat B) {
+                                                        bem_plist L, const __grid_constant__ BA B) {
   using F = far_shape<NF>;
   constexpr uint8_t FL = (uint8_t)(3 + F::T);
   __shared__ double acc[16][F::TB + 1];
-  __shared__ bem_qp qs;  // BT: the instance's parameters
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const long long nu = plist_units(L, npairs);
   const unsigned long long lb = plist_base(L);
@@ -622,14 +619,9 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
   __syncthreads();
   const int lp = threadIdx.x / F::NP, pt = threadIdx.x % F::NP;
   unsigned long long nterm = 0, npt = 0;
-  for (int b = 0; b < (BT ? B.nb : 1); ++b) {
-  double *__restrict__ G = G0, *__restrict__ H = H0;
-  if (BT) {
-    bat_stage(B, b, qs);
-    G = B.G[b];
-    H = B.H[b];
-  }
-  const bem_qp &q = BT ? qs : q0;
+  for (int b = 0; b < bat_n(B); ++b) {
+  double *__restrict__ G = bat_G(B, b, G0), *__restrict__ H = bat_H(B, b, H0);
+  const bem_qp &q = bat_q(B, b, q0);
   for (long long u0 = (long long)F::PB * blockIdx.x; u0 < nu; u0 += (long long)F::PB * gridDim.x) {
     const bool valid = threadIdx.x < F::TH && u0 + lp < nu;
     const long long pair = valid ? plist_pair(L, lb, pair0, u0 + lp) : 0;
@@ -819,24 +811,19 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *sm /* NV*N
   __syncthreads();
 }
 
-template <bool BT>
+template <class BA>
 __global__ void NP_BOUNDS k_q0_near(bem_dom_dev D, const __grid_constant__ bem_qp q0, const int *__restrict__ near_s,
                                                         const int *__restrict__ near_n, double *G0,
                                                         double *H0, double *__restrict__ nearF, unsigned *status,
-                                                        unsigned long long *terms, bem_bat B) {
-  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...; BT: block
-  // (p, y, b) those of instance b, and instance 0 alone writes the geometric sums
+                                                        unsigned long long *terms, const __grid_constant__ BA B) {
+  // blocks (p, y) take the node's near pairs y, y + gridDim.y, ...; a batch:
+  // block (p, y, b) those of instance b, and instance 0 alone writes the geometric sums
   const int p = blockIdx.x, nn = near_n[p];
   if ((int)blockIdx.y >= nn) return;
-  __shared__ bem_qp qs;
-  double *__restrict__ G = G0, *__restrict__ H = H0;
-  if (BT) {
-    bat_stage(B, blockIdx.z, qs);
-    G = B.G[blockIdx.z];
-    H = B.H[blockIdx.z];
-    if (blockIdx.z) nearF = nullptr;
-  }
-  const bem_qp &q = BT ? qs : q0;
+  const int bz = bat_is<BA>::on ? (int)blockIdx.z : 0;
+  double *__restrict__ G = bat_G(B, bz, G0), *__restrict__ H = bat_H(B, bz, H0);
+  if (bz) nearF = nullptr;
+  const bem_qp &q = bat_q(B, bz, q0);
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
@@ -998,24 +985,20 @@ __device__ __forceinline__ bool self_point(const bem_el &el, const double th[5],
   return rm >= 0.0;
 }
 
-template <bool BT>
+template <class BA>
 __global__ void NP_BOUNDS k_q0_self(bem_dom_dev D, const __grid_constant__ bem_qp q0, double *G0,
                                                         double *H0, double *__restrict__ selfF,
-                                                        unsigned *status, unsigned long long *terms, bem_bat B) {
+                                                        unsigned *status, unsigned long long *terms,
+                                                        const __grid_constant__ BA B) {
   const int p = blockIdx.x;
   const int t = p >> 2, tn = p & 3;
   const int te = abs(D.sid[t]) - 1;
   if (bem_is_tri(D, te)) return;  // k_q0_self_tri
-  // BT: block (p, 0, b) integrates instance b; instance 0 alone writes selfF
-  __shared__ bem_qp qs;
-  double *__restrict__ G = G0, *__restrict__ H = H0;
-  if (BT) {
-    bat_stage(B, blockIdx.z, qs);
-    G = B.G[blockIdx.z];
-    H = B.H[blockIdx.z];
-    if (blockIdx.z) selfF = nullptr;
-  }
-  const bem_qp &q = BT ? qs : q0;
+  // a batch: block (p, 0, b) integrates instance b; instance 0 alone writes selfF
+  const int bz = bat_is<BA>::on ? (int)blockIdx.z : 0;
+  double *__restrict__ G = bat_G(B, bz, G0), *__restrict__ H = bat_H(B, bz, H0);
+  if (bz) selfF = nullptr;
+  const bem_qp &q = bat_q(B, bz, q0);
   extern __shared__ double2 wts_s[];  // BEM_WT_SMEM bytes of dynamic shared memory
   const double2 *wts = bem_wtab_stage(q, wts_s);
   __syncthreads();
@@ -1993,21 +1976,21 @@ static bem_far far_params(const bem_dom_dev *D, const bem_qp *q, int periodic) {
 // empty blocks)
 static int near_grid_y(const bem_dom_dev *D) { return D->near_cap < 32 ? D->near_cap : 32; }
 
-template <bool BT>
+template <class BA>
 static int q0_smem_attrs_bt() {
   const int b = (int)BEM_WT_SMEM;
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (cudaFuncSetAttribute(k_q0_far<10, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<9, BT>, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_far<8, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<7, BT>, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_far<6, BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_regular<BT>, a, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_q0_near<BT>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self<BT>, a, b) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_q0_far<10, BA>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<9, BA>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<8, BA>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_far<7, BA>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_far<6, BA>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_regular<BA>, a, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_q0_near<BA>, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self<BA>, a, b) != cudaSuccess)
     return -1;
   return 0;
 }
 static int q0_smem_attrs() {
   const int b = (int)BEM_WT_SMEM;
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  if (q0_smem_attrs_bt<false>() || q0_smem_attrs_bt<true>()) return -1;
+  if (q0_smem_attrs_bt<bat_none>() || q0_smem_attrs_bt<bem_bat>()) return -1;
   if (cudaFuncSetAttribute(k_q0_regular_tri, a, b) != cudaSuccess || cudaFuncSetAttribute(k_q0_self_tri, a, b) != cudaSuccess)
     return -1;
   return 0;
@@ -2015,27 +1998,27 @@ static int q0_smem_attrs() {
 
 // tier NF's kernel over its list (L.e set: grid_list blocks striding over it)
 // or over the pair range [p0, p0 + np)
-template <int NF, bool BT>
+template <int NF, class BA>
 static void launch_far(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
-                       long long np, bem_plist L, unsigned grid_list, const bem_bat &B, cudaStream_t st) {
+                       long long np, bem_plist L, unsigned grid_list, const BA &B, cudaStream_t st) {
   using F = far_shape<NF>;
   L.type = 1 + F::T;
   const unsigned grid = L.e ? grid_list : (unsigned)((np + F::PB - 1) / F::PB);
   if (grid == 0) return;
-  k_q0_far<NF, BT><<<grid, F::TB, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np, L, B);
+  k_q0_far<NF, BA><<<grid, F::TB, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, p0, np, L, B);
   bem_count_launches(1);
 }
-template <bool BT = false>
+template <class BA = bat_none>
 static void launch_far_tiers(const bem_dom_dev *D, const bem_qp *q, bem_scratch *S, double *G, double *H, long long p0,
                              long long np, const bem_plist &L, unsigned grid_list, cudaStream_t st,
-                             const bem_bat &B = bem_bat{0, nullptr, nullptr, nullptr}) {
-  launch_far<10, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
-  launch_far<9, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
-  launch_far<8, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
-  launch_far<7, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
-  launch_far<6, BT>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+                             const BA &B = BA{}) {
+  launch_far<10>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<9>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<8>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<7>(D, q, S, G, H, p0, np, L, grid_list, B, st);
+  launch_far<6>(D, q, S, G, H, p0, np, L, grid_list, B, st);
 }
-static const bem_bat k_nobat = {0, nullptr, nullptr, nullptr};
+static const bat_none k_nobat = {};
 
 extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int periodic, int exterior, double k,
                                    bem_scratch *S, double *G, double *H, double *dG, double *dH, double *dF,
@@ -2078,7 +2061,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
         return -1;
       const unsigned grid = RP_MINB * (unsigned)nsm, grid_far = FP_MINB * (unsigned)nsm;
       const bem_plist Lreg = {S->plist, S->pcount, 0};
-      k_q0_regular<false><<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg,
+      k_q0_regular<bat_none><<<grid, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms, 0, npairs, Lreg,
                                                                          k_nobat);
       bem_count_launches(1);
       if (D->far_rule) launch_far_tiers(D, q, S, G, H, 0, npairs, Lreg, grid_far, st);
@@ -2091,7 +2074,7 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       const long long chunk = 1LL << 26;  // keep grid.x well inside limits
       for (long long p0 = 0; p0 < npairs; p0 += chunk) {
         const long long np = npairs - p0 < chunk ? npairs - p0 : chunk;
-        k_q0_regular<false><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+        k_q0_regular<bat_none><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                              p0, np, L0, k_nobat);
         bem_count_launches(1);
         if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);
@@ -2103,11 +2086,11 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
       }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    k_q0_near<false><<<dim3(N, near_grid_y(D)), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF,
+    k_q0_near<bat_none><<<dim3(N, near_grid_y(D)), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, G, H, S->nearF,
                                                                               S->status, S->terms, k_nobat);
     bem_count_launches(1);
     if (ev) cudaEventRecord(ev[3], st);
-    k_q0_self<false><<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms, k_nobat);
+    k_q0_self<bat_none><<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms, k_nobat);
     bem_count_launches(1);
     if (D->has_tri) {
       k_q0_self_tri<<<N, NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, G, H, S->selfF, S->status, S->terms);
@@ -2137,19 +2120,19 @@ extern "C" int bem_launch_assemble(const bem_dom_dev *D, const bem_qp *q, int pe
 // The periodic domain of a batch of nb problems on one body, media, lattice
 // and frequency (bem_bat).  One classification, with q (instance 0's
 // parameters: pair flags, rule tiers, lists and geometric sums depend on the
-// geometry, the lattice and k only), then each kernel launched once for all
-// instances: the regular-pair kernels stride over the lists instance after
-// instance, the near-singular and self kernels take the instance from
-// blockIdx.z; the diagonal per instance.  qp_d, G_d, H_d: the batch's arrays on
-// the device; Hh: the H pointers on the host.  Quad meshes with pair lists only
-// (-2 otherwise).
-extern "C" int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, int nb, const bem_qp *qp_d,
-                                         double *const *G_d, double *const *H_d, double *const *Hh, bem_scratch *S,
-                                         double *dF, cudaStream_t st) {
+// geometry, the lattice and k only), then each kernel launched once for up to
+// BEM_BAT_MAX instances: the regular-pair kernels stride over the lists
+// instance after instance, the near-singular and self kernels take the
+// instance from blockIdx.z; the diagonal per instance.  qps, Gh, Hh: the
+// instances' parameters and output pointers, on the host.  Quad meshes with
+// pair lists only (-2 otherwise).
+extern "C" int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, int nb, const bem_qp *qps,
+                                         double *const *Gh, double *const *Hh, bem_scratch *S, double *dF,
+                                         cudaStream_t st) {
   if (q0_smem_attrs()) return -1;
   const int N = D->ne * 4;
   if (D->ne <= 0 || nb <= 0) return 0;
-  if (D->has_tri || nb > 65535) return -2;
+  if (D->has_tri) return -2;
   const long long npairs = (long long)N * D->ne;
   if (!(S->plist && S->pcount && (unsigned long long)npairs <= S->pcap && npairs <= 0xffffffffLL)) return -2;
   if (cudaMemsetAsync(S->pcount, 0, 2 * BEM_NLIST * sizeof(unsigned), st) != cudaSuccess) return -1;
@@ -2162,18 +2145,26 @@ extern "C" int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, 
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0)
     return -1;
-  const bem_bat B = {nb, qp_d, G_d, H_d};
   const bem_plist Lreg = {S->plist, S->pcount, 0};
-  k_q0_regular<true><<<RP_MINB * (unsigned)nsm, RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, nullptr, nullptr, S->status,
-                                                                              S->terms, 0, npairs, Lreg, B);
-  bem_count_launches(1);
-  if (D->far_rule) launch_far_tiers<true>(D, q, S, nullptr, nullptr, 0, npairs, Lreg, FP_MINB * (unsigned)nsm, st, B);
-  k_q0_near<true><<<dim3(N, near_grid_y(D), nb), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->near_s, S->near_n, nullptr,
-                                                                                nullptr, S->nearF, S->status, S->terms, B);
-  bem_count_launches(1);
-  k_q0_self<true><<<dim3(N, 1, nb), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, nullptr, nullptr, S->selfF, S->status,
-                                                                   S->terms, B);
-  bem_count_launches(1);
+  bem_bat B;  // 20 KB on the host stack, copied into each launch's argument block
+  for (int b0 = 0; b0 < nb; b0 += BEM_BAT_MAX) {
+    B.nb = nb - b0 < BEM_BAT_MAX ? nb - b0 : BEM_BAT_MAX;
+    for (int i = 0; i < B.nb; ++i) {
+      B.qp[i] = qps[b0 + i];
+      B.G[i] = Gh[b0 + i];
+      B.H[i] = Hh[b0 + i];
+    }
+    k_q0_regular<bem_bat><<<RP_MINB * (unsigned)nsm, RP_THREADS, BEM_WT_SMEM, st>>>(
+        *D, *q, S->flag, nullptr, nullptr, S->status, S->terms, 0, npairs, Lreg, B);
+    bem_count_launches(1);
+    if (D->far_rule) launch_far_tiers(D, q, S, nullptr, nullptr, 0, npairs, Lreg, FP_MINB * (unsigned)nsm, st, B);
+    k_q0_near<bem_bat><<<dim3(N, near_grid_y(D), B.nb), NP_THREADS, BEM_WT_SMEM, st>>>(
+        *D, *q, S->near_s, S->near_n, nullptr, nullptr, S->nearF, S->status, S->terms, B);
+    bem_count_launches(1);
+    k_q0_self<bem_bat><<<dim3(N, 1, B.nb), NP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, nullptr, nullptr, S->selfF,
+                                                                       S->status, S->terms, B);
+    bem_count_launches(1);
+  }
   for (int b = 0; b < nb; ++b) {
     k_diag<<<(N + 127) / 128, 128, 0, st>>>(*D, 1, S->rowF, S->near_n, S->nearF, S->selfF, Hh[b], dF, S->status);
     bem_count_launches(1);
@@ -2199,7 +2190,7 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
       // the kernels of the assembly itself (over pair ranges, not lists):
       // quad sources, far pairs, and triangle sources when there are any
       const bem_plist L0 = {nullptr, nullptr, 0};
-      k_q0_regular<false><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
+      k_q0_regular<bat_none><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                            p0, np, L0, k_nobat);
       bem_count_launches(1);
       if (D->far_rule) launch_far_tiers(D, q, S, G, H, p0, np, L0, 0, st);

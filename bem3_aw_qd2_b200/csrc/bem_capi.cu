@@ -126,8 +126,9 @@ struct bemgpu_ctx {
   };
   std::vector<batch_inst> bat;
   int bat_cur = -1;
-  bem_qp *bat_qp_d = nullptr;
-  double **bat_G_d = nullptr, **bat_H_d = nullptr;
+  // instance buffers kept between batches (G, H, spectral table; bytes each)
+  struct batch_bufs { double *G = nullptr, *H = nullptr, *stab = nullptr; size_t gh = 0, st = 0; };
+  std::vector<batch_bufs> bat_pool;
 };
 
 
@@ -177,10 +178,7 @@ static void batch_clear(bemgpu_ctx *c) {
   c->G[0] = c->bat[0].G;
   c->H[0] = c->bat[0].H;
   c->qp = c->bat[0].qp;
-  for (size_t b = 1; b < c->bat.size(); ++b) {
-    dfree(c->bat[b].G); dfree(c->bat[b].H); dfree(c->bat[b].stab);
-  }
-  dfree(c->bat_qp_d); dfree(c->bat_G_d); dfree(c->bat_H_d);
+  // instance b >= 1's buffers stay in bat_pool[b - 1] for the next batch
   c->bat.clear();
   c->bat_cur = -1;
 }
@@ -190,6 +188,8 @@ static void batch_clear(bemgpu_ctx *c) {
 static void free_problem(bemgpu_ctx *c, bool release) {
   batch_clear(c);
   if (release) {
+    for (auto &p : c->bat_pool) { dfree(p.G); dfree(p.H); dfree(p.stab); }
+    c->bat_pool.clear();
     dfree(c->cr); dfree(c->cw); dfree(c->ren); dfree(c->wen); dfree(c->plane);
     dfree(c->sid); dfree(c->rowidx); dfree(c->npe); dfree(c->eni); dfree(c->md); dfree(c->dom_ne_d); dfree(c->dom_off_d);
     dfree(c->hk2); dfree(c->Pi); dfree(c->dPi); dfree(c->p_inc); dfree(c->v_inc); dfree(c->rho0_d); dfree(c->k2_d);
@@ -781,32 +781,31 @@ extern "C" int bemgpu_batch_load(bemgpu_ctx *c, int nb, const bemgpu_problem *co
     I.qp.wt_h = c->qp.wt_h;
     I.qp.wt_n = c->qp.wt_n;
     const size_t cnt = stab_window(&I.qp, c->zspan);
+    if ((int)c->bat_pool.size() < b) c->bat_pool.resize(b);
+    bemgpu_ctx::batch_bufs &P = c->bat_pool[b - 1];
     cudaError_t e = cudaSuccess;
-    if (cnt) {
-      e = dalloc(&I.stab, cnt);
-      if (e == cudaSuccess && bem_launch_stab(&I.qp, I.stab, c->stream) != 0) e = cudaGetLastError();
-      I.qp.st = I.stab;
+    if (P.gh < 2 * N * N) {
+      dfree(P.G); dfree(P.H);
+      P.gh = 0;
+      e = dalloc(&P.G, 2 * N * N);
+      if (e == cudaSuccess) e = dalloc(&P.H, 2 * N * N);
+      if (e == cudaSuccess) P.gh = 2 * N * N;
     }
-    if (e == cudaSuccess) e = dalloc(&I.G, 2 * N * N);
-    if (e == cudaSuccess) e = dalloc(&I.H, 2 * N * N);
+    if (e == cudaSuccess && cnt && P.st < cnt) {
+      dfree(P.stab);
+      P.st = 0;
+      e = dalloc(&P.stab, cnt);
+      if (e == cudaSuccess) P.st = cnt;
+    }
+    if (e == cudaSuccess && cnt && bem_launch_stab(&I.qp, P.stab, c->stream) != 0) e = cudaGetLastError();
     if (e != cudaSuccess) {
       batch_clear(c);
       return fail(c, "batch buffers", e);
     }
-  }
-  std::vector<bem_qp> qps(nb);
-  std::vector<double *> gs(nb), hs(nb);
-  for (int b = 0; b < nb; ++b) { qps[b] = c->bat[b].qp; gs[b] = c->bat[b].G; hs[b] = c->bat[b].H; }
-  cudaError_t e = dalloc(&c->bat_qp_d, (size_t)nb);
-  if (e == cudaSuccess) e = dalloc(&c->bat_G_d, (size_t)nb);
-  if (e == cudaSuccess) e = dalloc(&c->bat_H_d, (size_t)nb);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_qp_d, qps.data(), nb * sizeof(bem_qp), cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_G_d, gs.data(), nb * sizeof(double *), cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(c->bat_H_d, hs.data(), nb * sizeof(double *), cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // the host arrays go out of scope
-  if (e != cudaSuccess) {
-    batch_clear(c);
-    return fail(c, "batch tables", e);
+    I.G = P.G;
+    I.H = P.H;
+    I.stab = cnt ? P.stab : nullptr;
+    I.qp.st = I.stab;
   }
   c->bat_cur = 0;
   return 0;
@@ -827,11 +826,12 @@ extern "C" int bemgpu_batch_assemble(bemgpu_ctx *c) {
       return fail(c, "assembly launch", cudaGetLastError());
   }
   const int nb = (int)c->bat.size();
-  std::vector<double *> hs(nb);
-  for (int b = 0; b < nb; ++b) hs[b] = c->bat[b].H;
+  std::vector<bem_qp> qps(nb);
+  std::vector<double *> gs(nb), hs(nb);
+  for (int b = 0; b < nb; ++b) { qps[b] = c->bat[b].qp; gs[b] = c->bat[b].G; hs[b] = c->bat[b].H; }
   bem_dom_dev D = dom_view(c, 0);
-  const int r = bem_launch_assemble_batch(&D, &c->bat[0].qp, nb, c->bat_qp_d, c->bat_G_d, c->bat_H_d, hs.data(),
-                                          &c->scr, c->dF[0], c->stream);
+  const int r = bem_launch_assemble_batch(&D, &c->bat[0].qp, nb, qps.data(), gs.data(), hs.data(), &c->scr, c->dF[0],
+                                          c->stream);
   if (r == -2) { snprintf(c->err, sizeof(c->err), "batch assembly: quad meshes with pair lists only"); return -2; }
   if (r) return fail(c, "batch assembly launch", cudaGetLastError());
   if (c->MN >= 1) {

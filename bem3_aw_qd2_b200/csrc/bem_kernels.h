@@ -36,8 +36,8 @@ struct bem_scratch {
 extern "C" {
 // the periodic domain of nb problems that differ only in the Bloch wave
 // vector, each kernel launched once for all (bem_assemble.cu)
-int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, int nb, const bem_qp *qp_d, double *const *G_d,
-                              double *const *H_d, double *const *Hh, bem_scratch *S, double *dF, cudaStream_t st);
+int bem_launch_assemble_batch(const bem_dom_dev *D, const bem_qp *q, int nb, const bem_qp *qps, double *const *Gh,
+                              double *const *Hh, bem_scratch *S, double *dF, cudaStream_t st);
 int bem_set_constants(const double *xl, const double *wl, const double *xh, const double *wh);
 int bem_launch_faddeeva(const double *z, int n, double *w, cudaStream_t st);
 // table of w(x + i y), y in [0, 8), for the Ewald real-space terms (bem_qp.wt)

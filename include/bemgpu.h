@@ -123,8 +123,8 @@ int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
  * wave vector and incident field).  bemgpu_batch_load checks that, loads
  * probs[0] as bemgpu_load does and keeps every instance's Ewald parameters
  * (its own spectral table) and incident data, with device room for its
- * periodic-domain G and H (32 N_0^2 bytes each); quad meshes of at most 32768
- * elements.  bemgpu_batch_assemble assembles the free-space domains once and
+ * periodic-domain G and H (32 N_0^2 bytes each, kept for the next batch); quad
+ * meshes of at most 32768 elements.  bemgpu_batch_assemble assembles the free-space domains once and
  * the periodic domain of all instances with each kernel launched once (one
  * classification and one set of pair lists; the regular-pair kernels stride
  * over the lists instance after instance, the near-singular and self kernels
