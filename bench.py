@@ -107,6 +107,8 @@ def parse():
     ap.add_argument("--stream-sizes", default="6,10", help="--workload stream: cube-sphere n (6 n^2 quads)")
     ap.add_argument("--sweep-freqs", type=int, default=2, help="--workload sweep: frequencies (of 8)")
     ap.add_argument("--sweep-dirs", type=int, default=8, help="--workload sweep: incidence directions (of 64)")
+    ap.add_argument("--sweep-mesh-n", type=int, default=16,
+                    help="--workload sweep: cube-sphere with 6 n^2 quads (16: the 1536-quad body of the sweep)")
     ap.add_argument("--stream-requests", type=int, default=STREAM_REQUESTS,
                     help="requests of the headline stream in the default line (0: leave it out)")
     ap.add_argument("--lu-sizes", default="1728,4096,12288", help="--workload lu: matrix orders")
@@ -565,7 +567,7 @@ def run_sweep(args, rank, world):
     g.bemgpu_load.argtypes = [ctypes.c_void_p, ctypes.POINTER(api.Problem)]
     g.bemgpu_interior_reuses.argtypes = [ctypes.c_void_p]
     g.bemgpu_interior_reuses.restype = ctypes.c_longlong
-    inst = sweep_instances(args.sweep_freqs, args.sweep_dirs)
+    inst = sweep_instances(args.sweep_freqs, args.sweep_dirs, n=args.sweep_mesh_n)
     cases = [api.Case.from_files(*meshgen.write_inputs(tempfile.mkdtemp(prefix="sweep_"), **r)) for _, r in inst]
     probs = [c.problem() for c in cases]
     ctx = ctypes.c_void_p()
@@ -642,7 +644,7 @@ def run_sweep(args, rank, world):
             "dtype": "f64 assembly, complex-FP32 LU + FP64 refinement", "data": "synthetic",
             "config": {"workload": "sweep", "instances": len(probs), "frequencies": args.sweep_freqs,
                        "directions": args.sweep_dirs, "full_sweep": "64 directions x 8 frequencies (reduced here)",
-                       "mesh": "1536-quad cube-sphere r = 0.3, square lattice 0.8",
+                       "mesh": "%d-quad cube-sphere r = 0.3, square lattice 0.8" % (6 * args.sweep_mesh_n ** 2),
                        "order": "frequency-major: instances at one frequency share the interior domain"},
             "fp64": res["fp64"], "mixed": res["mixed"], "mixed_batched": res["mixed_batched"],
             "force_rel_err_mixed_vs_fp64": {"max": max(errs), "median": float(np.median(errs))}}
