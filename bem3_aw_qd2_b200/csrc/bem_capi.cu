@@ -736,6 +736,7 @@ static bool same_body(const bemgpu_problem *a, const bemgpu_problem *b) {
          !memcmp(a->cw, b->cw, ne * 9 * sizeof(double)) && !memcmp(a->ren, b->ren, ne * 12 * sizeof(double)) &&
          !memcmp(a->wen, b->wen, ne * 12 * sizeof(double)) && !memcmp(a->npe, b->npe, ne * sizeof(int)) &&
          !memcmp(a->eni, b->eni, ne * 4 * sizeof(int)) && !memcmp(a->plane, b->plane, ne) &&
+         !memcmp(a->md, b->md, ne * sizeof(int)) && !memcmp(a->sd, b->sd, ne * sizeof(int)) &&
          !memcmp(a->k0, b->k0, nd * sizeof(double)) && !memcmp(a->k2, b->k2, 2 * nd * sizeof(double)) &&
          !memcmp(a->rho0, b->rho0, nd * sizeof(double)) && !memcmp(a->c0, b->c0, nd * sizeof(double));
 }
