@@ -2188,7 +2188,7 @@ extern "C" int bem_time_regular(const bem_dom_dev *D, const bem_qp *q, bem_scrat
     const long long np = p0 + len <= npairs ? len : npairs - p0;
     if (np > 0) {
       // the kernels of the assembly itself (over pair ranges, not lists):
-      // quad sources, far pairs, and triangle sources when there are any
+      // quad sources, the shorter-rule tiers, and triangle sources when there are any
       const bem_plist L0 = {nullptr, nullptr, 0};
       k_q0_regular<bat_none><<<(unsigned)((np + 1) / 2), RP_THREADS, BEM_WT_SMEM, st>>>(*D, *q, S->flag, G, H, S->status, S->terms,
                                                                            p0, np, L0, k_nobat);

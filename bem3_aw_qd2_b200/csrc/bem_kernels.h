@@ -13,7 +13,7 @@ struct bem_dom_dev {
   const uint8_t *plane;         // 1 if the element is plane (bil_check_plane)
   const int *npe;               // nodes per element: 4 bilinear quad, 3 linear triangle
   int has_tri;                  // any triangle among the domain's elements
-  int far_rule;                 // periodic domain: 8 x 8 rule for far quad pairs (k_q0_far)
+  int far_rule;                 // periodic domain: shorter rules for regular pairs far from every lattice image (k_q0_far)
   int near_cap;                 // near-singular sources one collocation node can hold (<= 256):
                                 // the stride of bem_scratch.near_s / nearF
 };
