@@ -382,7 +382,12 @@ __global__ void __launch_bounds__(128) k_plist_fill(bem_dom_dev D, const uint8_t
 // own G and H.  The batched kernels (BA = bem_bat) read instance b's
 // parameters from the argument block (qp[b], like a single problem's q0) and
 // write G[b], H[b].
-#define BEM_BAT_MAX 32  // instances per launch (the parameters travel in the kernel's argument block)
+#ifndef BEM_BAT_MAX
+// instances per launch: the parameters travel in the kernel's argument block,
+// and the regular-pair kernels unroll their instance loop, so that each copy
+// reads its instance's parameters at fixed offsets (as constant-bank operands)
+#define BEM_BAT_MAX 8
+#endif
 struct bem_bat {
   int nb;
   bem_qp qp[BEM_BAT_MAX];
@@ -400,6 +405,8 @@ __device__ __forceinline__ double *bat_H(const bat_none &, int, double *H0) { re
 __device__ __forceinline__ double *bat_H(const bem_bat &B, int b, double *) { return B.H[b]; }
 template <class BA> struct bat_is { static constexpr bool on = false; };
 template <> struct bat_is<bem_bat> { static constexpr bool on = true; };
+// trip count of a kernel's instance loop (unrolled)
+template <class BA> struct bat_max { static constexpr int n = bat_is<BA>::on ? BEM_BAT_MAX : 1; };
 
 // ------------------------------------------------------------------ periodic regular pairs
 // 2 pairs x 144 points per block; one quasi-periodic Green's function per thread
@@ -422,7 +429,9 @@ __global__ void __launch_bounds__(RP_THREADS, RP_MINB) k_q0_regular(bem_dom_dev 
   const long long nu = plist_units(L, npairs);
   const unsigned long long lb = plist_base(L);
   unsigned long long nterm = 0, npt = 0;
-  for (int b = 0; b < bat_n(B); ++b) {
+#pragma unroll
+  for (int b = 0; b < bat_max<BA>::n; ++b) {
+  if (b >= bat_n(B)) break;
   double *__restrict__ G = bat_G(B, b, G0), *__restrict__ H = bat_H(B, b, H0);
   const bem_qp &q = bat_q(B, b, q0);
   for (long long u0 = 2LL * blockIdx.x; u0 < nu; u0 += 2LL * gridDim.x) {
@@ -619,7 +628,9 @@ __global__ void __launch_bounds__(FP_THREADS, FP_MINB) k_q0_far(bem_dom_dev D, c
   __syncthreads();
   const int lp = threadIdx.x / F::NP, pt = threadIdx.x % F::NP;
   unsigned long long nterm = 0, npt = 0;
-  for (int b = 0; b < bat_n(B); ++b) {
+#pragma unroll
+  for (int b = 0; b < bat_max<BA>::n; ++b) {
+  if (b >= bat_n(B)) break;
   double *__restrict__ G = bat_G(B, b, G0), *__restrict__ H = bat_H(B, b, H0);
   const bem_qp &q = bat_q(B, b, q0);
   for (long long u0 = (long long)F::PB * blockIdx.x; u0 < nu; u0 += (long long)F::PB * gridDim.x) {
