@@ -124,11 +124,12 @@ int bemgpu_autotune(bemgpu_ctx *ctx, double *best_scale);
  * probs[0] as bemgpu_load does and keeps every instance's Ewald parameters
  * (its own spectral table) and incident data, with device room for its
  * periodic-domain G and H (32 N_0^2 bytes each, kept for the next batch); quad
- * meshes of at most 32768 elements.  bemgpu_batch_assemble assembles the free-space domains once and
- * the periodic domain of all instances with each kernel launched once (one
- * classification and one set of pair lists; the regular-pair kernels stride
- * over the lists instance after instance, the near-singular and self kernels
- * take the instance from the grid).  bemgpu_batch_select(ctx, b) makes
+ * meshes of at most 32768 elements.  bemgpu_batch_assemble assembles the
+ * free-space domains once and the periodic domain of all instances with each
+ * kernel launched once per 8 instances (one classification and one set of
+ * pair lists; the regular-pair kernels stride over the lists instance after
+ * instance, the near-singular and self kernels take the instance from the
+ * grid).  bemgpu_batch_select(ctx, b) makes
  * instance b the context's problem: bemgpu_solve, bemgpu_force,
  * bemgpu_get_solution, bemgpu_get_matrix and the field functions then act on
  * it (the interior domains' dpv factors made by the first solve serve every
